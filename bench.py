@@ -1,0 +1,391 @@
+"""Benchmark of the WaveQ3D engine: ray-steps/s on the sloped Rayleigh workload.
+
+Workload (one bench "step" = one complete propagation of it): linear
+gradient profile 1500 + 0.0163 z m/s with Thorp attenuation, bottom sloping
+from 200 m at the source to 2000 m at 20 km (boundary_slope), Rayleigh
+bottom (1.5, 1.1, 0.5 dB/wavelength), 50 m source, 5 frequencies 100 Hz -
+3 kHz, 1801 D/E x 91 AZ rays (wrapping AZ fan), dt 0.05 s for 40 s (800
+wave_queue steps), 1024 targets on a 32 x 32 range/depth grid.  Inputs are
+synthetic (generated, no data files).
+
+value: whole-job ray-steps/s with the workload resident in HBM, timed with
+CUDA events on the engine's stream around the 800 steps.  e2e: the same
+metric through the public API with host buffers (queue creation from host
+arrays, propagation, eigenray records read back).  roofline: the CPA kernel
+(the dominant kernel) in FP64 operations against an FP64 throughput peak
+measured on this GPU by bench.py itself.  cpu_baseline: the CPU oracle (a
+restatement of the reference's CPU wave_queue) on a bounded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "ray-steps/s"
+WORKLOAD = "linear_slope_rayleigh_1801x91_1024tgt_5f_dt0.05_40s"
+
+# algorithmic work of the CPA search per (ray, target) pair and step: the
+# reference's distance2 (wave_front.cc:222-236: 15 FP64 operations) plus the
+# two time comparisons of detect_eigenrays (wave_queue.cc:386-393)
+FLOPS_PER_RAY_TARGET_STEP = 17
+# FP64 bytes the CPA kernel must read per interior ray and launch: four
+# distance2 terms (rho, theta, phi, sin theta) on three fronts plus on_edge
+BYTES_PER_RAY_CPA = 3 * 4 * 8 + 1
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=40)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- FP64 peak
+FP64_PEAK_SRC = r"""
+extern "C" __global__ void fp64_peak(double* out, int iters) {
+    double a = threadIdx.x * 1e-3, b = 1.0000001, c = 0.9999999, d = blockIdx.x * 1e-6;
+    double e = a + 1.0, f = d + 2.0, g = a * 0.5, h = d * 0.25;
+    for (int i = 0; i < iters; ++i) {
+        a = a * b + c; d = d * b + c; e = e * b + c; f = f * b + c;
+        g = g * b + c; h = h * b + c;
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = a + d + e + f + g + h;
+}
+"""
+
+
+# ---------------------------------------------------------------- engine arm
+def engine_arm(args, rank, world, dist):
+    import underseamodelinglibrary_b200 as u
+    from underseamodelinglibrary_b200 import scenarios as S
+
+    sc = S.linear_slope_rayleigh()
+    nde, naz = sc["de"].size(), sc["az"].size()
+    nt = sc["targets"].size1() * sc["targets"].size2()
+    # steps of one propagation: the reference loop "while (time() < 40) step()"
+    nsteps, t = 0, 0.0
+    while t < sc["time_max"]:
+        t += sc["dt"]
+        nsteps += 1
+    ray_steps = nde * naz * nsteps
+
+    def make():
+        return S.build_queue(sc, u.wave_queue, device=0)
+
+    # device-resident timing: queues built (inputs in HBM) before the timer
+    for _ in range(args.warmup):
+        q = make()
+        q.run(sc["time_max"])
+        q.take_eigenrays()
+        del q
+    queues = [make() for _ in range(args.steps)]
+    for q in queues:
+        q.set_timing(True)
+        q.timing(reset=True)
+    clocks = ClockSampler(rank)
+    clocks.start()
+    if dist is not None:
+        dist.barrier()
+    total_ms, cpa_ms, step_ms, eig_ms, launches, n_eig = 0.0, 0.0, 0.0, 0.0, 0, 0
+    for q in queues:
+        q.run(sc["time_max"])
+        tm = q.timing()
+        total_ms += tm["total_ms"]
+        cpa_ms += tm["cpa_ms"]
+        step_ms += tm["step_ms"]
+        eig_ms += tm["eigenray_ms"]
+        launches += tm["launches"]
+        n_eig += len(q.take_eigenrays())
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    del queues
+
+    # end to end through the public API with host buffers
+    e2e_times = []
+    h2d = d2h = 0
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        q = make()
+        q.run(sc["time_max"])
+        rays = q.take_eigenrays()
+        del q
+        e2e_times.append(time.perf_counter() - t0)
+        nf = sc["freq"].size()
+        h2d = 8 * (nf + 2 * nde + 2 * naz + 3 * nt) + 8 * 3
+        d2h = len(rays) * (96 + 16 * nf)
+
+    total_s = total_ms / 1000.0
+    e2e_s = sum(e2e_times)
+    if dist is not None:
+        import torch
+        tt = torch.tensor([total_s, e2e_s], dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_s, e2e_s = float(tt[0]), float(tt[1])
+    value = world * args.steps * ray_steps / total_s
+    e2e = world * args.steps * ray_steps / e2e_s
+
+    # roofline of the CPA kernel: algorithmic FP64 operations per launch
+    interior = (nde - 2) * ((naz - 1) if _wraps(sc["az"]) else (naz - 2))
+    launches_cpa = args.steps * nsteps
+    cpa_launch_s = (cpa_ms / 1000.0) / launches_cpa
+    flops_launch = FLOPS_PER_RAY_TARGET_STEP * interior * nt
+    achieved = flops_launch / cpa_launch_s / 1e12
+    fp64_peak = measure_fp64_peak_cupyless()
+    out = {
+        "metric": METRIC, "value": value, "unit": "ray-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rays": nde * naz, "num_de": nde, "num_az": naz,
+                   "targets": nt, "frequencies": sc["freq"].size(), "wave_steps": nsteps,
+                   "form": "FP64", "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "working set (4 fronts, %.0f MB) exceeds L2" % (nde * naz * 4 * 30 * 8 / 1e6)},
+        "eigenrays_per_s": world * n_eig / total_s,
+        "e2e": {"value": e2e, "unit": "ray-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "kernel_ms": {"step+edges": step_ms / args.steps, "cpa": cpa_ms / args.steps,
+                      "eigenray": eig_ms / args.steps},
+        "roofline": {"bound": "fp64", "achieved": achieved,
+                     "peak": fp64_peak["tflops"] if fp64_peak else None,
+                     "unit": "TFLOP/s",
+                     "frac": (achieved / fp64_peak["tflops"]) if fp64_peak else None,
+                     "traffic": None,
+                     "kernel": "k_cpa",
+                     "peak_source": fp64_peak["source"] if fp64_peak else "unavailable",
+                     "algorithmic_flops_per_launch": flops_launch},
+        "roofline_hbm": hbm_roofline(interior, cpa_launch_s),
+        "clocks": clk,
+    }
+    return out
+
+
+def _wraps(az):
+    a0, a1 = abs(az[0]), abs(az[az.size() - 1])
+    return math.fmod(a0 + 360.0, 360.0) == math.fmod(a1 + 360.0, 360.0)
+
+
+def hbm_roofline(interior, launch_s):
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs")
+    src = "measured (MEASURED_PEAKS.json)" if peak else "fallback 6650 GB/s"
+    peak = peak or 6650.0
+    achieved = interior * BYTES_PER_RAY_CPA / launch_s / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_source": src}
+
+
+def measure_fp64_peak_cupyless():
+    """FP64 FMA throughput measured with a small CUDA kernel built by nvcc
+    (6 independent FMA chains per thread, 148 x 8 blocks of 256 threads)."""
+    import ctypes as C
+    import tempfile
+    src = FP64_PEAK_SRC + r"""
+#include <cuda_runtime.h>
+extern "C" float run_peak(int iters) {
+    double* out; cudaMalloc(&out, 148 * 8 * 256 * sizeof(double));
+    cudaEvent_t a, b; cudaEventCreate(&a); cudaEventCreate(&b);
+    fp64_peak<<<148 * 8, 256>>>(out, 100);
+    cudaEventRecord(a);
+    fp64_peak<<<148 * 8, 256>>>(out, iters);
+    cudaEventRecord(b); cudaEventSynchronize(b);
+    float ms = 0; cudaEventElapsedTime(&ms, a, b);
+    cudaFree(out); cudaEventDestroy(a); cudaEventDestroy(b);
+    return ms;
+}
+"""
+    try:
+        d = tempfile.mkdtemp()
+        cu = os.path.join(d, "peak.cu")
+        so = os.path.join(d, "peak.so")
+        open(cu, "w").write(src)
+        subprocess.check_call(["nvcc", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+                               "-Xcompiler", "-fPIC", "-o", so, cu], stdout=subprocess.DEVNULL,
+                              stderr=subprocess.DEVNULL)
+        lib = C.CDLL(so)
+        lib.run_peak.restype = C.c_float
+        iters = 20000
+        ms = lib.run_peak(iters)
+        flops = 148 * 8 * 256 * iters * 6 * 2
+        return {"tflops": flops / (ms / 1e3) / 1e12,
+                "source": "measured by bench.py (FP64 FMA loop; MEASURED_PEAKS.json has no FP64 figure)"}
+    except Exception as e:  # noqa: BLE001
+        return {"tflops": None, "source": "unavailable: %s" % e}
+
+
+# ---------------------------------------------------------------- CPU arms
+def cpu_sample_scenario(sample_steps):
+    """A bounded sample of the same workload: the full 1801-ray D/E fan on
+    every 16th AZ column of the 91-ray fan (6 columns), all 1024 targets,
+    the first ``sample_steps`` wave_queue steps."""
+    from underseamodelinglibrary_b200 import scenarios as S
+    from underseamodelinglibrary_b200 import types as T
+    sc = S.linear_slope_rayleigh()
+    sc["az"] = T.seq_linear(0.0, 64.0, 6)
+    sc["time_max"] = sample_steps * sc["dt"] - 0.5 * sc["dt"]
+    return sc
+
+
+def cpu_run(sc, nthreads):
+    """Runs ``nthreads`` independent oracle queues concurrently (the
+    reference's thread_pool model: one wave_queue per worker)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_binding import OracleQueue
+    from underseamodelinglibrary_b200 import scenarios as S
+    queues = [S.build_queue(sc, OracleQueue) for _ in range(nthreads)]
+    done = [0] * nthreads
+
+    def work(i):
+        done[i] = queues[i].run(sc["time_max"])
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(nthreads)]
+    t0 = time.perf_counter()
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    dt = time.perf_counter() - t0
+    rays = sc["de"].size() * sc["az"].size()
+    return sum(done) * rays / dt, dt, done[0]
+
+
+def cpu_baseline(args):
+    sc = cpu_sample_scenario(args.cpu_sample_steps)
+    v, dt, n = cpu_run(sc, 1)
+    return {"value": v, "unit": "ray-steps/s", "cores": 1, "kind": "port",
+            "sample": "oracle (CPU restatement of the reference wave_queue), 1 thread: full 1801-ray "
+                      "D/E fan x every 16th AZ column (6 columns), all 1024 targets, first %d of 800 "
+                      "steps; %.1f s" % (n, dt)}
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return None
+    ncores = os.cpu_count() or 1
+    sc = cpu_sample_scenario(max(4, args.cpu_sample_steps // 4))
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        cpu_run(cpu_sample_scenario(2), ncores)
+    vals = []
+    for _ in range(args.steps):
+        v, dt, n = cpu_run(sc, ncores)
+        vals.append(v)
+    value = statistics.mean(vals)
+    return {"metric": METRIC, "value": value, "unit": "ray-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample": "every 16th AZ column, first %d steps" % n},
+            "cpu_baseline": {"value": value, "unit": "ray-steps/s", "cores": ncores, "kind": "port",
+                             "sample": "oracle restatement of the reference CPU wave_queue, %d "
+                                       "concurrent queues (thread_pool model), full D/E fan x 6 AZ "
+                                       "columns, 1024 targets, first %d steps" % (ncores, n)},
+            "e2e": {"value": value, "unit": "ray-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        tdist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    if args.impl == "reference":
+        out = reference_arm(args, rank)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    if world > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    out = engine_arm(args, rank, world, dist)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,356 @@
+/*
+ * wq3d.h -- C ABI of the B200-native WaveQ3D wavefront propagation engine.
+ *
+ * This is the drop-in boundary for USML's WaveQ3D propagator.  Every entry
+ * point below replaces one piece of the reference C++ interface; the
+ * reference location is cited beside each declaration (paths are relative
+ * to the USML source tree).  The ABI uses only plain C types: no C++
+ * exceptions, no torch types and no CUDA types cross it.  Every function
+ * returns an int status: WQ3D_OK (0) on success, a negative WQ3D_ERR_* code
+ * otherwise; wq3d_last_error_string() then describes the failure.
+ *
+ * Coordinates follow USML's spherical earth system (types/wposition.h):
+ *   rho   = distance from the earth's centre (m),
+ *   theta = colatitude (rad),  phi = longitude (rad).
+ * Ray fan angles are in degrees (D/E positive up, AZ clockwise from north),
+ * exactly as the reference seq_vector fans hold them.
+ *
+ * Device memory is owned by the library.  Host arrays passed in are copied
+ * during the call; the caller keeps ownership of them.
+ */
+#ifndef WQ3D_H
+#define WQ3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WQ3D_ABI_VERSION 1
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                        */
+/* ------------------------------------------------------------------ */
+enum {
+    WQ3D_OK = 0,
+    WQ3D_ERR_INVALID = -1,     /* bad argument (reference: std::invalid_argument) */
+    WQ3D_ERR_CUDA = -2,        /* CUDA runtime failure or no device          */
+    WQ3D_ERR_NOMEM = -3,       /* device or host allocation failed            */
+    WQ3D_ERR_OVERFLOW = -4,    /* a result buffer was too small               */
+    WQ3D_ERR_TIMEOUT = -5,     /* a bounded device wait gave up               */
+    WQ3D_ERR_UNSUPPORTED = -6, /* option not built into this library          */
+    WQ3D_ERR_NUMERIC = -7,     /* a kernel's own bounds/iteration check fired */
+    WQ3D_ERR_ABORTED = -8      /* caller's cancellation flag was set          */
+};
+
+/* ------------------------------------------------------------------ */
+/* ocean description (replaces ocean/ocean_model.h:31-124)             */
+/* ------------------------------------------------------------------ */
+
+/* sound speed profiles: ocean/profile_{linear,munk,catenary,n2,grid}.h */
+enum {
+    WQ3D_PROFILE_LINEAR = 0,   /* p = {c0, g0, z1, g1}      profile_linear.cc:14-40   */
+    WQ3D_PROFILE_MUNK = 1,     /* p = {axis_depth, scale, axis_speed, epsilon}
+                                                          profile_munk.cc:19-32     */
+    WQ3D_PROFILE_CATENARY = 2, /* p = {c1, g1, z1}        profile_catenary.cc:14-29 */
+    WQ3D_PROFILE_N2 = 3,       /* p = {c0, g0}            profile_n2.cc:14-24       */
+    WQ3D_PROFILE_GRID = 4      /* gen_grid over (rho[,theta[,phi]])  profile_grid.h:68-130 */
+};
+
+/* attenuation models: ocean/attenuation_{thorp,constant}.cc */
+enum {
+    WQ3D_ATTEN_THORP = 0,      /* default of profile_model (profile_model.h:40-47) */
+    WQ3D_ATTEN_CONSTANT = 1    /* coef * distance * frequency                      */
+};
+
+/* boundary height models: ocean/boundary_{flat,slope,grid}.h */
+enum {
+    WQ3D_BOUNDARY_FLAT = 0,    /* boundary_flat.cc:19-63  */
+    WQ3D_BOUNDARY_SLOPE = 1,   /* boundary_slope.cc:13-68 */
+    WQ3D_BOUNDARY_GRID = 2     /* boundary_grid.h:88-196  */
+};
+
+/* reflection loss models: ocean/reflect_loss_{constant,rayleigh,eckart}.h */
+enum {
+    WQ3D_LOSS_DEFAULT = -1,    /* the boundary's own default (boundary_model.h:77-90,
+                                  boundary_flat.cc:19-31)                           */
+    WQ3D_LOSS_CONSTANT = 0,    /* p = {amplitude_dB, phase_rad}                     */
+    WQ3D_LOSS_RAYLEIGH = 1,    /* p = {density, speed, att_bottom, speed_shear, att_shear}
+                                  (ratios to water, dB/wavelength)
+                                  reflect_loss_rayleigh.cc:68-144                   */
+    WQ3D_LOSS_ECKART = 2       /* p = {wind_speed}        reflect_loss_eckart.h:76-85 */
+};
+
+/* interpolation per grid axis (types/data_grid.h interp_enum) */
+enum {
+    WQ3D_INTERP_NEAREST = -1,
+    WQ3D_INTERP_LINEAR = 0,
+    WQ3D_INTERP_PCHIP = 1
+};
+
+/* N-dimensional rectilinear grid (types/gen_grid.h:83-520).  Data is
+ * row-major with the last axis fastest (types/data_grid.h:47-61). */
+typedef struct wq3d_grid_desc {
+    int ndim;                  /* 0 = unused, else 1..3 */
+    const double* axis[3];     /* axis values, monotonic */
+    size_t axis_size[3];
+    const double* data;        /* prod(axis_size) values */
+    int interp[3];             /* WQ3D_INTERP_* per axis */
+    int edge_limit[3];         /* nonzero: clamp outside the axis range */
+} wq3d_grid_desc;
+
+typedef struct wq3d_profile_desc {
+    int kind;                  /* WQ3D_PROFILE_* */
+    double p[4];
+    int flat_earth;            /* profile_model::flat_earth() (profile_model.cc:14-26) */
+    int attenuation;           /* WQ3D_ATTEN_* */
+    double attenuation_coef;   /* WQ3D_ATTEN_CONSTANT coefficient */
+    wq3d_grid_desc grid;       /* WQ3D_PROFILE_GRID sound speed (m/s) */
+} wq3d_profile_desc;
+
+typedef struct wq3d_reflect_loss_desc {
+    int kind;                  /* WQ3D_LOSS_* */
+    double p[5];
+} wq3d_reflect_loss_desc;
+
+typedef struct wq3d_boundary_desc {
+    int kind;                  /* WQ3D_BOUNDARY_* */
+    double depth;              /* flat: depth (m, 0 = ocean surface); slope: depth
+                                  at the reference location */
+    double location[3];        /* slope: reference location (rho, theta, phi) */
+    double lat_slope;          /* slope: radians */
+    double lng_slope;          /* slope: radians */
+    wq3d_grid_desc grid;       /* grid: boundary rho over (theta[, phi]) */
+    wq3d_reflect_loss_desc loss;
+} wq3d_boundary_desc;
+
+typedef struct wq3d_ocean_desc {
+    /* value of wposition::earth_radius when the boundaries were built; the
+     * reference bakes it into boundary heights at construction time
+     * (boundary_flat.cc:19-21, boundary_slope.cc:13-20) */
+    double earth_radius;
+    wq3d_profile_desc profile;
+    wq3d_boundary_desc surface;
+    wq3d_boundary_desc bottom;
+} wq3d_ocean_desc;
+
+typedef struct wq3d_ocean wq3d_ocean;
+
+/* Builds a device-resident ocean.  Replaces ocean_model::ocean_model
+ * (ocean/ocean_model.h:31-60) together with the profile/boundary ctors. */
+int wq3d_ocean_create(const wq3d_ocean_desc* desc, wq3d_ocean** out);
+int wq3d_ocean_destroy(wq3d_ocean* ocean);
+
+/* Evaluates the sound speed profile at n points on the GPU.  Replaces
+ * profile_model::sound_speed (ocean/profile_model.h:71-72).  grad may be
+ * NULL, else it receives 3*n values (rho, theta, phi blocks). */
+int wq3d_ocean_sound_speed(const wq3d_ocean* ocean, double earth_radius,
+                           size_t n, const double* rho, const double* theta,
+                           const double* phi, double* speed, double* grad);
+
+/* Evaluates a boundary height and normal at n points on the GPU.
+ * which = 0 surface, 1 bottom.  Replaces boundary_model::height
+ * (ocean/boundary_model.h:109-121).  normal may be NULL (else 3*n). */
+int wq3d_ocean_height(const wq3d_ocean* ocean, int which, size_t n,
+                      const double* rho, const double* theta,
+                      const double* phi, double* height, double* normal);
+
+/* Evaluates a boundary's reflection loss at n grazing angles for nf
+ * frequencies on the GPU.  Replaces boundary_model::reflect_loss
+ * (ocean/boundary_model.h:144-150).  amplitude and phase hold n*nf values. */
+int wq3d_ocean_reflect_loss(const wq3d_ocean* ocean, int which, size_t n,
+                            const double* rho, const double* theta,
+                            const double* phi, const double* grazing,
+                            size_t nf, const double* freq, double* amplitude,
+                            double* phase);
+
+/* ------------------------------------------------------------------ */
+/* wave queue (replaces waveq3d/wave_queue.h:122-264)                  */
+/* ------------------------------------------------------------------ */
+
+enum { WQ3D_CLASSIC_RAY = 0, WQ3D_HYBRID_GAUSSIAN = 1 }; /* wave_queue.h:90 */
+enum { WQ3D_FP64 = 0, WQ3D_FP32C = 1 };                   /* arithmetic form */
+
+typedef struct wq3d_queue_desc {
+    const double* freq;        /* frequencies (Hz), seq_vector freq       */
+    size_t num_freq;
+    double source[3];          /* rho, theta, phi of the source (wposition1) */
+    const double* de;          /* D/E fan values (deg), seq_vector de     */
+    const double* de_inc;      /* seq_vector::increment(i) for each i     */
+    size_t num_de;
+    const double* az;          /* AZ fan values (deg)                     */
+    const double* az_inc;
+    size_t num_az;
+    double time_step;          /* seconds                                 */
+    const double* targets;     /* 3*num_targets1*num_targets2 doubles: all rho,
+                                  then all theta, then all phi (row-major
+                                  t1,t2), or NULL for no eigenrays        */
+    size_t num_targets1;
+    size_t num_targets2;
+    int spreading;             /* WQ3D_CLASSIC_RAY or WQ3D_HYBRID_GAUSSIAN */
+    int precision;             /* WQ3D_FP64 or WQ3D_FP32C                  */
+    double earth_radius;       /* wposition::earth_radius while propagating */
+    size_t eigenray_capacity;  /* device records kept per step chunk; 0 = default */
+    int device;                /* CUDA device ordinal                     */
+    uint64_t run_id;           /* wave_queue::runID                       */
+} wq3d_queue_desc;
+
+typedef struct wq3d_thresholds {   /* waveq3d/wave_thresholds.h:38-199 */
+    double intensity;          /* dB, stored as abs() like the reference  */
+    double eigenverb;          /* dB, stored as abs()                     */
+    int max_bottom;
+    int max_surface;
+    int max_caustic;
+    int max_upper;
+    int max_lower;
+} wq3d_thresholds;
+
+/* One acoustic path (eigenrays/eigenray_model.h:24-102) plus the CPA
+ * bracket (step, de, az) that found it, which the reference does not
+ * record.  intensity[] and phase[] (num_freq values each) travel beside it. */
+typedef struct wq3d_eigenray {
+    double time;
+    double source_de;
+    double source_az;
+    double target_de;
+    double target_az;
+    int32_t surface;
+    int32_t bottom;
+    int32_t caustic;
+    int32_t upper;
+    int32_t lower;
+    int32_t t1;
+    int32_t t2;
+    int32_t de;
+    int32_t az;
+    int32_t pad;
+    int64_t step;
+} wq3d_eigenray;
+
+/* One boundary collision (waveq3d/reflection_listener.h:46-49). */
+typedef struct wq3d_reflection {
+    double time;
+    double dt;
+    double grazing;
+    double speed;
+    double position[3];        /* rho, theta, phi */
+    double ndirection[3];
+    int32_t de;
+    int32_t az;
+    int32_t type;              /* 0 bottom, 1 surface (eigenverb_model.h:42-47) */
+    int32_t pad;
+    int64_t step;
+} wq3d_reflection;
+
+/* Listener callbacks, invoked on the calling thread inside wq3d_queue_step
+ * in reference order: for every completed step, add_eigenray for each path
+ * in (t1, t2, de, az) order (wave_queue.cc:361-373) and then one
+ * check_eigenrays (wave_queue.cc:191).  Replaces eigenray_listener
+ * (eigenrays/eigenray_listener.h:41-53) and reflection_listener. */
+typedef struct wq3d_callbacks {
+    void (*add_eigenray)(void* ctx, size_t t1, size_t t2,
+                         const wq3d_eigenray* ray, const double* intensity,
+                         const double* phase, size_t num_freq,
+                         uint64_t run_id);
+    void (*check_eigenrays)(void* ctx, double time, uint64_t run_id);
+    void (*reflect)(void* ctx, const wq3d_reflection* reflection);
+} wq3d_callbacks;
+
+/* Host copy of one wavefront (waveq3d/wave_front.h:152-258).  Every pointer
+ * is optional (NULL = skip); arrays are num_de*num_az, row-major (de, az),
+ * attenuation/phase are num_de*num_az*num_freq with frequency fastest. */
+typedef struct wq3d_front_view {
+    double* rho;
+    double* theta;
+    double* phi;
+    double* pos_grad[3];
+    double* ndir[3];
+    double* ndir_grad[3];
+    double* sound_speed;
+    double* sound_grad[3];
+    double* distance;
+    double* path_length;
+    double* attenuation;
+    double* phase;
+    int32_t* surface;
+    int32_t* bottom;
+    int32_t* caustic;
+    int32_t* upper;
+    int32_t* lower;
+    uint8_t* on_edge;
+} wq3d_front_view;
+
+enum { WQ3D_FRONT_PAST = 0, WQ3D_FRONT_PREV = 1, WQ3D_FRONT_CURR = 2,
+       WQ3D_FRONT_NEXT = 3 };                /* wave_queue.h:179-216 */
+
+typedef struct wq3d_queue wq3d_queue;
+
+/* Builds the queue and runs the RK3 start-up on the GPU.  Replaces
+ * wave_queue::wave_queue (wave_queue.h:122-126, wave_queue.cc:30-98),
+ * including the 0.1 m source clamp (wave_queue.cc:58-68). */
+int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* desc,
+                      wq3d_queue** out);
+int wq3d_queue_destroy(wq3d_queue* q);
+
+/* Replaces the wave_thresholds setters (wave_thresholds.h:54-182). */
+int wq3d_queue_set_thresholds(wq3d_queue* q, const wq3d_thresholds* t);
+
+/* Replaces add/remove_*_listener (eigenray_notifier.h:41-70,
+ * reflection_notifier.h).  NULL callbacks = no listeners. */
+int wq3d_queue_set_callbacks(wq3d_queue* q, const wq3d_callbacks* cb,
+                             void* ctx);
+
+/* Advances nsteps calls of wave_queue::step() (wave_queue.cc:155-192).
+ * Callbacks fire before it returns. */
+int wq3d_queue_step(wq3d_queue* q, size_t nsteps);
+
+/* Advances while time() < time_max, the loop every reference caller uses
+ * (wavegen/wavefront_generator.cc:98-112).  *steps_done may be NULL. */
+int wq3d_queue_run(wq3d_queue* q, double time_max, size_t* steps_done);
+
+/* Read-only state: wave_queue::time(), source_pos(), num_de/az. */
+int wq3d_queue_time(const wq3d_queue* q, double* time);
+int wq3d_queue_source(const wq3d_queue* q, double* rho_theta_phi);
+int wq3d_queue_steps(const wq3d_queue* q, int64_t* steps);
+
+/* Copies one front (wave_queue::curr()/next()/prev()/past()) to the host. */
+int wq3d_queue_get_front(wq3d_queue* q, int which,
+                         const wq3d_front_view* view);
+
+/* Eigenrays found so far and not yet taken, in reference order.  With
+ * rays == NULL only *count is returned.  Taken records are removed. */
+int wq3d_queue_take_eigenrays(wq3d_queue* q, wq3d_eigenray* rays,
+                              double* intensity, double* phase,
+                              size_t capacity, size_t* count);
+
+/* Cooperative cancellation, polled between step chunks
+ * (thread_task::abort, wavegen/wavefront_generator.cc:55-58,100-108). */
+int wq3d_queue_abort(wq3d_queue* q);
+
+/* Device time (ms, CUDA events on the queue's stream) accumulated since
+ * the last reset: whole wq3d_queue_step/run calls (ms_total, including the
+ * host's result handling between chunks) and, while per-kernel timing is
+ * on, the step/edge, CPA and eigenray kernels; plus the number of kernel
+ * launches.  No reference counterpart: benchmarking aid. */
+int wq3d_queue_timing(wq3d_queue* q, double* ms_total, double* ms_step_kernels,
+                      double* ms_cpa_kernel, double* ms_eigenray_kernel,
+                      int64_t* launches, int reset);
+
+/* Turns per-kernel CUDA-event timing on (direct launches, events around
+ * every kernel) or off (chunks replayed as one CUDA graph, the default).
+ * No reference counterpart: benchmarking aid. */
+int wq3d_queue_set_timing(wq3d_queue* q, int on);
+
+/* ------------------------------------------------------------------ */
+/* misc                                                                */
+/* ------------------------------------------------------------------ */
+const char* wq3d_last_error_string(void);
+int wq3d_abi_version(void);
+int wq3d_device_count(int* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WQ3D_H */

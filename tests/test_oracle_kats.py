@@ -1,0 +1,172 @@
+"""Pins the CPU oracle to the reference's own known-answer tests.
+
+Each case rebuilds a scenario of waveq3d/test/*.cc and checks the oracle
+against the analytic values and tolerances those tests assert.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import underseamodelinglibrary_b200 as u
+from underseamodelinglibrary_b200 import scenarios as S
+from oracle_binding import OracleQueue
+
+
+def run(sc, **kw):
+    q = S.build_queue(sc, OracleQueue, **kw)
+    q.run(sc["time_max"])
+    return q
+
+
+def test_eigenray_basic():
+    """eigenray_test.cc:86-198"""
+    q = run(S.eigenray_basic())
+    rays = q.take_eigenrays()
+    assert len(rays) == 3
+    exp = [(66.9506, 0.1, 1.484018789, 0.002, 0.0, -0.01, 0.01, 0.01),
+           (69.5211, 0.1, 1.995102731, 0.002, -math.pi, 41.93623171, -41.93623171, 0.01),
+           (73.2126, 4.0, 3.051676949, 0.02, 0.0, None, None, None)]
+    for r, (tl, tl_tol, t, t_tol, ph, sde, tde, de_tol) in zip(rays, exp):
+        assert abs(r.intensity[0] - tl) < tl_tol
+        assert abs(r.travel_time - t) < t_tol
+        assert abs(r.phase[0] - ph) < 1e-6
+        if sde is not None:
+            assert abs(r.source_de - sde) < de_tol
+            assert abs(r.target_de - tde) < de_tol
+        assert abs(r.source_az) < 1e-6
+        assert abs(r.target_az) < 1e-6
+
+
+def test_eigenray_concave():
+    """eigenray_test.cc:232-332: four paths at 1.2 deg, times within 20 us"""
+    q = run(S.eigenray_concave())
+    rays = q.take_eigenrays()
+    assert len(rays) == 4
+    for r in rays:
+        if r.surface == 0:
+            th = (89.05102557, -0.578554378, 0.621445622)
+        elif r.source_de > 0.0:
+            th = (89.05369537, 0.337347599, 0.406539112)
+        elif r.source_de > -0.1:
+            th = (89.05379297, -0.053251329, 0.233038477)
+        else:
+            th = (89.05320459, -0.433973977, -0.48969753)
+        assert abs(r.travel_time - th[0]) < 2e-5
+        assert abs(r.source_de - th[1]) < 0.05
+        assert abs(r.target_de - th[2]) < 0.10
+
+
+def test_eigenray_branch_pt():
+    """eigenray_test.cc:428-534: exactly three paths per target, with the
+    eigenray_basic values on the 2226 m ring"""
+    q = run(S.eigenray_branch_pt())
+    rays = q.take_eigenrays()
+    assert len(rays) == 3 * 14
+    by_target = {}
+    for r in rays:
+        by_target.setdefault(r.t1, []).append(r)
+    for t in range(12):
+        lst = by_target[t]
+        assert len(lst) == 3
+        if t > 1:
+            r0, r1, r2 = lst
+            assert abs(r0.intensity[0] - 66.9506) < 0.1
+            assert abs(r0.travel_time - 1.484018789) < 0.002
+            assert abs(r0.phase[0]) < 1e-6
+            assert abs(r0.source_de + 0.01) < 0.01
+            assert abs(r0.target_de - 0.01) < 0.01
+            assert abs(r1.intensity[0] - 69.5211) < 0.1
+            assert abs(r1.travel_time - 1.995102731) < 0.002
+            assert abs(r1.phase[0] + math.pi) < 1e-6
+            assert abs(r1.source_de - 41.93623171) < 0.01
+            assert abs(r1.target_de + 41.93623171) < 0.01
+            assert abs(r2.travel_time - 3.051676949) < 0.02
+            assert abs(r2.phase[0]) < 1e-6
+            assert abs(r2.source_de + 60.91257162) < 1.0
+            assert abs(r2.target_de - 60.91257162) < 1.0
+
+
+def test_refraction_munk_range():
+    """refraction_test.cc:827-980: cycle ranges within 0.01 %, one upper and
+    one lower vertex per cycle"""
+    sc = S.refraction_munk_range()
+    q = S.build_queue(sc, OracleQueue)
+    de = sc["de"]
+    nde = de.size()
+    loop = np.zeros(nde)
+    up = np.zeros(nde)
+    low = np.zeros(nde)
+    alt1, lat1 = -1000.0, 45.0
+    checks = 0
+    while q.time() < 95.0:
+        q.step()
+        P, Cc, N = q.prev(), q.curr(), q.next()
+        R = u.earth_radius()
+        for d in range(nde):
+            Hp, Hc, Hn = (F.rho[d, 0] - R - alt1 for F in (P, Cc, N))
+            if Hc * Hn < 0.0 and Cc.ndirection[0][d, 0] * de[d] > 0.0:
+                loop[d] += 1.0
+                Rt = loop[d] * S.MUNK_CYCLE_RANGES[d]
+                Rp, Rc, Rn = (F.rho[d, 0] * u.to_radians(F.latitude()[d, 0] - lat1) for F in (P, Cc, N))
+                h = Hn - Hp
+                slope = (Rn - Rp) / h
+                h *= 0.5
+                curve = (Rn - 2.0 * Rc + Rp) / (h * h)
+                dx = -Hc
+                Rm = Rc + slope * dx + 0.5 * curve * dx * dx
+                assert abs(Rm - Rt) / Rt * 100.0 < 0.01
+                assert Cc.upper[d, 0] - up[d] == 1
+                assert Cc.lower[d, 0] - low[d] == 1
+                up[d], low[d] = Cc.upper[d, 0], Cc.lower[d, 0]
+                checks += 1
+    assert checks >= 29
+
+
+def test_reflect_flat():
+    """reflection_test.cc:168-280: reflection times within 0.1 ms and
+    latitudes within 1e-6 deg of the analytic bounce pattern"""
+    sc = S.reflect_flat()
+    q = S.build_queue(sc, OracleQueue, reflections=True)
+    q.run(sc["time_max"])
+    refl = q.take_reflections()
+    assert len(refl) >= 7
+    for k, r in enumerate(refl):
+        count = k + 1
+        assert abs(r.time - count * 7.450560973) < 1e-4
+        lat = 90.0 - r.position[1] * (180.0 / math.pi)
+        assert abs(lat - (45.0 + count * 0.1)) < 1e-6
+        assert r.type == (0 if count % 2 == 1 else 1)
+
+
+def test_proploss_limits():
+    """proploss_test.cc:250-280: sources are clamped 0.1 m inside the water"""
+    u.compute_earth_radius(45.0)
+    ocean = u.ocean_model(u.boundary_flat(), u.boundary_flat(1000.0), u.profile_linear())
+    freq = u.seq_linear(1000.0, 1.0, 1)
+    de = u.seq_rayfan()
+    az = u.seq_linear(-20.0, 5.0, 20.0)
+    pos = u.wposition1(45.0, -45.0, 10.0)
+    q = OracleQueue(ocean, freq, pos, de, az, 0.1)
+    assert abs((q.source_pos()[0] - u.earth_radius()) - (-0.1)) < 1e-6 * 0.1
+    pos = u.wposition1(45.0, -45.0, -1010.0)
+    q = OracleQueue(ocean, freq, pos, de, az, 0.1)
+    assert abs((q.source_pos()[0] - u.earth_radius()) - (-1000.0 + 0.1)) < 1e-6 * 1000
+
+
+def test_proploss_gaussian():
+    """proploss_test.cc:153-248: TL within 2 dB of 20 log10(R) for the
+    direct, surface and bottom paths at 200-1000 Hz"""
+    sc = S.proploss_gaussian()
+    q = run(sc)
+    rays = q.take_eigenrays()
+    paths = {}
+    for r in rays:
+        pl = 20.0 * math.log10(1500.0 * r.travel_time - 2.0)
+        key = "bottom" if (r.bottom == 1 and r.surface == 0) else (
+            "surface" if (r.bottom == 0 and r.surface == 1) else "direct")
+        paths[key] = (r, pl)
+    assert set(paths) == {"direct", "surface", "bottom"}
+    for j in range(1, sc["freq"].size()):
+        for r, pl in paths.values():
+            assert abs(r.intensity[j] - pl) < 2.0

@@ -1,0 +1,900 @@
+/*
+ * wq3d_api.cu -- host side of the C ABI declared in include/wq3d.h.
+ *
+ * Owns device memory, precomputes everything that depends only on inputs
+ * (fan trigonometry, target terms, spreading normalisation, boundary
+ * constants) with the same arithmetic the reference uses, runs the step
+ * loop in chunks of K steps (captured once as a CUDA graph and replayed),
+ * and turns the device's eigenray/reflection records into listener calls
+ * in the reference's order.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "wq3d_engine.cuh"
+
+using namespace wq3d;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define WQ_CK(x)                                                                  \
+    do {                                                                          \
+        cudaError_t e_ = (x);                                                     \
+        if (e_ != cudaSuccess)                                                    \
+            return fail(WQ3D_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+inline double to_radians(double t) { return t * (M_PI / 180.0); }
+inline double to_degrees(double t) { return t * (180.0 / M_PI); }
+
+/* reflect loss constants (reflect_loss_rayleigh.cc:17,68-78) and the
+ * defaults of boundary_model.h:77-90 / boundary_flat.cc:19-31 */
+void setup_boundary(BoundaryDev& b, const wq3d_boundary_desc& d, double R) {
+    std::memset(&b, 0, sizeof(b));
+    b.kind = d.kind;
+    b.loss.kind = d.loss.kind;
+    for (int k = 0; k < 5; ++k) b.loss.p[k] = d.loss.p[k];
+    if (d.kind == WQ3D_BOUNDARY_SLOPE) {
+        /* boundary_slope.cc:13-24 and the constant factors of :55-68 */
+        b.height = R - d.depth;
+        b.normal[1] = std::sin(d.lat_slope);
+        b.normal[2] = -std::sin(d.lng_slope);
+        b.normal[0] = std::sqrt(1.0 - b.normal[1] * b.normal[1] - b.normal[2] * b.normal[2]);
+        const double alpha = -std::asin(b.normal[1]);
+        const double beta = -std::asin(b.normal[2]);
+        b.loc_theta = d.location[1];
+        b.loc_phi = d.location[2];
+        b.slope_a = std::sin(d.location[1]) * std::tan(beta);
+        b.slope_b = std::tan(alpha);
+        if (b.loss.kind == WQ3D_LOSS_DEFAULT) {
+            b.loss.kind = WQ3D_LOSS_CONSTANT;
+            b.loss.p[0] = 0.0;
+            b.loss.p[1] = 0.0;
+        }
+    } else {
+        b.kind = WQ3D_BOUNDARY_FLAT;
+        b.height = R - std::abs(d.depth);
+        if (std::abs(d.depth) < 1e-6) {
+            b.normal[0] = -1.0;
+            if (b.loss.kind == WQ3D_LOSS_DEFAULT) {
+                b.loss.kind = WQ3D_LOSS_CONSTANT;
+                b.loss.p[0] = 0.0;
+                b.loss.p[1] = M_PI;
+            }
+        } else {
+            b.normal[0] = 1.0;
+        }
+        if (b.loss.kind == WQ3D_LOSS_DEFAULT) {
+            b.loss.kind = WQ3D_LOSS_CONSTANT;
+            b.loss.p[0] = 0.0;
+            b.loss.p[1] = 0.0;
+        }
+    }
+    if (b.loss.kind == WQ3D_LOSS_RAYLEIGH) {
+        const double ATT_CONVERT = 1.0 / (20.0 * M_LOG10E * (2.0 * M_PI));
+        b.loss.rl_den = 1000.0 * d.loss.p[0];
+        b.loss.rl_spd = 1500.0 * d.loss.p[1];
+        b.loss.rl_att = d.loss.p[2] * ATT_CONVERT;
+        b.loss.rl_shr = 1500.0 * d.loss.p[3];
+        b.loss.rl_satt = d.loss.p[4] * ATT_CONVERT;
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct wq3d_ocean {
+    OceanDev dev;
+    double build_radius;
+};
+
+struct PendingRay {
+    wq3d_eigenray rec;
+    std::vector<double> inten, phase;
+};
+
+struct wq3d_queue {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    QueueDev h{};
+    QueueDev* d_q = nullptr;
+    std::vector<void*> allocs;
+    void* pinned = nullptr;
+    int64_t* h_base = nullptr;
+    double* h_times = nullptr;
+    uint32_t* h_counts = nullptr; /* n_rec, n_refl, err, n_cand */
+    int64_t* d_base = nullptr;
+    double* d_times = nullptr;
+    uint32_t* d_counts = nullptr;
+    int chunk = 16;
+    cudaGraphExec_t graph = nullptr;
+    bool graph_failed = false;
+    double time = 0.0;
+    int64_t steps = 0;
+    double src_clamped[3] = {0, 0, 0};
+    wq3d_callbacks cb{};
+    void* cb_ctx = nullptr;
+    uint64_t run_id = 0;
+    std::vector<PendingRay> pending;
+    std::atomic<bool> abort_flag{false};
+    bool timing = false;
+    std::vector<cudaEvent_t> events;
+    double ms_step = 0.0, ms_cpa = 0.0, ms_eig = 0.0, ms_total = 0.0;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    int64_t launches = 0;
+    std::vector<wq3d_eigenray> h_rec;
+    std::vector<double> h_rinten, h_rphase;
+    std::vector<wq3d_reflection> h_refl;
+
+    ~wq3d_queue() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto e : events) cudaEventDestroy(e);
+        if (ev_begin) cudaEventDestroy(ev_begin);
+        if (ev_end) cudaEventDestroy(ev_end);
+        for (void* p : allocs) cudaFree(p);
+        if (d_q) cudaFree(d_q);
+        if (pinned) cudaFreeHost(pinned);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <class T>
+    int alloc(T** out, size_t count) {
+        void* p = nullptr;
+        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        WQ_CK(cudaMalloc(&p, bytes));
+        allocs.push_back(p);
+        *out = static_cast<T*>(p);
+        return WQ3D_OK;
+    }
+    template <class T>
+    int upload(const T** out, const std::vector<T>& v) {
+        T* p = nullptr;
+        int rc = alloc(&p, v.size());
+        if (rc) return rc;
+        if (!v.empty()) WQ_CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        *out = p;
+        return WQ3D_OK;
+    }
+
+    int launch_step(int k) {
+        const int n = h.n;
+        const dim3 blk(128);
+        const dim3 grd((n + 127) / 128);
+        cudaEvent_t* ev = timing ? &events[5 * k] : nullptr;
+        if (ev) cudaEventRecord(ev[0], stream);
+        k_step<<<grd, blk, 0, stream>>>(d_q, k);
+        if (ev) cudaEventRecord(ev[1], stream);
+        k_edges<<<grd, blk, 0, stream>>>(d_q, k);
+        launches += 2;
+        if (h.nt > 0) {
+            const dim3 cg((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS);
+            if (ev) cudaEventRecord(ev[2], stream);
+            k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d_q, k);
+            if (ev) cudaEventRecord(ev[3], stream);
+            k_eigenray<<<148, 64, 0, stream>>>(d_q, k);
+            if (ev) cudaEventRecord(ev[4], stream);
+            launches += 2;
+        } else if (ev) {
+            cudaEventRecord(ev[2], stream);
+            cudaEventRecord(ev[3], stream);
+            cudaEventRecord(ev[4], stream);
+        }
+        return WQ3D_OK;
+    }
+
+    int build_graph() {
+        if (graph || graph_failed) return WQ3D_OK;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            graph_failed = true;
+            cudaGetLastError();
+            return WQ3D_OK;
+        }
+        const bool save = timing;
+        timing = false;
+        const int64_t saved_launches = launches;
+        for (int k = 0; k < chunk; ++k) launch_step(k);
+        launches = saved_launches;
+        timing = save;
+        if (cudaStreamEndCapture(stream, &g) != cudaSuccess ||
+            cudaGraphInstantiate(&graph, g, 0) != cudaSuccess) {
+            graph_failed = true;
+            graph = nullptr;
+            cudaGetLastError();
+        }
+        if (g) cudaGraphDestroy(g);
+        return WQ3D_OK;
+    }
+
+    void deliver(int K, size_t nrec, size_t nrefl) {
+        const int nf = h.nf;
+        /* reference order: (step, t1, t2, de, az) for eigenrays
+         * (wave_queue.cc:361-373), (step, de, az) for reflections */
+        std::vector<size_t> order(nrec);
+        for (size_t i = 0; i < nrec; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+            const wq3d_eigenray& x = h_rec[a];
+            const wq3d_eigenray& y = h_rec[b];
+            if (x.step != y.step) return x.step < y.step;
+            if (x.t1 != y.t1) return x.t1 < y.t1;
+            if (x.t2 != y.t2) return x.t2 < y.t2;
+            if (x.de != y.de) return x.de < y.de;
+            return x.az < y.az;
+        });
+        std::vector<wq3d_reflection> refl(h_refl.begin(), h_refl.begin() + nrefl);
+        std::sort(refl.begin(), refl.end(), [](const wq3d_reflection& x, const wq3d_reflection& y) {
+            if (x.step != y.step) return x.step < y.step;
+            if (x.de != y.de) return x.de < y.de;
+            if (x.az != y.az) return x.az < y.az;
+            return x.pad < y.pad;
+        });
+        size_t ir = 0, ie = 0;
+        for (int k = 0; k < K; ++k) {
+            const int64_t step = steps + k + 1;
+            while (ir < refl.size() && refl[ir].step == step) {
+                if (cb.reflect) cb.reflect(cb_ctx, &refl[ir]);
+                ++ir;
+            }
+            while (ie < order.size() && h_rec[order[ie]].step == step) {
+                const size_t j = order[ie];
+                if (cb.add_eigenray) {
+                    cb.add_eigenray(cb_ctx, (size_t)h_rec[j].t1, (size_t)h_rec[j].t2, &h_rec[j],
+                                    &h_rinten[j * nf], &h_rphase[j * nf], (size_t)nf, run_id);
+                } else {
+                    PendingRay p;
+                    p.rec = h_rec[j];
+                    p.inten.assign(&h_rinten[j * nf], &h_rinten[j * nf] + nf);
+                    p.phase.assign(&h_rphase[j * nf], &h_rphase[j * nf] + nf);
+                    pending.push_back(std::move(p));
+                }
+                ++ie;
+            }
+            if (cb.check_eigenrays) cb.check_eigenrays(cb_ctx, h_times[k + 1], run_id);
+        }
+    }
+
+    int run_chunk(int K) {
+        h_base[0] = steps;
+        h_times[0] = time;
+        for (int k = 0; k < K; ++k) h_times[k + 1] = h_times[k] + h.dt;
+        WQ_CK(cudaMemcpyAsync(d_base, h_base, sizeof(int64_t), cudaMemcpyHostToDevice, stream));
+        WQ_CK(cudaMemcpyAsync(d_times, h_times, (K + 1) * sizeof(double), cudaMemcpyHostToDevice, stream));
+        WQ_CK(cudaMemsetAsync(d_counts, 0, 3 * sizeof(uint32_t), stream));
+        if (!timing && K == chunk) {
+            build_graph();
+        }
+        if (!timing && K == chunk && graph) {
+            WQ_CK(cudaGraphLaunch(graph, stream));
+            launches += (h.nt > 0 ? 4 : 2) * (int64_t)K;
+        } else {
+            for (int k = 0; k < K; ++k) launch_step(k);
+        }
+        WQ_CK(cudaGetLastError());
+        WQ_CK(cudaMemcpyAsync(h_counts, d_counts, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        WQ_CK(cudaStreamSynchronize(stream));
+        if (timing) {
+            for (int k = 0; k < K; ++k) {
+                float a = 0, b = 0, c = 0;
+                cudaEventElapsedTime(&a, events[5 * k], events[5 * k + 2]);
+                cudaEventElapsedTime(&b, events[5 * k + 2], events[5 * k + 3]);
+                cudaEventElapsedTime(&c, events[5 * k + 3], events[5 * k + 4]);
+                ms_step += a;
+                ms_cpa += b;
+                ms_eig += c;
+            }
+        }
+        const uint32_t nrec = std::min(h_counts[0], h.cap_rec);
+        const uint32_t nrefl = std::min(h_counts[1], h.cap_refl);
+        const uint32_t err = h_counts[2];
+        if (nrec > 0) {
+            if (h_rec.size() < nrec) {
+                h_rec.resize(nrec);
+                h_rinten.resize((size_t)nrec * h.nf);
+                h_rphase.resize((size_t)nrec * h.nf);
+            }
+            WQ_CK(cudaMemcpy(h_rec.data(), h.rec, nrec * sizeof(wq3d_eigenray), cudaMemcpyDeviceToHost));
+            WQ_CK(cudaMemcpy(h_rinten.data(), h.rec_inten, (size_t)nrec * h.nf * sizeof(double), cudaMemcpyDeviceToHost));
+            WQ_CK(cudaMemcpy(h_rphase.data(), h.rec_phase, (size_t)nrec * h.nf * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        if (nrefl > 0) {
+            if (h_refl.size() < nrefl) h_refl.resize(nrefl);
+            WQ_CK(cudaMemcpy(h_refl.data(), h.refl, nrefl * sizeof(wq3d_reflection), cudaMemcpyDeviceToHost));
+        }
+        deliver(K, nrec, nrefl);
+        steps += K;
+        time = h_times[K];
+        if (err & (ERR_CAND_OVERFLOW | ERR_REC_OVERFLOW | ERR_REFL_OVERFLOW))
+            return fail(WQ3D_ERR_OVERFLOW, "eigenray or reflection buffer overflow (error bits " +
+                                               std::to_string(err) + "); recreate the queue with a larger eigenray_capacity");
+        if (err)
+            return fail(WQ3D_ERR_NUMERIC, "kernel iteration bound reached (error bits " + std::to_string(err) + ")");
+        return WQ3D_OK;
+    }
+};
+
+extern "C" {
+
+const char* wq3d_last_error_string(void) { return g_err.c_str(); }
+int wq3d_abi_version(void) { return WQ3D_ABI_VERSION; }
+
+int wq3d_device_count(int* count) {
+    if (!count) return fail(WQ3D_ERR_INVALID, "null count");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail(WQ3D_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    }
+    *count = n;
+    return WQ3D_OK;
+}
+
+int wq3d_ocean_create(const wq3d_ocean_desc* d, wq3d_ocean** out) {
+    if (!d || !out) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (d->profile.kind < WQ3D_PROFILE_LINEAR || d->profile.kind > WQ3D_PROFILE_N2)
+        return fail(WQ3D_ERR_UNSUPPORTED, "profile kind not supported by this build");
+    if (d->bottom.kind == WQ3D_BOUNDARY_GRID || d->surface.kind == WQ3D_BOUNDARY_GRID)
+        return fail(WQ3D_ERR_UNSUPPORTED, "boundary grids not supported by this build");
+    wq3d_ocean* o = new wq3d_ocean();
+    std::memset(&o->dev, 0, sizeof(o->dev));
+    ProfileDev& p = o->dev.prof;
+    p.kind = d->profile.kind;
+    for (int k = 0; k < 4; ++k) p.p[k] = d->profile.p[k];
+    p.munk_k = -p.p[3] * p.p[2] * 2.0 / p.p[1];
+    p.n2_factor = 2.0 * p.p[1] / p.p[0];
+    p.flat_earth = d->profile.flat_earth;
+    p.atten = d->profile.attenuation;
+    p.atten_coef = d->profile.attenuation_coef;
+    setup_boundary(o->dev.surf, d->surface, d->earth_radius);
+    setup_boundary(o->dev.bot, d->bottom, d->earth_radius);
+    o->build_radius = d->earth_radius;
+    *out = o;
+    return WQ3D_OK;
+}
+
+int wq3d_ocean_destroy(wq3d_ocean* o) {
+    delete o;
+    return WQ3D_OK;
+}
+
+static int eval_points(size_t n, std::vector<double*>& dev_in, const std::vector<const double*>& host_in) {
+    for (size_t k = 0; k < host_in.size(); ++k) {
+        double* p = nullptr;
+        WQ_CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(double)));
+        dev_in.push_back(p);
+        if (host_in[k]) WQ_CK(cudaMemcpy(p, host_in[k], n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return WQ3D_OK;
+}
+
+int wq3d_ocean_sound_speed(const wq3d_ocean* o, double R, size_t n, const double* rho,
+                           const double* theta, const double* phi, double* speed, double* grad) {
+    if (!o || !rho || !speed) return fail(WQ3D_ERR_INVALID, "null argument");
+    std::vector<double*> d;
+    int rc = eval_points(n, d, {rho, theta, phi});
+    double *dc = nullptr, *dg = nullptr;
+    if (!rc && cudaMalloc(&dc, std::max<size_t>(n, 1) * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && cudaMalloc(&dg, std::max<size_t>(3 * n, 1) * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && n > 0) {
+        k_sound_speed<<<(unsigned)((n + 127) / 128), 128>>>(o->dev, R, (int)n, d[0], d[1], d[2], dc, dg);
+        if (cudaMemcpy(speed, dc, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+        if (!rc && grad && cudaMemcpy(grad, dg, 3 * n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = WQ3D_ERR_CUDA;
+    }
+    for (double* p : d) cudaFree(p);
+    cudaFree(dc);
+    cudaFree(dg);
+    if (rc) return fail(rc, "wq3d_ocean_sound_speed failed");
+    return WQ3D_OK;
+}
+
+int wq3d_ocean_height(const wq3d_ocean* o, int which, size_t n, const double* rho,
+                      const double* theta, const double* phi, double* height, double* normal) {
+    if (!o || !theta || !phi || !height) return fail(WQ3D_ERR_INVALID, "null argument");
+    (void)rho;
+    std::vector<double*> d;
+    int rc = eval_points(n, d, {theta, phi});
+    double *dh = nullptr, *dn = nullptr;
+    if (!rc && cudaMalloc(&dh, std::max<size_t>(n, 1) * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && cudaMalloc(&dn, std::max<size_t>(3 * n, 1) * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && n > 0) {
+        k_height<<<(unsigned)((n + 127) / 128), 128>>>(which == 0 ? o->dev.surf : o->dev.bot, (int)n, d[0],
+                                                        d[1], dh, dn);
+        if (cudaMemcpy(height, dh, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+        if (!rc && normal && cudaMemcpy(normal, dn, 3 * n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = WQ3D_ERR_CUDA;
+    }
+    for (double* p : d) cudaFree(p);
+    cudaFree(dh);
+    cudaFree(dn);
+    if (rc) return fail(rc, "wq3d_ocean_height failed");
+    return WQ3D_OK;
+}
+
+int wq3d_ocean_reflect_loss(const wq3d_ocean* o, int which, size_t n, const double* rho,
+                            const double* theta, const double* phi, const double* grazing,
+                            size_t nf, const double* freq, double* amplitude, double* phase) {
+    if (!o || !grazing || !freq || !amplitude) return fail(WQ3D_ERR_INVALID, "null argument");
+    (void)rho;
+    (void)theta;
+    (void)phi;
+    std::vector<double*> d;
+    int rc = eval_points(n, d, {grazing});
+    double *df = nullptr, *da = nullptr, *dp = nullptr;
+    if (!rc && cudaMalloc(&df, std::max<size_t>(nf, 1) * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && cudaMalloc(&da, std::max<size_t>(n * nf, 1) * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && cudaMalloc(&dp, std::max<size_t>(n * nf, 1) * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && n > 0) {
+        cudaMemcpy(df, freq, nf * sizeof(double), cudaMemcpyHostToDevice);
+        k_reflect_loss<<<(unsigned)((n + 127) / 128), 128>>>(which == 0 ? o->dev.surf : o->dev.bot, (int)n,
+                                                              d[0], (int)nf, df, da, dp);
+        if (cudaMemcpy(amplitude, da, n * nf * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = WQ3D_ERR_CUDA;
+        if (!rc && phase && cudaMemcpy(phase, dp, n * nf * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = WQ3D_ERR_CUDA;
+    }
+    for (double* p : d) cudaFree(p);
+    cudaFree(df);
+    cudaFree(da);
+    cudaFree(dp);
+    if (rc) return fail(rc, "wq3d_ocean_reflect_loss failed");
+    return WQ3D_OK;
+}
+
+int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_queue** out) {
+    if (!ocean || !d || !out) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (d->num_de < 1 || d->num_az < 1 || !d->de || !d->az || !d->de_inc || !d->az_inc)
+        return fail(WQ3D_ERR_INVALID, "ray fan must hold at least one D/E and one AZ angle");
+    if (d->num_freq < 1 || !d->freq) return fail(WQ3D_ERR_INVALID, "at least one frequency is required");
+    if (d->num_freq > (size_t)MAX_FREQ) return fail(WQ3D_ERR_UNSUPPORTED, "more than 64 frequencies");
+    if (d->num_az > (size_t)MAX_AZ) return fail(WQ3D_ERR_UNSUPPORTED, "more than 4096 AZ angles");
+    if (!(d->time_step > 0.0)) return fail(WQ3D_ERR_INVALID, "time_step must be positive");
+    if (d->precision != WQ3D_FP64) return fail(WQ3D_ERR_UNSUPPORTED, "only the FP64 form is built");
+    const size_t n = d->num_de * d->num_az;
+    if (n > (size_t)0x7fffffff) return fail(WQ3D_ERR_INVALID, "ray fan too large");
+    const size_t nt = (d->targets && d->num_targets1 * d->num_targets2 > 0)
+                          ? d->num_targets1 * d->num_targets2 : 0;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(WQ3D_ERR_CUDA, "no CUDA device is available");
+    if (d->device < 0 || d->device >= ndev) return fail(WQ3D_ERR_INVALID, "device ordinal out of range");
+    DeviceGuard guard(d->device);
+
+    wq3d_queue* q = new wq3d_queue();
+    q->device = d->device;
+    q->run_id = d->run_id;
+    QueueDev& h = q->h;
+    std::memset(&h, 0, sizeof(h));
+    h.oc = ocean->dev;
+    h.nde = (int)d->num_de;
+    h.naz = (int)d->num_az;
+    h.nf = (int)d->num_freq;
+    h.n = (int)n;
+    h.nt = (int)nt;
+    h.nt1 = nt ? (int)d->num_targets1 : 0;
+    h.nt2 = nt ? (int)d->num_targets2 : 1;
+    h.dt = d->time_step;
+    h.R = d->earth_radius;
+    h.spreading = d->spreading;
+    h.intensity_threshold = 300.0;
+    h.max_bottom = h.max_surface = h.max_caustic = h.max_upper = h.max_lower = 999;
+
+    auto cleanup = [&](int rc) {
+        std::string msg = g_err;
+        delete q;
+        g_err = msg;
+        return rc;
+    };
+    int rc = 0;
+    if (cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
+
+    /* host-side inputs */
+    const size_t nde = d->num_de, naz = d->num_az, nf = d->num_freq;
+    std::vector<double> freq(d->freq, d->freq + nf);
+    std::vector<double> de(d->de, d->de + nde), de_inc(d->de_inc, d->de_inc + nde);
+    std::vector<double> az(d->az, d->az + naz), az_inc(d->az_inc, d->az_inc + naz);
+
+    /* wave_queue.cc:47-53 */
+    h.az_boundary = 0;
+    if (naz > 1) {
+        const double a0 = std::abs(az[0]), a1 = std::abs(az[naz - 1]);
+        h.az_boundary = (std::fmod(a0 + 360.0, 360.0) == std::fmod(a1 + 360.0, 360.0)) ? 1 : 0;
+    }
+    /* wave_queue.cc:58-68: the clamp changes source_pos() only; init_wave
+     * receives the caller's position (wave_queue.cc:83) */
+    for (int k = 0; k < 3; ++k) h.source[k] = q->src_clamped[k] = d->source[k];
+    {
+        const double offset = 0.1;
+        double bottom_rho = boundary_height(h.oc.bot, d->source[1], d->source[2]) + offset;
+        if (q->src_clamped[0] - h.R > -offset) {
+            q->src_clamped[0] = -offset + h.R;
+        } else if (q->src_clamped[0] < bottom_rho) {
+            q->src_clamped[0] = bottom_rho;
+        }
+    }
+    {
+        double gr;
+        sound_speed(h.oc.prof, h.R, d->source[0], &h.c_source, &gr);
+    }
+    std::vector<double> cos_de(nde), sin_de(nde), cos_az(naz), sin_az(naz);
+    for (size_t i = 0; i < nde; ++i) {
+        cos_de[i] = std::cos(to_radians(de[i]));
+        sin_de[i] = std::sin(to_radians(de[i]));
+    }
+    for (size_t i = 0; i < naz; ++i) {
+        cos_az[i] = std::cos(to_radians(az[i]));
+        sin_az[i] = std::sin(to_radians(az[i]));
+    }
+    /* attenuation_thorp.cc:14-36 coefficient per frequency */
+    std::vector<double> alpha(nf);
+    for (size_t k = 0; k < nf; ++k) {
+        double F2 = freq[k];
+        F2 = 1e-6 * F2 * F2;
+        alpha[k] = 1e-3 * (3.3e-3 + F2 * (0.11 / (1.0 + F2) + 44.0 / (4100.0 + F2) + 3.0e-4)) /
+                   (1.0 - 5.88264e-6 * 1000.0);
+    }
+    /* targets (wave_queue.cc:54-56, :363-369; spreading_hybrid_gaussian.cc:70-83) */
+    std::vector<double> tr(nt), tt(nt), tp(nt), tsin(nt), tR2(nt), t2R(nt), tc(nt), tspread(nt * nf);
+    std::vector<uint8_t> tbranch(nt);
+    const double slat = 90.0 - to_degrees(q->src_clamped[1]);
+    const double slng = to_degrees(q->src_clamped[2]);
+    for (size_t t = 0; t < nt; ++t) {
+        tr[t] = d->targets[t];
+        tt[t] = d->targets[nt + t];
+        tp[t] = d->targets[2 * nt + t];
+        tsin[t] = std::sin(tt[t]);
+        tR2[t] = tr[t] * tr[t];
+        t2R[t] = 2.0 * tr[t];
+        double gr;
+        sound_speed(h.oc.prof, h.R, tr[t], &tc[t], &gr);
+        for (size_t k = 0; k < nf; ++k) {
+            const double s = 2.0 * M_PI * tc[t] / freq[k];
+            tspread[t * nf + k] = s * s;
+        }
+        const double tlat = 90.0 - to_degrees(tt[t]);
+        const double tlng = to_degrees(tp[t]);
+        tbranch[t] = (std::abs(slat - tlat) < 1e-4 && std::abs(slng - tlng) < 1e-4) ? 1 : 0;
+    }
+    /* spreading normalisation (spreading_hybrid_gaussian.cc:28-59,
+     * spreading_ray.cc:26-45) */
+    std::vector<double> norm_de(nde, 0.0), norm_az(n, 0.0), init_area(n, 0.0);
+    if (nde >= 3 && naz >= 3) {
+        for (size_t dd = 0; dd < nde - 1; ++dd) {
+            const double de1 = to_radians(de[dd]);
+            const double de2 = to_radians(de[dd + 1]);
+            norm_de[dd] = de2 - de1;
+            for (size_t a = 0; a < naz - 1; ++a) {
+                const double az1 = to_radians(az[a]);
+                const double az2 = to_radians(az[a + 1]);
+                init_area[dd * naz + a] = (std::sin(de2) - std::sin(de1)) * (az2 - az1);
+                norm_az[dd * naz + a] = init_area[dd * naz + a] / norm_de[dd];
+            }
+            norm_az[dd * naz + naz - 1] = norm_az[dd * naz + naz - 2];
+            init_area[dd * naz + naz - 1] = init_area[dd * naz + naz - 2];
+        }
+        norm_de[nde - 1] = norm_de[nde - 2];
+        for (size_t a = 0; a < naz - 1; ++a) {
+            init_area[(nde - 1) * naz + a] = init_area[(nde - 2) * naz + a];
+            norm_az[(nde - 1) * naz + a] = norm_az[(nde - 2) * naz + a];
+        }
+        const double s = std::sqrt(2.0 * M_PI);
+        for (auto& v : norm_de) v /= s;
+        for (auto& v : norm_az) v /= s;
+    }
+
+    if ((rc = q->upload(&h.freq, freq)) || (rc = q->upload(&h.alpha, alpha)) ||
+        (rc = q->upload(&h.de, de)) || (rc = q->upload(&h.de_inc, de_inc)) ||
+        (rc = q->upload(&h.az, az)) || (rc = q->upload(&h.az_inc, az_inc)) ||
+        (rc = q->upload(&h.cos_de, cos_de)) || (rc = q->upload(&h.sin_de, sin_de)) ||
+        (rc = q->upload(&h.cos_az, cos_az)) || (rc = q->upload(&h.sin_az, sin_az)) ||
+        (rc = q->upload(&h.tgt[0], tr)) || (rc = q->upload(&h.tgt[1], tt)) ||
+        (rc = q->upload(&h.tgt[2], tp)) || (rc = q->upload(&h.tgt_sin, tsin)) ||
+        (rc = q->upload(&h.tgt_R2, tR2)) || (rc = q->upload(&h.tgt_2R, t2R)) ||
+        (rc = q->upload(&h.tgt_spread2, tspread)) || (rc = q->upload(&h.tgt_c, tc)) ||
+        (rc = q->upload(&h.de_branch, tbranch)) || (rc = q->upload(&h.norm_de, norm_de)) ||
+        (rc = q->upload(&h.norm_az, norm_az)) || (rc = q->upload(&h.init_area, init_area)))
+        return cleanup(rc);
+
+    /* wavefront ring: one allocation carved into 256-byte aligned arrays */
+    {
+        const size_t nd_arrays = 22 + 2 * nf;
+        auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+        const size_t dbytes = al(n * sizeof(double));
+        const size_t ibytes = al(n * sizeof(int32_t));
+        const size_t bbytes = al(n);
+        const size_t per_front = nd_arrays * dbytes + 5 * ibytes + bbytes;
+        char* base = nullptr;
+        if ((rc = q->alloc(&base, 4 * per_front + 2 * bbytes))) return cleanup(rc);
+        if (cudaMemset(base, 0, 4 * per_front + 2 * bbytes) != cudaSuccess)
+            return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
+        char* p = base;
+        auto dtake = [&](size_t count) {
+            double* r = reinterpret_cast<double*>(p);
+            p += al(count * sizeof(double));
+            return r;
+        };
+        for (int f = 0; f < 4; ++f) {
+            FrontPtrs& F = h.F[f];
+            for (int k = 0; k < 3; ++k) {
+                F.pos[k] = dtake(n);
+                F.pg[k] = dtake(n);
+                F.nd[k] = dtake(n);
+                F.ng[k] = dtake(n);
+                F.sg[k] = dtake(n);
+            }
+            F.c = dtake(n);
+            F.dist = dtake(n);
+            F.plen = dtake(n);
+            for (int k = 0; k < 4; ++k) F.cpa[k] = dtake(n);
+            F.atten = dtake(n * nf);
+            F.phase = dtake(n * nf);
+            int32_t** ints[5] = {&F.surface, &F.bottom, &F.caustic, &F.upper, &F.lower};
+            for (auto ip : ints) {
+                *ip = reinterpret_cast<int32_t*>(p);
+                p += ibytes;
+            }
+            F.on_edge = reinterpret_cast<uint8_t*>(p);
+            p += bbytes;
+        }
+        h.flag[0] = reinterpret_cast<uint8_t*>(p);
+        p += bbytes;
+        h.flag[1] = reinterpret_cast<uint8_t*>(p);
+    }
+    /* result buffers and chunk control */
+    h.cap_cand = (uint32_t)(d->eigenray_capacity ? d->eigenray_capacity
+                                                 : std::max<size_t>(4096, 32 * nt));
+    h.cap_rec = (uint32_t)std::min<size_t>((size_t)h.cap_cand * q->chunk, (size_t)1 << 21);
+    h.cap_refl = (uint32_t)std::min<size_t>(std::max<size_t>(4096, 2 * n), (size_t)1 << 22);
+    uint32_t* cand = nullptr;
+    if ((rc = q->alloc(&cand, 2 * (size_t)h.cap_cand))) return cleanup(rc);
+    h.cand = cand;
+    if ((rc = q->alloc(&h.rec, h.cap_rec)) || (rc = q->alloc(&h.rec_inten, (size_t)h.cap_rec * nf)) ||
+        (rc = q->alloc(&h.rec_phase, (size_t)h.cap_rec * nf)) || (rc = q->alloc(&h.refl, h.cap_refl)))
+        return cleanup(rc);
+    if ((rc = q->alloc(&q->d_counts, 8)) || (rc = q->alloc(&q->d_base, 1)) ||
+        (rc = q->alloc(&q->d_times, (size_t)q->chunk + 1)))
+        return cleanup(rc);
+    h.n_rec = q->d_counts + 0;
+    h.n_refl = q->d_counts + 1;
+    h.err = q->d_counts + 2;
+    h.n_cand = q->d_counts + 3;
+    h.d_base = q->d_base;
+    h.d_times = q->d_times;
+    h.want_refl = 0;
+    if (cudaMallocHost(&q->pinned, 4096 + (q->chunk + 1) * sizeof(double)) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_NOMEM, "cudaMallocHost failed"));
+    q->h_base = static_cast<int64_t*>(q->pinned);
+    q->h_counts = reinterpret_cast<uint32_t*>(static_cast<char*>(q->pinned) + 64);
+    q->h_times = reinterpret_cast<double*>(static_cast<char*>(q->pinned) + 128);
+    if (cudaMemset(q->d_counts, 0, 8 * sizeof(uint32_t)) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
+
+    if (cudaMalloc(&q->d_q, sizeof(QueueDev)) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_CUDA, "cudaMalloc failed"));
+    if (cudaMemcpy(q->d_q, &h, sizeof(QueueDev), cudaMemcpyHostToDevice) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
+
+    /* wave_queue ctor: init_wave, update, init_wavefronts */
+    k_startup<<<(unsigned)((n + 127) / 128), 128, 0, q->stream>>>(q->d_q);
+    cudaError_t e = cudaStreamSynchronize(q->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cleanup(fail(WQ3D_ERR_CUDA, std::string("start-up kernel: ") + cudaGetErrorString(e)));
+    /* spreading_ray.cc:44: sound speed of ray (0,0) on the first front */
+    if (cudaMemcpy(&h.init_sound_speed, h.F[2].c, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
+    if (cudaMemcpy(q->d_q, &h, sizeof(QueueDev), cudaMemcpyHostToDevice) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
+    if (cudaEventCreate(&q->ev_begin) != cudaSuccess || cudaEventCreate(&q->ev_end) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+    q->events.resize(5 * (size_t)q->chunk);
+    for (auto& ev : q->events)
+        if (cudaEventCreate(&ev) != cudaSuccess) return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+    *out = q;
+    return WQ3D_OK;
+}
+
+int wq3d_queue_destroy(wq3d_queue* q) {
+    if (!q) return WQ3D_OK;
+    DeviceGuard guard(q->device);
+    delete q;
+    return WQ3D_OK;
+}
+
+int wq3d_queue_set_thresholds(wq3d_queue* q, const wq3d_thresholds* t) {
+    if (!q || !t) return fail(WQ3D_ERR_INVALID, "null argument");
+    DeviceGuard guard(q->device);
+    q->h.intensity_threshold = std::abs(t->intensity);
+    q->h.max_bottom = t->max_bottom;
+    q->h.max_surface = t->max_surface;
+    q->h.max_caustic = t->max_caustic;
+    q->h.max_upper = t->max_upper;
+    q->h.max_lower = t->max_lower;
+    WQ_CK(cudaMemcpy(q->d_q, &q->h, sizeof(QueueDev), cudaMemcpyHostToDevice));
+    return WQ3D_OK;
+}
+
+int wq3d_queue_set_callbacks(wq3d_queue* q, const wq3d_callbacks* cb, void* ctx) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    DeviceGuard guard(q->device);
+    if (cb)
+        q->cb = *cb;
+    else
+        q->cb = wq3d_callbacks{};
+    q->cb_ctx = ctx;
+    const int want = q->cb.reflect ? 1 : 0;
+    if (want != q->h.want_refl) {
+        q->h.want_refl = want;
+        WQ_CK(cudaMemcpy(q->d_q, &q->h, sizeof(QueueDev), cudaMemcpyHostToDevice));
+    }
+    return WQ3D_OK;
+}
+
+int wq3d_queue_step(wq3d_queue* q, size_t nsteps) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    DeviceGuard guard(q->device);
+    if (nsteps == 0) return WQ3D_OK;
+    WQ_CK(cudaEventRecord(q->ev_begin, q->stream));
+    int rc = WQ3D_OK;
+    while (nsteps > 0) {
+        if (q->abort_flag.exchange(false)) {
+            rc = fail(WQ3D_ERR_ABORTED, "aborted by caller");
+            break;
+        }
+        const int K = (int)std::min<size_t>(nsteps, (size_t)q->chunk);
+        rc = q->run_chunk(K);
+        if (rc) break;
+        nsteps -= (size_t)K;
+    }
+    WQ_CK(cudaEventRecord(q->ev_end, q->stream));
+    WQ_CK(cudaEventSynchronize(q->ev_end));
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, q->ev_begin, q->ev_end) == cudaSuccess) q->ms_total += ms;
+    return rc;
+}
+
+int wq3d_queue_run(wq3d_queue* q, double time_max, size_t* steps_done) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    size_t n = 0;
+    double t = q->time;
+    while (t < time_max) {
+        t += q->h.dt;
+        ++n;
+    }
+    const int rc = wq3d_queue_step(q, n);
+    if (steps_done) *steps_done = n;
+    return rc;
+}
+
+int wq3d_queue_time(const wq3d_queue* q, double* t) {
+    if (!q || !t) return fail(WQ3D_ERR_INVALID, "null argument");
+    *t = q->time;
+    return WQ3D_OK;
+}
+
+int wq3d_queue_source(const wq3d_queue* q, double* s) {
+    if (!q || !s) return fail(WQ3D_ERR_INVALID, "null argument");
+    for (int k = 0; k < 3; ++k) s[k] = q->src_clamped[k];
+    return WQ3D_OK;
+}
+
+int wq3d_queue_steps(const wq3d_queue* q, int64_t* steps) {
+    if (!q || !steps) return fail(WQ3D_ERR_INVALID, "null argument");
+    *steps = q->steps;
+    return WQ3D_OK;
+}
+
+int wq3d_queue_get_front(wq3d_queue* q, int which, const wq3d_front_view* v) {
+    if (!q || !v || which < 0 || which > 3) return fail(WQ3D_ERR_INVALID, "bad argument");
+    DeviceGuard guard(q->device);
+    const FrontPtrs& F = q->h.F[(q->steps + which) & 3];
+    const size_t n = q->h.n, nf = q->h.nf;
+    auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
+        if (!dst) return WQ3D_OK;
+        WQ_CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+        return WQ3D_OK;
+    };
+    int rc = 0;
+    rc |= cp(v->rho, F.pos[0], n * 8);
+    rc |= cp(v->theta, F.pos[1], n * 8);
+    rc |= cp(v->phi, F.pos[2], n * 8);
+    for (int k = 0; k < 3; ++k) {
+        rc |= cp(v->pos_grad[k], F.pg[k], n * 8);
+        rc |= cp(v->ndir[k], F.nd[k], n * 8);
+        rc |= cp(v->ndir_grad[k], F.ng[k], n * 8);
+        rc |= cp(v->sound_grad[k], F.sg[k], n * 8);
+    }
+    rc |= cp(v->sound_speed, F.c, n * 8);
+    rc |= cp(v->distance, F.dist, n * 8);
+    rc |= cp(v->path_length, F.plen, n * 8);
+    rc |= cp(v->surface, F.surface, n * 4);
+    rc |= cp(v->bottom, F.bottom, n * 4);
+    rc |= cp(v->caustic, F.caustic, n * 4);
+    rc |= cp(v->upper, F.upper, n * 4);
+    rc |= cp(v->lower, F.lower, n * 4);
+    rc |= cp(v->on_edge, F.on_edge, n);
+    if (v->attenuation || v->phase) {
+        std::vector<double> tmp(n * nf);
+        for (int w = 0; w < 2; ++w) {
+            double* dst = w ? v->phase : v->attenuation;
+            if (!dst) continue;
+            rc |= cp(tmp.data(), w ? F.phase : F.atten, n * nf * 8);
+            for (size_t f = 0; f < nf; ++f)
+                for (size_t i = 0; i < n; ++i) dst[i * nf + f] = tmp[f * n + i];
+        }
+    }
+    return rc ? WQ3D_ERR_CUDA : WQ3D_OK;
+}
+
+int wq3d_queue_take_eigenrays(wq3d_queue* q, wq3d_eigenray* rays, double* inten, double* phase,
+                              size_t capacity, size_t* count) {
+    if (!q || !count) return fail(WQ3D_ERR_INVALID, "null argument");
+    *count = q->pending.size();
+    if (!rays) return WQ3D_OK;
+    if (capacity < q->pending.size()) return fail(WQ3D_ERR_OVERFLOW, "capacity smaller than the pending count");
+    const size_t nf = q->h.nf;
+    for (size_t i = 0; i < q->pending.size(); ++i) {
+        rays[i] = q->pending[i].rec;
+        if (inten) std::memcpy(inten + i * nf, q->pending[i].inten.data(), nf * sizeof(double));
+        if (phase) std::memcpy(phase + i * nf, q->pending[i].phase.data(), nf * sizeof(double));
+    }
+    q->pending.clear();
+    return WQ3D_OK;
+}
+
+int wq3d_queue_abort(wq3d_queue* q) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    q->abort_flag.store(true);
+    return WQ3D_OK;
+}
+
+int wq3d_queue_timing(wq3d_queue* q, double* ms_total, double* ms_step, double* ms_cpa,
+                      double* ms_eig, int64_t* launches, int reset) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    if (ms_total) *ms_total = q->ms_total;
+    if (ms_step) *ms_step = q->ms_step;
+    if (ms_cpa) *ms_cpa = q->ms_cpa;
+    if (ms_eig) *ms_eig = q->ms_eig;
+    if (launches) *launches = q->launches;
+    if (reset) {
+        q->ms_step = q->ms_cpa = q->ms_eig = q->ms_total = 0.0;
+        q->launches = 0;
+    }
+    return WQ3D_OK;
+}
+
+/* Turns per-kernel CUDA-event timing on or off (direct launches instead of
+ * the chunk graph while on). */
+int wq3d_queue_set_timing(wq3d_queue* q, int on) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    q->timing = on != 0;
+    return WQ3D_OK;
+}
+
+}  // extern "C"

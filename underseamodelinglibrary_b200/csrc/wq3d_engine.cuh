@@ -1,0 +1,141 @@
+/*
+ * wq3d_engine.cuh -- device-side layout of one wave queue and the kernel
+ * entry points of the FP64 propagation engine.
+ *
+ * HBM layout: four wavefronts in a ring (the reference's past/prev/curr/next
+ * circular queue, waveq3d/wave_queue.h:350).  Every per-ray field is its
+ * own contiguous array of N = num_de * num_az values in (de, az) row-major
+ * order, so one thread per ray reads and writes fully coalesced.  Per
+ * frequency fields are frequency-major ([f][N]).  A ring role is selected by
+ * the step number: at the start of step s the roles are past = F[s&3],
+ * prev = F[(s+1)&3], curr = F[(s+2)&3], next = F[(s+3)&3], which is the
+ * reference's pointer rotation (wave_queue.cc:162-167) without copying.
+ *
+ * Instead of the reference's num_targets x N distance2 matrices per front
+ * (wave_front.h:258), each front keeps the four terms that
+ * compute_target_distance used when the front was last updated
+ * (rho, theta, phi, sin(theta)); the CPA kernels recompute distance2 from
+ * them.  A reflection re-initialises a ray's positions but, as in the
+ * reference, not its distance2, so these terms are only written by update.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "wq3d_models.cuh"
+
+namespace wq3d {
+
+constexpr int MAX_FREQ = 64;     /* frequencies per queue                */
+constexpr int MAX_AZ = 4096;     /* AZ fan size (duplicate bit mask)     */
+constexpr int MAX_BOUNCE = 64;   /* reflections of one ray in one step   */
+
+/* error bits written by kernels (never a trap) */
+enum : uint32_t {
+    ERR_BOUNCE_LIMIT = 1u,       /* more than MAX_BOUNCE reflections in a step */
+    ERR_CAND_OVERFLOW = 2u,      /* eigenray candidate list full               */
+    ERR_REC_OVERFLOW = 4u,       /* eigenray record buffer full                */
+    ERR_REFL_OVERFLOW = 8u,      /* reflection record buffer full              */
+    ERR_WALK_LIMIT = 16u         /* a Gaussian-beam walk exceeded its bound    */
+};
+
+struct FrontPtrs {
+    double* pos[3];
+    double* pg[3];
+    double* nd[3];
+    double* ng[3];
+    double* c;
+    double* sg[3];
+    double* dist;
+    double* plen;
+    double* atten;   /* [nf][n] */
+    double* phase;   /* [nf][n] */
+    double* cpa[4];  /* rho, theta, phi, sin(theta) at the last update */
+    int32_t* surface;
+    int32_t* bottom;
+    int32_t* caustic;
+    int32_t* upper;
+    int32_t* lower;
+    uint8_t* on_edge;
+};
+
+struct QueueDev {
+    FrontPtrs F[4];
+    OceanDev oc;
+    int nde, naz, nf, n;
+    int nt, nt1, nt2;
+    int az_boundary;
+    int spreading;
+    double dt;
+    double R;
+    /* fans and frequencies */
+    const double* freq;
+    const double* alpha;     /* Thorp coefficient per frequency */
+    const double* de;
+    const double* de_inc;
+    const double* az;
+    const double* az_inc;
+    const double* cos_de;
+    const double* sin_de;
+    const double* cos_az;
+    const double* sin_az;
+    double source[3];        /* unclamped, as passed to init_wave */
+    double c_source;
+    /* targets */
+    const double* tgt[3];
+    const double* tgt_sin;
+    const double* tgt_R2;
+    const double* tgt_2R;
+    const double* tgt_spread2;   /* [nt][nf] (2 pi c_target / f)^2 */
+    const double* tgt_c;         /* sound speed at each target */
+    const uint8_t* de_branch;
+    /* spreading normalisation */
+    const double* norm_de;
+    const double* norm_az;
+    const double* init_area;
+    double init_sound_speed;
+    /* thresholds */
+    double intensity_threshold;
+    int max_bottom, max_surface, max_caustic, max_upper, max_lower;
+    /* chunk control */
+    const int64_t* d_base;   /* steps completed before this chunk          */
+    const double* d_times;   /* time after base + k steps, k = 0..K         */
+    uint8_t* flag[2];        /* reflection decision for the "next" front    */
+    /* eigenray candidates of the current step */
+    uint32_t* cand;          /* packed: target index, ray index              */
+    uint32_t* n_cand;
+    uint32_t cap_cand;
+    /* eigenray records of the chunk */
+    wq3d_eigenray* rec;
+    double* rec_inten;       /* [cap][nf] */
+    double* rec_phase;
+    uint32_t* n_rec;
+    uint32_t cap_rec;
+    /* reflection records (only when a listener wants them) */
+    wq3d_reflection* refl;
+    uint32_t* n_refl;
+    uint32_t cap_refl;
+    int want_refl;
+    uint32_t* err;
+};
+
+/* kernels (wq3d_kernels.cu) */
+__global__ void k_startup(const QueueDev* q);
+__global__ void k_step(const QueueDev* q, int k);
+__global__ void k_edges(const QueueDev* q, int k);
+__global__ void k_cpa(const QueueDev* q, int k);
+__global__ void k_eigenray(const QueueDev* q, int k);
+__global__ void k_sound_speed(OceanDev oc, double R, int n, const double* rho,
+                              const double* theta, const double* phi,
+                              double* c, double* g);
+__global__ void k_height(BoundaryDev b, int n, const double* theta,
+                         const double* phi, double* h, double* nrm);
+__global__ void k_reflect_loss(BoundaryDev b, int n, const double* grazing,
+                               int nf, const double* freq, double* amp,
+                               double* ph);
+
+constexpr int CPA_THREADS = 128;     /* rays per CPA block            */
+constexpr int CPA_TARGETS = 64;      /* targets per CPA block (tile)  */
+
+}  // namespace wq3d

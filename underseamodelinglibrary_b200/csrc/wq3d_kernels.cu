@@ -1,0 +1,1340 @@
+/*
+ * wq3d_kernels.cu -- FP64 WaveQ3D propagation kernels for sm_100a.
+ *
+ * One step of wave_queue::step() (waveq3d/wave_queue.cc:155-192) is four
+ * launches:
+ *   k_step      one thread per ray: caustic hand-off from the D/E
+ *               neighbour, surface/bottom reflections with the RK3
+ *               re-initialisation, vertices, the queue rotation, the AB3
+ *               step and wave_front::update of the new front.
+ *   k_edges     one thread per ray: wave_front::find_edges on the front
+ *               that became "curr".
+ *   k_cpa       rays x targets: closest-point-of-approach test
+ *               (detect_eigenrays + is_closest_ray) with distance2
+ *               recomputed from per-front terms; the dominant kernel.
+ *   k_eigenray  one thread per CPA found: build_eigenray, compute_offsets,
+ *               hybrid Gaussian or classic spreading, target angles.
+ * All ray-local work of a step is fused into k_step because reflections
+ * and the AB3 step of a ray read only that ray's four fronts.  The only
+ * cross-ray reads in k_step are the D/E neighbour's values for the caustic
+ * test, which that neighbour leaves untouched unless it reflects; whether
+ * it reflects was decided by the previous launch and is read from a flag.
+ *
+ * Compiled with --fmad=false: every add and multiply rounds as in the
+ * reference, so the FP64 form differs from the CPU oracle only through the
+ * last-place differences between CUDA's and the host's sin/cos/exp.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "wq3d_engine.cuh"
+
+namespace wq3d {
+
+namespace {
+
+struct RayS {
+    double pos[3];
+    double pg[3];
+    double nd[3];
+    double ng[3];
+    double c;
+    double sg[3];
+    double dist;
+};
+
+struct Roles {
+    const FrontPtrs* P;
+    const FrontPtrs* V;
+    const FrontPtrs* C;
+    const FrontPtrs* X;
+};
+
+__device__ __forceinline__ void roles_at(const QueueDev& q, int64_t s,
+                                         Roles& r) {
+    r.P = &q.F[s & 3];
+    r.V = &q.F[(s + 1) & 3];
+    r.C = &q.F[(s + 2) & 3];
+    r.X = &q.F[(s + 3) & 3];
+}
+
+__device__ __forceinline__ void set_err(const QueueDev& q, uint32_t bit) {
+    atomicOr(q.err, bit);
+}
+
+/* profile evaluation for one point (analytic profiles have no horizontal
+ * gradient) */
+__device__ __forceinline__ void profile_at(const QueueDev& q, const double* pos,
+                                           double* c, double* sg) {
+    double gr;
+    sound_speed(q.oc.prof, q.R, pos[0], c, &gr);
+    sg[0] = gr;
+    sg[1] = 0.0;
+    sg[2] = 0.0;
+}
+
+/* wave_front::update on a 1x1 front without targets */
+__device__ __forceinline__ void update1(const QueueDev& q, RayS& y) {
+    profile_at(q, y.pos, &y.c, y.sg);
+    double st;
+    ray_derivs(y.c, y.sg[0], y.sg[1], y.sg[2], y.pos, y.nd, y.pg, y.ng, &st);
+}
+
+/* ode_integ.cc:20-126 */
+__device__ __forceinline__ void rk1(double h, const RayS& y0, RayS& y1) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        y1.pos[k] = y0.pos[k] + 0.5 * h * y0.pg[k];
+        y1.nd[k] = y0.nd[k] + 0.5 * h * y0.ng[k];
+    }
+}
+__device__ __forceinline__ void rk2(double h, const RayS& y0, const RayS& y1,
+                                    RayS& y2) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        y2.pos[k] = y0.pos[k] + h * (2.0 * y1.pg[k] - y0.pg[k]);
+        y2.nd[k] = y0.nd[k] + h * (2.0 * y1.ng[k] - y0.ng[k]);
+    }
+}
+__device__ __forceinline__ void rk3(double h, const RayS& y0, const RayS& y1,
+                                    const RayS& y2, RayS& y3) {
+    double p[3], d[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        p[k] = y0.pos[k] + h / 6.0 * (y0.pg[k] + 4.0 * y1.pg[k] + y2.pg[k]);
+        d[k] = y0.nd[k] + h / 6.0 * (y0.ng[k] + 4.0 * y1.ng[k] + y2.ng[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        y3.pos[k] = p[k];
+        y3.nd[k] = d[k];
+    }
+}
+/* ode_integ.cc:131-186, including the step distance of ab3_pos */
+__device__ __forceinline__ void ab3(double h, const RayS& y0, const RayS& y1,
+                                    const RayS& y2, RayS& y3) {
+    const double A2 = 23.0 / 12.0, A1 = 16.0 / 12.0, A0 = 5.0 / 12.0;
+    double d[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        d[k] = h * (A2 * y2.pg[k] - A1 * y1.pg[k] + A0 * y0.pg[k]);
+    const double b = y2.pos[0] * d[1];
+    const double cc = y2.pos[0] * (sin(y2.pos[1]) * d[2]);
+    y3.dist = sqrt(d[0] * d[0] + b * b + cc * cc);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        y3.pos[k] = y2.pos[k] + d[k];
+        y3.nd[k] = y2.nd[k] + h * (A2 * y2.ng[k] - A1 * y1.ng[k] + A0 * y0.ng[k]);
+    }
+}
+
+__device__ __forceinline__ void load_ray(const FrontPtrs& f, int r, RayS& y) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        y.pos[k] = f.pos[k][r];
+        y.pg[k] = f.pg[k][r];
+        y.nd[k] = f.nd[k][r];
+        y.ng[k] = f.ng[k][r];
+        y.sg[k] = f.sg[k][r];
+    }
+    y.c = f.c[r];
+    y.dist = f.dist[r];
+}
+
+/* reflection_model::reflection_copy (reflection_model.cc:335-360); the
+ * copied path_length of a fresh 1x1 front is zero, so it is left alone */
+__device__ __forceinline__ void copy_ray(const FrontPtrs& f, int r, const RayS& y) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        f.pos[k][r] = y.pos[k];
+        f.pg[k][r] = y.pg[k];
+        f.nd[k][r] = y.nd[k];
+        f.ng[k][r] = y.ng[k];
+        f.sg[k][r] = y.sg[k];
+    }
+    f.c[r] = y.c;
+    f.dist[r] = y.dist;
+}
+
+/* wave_front::update of the main front for one ray: profile, attenuation
+ * (attenuation_thorp.cc:14-36 / attenuation_constant.cc:14-25), cleared
+ * phase, derivatives and the distance2 terms */
+__device__ __forceinline__ void update_main(const QueueDev& q, const FrontPtrs& f,
+                                            int r, RayS& y, bool accumulate,
+                                            const FrontPtrs* src) {
+    profile_at(q, y.pos, &y.c, y.sg);
+    double st;
+    ray_derivs(y.c, y.sg[0], y.sg[1], y.sg[2], y.pos, y.nd, y.pg, y.ng, &st);
+    copy_ray(f, r, y);
+    f.cpa[0][r] = y.pos[0];
+    f.cpa[1][r] = y.pos[1];
+    f.cpa[2][r] = y.pos[2];
+    f.cpa[3][r] = st;
+    const double alt = y.pos[0] - q.R;
+    for (int k = 0; k < q.nf; ++k) {
+        double a;
+        if (q.oc.prof.atten == WQ3D_ATTEN_CONSTANT) {
+            a = q.oc.prof.atten_coef * y.dist * q.freq[k];
+        } else {
+            a = y.dist * q.alpha[k] * (1.0 + 5.88264e-6 * alt);
+        }
+        double p = 0.0;
+        if (accumulate) {
+            a += src->atten[(size_t)k * q.n + r];
+            p += src->phase[(size_t)k * q.n + r];
+        }
+        f.atten[(size_t)k * q.n + r] = a;
+        f.phase[(size_t)k * q.n + r] = p;
+    }
+}
+
+/* wave_queue::collision_location (wave_queue.cc:982-1057) */
+__device__ void collision_location(const QueueDev& q, const FrontPtrs& V,
+                                   const FrontPtrs& C, const FrontPtrs& X, int i,
+                                   double tw, double* pos, double* nd,
+                                   double* speed) {
+    const double dt = q.dt;
+    const double time1 = 2.0 * dt;
+    const double time2 = dt * dt;
+    const double dtime2 = tw * tw;
+    const double drho = (X.c[i] - V.c[i]) / time1;
+    const double d2rho = (X.c[i] + V.c[i] - 2.0 * C.c[i]) / time2;
+    *speed = C.c[i] + drho * tw + 0.5 * d2rho * dtime2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double v1 = (X.pos[k][i] - V.pos[k][i]) / time1;
+        const double v2 = (X.pos[k][i] + V.pos[k][i] - 2.0 * C.pos[k][i]) / time2;
+        pos[k] = C.pos[k][i] + v1 * tw + 0.5 * v2 * dtime2;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double v1 = (X.nd[k][i] - V.nd[k][i]) / time1;
+        const double v2 = (X.nd[k][i] + V.nd[k][i] - 2.0 * C.nd[k][i]) / time2;
+        nd[k] = C.nd[k][i] + v1 * tw + 0.5 * v2 * dtime2;
+    }
+}
+
+/* reflection_model::reflection_reinit (reflection_model.cc:248-330).
+ * Keeps the reference's past.update() at :315, which leaves "temp" with
+ * the derivatives of its first update. */
+__device__ void reflection_reinit(const QueueDev& q, const Roles& R, int i,
+                                  double tw, const double* pos,
+                                  const double* nd) {
+    RayS past1, prev1, curr1, next1, temp;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        temp.pos[k] = pos[k];
+        temp.nd[k] = nd[k];
+    }
+    next1.dist = 0.0;
+    past1.dist = 0.0;
+    prev1.dist = 0.0;
+    curr1.dist = 0.0;
+    temp.dist = 0.0;
+    update1(q, temp);
+    rk1(-tw, temp, next1);
+    update1(q, next1);
+    rk2(-tw, temp, next1, past1);
+    update1(q, past1);
+    rk3(-tw, temp, next1, past1, curr1);
+    update1(q, curr1);
+    copy_ray(*R.C, i, curr1);
+
+    const double h = q.dt;
+    rk1(-h, curr1, next1);
+    update1(q, next1);
+    rk2(-h, curr1, next1, past1);
+    update1(q, past1);
+    rk3(-h, curr1, next1, past1, prev1);
+    update1(q, prev1);
+    copy_ray(*R.V, i, prev1);
+
+    rk1(-h, prev1, next1);
+    update1(q, next1);
+    rk2(-h, prev1, next1, temp);
+    rk3(-h, prev1, next1, temp, past1);
+    update1(q, past1);
+    copy_ray(*R.P, i, past1);
+
+    ab3(h, past1, prev1, curr1, next1);
+    update1(q, next1);
+    copy_ray(*R.X, i, next1);
+}
+
+__device__ void record_reflection(const QueueDev& q, int64_t step, double t_old,
+                                  int i, double tw, double grazing, double c,
+                                  const double* pos, const double* nd, int type,
+                                  int seq) {
+    if (!q.want_refl) return;
+    const uint32_t slot = atomicAdd(q.n_refl, 1u);
+    if (slot >= q.cap_refl) {
+        set_err(q, ERR_REFL_OVERFLOW);
+        return;
+    }
+    wq3d_reflection r;
+    r.time = t_old + tw;
+    r.dt = tw;
+    r.grazing = grazing;
+    r.speed = c;
+    for (int k = 0; k < 3; ++k) {
+        r.position[k] = pos[k];
+        r.ndirection[k] = nd[k];
+    }
+    r.de = i / q.naz;
+    r.az = i % q.naz;
+    r.type = type;
+    r.pad = seq;
+    r.step = step;
+    q.refl[slot] = r;
+}
+
+/* reflection_model::surface_reflection (reflection_model.cc:187-243) */
+__device__ bool surface_reflection(const QueueDev& q, const Roles& R, int i,
+                                   int64_t step, double t_old, int seq) {
+    double c = R.C->c[i];
+    const double d = c * c * R.C->nd[0][i];
+    const double tw = (d == 0.0) ? 0.0 : -(R.C->pos[0][i] - q.R) / d;
+    double pos[3], nd[3];
+    collision_location(q, *R.V, *R.C, *R.X, i, tw, pos, nd, &c);
+    const double n1 = R.C->nd[1][i], n2 = R.C->nd[2][i];
+    const double grazing = atan2(R.C->nd[0][i], sqrt(n1 * n1 + n2 * n2));
+    if (grazing <= 0.0) return false;
+    record_reflection(q, step, t_old, i, tw, grazing, c, pos, nd, 1, seq);
+    const LossDev& L = q.oc.surf.loss;
+    double amp0, ph0;
+    if (L.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(L, grazing, &amp0, &ph0);
+    const double w2 = L.p[0] * L.p[0];
+    const double sg = sin(grazing);
+    for (int k = 0; k < q.nf; ++k) {
+        double a = amp0;
+        if (L.kind == WQ3D_LOSS_ECKART) {
+            const double x = q.freq[k] * w2 * sg;
+            a = 8.6e-9 * (x * x);
+        }
+        const size_t o = (size_t)k * q.n + i;
+        R.X->atten[o] += a;
+        R.X->phase[o] -= M_PI;
+    }
+    nd[0] = -nd[0];
+    reflection_reinit(q, R, i, tw, pos, nd);
+    return true;
+}
+
+/* reflection_model::bottom_reflection (reflection_model.cc:33-182) */
+__device__ void bottom_reflection(const QueueDev& q, const Roles& R, int i,
+                                  double depth, int64_t step, double t_old,
+                                  int seq) {
+    const BoundaryDev& B = q.oc.bot;
+    bool shallow = false;
+    double position[3] = {R.C->pos[0][i], R.C->pos[1][i], R.C->pos[2][i]};
+    double ndir[3] = {R.C->nd[0][i], R.C->nd[1][i], R.C->nd[2][i]};
+    double c = R.C->c[i];
+    double c2 = c * c;
+    double nrm[3] = {B.normal[0], B.normal[1], B.normal[2]};
+    double bottom_rho = boundary_height(B, position[1], position[2]);
+    double height_water = position[0] - bottom_rho;
+    const double TOO_SHALLOW = 300.0 * q.dt;
+    if ((q.R - bottom_rho) < TOO_SHALLOW) shallow = true;
+    double N;
+    if (shallow) {
+        N = sqrt(nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        nrm[0] = 0.0;
+        nrm[1] = nrm[1] / N;
+        nrm[2] = nrm[2] / N;
+    }
+    ndir[0] = c2 * ndir[0];
+    ndir[1] = c2 * ndir[1];
+    ndir[2] = c2 * ndir[2];
+    double dot_full = nrm[0] * ndir[0] + nrm[1] * ndir[1] + nrm[2] * ndir[2];
+    const double MIN_REFLECT = 6.0;
+    double max_dot = -fmax(MIN_REFLECT, (height_water + depth) * nrm[0]);
+    if (dot_full >= max_dot) dot_full = max_dot;
+    const double dot_water = -height_water * nrm[0];
+    const double time_water = fmax(0.0, dot_water / dot_full);
+
+    collision_location(q, *R.V, *R.C, *R.X, i, time_water, position, ndir, &c);
+    bottom_rho = boundary_height(B, position[1], position[2]);
+    nrm[0] = B.normal[0];
+    nrm[1] = B.normal[1];
+    nrm[2] = B.normal[2];
+    if (shallow) {
+        N = sqrt(nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        nrm[0] = 0.0;
+        nrm[1] = nrm[1] / N;
+        nrm[2] = nrm[2] / N;
+    }
+    c2 = c * c;
+    height_water = position[0] - bottom_rho;
+    ndir[0] = c2 * ndir[0];
+    ndir[1] = c2 * ndir[1];
+    ndir[2] = c2 * ndir[2];
+    dot_full = nrm[0] * ndir[0] + nrm[1] * ndir[1] + nrm[2] * ndir[2];
+    max_dot = -fmax(MIN_REFLECT, (height_water + depth) * nrm[0]);
+    if (dot_full >= max_dot) dot_full = max_dot;
+
+    double grazing;
+    if (dot_full / c >= 1.0) {
+        grazing = -M_PI_2;
+    } else if (dot_full / c <= -1.0) {
+        grazing = M_PI_2;
+    } else {
+        grazing = asin(-dot_full / c);
+    }
+    record_reflection(q, step, t_old, i, time_water, grazing, c, position, ndir, 0, seq);
+
+    const LossDev& L = B.loss;
+    double amp0 = 0.0, ph0 = 0.0;
+    if (L.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(L, grazing, &amp0, &ph0);
+    const double w2 = L.p[0] * L.p[0];
+    const double sgz = sin(grazing);
+    for (int k = 0; k < q.nf; ++k) {
+        double a = amp0, p = ph0;
+        if (L.kind == WQ3D_LOSS_ECKART) {
+            const double x = q.freq[k] * w2 * sgz;
+            a = 8.6e-9 * (x * x);
+            p = M_PI;
+        }
+        const size_t o = (size_t)k * q.n + i;
+        R.X->atten[o] += a;
+        R.X->phase[o] += p;
+    }
+    dot_full *= 2.0;
+    ndir[0] = ndir[0] - dot_full * nrm[0];
+    ndir[1] = ndir[1] - dot_full * nrm[1];
+    ndir[2] = ndir[2] - dot_full * nrm[2];
+    N = sqrt(ndir[0] * ndir[0] + ndir[1] * ndir[1] + ndir[2] * ndir[2]) * c;
+    ndir[0] = ndir[0] / N;
+    ndir[1] = ndir[1] / N;
+    ndir[2] = ndir[2] / N;
+    reflection_reinit(q, R, i, time_water, position, ndir);
+}
+
+/* whether the "next" ray reflects at the start of the following step:
+ * surface if above the surface and heading up (surface_reflection's
+ * grazing > 0), else bottom if below the bottom (wave_queue.cc:222-256) */
+__device__ __forceinline__ uint8_t reflect_decision(const QueueDev& q,
+                                                    const double* xpos,
+                                                    const double* cnd) {
+    if (xpos[0] - q.R > 0.0) {
+        const double grazing = atan2(cnd[0], sqrt(cnd[1] * cnd[1] + cnd[2] * cnd[2]));
+        if (grazing > 0.0) return 1;
+    }
+    const double h = boundary_height(q.oc.bot, xpos[1], xpos[2]);
+    return (h - xpos[0] > 0.0) ? 1 : 0;
+}
+
+__device__ __forceinline__ void inc_count(const Roles& R, int32_t* FrontPtrs::*field, int i) {
+    const int32_t v = (R.X->*field)[i] + 1;
+    (R.X->*field)[i] = v;
+    (R.C->*field)[i] = v;
+    (R.V->*field)[i] = v;
+    (R.P->*field)[i] = v;
+}
+
+}  // namespace
+
+/* ------------------------------------------------------------------ */
+/* start-up: wave_queue ctor (wave_queue.cc:83-85) for one ray         */
+/* ------------------------------------------------------------------ */
+__global__ void __launch_bounds__(128) k_startup(const QueueDev* __restrict__ qp) {
+    const QueueDev& q = *qp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q.n) return;
+    const int d = i / q.naz, a = i % q.naz;
+    const FrontPtrs& past = q.F[0];
+    const FrontPtrs& prev = q.F[1];
+    const FrontPtrs& curr = q.F[2];
+    const FrontPtrs& next = q.F[3];
+    /* wave_front::init_wave (wave_front.cc:84-121) */
+    RayS c0;
+    c0.nd[0] = q.sin_de[d] / q.c_source;
+    c0.nd[1] = (-q.cos_de[d] * q.cos_az[a]) / q.c_source;
+    c0.nd[2] = (q.cos_de[d] * q.sin_az[a]) / q.c_source;
+    c0.pos[0] = q.source[0];
+    c0.pos[1] = q.source[1];
+    c0.pos[2] = q.source[2];
+    c0.dist = 0.0;
+    update_main(q, curr, i, c0, false, nullptr);
+    /* init_wavefronts (wave_queue.cc:114-150); intermediate updates of the
+     * reference's _next land in registers, only final values are stored */
+    const double h = -q.dt;
+    RayS n1, p1, v1;
+    n1.dist = 0.0;
+    p1.dist = 0.0;
+    v1.dist = 0.0;
+    rk1(h, c0, n1);
+    update1(q, n1);
+    rk2(h, c0, n1, p1);
+    update1(q, p1);
+    rk3(h, c0, n1, p1, v1);
+    update_main(q, prev, i, v1, false, nullptr);
+    rk1(h, v1, n1);
+    update1(q, n1);
+    rk2(h, v1, n1, p1);
+    update1(q, p1);
+    rk3(h, v1, n1, p1, p1);
+    update_main(q, past, i, p1, false, nullptr);
+    RayS x;
+    ab3(q.dt, p1, v1, c0, x);
+    update_main(q, next, i, x, false, nullptr);
+    next.plen[i] = x.dist + 0.0;
+    curr.plen[i] = 0.0;
+    prev.plen[i] = 0.0;
+    past.plen[i] = 0.0;
+    for (int f = 0; f < 4; ++f) {
+        const FrontPtrs& F = q.F[f];
+        F.surface[i] = 0;
+        F.bottom[i] = 0;
+        F.caustic[i] = 0;
+        F.upper[i] = 0;
+        F.lower[i] = 0;
+        F.on_edge[i] = 0;
+    }
+    q.flag[0][i] = reflect_decision(q, x.pos, c0.nd);
+    (void)a;
+}
+
+/* ------------------------------------------------------------------ */
+/* one step for one ray                                                */
+/* ------------------------------------------------------------------ */
+__global__ void __launch_bounds__(128) k_step(const QueueDev* __restrict__ qp, int k) {
+    const QueueDev& q = *qp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t s = *q.d_base + k;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *q.n_cand = 0;
+    if (i >= q.n) return;
+    const double t_old = q.d_times[k];
+    Roles R;
+    roles_at(q, s, R);
+    const int d = i / q.naz;
+    const uint8_t* flag_in = q.flag[s & 1];
+    uint8_t* flag_out = q.flag[(s + 1) & 1];
+
+    /* detect_caustics of the D/E neighbour below (wave_queue.cc:274-292):
+     * the reference runs it for ray (d-1) before ray d is reflected */
+    if (d >= 1 && !flag_in[i - q.naz]) {
+        const int j = i - q.naz;
+        const double A = R.C->pos[0][i];
+        const double B = R.C->pos[0][j];
+        const double Cc = R.X->pos[0][i];
+        const double D = R.X->pos[0][j];
+        const bool fold = (R.X->surface[i] == R.X->surface[j]) && (R.X->bottom[i] == R.X->bottom[j]);
+        if ((Cc - D) * (A - B) < 0 && fold) {
+            R.X->caustic[i] += 1;
+            for (int f = 0; f < q.nf; ++f) R.X->phase[(size_t)f * q.n + i] -= M_PI_2;
+        }
+    }
+
+    /* detect_reflections for this ray (wave_queue.cc:197-256) */
+    bool reflected = false;
+    int seq = 0;
+    int next_try = -1; /* 0: try bottom next, 1: try surface next */
+    if (R.X->pos[0][i] - q.R > 0.0 && surface_reflection(q, R, i, s + 1, t_old, seq)) {
+        ++seq;
+        inc_count(R, &FrontPtrs::surface, i);
+        reflected = true;
+        next_try = 0;
+    } else {
+        const double depth = boundary_height(q.oc.bot, R.X->pos[1][i], R.X->pos[2][i]) - R.X->pos[0][i];
+        if (depth > 0.0) {
+            bottom_reflection(q, R, i, depth, s + 1, t_old, seq);
+            ++seq;
+            inc_count(R, &FrontPtrs::bottom, i);
+            reflected = true;
+            next_try = 1;
+        }
+    }
+    if (reflected) {
+        int it = 0;
+        for (; it < MAX_BOUNCE; ++it) {
+            if (next_try == 0) {
+                const double depth = boundary_height(q.oc.bot, R.X->pos[1][i], R.X->pos[2][i]) - R.X->pos[0][i];
+                if (!(depth > 0.0)) break;
+                bottom_reflection(q, R, i, depth, s + 1, t_old, seq);
+                ++seq;
+                inc_count(R, &FrontPtrs::bottom, i);
+                next_try = 1;
+            } else {
+                if (!(R.X->pos[0][i] - q.R > 0.0 && surface_reflection(q, R, i, s + 1, t_old, seq))) break;
+                ++seq;
+                inc_count(R, &FrontPtrs::surface, i);
+                next_try = 0;
+            }
+        }
+        if (it == MAX_BOUNCE) set_err(q, ERR_BOUNCE_LIMIT);
+    } else {
+        /* detect_vertices (wave_queue.cc:261-269) */
+        const double L = R.C->nd[0][i];
+        const double Rn = R.X->nd[0][i];
+        if (L * Rn < 0.0 && Rn < 0.0) {
+            R.X->upper[i] += 1;
+        } else if (L * Rn < 0.0 && 0.0 < Rn) {
+            R.X->lower[i] += 1;
+        }
+    }
+
+    /* rotate (wave_queue.cc:162-167): past<-prev, prev<-curr, curr<-next,
+     * next<-old past; then AB3 and update (wave_queue.cc:171-183) */
+    RayS y0, y1, y2, y3;
+    load_ray(*R.V, i, y0);
+    load_ray(*R.C, i, y1);
+    load_ray(*R.X, i, y2);
+    ab3(q.dt, y0, y1, y2, y3);
+    update_main(q, *R.P, i, y3, true, R.X);
+    R.P->plen[i] = y3.dist + R.X->plen[i];
+    R.P->surface[i] = R.X->surface[i];
+    R.P->bottom[i] = R.X->bottom[i];
+    R.P->upper[i] = R.X->upper[i];
+    R.P->lower[i] = R.X->lower[i];
+    R.P->caustic[i] = R.X->caustic[i];
+    flag_out[i] = reflect_decision(q, y3.pos, y2.nd);
+}
+
+/* ------------------------------------------------------------------ */
+/* wave_front::find_edges (wave_front.cc:184-216) on the new "curr"     */
+/* ------------------------------------------------------------------ */
+__global__ void __launch_bounds__(128) k_edges(const QueueDev* __restrict__ qp, int k) {
+    const QueueDev& q = *qp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q.n) return;
+    const int64_t s = *q.d_base + k;
+    const FrontPtrs& f = q.F[(s + 3) & 3];
+    const int naz = q.naz;
+    const int d = i / naz;
+    const int max_de = q.nde - 1;
+    const double* rho = f.pos[0];
+    const double* ndr = f.nd[0];
+    auto extremum = [&](int dd) -> bool {
+        if (dd < 1 || dd > max_de - 1) return false;
+        const int j = i + (dd - d) * naz;
+        const double r0 = rho[j], rp = rho[j + naz], rm = rho[j - naz];
+        return (r0 < rp && r0 < rm) || (r0 > rp && r0 > rm);
+    };
+    bool edge = (d == 0) || (d == max_de) || extremum(d);
+    if (!edge && extremum(d + 1)) {
+        /* ray d+1 is an extremum and marks d when |n(d+1)-n(d)| > |n(d+1)-n(d+2)| */
+        const double n0 = ndr[i + naz];
+        if (fabs(n0 - ndr[i]) > fabs(n0 - ndr[i + 2 * naz])) edge = true;
+    }
+    if (!edge && extremum(d - 1)) {
+        const double n0 = ndr[i - naz];
+        if (!(fabs(n0 - ndr[i - 2 * naz]) > fabs(n0 - ndr[i]))) edge = true;
+    }
+    f.on_edge[i] = edge ? 1 : 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* CPA search (wave_queue.cc:351-488)                                  */
+/* ------------------------------------------------------------------ */
+namespace {
+
+struct TgtS {
+    double th, ph, sn, R2, twoR;
+};
+
+__device__ __forceinline__ double d2_at(const FrontPtrs& f, int i, const TgtS& t) {
+    const double rho = f.cpa[0][i];
+    return target_distance2(rho, rho * rho, f.cpa[1][i], f.cpa[2][i], f.cpa[3][i],
+                            t.th, t.ph, t.sn, t.R2, t.twoR);
+}
+
+__device__ __forceinline__ int wrap_az(const QueueDev& q, int az, int na) {
+    int a = az + na - 1;
+    if (q.az_boundary) {
+        if (az + na == 0) {
+            a = q.naz - 2;
+        } else if (a >= q.naz - 1) {
+            a = 0;
+        }
+    }
+    return a;
+}
+
+/* is_closest_ray (wave_queue.cc:411-488); also fills the cube */
+__device__ bool is_closest(const QueueDev& q, const FrontPtrs& V, const FrontPtrs& C,
+                           const FrontPtrs& X, const TgtS& t, bool de_branch, int de,
+                           int az, double center, double cube[3][3][3]) {
+    const int max_az = q.naz - 1;
+    for (int nd_ = 0; nd_ < 3; ++nd_) {
+        for (int na = 0; na < 3; ++na) {
+            if (nd_ == 1 && na == 1) continue;
+            const int d = de + nd_ - 1;
+            const int a = wrap_az(q, az, na);
+            const int i = d * q.naz + a;
+            cube[0][nd_][na] = d2_at(V, i, t);
+            cube[1][nd_][na] = d2_at(C, i, t);
+            cube[2][nd_][na] = d2_at(X, i, t);
+            if (a == 0 && !q.az_boundary) continue;
+            if (a == max_az) continue;
+            if (de_branch) {
+                if (C.on_edge[i]) continue;
+            } else {
+                if (nd_ != 1 && C.on_edge[i]) continue;
+            }
+            if (nd_ == 2 || na == 2) {
+                if (de_branch) {
+                    if (az == 0) {
+                        if (cube[1][nd_][na] < center) return false;
+                    } else {
+                        return false;
+                    }
+                } else {
+                    if (cube[1][nd_][na] <= center) return false;
+                }
+            } else {
+                if (cube[1][nd_][na] < center) return false;
+            }
+            if (cube[2][nd_][na] <= center) return false;
+            if (cube[0][nd_][na] < center) return false;
+        }
+    }
+    return true;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(CPA_THREADS) k_cpa(const QueueDev* __restrict__ qp, int k) {
+    const QueueDev& q = *qp;
+    __shared__ TgtS tile[CPA_TARGETS];
+    const int64_t s = *q.d_base + k + 1; /* roles after this step's rotation */
+    const FrontPtrs& V = q.F[(s + 1) & 3];
+    const FrontPtrs& C = q.F[(s + 2) & 3];
+    const FrontPtrs& X = q.F[(s + 3) & 3];
+    const int t0 = blockIdx.y * CPA_TARGETS;
+    const int nt_tile = min(CPA_TARGETS, q.nt - t0);
+    for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
+        const int t = t0 + j;
+        tile[j] = TgtS{q.tgt[1][t], q.tgt[2][t], q.tgt_sin[t], q.tgt_R2[t], q.tgt_2R[t]};
+    }
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q.n) return;
+    /* the spreading models need a 3 x 3 fan (wave_queue.cc:88); the
+     * reference would dereference a null model on a wrapped 2-ray AZ fan */
+    if (q.nde < 3 || q.naz < 3) return;
+    const int de = i / q.naz, az = i % q.naz;
+    const int az_start = q.az_boundary ? 0 : 1;
+    if (de < 1 || de >= q.nde - 1 || az < az_start || az >= q.naz - 1) return;
+    if (C.on_edge[i]) return;
+    const double rC = C.cpa[0][i], tC = C.cpa[1][i], pC = C.cpa[2][i], sC = C.cpa[3][i];
+    const double rX = X.cpa[0][i], tX = X.cpa[1][i], pX = X.cpa[2][i], sX = X.cpa[3][i];
+    const double rV = V.cpa[0][i], tV = V.cpa[1][i], pV = V.cpa[2][i], sV = V.cpa[3][i];
+    const double rC2 = rC * rC, rX2 = rX * rX, rV2 = rV * rV;
+    for (int j = 0; j < nt_tile; ++j) {
+        const TgtS t = tile[j];
+        const double center = target_distance2(rC, rC2, tC, pC, sC, t.th, t.ph, t.sn, t.R2, t.twoR);
+        const double dn = target_distance2(rX, rX2, tX, pX, sX, t.th, t.ph, t.sn, t.R2, t.twoR);
+        if (dn <= center) continue;
+        const double dp = target_distance2(rV, rV2, tV, pV, sV, t.th, t.ph, t.sn, t.R2, t.twoR);
+        if (dp < center) continue;
+        double cube[3][3][3];
+        if (!is_closest(q, V, C, X, t, q.de_branch[t0 + j] != 0, de, az, center, cube)) continue;
+        const uint32_t slot = atomicAdd(q.n_cand, 1u);
+        if (slot < q.cap_cand) {
+            q.cand[2 * slot] = (uint32_t)(t0 + j);
+            q.cand[2 * slot + 1] = (uint32_t)i;
+        } else {
+            set_err(q, ERR_CAND_OVERFLOW);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* eigenray construction (wave_queue.cc:495-977 + spreading models)    */
+/* ------------------------------------------------------------------ */
+namespace {
+
+struct Build {
+    const QueueDev* q;
+    const FrontPtrs* pV;
+    const FrontPtrs* pC;
+    const FrontPtrs* pX;
+    int t;
+    double inten_de[MAX_FREQ];
+    double inten_az[MAX_FREQ];
+    const double* spread2;
+    uint32_t dup[MAX_AZ / 32];
+
+    __device__ double fdist(const FrontPtrs& f, int d1, int a1, int d2, int a2) const {
+        const int i = d1 * q->naz + a1, j = d2 * q->naz + a2;
+        return sqrt(wdist2(f.pos[0][i], f.pos[1][i], f.pos[2][i], f.pos[0][j],
+                           f.pos[1][j], f.pos[2][j]));
+    }
+    __device__ double de_inc(int d) const { return q->de_inc[min(max(d, 0), q->nde - 1)]; }
+    __device__ double az_inc(int a) const { return q->az_inc[min(max(a, 0), q->naz - 1)]; }
+
+    /* spreading_hybrid_gaussian.h:148-153, accumulated into acc */
+    __device__ void gauss_add(double d, double w, double A, double* acc, bool first) {
+        for (int k = 0; k < q->nf; ++k) {
+            const double bw = spread2[k] + 2.0 * 2.0 * w * w;
+            const double g = exp((-0.5 * d * d) / bw) / sqrt(bw) * A;
+            acc[k] = first ? g : acc[k] + g;
+        }
+    }
+
+    /* spreading_hybrid_gaussian.cc:430-495 */
+    __device__ double width_de(int d, int a, const double* offset) {
+        const double u = fabs(offset[0]) / q->dt;
+        const double v = fabs(offset[2]) / az_inc(a);
+        const int max_az = q->naz - 1;
+        const int az_wrap = (a + 1 >= max_az) ? 0 : a + 1;
+        const FrontPtrs& C = *pC;
+        double L1 = fdist(C, d, a, d + 1, a), L2, length1, length2;
+        if (v < 1e-10) {
+            length1 = L1;
+        } else {
+            L2 = fdist(C, d, az_wrap, d + 1, az_wrap);
+            length1 = (1.0 - v) * L1 + v * L2;
+        }
+        if (u < 1e-10) return 0.5 * length1;
+        const FrontPtrs& p2 = (offset[0] < 0.0) ? *pV : *pX;
+        L1 = fdist(p2, d, a, d + 1, a);
+        if (v < 1e-10) {
+            length2 = L1;
+        } else {
+            L2 = fdist(p2, d, az_wrap + 1, d + 1, az_wrap + 1);
+            length2 = (1.0 - v) * L1 + v * L2;
+        }
+        return 0.5 * ((1.0 - u) * length1 + u * length2);
+    }
+
+    /* spreading_hybrid_gaussian.cc:500-571 */
+    __device__ double width_az(int d, int a, const double* offset) {
+        const double u = fabs(offset[0]) / q->dt;
+        const double v = fabs(offset[1]) / de_inc(d);
+        const int max_az = q->naz - 1;
+        const int max_de = q->nde - 1;
+        const int de_upper = (d + 1 >= max_de) ? max_de - 2 : d;
+        const int az_wrap = (a + 1 > max_az) ? 0 : a + 1;
+        const FrontPtrs& C = *pC;
+        double L1 = fdist(C, d, a, d, az_wrap), L2, length1, length2;
+        if (v < 1e-10 || fabs(v - 1.0) < 1e-10) {
+            length1 = L1;
+        } else {
+            L2 = fdist(C, de_upper + 1, a, de_upper + 1, az_wrap);
+            length1 = (1.0 - v) * L1 + v * L2;
+        }
+        if (u < 1e-10) return 0.5 * length1;
+        const FrontPtrs& p2 = (offset[0] < 0.0) ? *pV : *pX;
+        L1 = fdist(p2, d, a, d, az_wrap);
+        if (v < 1e-10 || fabs(v - 1.0) < 1e-10) {
+            length2 = L1;
+        } else {
+            L2 = fdist(p2, de_upper + 1, a, de_upper + 1, az_wrap);
+            length2 = (1.0 - v) * L1 + v * L2;
+        }
+        return 0.5 * ((1.0 - u) * length1 + u * length2);
+    }
+
+    /* spreading_hybrid_gaussian.cc:124-258 */
+    __device__ void intensity_de(int de0, int a, const double* offset, const double* distance) {
+        const QueueDev& Q = *q;
+        const FrontPtrs& C = *pC;
+        int d = de0;
+        double cell_width = width_de(d, a, offset);
+        const double initial_width = cell_width;
+        const double L = distance[1];
+        double cell_dist = L - cell_width;
+        gauss_add(cell_dist, cell_width, Q.norm_de[d], inten_de, true);
+        d = de0 - 1;
+        cell_width = width_de(d, a, offset);
+        cell_dist = L + cell_width;
+        gauss_add(cell_dist, cell_width, Q.norm_de[d], inten_de, false);
+        if (inten_de[0] < 1e-10) return;
+        for (d = de0 - 2; d >= 0; --d) {
+            const bool virtual_ray = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
+            double new_norm;
+            cell_dist += cell_width;
+            if (virtual_ray) {
+                cell_dist += cell_width;
+                new_norm = Q.norm_de[d + 1];
+            } else {
+                cell_width = width_de(d, a, offset);
+                cell_dist += cell_width;
+                new_norm = Q.norm_de[d];
+            }
+            const double old_tl = inten_de[0];
+            gauss_add(cell_dist, cell_width, new_norm, inten_de, false);
+            if (inten_de[0] / old_tl < 1.002305238) break;
+            if (virtual_ray) break;
+        }
+        cell_width = initial_width;
+        cell_dist = L - cell_width;
+        const int size = Q.nde - 1;
+        for (d = de0 + 1; d < size; ++d) {
+            const bool virtual_ray = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
+            double new_norm;
+            cell_dist -= cell_width;
+            if (virtual_ray) {
+                cell_dist -= cell_width;
+                new_norm = Q.norm_de[d - 1];
+            } else {
+                cell_width = width_de(d, a, offset);
+                cell_dist -= cell_width;
+                new_norm = Q.norm_de[d];
+            }
+            const double old_tl = inten_de[0];
+            gauss_add(cell_dist, cell_width, new_norm, inten_de, false);
+            if (inten_de[0] / old_tl < 1.002305238) break;
+            if (virtual_ray) break;
+        }
+    }
+
+    __device__ bool dup_test_set(int a) {
+        const uint32_t m = 1u << (a & 31);
+        const bool was = (dup[a >> 5] & m) != 0;
+        dup[a >> 5] |= m;
+        return was;
+    }
+
+    /* spreading_hybrid_gaussian.cc:264-425 */
+    __device__ void intensity_az(int d, int az0, const double* offset, const double* distance) {
+        const QueueDev& Q = *q;
+        const FrontPtrs& C = *pC;
+        const int max_de = Q.nde - 2;
+        const int max_az = Q.naz - 1;
+        int az_upper, az_lower;
+        if (Q.az_boundary) {
+            az_lower = az_upper = az0;
+        } else {
+            az_lower = 0;
+            az_upper = max_az - 1;
+        }
+        for (int w = 0; w < (Q.naz + 31) / 32; ++w) dup[w] = 0u;
+        auto norm = [&](int a) { return (d >= max_de) ? Q.norm_az[1 * Q.naz + a] : Q.norm_az[d * Q.naz + a]; };
+        int a = az0;
+        dup_test_set(a);
+        double cell_width = width_az(d, a, offset);
+        const double initial_width = cell_width;
+        const double L = distance[2];
+        double cell_dist = L - cell_width;
+        gauss_add(cell_dist, cell_width, norm(a), inten_az, true);
+        a = (az0 < 1) ? max_az - 1 : az0 - 1;
+        dup_test_set(a);
+        cell_width = width_az(d, a, offset);
+        cell_dist = L + cell_width;
+        gauss_add(cell_dist, cell_width, norm(a), inten_az, false);
+        if (inten_az[0] < 1e-10) return;
+        if (a < 1) {
+            a = max_az - 1;
+        } else {
+            --a;
+        }
+        int guard = 0;
+        while ((a % max_az) != az_lower) {
+            if (++guard > Q.naz + 2) {
+                set_err(Q, ERR_WALK_LIMIT);
+                break;
+            }
+            if (dup_test_set(a)) break;
+            if (C.on_edge[d * Q.naz + a]) break;
+            cell_dist += cell_width;
+            cell_width = width_az(d, a, offset);
+            cell_dist += cell_width;
+            const double old_tl = inten_az[0];
+            gauss_add(cell_dist, cell_width, norm(a), inten_az, false);
+            if (inten_az[0] / old_tl < 1.002305238) break;
+            if (a == 0) {
+                a += max_az - 1;
+            } else {
+                --a;
+            }
+        }
+        cell_width = initial_width;
+        cell_dist = L - cell_width;
+        a = az0 + 1;
+        guard = 0;
+        while ((a % max_az) != az_upper) {
+            if (++guard > Q.naz + 2) {
+                set_err(Q, ERR_WALK_LIMIT);
+                break;
+            }
+            if (a == max_az) a = 0;
+            if (dup_test_set(a)) break;
+            if (C.on_edge[d * Q.naz + a]) break;
+            cell_dist -= cell_width;
+            cell_width = width_az(d, a, offset);
+            cell_dist -= cell_width;
+            const double old_tl = inten_az[0];
+            gauss_add(cell_dist, cell_width, norm(a), inten_az, false);
+            if (inten_az[0] / old_tl < 1.002305238) break;
+            ++a;
+        }
+    }
+
+    /* wvector1::area on four points (types/wvector1.cc) */
+    __device__ double area4(const FrontPtrs& f, int d, int a) const {
+        auto dist = [&](int d1, int a1, int d2, int a2) { return fdist(f, d1, a1, d2, a2); };
+        double aa = dist(d, a, d + 1, a);
+        const double b = dist(d, a, d + 1, a + 1);
+        double c = dist(d + 1, a, d + 1, a + 1);
+        const double area1 = 0.25 * sqrt((aa + b + c) * (b + c - aa) * (c + aa - b) * (aa + b - c));
+        aa = dist(d, a, d, a + 1);
+        c = dist(d, a + 1, d + 1, a + 1);
+        const double area2 = 0.25 * sqrt((aa + b + c) * (b + c - aa) * (c + aa - b) * (aa + b - c));
+        return area1 + area2;
+    }
+};
+
+__device__ __forceinline__ void make_taylor_coeff(const double v[3][3][3], const double* delta,
+                                                  double& center, double* g, double h[3][3]) {
+    const double d0 = 2.0 * delta[0];
+    const double d1 = 2.0 * delta[1];
+    const double d2 = 2.0 * delta[2];
+    center = v[1][1][1];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) h[r][c] = 0.0;
+    h[0][0] = (v[2][1][1] + v[0][1][1] - 2.0 * center) / (delta[0] * delta[0]);
+    h[1][1] = (v[1][2][1] + v[1][0][1] - 2.0 * center) / (delta[1] * delta[1]);
+    h[2][2] = (v[1][1][2] + v[1][1][0] - 2.0 * center) / (delta[2] * delta[2]);
+    g[0] = (v[2][0][1] - v[0][0][1]) / d0;
+    g[2] = (v[2][2][1] - v[0][2][1]) / d0;
+    h[0][1] = (g[2] - g[0]) / d1;
+    h[1][0] = h[0][1];
+    g[0] = (v[2][1][0] - v[0][1][0]) / d0;
+    g[2] = (v[2][1][2] - v[0][1][2]) / d0;
+    h[0][2] = (g[2] - g[0]) / d2;
+    h[2][0] = h[0][2];
+    g[0] = (v[1][2][0] - v[1][0][0]) / d1;
+    g[2] = (v[1][2][2] - v[1][0][2]) / d1;
+    h[1][2] = (g[2] - g[0]) / d2;
+    h[2][1] = h[1][2];
+    g[0] = (v[2][1][1] - v[0][1][1]) / d0;
+    g[1] = (v[1][2][1] - v[1][0][1]) / d1;
+    g[2] = (v[1][1][2] - v[1][1][0]) / d2;
+}
+
+__device__ __forceinline__ double dot3(const double* a, const double* b) {
+    double t = 0.0;
+    t += a[0] * b[0];
+    t += a[1] * b[1];
+    t += a[2] * b[2];
+    return t;
+}
+__device__ __forceinline__ void matvec(const double m[3][3], const double* x, double* y) {
+    for (int r = 0; r < 3; ++r) {
+        double t = 0.0;
+        t += m[r][0] * x[0];
+        t += m[r][1] * x[1];
+        t += m[r][2] * x[2];
+        y[r] = t;
+    }
+}
+__device__ __forceinline__ double norm2(const double* g) {
+    double t = 0.0;
+    t += fabs(g[0]) * fabs(g[0]);
+    t += fabs(g[1]) * fabs(g[1]);
+    t += fabs(g[2]) * fabs(g[2]);
+    return sqrt(t);
+}
+
+/* wave_queue::compute_offsets (wave_queue.cc:708-924) */
+__device__ void compute_offsets(const QueueDev& q, const FrontPtrs& V, const FrontPtrs& C,
+                                const FrontPtrs& X, int t, int de0, int az0,
+                                const double cube[3][3][3], const double* delta,
+                                double* offset, double* distance) {
+    bool unstable = false;
+    const int ic = de0 * q.naz + az0;
+    const int surface = C.surface[ic], bottom = C.bottom[ic], caustic = C.caustic[ic];
+    for (int nd_ = 0; nd_ < 3 && !unstable; ++nd_) {
+        const int d = de0 + nd_ - 1;
+        for (int na = 0; na < 3 && !unstable; ++na) {
+            const int a = wrap_az(q, az0, na);
+            const int i = d * q.naz + a;
+            if (V.surface[i] != surface || C.surface[i] != surface || X.surface[i] != surface ||
+                V.bottom[i] != bottom || C.bottom[i] != bottom || X.bottom[i] != bottom ||
+                V.caustic[i] != caustic || C.caustic[i] != caustic || X.caustic[i] != caustic ||
+                V.on_edge[i]) {
+                unstable = true;
+            }
+        }
+    }
+    double center, g[3], h[3][3], inv[3][3];
+    make_taylor_coeff(cube, delta, center, g, h);
+    /* kept: hessian(2,1)*hessian(2,0) in the last cofactor (wave_queue.cc:762-763) */
+    double determinant = fmax(1e-6, h[0][0] * (h[1][1] * h[2][2] - h[1][2] * h[2][1]) +
+                                        h[0][1] * (h[1][2] * h[2][0] - h[1][0] * h[2][2]) +
+                                        h[0][2] * (h[1][0] * h[2][1] - h[2][1] * h[2][0]));
+    unstable = unstable || determinant < norm2(g);
+    for (int k = 0; k < 3; ++k) {
+        const double hh = fmax(1e-10, h[k][k]);
+        offset[k] = -g[k] / hh;
+        if (fabs(offset[k] / delta[k]) > 0.5) {
+            unstable = true;
+            offset[k] = (offset[k] < 0.0) ? -(0.5 * delta[k]) : 0.5 * delta[k];
+        }
+    }
+    if (!unstable) {
+        inv[0][0] = h[1][1] * h[2][2] - h[1][2] * h[2][1];
+        inv[1][0] = h[1][2] * h[2][0] - h[1][0] * h[2][2];
+        inv[2][0] = h[1][0] * h[2][1] - h[1][1] * h[2][0];
+        inv[0][1] = inv[1][0];
+        inv[1][1] = h[0][0] * h[2][2] - h[0][2] * h[2][0];
+        inv[2][1] = h[2][0] * h[0][1] - h[0][0] * h[2][1];
+        inv[0][2] = inv[2][0];
+        inv[1][2] = inv[2][1];
+        inv[2][2] = h[0][0] * h[1][1] - h[0][1] * h[1][0];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) inv[r][c] /= determinant;
+        const double ng[3] = {-g[0], -g[1], -g[2]};
+        matvec(inv, ng, offset);
+        unstable = unstable || fabs(offset[1]) >= 0.5 * fabs(delta[1]);
+    } else {
+        const double save_offset = offset[1];
+        g[1] = 0.0;
+        determinant = h[0][0] * h[2][2] - h[0][2] * h[2][0];
+        if (determinant >= norm2(g)) {
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) inv[r][c] = 0.0;
+            inv[0][0] = h[2][2];
+            inv[0][2] = -h[0][2];
+            inv[1][1] = 1.0;
+            inv[2][0] = -h[2][0];
+            inv[2][2] = h[0][0];
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) inv[r][c] /= determinant;
+            const double ng[3] = {-g[0], -g[1], -g[2]};
+            matvec(inv, ng, offset);
+            offset[1] = save_offset;
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        distance[k] = -g[k] * offset[k] - 0.5 * h[k][k] * offset[k] * offset[k];
+        distance[k] = sqrt(fmax(0.0, distance[k]));
+        if (offset[k] < 0.0) distance[k] *= -1.0;
+    }
+    if (unstable) {
+        distance[1] = center - distance[0] * distance[0] - distance[2] * distance[2];
+        if (distance[1] <= 0.0) {
+            distance[1] = 0.0;
+            offset[1] = 0.0;
+        } else {
+            distance[1] = sqrt(distance[1]);
+            offset[1] = fabs(offset[1]);
+            double cpa[3], nxt[3], prv[3], dir[3], speed;
+            collision_location(q, V, C, X, ic, offset[0], cpa, dir, &speed);
+            collision_location(q, V, C, X, ic + q.naz, offset[0], nxt, dir, &speed);
+            collision_location(q, V, C, X, ic - q.naz, offset[0], prv, dir, &speed);
+            double nxt_dir[3], tgt_dir[3];
+            nxt_dir[0] = nxt[0] - cpa[0];
+            nxt_dir[1] = (nxt[1] - prv[1]) * cpa[0];
+            nxt_dir[2] = (nxt[2] - prv[2]) * cpa[0] * sin(cpa[1]);
+            if (fabs(nxt_dir[0]) < 0.01) nxt_dir[0] = 0.0;
+            tgt_dir[0] = q.tgt[0][t] - cpa[0];
+            tgt_dir[1] = (q.tgt[1][t] - cpa[1]) * cpa[0];
+            tgt_dir[2] = (q.tgt[2][t] - cpa[2]) * cpa[0] * sin(cpa[1]);
+            if (dot3(nxt_dir, tgt_dir) < 0.0) {
+                distance[1] *= -1.0;
+                offset[1] *= -1.0;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(64) k_eigenray(const QueueDev* __restrict__ qp, int k) {
+    const QueueDev& q = *qp;
+    const int64_t s = *q.d_base + k + 1;
+    const double time = q.d_times[k + 1];
+    const uint32_t ncand = min(*q.n_cand, q.cap_cand);
+    Build B;
+    B.q = qp;
+    B.pV = &q.F[(s + 1) & 3];
+    B.pC = &q.F[(s + 2) & 3];
+    B.pX = &q.F[(s + 3) & 3];
+    const FrontPtrs& V = *B.pV;
+    const FrontPtrs& C = *B.pC;
+    const FrontPtrs& X = *B.pX;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncand; c += gridDim.x * blockDim.x) {
+        const int t = (int)q.cand[2 * c];
+        const int i = (int)q.cand[2 * c + 1];
+        const int de0 = i / q.naz, az0 = i % q.naz;
+        /* above_bounce_threshold (wave_thresholds.h:192-199) */
+        if (C.bottom[i] > q.max_bottom || C.surface[i] > q.max_surface ||
+            C.caustic[i] > q.max_caustic || C.upper[i] > q.max_upper || C.lower[i] > q.max_lower)
+            continue;
+        const TgtS tg{q.tgt[1][t], q.tgt[2][t], q.tgt_sin[t], q.tgt_R2[t], q.tgt_2R[t]};
+        double cube[3][3][3];
+        for (int nd_ = 0; nd_ < 3; ++nd_)
+            for (int na = 0; na < 3; ++na) {
+                const int j = (de0 + nd_ - 1) * q.naz + wrap_az(q, az0, na);
+                cube[0][nd_][na] = d2_at(V, j, tg);
+                cube[1][nd_][na] = d2_at(C, j, tg);
+                cube[2][nd_][na] = d2_at(X, j, tg);
+            }
+        double delta[3] = {q.dt, q.de_inc[de0], q.az_inc[az0]};
+        double offset[3], distance[3];
+        compute_offsets(q, V, C, X, t, de0, az0, cube, delta, offset, distance);
+
+        double si[MAX_FREQ];
+        B.t = t;
+        B.spread2 = q.tgt_spread2 + (size_t)t * q.nf;
+        if (q.spreading == WQ3D_HYBRID_GAUSSIAN) {
+            /* spreading_hybrid_gaussian.cc:65-119 */
+            int a = az0;
+            double no[3] = {offset[0], offset[1], offset[2]};
+            if (offset[2] < 0.0) {
+                if (az0 > 0) {
+                    a = az0 - 1;
+                } else if (q.az_boundary) {
+                    a = q.naz - 2;
+                }
+                no[2] = offset[2] + B.az_inc(a);
+            }
+            B.intensity_de(de0, a, no, distance);
+            no[2] = offset[2];
+            int d = de0;
+            if (offset[1] < 0.0 && !C.on_edge[i - q.naz]) {
+                d = de0 - 1;
+                no[1] = offset[1] + B.de_inc(d);
+            }
+            B.intensity_az(d, az0, no, distance);
+            for (int f = 0; f < q.nf; ++f) si[f] = B.inten_de[f] * B.inten_az[f];
+        } else {
+            /* spreading_ray.cc:47-133; an AZ wrap below index 0 is wrapped */
+            int d = de0, a = az0;
+            if (offset[1] < 0.0) --d;
+            if (offset[2] < 0.0) a = (a == 0) ? q.naz - 2 : a - 1;
+            const double area1 = B.area4(C, d, a);
+            const double area2 = (offset[0] < 0.0) ? B.area4(V, d, a) : B.area4(X, d, a);
+            double u = fabs(offset[0]) / q.dt;
+            const double area = (1.0 - u) * area1 + u * area2;
+            const double loss = q.init_area[d * q.naz + a] * q.tgt_c[t] / (area * q.init_sound_speed);
+            bool zero = false;
+            u = fabs(offset[1]) / B.de_inc(d) - 1.0;
+            if (u > 4.0) zero = true;
+            u = fabs(offset[2]) / B.az_inc(a) - 1.0;
+            if (u > 4.0) zero = true;
+            for (int f = 0; f < q.nf; ++f) si[f] = zero ? loss * 0.0 : loss;
+        }
+        bool bad = false;
+        for (int f = 0; f < q.nf; ++f)
+            if (isnan(si[f])) bad = true;
+        if (bad) continue;
+        double inten[MAX_FREQ];
+        for (int f = 0; f < q.nf; ++f) inten[f] = -10.0 * log10(fmax(si[f], 1e-30));
+        double ddt = offset[0] / q.dt;
+        if (ddt >= 0.0) {
+            for (int f = 0; f < q.nf; ++f)
+                inten[f] = inten[f] + C.atten[(size_t)f * q.n + i] * (1.0 - ddt) +
+                           X.atten[(size_t)f * q.n + i] * ddt;
+        } else {
+            ddt = 1.0 + ddt;
+            for (int f = 0; f < q.nf; ++f)
+                inten[f] = inten[f] + V.atten[(size_t)f * q.n + i] * (1.0 - ddt) +
+                           C.atten[(size_t)f * q.n + i] * ddt;
+        }
+        bool above = false;
+        for (int f = 0; f < q.nf; ++f)
+            if (inten[f] < q.intensity_threshold) above = true;
+        if (!above) continue;
+
+        /* target D/E and AZ by a 2nd-order Taylor series (wave_queue.cc:620-689) */
+        double tde = 0.0, taz = 0.0;
+        for (int which = 0; which < 2; ++which) {
+            double ang[3][3][3];
+            for (int nd_ = 0; nd_ < 3; ++nd_)
+                for (int na = 0; na < 3; ++na) {
+                    const int j = (de0 + nd_ - 1) * q.naz + wrap_az(q, az0, na);
+                    const FrontPtrs* fs[3] = {&V, &C, &X};
+                    for (int m = 0; m < 3; ++m) {
+                        const double n0 = fs[m]->nd[0][j], n1 = fs[m]->nd[1][j], n2 = fs[m]->nd[2][j];
+                        ang[m][nd_][na] = (which == 0)
+                                              ? atan2(n0, sqrt(n1 * n1 + n2 * n2)) * (180.0 / M_PI)
+                                              : atan2(n2, -n1) * (180.0 / M_PI);
+                    }
+                }
+            double center, g[3], h[3][3], hv[3];
+            make_taylor_coeff(ang, delta, center, g, h);
+            matvec(h, offset, hv);
+            const double val = center + dot3(g, offset) + 0.5 * dot3(offset, hv);
+            if (which == 0)
+                tde = val;
+            else
+                taz = val;
+        }
+        const uint32_t slot = atomicAdd(q.n_rec, 1u);
+        if (slot >= q.cap_rec) {
+            set_err(q, ERR_REC_OVERFLOW);
+            continue;
+        }
+        wq3d_eigenray r;
+        r.time = time + offset[0];
+        r.source_de = q.de[de0] + offset[1];
+        r.source_az = q.az[az0] + offset[2];
+        r.target_de = tde;
+        r.target_az = taz;
+        r.surface = C.surface[i];
+        r.bottom = C.bottom[i];
+        r.caustic = C.caustic[i];
+        r.upper = C.upper[i];
+        r.lower = C.lower[i];
+        r.t1 = t / q.nt2;
+        r.t2 = t % q.nt2;
+        r.de = de0;
+        r.az = az0;
+        r.pad = 0;
+        r.step = s;
+        q.rec[slot] = r;
+        for (int f = 0; f < q.nf; ++f) {
+            q.rec_inten[(size_t)slot * q.nf + f] = inten[f];
+            q.rec_phase[(size_t)slot * q.nf + f] = C.phase[(size_t)f * q.n + i];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* single-point model evaluations (ocean parity tests)                 */
+/* ------------------------------------------------------------------ */
+__global__ void k_sound_speed(OceanDev oc, double R, int n, const double* rho,
+                              const double* theta, const double* phi, double* c,
+                              double* g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double cc, gr;
+    sound_speed(oc.prof, R, rho[i], &cc, &gr);
+    c[i] = cc;
+    if (g) {
+        g[i] = gr;
+        g[n + i] = 0.0;
+        g[2 * n + i] = 0.0;
+    }
+    (void)theta;
+    (void)phi;
+}
+
+__global__ void k_height(BoundaryDev b, int n, const double* theta, const double* phi,
+                         double* h, double* nrm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    h[i] = boundary_height(b, theta[i], phi[i]);
+    if (nrm) {
+        nrm[i] = b.normal[0];
+        nrm[n + i] = b.normal[1];
+        nrm[2 * n + i] = b.normal[2];
+    }
+}
+
+__global__ void k_reflect_loss(BoundaryDev b, int n, const double* grazing, int nf,
+                               const double* freq, double* amp, double* ph) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const LossDev& L = b.loss;
+    double a0 = 0.0, p0 = 0.0;
+    if (L.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(L, grazing[i], &a0, &p0);
+    const double w2 = L.p[0] * L.p[0];
+    const double sg = sin(grazing[i]);
+    for (int f = 0; f < nf; ++f) {
+        double a = a0, p = p0;
+        if (L.kind == WQ3D_LOSS_ECKART) {
+            const double x = freq[f] * w2 * sg;
+            a = 8.6e-9 * (x * x);
+            p = M_PI;
+        }
+        amp[(size_t)i * nf + f] = a;
+        if (ph) ph[(size_t)i * nf + f] = p;
+    }
+}
+
+}  // namespace wq3d

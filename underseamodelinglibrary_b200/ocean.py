@@ -1,0 +1,278 @@
+"""Host mirror of the USML ocean models that the WaveQ3D path calls.
+
+Each class records its parameters the way the reference constructor does
+(including the earth radius that boundaries bake in at construction,
+ocean/boundary_flat.cc:19-21) and contributes to a ``wq3d_ocean_desc``.
+The models are evaluated on the GPU by the engine; ``ocean_model`` also
+exposes the engine's point evaluations for model-level checks.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .types import earth_radius
+
+
+class attenuation_thorp:
+    """ocean/attenuation_thorp.cc:14-36 (the profile default)."""
+    kind = _abi.ATTEN_THORP
+    coefficient = 0.0
+
+
+class attenuation_constant:
+    """ocean/attenuation_constant.cc:14-25: coefficient * distance * frequency."""
+    kind = _abi.ATTEN_CONSTANT
+
+    def __init__(self, coefficient):
+        self.coefficient = float(coefficient)
+
+
+class profile_model:
+    kind = None
+    params = (0.0, 0.0, 0.0, 0.0)
+
+    def __init__(self, attmodel=None):
+        self._atten = attmodel if attmodel is not None else attenuation_thorp()
+        self._flat_earth = False
+
+    def flat_earth(self, flat):
+        """profile_model::flat_earth (profile_model.h:61)."""
+        self._flat_earth = bool(flat)
+
+    def attenuation(self, model):
+        self._atten = model
+
+    def fill(self, d):
+        d.kind = self.kind
+        for k in range(4):
+            d.p[k] = self.params[k]
+        d.flat_earth = 1 if self._flat_earth else 0
+        d.attenuation = self._atten.kind
+        d.attenuation_coef = self._atten.coefficient
+
+
+class profile_linear(profile_model):
+    """profile_linear(c0[, g0[, z1, g1]][, attmodel]) (profile_linear.h)."""
+    kind = _abi.PROFILE_LINEAR
+
+    def __init__(self, c0=1500.0, *args):
+        att = None
+        nums = []
+        for a in args:
+            if isinstance(a, (int, float)):
+                nums.append(float(a))
+            else:
+                att = a
+        super().__init__(att)
+        if len(nums) == 0:
+            self.params = (float(c0), 0.0, 0.0, 0.0)
+        elif len(nums) == 1:
+            self.params = (float(c0), nums[0], 0.0, nums[0])
+        elif len(nums) == 3:
+            self.params = (float(c0), nums[0], nums[1], nums[2])
+        else:
+            raise TypeError("profile_linear(c0, g0) or profile_linear(c0, g0, z1, g1)")
+
+
+class profile_munk(profile_model):
+    """profile_munk.h:40-60 defaults: axis 1300 m, scale 1300 m, 1500 m/s, 7.37e-3."""
+    kind = _abi.PROFILE_MUNK
+
+    def __init__(self, axis_depth=1300.0, scale=1300.0, axis_speed=1500.0,
+                 epsilon=7.37e-3, attmodel=None):
+        super().__init__(attmodel)
+        self.params = (float(axis_depth), float(scale), float(axis_speed), float(epsilon))
+
+
+class profile_catenary(profile_model):
+    kind = _abi.PROFILE_CATENARY
+
+    def __init__(self, c1, g1, z1, attmodel=None):
+        super().__init__(attmodel)
+        self.params = (float(c1), float(g1), float(z1), 0.0)
+
+
+class profile_n2(profile_model):
+    kind = _abi.PROFILE_N2
+
+    def __init__(self, c0, g0, attmodel=None):
+        super().__init__(attmodel)
+        self.params = (float(c0), float(g0), 0.0, 0.0)
+
+
+class reflect_loss_constant:
+    """reflect_loss_constant.h:42-52."""
+    kind = _abi.LOSS_CONSTANT
+
+    def __init__(self, amplitude, phase=0.0):
+        self.params = (float(amplitude), float(phase), 0.0, 0.0, 0.0)
+
+
+class reflect_loss_rayleigh:
+    """reflect_loss_rayleigh(density, speed, att_bottom, speed_shear, att_shear)
+    as ratios to water (reflect_loss_rayleigh.cc:68-78), or a bottom type."""
+    kind = _abi.LOSS_RAYLEIGH
+    # Jensen et al. table 1.3 (reflect_loss_rayleigh.cc:27-39)
+    TABLE = {"clay": (1.5, 1.00, 0.2, 0.00, 1.0), "silt": (1.7, 1.05, 1.0, 0.00, 1.5),
+             "sand": (1.9, 1.10, 0.8, 0.00, 2.5), "gravel": (2.0, 1.20, 0.6, 0.00, 1.5),
+             "moraine": (2.1, 1.30, 0.4, 0.40, 1.0), "chalk": (2.2, 1.60, 0.2, 0.67, 0.5),
+             "limestone": (2.4, 2.00, 0.1, 1.00, 0.2), "basalt": (2.7, 3.50, 0.1, 1.67, 0.2)}
+
+    def __init__(self, density, speed=None, att_bottom=0.0, speed_shear=0.0, att_shear=0.0):
+        if isinstance(density, str):
+            self.params = self.TABLE[density]
+        else:
+            self.params = (float(density), float(speed), float(att_bottom),
+                           float(speed_shear), float(att_shear))
+
+
+class reflect_loss_eckart:
+    """reflect_loss_eckart.h:76-85."""
+    kind = _abi.LOSS_ECKART
+
+    def __init__(self, wind_speed):
+        self.params = (float(wind_speed), 0.0, 0.0, 0.0, 0.0)
+
+
+class boundary_model:
+    kind = None
+
+    def __init__(self, reflect_loss=None):
+        self._loss = reflect_loss
+        self._radius = earth_radius()
+
+    def reflect_loss(self, model):
+        self._loss = model
+
+    def fill(self, d):
+        d.kind = self.kind
+        if self._loss is None:
+            d.loss.kind = _abi.LOSS_DEFAULT
+        else:
+            d.loss.kind = self._loss.kind
+            for k in range(5):
+                d.loss.p[k] = self._loss.params[k]
+
+
+class boundary_flat(boundary_model):
+    """boundary_flat(depth=0, reflect_loss) (boundary_flat.cc:19-31)."""
+    kind = _abi.BOUNDARY_FLAT
+
+    def __init__(self, depth=0.0, reflect_loss=None):
+        super().__init__(reflect_loss)
+        self.depth = float(depth)
+
+    def fill(self, d):
+        super().fill(d)
+        d.depth = self.depth
+
+
+class boundary_slope(boundary_model):
+    """boundary_slope(location, depth, lat_slope, lng_slope, reflect_loss)
+    (boundary_slope.cc:13-24).  The reference keeps a reference to the
+    caller's location; this copies it."""
+    kind = _abi.BOUNDARY_SLOPE
+
+    def __init__(self, location, depth, lat_slope, lng_slope=0.0, reflect_loss=None):
+        super().__init__(reflect_loss)
+        self.location = (location.rho, location.theta, location.phi)
+        self.depth = float(depth)
+        self.lat_slope = float(lat_slope)
+        self.lng_slope = float(lng_slope)
+
+    def fill(self, d):
+        super().fill(d)
+        d.depth = self.depth
+        for k in range(3):
+            d.location[k] = self.location[k]
+        d.lat_slope = self.lat_slope
+        d.lng_slope = self.lng_slope
+
+
+class ocean_model:
+    """ocean_model(surface, bottom, profile) (ocean/ocean_model.h:31-60)."""
+
+    def __init__(self, surface, bottom, profile):
+        self._surface = surface
+        self._bottom = bottom
+        self._profile = profile
+        self._handle = None
+        self._lib = None
+
+    def surface(self):
+        return self._surface
+
+    def bottom(self):
+        return self._bottom
+
+    def profile(self):
+        return self._profile
+
+    def descriptor(self):
+        d = _abi.wq3d_ocean_desc()
+        d.earth_radius = self._bottom._radius
+        self._profile.fill(d.profile)
+        self._surface.fill(d.surface)
+        self._bottom.fill(d.bottom)
+        # one construction radius serves both boundaries: build them under
+        # the same wposition earth radius, as every reference caller does
+        return d
+
+    def handle(self):
+        """Device-resident copy (built on first use)."""
+        if self._handle is None:
+            lib = _abi.load_engine()
+            h = C.c_void_p()
+            _abi.check(lib, lib.wq3d_ocean_create(C.byref(self.descriptor()), C.byref(h)))
+            self._handle = h
+            self._lib = lib
+        return self._handle
+
+    def __del__(self):
+        if self._handle is not None and self._lib is not None:
+            try:
+                self._lib.wq3d_ocean_destroy(self._handle)
+            except Exception:
+                pass
+
+    # GPU point evaluations (profile_model::sound_speed, boundary_model::height,
+    # boundary_model::reflect_loss)
+    def sound_speed(self, rho, theta=None, phi=None):
+        rho = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+        n = rho.size
+        theta = np.zeros(n) if theta is None else np.ascontiguousarray(theta, dtype=np.float64).ravel()
+        phi = np.zeros(n) if phi is None else np.ascontiguousarray(phi, dtype=np.float64).ravel()
+        c = np.empty(n)
+        g = np.empty(3 * n)
+        lib = _abi.load_engine()
+        _abi.check(lib, lib.wq3d_ocean_sound_speed(self.handle(), earth_radius(), n, _abi.as_dp(rho),
+                                                   _abi.as_dp(theta), _abi.as_dp(phi),
+                                                   _abi.as_dp(c), _abi.as_dp(g)))
+        return c, g.reshape(3, n)
+
+    def height(self, which, theta, phi):
+        theta = np.ascontiguousarray(theta, dtype=np.float64).ravel()
+        phi = np.ascontiguousarray(phi, dtype=np.float64).ravel()
+        n = theta.size
+        h = np.empty(n)
+        nrm = np.empty(3 * n)
+        rho = np.zeros(n)
+        lib = _abi.load_engine()
+        _abi.check(lib, lib.wq3d_ocean_height(self.handle(), int(which), n, _abi.as_dp(rho),
+                                              _abi.as_dp(theta), _abi.as_dp(phi),
+                                              _abi.as_dp(h), _abi.as_dp(nrm)))
+        return h, nrm.reshape(3, n)
+
+    def reflect_loss(self, which, grazing, freq):
+        g = np.ascontiguousarray(grazing, dtype=np.float64).ravel()
+        f = np.ascontiguousarray(freq, dtype=np.float64).ravel()
+        n, nf = g.size, f.size
+        z = np.zeros(n)
+        amp = np.empty(n * nf)
+        ph = np.empty(n * nf)
+        lib = _abi.load_engine()
+        _abi.check(lib, lib.wq3d_ocean_reflect_loss(self.handle(), int(which), n, _abi.as_dp(z),
+                                                    _abi.as_dp(z), _abi.as_dp(z), _abi.as_dp(g), nf,
+                                                    _abi.as_dp(f), _abi.as_dp(amp), _abi.as_dp(ph)))
+        return amp.reshape(n, nf), ph.reshape(n, nf)

@@ -1,0 +1,170 @@
+"""Named propagation scenarios.
+
+* The reference's own test scenarios (waveq3d/test/*.cc), rebuilt with the
+  same constructors and arguments, so a test here reads like the
+  reference's test and can check the same known answers.
+* The synthetic benchmark workloads ("munk_flat_181x37" and
+  "linear_slope_rayleigh_1801x91"), whose shapes and value ranges are the
+  published benchmark configurations of this engine; inputs are generated,
+  not read from data files.
+
+Every builder returns a dict with keys ocean, freq, pos, de, az, dt,
+targets, time_max, type and the earth radius it set.
+"""
+import math
+
+import numpy as np
+
+from . import types as T
+from .ocean import (attenuation_constant, boundary_flat, boundary_slope, ocean_model,
+                    profile_linear, profile_munk, reflect_loss_constant,
+                    reflect_loss_rayleigh)
+from ._abi import HYBRID_GAUSSIAN
+
+
+def _pack(**kw):
+    kw.setdefault("type", HYBRID_GAUSSIAN)
+    kw["earth_radius"] = T.earth_radius()
+    return kw
+
+
+def eigenray_basic():
+    """waveq3d/test/eigenray_test.cc:86-198 -- isovelocity, 3000 m flat
+    bottom, direct / surface / bottom paths to one target."""
+    T.compute_earth_radius(45.0)
+    profile = profile_linear(1500.0, attenuation_constant(0.0))
+    ocean = ocean_model(boundary_flat(), boundary_flat(3000.0), profile)
+    return _pack(ocean=ocean, freq=T.seq_log(10e3, 2.0, 3), pos=T.wposition1(45.0, -45.0, -1000.0),
+                 de=T.seq_linear(-60.0, 5.0, 60.0), az=T.seq_linear(-4.0, 1.0, 4.0), dt=0.1,
+                 targets=T.wposition(1, 1, 45.02, -45.0, -1000.0), time_max=3.5)
+
+
+def eigenray_concave():
+    """eigenray_test.cc:232-332 -- target 1.2 deg away, 4 paths."""
+    T.compute_earth_radius(45.0)
+    profile = profile_linear(1500.0, attenuation_constant(0.0))
+    ocean = ocean_model(boundary_flat(), boundary_flat(1e5), profile)
+    return _pack(ocean=ocean, freq=T.seq_log(2000.0, 1.0, 1), pos=T.wposition1(45.0, -45.0, -200.0),
+                 de=T.seq_linear(-1.0, 0.05, 1.0), az=T.seq_linear(-4.0, 1.0, 4.0), dt=0.1,
+                 targets=T.wposition(1, 1, 46.2, -45.0, -150.0), time_max=120.0)
+
+
+def eigenray_branch_pt():
+    """eigenray_test.cc:428-534 -- AZ fan wrapping 0/360, targets directly
+    above and below the source and on a 2226 m ring."""
+    T.compute_earth_radius(0.0)
+    profile = profile_linear(1500.0, attenuation_constant(0.0))
+    ocean = ocean_model(boundary_flat(), boundary_flat(3000.0), profile)
+    pos = T.wposition1(0.0, 0.0, -1000.0)
+    num = 12
+    tgt = T.wposition(num + 2, 1, 0.0, 0.0, -1000.0)
+    tgt.altitude(0, 0, -1000.0 - 500)
+    tgt.altitude(1, 0, -1000.0 + 500)
+    angle = 2.0 * math.pi / num
+    bearing = 0.0
+    for n in range(2, num + 2):
+        t = T.wposition1(pos, 2226.0, bearing)
+        tgt.latitude(n, 0, t.latitude())
+        tgt.longitude(n, 0, t.longitude())
+        tgt.altitude(n, 0, t.altitude())
+        bearing = bearing + angle
+    return _pack(ocean=ocean, freq=T.seq_log(1000.0, 1.0, 1), pos=pos,
+                 de=T.seq_linear(-90.0, 1.0, 90.0), az=T.seq_linear(0.0, 15.0, 360.0), dt=0.1,
+                 targets=tgt, time_max=3.5)
+
+
+def proploss_gaussian():
+    """waveq3d/test/proploss_test.cc:153-248 -- ten frequencies."""
+    T.compute_earth_radius(45.0)
+    profile = profile_linear(1500.0, attenuation_constant(0.0))
+    ocean = ocean_model(boundary_flat(), boundary_flat(3000.0), profile)
+    return _pack(ocean=ocean, freq=T.seq_linear(100.0, 100.0, 1000.0),
+                 pos=T.wposition1(45.0, -45.0, -1000.0), de=T.seq_linear(-90.0, 1.0, 90.0),
+                 az=T.seq_linear(-5.0, 1.0, 5.0), dt=0.1,
+                 targets=T.wposition(1, 1, 45.02, -45.0, -1000.0), time_max=3.5)
+
+
+def refraction_munk_range():
+    """waveq3d/test/refraction_test.cc:827-980 -- Munk profile with the
+    flat earth correction, rays launched from the channel axis."""
+    T.set_earth_radius(6371000.0)
+    ssp = profile_munk()
+    ssp.flat_earth(True)
+    ocean = ocean_model(boundary_flat(), boundary_flat(5000.0), ssp)
+    return _pack(ocean=ocean, freq=T.seq_log(10e3, 1.0, 1), pos=T.wposition1(45.0, -45.0, -1000.0),
+                 de=T.seq_linear(-14.0, 1.0, 14.0), az=T.seq_linear(0.0, 0.0, 1), dt=0.1,
+                 targets=None, time_max=95.0)
+
+
+# analytic cycle ranges for D/E -14..14 (refraction_test.cc:836-842)
+MUNK_CYCLE_RANGES = [
+    64977.771509, 62686.699943, 60536.790347, 58539.834823, 56706.277890,
+    55044.418981, 53559.948084, 52255.876772, 51132.827760, 50189.572079,
+    49423.683193, 48832.195747, 48412.185973, 48161.238557, 48077.771909,
+    48161.238557, 48412.185973, 48832.195747, 49423.683193, 50189.572079,
+    51132.827760, 52255.876772, 53559.948084, 55044.418981, 56706.277890,
+    58539.834823, 60536.790347, 62686.699943, 64977.771509]
+
+
+def reflect_flat():
+    """waveq3d/test/reflection_test.cc:168-280 -- one ray bouncing between
+    the surface and a 1000 m flat bottom."""
+    T.compute_earth_radius(45.0)
+    ocean = ocean_model(boundary_flat(), boundary_flat(1000.0), profile_linear())
+    return _pack(ocean=ocean, freq=T.seq_log(10.0, 10.0, 1), pos=T.wposition1(45.0, -45.0, 0.0),
+                 de=T.seq_linear(-5.183617057, 0.0, 1), az=T.seq_linear(0.0, 0.0, 1), dt=0.1,
+                 targets=None, time_max=60.0)
+
+
+def munk_flat(num_de=181, num_az=37, n_targets=10, time_max=60.0):
+    """Plain FP64 workload: Munk profile, 5000 m flat bottom with 0 dB
+    loss, source 1000 m at 45N 45W, 10 Hz, tangent-spaced D/E fan from -90
+    to 90 deg x AZ 0..180 deg in 5 deg steps, dt 0.1 s for 60 s, targets at
+    500 m depth on a 10 x 10 lat/lon grid 0.1-0.9 deg from the source."""
+    T.compute_earth_radius(45.0)
+    profile = profile_munk(attmodel=attenuation_constant(0.0))
+    ocean = ocean_model(boundary_flat(), boundary_flat(5000.0, reflect_loss_constant(0.0)), profile)
+    lat = [45.0 + 0.1 + k * 0.8 / (n_targets - 1) for k in range(n_targets)]
+    lng = [-45.0 + 0.1 + k * 0.8 / (n_targets - 1) for k in range(n_targets)]
+    tgt = T.wposition.mesh(lat, lng, -500.0)
+    az = T.seq_linear(0.0, 5.0, 180.0) if num_az == 37 else T.seq_linear(0.0, 180.0 / (num_az - 1), num_az)
+    return _pack(ocean=ocean, freq=T.seq_log(10.0, 1.0, 1), pos=T.wposition1(45.0, -45.0, -1000.0),
+                 de=T.seq_rayfan(-90.0, 90.0, num_de), az=az, dt=0.1, targets=tgt,
+                 time_max=time_max, name="munk_flat_%dx%d" % (num_de, num_az))
+
+
+def linear_slope_rayleigh(num_de=1801, num_az=91, n_range=32, n_depth=32, time_max=40.0):
+    """Linear-gradient profile c(z) = 1500 + 0.0163 z with Thorp attenuation
+    over a bottom sloping from 200 m at the source to 2000 m at 20 km north
+    (boundary_slope), Rayleigh bottom (density 1.5, speed 1.1, 0.5
+    dB/wavelength).  Source 50 m deep at 45N 45W, 5 log-spaced frequencies
+    100 Hz - 3 kHz, tangent-spaced D/E fan x AZ 0..360 deg (wrapping), dt
+    0.05 s for 40 s, targets on a range x depth grid (0.5-20 km north,
+    10-2000 m)."""
+    T.compute_earth_radius(45.0)
+    src = T.wposition1(45.0, -45.0, -50.0)
+    profile = profile_linear(1500.0, 0.0163)
+    bottom = boundary_slope(src, 200.0, -math.atan(1800.0 / 20000.0), 0.0,
+                            reflect_loss_rayleigh(1.5, 1.1, 0.5))
+    ocean = ocean_model(boundary_flat(), bottom, profile)
+    freq = T.seq_log(100.0, 30.0 ** 0.25, 5)
+    ranges = np.linspace(500.0, 20000.0, n_range)
+    depths = np.linspace(10.0, 2000.0, n_depth)
+    tgt = T.wposition(n_range, n_depth, 0.0, 0.0, 0.0)
+    for i, r in enumerate(ranges):
+        p = T.wposition1(src, float(r), 0.0)
+        for j, z in enumerate(depths):
+            tgt.latitude(i, j, p.latitude())
+            tgt.longitude(i, j, p.longitude())
+            tgt.altitude(i, j, -float(z))
+    az = T.seq_linear(0.0, 4.0, 360.0) if num_az == 91 else T.seq_linear(0.0, 360.0 / (num_az - 1), num_az)
+    return _pack(ocean=ocean, freq=freq, pos=src, de=T.seq_rayfan(-90.0, 90.0, num_de), az=az,
+                 dt=0.05, targets=tgt, time_max=time_max,
+                 name="linear_slope_rayleigh_%dx%d" % (num_de, num_az))
+
+
+def build_queue(sc, queue_cls, **kw):
+    """Constructs ``queue_cls(ocean, freq, pos, de, az, dt, targets, type)``."""
+    T.set_earth_radius(sc["earth_radius"])
+    return queue_cls(sc["ocean"], sc["freq"], sc["pos"], sc["de"], sc["az"], sc["dt"],
+                     sc["targets"], sc["type"], **kw)

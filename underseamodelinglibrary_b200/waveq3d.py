@@ -1,0 +1,360 @@
+"""Drop-in mirror of USML's WaveQ3D wave_queue API over the CUDA engine.
+
+``wave_queue(ocean, freq, pos, de, az, time_step, target_pos, type)`` keeps
+the reference constructor (waveq3d/wave_queue.h:122-126), ``step()``,
+``time()``, ``source_pos()``, the front accessors ``curr()/next()/prev()/
+past()``, the wave_thresholds setters and the listener registration of
+eigenray_notifier / reflection_notifier.  All propagation runs in
+libwq3d.so on the GPU; this module only marshals arguments and dispatches
+listener callbacks in the reference's order.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .types import earth_radius, wposition1
+
+
+class eigenray_model:
+    """eigenrays/eigenray_model.h:24-102 plus the CPA bracket (step, de, az)."""
+
+    __slots__ = ("travel_time", "intensity", "phase", "source_de", "source_az",
+                 "target_de", "target_az", "surface", "bottom", "caustic", "upper",
+                 "lower", "frequencies", "step", "de_index", "az_index", "t1", "t2")
+
+    @classmethod
+    def from_record(cls, rec, intensity, phase, freq):
+        r = cls()
+        r.travel_time = rec.time
+        r.intensity = np.array(intensity, dtype=np.float64)
+        r.phase = np.array(phase, dtype=np.float64)
+        r.source_de = rec.source_de
+        r.source_az = rec.source_az
+        r.target_de = rec.target_de
+        r.target_az = rec.target_az
+        r.surface = rec.surface
+        r.bottom = rec.bottom
+        r.caustic = rec.caustic
+        r.upper = rec.upper
+        r.lower = rec.lower
+        r.frequencies = freq
+        r.step = rec.step
+        r.de_index = rec.de
+        r.az_index = rec.az
+        r.t1 = rec.t1
+        r.t2 = rec.t2
+        return r
+
+
+class eigenray_listener:
+    """eigenrays/eigenray_listener.h:41-53."""
+
+    def add_eigenray(self, t1, t2, ray, run_id):
+        raise NotImplementedError
+
+    def check_eigenrays(self, time, run_id):
+        pass
+
+
+class reflection_listener:
+    """waveq3d/reflection_listener.h:46-49."""
+
+    def reflect(self, time, de, az, dt, grazing, speed, position, ndirection, type):
+        raise NotImplementedError
+
+
+class wave_front_view:
+    """Host copy of one wavefront (wave_front.h:152-258)."""
+
+    def __init__(self, getter, q, which, num_de, num_az, nf, check=None):
+        n = num_de * num_az
+        shape = (num_de, num_az)
+        self.num_de, self.num_az = num_de, num_az
+        f = {k: np.empty(n) for k in ("rho", "theta", "phi", "c", "dist", "plen")}
+        vec = {k: [np.empty(n) for _ in range(3)] for k in ("pg", "nd", "ng", "sg")}
+        att = np.empty(n * nf)
+        ph = np.empty(n * nf)
+        ints = {k: np.empty(n, dtype=np.int32) for k in ("surface", "bottom", "caustic", "upper", "lower")}
+        edge = np.empty(n, dtype=np.uint8)
+        v = _abi.wq3d_front_view()
+        v.rho, v.theta, v.phi = (_abi.as_dp(f["rho"]), _abi.as_dp(f["theta"]), _abi.as_dp(f["phi"]))
+        for k in range(3):
+            v.pos_grad[k] = _abi.as_dp(vec["pg"][k])
+            v.ndir[k] = _abi.as_dp(vec["nd"][k])
+            v.ndir_grad[k] = _abi.as_dp(vec["ng"][k])
+            v.sound_grad[k] = _abi.as_dp(vec["sg"][k])
+        v.sound_speed = _abi.as_dp(f["c"])
+        v.distance = _abi.as_dp(f["dist"])
+        v.path_length = _abi.as_dp(f["plen"])
+        v.attenuation = _abi.as_dp(att)
+        v.phase = _abi.as_dp(ph)
+        for k, a in ints.items():
+            setattr(v, k, a.ctypes.data_as(C.POINTER(C.c_int32)))
+        v.on_edge = edge.ctypes.data_as(C.POINTER(C.c_uint8))
+        rc = getter(q, which, C.byref(v))
+        if check is not None:
+            check(rc)
+        self.rho = f["rho"].reshape(shape)
+        self.theta = f["theta"].reshape(shape)
+        self.phi = f["phi"].reshape(shape)
+        self.pos_gradient = [a.reshape(shape) for a in vec["pg"]]
+        self.ndirection = [a.reshape(shape) for a in vec["nd"]]
+        self.ndir_gradient = [a.reshape(shape) for a in vec["ng"]]
+        self.sound_gradient = [a.reshape(shape) for a in vec["sg"]]
+        self.sound_speed = f["c"].reshape(shape)
+        self.distance = f["dist"].reshape(shape)
+        self.path_length = f["plen"].reshape(shape)
+        self.attenuation = att.reshape(num_de, num_az, nf)
+        self.phase = ph.reshape(num_de, num_az, nf)
+        for k, a in ints.items():
+            setattr(self, k, a.reshape(shape))
+        self.on_edge = edge.reshape(shape).astype(bool)
+
+    def altitude(self):
+        return self.rho - earth_radius()
+
+    def latitude(self):
+        return 90.0 - self.theta * (180.0 / np.pi)
+
+
+def make_queue_desc(freq, pos, de, az, time_step, target_pos=None, type=_abi.HYBRID_GAUSSIAN,
+                    precision=_abi.FP64, device=0, eigenray_capacity=0, run_id=0):
+    """Fills a wq3d_queue_desc from reference-style arguments.  Returns the
+    descriptor and the numpy arrays it points into (keep them alive)."""
+    d = _abi.wq3d_queue_desc()
+    fr = np.ascontiguousarray(freq.data, dtype=np.float64)
+    dv = np.ascontiguousarray(de.data, dtype=np.float64)
+    di = np.ascontiguousarray(de.increments, dtype=np.float64)
+    av = np.ascontiguousarray(az.data, dtype=np.float64)
+    ai = np.ascontiguousarray(az.increments, dtype=np.float64)
+    keep = [fr, dv, di, av, ai]
+    d.freq, d.num_freq = _abi.as_dp(fr), fr.size
+    d.source[0], d.source[1], d.source[2] = pos.rho, pos.theta, pos.phi
+    d.de, d.de_inc, d.num_de = _abi.as_dp(dv), _abi.as_dp(di), dv.size
+    d.az, d.az_inc, d.num_az = _abi.as_dp(av), _abi.as_dp(ai), av.size
+    d.time_step = float(time_step)
+    if target_pos is not None:
+        tg = target_pos.packed()
+        keep.append(tg)
+        d.targets = _abi.as_dp(tg)
+        d.num_targets1, d.num_targets2 = target_pos.size1(), target_pos.size2()
+    d.spreading = int(type)
+    d.precision = int(precision)
+    d.earth_radius = earth_radius()
+    d.eigenray_capacity = int(eigenray_capacity)
+    d.device = int(device)
+    d.run_id = int(run_id)
+    return d, keep
+
+
+class wave_queue:
+    CLASSIC_RAY = _abi.CLASSIC_RAY
+    HYBRID_GAUSSIAN = _abi.HYBRID_GAUSSIAN
+
+    def __init__(self, ocean, freq, pos, de, az, time_step, target_pos=None,
+                 type=_abi.HYBRID_GAUSSIAN, precision=_abi.FP64, device=0,
+                 eigenray_capacity=0, run_id=0):
+        self._lib = _abi.load_engine()
+        self._ocean = ocean
+        self._freq = freq
+        self._de = de
+        self._az = az
+        self._targets = target_pos
+        d, self._keep = make_queue_desc(freq, pos, de, az, time_step, target_pos, type,
+                                        precision, device, eigenray_capacity, run_id)
+        h = C.c_void_p()
+        _abi.check(self._lib, self._lib.wq3d_queue_create(ocean.handle(), C.byref(d), C.byref(h)))
+        self._q = h
+        self._time_step = float(time_step)
+        self._eig_listeners = []
+        self._refl_listeners = []
+        self._run_id = int(run_id)
+        self._thresh = _abi.wq3d_thresholds(300.0, 300.0, 999, 999, 999, 999, 999)
+        self._cb = None
+
+    def __del__(self):
+        if getattr(self, "_q", None) is not None:
+            try:
+                self._lib.wq3d_queue_destroy(self._q)
+            except Exception:
+                pass
+            self._q = None
+
+    # ---------------- reference accessors ----------------
+    def time(self):
+        t = C.c_double()
+        _abi.check(self._lib, self._lib.wq3d_queue_time(self._q, C.byref(t)))
+        return t.value
+
+    def time_step(self):
+        return self._time_step
+
+    def num_de(self):
+        return self._de.size()
+
+    def num_az(self):
+        return self._az.size()
+
+    def source_de(self, i):
+        return self._de[i]
+
+    def source_az(self, i):
+        return self._az[i]
+
+    def frequencies(self):
+        return self._freq
+
+    def targets(self):
+        return self._targets
+
+    def runID(self, id=None):
+        if id is None:
+            return self._run_id
+        self._run_id = int(id)
+
+    def source_pos(self):
+        s = (C.c_double * 3)()
+        _abi.check(self._lib, self._lib.wq3d_queue_source(self._q, s))
+        p = wposition1()
+        p.rho, p.theta, p.phi = s[0], s[1], s[2]
+        return p
+
+    def steps(self):
+        v = C.c_int64()
+        _abi.check(self._lib, self._lib.wq3d_queue_steps(self._q, C.byref(v)))
+        return v.value
+
+    def _front(self, which):
+        return wave_front_view(self._lib.wq3d_queue_get_front, self._q, which, self.num_de(),
+                               self.num_az(), self._freq.size(),
+                               check=lambda rc: _abi.check(self._lib, rc))
+
+    def past(self):
+        return self._front(_abi.FRONT_PAST)
+
+    def prev(self):
+        return self._front(_abi.FRONT_PREV)
+
+    def curr(self):
+        return self._front(_abi.FRONT_CURR)
+
+    def next(self):
+        return self._front(_abi.FRONT_NEXT)
+
+    # ---------------- wave_thresholds (wave_thresholds.h:54-182) ----------------
+    def _push_thresholds(self):
+        _abi.check(self._lib, self._lib.wq3d_queue_set_thresholds(self._q, C.byref(self._thresh)))
+
+    def intensity_threshold(self, value):
+        self._thresh.intensity = abs(float(value))
+        self._push_thresholds()
+
+    def max_bottom(self, v):
+        self._thresh.max_bottom = int(v)
+        self._push_thresholds()
+
+    def max_surface(self, v):
+        self._thresh.max_surface = int(v)
+        self._push_thresholds()
+
+    def max_caustic(self, v):
+        self._thresh.max_caustic = int(v)
+        self._push_thresholds()
+
+    def max_upper(self, v):
+        self._thresh.max_upper = int(v)
+        self._push_thresholds()
+
+    # ---------------- listeners ----------------
+    def _install_callbacks(self):
+        if not self._eig_listeners and not self._refl_listeners:
+            _abi.check(self._lib, self._lib.wq3d_queue_set_callbacks(self._q, None, None))
+            self._cb = None
+            return
+        freq = self._freq
+
+        def add(ctx, t1, t2, rec, inten, phase, nf, run_id):
+            r = eigenray_model.from_record(rec.contents, inten[:nf], phase[:nf], freq)
+            for l in self._eig_listeners:
+                l.add_eigenray(t1, t2, r, run_id)
+
+        def check(ctx, time, run_id):
+            for l in self._eig_listeners:
+                l.check_eigenrays(time, run_id)
+
+        def reflect(ctx, rp):
+            r = rp.contents
+            pos = wposition1()
+            pos.rho, pos.theta, pos.phi = r.position[0], r.position[1], r.position[2]
+            nd = (r.ndirection[0], r.ndirection[1], r.ndirection[2])
+            for l in self._refl_listeners:
+                l.reflect(r.time, r.de, r.az, r.dt, r.grazing, r.speed, pos, nd, r.type)
+
+        cb = _abi.wq3d_callbacks()
+        cb.add_eigenray = _abi.ADD_EIGENRAY(add) if self._eig_listeners else _abi.ADD_EIGENRAY()
+        cb.check_eigenrays = _abi.CHECK_EIGENRAYS(check) if self._eig_listeners else _abi.CHECK_EIGENRAYS()
+        cb.reflect = _abi.REFLECT(reflect) if self._refl_listeners else _abi.REFLECT()
+        self._cb = cb
+        _abi.check(self._lib, self._lib.wq3d_queue_set_callbacks(self._q, C.byref(cb), None))
+
+    def add_eigenray_listener(self, listener):
+        if listener not in self._eig_listeners:
+            self._eig_listeners.append(listener)
+        self._install_callbacks()
+
+    def remove_eigenray_listener(self, listener):
+        if listener in self._eig_listeners:
+            self._eig_listeners.remove(listener)
+        self._install_callbacks()
+
+    def add_reflection_listener(self, listener):
+        if listener not in self._refl_listeners:
+            self._refl_listeners.append(listener)
+        self._install_callbacks()
+
+    def remove_reflection_listener(self, listener):
+        if listener in self._refl_listeners:
+            self._refl_listeners.remove(listener)
+        self._install_callbacks()
+
+    # ---------------- propagation ----------------
+    def step(self, nsteps=1):
+        """wave_queue::step() (wave_queue.cc:155-192); nsteps > 1 runs several."""
+        _abi.check(self._lib, self._lib.wq3d_queue_step(self._q, int(nsteps)))
+
+    def run(self, time_max):
+        """``while (time() < time_max) step();`` in one call."""
+        n = C.c_size_t()
+        _abi.check(self._lib, self._lib.wq3d_queue_run(self._q, float(time_max), C.byref(n)))
+        return n.value
+
+    def abort(self):
+        _abi.check(self._lib, self._lib.wq3d_queue_abort(self._q))
+
+    def take_eigenrays(self):
+        """Eigenrays found since the last call (when no eigenray listener is
+        registered), as a structured numpy array plus intensity and phase."""
+        n = C.c_size_t()
+        _abi.check(self._lib, self._lib.wq3d_queue_take_eigenrays(self._q, None, None, None, 0, C.byref(n)))
+        cnt = n.value
+        nf = self._freq.size()
+        recs = (_abi.wq3d_eigenray * max(cnt, 1))()
+        inten = np.empty(max(cnt, 1) * nf)
+        phase = np.empty(max(cnt, 1) * nf)
+        _abi.check(self._lib, self._lib.wq3d_queue_take_eigenrays(self._q, recs, _abi.as_dp(inten),
+                                                                  _abi.as_dp(phase), cnt, C.byref(n)))
+        out = [eigenray_model.from_record(recs[i], inten[i * nf:(i + 1) * nf],
+                                          phase[i * nf:(i + 1) * nf], self._freq) for i in range(cnt)]
+        return out
+
+    def set_timing(self, on):
+        _abi.check(self._lib, self._lib.wq3d_queue_set_timing(self._q, 1 if on else 0))
+
+    def timing(self, reset=False):
+        t, a, b, c = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        n = C.c_int64()
+        _abi.check(self._lib, self._lib.wq3d_queue_timing(self._q, C.byref(t), C.byref(a), C.byref(b),
+                                                          C.byref(c), C.byref(n), 1 if reset else 0))
+        return {"total_ms": t.value, "step_ms": a.value, "cpa_ms": b.value, "eigenray_ms": c.value,
+                "launches": n.value}
