@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="profiling mode: one queue of the workload, this many wave steps, no output")
     return ap.parse_args()
 
 
@@ -378,6 +380,14 @@ def main():
         return
     if world > 1:
         os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    if args.profile_steps:
+        import underseamodelinglibrary_b200 as u
+        from underseamodelinglibrary_b200 import scenarios as S
+        sc = S.linear_slope_rayleigh()
+        q = S.build_queue(sc, u.wave_queue, device=0)
+        q.step(args.profile_steps)
+        print("profile run: %d steps, %d eigenrays" % (q.steps(), len(q.take_eigenrays())))
+        return
     out = engine_arm(args, rank, world, dist)
     if rank == 0:
         if not args.no_cpu_baseline:

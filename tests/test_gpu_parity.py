@@ -250,7 +250,7 @@ def test_ocean_point_evaluations(engine):
     u.compute_earth_radius(45.0)
     src = u.wposition1(45.0, -45.0, -50.0)
     for prof in (u.profile_munk(), u.profile_linear(1500.0, 0.0163), u.profile_linear(1480.0, 0.02, 500.0, 0.01),
-                 u.profile_catenary(1500.0, 0.02, 1000.0), u.profile_n2(1550.0, 1.2)):
+                 u.profile_catenary(1500.0, 1500.0, 1000.0), u.profile_n2(1550.0, 1.2)):
         for flat in (False, True):
             prof.flat_earth(flat)
             bottom = u.boundary_slope(src, 200.0, -0.09, 0.01, u.reflect_loss_rayleigh(1.5, 1.1, 0.5))
