@@ -112,17 +112,59 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- FP64 peak
-FP64_PEAK_SRC = r"""
-extern "C" __global__ void fp64_peak(double* out, int iters) {
-    double a = threadIdx.x * 1e-3, b = 1.0000001, c = 0.9999999, d = blockIdx.x * 1e-6;
-    double e = a + 1.0, f = d + 2.0, g = a * 0.5, h = d * 0.25;
+PEAK_SRC = r"""
+#include <cuda_runtime.h>
+template <class T>
+__global__ void fma_peak(T* out, int iters) {
+    T a = threadIdx.x * (T)1e-3, b = (T)1.0000001, c = (T)0.9999999, d = blockIdx.x * (T)1e-6;
+    T e = a + (T)1, f = d + (T)2, g = a * (T)0.5, h = d * (T)0.25;
     for (int i = 0; i < iters; ++i) {
         a = a * b + c; d = d * b + c; e = e * b + c; f = f * b + c;
         g = g * b + c; h = h * b + c;
     }
     out[blockIdx.x * blockDim.x + threadIdx.x] = a + d + e + f + g + h;
 }
+template <class T>
+float run(int iters) {
+    T* out; cudaMalloc(&out, 148 * 8 * 256 * sizeof(T));
+    cudaEvent_t x, y; cudaEventCreate(&x); cudaEventCreate(&y);
+    fma_peak<T><<<148 * 8, 256>>>(out, 100);
+    cudaEventRecord(x);
+    fma_peak<T><<<148 * 8, 256>>>(out, iters);
+    cudaEventRecord(y); cudaEventSynchronize(y);
+    float ms = 0; cudaEventElapsedTime(&ms, x, y);
+    cudaFree(out); cudaEventDestroy(x); cudaEventDestroy(y);
+    return ms;
+}
+extern "C" float run_peak64(int iters) { return run<double>(iters); }
+extern "C" float run_peak32(int iters) { return run<float>(iters); }
 """
+
+
+def measure_fma_peaks():
+    """FP64 and FP32 FMA throughput (TFLOP/s, an FMA counted as 2 flops) of
+    this GPU: 6 independent FMA chains per thread, 148 x 8 blocks of 256
+    threads.  MEASURED_PEAKS.json carries only HBM and bf16 tensor figures."""
+    import ctypes as C
+    import tempfile
+    out = {"fp64": None, "fp32": None, "source": "measured by bench.py (FMA loop)"}
+    try:
+        d = tempfile.mkdtemp()
+        cu = os.path.join(d, "peak.cu")
+        so = os.path.join(d, "peak.so")
+        open(cu, "w").write(PEAK_SRC)
+        subprocess.check_call(["nvcc", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+                               "-Xcompiler", "-fPIC", "-o", so, cu], stdout=subprocess.DEVNULL,
+                              stderr=subprocess.DEVNULL)
+        lib = C.CDLL(so)
+        for name, key, iters in (("run_peak64", "fp64", 20000), ("run_peak32", "fp32", 40000)):
+            fn = getattr(lib, name)
+            fn.restype = C.c_float
+            ms = fn(iters)
+            out[key] = 148 * 8 * 256 * iters * 6 * 2 / (ms / 1e3) / 1e12
+    except Exception as e:  # noqa: BLE001
+        out["source"] = "unavailable: %s" % e
+    return out
 
 
 # ---------------------------------------------------------------- engine arm
@@ -140,8 +182,29 @@ def engine_arm(args, rank, world, dist):
         nsteps += 1
     ray_steps = nde * naz * nsteps
 
-    def make():
-        return S.build_queue(sc, u.wave_queue, device=0)
+    from underseamodelinglibrary_b200 import _abi
+
+    def make(precision=_abi.FP32C):
+        return S.build_queue(sc, u.wave_queue, device=0, precision=precision)
+
+    def timed_runs(precision, count):
+        """device time (ms) of ``count`` propagations, queues built first"""
+        qs = [make(precision) for _ in range(count)]
+        for q in qs:
+            q.set_timing(True)
+            q.timing(reset=True)
+        tot = cpa = stp = eig = 0.0
+        launches = neig = 0
+        for q in qs:
+            q.run(sc["time_max"])
+            tm = q.timing()
+            tot += tm["total_ms"]
+            cpa += tm["cpa_ms"]
+            stp += tm["step_ms"]
+            eig += tm["eigenray_ms"]
+            launches += tm["launches"]
+            neig += len(q.take_eigenrays())
+        return tot, cpa, stp, eig, launches, neig
 
     # device-resident timing: queues built (inputs in HBM) before the timer
     for _ in range(args.warmup):
@@ -149,28 +212,16 @@ def engine_arm(args, rank, world, dist):
         q.run(sc["time_max"])
         q.take_eigenrays()
         del q
-    queues = [make() for _ in range(args.steps)]
-    for q in queues:
-        q.set_timing(True)
-        q.timing(reset=True)
     clocks = ClockSampler(rank)
     clocks.start()
     if dist is not None:
         dist.barrier()
-    total_ms, cpa_ms, step_ms, eig_ms, launches, n_eig = 0.0, 0.0, 0.0, 0.0, 0, 0
-    for q in queues:
-        q.run(sc["time_max"])
-        tm = q.timing()
-        total_ms += tm["total_ms"]
-        cpa_ms += tm["cpa_ms"]
-        step_ms += tm["step_ms"]
-        eig_ms += tm["eigenray_ms"]
-        launches += tm["launches"]
-        n_eig += len(q.take_eigenrays())
+    total_ms, cpa_ms, step_ms, eig_ms, launches, n_eig = timed_runs(_abi.FP32C, args.steps)
     if dist is not None:
         dist.barrier()
     clk = clocks.stop()
-    del queues
+    # the plain FP64 form on the same workload, for the FP32C:FP64 ratio
+    f64_total, f64_cpa, f64_step, f64_eig, _, f64_neig = timed_runs(_abi.FP64, 1)
 
     # end to end through the public API with host buffers
     e2e_times = []
@@ -202,29 +253,37 @@ def engine_arm(args, rank, world, dist):
     cpa_launch_s = (cpa_ms / 1000.0) / launches_cpa
     flops_launch = FLOPS_PER_RAY_TARGET_STEP * interior * nt
     achieved = flops_launch / cpa_launch_s / 1e12
-    fp64_peak = measure_fp64_peak_cupyless()
+    peaks = measure_fma_peaks()
+    fp32_peak = peaks["fp32"]
     out = {
         "metric": METRIC, "value": value, "unit": "ray-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "rays": nde * naz, "num_de": nde, "num_az": naz,
                    "targets": nt, "frequencies": sc["freq"].size(), "wave_steps": nsteps,
-                   "form": "FP64", "parallelism": "replicas" if world > 1 else "single",
+                   "form": "FP32C (FP32-screened CPA, FP64 state)", "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set (4 fronts, %.0f MB) exceeds L2" % (nde * naz * 4 * 30 * 8 / 1e6)},
         "eigenrays_per_s": world * n_eig / total_s,
         "e2e": {"value": e2e, "unit": "ray-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
+        "fp64_form": {"value": ray_steps / (f64_total / 1000.0), "ms_per_step": f64_total,
+                      "kernel_ms": {"step+edges": f64_step, "cpa": f64_cpa, "eigenray": f64_eig},
+                      "eigenrays": f64_neig},
+        "eigenrays_per_propagation": n_eig / args.steps,
         "kernel_ms": {"step+edges": step_ms / args.steps, "cpa": cpa_ms / args.steps,
                       "eigenray": eig_ms / args.steps},
-        "roofline": {"bound": "fp64", "achieved": achieved,
-                     "peak": fp64_peak["tflops"] if fp64_peak else None,
+        "roofline": {"bound": "fp32", "achieved": achieved,
+                     "peak": fp32_peak,
                      "unit": "TFLOP/s",
-                     "frac": (achieved / fp64_peak["tflops"]) if fp64_peak else None,
+                     "frac": (achieved / fp32_peak) if fp32_peak else None,
                      "traffic": None,
-                     "kernel": "k_cpa",
-                     "peak_source": fp64_peak["source"] if fp64_peak else "unavailable",
+                     "kernel": "k_cpa_f32",
+                     "peak_source": peaks["source"] + "; MEASURED_PEAKS.json has no FP32/FP64 CUDA-core figure",
+                     "fp64_peak": peaks["fp64"],
+                     "fp64_form_cpa_frac_of_fp64_peak": (
+                         flops_launch / (f64_cpa / 1000.0 / nsteps) / 1e12 / peaks["fp64"]) if peaks["fp64"] else None,
                      "algorithmic_flops_per_launch": flops_launch},
         "roofline_hbm": hbm_roofline(interior, cpa_launch_s),
         "clocks": clk,
@@ -249,44 +308,6 @@ def hbm_roofline(interior, launch_s):
     achieved = interior * BYTES_PER_RAY_CPA / launch_s / 1e9
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": None, "peak_source": src}
-
-
-def measure_fp64_peak_cupyless():
-    """FP64 FMA throughput measured with a small CUDA kernel built by nvcc
-    (6 independent FMA chains per thread, 148 x 8 blocks of 256 threads)."""
-    import ctypes as C
-    import tempfile
-    src = FP64_PEAK_SRC + r"""
-#include <cuda_runtime.h>
-extern "C" float run_peak(int iters) {
-    double* out; cudaMalloc(&out, 148 * 8 * 256 * sizeof(double));
-    cudaEvent_t a, b; cudaEventCreate(&a); cudaEventCreate(&b);
-    fp64_peak<<<148 * 8, 256>>>(out, 100);
-    cudaEventRecord(a);
-    fp64_peak<<<148 * 8, 256>>>(out, iters);
-    cudaEventRecord(b); cudaEventSynchronize(b);
-    float ms = 0; cudaEventElapsedTime(&ms, a, b);
-    cudaFree(out); cudaEventDestroy(a); cudaEventDestroy(b);
-    return ms;
-}
-"""
-    try:
-        d = tempfile.mkdtemp()
-        cu = os.path.join(d, "peak.cu")
-        so = os.path.join(d, "peak.so")
-        open(cu, "w").write(src)
-        subprocess.check_call(["nvcc", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
-                               "-Xcompiler", "-fPIC", "-o", so, cu], stdout=subprocess.DEVNULL,
-                              stderr=subprocess.DEVNULL)
-        lib = C.CDLL(so)
-        lib.run_peak.restype = C.c_float
-        iters = 20000
-        ms = lib.run_peak(iters)
-        flops = 148 * 8 * 256 * iters * 6 * 2
-        return {"tflops": flops / (ms / 1e3) / 1e12,
-                "source": "measured by bench.py (FP64 FMA loop; MEASURED_PEAKS.json has no FP64 figure)"}
-    except Exception as e:  # noqa: BLE001
-        return {"tflops": None, "source": "unavailable: %s" % e}
 
 
 # ---------------------------------------------------------------- CPU arms

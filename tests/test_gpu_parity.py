@@ -319,3 +319,42 @@ def test_abort_between_chunks(engine):
     assert ei.value.code == _abi.WQ3D_ERR_ABORTED
     q.step(5)  # the flag is consumed; propagation continues
     assert q.steps() == 5
+
+
+def _identical(ra, rb):
+    assert [key(r) for r in ra] == [key(r) for r in rb]
+    for x, y in zip(ra, rb):
+        assert x.travel_time == y.travel_time
+        assert np.array_equal(x.intensity, y.intensity)
+        assert (x.source_de, x.source_az, x.target_de, x.target_az) == \
+            (y.source_de, y.source_az, y.target_de, y.target_az)
+        assert (x.surface, x.bottom, x.caustic, x.upper, x.lower) == \
+            (y.surface, y.bottom, y.caustic, y.upper, y.lower)
+
+
+@pytest.mark.parametrize("builder", [
+    lambda: S.munk_flat(),
+    lambda: S.linear_slope_rayleigh(num_de=451, num_az=31, n_range=16, n_depth=16, time_max=20.0),
+    lambda: S.eigenray_branch_pt(),
+])
+def test_fp32c_screen_matches_fp64(engine, builder):
+    """The FP32C form screens CPA comparisons in FP32 and falls back to the
+    FP64 expression inside its error bound, so every eigenray must equal
+    the FP64 form's, bit for bit."""
+    sc = builder()
+    a = S.build_queue(sc, u.wave_queue, precision=_abi.FP64)
+    b = S.build_queue(sc, u.wave_queue, precision=_abi.FP32C)
+    a.run(sc["time_max"])
+    b.run(sc["time_max"])
+    ra, rb = a.take_eigenrays(), b.take_eigenrays()
+    assert len(ra) > 0
+    _identical(ra, rb)
+
+
+def test_fp32c_matches_oracle_on_sloped_workload(engine):
+    sc = S.linear_slope_rayleigh(num_de=181, num_az=19, n_range=8, n_depth=8, time_max=10.0)
+    q = S.build_queue(sc, u.wave_queue, precision=_abi.FP32C)
+    o = S.build_queue(sc, OracleQueue)
+    q.run(sc["time_max"])
+    o.run(sc["time_max"])
+    compare_eigenrays(q.take_eigenrays(), o.take_eigenrays())

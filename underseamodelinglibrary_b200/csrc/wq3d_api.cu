@@ -195,9 +195,12 @@ struct wq3d_queue {
         if (h.nt > 0) {
             const dim3 cg((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS);
             if (ev) cudaEventRecord(ev[2], stream);
-            k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d_q, k);
+            if (h.precision == WQ3D_FP32C)
+                k_cpa_f32<<<cg, CPA_THREADS, 0, stream>>>(d_q, k);
+            else
+                k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d_q, k);
             if (ev) cudaEventRecord(ev[3], stream);
-            k_eigenray<<<148, 64, 0, stream>>>(d_q, k);
+            k_eigenray<<<148, 128, 0, stream>>>(d_q, k);
             if (ev) cudaEventRecord(ev[4], stream);
             launches += 2;
         } else if (ev) {
@@ -475,7 +478,8 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     if (d->num_freq > (size_t)MAX_FREQ) return fail(WQ3D_ERR_UNSUPPORTED, "more than 64 frequencies");
     if (d->num_az > (size_t)MAX_AZ) return fail(WQ3D_ERR_UNSUPPORTED, "more than 4096 AZ angles");
     if (!(d->time_step > 0.0)) return fail(WQ3D_ERR_INVALID, "time_step must be positive");
-    if (d->precision != WQ3D_FP64) return fail(WQ3D_ERR_UNSUPPORTED, "only the FP64 form is built");
+    if (d->precision != WQ3D_FP64 && d->precision != WQ3D_FP32C)
+        return fail(WQ3D_ERR_INVALID, "precision must be WQ3D_FP64 or WQ3D_FP32C");
     const size_t n = d->num_de * d->num_az;
     if (n > (size_t)0x7fffffff) return fail(WQ3D_ERR_INVALID, "ray fan too large");
     const size_t nt = (d->targets && d->num_targets1 * d->num_targets2 > 0)
@@ -502,6 +506,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.dt = d->time_step;
     h.R = d->earth_radius;
     h.spreading = d->spreading;
+    h.precision = d->precision;
     h.intensity_threshold = 300.0;
     h.max_bottom = h.max_surface = h.max_caustic = h.max_upper = h.max_lower = 999;
 

@@ -67,6 +67,7 @@ struct QueueDev {
     int nt, nt1, nt2;
     int az_boundary;
     int spreading;
+    int precision;
     double dt;
     double R;
     /* fans and frequencies */
@@ -125,6 +126,7 @@ __global__ void k_startup(const QueueDev* q);
 __global__ void k_step(const QueueDev* q, int k);
 __global__ void k_edges(const QueueDev* q, int k);
 __global__ void k_cpa(const QueueDev* q, int k);
+__global__ void k_cpa_f32(const QueueDev* q, int k);
 __global__ void k_eigenray(const QueueDev* q, int k);
 __global__ void k_sound_speed(OceanDev oc, double R, int n, const double* rho,
                               const double* theta, const double* phi,

@@ -740,20 +740,172 @@ __global__ void __launch_bounds__(CPA_THREADS) k_cpa(const QueueDev* __restrict_
 }
 
 /* ------------------------------------------------------------------ */
+/* CPA search with an FP32 screen (FP32C form)                         */
+/* ------------------------------------------------------------------ */
+/* The two comparisons that reject almost every (ray, target) pair --
+ * "next <= curr" and "prev < curr" on distance2 (wave_queue.cc:386-393) --
+ * are first decided in FP32 on the algebraically equal form
+ *     distance2 = (rho - R)^2 + rho R ((theta - Theta)^2 + sinT sin(theta) (phi - Phi)^2)
+ * with every coordinate taken relative to a reference ray of the block, so
+ * that all terms are non-negative and small.  A comparison is accepted only
+ * when the FP32 difference exceeds a bound on the error of both the FP32
+ * value and the reference's own FP64 expression; otherwise the FP64
+ * expression decides, exactly as k_cpa does.  Pairs that pass both go
+ * through the FP64 is_closest test.  The accepted decisions therefore equal
+ * the FP64 decisions, and so does the set of eigenrays.
+ *
+ * Error bound (u = 2^-24): relative error <= 17 u, plus an absolute term
+ * 2u (E_rho^2 + rho R (E_theta^2 + E_phi^2)) from the block-relative
+ * coordinates (E = largest offset of a ray of the block from the reference
+ * ray), plus the FP64 expression's own rounding, <= 8 * 2^-53 (rho^2 + R^2).
+ * The kernel uses 4x / 4x / 8x those figures. */
+namespace {
+struct TgtF {
+    float R, T, P, S, Rf;
+};
+}  // namespace
+
+__global__ void __launch_bounds__(CPA_THREADS) k_cpa_f32(const QueueDev* __restrict__ qp, int k) {
+    const QueueDev& q = *qp;
+    __shared__ TgtS tile[CPA_TARGETS];
+    __shared__ TgtF tf[CPA_TARGETS];
+    __shared__ float red[4][CPA_THREADS / 32];
+    const int64_t s = *q.d_base + k + 1;
+    const FrontPtrs& V = q.F[(s + 1) & 3];
+    const FrontPtrs& C = q.F[(s + 2) & 3];
+    const FrontPtrs& X = q.F[(s + 3) & 3];
+    const int t0 = blockIdx.y * CPA_TARGETS;
+    const int nt_tile = min(CPA_TARGETS, q.nt - t0);
+    const int i_ref = min((int)(blockIdx.x * blockDim.x), q.n - 1);
+    const double rho_ref = C.cpa[0][i_ref], th_ref = C.cpa[1][i_ref], ph_ref = C.cpa[2][i_ref];
+    float Rmax = 0.0f;
+    for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
+        const int t = t0 + j;
+        const double R = q.tgt[0][t], T = q.tgt[1][t], P = q.tgt[2][t];
+        tile[j] = TgtS{T, P, q.tgt_sin[t], q.tgt_R2[t], q.tgt_2R[t]};
+        tf[j] = TgtF{(float)(R - rho_ref), (float)(T - th_ref), (float)(P - ph_ref),
+                     (float)q.tgt_sin[t], (float)R};
+        Rmax = fmaxf(Rmax, (float)R);
+    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ic = min(i, q.n - 1);
+    /* block-relative coordinates of this ray on the three fronts */
+    float r32[3], t32[3], p32[3], s32[3], k32[3];
+    float Er = 0.0f, Et = 0.0f, Ep = 0.0f, rmax = 0.0f;
+    const FrontPtrs* fr[3] = {&V, &C, &X};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const double rho = fr[m]->cpa[0][ic], th = fr[m]->cpa[1][ic], ph = fr[m]->cpa[2][ic];
+        r32[m] = (float)(rho - rho_ref);
+        t32[m] = (float)(th - th_ref);
+        p32[m] = (float)(ph - ph_ref);
+        s32[m] = (float)fr[m]->cpa[3][ic];
+        k32[m] = (float)rho;
+        Er = fmaxf(Er, fabsf(r32[m]));
+        Et = fmaxf(Et, fabsf(t32[m]));
+        Ep = fmaxf(Ep, fabsf(p32[m]));
+        rmax = fmaxf(rmax, k32[m]);
+    }
+    /* block maxima */
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        Er = fmaxf(Er, __shfl_xor_sync(0xffffffffu, Er, o));
+        Et = fmaxf(Et, __shfl_xor_sync(0xffffffffu, Et, o));
+        Ep = fmaxf(Ep, __shfl_xor_sync(0xffffffffu, Ep, o));
+        rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        Rmax = fmaxf(Rmax, __shfl_xor_sync(0xffffffffu, Rmax, o));
+    }
+    if (l == 0) {
+        red[0][w] = Er;
+        red[1][w] = fmaxf(Et, Ep);
+        red[2][w] = rmax;
+        red[3][w] = Rmax;
+    }
+    __syncthreads();
+    float bEr = 0.0f, bEa = 0.0f, brm = 0.0f, bRm = 0.0f;
+#pragma unroll
+    for (int j = 0; j < CPA_THREADS / 32; ++j) {
+        bEr = fmaxf(bEr, red[0][j]);
+        bEa = fmaxf(bEa, red[1][j]);
+        brm = fmaxf(brm, red[2][j]);
+        bRm = fmaxf(bRm, red[3][j]);
+    }
+    const float u = 5.9604645e-8f;
+    const float c_rel = 4.0f * 17.0f * u;
+    const float Kmax = brm * bRm * 1.0001f;
+    const float c_abs = 4.0f * 2.0f * u * (bEr * bEr + Kmax * 2.0f * bEa * bEa) +
+                        8.0f * 8.0f * 1.1102230e-16f * (brm * brm + bRm * bRm) + 1e-3f;
+
+    if (i >= q.n) return;
+    if (q.nde < 3 || q.naz < 3) return;
+    const int de = i / q.naz, az = i % q.naz;
+    const int az_start = q.az_boundary ? 0 : 1;
+    if (de < 1 || de >= q.nde - 1 || az < az_start || az >= q.naz - 1) return;
+    if (C.on_edge[i]) return;
+    for (int j = 0; j < nt_tile; ++j) {
+        const TgtF g = tf[j];
+        float d32[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const float dr = r32[m] - g.R;
+            const float x = t32[m] - g.T;
+            const float y = p32[m] - g.P;
+            const float e = fmaf(x, x, (s32[m] * g.S) * (y * y));
+            d32[m] = fmaf(dr, dr, (k32[m] * g.Rf) * e);
+        }
+        /* next <= curr ? */
+        const float gX = fmaf(c_rel, d32[2] + d32[1], 2.0f * c_abs);
+        const float dXC = d32[2] - d32[1];
+        double center = 0.0;
+        bool have_center = false;
+        if (dXC < -gX) continue;
+        if (!(dXC > gX)) {
+            const TgtS t = tile[j];
+            center = d2_at(C, i, t);
+            have_center = true;
+            if (d2_at(X, i, t) <= center) continue;
+        }
+        /* prev < curr ? */
+        const float gV = fmaf(c_rel, d32[0] + d32[1], 2.0f * c_abs);
+        const float dVC = d32[0] - d32[1];
+        if (dVC < -gV) continue;
+        const TgtS t = tile[j];
+        if (!have_center) center = d2_at(C, i, t);
+        if (!(dVC > gV)) {
+            if (d2_at(V, i, t) < center) continue;
+        }
+        double cube[3][3][3];
+        if (!is_closest(q, V, C, X, t, q.de_branch[t0 + j] != 0, de, az, center, cube)) continue;
+        const uint32_t slot = atomicAdd(q.n_cand, 1u);
+        if (slot < q.cap_cand) {
+            q.cand[2 * slot] = (uint32_t)(t0 + j);
+            q.cand[2 * slot + 1] = (uint32_t)i;
+        } else {
+            set_err(q, ERR_CAND_OVERFLOW);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* eigenray construction (wave_queue.cc:495-977 + spreading models)    */
 /* ------------------------------------------------------------------ */
 namespace {
 
-struct Build {
+/* One warp builds one eigenray.  Lanes share the parallel parts (the 27
+ * distance2 values, the 54 direction angles, the cell widths and Gaussian
+ * terms of the beam walks, the per-frequency sums); every value that feeds
+ * a rounding-sensitive recurrence (cell distances, the running intensity
+ * and its threshold test) is formed in the reference's sequential order,
+ * so results equal the one-thread-per-eigenray evaluation. */
+struct WarpBuild {
     const QueueDev* q;
     const FrontPtrs* pV;
     const FrontPtrs* pC;
     const FrontPtrs* pX;
-    int t;
-    double inten_de[MAX_FREQ];
-    double inten_az[MAX_FREQ];
-    const double* spread2;
-    uint32_t dup[MAX_AZ / 32];
+    const double* spread2;   /* [nf] for this target */
+    int lane;
+    double Ilo, Ihi;         /* running intensity of frequencies lane, lane+32 */
 
     __device__ double fdist(const FrontPtrs& f, int d1, int a1, int d2, int a2) const {
         const int i = d1 * q->naz + a1, j = d2 * q->naz + a2;
@@ -763,17 +915,27 @@ struct Build {
     __device__ double de_inc(int d) const { return q->de_inc[min(max(d, 0), q->nde - 1)]; }
     __device__ double az_inc(int a) const { return q->az_inc[min(max(a, 0), q->naz - 1)]; }
 
-    /* spreading_hybrid_gaussian.h:148-153, accumulated into acc */
-    __device__ void gauss_add(double d, double w, double A, double* acc, bool first) {
-        for (int k = 0; k < q->nf; ++k) {
-            const double bw = spread2[k] + 2.0 * 2.0 * w * w;
-            const double g = exp((-0.5 * d * d) / bw) / sqrt(bw) * A;
-            acc[k] = first ? g : acc[k] + g;
+    /* spreading_hybrid_gaussian.h:148-153 for one frequency */
+    __device__ double gauss(double d, double w, double A, int f) const {
+        const double bw = spread2[f] + 2.0 * 2.0 * w * w;
+        return exp((-0.5 * d * d) / bw) / sqrt(bw) * A;
+    }
+    /* running intensity += gaussian, frequencies spread over the lanes */
+    __device__ void acc(double d, double w, double A, bool first) {
+        const int nf = q->nf;
+        if (lane < nf) {
+            const double g = gauss(d, w, A, lane);
+            Ilo = first ? g : Ilo + g;
+        }
+        if (lane + 32 < nf) {
+            const double g = gauss(d, w, A, lane + 32);
+            Ihi = first ? g : Ihi + g;
         }
     }
+    __device__ double I0() const { return __shfl_sync(0xffffffffu, Ilo, 0); }
 
     /* spreading_hybrid_gaussian.cc:430-495 */
-    __device__ double width_de(int d, int a, const double* offset) {
+    __device__ double width_de(int d, int a, const double* offset) const {
         const double u = fabs(offset[0]) / q->dt;
         const double v = fabs(offset[2]) / az_inc(a);
         const int max_az = q->naz - 1;
@@ -799,7 +961,7 @@ struct Build {
     }
 
     /* spreading_hybrid_gaussian.cc:500-571 */
-    __device__ double width_az(int d, int a, const double* offset) {
+    __device__ double width_az(int d, int a, const double* offset) const {
         const double u = fabs(offset[0]) / q->dt;
         const double v = fabs(offset[1]) / de_inc(d);
         const int max_az = q->naz - 1;
@@ -826,151 +988,267 @@ struct Build {
         return 0.5 * ((1.0 - u) * length1 + u * length2);
     }
 
+    /* Processes up to 32 prepared cells of one walk.  Lane k holds cell k's
+     * width (w_k), whether the cell is a virtual ray (virt_k) and the two
+     * normalisation candidates.  sign = +1 for a walk away from the lower
+     * side (cell distances grow), -1 otherwise.  Returns true when the walk
+     * stops inside these cells. */
+    __device__ bool run_cells(int ncell, double w_k, bool virt_k, double norm_k,
+                              double norm_virt_k, double sign, double& cell_dist,
+                              double& cell_width) {
+        double my_cd = 0.0, my_cw = 0.0, my_nm = 0.0;
+        int nend = ncell;
+        bool stop = false;
+        for (int k = 0; k < ncell; ++k) {
+            const bool v = __shfl_sync(0xffffffffu, virt_k, k);
+            const double wk = __shfl_sync(0xffffffffu, w_k, k);
+            const double nk = __shfl_sync(0xffffffffu, v ? norm_virt_k : norm_k, k);
+            if (sign > 0.0) {
+                cell_dist += cell_width;
+                if (v) {
+                    cell_dist += cell_width;
+                } else {
+                    cell_width = wk;
+                    cell_dist += cell_width;
+                }
+            } else {
+                cell_dist -= cell_width;
+                if (v) {
+                    cell_dist -= cell_width;
+                } else {
+                    cell_width = wk;
+                    cell_dist -= cell_width;
+                }
+            }
+            if (lane == k) {
+                my_cd = cell_dist;
+                my_cw = cell_width;
+                my_nm = nk;
+            }
+            if (v) {
+                nend = k + 1;
+                stop = true;
+                break;
+            }
+        }
+        /* threshold scan on the lowest frequency, in order */
+        const double g0 = (lane < nend) ? gauss(my_cd, my_cw, my_nm, 0) : 0.0;
+        double i0 = I0();
+        int kstar = nend - 1;
+        for (int k = 0; k < nend; ++k) {
+            const double old = i0;
+            i0 += __shfl_sync(0xffffffffu, g0, k);
+            if (i0 / old < 1.002305238) {
+                kstar = k;
+                stop = true;
+                break;
+            }
+        }
+        /* accumulate every frequency over cells 0..kstar, in order */
+        for (int k = 0; k <= kstar; ++k) {
+            const double cd = __shfl_sync(0xffffffffu, my_cd, k);
+            const double cw = __shfl_sync(0xffffffffu, my_cw, k);
+            const double nm = __shfl_sync(0xffffffffu, my_nm, k);
+            acc(cd, cw, nm, false);
+        }
+        return stop;
+    }
+
     /* spreading_hybrid_gaussian.cc:124-258 */
     __device__ void intensity_de(int de0, int a, const double* offset, const double* distance) {
         const QueueDev& Q = *q;
         const FrontPtrs& C = *pC;
-        int d = de0;
-        double cell_width = width_de(d, a, offset);
-        const double initial_width = cell_width;
+        double wl = 0.0, wc = 0.0;
+        if (lane == 0) wc = width_de(de0, a, offset);
+        if (lane == 1) wl = width_de(de0 - 1, a, offset);
+        wc = __shfl_sync(0xffffffffu, wc, 0);
+        wl = __shfl_sync(0xffffffffu, wl, 1);
         const double L = distance[1];
-        double cell_dist = L - cell_width;
-        gauss_add(cell_dist, cell_width, Q.norm_de[d], inten_de, true);
-        d = de0 - 1;
-        cell_width = width_de(d, a, offset);
-        cell_dist = L + cell_width;
-        gauss_add(cell_dist, cell_width, Q.norm_de[d], inten_de, false);
-        if (inten_de[0] < 1e-10) return;
-        for (d = de0 - 2; d >= 0; --d) {
-            const bool virtual_ray = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
-            double new_norm;
-            cell_dist += cell_width;
-            if (virtual_ray) {
-                cell_dist += cell_width;
-                new_norm = Q.norm_de[d + 1];
-            } else {
-                cell_width = width_de(d, a, offset);
-                cell_dist += cell_width;
-                new_norm = Q.norm_de[d];
+        acc(L - wc, wc, Q.norm_de[de0], true);
+        acc(L + wl, wl, Q.norm_de[de0 - 1], false);
+        if (I0() < 1e-10) return;
+        /* lower D/E cells: de0-2 down to 0 */
+        double cell_width = wl, cell_dist = L + wl;
+        for (int d0 = de0 - 2; d0 >= 0; d0 -= 32) {
+            const int d = d0 - lane;
+            const int ncell = min(32, d0 + 1);
+            bool virt = false;
+            double w = 0.0, nm = 0.0, nmv = 0.0;
+            if (lane < ncell) {
+                virt = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
+                if (!virt) w = width_de(d, a, offset);
+                nm = Q.norm_de[d];
+                nmv = Q.norm_de[d + 1];
             }
-            const double old_tl = inten_de[0];
-            gauss_add(cell_dist, cell_width, new_norm, inten_de, false);
-            if (inten_de[0] / old_tl < 1.002305238) break;
-            if (virtual_ray) break;
+            if (run_cells(ncell, w, virt, nm, nmv, 1.0, cell_dist, cell_width)) break;
         }
-        cell_width = initial_width;
-        cell_dist = L - cell_width;
+        /* upper D/E cells: de0+1 up to num_de-2 */
+        cell_width = wc;
+        cell_dist = L - wc;
         const int size = Q.nde - 1;
-        for (d = de0 + 1; d < size; ++d) {
-            const bool virtual_ray = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
-            double new_norm;
-            cell_dist -= cell_width;
-            if (virtual_ray) {
-                cell_dist -= cell_width;
-                new_norm = Q.norm_de[d - 1];
-            } else {
-                cell_width = width_de(d, a, offset);
-                cell_dist -= cell_width;
-                new_norm = Q.norm_de[d];
+        for (int d0 = de0 + 1; d0 < size; d0 += 32) {
+            const int d = d0 + lane;
+            const int ncell = min(32, size - d0);
+            bool virt = false;
+            double w = 0.0, nm = 0.0, nmv = 0.0;
+            if (lane < ncell) {
+                virt = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
+                if (!virt) w = width_de(d, a, offset);
+                nm = Q.norm_de[d];
+                nmv = Q.norm_de[d - 1];
             }
-            const double old_tl = inten_de[0];
-            gauss_add(cell_dist, cell_width, new_norm, inten_de, false);
-            if (inten_de[0] / old_tl < 1.002305238) break;
-            if (virtual_ray) break;
+            if (run_cells(ncell, w, virt, nm, nmv, -1.0, cell_dist, cell_width)) break;
         }
     }
 
-    __device__ bool dup_test_set(int a) {
-        const uint32_t m = 1u << (a & 31);
-        const bool was = (dup[a >> 5] & m) != 0;
-        dup[a >> 5] |= m;
-        return was;
-    }
-
-    /* spreading_hybrid_gaussian.cc:264-425 */
+    /* spreading_hybrid_gaussian.cc:264-425.  The duplicate mask of the
+     * reference is a cyclic range: the lower walk marks a contiguous run of
+     * AZ indices below the centre, so membership is a range test. */
     __device__ void intensity_az(int d, int az0, const double* offset, const double* distance) {
         const QueueDev& Q = *q;
         const FrontPtrs& C = *pC;
         const int max_de = Q.nde - 2;
         const int max_az = Q.naz - 1;
-        int az_upper, az_lower;
-        if (Q.az_boundary) {
-            az_lower = az_upper = az0;
-        } else {
-            az_lower = 0;
-            az_upper = max_az - 1;
-        }
-        for (int w = 0; w < (Q.naz + 31) / 32; ++w) dup[w] = 0u;
-        auto norm = [&](int a) { return (d >= max_de) ? Q.norm_az[1 * Q.naz + a] : Q.norm_az[d * Q.naz + a]; };
-        int a = az0;
-        dup_test_set(a);
-        double cell_width = width_az(d, a, offset);
-        const double initial_width = cell_width;
+        const int az_lower = Q.az_boundary ? az0 : 0;
+        const int az_upper = Q.az_boundary ? az0 : max_az - 1;
+        auto norm = [&](int aa) { return (d >= max_de) ? Q.norm_az[1 * Q.naz + aa] : Q.norm_az[d * Q.naz + aa]; };
+        const int a1 = (az0 < 1) ? max_az - 1 : az0 - 1;
+        double wc = 0.0, wl = 0.0;
+        if (lane == 0) wc = width_az(d, az0, offset);
+        if (lane == 1) wl = width_az(d, a1, offset);
+        wc = __shfl_sync(0xffffffffu, wc, 0);
+        wl = __shfl_sync(0xffffffffu, wl, 1);
         const double L = distance[2];
-        double cell_dist = L - cell_width;
-        gauss_add(cell_dist, cell_width, norm(a), inten_az, true);
-        a = (az0 < 1) ? max_az - 1 : az0 - 1;
-        dup_test_set(a);
-        cell_width = width_az(d, a, offset);
-        cell_dist = L + cell_width;
-        gauss_add(cell_dist, cell_width, norm(a), inten_az, false);
-        if (inten_az[0] < 1e-10) return;
-        if (a < 1) {
-            a = max_az - 1;
-        } else {
-            --a;
-        }
-        int guard = 0;
-        while ((a % max_az) != az_lower) {
-            if (++guard > Q.naz + 2) {
-                set_err(Q, ERR_WALK_LIMIT);
-                break;
+        acc(L - wc, wc, norm(az0), true);
+        acc(L + wl, wl, norm(a1), false);
+        if (I0() < 1e-10) return;
+        /* lower walk: a1-1, a1-2, ... (cyclic) until az_lower */
+        const int start = (a1 < 1) ? max_az - 1 : a1 - 1;
+        double cell_width = wl, cell_dist = L + wl;
+        int marked = -1; /* index (in walk order) of the last cell marked */
+        bool done = false;
+        for (int k0 = 0; !done && k0 < max_az; k0 += 32) {
+            const int k = k0 + lane;
+            int a = start - k;
+            a = ((a % max_az) + max_az) % max_az;
+            /* per-cell stop tests, in the reference's order */
+            int kind = 0; /* 0 process, 1 loop end (not marked), 2 marked stop */
+            if (k >= max_az || a == az_lower) {
+                kind = 1;
+            } else if (a == az0 || a == a1) {
+                kind = 1;
+            } else if (C.on_edge[d * Q.naz + a]) {
+                kind = 2;
             }
-            if (dup_test_set(a)) break;
-            if (C.on_edge[d * Q.naz + a]) break;
-            cell_dist += cell_width;
-            cell_width = width_az(d, a, offset);
-            cell_dist += cell_width;
-            const double old_tl = inten_az[0];
-            gauss_add(cell_dist, cell_width, norm(a), inten_az, false);
-            if (inten_az[0] / old_tl < 1.002305238) break;
-            if (a == 0) {
-                a += max_az - 1;
+            const unsigned stopmask = __ballot_sync(0xffffffffu, kind != 0);
+            int first = 32, fk = 0;
+            if (stopmask) {
+                first = __ffs(stopmask) - 1;
+                fk = __shfl_sync(0xffffffffu, kind, first);
+            }
+            const int ncell = first;
+            double w = 0.0;
+            if (lane < ncell) w = width_az(d, a, offset);
+            const double nm = (lane < ncell) ? norm(a) : 0.0;
+            int kst = -1;
+            const bool brk = (ncell > 0) && run_cells_az(ncell, w, nm, 1.0, cell_dist, cell_width, kst);
+            if (brk) {
+                marked = k0 + kst; /* the threshold stop happens on a marked cell */
+                done = true;
             } else {
-                --a;
+                if (ncell > 0) marked = k0 + ncell - 1;
+                if (stopmask) {
+                    done = true;
+                    if (fk == 2) marked = k0 + first; /* on_edge cells are marked, not used */
+                }
             }
         }
-        cell_width = initial_width;
-        cell_dist = L - cell_width;
-        a = az0 + 1;
-        guard = 0;
-        while ((a % max_az) != az_upper) {
-            if (++guard > Q.naz + 2) {
-                set_err(Q, ERR_WALK_LIMIT);
+        /* upper walk: az0+1, az0+2, ... (cyclic) until az_upper */
+        cell_width = wc;
+        cell_dist = L - wc;
+        done = false;
+        for (int k0 = 0; !done && k0 < max_az; k0 += 32) {
+            const int k = k0 + lane;
+            const int a = (az0 + 1 + k) % max_az;
+            int kind = 0;
+            /* membership of the lower walk's marked cells: start-j, j <= marked */
+            const int off = ((start - a) % max_az + max_az) % max_az;
+            const bool dup = (a == az0) || (a == a1) || (marked >= 0 && off <= marked);
+            if (k >= max_az || a == az_upper) {
+                kind = 1;
+            } else if (dup) {
+                kind = 1;
+            } else if (C.on_edge[d * Q.naz + a]) {
+                kind = 1;
+            }
+            const unsigned stopmask = __ballot_sync(0xffffffffu, kind != 0);
+            int ncell = 32;
+            if (stopmask) {
+                ncell = __ffs(stopmask) - 1;
+                done = true;
+            }
+            double w = 0.0;
+            if (lane < ncell) w = width_az(d, a, offset);
+            const double nm = (lane < ncell) ? norm(a) : 0.0;
+            int kst = -1;
+            if (ncell > 0 && run_cells_az(ncell, w, nm, -1.0, cell_dist, cell_width, kst)) done = true;
+        }
+    }
+
+    /* AZ walks have no virtual rays; a threshold stop marks the cell it
+     * happened on (for the upper walk's duplicate test) */
+    __device__ bool run_cells_az(int ncell, double w_k, double norm_k, double sign,
+                                 double& cell_dist, double& cell_width, int& kstop) {
+        double my_cd = 0.0, my_cw = 0.0, my_nm = 0.0;
+        for (int k = 0; k < ncell; ++k) {
+            const double wk = __shfl_sync(0xffffffffu, w_k, k);
+            const double nk = __shfl_sync(0xffffffffu, norm_k, k);
+            if (sign > 0.0) {
+                cell_dist += cell_width;
+                cell_width = wk;
+                cell_dist += cell_width;
+            } else {
+                cell_dist -= cell_width;
+                cell_width = wk;
+                cell_dist -= cell_width;
+            }
+            if (lane == k) {
+                my_cd = cell_dist;
+                my_cw = cell_width;
+                my_nm = nk;
+            }
+        }
+        const double g0 = (lane < ncell) ? gauss(my_cd, my_cw, my_nm, 0) : 0.0;
+        double i0 = I0();
+        int kstar = ncell - 1;
+        bool stop = false;
+        for (int k = 0; k < ncell; ++k) {
+            const double old = i0;
+            i0 += __shfl_sync(0xffffffffu, g0, k);
+            if (i0 / old < 1.002305238) {
+                kstar = k;
+                stop = true;
                 break;
             }
-            if (a == max_az) a = 0;
-            if (dup_test_set(a)) break;
-            if (C.on_edge[d * Q.naz + a]) break;
-            cell_dist -= cell_width;
-            cell_width = width_az(d, a, offset);
-            cell_dist -= cell_width;
-            const double old_tl = inten_az[0];
-            gauss_add(cell_dist, cell_width, norm(a), inten_az, false);
-            if (inten_az[0] / old_tl < 1.002305238) break;
-            ++a;
         }
+        for (int k = 0; k <= kstar; ++k) {
+            const double cd = __shfl_sync(0xffffffffu, my_cd, k);
+            const double cw = __shfl_sync(0xffffffffu, my_cw, k);
+            const double nm = __shfl_sync(0xffffffffu, my_nm, k);
+            acc(cd, cw, nm, false);
+        }
+        if (stop) kstop = kstar;
+        return stop;
     }
 
     /* wvector1::area on four points (types/wvector1.cc) */
     __device__ double area4(const FrontPtrs& f, int d, int a) const {
-        auto dist = [&](int d1, int a1, int d2, int a2) { return fdist(f, d1, a1, d2, a2); };
-        double aa = dist(d, a, d + 1, a);
-        const double b = dist(d, a, d + 1, a + 1);
-        double c = dist(d + 1, a, d + 1, a + 1);
+        double aa = fdist(f, d, a, d + 1, a);
+        const double b = fdist(f, d, a, d + 1, a + 1);
+        double c = fdist(f, d + 1, a, d + 1, a + 1);
         const double area1 = 0.25 * sqrt((aa + b + c) * (b + c - aa) * (c + aa - b) * (aa + b - c));
-        aa = dist(d, a, d, a + 1);
-        c = dist(d, a + 1, d + 1, a + 1);
+        aa = fdist(f, d, a, d, a + 1);
+        c = fdist(f, d, a + 1, d + 1, a + 1);
         const double area2 = 0.25 * sqrt((aa + b + c) * (b + c - aa) * (c + aa - b) * (aa + b - c));
         return area1 + area2;
     }
@@ -1133,20 +1411,30 @@ __device__ void compute_offsets(const QueueDev& q, const FrontPtrs& V, const Fro
 
 }  // namespace
 
-__global__ void __launch_bounds__(64) k_eigenray(const QueueDev* __restrict__ qp, int k) {
+constexpr int EIG_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(const QueueDev* __restrict__ qp, int k) {
     const QueueDev& q = *qp;
+    __shared__ double s_cube[EIG_WARPS][27];
+    __shared__ double s_ang[EIG_WARPS][2][27];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const int64_t s = *q.d_base + k + 1;
     const double time = q.d_times[k + 1];
     const uint32_t ncand = min(*q.n_cand, q.cap_cand);
-    Build B;
+    WarpBuild B;
     B.q = qp;
     B.pV = &q.F[(s + 1) & 3];
     B.pC = &q.F[(s + 2) & 3];
     B.pX = &q.F[(s + 3) & 3];
+    B.lane = lane;
     const FrontPtrs& V = *B.pV;
     const FrontPtrs& C = *B.pC;
     const FrontPtrs& X = *B.pX;
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncand; c += gridDim.x * blockDim.x) {
+    double (*cube)[3][3] = reinterpret_cast<double (*)[3][3]>(s_cube[warp]);
+    const uint32_t nwarps = gridDim.x * EIG_WARPS;
+    for (uint32_t c = blockIdx.x * EIG_WARPS + warp; c < ncand; c += nwarps) {
+        __syncwarp();
         const int t = (int)q.cand[2 * c];
         const int i = (int)q.cand[2 * c + 1];
         const int de0 = i / q.naz, az0 = i % q.naz;
@@ -1155,20 +1443,20 @@ __global__ void __launch_bounds__(64) k_eigenray(const QueueDev* __restrict__ qp
             C.caustic[i] > q.max_caustic || C.upper[i] > q.max_upper || C.lower[i] > q.max_lower)
             continue;
         const TgtS tg{q.tgt[1][t], q.tgt[2][t], q.tgt_sin[t], q.tgt_R2[t], q.tgt_2R[t]};
-        double cube[3][3][3];
-        for (int nd_ = 0; nd_ < 3; ++nd_)
-            for (int na = 0; na < 3; ++na) {
-                const int j = (de0 + nd_ - 1) * q.naz + wrap_az(q, az0, na);
-                cube[0][nd_][na] = d2_at(V, j, tg);
-                cube[1][nd_][na] = d2_at(C, j, tg);
-                cube[2][nd_][na] = d2_at(X, j, tg);
-            }
+        /* the 27 distance2 values, one per lane */
+        if (lane < 27) {
+            const int m = lane / 9, nd_ = (lane / 3) % 3, na = lane % 3;
+            const int j = (de0 + nd_ - 1) * q.naz + wrap_az(q, az0, na);
+            const FrontPtrs& F = (m == 0) ? V : (m == 1) ? C : X;
+            s_cube[warp][lane] = d2_at(F, j, tg);
+        }
+        __syncwarp();
         double delta[3] = {q.dt, q.de_inc[de0], q.az_inc[az0]};
         double offset[3], distance[3];
         compute_offsets(q, V, C, X, t, de0, az0, cube, delta, offset, distance);
 
-        double si[MAX_FREQ];
-        B.t = t;
+        /* spreading: lane f holds frequency f (and f + 32) */
+        double si_lo = 0.0, si_hi = 0.0;
         B.spread2 = q.tgt_spread2 + (size_t)t * q.nf;
         if (q.spreading == WQ3D_HYBRID_GAUSSIAN) {
             /* spreading_hybrid_gaussian.cc:65-119 */
@@ -1182,15 +1470,19 @@ __global__ void __launch_bounds__(64) k_eigenray(const QueueDev* __restrict__ qp
                 }
                 no[2] = offset[2] + B.az_inc(a);
             }
+            B.Ilo = B.Ihi = 0.0;
             B.intensity_de(de0, a, no, distance);
+            const double de_lo = B.Ilo, de_hi = B.Ihi;
             no[2] = offset[2];
             int d = de0;
             if (offset[1] < 0.0 && !C.on_edge[i - q.naz]) {
                 d = de0 - 1;
                 no[1] = offset[1] + B.de_inc(d);
             }
+            B.Ilo = B.Ihi = 0.0;
             B.intensity_az(d, az0, no, distance);
-            for (int f = 0; f < q.nf; ++f) si[f] = B.inten_de[f] * B.inten_az[f];
+            si_lo = de_lo * B.Ilo;
+            si_hi = de_hi * B.Ihi;
         } else {
             /* spreading_ray.cc:47-133; an AZ wrap below index 0 is wrapped */
             int d = de0, a = az0;
@@ -1206,81 +1498,82 @@ __global__ void __launch_bounds__(64) k_eigenray(const QueueDev* __restrict__ qp
             if (u > 4.0) zero = true;
             u = fabs(offset[2]) / B.az_inc(a) - 1.0;
             if (u > 4.0) zero = true;
-            for (int f = 0; f < q.nf; ++f) si[f] = zero ? loss * 0.0 : loss;
+            si_lo = si_hi = zero ? loss * 0.0 : loss;
         }
-        bool bad = false;
-        for (int f = 0; f < q.nf; ++f)
-            if (isnan(si[f])) bad = true;
-        if (bad) continue;
-        double inten[MAX_FREQ];
-        for (int f = 0; f < q.nf; ++f) inten[f] = -10.0 * log10(fmax(si[f], 1e-30));
+        const bool has_lo = lane < q.nf, has_hi = lane + 32 < q.nf;
+        const bool bad = (has_lo && isnan(si_lo)) || (has_hi && isnan(si_hi));
+        if (__any_sync(0xffffffffu, bad)) continue;
+        double tl_lo = -10.0 * log10(fmax(si_lo, 1e-30));
+        double tl_hi = -10.0 * log10(fmax(si_hi, 1e-30));
         double ddt = offset[0] / q.dt;
-        if (ddt >= 0.0) {
-            for (int f = 0; f < q.nf; ++f)
-                inten[f] = inten[f] + C.atten[(size_t)f * q.n + i] * (1.0 - ddt) +
-                           X.atten[(size_t)f * q.n + i] * ddt;
-        } else {
-            ddt = 1.0 + ddt;
-            for (int f = 0; f < q.nf; ++f)
-                inten[f] = inten[f] + V.atten[(size_t)f * q.n + i] * (1.0 - ddt) +
-                           C.atten[(size_t)f * q.n + i] * ddt;
-        }
-        bool above = false;
-        for (int f = 0; f < q.nf; ++f)
-            if (inten[f] < q.intensity_threshold) above = true;
-        if (!above) continue;
+        const FrontPtrs& A0 = (ddt >= 0.0) ? C : V;
+        const FrontPtrs& A1 = (ddt >= 0.0) ? X : C;
+        if (ddt < 0.0) ddt = 1.0 + ddt;
+        if (has_lo)
+            tl_lo = tl_lo + A0.atten[(size_t)lane * q.n + i] * (1.0 - ddt) +
+                    A1.atten[(size_t)lane * q.n + i] * ddt;
+        if (has_hi)
+            tl_hi = tl_hi + A0.atten[(size_t)(lane + 32) * q.n + i] * (1.0 - ddt) +
+                    A1.atten[(size_t)(lane + 32) * q.n + i] * ddt;
+        const bool above = (has_lo && tl_lo < q.intensity_threshold) ||
+                           (has_hi && tl_hi < q.intensity_threshold);
+        if (!__any_sync(0xffffffffu, above)) continue;
 
-        /* target D/E and AZ by a 2nd-order Taylor series (wave_queue.cc:620-689) */
-        double tde = 0.0, taz = 0.0;
-        for (int which = 0; which < 2; ++which) {
-            double ang[3][3][3];
-            for (int nd_ = 0; nd_ < 3; ++nd_)
-                for (int na = 0; na < 3; ++na) {
-                    const int j = (de0 + nd_ - 1) * q.naz + wrap_az(q, az0, na);
-                    const FrontPtrs* fs[3] = {&V, &C, &X};
-                    for (int m = 0; m < 3; ++m) {
-                        const double n0 = fs[m]->nd[0][j], n1 = fs[m]->nd[1][j], n2 = fs[m]->nd[2][j];
-                        ang[m][nd_][na] = (which == 0)
-                                              ? atan2(n0, sqrt(n1 * n1 + n2 * n2)) * (180.0 / M_PI)
-                                              : atan2(n2, -n1) * (180.0 / M_PI);
-                    }
-                }
-            double center, g[3], h[3][3], hv[3];
-            make_taylor_coeff(ang, delta, center, g, h);
-            matvec(h, offset, hv);
-            const double val = center + dot3(g, offset) + 0.5 * dot3(offset, hv);
-            if (which == 0)
-                tde = val;
-            else
-                taz = val;
+        /* direction angles of the 27 neighbours on three fronts
+         * (wvector1::direction, types/wvector1.cc) */
+        if (lane < 27) {
+            const int m = lane / 9, nd_ = (lane / 3) % 3, na = lane % 3;
+            const int j = (de0 + nd_ - 1) * q.naz + wrap_az(q, az0, na);
+            const FrontPtrs& F = (m == 0) ? V : (m == 1) ? C : X;
+            const double n0 = F.nd[0][j], n1 = F.nd[1][j], n2 = F.nd[2][j];
+            s_ang[warp][0][lane] = atan2(n0, sqrt(n1 * n1 + n2 * n2)) * (180.0 / M_PI);
+            s_ang[warp][1][lane] = atan2(n2, -n1) * (180.0 / M_PI);
         }
-        const uint32_t slot = atomicAdd(q.n_rec, 1u);
+        __syncwarp();
+        double tang[2];
+        for (int which = 0; which < 2; ++which) {
+            double center, g[3], h[3][3], hv[3];
+            make_taylor_coeff(reinterpret_cast<double (*)[3][3]>(s_ang[warp][which]), delta, center, g, h);
+            matvec(h, offset, hv);
+            tang[which] = center + dot3(g, offset) + 0.5 * dot3(offset, hv);
+        }
+        uint32_t slot = 0;
+        if (lane == 0) slot = atomicAdd(q.n_rec, 1u);
+        slot = __shfl_sync(0xffffffffu, slot, 0);
         if (slot >= q.cap_rec) {
-            set_err(q, ERR_REC_OVERFLOW);
+            if (lane == 0) set_err(q, ERR_REC_OVERFLOW);
+            __syncwarp();
             continue;
         }
-        wq3d_eigenray r;
-        r.time = time + offset[0];
-        r.source_de = q.de[de0] + offset[1];
-        r.source_az = q.az[az0] + offset[2];
-        r.target_de = tde;
-        r.target_az = taz;
-        r.surface = C.surface[i];
-        r.bottom = C.bottom[i];
-        r.caustic = C.caustic[i];
-        r.upper = C.upper[i];
-        r.lower = C.lower[i];
-        r.t1 = t / q.nt2;
-        r.t2 = t % q.nt2;
-        r.de = de0;
-        r.az = az0;
-        r.pad = 0;
-        r.step = s;
-        q.rec[slot] = r;
-        for (int f = 0; f < q.nf; ++f) {
-            q.rec_inten[(size_t)slot * q.nf + f] = inten[f];
-            q.rec_phase[(size_t)slot * q.nf + f] = C.phase[(size_t)f * q.n + i];
+        if (lane == 0) {
+            wq3d_eigenray r;
+            r.time = time + offset[0];
+            r.source_de = q.de[de0] + offset[1];
+            r.source_az = q.az[az0] + offset[2];
+            r.target_de = tang[0];
+            r.target_az = tang[1];
+            r.surface = C.surface[i];
+            r.bottom = C.bottom[i];
+            r.caustic = C.caustic[i];
+            r.upper = C.upper[i];
+            r.lower = C.lower[i];
+            r.t1 = t / q.nt2;
+            r.t2 = t % q.nt2;
+            r.de = de0;
+            r.az = az0;
+            r.pad = 0;
+            r.step = s;
+            q.rec[slot] = r;
         }
+        if (has_lo) {
+            q.rec_inten[(size_t)slot * q.nf + lane] = tl_lo;
+            q.rec_phase[(size_t)slot * q.nf + lane] = C.phase[(size_t)lane * q.n + i];
+        }
+        if (has_hi) {
+            q.rec_inten[(size_t)slot * q.nf + lane + 32] = tl_hi;
+            q.rec_phase[(size_t)slot * q.nf + lane + 32] = C.phase[(size_t)(lane + 32) * q.n + i];
+        }
+        __syncwarp();
     }
 }
 
