@@ -138,6 +138,7 @@ __global__ void k_reflect_loss(BoundaryDev b, int n, const double* grazing,
                                double* ph);
 
 constexpr int CPA_THREADS = 128;     /* rays per CPA block            */
-constexpr int CPA_TARGETS = 64;      /* targets per CPA block (tile)  */
+constexpr int CPA_TARGETS = 64;      /* targets per FP64 CPA block    */
+constexpr int CPA_F32_TARGETS = 256; /* targets per FP32C CPA block   */
 
 }  // namespace wq3d

@@ -742,149 +742,182 @@ __global__ void __launch_bounds__(CPA_THREADS) k_cpa(const QueueDev* __restrict_
 /* ------------------------------------------------------------------ */
 /* CPA search with an FP32 screen (FP32C form)                         */
 /* ------------------------------------------------------------------ */
-/* The two comparisons that reject almost every (ray, target) pair --
- * "next <= curr" and "prev < curr" on distance2 (wave_queue.cc:386-393) --
- * are first decided in FP32 on the algebraically equal form
- *     distance2 = (rho - R)^2 + rho R ((theta - Theta)^2 + sinT sin(theta) (phi - Phi)^2)
- * with every coordinate taken relative to a reference ray of the block, so
- * that all terms are non-negative and small.  A comparison is accepted only
- * when the FP32 difference exceeds a bound on the error of both the FP32
- * value and the reference's own FP64 expression; otherwise the FP64
- * expression decides, exactly as k_cpa does.  Pairs that pass both go
- * through the FP64 is_closest test.  The accepted decisions therefore equal
- * the FP64 decisions, and so does the set of eigenrays.
- *
- * Error bound (u = 2^-24): relative error <= 17 u, plus an absolute term
- * 2u (E_rho^2 + rho R (E_theta^2 + E_phi^2)) from the block-relative
- * coordinates (E = largest offset of a ray of the block from the reference
- * ray), plus the FP64 expression's own rounding, <= 8 * 2^-53 (rho^2 + R^2).
- * The kernel uses 4x / 4x / 8x those figures. */
+/* The comparisons that reject almost every (ray, target) pair -- "next <=
+ * curr" and "prev < curr" on distance2 (wave_queue.cc:386-393) -- are
+ * decided from the sign of a distance2 difference.  With coordinates
+ * relative to a reference ray of the block (r = rho - rho0, x = theta -
+ * theta0, y = phi - phi0; target Rr, X, Y likewise) the reference's
+ * distance2 is, in exact arithmetic,
+ *     Rr^2 + sum_k w_k(target) q_k(ray)
+ *     q = (r^2, r, rho x^2, rho x, rho, rho s y^2, rho s y, rho s)
+ *     w = (1, -2 Rr, R, -2 R X, R X^2, R S, -2 R S Y, R S Y^2)
+ * (s = sin theta, S = sin Theta), so a difference of two fronts is
+ * sum_k w_k dq_k: the per-ray feature differences dq_k are formed once in
+ * FP64, and each pair costs 8 FP32 FMAs per comparison.  A comparison is
+ * accepted in FP32 only when the difference exceeds 32 u sum_k W_k |dq_k|
+ * (W_k = largest |w_k| of the target tile, u = 2^-24; the FP32 evaluation
+ * error is below 12 u of that sum) plus max(1 m^2, 4e-15 (rho^2 + R^2))
+ * for the rounding of the reference's FP64 expression on the two fronts
+ * (each within 5 x 2^-53 (rho^2 + R^2), 0.05 m^2 at earth radius).  The
+ * screen only rejects; every pair it does not reject is queued per warp and
+ * finished in FP64 exactly as k_cpa does, 32 at a time so the lanes stay
+ * converged.  Hence the eigenrays equal the FP64 form's. */
 namespace {
-struct TgtF {
-    float R, T, P, S, Rf;
+constexpr int F32_TARGETS = CPA_F32_TARGETS;
+struct TgtW {
+    float w[8];
 };
+struct WarpQueue {
+    uint32_t e[64];
+};
+
+/* finishes queued pairs in FP64: entry = (lane of the ray << 16) | target */
+__device__ void cpa_finish(const QueueDev& q, const FrontPtrs& V, const FrontPtrs& C,
+                           const FrontPtrs& X, const TgtS* tile, int t0, int ray_base,
+                           const uint32_t* e, int count, int lane) {
+    if (lane >= count) return;
+    const uint32_t v = e[lane];
+    const int j = (int)(v & 0xffffu);
+    const int i = ray_base + (int)(v >> 16);
+    const int de = i / q.naz, az = i % q.naz;
+    const TgtS t = tile[j];
+    const double center = d2_at(C, i, t);
+    if (d2_at(X, i, t) <= center) return;
+    if (d2_at(V, i, t) < center) return;
+    double cube[3][3][3];
+    if (!is_closest(q, V, C, X, t, q.de_branch[t0 + j] != 0, de, az, center, cube)) return;
+    const uint32_t slot = atomicAdd(q.n_cand, 1u);
+    if (slot < q.cap_cand) {
+        q.cand[2 * slot] = (uint32_t)(t0 + j);
+        q.cand[2 * slot + 1] = (uint32_t)i;
+    } else {
+        set_err(q, ERR_CAND_OVERFLOW);
+    }
+}
 }  // namespace
 
 __global__ void __launch_bounds__(CPA_THREADS) k_cpa_f32(const QueueDev* __restrict__ qp, int k) {
     const QueueDev& q = *qp;
-    __shared__ TgtS tile[CPA_TARGETS];
-    __shared__ TgtF tf[CPA_TARGETS];
-    __shared__ float red[4][CPA_THREADS / 32];
+    __shared__ TgtS tile[F32_TARGETS];
+    __shared__ TgtW tw[F32_TARGETS];
+    __shared__ float wmax[CPA_THREADS / 32][8];
+    __shared__ WarpQueue wq[CPA_THREADS / 32];
     const int64_t s = *q.d_base + k + 1;
     const FrontPtrs& V = q.F[(s + 1) & 3];
     const FrontPtrs& C = q.F[(s + 2) & 3];
     const FrontPtrs& X = q.F[(s + 3) & 3];
-    const int t0 = blockIdx.y * CPA_TARGETS;
-    const int nt_tile = min(CPA_TARGETS, q.nt - t0);
-    const int i_ref = min((int)(blockIdx.x * blockDim.x), q.n - 1);
-    const double rho_ref = C.cpa[0][i_ref], th_ref = C.cpa[1][i_ref], ph_ref = C.cpa[2][i_ref];
-    float Rmax = 0.0f;
+    const int t0 = blockIdx.y * F32_TARGETS;
+    const int nt_tile = min(F32_TARGETS, q.nt - t0);
+    const int ray_base = blockIdx.x * blockDim.x;
+    const int i_ref = min(ray_base, q.n - 1);
+    const double rho0 = C.cpa[0][i_ref], th0 = C.cpa[1][i_ref], ph0 = C.cpa[2][i_ref];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float W[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
         const int t = t0 + j;
-        const double R = q.tgt[0][t], T = q.tgt[1][t], P = q.tgt[2][t];
-        tile[j] = TgtS{T, P, q.tgt_sin[t], q.tgt_R2[t], q.tgt_2R[t]};
-        tf[j] = TgtF{(float)(R - rho_ref), (float)(T - th_ref), (float)(P - ph_ref),
-                     (float)q.tgt_sin[t], (float)R};
-        Rmax = fmaxf(Rmax, (float)R);
-    }
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ic = min(i, q.n - 1);
-    /* block-relative coordinates of this ray on the three fronts */
-    float r32[3], t32[3], p32[3], s32[3], k32[3];
-    float Er = 0.0f, Et = 0.0f, Ep = 0.0f, rmax = 0.0f;
-    const FrontPtrs* fr[3] = {&V, &C, &X};
+        const double R = q.tgt[0][t], T = q.tgt[1][t], P = q.tgt[2][t], S = q.tgt_sin[t];
+        tile[j] = TgtS{T, P, S, q.tgt_R2[t], q.tgt_2R[t]};
+        const double Rr = R - rho0, Xo = T - th0, Yo = P - ph0, RS = R * S;
+        TgtW g;
+        g.w[0] = 1.0f;
+        g.w[1] = (float)(-2.0 * Rr);
+        g.w[2] = (float)R;
+        g.w[3] = (float)(-2.0 * R * Xo);
+        g.w[4] = (float)(R * Xo * Xo);
+        g.w[5] = (float)RS;
+        g.w[6] = (float)(-2.0 * RS * Yo);
+        g.w[7] = (float)(RS * Yo * Yo);
+        tw[j] = g;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        const double rho = fr[m]->cpa[0][ic], th = fr[m]->cpa[1][ic], ph = fr[m]->cpa[2][ic];
-        r32[m] = (float)(rho - rho_ref);
-        t32[m] = (float)(th - th_ref);
-        p32[m] = (float)(ph - ph_ref);
-        s32[m] = (float)fr[m]->cpa[3][ic];
-        k32[m] = (float)rho;
-        Er = fmaxf(Er, fabsf(r32[m]));
-        Et = fmaxf(Et, fabsf(t32[m]));
-        Ep = fmaxf(Ep, fabsf(p32[m]));
-        rmax = fmaxf(rmax, k32[m]);
+        for (int m = 0; m < 8; ++m) W[m] = fmaxf(W[m], fabsf(g.w[m]));
     }
-    /* block maxima */
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        Er = fmaxf(Er, __shfl_xor_sync(0xffffffffu, Er, o));
-        Et = fmaxf(Et, __shfl_xor_sync(0xffffffffu, Et, o));
-        Ep = fmaxf(Ep, __shfl_xor_sync(0xffffffffu, Ep, o));
-        rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-        Rmax = fmaxf(Rmax, __shfl_xor_sync(0xffffffffu, Rmax, o));
+    for (int m = 0; m < 8; ++m) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) W[m] = fmaxf(W[m], __shfl_xor_sync(0xffffffffu, W[m], o));
     }
-    if (l == 0) {
-        red[0][w] = Er;
-        red[1][w] = fmaxf(Et, Ep);
-        red[2][w] = rmax;
-        red[3][w] = Rmax;
-    }
+    if (lane == 0)
+        for (int m = 0; m < 8; ++m) wmax[w][m] = W[m];
     __syncthreads();
-    float bEr = 0.0f, bEa = 0.0f, brm = 0.0f, bRm = 0.0f;
 #pragma unroll
-    for (int j = 0; j < CPA_THREADS / 32; ++j) {
-        bEr = fmaxf(bEr, red[0][j]);
-        bEa = fmaxf(bEa, red[1][j]);
-        brm = fmaxf(brm, red[2][j]);
-        bRm = fmaxf(bRm, red[3][j]);
+    for (int m = 0; m < 8; ++m) {
+        float v = 0.0f;
+        for (int j = 0; j < CPA_THREADS / 32; ++j) v = fmaxf(v, wmax[j][m]);
+        W[m] = v * 1.0001f;
     }
-    const float u = 5.9604645e-8f;
-    const float c_rel = 4.0f * 17.0f * u;
-    const float Kmax = brm * bRm * 1.0001f;
-    const float c_abs = 4.0f * 2.0f * u * (bEr * bEr + Kmax * 2.0f * bEa * bEa) +
-                        8.0f * 8.0f * 1.1102230e-16f * (brm * brm + bRm * bRm) + 1e-3f;
 
-    if (i >= q.n) return;
-    if (q.nde < 3 || q.naz < 3) return;
-    const int de = i / q.naz, az = i % q.naz;
-    const int az_start = q.az_boundary ? 0 : 1;
-    if (de < 1 || de >= q.nde - 1 || az < az_start || az >= q.naz - 1) return;
-    if (C.on_edge[i]) return;
-    for (int j = 0; j < nt_tile; ++j) {
-        const TgtF g = tf[j];
-        float d32[3];
+    /* this thread's ray: feature differences next-curr and prev-curr */
+    const int i = ray_base + threadIdx.x;
+    bool active = i < q.n && q.nde >= 3 && q.naz >= 3;
+    if (active) {
+        const int de = i / q.naz, az = i % q.naz;
+        const int az_start = q.az_boundary ? 0 : 1;
+        active = !(de < 1 || de >= q.nde - 1 || az < az_start || az >= q.naz - 1) && !C.on_edge[i];
+    }
+    float dxc[8], dvc[8];
+    float gxc = 0.0f, gvc = 0.0f;
+    {
+        const int ic = min(i, q.n - 1);
+        double fq[3][8];
+        const FrontPtrs* fr[3] = {&V, &C, &X};
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            const float dr = r32[m] - g.R;
-            const float x = t32[m] - g.T;
-            const float y = p32[m] - g.P;
-            const float e = fmaf(x, x, (s32[m] * g.S) * (y * y));
-            d32[m] = fmaf(dr, dr, (k32[m] * g.Rf) * e);
+            const double rho = fr[m]->cpa[0][ic], sn = fr[m]->cpa[3][ic];
+            const double r = rho - rho0, x = fr[m]->cpa[1][ic] - th0, y = fr[m]->cpa[2][ic] - ph0;
+            const double rs = rho * sn;
+            fq[m][0] = r * r;
+            fq[m][1] = r;
+            fq[m][2] = rho * x * x;
+            fq[m][3] = rho * x;
+            fq[m][4] = rho;
+            fq[m][5] = rs * y * y;
+            fq[m][6] = rs * y;
+            fq[m][7] = rs;
         }
-        /* next <= curr ? */
-        const float gX = fmaf(c_rel, d32[2] + d32[1], 2.0f * c_abs);
-        const float dXC = d32[2] - d32[1];
-        double center = 0.0;
-        bool have_center = false;
-        if (dXC < -gX) continue;
-        if (!(dXC > gX)) {
-            const TgtS t = tile[j];
-            center = d2_at(C, i, t);
-            have_center = true;
-            if (d2_at(X, i, t) <= center) continue;
+        const float u = 5.9604645e-8f;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            dxc[m] = (float)(fq[2][m] - fq[1][m]);
+            dvc[m] = (float)(fq[0][m] - fq[1][m]);
+            gxc = fmaf(W[m], fabsf(dxc[m]), gxc);
+            gvc = fmaf(W[m], fabsf(dvc[m]), gvc);
         }
-        /* prev < curr ? */
-        const float gV = fmaf(c_rel, d32[0] + d32[1], 2.0f * c_abs);
-        const float dVC = d32[0] - d32[1];
-        if (dVC < -gV) continue;
-        const TgtS t = tile[j];
-        if (!have_center) center = d2_at(C, i, t);
-        if (!(dVC > gV)) {
-            if (d2_at(V, i, t) < center) continue;
+        /* rounding of the reference's FP64 expression on both fronts */
+        const float r0 = (float)rho0;
+        const float c0 = fmaxf(1.0f, 4.0e-15f * (r0 * r0 + W[2] * W[2]));
+        gxc = fmaf(32.0f * u, gxc, c0);
+        gvc = fmaf(32.0f * u, gvc, c0);
+    }
+    uint32_t* myq = wq[w].e;
+    int qn = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int j = 0; j < nt_tile; ++j) {
+        const TgtW g = tw[j];
+        float a = dxc[0];
+#pragma unroll
+        for (int m = 1; m < 8; ++m) a = fmaf(g.w[m], dxc[m], a);
+        bool want = active && !(a < -gxc);
+        if (want) {
+            float b = dvc[0];
+#pragma unroll
+            for (int m = 1; m < 8; ++m) b = fmaf(g.w[m], dvc[m], b);
+            want = !(b < -gvc);
         }
-        double cube[3][3][3];
-        if (!is_closest(q, V, C, X, t, q.de_branch[t0 + j] != 0, de, az, center, cube)) continue;
-        const uint32_t slot = atomicAdd(q.n_cand, 1u);
-        if (slot < q.cap_cand) {
-            q.cand[2 * slot] = (uint32_t)(t0 + j);
-            q.cand[2 * slot + 1] = (uint32_t)i;
-        } else {
-            set_err(q, ERR_CAND_OVERFLOW);
+        const unsigned mask = __ballot_sync(0xffffffffu, want);
+        if (mask) {
+            if (want) myq[qn + __popc(mask & lt)] = ((uint32_t)(w * 32 + lane) << 16) | (uint32_t)j;
+            qn += __popc(mask);
+            __syncwarp();
+            if (qn >= 32) {
+                cpa_finish(q, V, C, X, tile, t0, ray_base, myq, 32, lane);
+                __syncwarp();
+                if (lane < qn - 32) myq[lane] = myq[32 + lane];
+                __syncwarp();
+                qn -= 32;
+            }
         }
     }
+    if (qn > 0) cpa_finish(q, V, C, X, tile, t0, ray_base, myq, qn, lane);
 }
 
 /* ------------------------------------------------------------------ */
