@@ -269,10 +269,10 @@ def engine_arm(args, rank, world, dist):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "fp64_form": {"value": ray_steps / (f64_total / 1000.0), "ms_per_step": f64_total,
-                      "kernel_ms": {"step+edges": f64_step, "cpa": f64_cpa, "eigenray": f64_eig},
+                      "kernel_ms": {"reflect+advance": f64_step, "cpa": f64_cpa, "eigenray": f64_eig},
                       "eigenrays": f64_neig},
         "eigenrays_per_propagation": n_eig / args.steps,
-        "kernel_ms": {"step+edges": step_ms / args.steps, "cpa": cpa_ms / args.steps,
+        "kernel_ms": {"reflect+advance": step_ms / args.steps, "cpa": cpa_ms / args.steps,
                       "eigenray": eig_ms / args.steps},
         "roofline": {"bound": "fp32", "achieved": achieved,
                      "peak": fp32_peak,

@@ -188,9 +188,9 @@ struct wq3d_queue {
         const dim3 grd((n + 127) / 128);
         cudaEvent_t* ev = timing ? &events[5 * k] : nullptr;
         if (ev) cudaEventRecord(ev[0], stream);
-        k_step<<<grd, blk, 0, stream>>>(d_q, k);
+        k_reflect<<<std::max(1, std::min(4 * 148, (n + 63) / 64)), 64, 0, stream>>>(d_q, k);
         if (ev) cudaEventRecord(ev[1], stream);
-        k_edges<<<grd, blk, 0, stream>>>(d_q, k);
+        k_advance<<<grd, blk, 0, stream>>>(d_q, k);
         launches += 2;
         if (h.nt > 0) {
             const dim3 cg((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS);
@@ -691,6 +691,9 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.n_refl = q->d_counts + 1;
     h.err = q->d_counts + 2;
     h.n_cand = q->d_counts + 3;
+    h.n_work[0] = q->d_counts + 4;
+    h.n_work[1] = q->d_counts + 5;
+    if ((rc = q->alloc(&h.work[0], n)) || (rc = q->alloc(&h.work[1], n))) return cleanup(rc);
     h.d_base = q->d_base;
     h.d_times = q->d_times;
     h.want_refl = 0;

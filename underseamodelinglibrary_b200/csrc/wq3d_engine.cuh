@@ -103,6 +103,8 @@ struct QueueDev {
     const int64_t* d_base;   /* steps completed before this chunk          */
     const double* d_times;   /* time after base + k steps, k = 0..K         */
     uint8_t* flag[2];        /* reflection decision for the "next" front    */
+    uint32_t* work[2];       /* rays that reflect at the start of a step     */
+    uint32_t* n_work[2];
     /* eigenray candidates of the current step */
     uint32_t* cand;          /* packed: target index, ray index              */
     uint32_t* n_cand;
@@ -123,8 +125,8 @@ struct QueueDev {
 
 /* kernels (wq3d_kernels.cu) */
 __global__ void k_startup(const QueueDev* q);
-__global__ void k_step(const QueueDev* q, int k);
-__global__ void k_edges(const QueueDev* q, int k);
+__global__ void k_reflect(const QueueDev* q, int k);
+__global__ void k_advance(const QueueDev* q, int k);
 __global__ void k_cpa(const QueueDev* q, int k);
 __global__ void k_cpa_f32(const QueueDev* q, int k);
 __global__ void k_eigenray(const QueueDev* q, int k);

@@ -490,79 +490,119 @@ __global__ void __launch_bounds__(128) k_startup(const QueueDev* __restrict__ qp
         F.lower[i] = 0;
         F.on_edge[i] = 0;
     }
-    q.flag[0][i] = reflect_decision(q, x.pos, c0.nd);
+    const uint8_t f = reflect_decision(q, x.pos, c0.nd);
+    q.flag[0][i] = f;
+    if (f) {
+        const uint32_t slot = atomicAdd(q.n_work[0], 1u);
+        if (slot < (uint32_t)q.n) q.work[0][slot] = (uint32_t)i;
+    }
     (void)a;
 }
 
 /* ------------------------------------------------------------------ */
-/* one step for one ray                                                */
+/* one step: reflecting rays first, then every ray advances            */
 /* ------------------------------------------------------------------ */
-__global__ void __launch_bounds__(128) k_step(const QueueDev* __restrict__ qp, int k) {
+namespace {
+
+/* detect_caustics of the D/E neighbour below (wave_queue.cc:274-292): the
+ * reference runs it for ray (d-1) before ray d is reflected; it only reads
+ * the neighbour when that neighbour does not reflect this step */
+__device__ __forceinline__ void caustic_from_below(const QueueDev& q, const Roles& R, int i,
+                                                   const uint8_t* flag_in) {
+    const int d = i / q.naz;
+    if (d < 1 || flag_in[i - q.naz]) return;
+    const int j = i - q.naz;
+    const double A = R.C->pos[0][i];
+    const double B = R.C->pos[0][j];
+    const double Cc = R.X->pos[0][i];
+    const double D = R.X->pos[0][j];
+    const bool fold = (R.X->surface[i] == R.X->surface[j]) && (R.X->bottom[i] == R.X->bottom[j]);
+    if ((Cc - D) * (A - B) < 0 && fold) {
+        R.X->caustic[i] += 1;
+        for (int f = 0; f < q.nf; ++f) R.X->phase[(size_t)f * q.n + i] -= M_PI_2;
+    }
+}
+
+}  // namespace
+
+/* Reflecting rays of this step (the previous launch listed them): caustic
+ * hand-off, then the surface/bottom reflection chain with re-initialisation
+ * of the ray's four fronts (wave_queue.cc:197-256). */
+__global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp, int k) {
     const QueueDev& q = *qp;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t s = *q.d_base + k;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *q.n_cand = 0;
-    if (i >= q.n) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *q.n_cand = 0;
+        *q.n_work[(s + 1) & 1] = 0;
+    }
+    const uint32_t nwork = min(*q.n_work[s & 1], (uint32_t)q.n);
+    const uint32_t* work = q.work[s & 1];
     const double t_old = q.d_times[k];
     Roles R;
     roles_at(q, s, R);
-    const int d = i / q.naz;
     const uint8_t* flag_in = q.flag[s & 1];
-    uint8_t* flag_out = q.flag[(s + 1) & 1];
-
-    /* detect_caustics of the D/E neighbour below (wave_queue.cc:274-292):
-     * the reference runs it for ray (d-1) before ray d is reflected */
-    if (d >= 1 && !flag_in[i - q.naz]) {
-        const int j = i - q.naz;
-        const double A = R.C->pos[0][i];
-        const double B = R.C->pos[0][j];
-        const double Cc = R.X->pos[0][i];
-        const double D = R.X->pos[0][j];
-        const bool fold = (R.X->surface[i] == R.X->surface[j]) && (R.X->bottom[i] == R.X->bottom[j]);
-        if ((Cc - D) * (A - B) < 0 && fold) {
-            R.X->caustic[i] += 1;
-            for (int f = 0; f < q.nf; ++f) R.X->phase[(size_t)f * q.n + i] -= M_PI_2;
-        }
-    }
-
-    /* detect_reflections for this ray (wave_queue.cc:197-256) */
-    bool reflected = false;
-    int seq = 0;
-    int next_try = -1; /* 0: try bottom next, 1: try surface next */
-    if (R.X->pos[0][i] - q.R > 0.0 && surface_reflection(q, R, i, s + 1, t_old, seq)) {
-        ++seq;
-        inc_count(R, &FrontPtrs::surface, i);
-        reflected = true;
-        next_try = 0;
-    } else {
-        const double depth = boundary_height(q.oc.bot, R.X->pos[1][i], R.X->pos[2][i]) - R.X->pos[0][i];
-        if (depth > 0.0) {
-            bottom_reflection(q, R, i, depth, s + 1, t_old, seq);
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
+        const int i = (int)work[w];
+        caustic_from_below(q, R, i, flag_in);
+        bool reflected = false;
+        int seq = 0;
+        int next_try = -1; /* 0: try bottom next, 1: try surface next */
+        if (R.X->pos[0][i] - q.R > 0.0 && surface_reflection(q, R, i, s + 1, t_old, seq)) {
             ++seq;
-            inc_count(R, &FrontPtrs::bottom, i);
+            inc_count(R, &FrontPtrs::surface, i);
             reflected = true;
-            next_try = 1;
-        }
-    }
-    if (reflected) {
-        int it = 0;
-        for (; it < MAX_BOUNCE; ++it) {
-            if (next_try == 0) {
-                const double depth = boundary_height(q.oc.bot, R.X->pos[1][i], R.X->pos[2][i]) - R.X->pos[0][i];
-                if (!(depth > 0.0)) break;
+            next_try = 0;
+        } else {
+            const double depth = boundary_height(q.oc.bot, R.X->pos[1][i], R.X->pos[2][i]) - R.X->pos[0][i];
+            if (depth > 0.0) {
                 bottom_reflection(q, R, i, depth, s + 1, t_old, seq);
                 ++seq;
                 inc_count(R, &FrontPtrs::bottom, i);
+                reflected = true;
                 next_try = 1;
-            } else {
-                if (!(R.X->pos[0][i] - q.R > 0.0 && surface_reflection(q, R, i, s + 1, t_old, seq))) break;
-                ++seq;
-                inc_count(R, &FrontPtrs::surface, i);
-                next_try = 0;
             }
         }
-        if (it == MAX_BOUNCE) set_err(q, ERR_BOUNCE_LIMIT);
-    } else {
+        if (reflected) {
+            int it = 0;
+            for (; it < MAX_BOUNCE; ++it) {
+                if (next_try == 0) {
+                    const double depth =
+                        boundary_height(q.oc.bot, R.X->pos[1][i], R.X->pos[2][i]) - R.X->pos[0][i];
+                    if (!(depth > 0.0)) break;
+                    bottom_reflection(q, R, i, depth, s + 1, t_old, seq);
+                    ++seq;
+                    inc_count(R, &FrontPtrs::bottom, i);
+                    next_try = 1;
+                } else {
+                    if (!(R.X->pos[0][i] - q.R > 0.0 && surface_reflection(q, R, i, s + 1, t_old, seq))) break;
+                    ++seq;
+                    inc_count(R, &FrontPtrs::surface, i);
+                    next_try = 0;
+                }
+            }
+            if (it == MAX_BOUNCE) set_err(q, ERR_BOUNCE_LIMIT);
+        }
+    }
+}
+
+/* Every ray: caustic hand-off and vertices for rays that did not reflect,
+ * find_edges of the front that becomes "curr" (wave_front.cc:184-216; it
+ * reads positions and directions that are final once k_reflect is done),
+ * the rotation, AB3 and update of the new front (wave_queue.cc:162-183),
+ * and the reflection decision for the next step. */
+__global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp, int k) {
+    const QueueDev& q = *qp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q.n) return;
+    const int64_t s = *q.d_base + k;
+    Roles R;
+    roles_at(q, s, R);
+    const uint8_t* flag_in = q.flag[s & 1];
+    uint8_t* flag_out = q.flag[(s + 1) & 1];
+    const int naz = q.naz;
+    const int d = i / naz;
+    if (!flag_in[i]) {
+        caustic_from_below(q, R, i, flag_in);
         /* detect_vertices (wave_queue.cc:261-269) */
         const double L = R.C->nd[0][i];
         const double Rn = R.X->nd[0][i];
@@ -572,9 +612,29 @@ __global__ void __launch_bounds__(128) k_step(const QueueDev* __restrict__ qp, i
             R.X->lower[i] += 1;
         }
     }
-
-    /* rotate (wave_queue.cc:162-167): past<-prev, prev<-curr, curr<-next,
-     * next<-old past; then AB3 and update (wave_queue.cc:171-183) */
+    /* find_edges on X */
+    {
+        const int max_de = q.nde - 1;
+        const double* rho = R.X->pos[0];
+        const double* ndr = R.X->nd[0];
+        auto extremum = [&](int dd) -> bool {
+            if (dd < 1 || dd > max_de - 1) return false;
+            const int j = i + (dd - d) * naz;
+            const double r0 = rho[j], rp = rho[j + naz], rm = rho[j - naz];
+            return (r0 < rp && r0 < rm) || (r0 > rp && r0 > rm);
+        };
+        bool edge = (d == 0) || (d == max_de) || extremum(d);
+        if (!edge && extremum(d + 1)) {
+            const double n0 = ndr[i + naz];
+            if (fabs(n0 - ndr[i]) > fabs(n0 - ndr[i + 2 * naz])) edge = true;
+        }
+        if (!edge && extremum(d - 1)) {
+            const double n0 = ndr[i - naz];
+            if (!(fabs(n0 - ndr[i - 2 * naz]) > fabs(n0 - ndr[i]))) edge = true;
+        }
+        R.X->on_edge[i] = edge ? 1 : 0;
+    }
+    /* rotate and take the AB3 step */
     RayS y0, y1, y2, y3;
     load_ray(*R.V, i, y0);
     load_ray(*R.C, i, y1);
@@ -587,40 +647,12 @@ __global__ void __launch_bounds__(128) k_step(const QueueDev* __restrict__ qp, i
     R.P->upper[i] = R.X->upper[i];
     R.P->lower[i] = R.X->lower[i];
     R.P->caustic[i] = R.X->caustic[i];
-    flag_out[i] = reflect_decision(q, y3.pos, y2.nd);
-}
-
-/* ------------------------------------------------------------------ */
-/* wave_front::find_edges (wave_front.cc:184-216) on the new "curr"     */
-/* ------------------------------------------------------------------ */
-__global__ void __launch_bounds__(128) k_edges(const QueueDev* __restrict__ qp, int k) {
-    const QueueDev& q = *qp;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= q.n) return;
-    const int64_t s = *q.d_base + k;
-    const FrontPtrs& f = q.F[(s + 3) & 3];
-    const int naz = q.naz;
-    const int d = i / naz;
-    const int max_de = q.nde - 1;
-    const double* rho = f.pos[0];
-    const double* ndr = f.nd[0];
-    auto extremum = [&](int dd) -> bool {
-        if (dd < 1 || dd > max_de - 1) return false;
-        const int j = i + (dd - d) * naz;
-        const double r0 = rho[j], rp = rho[j + naz], rm = rho[j - naz];
-        return (r0 < rp && r0 < rm) || (r0 > rp && r0 > rm);
-    };
-    bool edge = (d == 0) || (d == max_de) || extremum(d);
-    if (!edge && extremum(d + 1)) {
-        /* ray d+1 is an extremum and marks d when |n(d+1)-n(d)| > |n(d+1)-n(d+2)| */
-        const double n0 = ndr[i + naz];
-        if (fabs(n0 - ndr[i]) > fabs(n0 - ndr[i + 2 * naz])) edge = true;
+    const uint8_t f = reflect_decision(q, y3.pos, y2.nd);
+    flag_out[i] = f;
+    if (f) {
+        const uint32_t slot = atomicAdd(q.n_work[(s + 1) & 1], 1u);
+        if (slot < (uint32_t)q.n) q.work[(s + 1) & 1][slot] = (uint32_t)i;
     }
-    if (!edge && extremum(d - 1)) {
-        const double n0 = ndr[i - naz];
-        if (!(fabs(n0 - ndr[i - 2 * naz]) > fabs(n0 - ndr[i]))) edge = true;
-    }
-    f.on_edge[i] = edge ? 1 : 0;
 }
 
 /* ------------------------------------------------------------------ */
