@@ -166,6 +166,26 @@ int wq3d_ocean_reflect_loss(const wq3d_ocean* ocean, int which, size_t n,
                             size_t nf, const double* freq, double* amplitude,
                             double* phase);
 
+/* Largest number of points one wq3d_ocean_sound_speed_noalloc call takes. */
+#define WQ3D_NOALLOC_MAX_POINTS 16384
+
+/* Same evaluation as wq3d_ocean_sound_speed, for callers that cannot
+ * allocate device memory when they need it (for example a processing loop
+ * that reserves its GPU memory up front, or code under a real-time budget
+ * where cudaMalloc's latency and synchronisation are not allowed).  It has
+ * no counterpart in the reference.  The points are staged in one fixed
+ * device array built into the library (7 doubles per point, 0.9 MB per
+ * device, kept until the process exits); nothing is allocated or freed.
+ * n above WQ3D_NOALLOC_MAX_POINTS returns WQ3D_ERR_INVALID.  All calls on a
+ * device share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the
+ * array's address with that device current; make it before any CUDA stream
+ * capture starts. */
+int wq3d_ocean_sound_speed_noalloc(const wq3d_ocean* ocean, double earth_radius,
+                                   size_t n, const double* rho,
+                                   const double* theta, const double* phi,
+                                   double* speed, double* grad);
+
 /* ------------------------------------------------------------------ */
 /* wave queue (replaces waveq3d/wave_queue.h:122-264)                  */
 /* ------------------------------------------------------------------ */

@@ -19,6 +19,7 @@ WQ3D_ERR_TIMEOUT = -5
 WQ3D_ERR_UNSUPPORTED = -6
 WQ3D_ERR_NUMERIC = -7
 WQ3D_ERR_ABORTED = -8
+WQ3D_NOALLOC_MAX_POINTS = 16384
 
 PROFILE_LINEAR, PROFILE_MUNK, PROFILE_CATENARY, PROFILE_N2, PROFILE_GRID = range(5)
 ATTEN_THORP, ATTEN_CONSTANT = 0, 1
@@ -118,6 +119,7 @@ SIGNATURES = {
     "wq3d_ocean_destroy": (C.c_int, [C.c_void_p]),
     "wq3d_ocean_sound_speed": (C.c_int, [C.c_void_p, C.c_double, C.c_size_t, dp, dp, dp, dp, dp]),
     "wq3d_ocean_height": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, dp, dp, dp, dp, dp]),
+    "wq3d_ocean_sound_speed_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_size_t, dp, dp, dp, dp, dp]),
     "wq3d_ocean_reflect_loss": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, dp, dp, dp, dp,
                                           C.c_size_t, dp, dp, dp]),
     "wq3d_queue_create": (C.c_int, [C.c_void_p, C.POINTER(wq3d_queue_desc), C.POINTER(C.c_void_p)]),

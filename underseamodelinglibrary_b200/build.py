@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwq3d.so")
-SOURCES = ["wq3d_api.cu", "wq3d_kernels.cu"]
+SOURCES = ["wq3d_api.cu", "wq3d_kernels.cu", "wq3d_noalloc.cu"]
 HEADERS = ["wq3d_engine.cuh", "wq3d_models.cuh"]
 
 NVCC_FLAGS = [

@@ -345,6 +345,15 @@ struct wq3d_queue {
 extern "C" {
 
 const char* wq3d_last_error_string(void) { return g_err.c_str(); }
+
+/* Internal hooks for the other source files of the library. */
+void wq3d_internal_set_error(const char* msg) { g_err = msg ? msg : ""; }
+
+int wq3d_internal_ocean_model(const wq3d_ocean* ocean, OceanDev* out) {
+    if (!ocean || !out) return WQ3D_ERR_INVALID;
+    *out = ocean->dev;
+    return WQ3D_OK;
+}
 int wq3d_abi_version(void) { return WQ3D_ABI_VERSION; }
 
 int wq3d_device_count(int* count) {
