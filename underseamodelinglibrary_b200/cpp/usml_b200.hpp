@@ -1,0 +1,520 @@
+/*
+ * usml_b200.hpp -- C++ drop-in for USML's WaveQ3D interface, over the C ABI
+ * of include/wq3d.h (header only; link with libwq3d.so).
+ *
+ * The classes keep the reference's names, constructor arguments and call
+ * order (types/seq_*.h, types/wposition*.h, ocean/*.h, waveq3d/wave_queue.h,
+ * eigenrays/eigenray_collection.h), with std::vector in place of Boost
+ * uBLAS.  Engine errors become std::runtime_error / std::invalid_argument,
+ * as the reference throws.
+ */
+#pragma once
+
+#include <cmath>
+#include <complex>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "wq3d.h"
+
+namespace usml_b200 {
+
+inline void check(int rc) {
+    if (rc == WQ3D_OK) return;
+    const std::string msg = wq3d_last_error_string();
+    if (rc == WQ3D_ERR_INVALID) throw std::invalid_argument(msg);
+    throw std::runtime_error("wq3d error " + std::to_string(rc) + ": " + msg);
+}
+
+namespace types {
+
+inline double to_radians(double t) { return t * (M_PI / 180.0); }
+inline double to_degrees(double t) { return t * (180.0 / M_PI); }
+
+/* seq_vector family (types/seq_vector.h, seq_linear.h, seq_log.h,
+ * seq_data.h, seq_rayfan.cc) */
+class seq_vector {
+   public:
+    typedef std::shared_ptr<const seq_vector> csptr;
+    size_t size() const { return _data.size(); }
+    double operator()(size_t i) const { return _data[i]; }
+    double increment(size_t i) const {
+        if (i > _data.size() - 1) i = _data.size() - 1;
+        return _inc[i];
+    }
+    const std::vector<double>& data() const { return _data; }
+    const std::vector<double>& increments() const { return _inc; }
+    virtual ~seq_vector() {}
+
+   protected:
+    std::vector<double> _data, _inc;
+};
+
+class seq_linear : public seq_vector {
+   public:
+    seq_linear(double first, double increment, int size) { init(first, increment, (size_t)size); }
+    seq_linear(double first, double increment, double last) {
+        const size_t n = (increment == 0.0)
+                             ? 1
+                             : (size_t)std::max(1.0, std::floor(1.0 + (last + increment / 10 - first) / increment));
+        init(first, increment, n);
+    }
+
+   private:
+    void init(double first, double inc, size_t n) {
+        _data.resize(n);
+        _inc.assign(n, inc);
+        double v = first;
+        for (size_t k = 0; k < n; ++k) {
+            _data[k] = v;
+            v += inc;
+        }
+    }
+};
+
+class seq_log : public seq_vector {
+   public:
+    seq_log(double first, double increment, int size) { init(first, increment, (size_t)size); }
+    seq_log(double first, double increment, double last) {
+        const size_t n = (increment == 1.0)
+                             ? 1
+                             : (size_t)std::max(1.0, std::floor(1.0 + std::log((last + increment / 10) / first) /
+                                                                          std::log(increment)));
+        init(first, increment, n);
+    }
+
+   private:
+    void init(double first, double inc, size_t n) {
+        _data.resize(n);
+        _inc.assign(n, 0.0);
+        double v = first;
+        for (size_t k = 0; k < n; ++k) {
+            _data[k] = v;
+            v *= inc;
+            if (k > 0) {
+                _inc[k - 1] = _data[k] - _data[k - 1];
+                _inc[k] = _inc[k - 1];
+            }
+        }
+    }
+};
+
+class seq_data : public seq_vector {
+   public:
+    explicit seq_data(const std::vector<double>& v) { init(v); }
+
+   protected:
+    seq_data() {}
+    void init(const std::vector<double>& v) {
+        _data = v;
+        _inc.assign(v.size(), 0.0);
+        if (v.size() < 2) return;
+        double left = v[1] - v[0];
+        _inc[0] = left;
+        for (size_t n = 1; n < v.size(); ++n) {
+            double right = left;
+            if (n < v.size() - 1) {
+                right = v[n + 1] - v[n];
+                if (left * right <= 0) throw std::invalid_argument("series not monotonic");
+            }
+            left = right;
+            _inc[n] = left;
+        }
+    }
+};
+
+class seq_rayfan : public seq_data {
+   public:
+    seq_rayfan(double first = -90.0, double last = 90.0, size_t size = 181, double center = 0.0,
+               double spread = 6.0) {
+        if (first > last) std::swap(first, last);
+        const double a0 = std::atan((first - center) / spread);
+        const double a1 = std::atan((last - center) / spread);
+        const double scale = (a1 - a0) / double(size - 1);
+        std::vector<double> v(size);
+        for (size_t n = 0; n < size; ++n) v[n] = center + std::tan(a0 + scale * (double)n) * spread;
+        init(v);
+    }
+};
+
+/* wposition::earth_radius and compute_earth_radius (types/wposition.cc) */
+struct earth {
+    static double& radius() {
+        static double r = 6371000.0;
+        return r;
+    }
+};
+inline void compute_earth_radius(double latitude) {
+    const double a = 6378137.0, f = 1.0 / 298.257223563, e2 = f * (2.0 - f);
+    const double s = std::sin(to_radians(latitude));
+    const double w = std::sqrt(1.0 - e2 * s * s);
+    earth::radius() = std::sqrt((a * (1 - e2) / (w * w * w)) * (a / w));
+}
+
+class wposition1 {
+   public:
+    wposition1() {}
+    wposition1(double lat, double lng, double alt) {
+        latitude(lat);
+        longitude(lng);
+        altitude(alt);
+    }
+    double rho() const { return _r; }
+    double theta() const { return _t; }
+    double phi() const { return _p; }
+    void rho(double v) { _r = v; }
+    double latitude() const { return 90.0 - to_degrees(_t); }
+    double longitude() const { return to_degrees(_p); }
+    double altitude() const { return _r - earth::radius(); }
+    void latitude(double v) { _t = to_radians(90.0 - v); }
+    void longitude(double v) { _p = to_radians(v); }
+    void altitude(double v) { _r = v + earth::radius(); }
+
+   private:
+    double _r = 0, _t = 0, _p = 0;
+};
+
+class wposition {
+   public:
+    wposition(size_t rows = 1, size_t cols = 1, double lat = 0.0, double lng = 0.0, double alt = 0.0)
+        : _n1(rows), _n2(cols), _v(rows * cols, wposition1(lat, lng, alt)) {}
+    size_t size1() const { return _n1; }
+    size_t size2() const { return _n2; }
+    wposition1& at(size_t r, size_t c) { return _v[r * _n2 + c]; }
+    const wposition1& at(size_t r, size_t c) const { return _v[r * _n2 + c]; }
+    std::vector<double> packed() const {
+        const size_t n = _v.size();
+        std::vector<double> out(3 * n);
+        for (size_t i = 0; i < n; ++i) {
+            out[i] = _v[i].rho();
+            out[n + i] = _v[i].theta();
+            out[2 * n + i] = _v[i].phi();
+        }
+        return out;
+    }
+
+   private:
+    size_t _n1, _n2;
+    std::vector<wposition1> _v;
+};
+
+}  // namespace types
+
+namespace ocean {
+
+struct attenuation_model {
+    typedef std::shared_ptr<const attenuation_model> csptr;
+    int kind = WQ3D_ATTEN_THORP;
+    double coef = 0.0;
+};
+struct attenuation_thorp : attenuation_model {};
+struct attenuation_constant : attenuation_model {
+    explicit attenuation_constant(double c) {
+        kind = WQ3D_ATTEN_CONSTANT;
+        coef = c;
+    }
+};
+
+class profile_model {
+   public:
+    typedef std::shared_ptr<const profile_model> csptr;
+    explicit profile_model(const attenuation_model::csptr& a) : _atten(a) {}
+    void flat_earth(bool f) { _flat = f; }
+    void fill(wq3d_profile_desc* d) const {
+        d->kind = _kind;
+        for (int k = 0; k < 4; ++k) d->p[k] = _p[k];
+        d->flat_earth = _flat ? 1 : 0;
+        d->attenuation = _atten ? _atten->kind : WQ3D_ATTEN_THORP;
+        d->attenuation_coef = _atten ? _atten->coef : 0.0;
+    }
+    virtual ~profile_model() {}
+
+   protected:
+    int _kind = WQ3D_PROFILE_LINEAR;
+    double _p[4] = {0, 0, 0, 0};
+    bool _flat = false;
+    attenuation_model::csptr _atten;
+};
+
+struct profile_linear : profile_model {
+    explicit profile_linear(double c0 = 1500.0, const attenuation_model::csptr& a = nullptr) : profile_model(a) {
+        _p[0] = c0;
+    }
+    profile_linear(double c0, double g0, const attenuation_model::csptr& a = nullptr) : profile_model(a) {
+        _p[0] = c0;
+        _p[1] = g0;
+        _p[3] = g0;
+    }
+    profile_linear(double c0, double g0, double z1, double g1, const attenuation_model::csptr& a = nullptr)
+        : profile_model(a) {
+        _p[0] = c0;
+        _p[1] = g0;
+        _p[2] = z1;
+        _p[3] = g1;
+    }
+};
+
+struct profile_munk : profile_model {
+    explicit profile_munk(double axis_depth = 1300.0, double scale = 1300.0, double axis_speed = 1500.0,
+                          double epsilon = 7.37e-3, const attenuation_model::csptr& a = nullptr)
+        : profile_model(a) {
+        _kind = WQ3D_PROFILE_MUNK;
+        _p[0] = axis_depth;
+        _p[1] = scale;
+        _p[2] = axis_speed;
+        _p[3] = epsilon;
+    }
+};
+
+struct reflect_loss_model {
+    typedef std::shared_ptr<const reflect_loss_model> csptr;
+    wq3d_reflect_loss_desc d{WQ3D_LOSS_DEFAULT, {0, 0, 0, 0, 0}};
+};
+struct reflect_loss_constant : reflect_loss_model {
+    explicit reflect_loss_constant(double amp, double phase = 0.0) { d = {WQ3D_LOSS_CONSTANT, {amp, phase, 0, 0, 0}}; }
+};
+struct reflect_loss_rayleigh : reflect_loss_model {
+    reflect_loss_rayleigh(double density, double speed, double att = 0.0, double shear = 0.0, double satt = 0.0) {
+        d = {WQ3D_LOSS_RAYLEIGH, {density, speed, att, shear, satt}};
+    }
+};
+
+class boundary_model {
+   public:
+    typedef std::shared_ptr<const boundary_model> csptr;
+    virtual void fill(wq3d_boundary_desc* d) const = 0;
+    virtual ~boundary_model() {}
+};
+
+class boundary_flat : public boundary_model {
+   public:
+    explicit boundary_flat(double depth = 0.0, const reflect_loss_model::csptr& loss = nullptr)
+        : _depth(depth), _loss(loss) {}
+    void fill(wq3d_boundary_desc* d) const override {
+        d->kind = WQ3D_BOUNDARY_FLAT;
+        d->depth = _depth;
+        d->loss = _loss ? _loss->d : wq3d_reflect_loss_desc{WQ3D_LOSS_DEFAULT, {0, 0, 0, 0, 0}};
+    }
+
+   private:
+    double _depth;
+    reflect_loss_model::csptr _loss;
+};
+
+class boundary_slope : public boundary_model {
+   public:
+    boundary_slope(const types::wposition1& loc, double depth, double lat_slope, double lng_slope = 0.0,
+                   const reflect_loss_model::csptr& loss = nullptr)
+        : _loc(loc), _depth(depth), _lat(lat_slope), _lng(lng_slope), _loss(loss) {}
+    void fill(wq3d_boundary_desc* d) const override {
+        d->kind = WQ3D_BOUNDARY_SLOPE;
+        d->depth = _depth;
+        d->location[0] = _loc.rho();
+        d->location[1] = _loc.theta();
+        d->location[2] = _loc.phi();
+        d->lat_slope = _lat;
+        d->lng_slope = _lng;
+        d->loss = _loss ? _loss->d : wq3d_reflect_loss_desc{WQ3D_LOSS_DEFAULT, {0, 0, 0, 0, 0}};
+    }
+
+   private:
+    types::wposition1 _loc;
+    double _depth, _lat, _lng;
+    reflect_loss_model::csptr _loss;
+};
+
+/* ocean_model (ocean/ocean_model.h); the device copy is built on first use */
+class ocean_model {
+   public:
+    typedef std::shared_ptr<const ocean_model> csptr;
+    ocean_model(const boundary_model::csptr& surface, const boundary_model::csptr& bottom,
+                const profile_model::csptr& profile)
+        : _radius(types::earth::radius()) {
+        wq3d_ocean_desc d{};
+        d.earth_radius = _radius;
+        profile->fill(&d.profile);
+        surface->fill(&d.surface);
+        bottom->fill(&d.bottom);
+        wq3d_ocean* o = nullptr;
+        check(wq3d_ocean_create(&d, &o));
+        _h.reset(o, [](wq3d_ocean* p) { wq3d_ocean_destroy(p); });
+    }
+    const wq3d_ocean* handle() const { return _h.get(); }
+
+   private:
+    double _radius;
+    std::shared_ptr<wq3d_ocean> _h;
+};
+
+}  // namespace ocean
+
+namespace eigenrays {
+
+/* eigenrays/eigenray_model.h */
+struct eigenray_model {
+    typedef std::shared_ptr<const eigenray_model> csptr;
+    double travel_time = 0, source_de = 0, source_az = 0, target_de = 0, target_az = 0;
+    std::vector<double> intensity, phase;
+    int surface = 0, bottom = 0, caustic = 0, upper = 0, lower = 0;
+};
+
+/* eigenrays/eigenray_listener.h:41-53 */
+class eigenray_listener {
+   public:
+    virtual void add_eigenray(size_t t1, size_t t2, eigenray_model::csptr ray, size_t run_id) = 0;
+    virtual void check_eigenrays(double /*time*/, size_t /*run_id*/) {}
+    virtual ~eigenray_listener() {}
+};
+
+/* eigenrays/eigenray_collection.{h,cc} (add and coherent sum) */
+class eigenray_collection : public eigenray_listener {
+   public:
+    eigenray_collection(const types::seq_vector::csptr& freq, const types::wposition1&,
+                        const types::wposition& targets, size_t = 0, bool coherent = true)
+        : _freq(freq), _n1(targets.size1()), _n2(targets.size2()), _rays(_n1 * _n2), _total(_n1 * _n2),
+          _coherent(coherent) {}
+    void add_eigenray(size_t t1, size_t t2, eigenray_model::csptr ray, size_t) override {
+        _rays[t1 * _n2 + t2].push_back(ray);
+    }
+    const std::vector<eigenray_model::csptr>& eigenrays(size_t t1, size_t t2) const { return _rays[t1 * _n2 + t2]; }
+    const eigenray_model& total(size_t t1, size_t t2) const { return _total[t1 * _n2 + t2]; }
+    void sum_eigenrays() {
+        const double TWO_PI = 2.0 * M_PI;
+        for (size_t t = 0; t < _rays.size(); ++t) {
+            eigenray_model& tot = _total[t];
+            const size_t nf = _freq->size();
+            tot.intensity.assign(nf, 0.0);
+            tot.phase.assign(nf, 0.0);
+            double time = 0, wgt = 0, sde = 0, tde = 0, max_a = 0;
+            for (size_t f = 0; f < nf; ++f) {
+                std::complex<double> ph(0.0, 0.0);
+                for (const auto& r : _rays[t]) {
+                    double a = std::pow(10.0, r->intensity[f] / -20.0);
+                    if (_coherent) {
+                        double p = std::fmod(TWO_PI * (*_freq)(f) * r->travel_time + r->phase[f], TWO_PI);
+                        ph += std::complex<double>(a * std::cos(p), a * std::sin(p));
+                    } else {
+                        ph += a;
+                    }
+                    a *= a;
+                    wgt += a;
+                    time += a * r->travel_time;
+                    sde += a * r->source_de;
+                    tde += a * r->target_de;
+                    if (a > max_a) {
+                        max_a = a;
+                        tot.surface = r->surface;
+                        tot.bottom = r->bottom;
+                        tot.caustic = r->caustic;
+                    }
+                }
+                tot.intensity[f] = -20.0 * std::log10(std::max(1e-15, std::abs(ph)));
+                tot.phase[f] = std::arg(ph);
+            }
+            tot.travel_time = time / wgt;
+            tot.source_de = sde / wgt;
+            tot.target_de = tde / wgt;
+        }
+    }
+
+   private:
+    types::seq_vector::csptr _freq;
+    size_t _n1, _n2;
+    std::vector<std::vector<eigenray_model::csptr>> _rays;
+    std::vector<eigenray_model> _total;
+    bool _coherent;
+};
+
+}  // namespace eigenrays
+
+namespace waveq3d {
+
+/* wave_queue (waveq3d/wave_queue.h:122-264) */
+class wave_queue {
+   public:
+    enum spreading_type { CLASSIC_RAY = WQ3D_CLASSIC_RAY, HYBRID_GAUSSIAN = WQ3D_HYBRID_GAUSSIAN };
+
+    wave_queue(const ocean::ocean_model::csptr& ocean, const types::seq_vector::csptr& freq,
+               const types::wposition1& pos, const types::seq_vector::csptr& de,
+               const types::seq_vector::csptr& az, double time_step, const types::wposition* targets = nullptr,
+               spreading_type type = HYBRID_GAUSSIAN, int precision = WQ3D_FP32C)
+        : _ocean(ocean), _freq(freq) {
+        wq3d_queue_desc d{};
+        d.freq = freq->data().data();
+        d.num_freq = freq->size();
+        d.source[0] = pos.rho();
+        d.source[1] = pos.theta();
+        d.source[2] = pos.phi();
+        d.de = de->data().data();
+        d.de_inc = de->increments().data();
+        d.num_de = de->size();
+        d.az = az->data().data();
+        d.az_inc = az->increments().data();
+        d.num_az = az->size();
+        d.time_step = time_step;
+        std::vector<double> tg;
+        if (targets) {
+            tg = targets->packed();
+            d.targets = tg.data();
+            d.num_targets1 = targets->size1();
+            d.num_targets2 = targets->size2();
+        }
+        d.spreading = type;
+        d.precision = precision;
+        d.earth_radius = types::earth::radius();
+        wq3d_queue* q = nullptr;
+        check(wq3d_queue_create(ocean->handle(), &d, &q));
+        _q.reset(q, [](wq3d_queue* p) { wq3d_queue_destroy(p); });
+    }
+
+    void add_eigenray_listener(eigenrays::eigenray_listener* l) {
+        _listeners.push_back(l);
+        wq3d_callbacks cb{&wave_queue::on_ray, &wave_queue::on_check, nullptr};
+        check(wq3d_queue_set_callbacks(_q.get(), &cb, this));
+    }
+    void step() { check(wq3d_queue_step(_q.get(), 1)); }
+    void run(double time_max) { check(wq3d_queue_run(_q.get(), time_max, nullptr)); }
+    double time() const {
+        double t = 0.0;
+        check(wq3d_queue_time(_q.get(), &t));
+        return t;
+    }
+    void intensity_threshold(double v) {
+        _th.intensity = std::abs(v);
+        check(wq3d_queue_set_thresholds(_q.get(), &_th));
+    }
+
+   private:
+    static void on_ray(void* ctx, size_t t1, size_t t2, const wq3d_eigenray* r, const double* inten,
+                       const double* phase, size_t nf, uint64_t run) {
+        auto* self = static_cast<wave_queue*>(ctx);
+        auto ray = std::make_shared<eigenrays::eigenray_model>();
+        ray->travel_time = r->time;
+        ray->source_de = r->source_de;
+        ray->source_az = r->source_az;
+        ray->target_de = r->target_de;
+        ray->target_az = r->target_az;
+        ray->surface = r->surface;
+        ray->bottom = r->bottom;
+        ray->caustic = r->caustic;
+        ray->upper = r->upper;
+        ray->lower = r->lower;
+        ray->intensity.assign(inten, inten + nf);
+        ray->phase.assign(phase, phase + nf);
+        for (auto* l : self->_listeners) l->add_eigenray(t1, t2, ray, run);
+    }
+    static void on_check(void* ctx, double time, uint64_t run) {
+        for (auto* l : static_cast<wave_queue*>(ctx)->_listeners) l->check_eigenrays(time, run);
+    }
+
+    ocean::ocean_model::csptr _ocean;
+    types::seq_vector::csptr _freq;
+    std::shared_ptr<wq3d_queue> _q;
+    std::vector<eigenrays::eigenray_listener*> _listeners;
+    wq3d_thresholds _th{300.0, 300.0, 999, 999, 999, 999, 999};
+};
+
+}  // namespace waveq3d
+}  // namespace usml_b200

@@ -122,6 +122,8 @@ struct PendingRay {
 struct wq3d_queue {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;
+    std::vector<cudaEvent_t> fork_ev, join_ev;
     QueueDev h{};
     QueueDev* d_q = nullptr;
     std::vector<void*> allocs;
@@ -155,6 +157,9 @@ struct wq3d_queue {
     ~wq3d_queue() {
         if (graph) cudaGraphExecDestroy(graph);
         for (auto e : events) cudaEventDestroy(e);
+        for (auto e : fork_ev) cudaEventDestroy(e);
+        for (auto e : join_ev) cudaEventDestroy(e);
+        if (side) cudaStreamDestroy(side);
         if (ev_begin) cudaEventDestroy(ev_begin);
         if (ev_end) cudaEventDestroy(ev_end);
         for (void* p : allocs) cudaFree(p);
@@ -182,32 +187,47 @@ struct wq3d_queue {
         return WQ3D_OK;
     }
 
-    int launch_step(int k) {
+    /* One chunk of K steps.  Step k's reflections run on the side stream
+     * while step k-1's CPA search and eigenray construction run on the main
+     * stream (k_reflect only reads the fronts and writes shadow slots);
+     * k_advance(k) waits for both. */
+    int launch_chunk(int K) {
         const int n = h.n;
         const dim3 blk(128);
         const dim3 grd((n + 127) / 128);
-        cudaEvent_t* ev = timing ? &events[5 * k] : nullptr;
-        if (ev) cudaEventRecord(ev[0], stream);
-        k_reflect<<<std::max(1, std::min(4 * 148, (n + 63) / 64)), 64, 0, stream>>>(d_q, k);
-        if (ev) cudaEventRecord(ev[1], stream);
-        k_advance<<<grd, blk, 0, stream>>>(d_q, k);
-        launches += 2;
-        if (h.nt > 0) {
-            const dim3 cg((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS);
+        const int rgrid = std::max(1, std::min(4 * 148, (n + 63) / 64));
+        k_reflect<<<rgrid, 64, 0, stream>>>(d_q, 0);
+        launches += 1;
+        for (int k = 0; k < K; ++k) {
+            cudaEvent_t* ev = timing ? &events[5 * k] : nullptr;
+            if (ev) cudaEventRecord(ev[0], stream);
+            k_advance<<<grd, blk, 0, stream>>>(d_q, k);
+            if (ev) cudaEventRecord(ev[1], stream);
+            launches += 1;
+            const bool more = k + 1 < K;
+            if (more) {
+                cudaEventRecord(fork_ev[k], stream);
+                cudaStreamWaitEvent(side, fork_ev[k], 0);
+                k_reflect<<<rgrid, 64, 0, side>>>(d_q, k + 1);
+                cudaEventRecord(join_ev[k], side);
+                launches += 1;
+            }
             if (ev) cudaEventRecord(ev[2], stream);
-            if (h.precision == WQ3D_FP32C)
-                k_cpa_f32<<<dim3(cg.x, (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS), CPA_THREADS, 0,
-                            stream>>>(d_q, k);
-            else
-                k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d_q, k);
-            if (ev) cudaEventRecord(ev[3], stream);
-            k_eigenray<<<148, 128, 0, stream>>>(d_q, k);
+            if (h.nt > 0) {
+                const dim3 cg((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS);
+                if (h.precision == WQ3D_FP32C)
+                    k_cpa_f32<<<dim3(cg.x, (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS), CPA_THREADS, 0,
+                                stream>>>(d_q, k);
+                else
+                    k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d_q, k);
+                if (ev) cudaEventRecord(ev[3], stream);
+                k_eigenray<<<148, 128, 0, stream>>>(d_q, k);
+                launches += 2;
+            } else if (ev) {
+                cudaEventRecord(ev[3], stream);
+            }
             if (ev) cudaEventRecord(ev[4], stream);
-            launches += 2;
-        } else if (ev) {
-            cudaEventRecord(ev[2], stream);
-            cudaEventRecord(ev[3], stream);
-            cudaEventRecord(ev[4], stream);
+            if (more) cudaStreamWaitEvent(stream, join_ev[k], 0);
         }
         return WQ3D_OK;
     }
@@ -223,7 +243,7 @@ struct wq3d_queue {
         const bool save = timing;
         timing = false;
         const int64_t saved_launches = launches;
-        for (int k = 0; k < chunk; ++k) launch_step(k);
+        launch_chunk(chunk);
         launches = saved_launches;
         timing = save;
         if (cudaStreamEndCapture(stream, &g) != cudaSuccess ||
@@ -297,7 +317,7 @@ struct wq3d_queue {
             WQ_CK(cudaGraphLaunch(graph, stream));
             launches += (h.nt > 0 ? 4 : 2) * (int64_t)K;
         } else {
-            for (int k = 0; k < K; ++k) launch_step(k);
+            launch_chunk(K);
         }
         WQ_CK(cudaGetLastError());
         WQ_CK(cudaMemcpyAsync(h_counts, d_counts, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -305,7 +325,7 @@ struct wq3d_queue {
         if (timing) {
             for (int k = 0; k < K; ++k) {
                 float a = 0, b = 0, c = 0;
-                cudaEventElapsedTime(&a, events[5 * k], events[5 * k + 2]);
+                cudaEventElapsedTime(&a, events[5 * k], events[5 * k + 1]);
                 cudaEventElapsedTime(&b, events[5 * k + 2], events[5 * k + 3]);
                 cudaEventElapsedTime(&c, events[5 * k + 3], events[5 * k + 4]);
                 ms_step += a;
@@ -702,6 +722,13 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.n_cand = q->d_counts + 3;
     h.n_work[0] = q->d_counts + 4;
     h.n_work[1] = q->d_counts + 5;
+    h.n_done = q->d_counts + 6;
+    {
+        const size_t stride = 51 + 2 * nf;
+        if ((rc = q->alloc(&h.shadow, n * stride)) || (rc = q->alloc(&h.shadow_cnt, 3 * n)) ||
+            (rc = q->alloc(&h.shadow_slot, n)))
+            return cleanup(rc);
+    }
     if ((rc = q->alloc(&h.work[0], n)) || (rc = q->alloc(&h.work[1], n))) return cleanup(rc);
     h.d_base = q->d_base;
     h.d_times = q->d_times;
@@ -731,6 +758,14 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
     if (cudaEventCreate(&q->ev_begin) != cudaSuccess || cudaEventCreate(&q->ev_end) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+    if (cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
+    q->fork_ev.resize(q->chunk);
+    q->join_ev.resize(q->chunk);
+    for (int k = 0; k < q->chunk; ++k)
+        if (cudaEventCreateWithFlags(&q->fork_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&q->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
+            return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
     q->events.resize(5 * (size_t)q->chunk);
     for (auto& ev : q->events)
         if (cudaEventCreate(&ev) != cudaSuccess) return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));

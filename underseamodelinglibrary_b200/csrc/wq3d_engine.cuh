@@ -105,6 +105,10 @@ struct QueueDev {
     uint8_t* flag[2];        /* reflection decision for the "next" front    */
     uint32_t* work[2];       /* rays that reflect at the start of a step     */
     uint32_t* n_work[2];
+    uint32_t* n_done;        /* finished blocks of k_reflect              */
+    double* shadow;          /* reflected prev/curr/next per worklist slot  */
+    int32_t* shadow_cnt;     /* surface, bottom, caustic per slot           */
+    int32_t* shadow_slot;    /* worklist slot of each reflecting ray        */
     /* eigenray candidates of the current step */
     uint32_t* cand;          /* packed: target index, ray index              */
     uint32_t* n_cand;

@@ -214,12 +214,49 @@ __device__ void collision_location(const QueueDev& q, const FrontPtrs& V,
     }
 }
 
+/* One reflecting ray's prev/curr/next state and next-front losses, held
+ * privately while k_reflect works on it.  The results go to a shadow slot
+ * that k_advance commits, so k_cpa / k_eigenray of the previous step can
+ * read the fronts at the same time.  (The reference also rewrites the
+ * ray's "past" entry, reflection_model.cc:320, but the AB3 step of the
+ * same wave_queue::step overwrites that entry before anything reads it.) */
+struct RayLocal {
+    RayS v, c, x;
+    double att[MAX_FREQ];
+    double ph[MAX_FREQ];
+    int surface, bottom, caustic;
+};
+
+/* collision_location (wave_queue.cc:982-1057) on the private state */
+__device__ void collision_local(const QueueDev& q, const RayLocal& L, double tw, double* pos,
+                                double* nd, double* speed) {
+    const double dt = q.dt;
+    const double time1 = 2.0 * dt;
+    const double time2 = dt * dt;
+    const double dtime2 = tw * tw;
+    const double drho = (L.x.c - L.v.c) / time1;
+    const double d2rho = (L.x.c + L.v.c - 2.0 * L.c.c) / time2;
+    *speed = L.c.c + drho * tw + 0.5 * d2rho * dtime2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double v1 = (L.x.pos[k] - L.v.pos[k]) / time1;
+        const double v2 = (L.x.pos[k] + L.v.pos[k] - 2.0 * L.c.pos[k]) / time2;
+        pos[k] = L.c.pos[k] + v1 * tw + 0.5 * v2 * dtime2;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double v1 = (L.x.nd[k] - L.v.nd[k]) / time1;
+        const double v2 = (L.x.nd[k] + L.v.nd[k] - 2.0 * L.c.nd[k]) / time2;
+        nd[k] = L.c.nd[k] + v1 * tw + 0.5 * v2 * dtime2;
+    }
+}
+
 /* reflection_model::reflection_reinit (reflection_model.cc:248-330).
  * Keeps the reference's past.update() at :315, which leaves "temp" with
- * the derivatives of its first update. */
-__device__ void reflection_reinit(const QueueDev& q, const Roles& R, int i,
-                                  double tw, const double* pos,
-                                  const double* nd) {
+ * the derivatives of its first update.  reflection_copy copies position,
+ * gradients, sound speed and step distance (reflection_model.cc:335-360). */
+__device__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const double* pos,
+                             const double* nd) {
     RayS past1, prev1, curr1, next1, temp;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -238,7 +275,6 @@ __device__ void reflection_reinit(const QueueDev& q, const Roles& R, int i,
     update1(q, past1);
     rk3(-tw, temp, next1, past1, curr1);
     update1(q, curr1);
-    copy_ray(*R.C, i, curr1);
 
     const double h = q.dt;
     rk1(-h, curr1, next1);
@@ -247,18 +283,18 @@ __device__ void reflection_reinit(const QueueDev& q, const Roles& R, int i,
     update1(q, past1);
     rk3(-h, curr1, next1, past1, prev1);
     update1(q, prev1);
-    copy_ray(*R.V, i, prev1);
 
     rk1(-h, prev1, next1);
     update1(q, next1);
     rk2(-h, prev1, next1, temp);
     rk3(-h, prev1, next1, temp, past1);
     update1(q, past1);
-    copy_ray(*R.P, i, past1);
 
     ab3(h, past1, prev1, curr1, next1);
     update1(q, next1);
-    copy_ray(*R.X, i, next1);
+    L.c = curr1;
+    L.v = prev1;
+    L.x = next1;
 }
 
 __device__ void record_reflection(const QueueDev& q, int64_t step, double t_old,
@@ -289,46 +325,44 @@ __device__ void record_reflection(const QueueDev& q, int64_t step, double t_old,
 }
 
 /* reflection_model::surface_reflection (reflection_model.cc:187-243) */
-__device__ bool surface_reflection(const QueueDev& q, const Roles& R, int i,
-                                   int64_t step, double t_old, int seq) {
-    double c = R.C->c[i];
-    const double d = c * c * R.C->nd[0][i];
-    const double tw = (d == 0.0) ? 0.0 : -(R.C->pos[0][i] - q.R) / d;
+__device__ bool surface_local(const QueueDev& q, RayLocal& L, int i, int64_t step, double t_old,
+                              int seq) {
+    double c = L.c.c;
+    const double d = c * c * L.c.nd[0];
+    const double tw = (d == 0.0) ? 0.0 : -(L.c.pos[0] - q.R) / d;
     double pos[3], nd[3];
-    collision_location(q, *R.V, *R.C, *R.X, i, tw, pos, nd, &c);
-    const double n1 = R.C->nd[1][i], n2 = R.C->nd[2][i];
-    const double grazing = atan2(R.C->nd[0][i], sqrt(n1 * n1 + n2 * n2));
+    collision_local(q, L, tw, pos, nd, &c);
+    const double n1 = L.c.nd[1], n2 = L.c.nd[2];
+    const double grazing = atan2(L.c.nd[0], sqrt(n1 * n1 + n2 * n2));
     if (grazing <= 0.0) return false;
     record_reflection(q, step, t_old, i, tw, grazing, c, pos, nd, 1, seq);
-    const LossDev& L = q.oc.surf.loss;
-    double amp0, ph0;
-    if (L.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(L, grazing, &amp0, &ph0);
-    const double w2 = L.p[0] * L.p[0];
+    const LossDev& Lo = q.oc.surf.loss;
+    double amp0 = 0.0, ph0 = 0.0;
+    if (Lo.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(Lo, grazing, &amp0, &ph0);
+    const double w2 = Lo.p[0] * Lo.p[0];
     const double sg = sin(grazing);
     for (int k = 0; k < q.nf; ++k) {
         double a = amp0;
-        if (L.kind == WQ3D_LOSS_ECKART) {
+        if (Lo.kind == WQ3D_LOSS_ECKART) {
             const double x = q.freq[k] * w2 * sg;
             a = 8.6e-9 * (x * x);
         }
-        const size_t o = (size_t)k * q.n + i;
-        R.X->atten[o] += a;
-        R.X->phase[o] -= M_PI;
+        L.att[k] += a;
+        L.ph[k] -= M_PI;
     }
     nd[0] = -nd[0];
-    reflection_reinit(q, R, i, tw, pos, nd);
+    reinit_local(q, L, tw, pos, nd);
     return true;
 }
 
 /* reflection_model::bottom_reflection (reflection_model.cc:33-182) */
-__device__ void bottom_reflection(const QueueDev& q, const Roles& R, int i,
-                                  double depth, int64_t step, double t_old,
-                                  int seq) {
+__device__ void bottom_local(const QueueDev& q, RayLocal& L, int i, double depth, int64_t step,
+                             double t_old, int seq) {
     const BoundaryDev& B = q.oc.bot;
     bool shallow = false;
-    double position[3] = {R.C->pos[0][i], R.C->pos[1][i], R.C->pos[2][i]};
-    double ndir[3] = {R.C->nd[0][i], R.C->nd[1][i], R.C->nd[2][i]};
-    double c = R.C->c[i];
+    double position[3] = {L.c.pos[0], L.c.pos[1], L.c.pos[2]};
+    double ndir[3] = {L.c.nd[0], L.c.nd[1], L.c.nd[2]};
+    double c = L.c.c;
     double c2 = c * c;
     double nrm[3] = {B.normal[0], B.normal[1], B.normal[2]};
     double bottom_rho = boundary_height(B, position[1], position[2]);
@@ -352,7 +386,7 @@ __device__ void bottom_reflection(const QueueDev& q, const Roles& R, int i,
     const double dot_water = -height_water * nrm[0];
     const double time_water = fmax(0.0, dot_water / dot_full);
 
-    collision_location(q, *R.V, *R.C, *R.X, i, time_water, position, ndir, &c);
+    collision_local(q, L, time_water, position, ndir, &c);
     bottom_rho = boundary_height(B, position[1], position[2]);
     nrm[0] = B.normal[0];
     nrm[1] = B.normal[1];
@@ -382,21 +416,20 @@ __device__ void bottom_reflection(const QueueDev& q, const Roles& R, int i,
     }
     record_reflection(q, step, t_old, i, time_water, grazing, c, position, ndir, 0, seq);
 
-    const LossDev& L = B.loss;
+    const LossDev& Lo = B.loss;
     double amp0 = 0.0, ph0 = 0.0;
-    if (L.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(L, grazing, &amp0, &ph0);
-    const double w2 = L.p[0] * L.p[0];
+    if (Lo.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(Lo, grazing, &amp0, &ph0);
+    const double w2 = Lo.p[0] * Lo.p[0];
     const double sgz = sin(grazing);
     for (int k = 0; k < q.nf; ++k) {
         double a = amp0, p = ph0;
-        if (L.kind == WQ3D_LOSS_ECKART) {
+        if (Lo.kind == WQ3D_LOSS_ECKART) {
             const double x = q.freq[k] * w2 * sgz;
             a = 8.6e-9 * (x * x);
             p = M_PI;
         }
-        const size_t o = (size_t)k * q.n + i;
-        R.X->atten[o] += a;
-        R.X->phase[o] += p;
+        L.att[k] += a;
+        L.ph[k] += p;
     }
     dot_full *= 2.0;
     ndir[0] = ndir[0] - dot_full * nrm[0];
@@ -406,7 +439,7 @@ __device__ void bottom_reflection(const QueueDev& q, const Roles& R, int i,
     ndir[0] = ndir[0] / N;
     ndir[1] = ndir[1] / N;
     ndir[2] = ndir[2] / N;
-    reflection_reinit(q, R, i, time_water, position, ndir);
+    reinit_local(q, L, time_water, position, ndir);
 }
 
 /* whether the "next" ray reflects at the start of the following step:
@@ -423,12 +456,32 @@ __device__ __forceinline__ uint8_t reflect_decision(const QueueDev& q,
     return (h - xpos[0] > 0.0) ? 1 : 0;
 }
 
-__device__ __forceinline__ void inc_count(const Roles& R, int32_t* FrontPtrs::*field, int i) {
-    const int32_t v = (R.X->*field)[i] + 1;
-    (R.X->*field)[i] = v;
-    (R.C->*field)[i] = v;
-    (R.V->*field)[i] = v;
-    (R.P->*field)[i] = v;
+/* shadow slot of a reflecting ray: prev, curr, next (17 doubles each), the
+ * next front's attenuation and phase (nf each); counts in shadow_cnt */
+__device__ __forceinline__ size_t shadow_stride(const QueueDev& q) { return 51 + 2 * (size_t)q.nf; }
+
+__device__ __forceinline__ void ray_to(double* dst, const RayS& y) {
+    for (int k = 0; k < 3; ++k) {
+        dst[k] = y.pos[k];
+        dst[3 + k] = y.pg[k];
+        dst[6 + k] = y.nd[k];
+        dst[9 + k] = y.ng[k];
+        dst[13 + k] = y.sg[k];
+    }
+    dst[12] = y.c;
+    dst[16] = y.dist;
+}
+
+__device__ __forceinline__ void ray_from(const double* src, RayS& y) {
+    for (int k = 0; k < 3; ++k) {
+        y.pos[k] = src[k];
+        y.pg[k] = src[3 + k];
+        y.nd[k] = src[6 + k];
+        y.ng[k] = src[9 + k];
+        y.sg[k] = src[13 + k];
+    }
+    y.c = src[12];
+    y.dist = src[16];
 }
 
 }  // namespace
@@ -500,64 +553,67 @@ __global__ void __launch_bounds__(128) k_startup(const QueueDev* __restrict__ qp
 }
 
 /* ------------------------------------------------------------------ */
-/* one step: reflecting rays first, then every ray advances            */
+/* one step: reflections (overlapping the previous step's CPA work),   */
+/* then every ray advances                                             */
 /* ------------------------------------------------------------------ */
-namespace {
 
-/* detect_caustics of the D/E neighbour below (wave_queue.cc:274-292): the
- * reference runs it for ray (d-1) before ray d is reflected; it only reads
- * the neighbour when that neighbour does not reflect this step */
-__device__ __forceinline__ void caustic_from_below(const QueueDev& q, const Roles& R, int i,
-                                                   const uint8_t* flag_in) {
-    const int d = i / q.naz;
-    if (d < 1 || flag_in[i - q.naz]) return;
-    const int j = i - q.naz;
-    const double A = R.C->pos[0][i];
-    const double B = R.C->pos[0][j];
-    const double Cc = R.X->pos[0][i];
-    const double D = R.X->pos[0][j];
-    const bool fold = (R.X->surface[i] == R.X->surface[j]) && (R.X->bottom[i] == R.X->bottom[j]);
-    if ((Cc - D) * (A - B) < 0 && fold) {
-        R.X->caustic[i] += 1;
-        for (int f = 0; f < q.nf; ++f) R.X->phase[(size_t)f * q.n + i] -= M_PI_2;
-    }
-}
-
-}  // namespace
-
-/* Reflecting rays of this step (the previous launch listed them): caustic
- * hand-off, then the surface/bottom reflection chain with re-initialisation
- * of the ray's four fronts (wave_queue.cc:197-256). */
+/* Reflecting rays of step s (listed by the launch that produced the
+ * "next" front): caustic hand-off from the D/E neighbour below, then the
+ * surface/bottom reflection chain (wave_queue.cc:197-256) on a private
+ * copy of the ray.  The result goes to the ray's shadow slot; k_advance
+ * commits it.  The fronts are only read here, so this kernel runs
+ * concurrently with k_cpa / k_eigenray of step s-1. */
 __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp, int k) {
     const QueueDev& q = *qp;
     const int64_t s = *q.d_base + k;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        *q.n_cand = 0;
-        *q.n_work[(s + 1) & 1] = 0;
-    }
     const uint32_t nwork = min(*q.n_work[s & 1], (uint32_t)q.n);
     const uint32_t* work = q.work[s & 1];
     const double t_old = q.d_times[k];
     Roles R;
     roles_at(q, s, R);
     const uint8_t* flag_in = q.flag[s & 1];
+    const size_t stride = shadow_stride(q);
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
         const int i = (int)work[w];
-        caustic_from_below(q, R, i, flag_in);
+        RayLocal L;
+        load_ray(*R.V, i, L.v);
+        load_ray(*R.C, i, L.c);
+        load_ray(*R.X, i, L.x);
+        for (int f = 0; f < q.nf; ++f) {
+            L.att[f] = R.X->atten[(size_t)f * q.n + i];
+            L.ph[f] = R.X->phase[(size_t)f * q.n + i];
+        }
+        L.surface = R.X->surface[i];
+        L.bottom = R.X->bottom[i];
+        L.caustic = R.X->caustic[i];
+        /* detect_caustics of the neighbour below (wave_queue.cc:274-292),
+         * which the reference runs before this ray reflects; that
+         * neighbour is read only when it does not reflect */
+        const int d = i / q.naz;
+        if (d >= 1 && !flag_in[i - q.naz]) {
+            const int j = i - q.naz;
+            const double A = L.c.pos[0], B = R.C->pos[0][j];
+            const double Cc = L.x.pos[0], D = R.X->pos[0][j];
+            const bool fold = (L.surface == R.X->surface[j]) && (L.bottom == R.X->bottom[j]);
+            if ((Cc - D) * (A - B) < 0 && fold) {
+                L.caustic += 1;
+                for (int f = 0; f < q.nf; ++f) L.ph[f] -= M_PI_2;
+            }
+        }
         bool reflected = false;
         int seq = 0;
         int next_try = -1; /* 0: try bottom next, 1: try surface next */
-        if (R.X->pos[0][i] - q.R > 0.0 && surface_reflection(q, R, i, s + 1, t_old, seq)) {
+        if (L.x.pos[0] - q.R > 0.0 && surface_local(q, L, i, s + 1, t_old, seq)) {
             ++seq;
-            inc_count(R, &FrontPtrs::surface, i);
+            L.surface += 1;
             reflected = true;
             next_try = 0;
         } else {
-            const double depth = boundary_height(q.oc.bot, R.X->pos[1][i], R.X->pos[2][i]) - R.X->pos[0][i];
+            const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
             if (depth > 0.0) {
-                bottom_reflection(q, R, i, depth, s + 1, t_old, seq);
+                bottom_local(q, L, i, depth, s + 1, t_old, seq);
                 ++seq;
-                inc_count(R, &FrontPtrs::bottom, i);
+                L.bottom += 1;
                 reflected = true;
                 next_try = 1;
             }
@@ -566,33 +622,57 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
             int it = 0;
             for (; it < MAX_BOUNCE; ++it) {
                 if (next_try == 0) {
-                    const double depth =
-                        boundary_height(q.oc.bot, R.X->pos[1][i], R.X->pos[2][i]) - R.X->pos[0][i];
+                    const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
                     if (!(depth > 0.0)) break;
-                    bottom_reflection(q, R, i, depth, s + 1, t_old, seq);
+                    bottom_local(q, L, i, depth, s + 1, t_old, seq);
                     ++seq;
-                    inc_count(R, &FrontPtrs::bottom, i);
+                    L.bottom += 1;
                     next_try = 1;
                 } else {
-                    if (!(R.X->pos[0][i] - q.R > 0.0 && surface_reflection(q, R, i, s + 1, t_old, seq))) break;
+                    if (!(L.x.pos[0] - q.R > 0.0 && surface_local(q, L, i, s + 1, t_old, seq))) break;
                     ++seq;
-                    inc_count(R, &FrontPtrs::surface, i);
+                    L.surface += 1;
                     next_try = 0;
                 }
             }
             if (it == MAX_BOUNCE) set_err(q, ERR_BOUNCE_LIMIT);
         }
+        double* sh = q.shadow + (size_t)w * stride;
+        ray_to(sh, L.v);
+        ray_to(sh + 17, L.c);
+        ray_to(sh + 34, L.x);
+        for (int f = 0; f < q.nf; ++f) {
+            sh[51 + f] = L.att[f];
+            sh[51 + q.nf + f] = L.ph[f];
+        }
+        q.shadow_cnt[3 * (size_t)w] = L.surface;
+        q.shadow_cnt[3 * (size_t)w + 1] = L.bottom;
+        q.shadow_cnt[3 * (size_t)w + 2] = L.caustic;
+        q.shadow_slot[i] = (int32_t)w;
+    }
+    /* the last block to finish empties this step's worklist, which the
+     * advance of step s+1 refills (every block has read the count by then;
+     * the advance of step s fills the other list) */
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t prev = atomicAdd(q.n_done, 1u);
+        if (prev == gridDim.x - 1) {
+            *q.n_work[s & 1] = 0;
+            *q.n_done = 0;
+        }
     }
 }
 
-/* Every ray: caustic hand-off and vertices for rays that did not reflect,
- * find_edges of the front that becomes "curr" (wave_front.cc:184-216; it
- * reads positions and directions that are final once k_reflect is done),
- * the rotation, AB3 and update of the new front (wave_queue.cc:162-183),
- * and the reflection decision for the next step. */
+/* Every ray: commit of a reflected ray's shadow slot, caustic hand-off and
+ * vertices for rays that did not reflect, find_edges of the front that
+ * becomes "curr" (wave_front.cc:184-216; reflecting neighbours are read
+ * from their shadow slots), the rotation, AB3 and update of the new front
+ * (wave_queue.cc:162-183), and the reflection decision of the next step. */
 __global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp, int k) {
     const QueueDev& q = *qp;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *q.n_cand = 0;
     if (i >= q.n) return;
     const int64_t s = *q.d_base + k;
     Roles R;
@@ -601,44 +681,77 @@ __global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp
     uint8_t* flag_out = q.flag[(s + 1) & 1];
     const int naz = q.naz;
     const int d = i / naz;
-    if (!flag_in[i]) {
-        caustic_from_below(q, R, i, flag_in);
+    const size_t stride = shadow_stride(q);
+    RayS y0, y1, y2, y3;
+    if (flag_in[i]) {
+        /* commit the reflected ray (reflection_copy into prev, curr, next) */
+        const int32_t w = q.shadow_slot[i];
+        const double* sh = q.shadow + (size_t)w * stride;
+        ray_from(sh, y0);
+        ray_from(sh + 17, y1);
+        ray_from(sh + 34, y2);
+        copy_ray(*R.V, i, y0);
+        copy_ray(*R.C, i, y1);
+        copy_ray(*R.X, i, y2);
+        for (int f = 0; f < q.nf; ++f) {
+            R.X->atten[(size_t)f * q.n + i] = sh[51 + f];
+            R.X->phase[(size_t)f * q.n + i] = sh[51 + q.nf + f];
+        }
+        const int32_t sf = q.shadow_cnt[3 * (size_t)w], bt = q.shadow_cnt[3 * (size_t)w + 1];
+        R.V->surface[i] = R.C->surface[i] = R.X->surface[i] = sf;
+        R.V->bottom[i] = R.C->bottom[i] = R.X->bottom[i] = bt;
+        R.X->caustic[i] = q.shadow_cnt[3 * (size_t)w + 2];
+    } else {
+        load_ray(*R.V, i, y0);
+        load_ray(*R.C, i, y1);
+        load_ray(*R.X, i, y2);
+        /* detect_caustics of the neighbour below (wave_queue.cc:274-292) */
+        if (d >= 1 && !flag_in[i - naz]) {
+            const int j = i - naz;
+            const double A = y1.pos[0], B = R.C->pos[0][j];
+            const double Cc = y2.pos[0], D = R.X->pos[0][j];
+            const bool fold = (R.X->surface[i] == R.X->surface[j]) && (R.X->bottom[i] == R.X->bottom[j]);
+            if ((Cc - D) * (A - B) < 0 && fold) {
+                R.X->caustic[i] += 1;
+                for (int f = 0; f < q.nf; ++f) R.X->phase[(size_t)f * q.n + i] -= M_PI_2;
+            }
+        }
         /* detect_vertices (wave_queue.cc:261-269) */
-        const double L = R.C->nd[0][i];
-        const double Rn = R.X->nd[0][i];
+        const double L = y1.nd[0];
+        const double Rn = y2.nd[0];
         if (L * Rn < 0.0 && Rn < 0.0) {
             R.X->upper[i] += 1;
         } else if (L * Rn < 0.0 && 0.0 < Rn) {
             R.X->lower[i] += 1;
         }
     }
-    /* find_edges on X */
+    /* find_edges on the post-reflection "next" front */
     {
         const int max_de = q.nde - 1;
-        const double* rho = R.X->pos[0];
-        const double* ndr = R.X->nd[0];
+        auto rho_at = [&](int j) {
+            return flag_in[j] ? q.shadow[(size_t)q.shadow_slot[j] * stride + 34] : R.X->pos[0][j];
+        };
+        auto ndr_at = [&](int j) {
+            return flag_in[j] ? q.shadow[(size_t)q.shadow_slot[j] * stride + 34 + 6] : R.X->nd[0][j];
+        };
         auto extremum = [&](int dd) -> bool {
             if (dd < 1 || dd > max_de - 1) return false;
             const int j = i + (dd - d) * naz;
-            const double r0 = rho[j], rp = rho[j + naz], rm = rho[j - naz];
+            const double r0 = rho_at(j), rp = rho_at(j + naz), rm = rho_at(j - naz);
             return (r0 < rp && r0 < rm) || (r0 > rp && r0 > rm);
         };
         bool edge = (d == 0) || (d == max_de) || extremum(d);
         if (!edge && extremum(d + 1)) {
-            const double n0 = ndr[i + naz];
-            if (fabs(n0 - ndr[i]) > fabs(n0 - ndr[i + 2 * naz])) edge = true;
+            const double n0 = ndr_at(i + naz);
+            if (fabs(n0 - y2.nd[0]) > fabs(n0 - ndr_at(i + 2 * naz))) edge = true;
         }
         if (!edge && extremum(d - 1)) {
-            const double n0 = ndr[i - naz];
-            if (!(fabs(n0 - ndr[i - 2 * naz]) > fabs(n0 - ndr[i]))) edge = true;
+            const double n0 = ndr_at(i - naz);
+            if (!(fabs(n0 - ndr_at(i - 2 * naz)) > fabs(n0 - y2.nd[0]))) edge = true;
         }
         R.X->on_edge[i] = edge ? 1 : 0;
     }
     /* rotate and take the AB3 step */
-    RayS y0, y1, y2, y3;
-    load_ray(*R.V, i, y0);
-    load_ray(*R.C, i, y1);
-    load_ray(*R.X, i, y2);
     ab3(q.dt, y0, y1, y2, y3);
     update_main(q, *R.P, i, y3, true, R.X);
     R.P->plen[i] = y3.dist + R.X->plen[i];
