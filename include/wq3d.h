@@ -92,10 +92,16 @@ enum {
 
 /* N-dimensional rectilinear grid (types/gen_grid.h:83-520).  Data is
  * row-major with the last axis fastest (types/data_grid.h:47-61). */
+/* sequence kinds of a grid axis; they differ in find_index
+ * (types/seq_linear.h:89-94, seq_log.h:88-94, seq_data.cc:15-36) */
+enum { WQ3D_AXIS_LINEAR = 0, WQ3D_AXIS_LOG = 1, WQ3D_AXIS_DATA = 2 };
+
 typedef struct wq3d_grid_desc {
     int ndim;                  /* 0 = unused, else 1..3 */
-    const double* axis[3];     /* axis values, monotonic */
+    const double* axis[3];     /* axis values, monotonic, at least 2 each */
+    const double* axis_inc[3]; /* seq_vector::increment(i) of each axis */
     size_t axis_size[3];
+    int axis_kind[3];          /* WQ3D_AXIS_* */
     const double* data;        /* prod(axis_size) values */
     int interp[3];             /* WQ3D_INTERP_* per axis */
     int edge_limit[3];         /* nonzero: clamp outside the axis range */

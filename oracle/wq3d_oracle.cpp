@@ -53,13 +53,250 @@ std::string g_err;
 /* ocean models                                                        */
 /* ------------------------------------------------------------------ */
 
+/* seq_vector axis used by a grid (types/seq_vector.h) */
+struct Axis {
+    std::vector<double> x, inc;
+    int kind = WQ3D_AXIS_LINEAR;
+    double sign = 1.0;
+    size_t size() const { return x.size(); }
+    /* seq_vector::increment clamps (seq_vector.h:140-143) */
+    double increment(size_t i) const { return inc[std::max((size_t)0, std::min(x.size() - 1, i))]; }
+    /* seq_linear.h:89-94, seq_log.h:88-94, seq_data.cc:15-36 */
+    size_t find_index(double value) const {
+        if (kind == WQ3D_AXIS_LINEAR) {
+            return (size_t)std::max((long)0, std::min((long)size() - 2, (long)std::floor((value - x[0]) / inc[0])));
+        }
+        if (kind == WQ3D_AXIS_LOG) {
+            return (size_t)std::max((long)0, std::min((long)size() - 2,
+                                                      (long)std::floor(std::log(value / x[0]) / std::log(inc[1] / inc[0]))));
+        }
+        value *= sign;
+        const size_t max_index = size() - 1;
+        if (max_index < 1) return 0;
+        if (value <= sign * x[0]) return 0;
+        if (value >= sign * x[max_index - 1]) return max_index - 1;
+        /* std::map<key, index>::upper_bound over keys sign*x[n] */
+        size_t n = 0;
+        while (n < size() && !(sign * x[n] > value)) ++n;
+        return n - 1;
+    }
+};
+
+/* gen_grid<N, double> (types/gen_grid.h:83-520) */
 struct Grid {
     int ndim = 0;
-    std::vector<double> axis[3];
+    Axis axis[3];
     std::vector<double> data;
     int interp[3] = {0, 0, 0};
     int edge[3] = {1, 1, 1};
+
+    double at(const size_t* index) const {
+        size_t off = index[0];
+        for (int d = 1; d < ndim; ++d) off = index[d] + axis[d].size() * off;
+        return data[off];
+    }
+    double interp_dim(int dim, const size_t* index, const double* loc, double& deriv, double* dv) const {
+        if (dim < 0) return at(index);
+        if (axis[dim].size() < 2) return nearest(dim, index, loc, deriv, dv);
+        switch (interp[dim]) {
+            case WQ3D_INTERP_NEAREST:
+                return nearest(dim, index, loc, deriv, dv);
+            case WQ3D_INTERP_PCHIP:
+                return pchip(dim, index, loc, deriv, dv);
+            default:
+                return linear(dim, index, loc, deriv, dv);
+        }
+    }
+    double nearest(int dim, const size_t* index, const double* loc, double& deriv, double* dv) const {
+        double result, da = 0.0;
+        const size_t k = index[dim];
+        const Axis& ax = axis[dim];
+        const double u = (loc[dim] - ax.x[k]) / ax.increment(k);
+        if (u < 0.5) {
+            result = interp_dim(dim - 1, index, loc, da, dv);
+        } else {
+            size_t next[3] = {index[0], index[1], index[2]};
+            ++next[dim];
+            result = interp_dim(dim - 1, next, loc, da, dv);
+        }
+        if (dv) {
+            dv[dim] = deriv;
+            if (dim > 0) dv[dim - 1] = da;
+        }
+        return result;
+    }
+    double linear(int dim, const size_t* index, const double* loc, double& deriv, double* dv) const {
+        double da = 0.0, db = 0.0;
+        const double a = interp_dim(dim - 1, index, loc, da, dv);
+        size_t next[3] = {index[0], index[1], index[2]};
+        ++next[dim];
+        const double b = interp_dim(dim - 1, next, loc, db, dv);
+        const size_t k = index[dim];
+        const Axis& ax = axis[dim];
+        const double h = ax.increment(k);
+        const double u = (loc[dim] - ax.x[k]) / h;
+        const double result = a * (1.0 - u) + b * u;
+        if (dv) {
+            deriv = (b - a) / h;
+            dv[dim] = deriv;
+            if (dim > 0) dv[dim - 1] = da * (1.0 - u) + db * u;
+        }
+        return result;
+    }
+    /* gen_grid_utils.h derivative<double> / end_point_derivative<double> */
+    static void harmonic(double d0, double d1, double dd0, double dd1, double w0, double w1, bool deriv,
+                         double& m, double& dm) {
+        if (d0 * d1 > 0.0) m = (w0 + w1) / (w0 / d0 + w1 / d1);
+        if (deriv && dd0 * dd1 > 0.0) dm = (w0 + w1) / (w0 / dd0 + w1 / dd1);
+    }
+    static void end_point(double d0, double d1, double dd0, double dd1, bool deriv, double& m, double& dm) {
+        if (m * d0 < 0.0) {
+            m = 0.0;
+        } else if ((d0 * d1 < 0.0) && (std::abs(m) > std::abs(3.0 * d1))) {
+            m = 3.0 * d1;
+        }
+        if (deriv) {
+            if (dm * dd0 < 0.0) {
+                dm = 0.0;
+            } else if ((dd0 * dd1 < 0.0) && (std::abs(dm) > std::abs(3.0 * dd0))) {
+                dm = 3.0 * dd0;
+            }
+        } else {
+            dm = 0.0;
+        }
+    }
+    /* gen_grid.h pchip, with its end-point formulas as written */
+    double pchip(int dim, const size_t* index, const double* loc, double& deriv, double* dv) const {
+        const Axis& ax = axis[dim];
+        const size_t kmin = 1u;
+        const size_t kmax = ax.size() - 3u;
+        double y0, y1, y2, y3, dy0 = 0.0, dy1 = 0.0, dy2 = 0.0, dy3 = 0.0;
+        const size_t k = index[dim];
+        y1 = interp_dim(dim - 1, index, loc, dy1, dv);
+        if (k >= kmin) {
+            size_t prev[3] = {index[0], index[1], index[2]};
+            --prev[dim];
+            y0 = interp_dim(dim - 1, prev, loc, dy0, dv);
+        } else {
+            y0 = y1;
+            dy0 = dy1;
+        }
+        size_t next[3] = {index[0], index[1], index[2]};
+        ++next[dim];
+        y2 = interp_dim(dim - 1, next, loc, dy2, dv);
+        if (k <= kmax) {
+            size_t last[3] = {next[0], next[1], next[2]};
+            ++last[dim];
+            y3 = interp_dim(dim - 1, last, loc, dy3, dv);
+        } else {
+            y3 = y2;
+            dy3 = dy2;
+        }
+        const double h0 = ax.increment(k - 1);
+        const double h1 = ax.increment(k);
+        const double h2 = ax.increment(k + 1);
+        const double h1_2 = h1 * h1;
+        const double h1_3 = h1_2 * h1;
+        const double s = loc[dim] - ax.x[k];
+        const double s_2 = s * s, s_3 = s_2 * s;
+        const double sh_minus = s - h1;
+        const double sh_term = 3.0 * h1 * s_2 - 2.0 * s_3;
+        const double deriv0 = (y1 - y0) / h0;
+        const double deriv1 = (y2 - y1) / h1;
+        const double deriv2 = (y3 - y2) / h2;
+        double dderiv0 = 0.0, dderiv1 = 0.0, dderiv2 = 0.0;
+        if (dv) {
+            dderiv0 = (dy1 - dy0) / h0;
+            dderiv1 = (dy2 - dy1) / h1;
+            dderiv2 = (dy3 - dy2) / h2;
+        }
+        double slope1 = 0.0, dslope1 = 0.0;
+        if (k >= kmin) {
+            const double w0 = 2.0 * h1 + h0;
+            const double w1 = h1 + 2.0 * h0;
+            harmonic(deriv0, deriv1, dderiv0, dderiv1, w0, w1, dv != nullptr, slope1, dslope1);
+        } else {
+            slope1 = ((2.0 + h1 + h2) * deriv1 - h1 * deriv2) / (h1 + h2);
+            dslope1 = ((2.0 + h1 + h2) * dderiv1 - h1 * dderiv2) / (h1 + h2);
+            end_point(deriv1, deriv2, dderiv1, dderiv2, dv != nullptr, slope1, dslope1);
+        }
+        double slope2 = 0.0, dslope2 = 0.0;
+        if (k <= kmax) {
+            const double w1 = 2.0 * h1 + h0;
+            const double w2 = h1 + 2.0 * h0;
+            harmonic(deriv1, deriv2, dderiv1, dderiv2, w1, w2, dv != nullptr, slope2, dslope2);
+        } else {
+            slope2 = ((2.0 + h1 + h2) * deriv1 - h1 * deriv0) / (h1 + h0);
+            dslope2 = ((2.0 + h1 + h2) * dderiv1 - h1 * dderiv0) / (h1 + h0);
+            end_point(deriv1, deriv0, dderiv1, dderiv0, dv != nullptr, slope2, dslope2);
+        }
+        const double result = y2 * sh_term / h1_3 + y1 * (h1_3 - sh_term) / h1_3 +
+                              slope2 * s_2 * sh_minus / h1_2 + slope1 * s * sh_minus * sh_minus / h1_2;
+        if (dv) {
+            const double v = s / h1;
+            deriv = slope1 * (1.0 - v) + slope2 * v;
+            dv[dim] = deriv;
+            if (dim > 0)
+                dv[dim - 1] = dy2 * sh_term / h1_3 + dy1 * (h1_3 - sh_term) / h1_3 +
+                              dslope2 * s_2 * sh_minus / h1_2 + dslope1 * s * sh_minus * sh_minus / h1_2;
+        }
+        return result;
+    }
+    /* gen_grid::interpolate (gen_grid.h:83-123) */
+    double interpolate(const double* location, double* dv) const {
+        size_t index[3] = {0, 0, 0};
+        double loc[3] = {0, 0, 0};
+        for (int d = 0; d < ndim; ++d) loc[d] = location[d];
+        for (int d = 0; d < ndim; ++d) {
+            const Axis& ax = axis[d];
+            if (ax.size() < 2) {
+                loc[d] = ax.x[0];
+                index[d] = 0;
+            } else if (edge[d]) {
+                const double a = ax.x[0];
+                const double b = ax.x[ax.size() - 1];
+                const double sign = (ax.increment(0) < 0) ? -1.0 : 1.0;
+                const double dd = loc[d] * sign;
+                if (dd <= a * sign) {
+                    loc[d] = a;
+                    index[d] = 0;
+                } else if (dd >= b * sign) {
+                    loc[d] = b;
+                    index[d] = ax.size() - 2;
+                } else {
+                    index[d] = ax.find_index(loc[d]);
+                }
+            } else {
+                index[d] = ax.find_index(loc[d]);
+            }
+        }
+        double dresult = 0.0;
+        return interp_dim(ndim - 1, index, loc, dresult, dv);
+    }
 };
+
+void load_grid(Grid& g, const wq3d_grid_desc& d) {
+    g.ndim = d.ndim;
+    size_t total = 1;
+    for (int k = 0; k < d.ndim; ++k) {
+        const size_t n = d.axis_size[k];
+        g.axis[k].x.assign(d.axis[k], d.axis[k] + n);
+        g.axis[k].inc.assign(d.axis_inc[k], d.axis_inc[k] + n);
+        g.axis[k].kind = d.axis_kind[k];
+        g.axis[k].sign = (n > 1 && d.axis[k][1] - d.axis[k][0] < 0) ? -1.0 : 1.0;
+        int it = d.interp[k];
+        /* data_grid::interp_type (data_grid.h:137-145) */
+        if (it > WQ3D_INTERP_NEAREST && n < 2) {
+            it = WQ3D_INTERP_NEAREST;
+        } else if (it > WQ3D_INTERP_LINEAR && n < 4) {
+            it = WQ3D_INTERP_LINEAR;
+        }
+        g.interp[k] = it;
+        g.edge[k] = d.edge_limit[k] ? 1 : 0;
+        total *= n;
+    }
+    g.data.assign(d.data, d.data + total);
+}
 
 struct Boundary {
     int kind = WQ3D_BOUNDARY_FLAT;
@@ -84,8 +321,6 @@ struct Ocean {
  * profile_n2.cc:14-24, with profile_model::adjust_speed (profile_model.cc:14-26) */
 void sound_speed(const Ocean& oc, double R, double rho, double theta,
                  double phi, double* c, double* g) {
-    (void)theta;
-    (void)phi;
     const double* p = oc.prof.p;
     const double alt = rho - R;
     double gr = 0.0, gt = 0.0, gp = 0.0;
@@ -119,6 +354,16 @@ void sound_speed(const Ocean& oc, double R, double rho, double theta,
             gr = std::pow(cc, 3.0) * factor / (2.0 * p[0] * p[0]);
             break;
         }
+        case WQ3D_PROFILE_GRID: {
+            /* profile_grid.h:68-130 */
+            const double loc[3] = {rho, theta, phi};
+            double dv[3] = {0.0, 0.0, 0.0};
+            cc = oc.pgrid.interpolate(loc, dv);
+            gr = dv[0];
+            if (oc.pgrid.ndim >= 2) gt = dv[1];
+            if (oc.pgrid.ndim >= 3) gp = dv[2];
+            break;
+        }
         default:
             cc = 1500.0;
     }
@@ -138,6 +383,29 @@ void sound_speed(const Ocean& oc, double R, double rho, double theta,
 void height(const Boundary& b, double rho, double theta, double phi,
             double* h, double* n) {
     (void)rho;
+    if (b.kind == WQ3D_BOUNDARY_GRID) {
+        /* boundary_grid.h:150-196 */
+        const double loc[2] = {theta, phi};
+        double grad[2] = {0.0, 0.0};
+        *h = b.grid.interpolate(loc, n ? grad : nullptr);
+        if (n) {
+            if (b.grid.ndim == 1) {
+                const double t = -grad[0] / (*h);
+                const double N = std::sqrt(1 + t * t);
+                n[0] = 1.0 / N;
+                n[1] = t / N;
+                n[2] = 0.0;
+            } else {
+                const double t = -grad[0] / (*h);
+                const double pp = -grad[1] / ((*h) * std::sin(theta));
+                const double N = std::sqrt(1 + t * t + pp * pp);
+                n[0] = 1.0 / N;
+                n[1] = t / N;
+                n[2] = pp / N;
+            }
+        }
+        return;
+    }
     if (b.kind == WQ3D_BOUNDARY_SLOPE) {
         const double alpha = -std::asin(b.nrm[1]);
         const double beta = -std::asin(b.nrm[2]);
@@ -238,6 +506,14 @@ void setup_boundary(Boundary& b, const wq3d_boundary_desc& d, double R,
             b.loss.p[0] = 0.0;
             b.loss.p[1] = 0.0;
         }
+    } else if (d.kind == WQ3D_BOUNDARY_GRID) {
+        load_grid(b.grid, d.grid);
+        /* boundary_grid.h:56-59 */
+        if (d.loss.kind == WQ3D_LOSS_DEFAULT) {
+            b.loss.kind = WQ3D_LOSS_RAYLEIGH;
+            const double sand[5] = {1.9, 1.10, 0.8, 0.00, 2.5};
+            for (int k = 0; k < 5; ++k) b.loss.p[k] = sand[k];
+        }
     } else {
         /* boundary_flat.cc:19-31 */
         b.kind = WQ3D_BOUNDARY_FLAT;
@@ -262,11 +538,11 @@ void setup_boundary(Boundary& b, const wq3d_boundary_desc& d, double R,
     if (b.loss.kind == WQ3D_LOSS_RAYLEIGH) {
         /* reflect_loss_rayleigh.cc:17,68-78 */
         const double ATT_CONVERT = 1.0 / (20.0 * M_LOG10E * TWO_PI);
-        b.rl_den = 1000.0 * d.loss.p[0];
-        b.rl_spd = 1500.0 * d.loss.p[1];
-        b.rl_att = d.loss.p[2] * ATT_CONVERT;
-        b.rl_shr = 1500.0 * d.loss.p[3];
-        b.rl_satt = d.loss.p[4] * ATT_CONVERT;
+        b.rl_den = 1000.0 * b.loss.p[0];
+        b.rl_spd = 1500.0 * b.loss.p[1];
+        b.rl_att = b.loss.p[2] * ATT_CONVERT;
+        b.rl_shr = 1500.0 * b.loss.p[3];
+        b.rl_satt = b.loss.p[4] * ATT_CONVERT;
     }
 }
 
@@ -533,10 +809,7 @@ struct Queue {
         oc.build_radius = od->earth_radius;
         setup_boundary(oc.surf, od->surface, od->earth_radius, true);
         setup_boundary(oc.bot, od->bottom, od->earth_radius, false);
-        if (oc.prof.kind == WQ3D_PROFILE_GRID) {
-            g_err = "oracle: profile grids not restated";
-            return WQ3D_ERR_UNSUPPORTED;
-        }
+        if (oc.prof.kind == WQ3D_PROFILE_GRID) load_grid(oc.pgrid, od->profile.grid);
         R = qd->earth_radius;
         nde = qd->num_de;
         naz = qd->num_az;
@@ -1829,6 +2102,7 @@ int oracle_sound_speed(const wq3d_ocean_desc* od, double R, size_t n,
                        double* speed, double* grad) {
     Ocean oc;
     oc.prof = od->profile;
+    if (oc.prof.kind == WQ3D_PROFILE_GRID) load_grid(oc.pgrid, od->profile.grid);
     for (size_t i = 0; i < n; ++i) {
         double g[3];
         sound_speed(oc, R, rho[i], theta[i], phi[i], &speed[i], g);

@@ -13,7 +13,7 @@ from .types import (seq_vector, seq_linear, seq_log, seq_data, seq_rayfan,
 from .ocean import (attenuation_thorp, attenuation_constant, profile_linear,
                     profile_munk, profile_catenary, profile_n2, reflect_loss_constant,
                     reflect_loss_rayleigh, reflect_loss_eckart, boundary_flat,
-                    boundary_slope, ocean_model)
+                    boundary_slope, ocean_model, data_grid, profile_grid, boundary_grid)
 from .waveq3d import (wave_queue, eigenray_listener, reflection_listener,
                       eigenray_model)
 from .eigenrays import eigenray_collection
@@ -28,7 +28,8 @@ __all__ = [
     "to_degrees", "to_radians", "attenuation_thorp", "attenuation_constant",
     "profile_linear", "profile_munk", "profile_catenary", "profile_n2",
     "reflect_loss_constant", "reflect_loss_rayleigh", "reflect_loss_eckart",
-    "boundary_flat", "boundary_slope", "ocean_model", "wave_queue",
+    "boundary_flat", "boundary_slope", "ocean_model", "data_grid", "profile_grid",
+    "boundary_grid", "wave_queue",
     "eigenray_listener", "reflection_listener", "eigenray_model",
     "eigenray_collection", "load_engine", "EngineError", "LIB_PATH",
 ]

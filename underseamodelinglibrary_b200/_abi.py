@@ -33,8 +33,12 @@ FRONT_PAST, FRONT_PREV, FRONT_CURR, FRONT_NEXT = 0, 1, 2, 3
 dp = C.POINTER(C.c_double)
 
 
+AXIS_LINEAR, AXIS_LOG, AXIS_DATA = 0, 1, 2
+
+
 class wq3d_grid_desc(C.Structure):
-    _fields_ = [("ndim", C.c_int), ("axis", dp * 3), ("axis_size", C.c_size_t * 3),
+    _fields_ = [("ndim", C.c_int), ("axis", dp * 3), ("axis_inc", dp * 3),
+                ("axis_size", C.c_size_t * 3), ("axis_kind", C.c_int * 3),
                 ("data", dp), ("interp", C.c_int * 3), ("edge_limit", C.c_int * 3)]
 
 

@@ -8,19 +8,25 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwq3d.so")
 SOURCES = ["wq3d_api.cu", "wq3d_kernels.cu", "wq3d_noalloc.cu"]
+# (object name, source, extra flags): wq3d_kernels.cu is compiled a second
+# time for the ray-stepping kernels of oceans without gridded models
+OBJECTS = [(f, f, []) for f in SOURCES] + [
+    ("wq3d_kernels_analytic.cu", "wq3d_kernels.cu",
+     ["-DWQ3D_WITH_GRID=0", "-DWQ3D_KERNEL_NS=analytic", "-DWQ3D_STEP_KERNELS_ONLY=1"]),
+]
 HEADERS = ["wq3d_engine.cuh", "wq3d_models.cuh"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "--fmad=false", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
-    "-shared",
 ]
 
 
@@ -41,13 +47,26 @@ def stale():
 
 
 def build(force=False, verbose=False):
+    """Compiles each source to an object in parallel, then links them."""
     if not force and not stale():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp"]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.check_call(cmd)
+    with tempfile.TemporaryDirectory(prefix="wq3d_build_") as tmp:
+        objs, procs = [], []
+        for name, f, extra in OBJECTS:
+            obj = os.path.join(tmp, name + ".o")
+            cmd = [nvcc()] + NVCC_FLAGS + extra + ["-I", os.path.join(ROOT, "include"), "-c",
+                                                   os.path.join(CSRC, f), "-o", obj]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            procs.append((cmd, subprocess.Popen(cmd)))
+            objs.append(obj)
+        failed = [cmd for cmd, p in procs if p.wait() != 0]
+        if failed:
+            raise subprocess.CalledProcessError(1, failed[0])
+        link = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB + ".tmp"] + objs
+        if verbose:
+            print(" ".join(link), file=sys.stderr)
+        subprocess.check_call(link)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

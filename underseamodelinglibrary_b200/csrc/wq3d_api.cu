@@ -65,6 +65,13 @@ void setup_boundary(BoundaryDev& b, const wq3d_boundary_desc& d, double R) {
             b.loss.p[0] = 0.0;
             b.loss.p[1] = 0.0;
         }
+    } else if (d.kind == WQ3D_BOUNDARY_GRID) {
+        /* boundary_grid.h:56-59: Rayleigh sand unless a loss is given */
+        if (b.loss.kind == WQ3D_LOSS_DEFAULT) {
+            b.loss.kind = WQ3D_LOSS_RAYLEIGH;
+            const double sand[5] = {1.9, 1.10, 0.8, 0.00, 2.5};
+            for (int k = 0; k < 5; ++k) b.loss.p[k] = sand[k];
+        }
     } else {
         b.kind = WQ3D_BOUNDARY_FLAT;
         b.height = R - std::abs(d.depth);
@@ -86,11 +93,11 @@ void setup_boundary(BoundaryDev& b, const wq3d_boundary_desc& d, double R) {
     }
     if (b.loss.kind == WQ3D_LOSS_RAYLEIGH) {
         const double ATT_CONVERT = 1.0 / (20.0 * M_LOG10E * (2.0 * M_PI));
-        b.loss.rl_den = 1000.0 * d.loss.p[0];
-        b.loss.rl_spd = 1500.0 * d.loss.p[1];
-        b.loss.rl_att = d.loss.p[2] * ATT_CONVERT;
-        b.loss.rl_shr = 1500.0 * d.loss.p[3];
-        b.loss.rl_satt = d.loss.p[4] * ATT_CONVERT;
+        b.loss.rl_den = 1000.0 * b.loss.p[0];
+        b.loss.rl_spd = 1500.0 * b.loss.p[1];
+        b.loss.rl_att = b.loss.p[2] * ATT_CONVERT;
+        b.loss.rl_shr = 1500.0 * b.loss.p[3];
+        b.loss.rl_satt = b.loss.p[4] * ATT_CONVERT;
     }
 }
 
@@ -110,9 +117,70 @@ struct DeviceGuard {
 }  // namespace
 
 struct wq3d_ocean {
-    OceanDev dev;
+    OceanDev dev;   /* device pointers, passed to kernels        */
+    OceanDev host;  /* host pointers, for host-side evaluations  */
     double build_radius;
+    std::vector<std::vector<double>> store;  /* host copies of grid arrays */
+    std::vector<void*> dmem;                 /* device copies             */
+    ~wq3d_ocean() {
+        for (void* p : dmem) cudaFree(p);
+    }
 };
+
+namespace {
+
+/* Copies a grid description into a host GridDev and a device GridDev.
+ * Interpolation types follow data_grid::interp_type (data_grid.h:137-145):
+ * PCHIP needs 4 points and anything but nearest needs 2. */
+int make_grid(wq3d_ocean* o, const wq3d_grid_desc& d, int max_dims, GridDev* hg, GridDev* dg) {
+    if (d.ndim < 1 || d.ndim > max_dims) return fail(WQ3D_ERR_INVALID, "grid dimension out of range");
+    std::memset(hg, 0, sizeof(*hg));
+    hg->ndim = d.ndim;
+    size_t total = 1;
+    for (int k = 0; k < d.ndim; ++k) {
+        const size_t n = d.axis_size[k];
+        if (n < 2 || !d.axis[k] || !d.axis_inc[k]) return fail(WQ3D_ERR_INVALID, "grid axes need at least 2 values");
+        if (d.axis_kind[k] < WQ3D_AXIS_LINEAR || d.axis_kind[k] > WQ3D_AXIS_DATA)
+            return fail(WQ3D_ERR_INVALID, "bad axis kind");
+        total *= n;
+        o->store.emplace_back(d.axis[k], d.axis[k] + n);
+        hg->ax[k].x = o->store.back().data();
+        o->store.emplace_back(d.axis_inc[k], d.axis_inc[k] + n);
+        hg->ax[k].inc = o->store.back().data();
+        hg->ax[k].n = (int)n;
+        hg->ax[k].kind = d.axis_kind[k];
+        hg->ax[k].sign = (d.axis[k][1] - d.axis[k][0] < 0) ? -1.0 : 1.0;
+        int it = d.interp[k];
+        if (it > WQ3D_INTERP_NEAREST && n < 2) {
+            it = WQ3D_INTERP_NEAREST;
+        } else if (it > WQ3D_INTERP_LINEAR && n < 4) {
+            it = WQ3D_INTERP_LINEAR;
+        }
+        hg->interp[k] = it;
+        hg->edge[k] = d.edge_limit[k] ? 1 : 0;
+    }
+    if (!d.data) return fail(WQ3D_ERR_INVALID, "grid data missing");
+    o->store.emplace_back(d.data, d.data + total);
+    hg->data = o->store.back().data();
+    *dg = *hg;
+    auto up = [&](const double* src, size_t n, const double** out) -> int {
+        void* p = nullptr;
+        WQ_CK(cudaMalloc(&p, n * sizeof(double)));
+        o->dmem.push_back(p);
+        WQ_CK(cudaMemcpy(p, src, n * sizeof(double), cudaMemcpyHostToDevice));
+        *out = static_cast<const double*>(p);
+        return WQ3D_OK;
+    };
+    int rc = 0;
+    for (int k = 0; k < d.ndim && !rc; ++k) {
+        rc = up(hg->ax[k].x, hg->ax[k].n, &dg->ax[k].x);
+        if (!rc) rc = up(hg->ax[k].inc, hg->ax[k].n, &dg->ax[k].inc);
+    }
+    if (!rc) rc = up(hg->data, total, &dg->data);
+    return rc;
+}
+
+}  // namespace
 
 struct PendingRay {
     wq3d_eigenray rec;
@@ -150,6 +218,10 @@ struct wq3d_queue {
     double ms_step = 0.0, ms_cpa = 0.0, ms_eig = 0.0, ms_total = 0.0;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     int64_t launches = 0;
+    /* the stepping kernels' build: "gridded" when the ocean has a grid */
+    bool gridded = false;
+    void (*k_reflect_fn)(const QueueDev*, int) = analytic::k_reflect;
+    void (*k_advance_fn)(const QueueDev*, int) = analytic::k_advance;
     std::vector<wq3d_eigenray> h_rec;
     std::vector<double> h_rinten, h_rphase;
     std::vector<wq3d_reflection> h_refl;
@@ -196,19 +268,19 @@ struct wq3d_queue {
         const dim3 blk(128);
         const dim3 grd((n + 127) / 128);
         const int rgrid = std::max(1, std::min(4 * 148, (n + 63) / 64));
-        k_reflect<<<rgrid, 64, 0, stream>>>(d_q, 0);
+        k_reflect_fn<<<rgrid, 64, 0, stream>>>(d_q, 0);
         launches += 1;
         for (int k = 0; k < K; ++k) {
             cudaEvent_t* ev = timing ? &events[5 * k] : nullptr;
             if (ev) cudaEventRecord(ev[0], stream);
-            k_advance<<<grd, blk, 0, stream>>>(d_q, k);
+            k_advance_fn<<<grd, blk, 0, stream>>>(d_q, k);
             if (ev) cudaEventRecord(ev[1], stream);
             launches += 1;
             const bool more = k + 1 < K;
             if (more) {
                 cudaEventRecord(fork_ev[k], stream);
                 cudaStreamWaitEvent(side, fork_ev[k], 0);
-                k_reflect<<<rgrid, 64, 0, side>>>(d_q, k + 1);
+                k_reflect_fn<<<rgrid, 64, 0, side>>>(d_q, k + 1);
                 cudaEventRecord(join_ev[k], side);
                 launches += 1;
             }
@@ -390,10 +462,11 @@ int wq3d_device_count(int* count) {
 
 int wq3d_ocean_create(const wq3d_ocean_desc* d, wq3d_ocean** out) {
     if (!d || !out) return fail(WQ3D_ERR_INVALID, "null argument");
-    if (d->profile.kind < WQ3D_PROFILE_LINEAR || d->profile.kind > WQ3D_PROFILE_N2)
+    if (d->profile.kind < WQ3D_PROFILE_LINEAR || d->profile.kind > WQ3D_PROFILE_GRID)
         return fail(WQ3D_ERR_UNSUPPORTED, "profile kind not supported by this build");
-    if (d->bottom.kind == WQ3D_BOUNDARY_GRID || d->surface.kind == WQ3D_BOUNDARY_GRID)
-        return fail(WQ3D_ERR_UNSUPPORTED, "boundary grids not supported by this build");
+    for (const wq3d_boundary_desc* b : {&d->surface, &d->bottom})
+        if (b->kind < WQ3D_BOUNDARY_FLAT || b->kind > WQ3D_BOUNDARY_GRID)
+            return fail(WQ3D_ERR_UNSUPPORTED, "boundary kind not supported by this build");
     wq3d_ocean* o = new wq3d_ocean();
     std::memset(&o->dev, 0, sizeof(o->dev));
     ProfileDev& p = o->dev.prof;
@@ -406,6 +479,20 @@ int wq3d_ocean_create(const wq3d_ocean_desc* d, wq3d_ocean** out) {
     p.atten_coef = d->profile.attenuation_coef;
     setup_boundary(o->dev.surf, d->surface, d->earth_radius);
     setup_boundary(o->dev.bot, d->bottom, d->earth_radius);
+    o->host = o->dev;
+    int rc = WQ3D_OK;
+    if (p.kind == WQ3D_PROFILE_GRID)
+        rc = make_grid(o, d->profile.grid, 3, &o->host.prof.grid, &o->dev.prof.grid);
+    if (!rc && d->surface.kind == WQ3D_BOUNDARY_GRID)
+        rc = make_grid(o, d->surface.grid, 2, &o->host.surf.grid, &o->dev.surf.grid);
+    if (!rc && d->bottom.kind == WQ3D_BOUNDARY_GRID)
+        rc = make_grid(o, d->bottom.grid, 2, &o->host.bot.grid, &o->dev.bot.grid);
+    if (rc) {
+        const std::string msg = g_err;
+        delete o;
+        g_err = msg;
+        return rc;
+    }
     o->build_radius = d->earth_radius;
     *out = o;
     return WQ3D_OK;
@@ -564,10 +651,11 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     }
     /* wave_queue.cc:58-68: the clamp changes source_pos() only; init_wave
      * receives the caller's position (wave_queue.cc:83) */
+    const OceanDev& hoc = ocean->host;
     for (int k = 0; k < 3; ++k) h.source[k] = q->src_clamped[k] = d->source[k];
     {
         const double offset = 0.1;
-        double bottom_rho = boundary_height(h.oc.bot, d->source[1], d->source[2]) + offset;
+        double bottom_rho = boundary_height(hoc.bot, d->source[1], d->source[2]) + offset;
         if (q->src_clamped[0] - h.R > -offset) {
             q->src_clamped[0] = -offset + h.R;
         } else if (q->src_clamped[0] < bottom_rho) {
@@ -575,8 +663,8 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         }
     }
     {
-        double gr;
-        sound_speed(h.oc.prof, h.R, d->source[0], &h.c_source, &gr);
+        double g3[3];
+        sound_speed(hoc.prof, h.R, d->source[0], d->source[1], d->source[2], &h.c_source, g3);
     }
     std::vector<double> cos_de(nde), sin_de(nde), cos_az(naz), sin_az(naz);
     for (size_t i = 0; i < nde; ++i) {
@@ -607,8 +695,8 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         tsin[t] = std::sin(tt[t]);
         tR2[t] = tr[t] * tr[t];
         t2R[t] = 2.0 * tr[t];
-        double gr;
-        sound_speed(h.oc.prof, h.R, tr[t], &tc[t], &gr);
+        double g3[3];
+        sound_speed(hoc.prof, h.R, tr[t], tt[t], tp[t], &tc[t], g3);
         for (size_t k = 0; k < nf; ++k) {
             const double s = 2.0 * M_PI * tc[t] / freq[k];
             tspread[t * nf + k] = s * s;
@@ -747,7 +835,12 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
 
     /* wave_queue ctor: init_wave, update, init_wavefronts */
-    k_startup<<<(unsigned)((n + 127) / 128), 128, 0, q->stream>>>(q->d_q);
+    q->gridded = ocean->dev.prof.kind == WQ3D_PROFILE_GRID || ocean->dev.surf.kind == WQ3D_BOUNDARY_GRID ||
+                 ocean->dev.bot.kind == WQ3D_BOUNDARY_GRID;
+    q->k_reflect_fn = q->gridded ? gridded::k_reflect : analytic::k_reflect;
+    q->k_advance_fn = q->gridded ? gridded::k_advance : analytic::k_advance;
+    (q->gridded ? gridded::k_startup : analytic::k_startup)<<<(unsigned)((n + 127) / 128), 128, 0, q->stream>>>(
+        q->d_q);
     cudaError_t e = cudaStreamSynchronize(q->stream);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return cleanup(fail(WQ3D_ERR_CUDA, std::string("start-up kernel: ") + cudaGetErrorString(e)));

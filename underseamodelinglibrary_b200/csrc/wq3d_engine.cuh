@@ -127,10 +127,20 @@ struct QueueDev {
     uint32_t* err;
 };
 
-/* kernels (wq3d_kernels.cu) */
-__global__ void k_startup(const QueueDev* q);
-__global__ void k_reflect(const QueueDev* q, int k);
-__global__ void k_advance(const QueueDev* q, int k);
+/* kernels (wq3d_kernels.cu).  The ray-stepping kernels come in two
+ * builds: "gridded" evaluates every profile and boundary kind, "analytic"
+ * leaves out the gridded ones (whose out-of-line interpolation calls cost
+ * the stepping kernels registers) and serves oceans without grids. */
+#define WQ3D_DECLARE_STEP_KERNELS                         \
+    __global__ void k_startup(const QueueDev* q);         \
+    __global__ void k_reflect(const QueueDev* q, int k);  \
+    __global__ void k_advance(const QueueDev* q, int k);
+namespace gridded {
+WQ3D_DECLARE_STEP_KERNELS
+}
+namespace analytic {
+WQ3D_DECLARE_STEP_KERNELS
+}
 __global__ void k_cpa(const QueueDev* q, int k);
 __global__ void k_cpa_f32(const QueueDev* q, int k);
 __global__ void k_eigenray(const QueueDev* q, int k);

@@ -3,27 +3,39 @@
  *
  * One step of wave_queue::step() (waveq3d/wave_queue.cc:155-192) is four
  * launches:
- *   k_step      one thread per ray: caustic hand-off from the D/E
- *               neighbour, surface/bottom reflections with the RK3
- *               re-initialisation, vertices, the queue rotation, the AB3
- *               step and wave_front::update of the new front.
- *   k_edges     one thread per ray: wave_front::find_edges on the front
- *               that became "curr".
+ *   k_reflect   one thread per ray on the worklist of rays that reflect in
+ *               this step: caustic hand-off from the D/E neighbour and the
+ *               surface/bottom reflection chain with the RK3
+ *               re-initialisation, on a private copy of the ray written to
+ *               its shadow slot.  It only reads the fronts, so it runs on a
+ *               side stream beside the previous step's k_cpa / k_eigenray.
+ *   k_advance   one thread per ray: commits shadow slots, caustic hand-off
+ *               and vertices of the other rays, wave_front::find_edges,
+ *               the queue rotation, the AB3 step and wave_front::update of
+ *               the new front, and the next step's reflection worklist.
  *   k_cpa       rays x targets: closest-point-of-approach test
  *               (detect_eigenrays + is_closest_ray) with distance2
- *               recomputed from per-front terms; the dominant kernel.
- *   k_eigenray  one thread per CPA found: build_eigenray, compute_offsets,
+ *               recomputed from per-front terms; k_cpa_f32 is its FP32
+ *               screen with an exact FP64 finish.
+ *   k_eigenray  one warp per CPA found: build_eigenray, compute_offsets,
  *               hybrid Gaussian or classic spreading, target angles.
- * All ray-local work of a step is fused into k_step because reflections
- * and the AB3 step of a ray read only that ray's four fronts.  The only
- * cross-ray reads in k_step are the D/E neighbour's values for the caustic
- * test, which that neighbour leaves untouched unless it reflects; whether
- * it reflects was decided by the previous launch and is read from a flag.
  *
  * Compiled with --fmad=false: every add and multiply rounds as in the
  * reference, so the FP64 form differs from the CPU oracle only through the
  * last-place differences between CUDA's and the host's sin/cos/exp.
+ *
+ * The file is compiled twice.  The full build defines every kernel, with
+ * the stepping kernels in namespace "gridded" (all ocean model kinds).  The
+ * second build (WQ3D_WITH_GRID=0, WQ3D_KERNEL_NS=analytic,
+ * WQ3D_STEP_KERNELS_ONLY=1) defines only the stepping kernels, in
+ * namespace "analytic", without the gridded models.
  */
+#ifndef WQ3D_KERNEL_NS
+#define WQ3D_KERNEL_NS gridded
+#endif
+#ifndef WQ3D_STEP_KERNELS_ONLY
+#define WQ3D_STEP_KERNELS_ONLY 0
+#endif
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -62,15 +74,10 @@ __device__ __forceinline__ void set_err(const QueueDev& q, uint32_t bit) {
     atomicOr(q.err, bit);
 }
 
-/* profile evaluation for one point (analytic profiles have no horizontal
- * gradient) */
+/* profile evaluation for one point (profile_model::sound_speed) */
 __device__ __forceinline__ void profile_at(const QueueDev& q, const double* pos,
                                            double* c, double* sg) {
-    double gr;
-    sound_speed(q.oc.prof, q.R, pos[0], c, &gr);
-    sg[0] = gr;
-    sg[1] = 0.0;
-    sg[2] = 0.0;
+    sound_speed(q.oc.prof, q.R, pos[0], pos[1], pos[2], c, sg);
 }
 
 /* wave_front::update on a 1x1 front without targets */
@@ -188,6 +195,7 @@ __device__ __forceinline__ void update_main(const QueueDev& q, const FrontPtrs& 
     }
 }
 
+#if !WQ3D_STEP_KERNELS_ONLY
 /* wave_queue::collision_location (wave_queue.cc:982-1057) */
 __device__ void collision_location(const QueueDev& q, const FrontPtrs& V,
                                    const FrontPtrs& C, const FrontPtrs& X, int i,
@@ -213,6 +221,7 @@ __device__ void collision_location(const QueueDev& q, const FrontPtrs& V,
         nd[k] = C.nd[k][i] + v1 * tw + 0.5 * v2 * dtime2;
     }
 }
+#endif
 
 /* One reflecting ray's prev/curr/next state and next-front losses, held
  * privately while k_reflect works on it.  The results go to a shadow slot
@@ -364,8 +373,8 @@ __device__ void bottom_local(const QueueDev& q, RayLocal& L, int i, double depth
     double ndir[3] = {L.c.nd[0], L.c.nd[1], L.c.nd[2]};
     double c = L.c.c;
     double c2 = c * c;
-    double nrm[3] = {B.normal[0], B.normal[1], B.normal[2]};
-    double bottom_rho = boundary_height(B, position[1], position[2]);
+    double nrm[3];
+    double bottom_rho = boundary_height_normal(B, position[1], position[2], nrm);
     double height_water = position[0] - bottom_rho;
     const double TOO_SHALLOW = 300.0 * q.dt;
     if ((q.R - bottom_rho) < TOO_SHALLOW) shallow = true;
@@ -387,10 +396,7 @@ __device__ void bottom_local(const QueueDev& q, RayLocal& L, int i, double depth
     const double time_water = fmax(0.0, dot_water / dot_full);
 
     collision_local(q, L, time_water, position, ndir, &c);
-    bottom_rho = boundary_height(B, position[1], position[2]);
-    nrm[0] = B.normal[0];
-    nrm[1] = B.normal[1];
-    nrm[2] = B.normal[2];
+    bottom_rho = boundary_height_normal(B, position[1], position[2], nrm);
     if (shallow) {
         N = sqrt(nrm[1] * nrm[1] + nrm[2] * nrm[2]);
         nrm[0] = 0.0;
@@ -485,6 +491,8 @@ __device__ __forceinline__ void ray_from(const double* src, RayS& y) {
 }
 
 }  // namespace
+
+namespace WQ3D_KERNEL_NS {
 
 /* ------------------------------------------------------------------ */
 /* start-up: wave_queue ctor (wave_queue.cc:83-85) for one ray         */
@@ -768,6 +776,9 @@ __global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp
     }
 }
 
+}  // namespace WQ3D_KERNEL_NS
+
+#if !WQ3D_STEP_KERNELS_ONLY
 /* ------------------------------------------------------------------ */
 /* CPA search (wave_queue.cc:351-488)                                  */
 /* ------------------------------------------------------------------ */
@@ -1763,27 +1774,26 @@ __global__ void k_sound_speed(OceanDev oc, double R, int n, const double* rho,
                               double* g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double cc, gr;
-    sound_speed(oc.prof, R, rho[i], &cc, &gr);
+    double cc, gg[3];
+    sound_speed(oc.prof, R, rho[i], theta[i], phi[i], &cc, gg);
     c[i] = cc;
     if (g) {
-        g[i] = gr;
-        g[n + i] = 0.0;
-        g[2 * n + i] = 0.0;
+        g[i] = gg[0];
+        g[n + i] = gg[1];
+        g[2 * n + i] = gg[2];
     }
-    (void)theta;
-    (void)phi;
 }
 
 __global__ void k_height(BoundaryDev b, int n, const double* theta, const double* phi,
                          double* h, double* nrm) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    h[i] = boundary_height(b, theta[i], phi[i]);
+    double nn[3];
+    h[i] = boundary_height_normal(b, theta[i], phi[i], nn);
     if (nrm) {
-        nrm[i] = b.normal[0];
-        nrm[n + i] = b.normal[1];
-        nrm[2 * n + i] = b.normal[2];
+        nrm[i] = nn[0];
+        nrm[n + i] = nn[1];
+        nrm[2 * n + i] = nn[2];
     }
 }
 
@@ -1807,5 +1817,7 @@ __global__ void k_reflect_loss(BoundaryDev b, int n, const double* grazing, int 
         if (ph) ph[(size_t)i * nf + f] = p;
     }
 }
+
+#endif  // !WQ3D_STEP_KERNELS_ONLY
 
 }  // namespace wq3d

@@ -16,10 +16,23 @@
 
 #include "../../include/wq3d.h"
 
+/* WQ3D_WITH_GRID=0 compiles the models without the gridded profile and
+ * boundary kinds (they then read as the default kind); the host never
+ * hands such a build an ocean that has a grid. */
+#ifndef WQ3D_WITH_GRID
+#define WQ3D_WITH_GRID 1
+#endif
+
 #ifdef __CUDACC__
 #define WQ_HD __host__ __device__ __forceinline__
+/* Out-of-line device functions: the per-dimension grid interpolation calls
+ * the next dimension 1, 2 or 4 times per interpolation kind, so inlining
+ * the chain would copy the innermost level hundreds of times into every
+ * caller of sound_speed. */
+#define WQ_NOINL __host__ __device__ __noinline__
 #else
 #define WQ_HD inline
+#define WQ_NOINL inline
 #endif
 
 namespace wq3d {
@@ -38,15 +51,288 @@ struct LossDev {
     double rl_den, rl_spd, rl_att, rl_shr, rl_satt;
 };
 
-/* rectilinear grid with up to 3 axes (types/gen_grid.h) */
+/* ------------------------------------------------------------------ */
+/* rectilinear grids (types/gen_grid.h:83-520, gen_grid_utils.h)        */
+/* ------------------------------------------------------------------ */
+struct AxisDev {
+    const double* x;
+    const double* inc;
+    int n;
+    int kind;       /* WQ3D_AXIS_* */
+    double sign;    /* seq_data: -1 for a decreasing axis */
+};
+
 struct GridDev {
     int ndim;
-    const double* axis[3];
-    int n[3];
+    AxisDev ax[3];
     int interp[3];
     int edge[3];
     const double* data;
 };
+
+/* seq_vector::increment clamps its index (seq_vector.h:140-143) */
+WQ_HD double axis_inc(const AxisDev& a, long k) {
+    /* a negative index wraps to a huge size_t there, so it clamps high too */
+    if (k < 0 || k > a.n - 1) k = a.n - 1;
+    return a.inc[k];
+}
+
+/* find_index of seq_linear (seq_linear.h:89-94), seq_log (seq_log.h:88-94)
+ * and seq_data (seq_data.cc:15-36) */
+WQ_HD int axis_find(const AxisDev& a, double v) {
+    if (a.kind == WQ3D_AXIS_LINEAR) {
+        const double f = floor((v - a.x[0]) / a.inc[0]);
+        long k = (long)f;
+        if (k > a.n - 2) k = a.n - 2;
+        if (k < 0) k = 0;
+        return (int)k;
+    }
+    if (a.kind == WQ3D_AXIS_LOG) {
+        const double f = floor(log(v / a.x[0]) / log(a.inc[1] / a.inc[0]));
+        long k = (long)f;
+        if (k > a.n - 2) k = a.n - 2;
+        if (k < 0) k = 0;
+        return (int)k;
+    }
+    const double s = a.sign;
+    v *= s;
+    const int max_index = a.n - 1;
+    if (max_index < 1) return 0;
+    if (v <= s * a.x[0]) return 0;
+    if (v >= s * a.x[max_index - 1]) return max_index - 1;
+    /* first entry whose key exceeds v (std::map::upper_bound), minus one */
+    int lo = 0, hi = a.n; /* keys s*x[] increase */
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (s * a.x[mid] > v) hi = mid; else lo = mid + 1;
+    }
+    return lo - 1;
+}
+
+template <int NDIM, int DIM>
+struct GridInterp;
+
+/* dim < 0: the data point at the corner index (data_grid_compute_offset) */
+template <int NDIM>
+struct GridInterp<NDIM, -1> {
+    WQ_HD static double run(const GridDev& g, const int* index, const double*, double&, double*) {
+        size_t off = (size_t)index[0];
+        for (int d = 1; d < NDIM; ++d) off = (size_t)index[d] + (size_t)g.ax[d].n * off;
+        return g.data[off];
+    }
+};
+
+template <int NDIM, int DIM>
+struct GridInterp {
+    WQ_HD static double nearest(const GridDev& g, const int* index, const double* loc, double& deriv,
+                                double* dv) {
+        double result;
+        double da = 0.0;
+        const int k = index[DIM];
+        const AxisDev& ax = g.ax[DIM];
+        const double u = (loc[DIM] - ax.x[k]) / axis_inc(ax, k);
+        if (u < 0.5) {
+            result = GridInterp<NDIM, DIM - 1>::run(g, index, loc, da, dv);
+        } else {
+            int next[NDIM];
+            for (int d = 0; d < NDIM; ++d) next[d] = index[d];
+            ++next[DIM];
+            result = GridInterp<NDIM, DIM - 1>::run(g, next, loc, da, dv);
+        }
+        if (dv) {
+            dv[DIM] = deriv;
+            if (DIM > 0) dv[DIM > 0 ? DIM - 1 : 0] = da;
+        }
+        return result;
+    }
+
+    WQ_HD static double linear(const GridDev& g, const int* index, const double* loc, double& deriv,
+                               double* dv) {
+        double da = 0.0, db = 0.0;
+        const double a = GridInterp<NDIM, DIM - 1>::run(g, index, loc, da, dv);
+        int next[NDIM];
+        for (int d = 0; d < NDIM; ++d) next[d] = index[d];
+        ++next[DIM];
+        const double b = GridInterp<NDIM, DIM - 1>::run(g, next, loc, db, dv);
+        const int k = index[DIM];
+        const AxisDev& ax = g.ax[DIM];
+        const double h = axis_inc(ax, k);
+        const double u = (loc[DIM] - ax.x[k]) / h;
+        const double result = a * (1.0 - u) + b * u;
+        if (dv) {
+            deriv = (b - a) / h;
+            dv[DIM] = deriv;
+            if (DIM > 0) dv[DIM > 0 ? DIM - 1 : 0] = da * (1.0 - u) + db * u;
+        }
+        return result;
+    }
+
+    /* harmonic mean slope (gen_grid_utils.h derivative<T>::compute) */
+    WQ_HD static void harmonic(double d0, double d1, double dd0, double dd1, double w0, double w1,
+                               bool deriv, double& m, double& dm) {
+        if (d0 * d1 > 0.0) m = (w0 + w1) / (w0 / d0 + w1 / d1);
+        if (deriv && dd0 * dd1 > 0.0) dm = (w0 + w1) / (w0 / dd0 + w1 / dd1);
+    }
+    /* end_point_derivative<T>::compute for scalars */
+    WQ_HD static void end_point(double d0, double d1, double dd0, double dd1, bool deriv, double& m,
+                                double& dm) {
+        if (m * d0 < 0.0) {
+            m = 0.0;
+        } else if ((d0 * d1 < 0.0) && (fabs(m) > fabs(3.0 * d1))) {
+            m = 3.0 * d1;
+        }
+        if (deriv) {
+            if (dm * dd0 < 0.0) {
+                dm = 0.0;
+            } else if ((dd0 * dd1 < 0.0) && (fabs(dm) > fabs(3.0 * dd0))) {
+                dm = 3.0 * dd0;
+            }
+        } else {
+            dm = 0.0;
+        }
+    }
+
+    /* gen_grid.h pchip, keeping the end-point slope "(2.0 + h1 + h2)" and
+     * the slope2 weights built from h0 (gen_grid.h:458-488) */
+    WQ_HD static double pchip(const GridDev& g, const int* index, const double* loc, double& deriv,
+                              double* dv) {
+        const AxisDev& ax = g.ax[DIM];
+        const int kmin = 1;
+        const int kmax = ax.n - 3;
+        double y0, y1, y2, y3, dy0 = 0.0, dy1 = 0.0, dy2 = 0.0, dy3 = 0.0;
+        const int k = index[DIM];
+        y1 = GridInterp<NDIM, DIM - 1>::run(g, index, loc, dy1, dv);
+        if (k >= kmin) {
+            int prev[NDIM];
+            for (int d = 0; d < NDIM; ++d) prev[d] = index[d];
+            --prev[DIM];
+            y0 = GridInterp<NDIM, DIM - 1>::run(g, prev, loc, dy0, dv);
+        } else {
+            y0 = y1;
+            dy0 = dy1;
+        }
+        int next[NDIM];
+        for (int d = 0; d < NDIM; ++d) next[d] = index[d];
+        ++next[DIM];
+        y2 = GridInterp<NDIM, DIM - 1>::run(g, next, loc, dy2, dv);
+        if (k <= kmax) {
+            int last[NDIM];
+            for (int d = 0; d < NDIM; ++d) last[d] = next[d];
+            ++last[DIM];
+            y3 = GridInterp<NDIM, DIM - 1>::run(g, last, loc, dy3, dv);
+        } else {
+            y3 = y2;
+            dy3 = dy2;
+        }
+        const double h0 = axis_inc(ax, (long)k - 1);
+        const double h1 = axis_inc(ax, k);
+        const double h2 = axis_inc(ax, (long)k + 1);
+        const double h1_2 = h1 * h1;
+        const double h1_3 = h1_2 * h1;
+        const double s = loc[DIM] - ax.x[k];
+        const double s_2 = s * s, s_3 = s_2 * s;
+        const double sh_minus = s - h1;
+        const double sh_term = 3.0 * h1 * s_2 - 2.0 * s_3;
+        const double deriv0 = (y1 - y0) / h0;
+        const double deriv1 = (y2 - y1) / h1;
+        const double deriv2 = (y3 - y2) / h2;
+        double dderiv0 = 0.0, dderiv1 = 0.0, dderiv2 = 0.0;
+        if (dv) {
+            dderiv0 = (dy1 - dy0) / h0;
+            dderiv1 = (dy2 - dy1) / h1;
+            dderiv2 = (dy3 - dy2) / h2;
+        }
+        double slope1 = 0.0, dslope1 = 0.0;
+        if (k >= kmin) {
+            const double w0 = 2.0 * h1 + h0;
+            const double w1 = h1 + 2.0 * h0;
+            harmonic(deriv0, deriv1, dderiv0, dderiv1, w0, w1, dv != nullptr, slope1, dslope1);
+        } else {
+            slope1 = ((2.0 + h1 + h2) * deriv1 - h1 * deriv2) / (h1 + h2);
+            dslope1 = ((2.0 + h1 + h2) * dderiv1 - h1 * dderiv2) / (h1 + h2);
+            end_point(deriv1, deriv2, dderiv1, dderiv2, dv != nullptr, slope1, dslope1);
+        }
+        double slope2 = 0.0, dslope2 = 0.0;
+        if (k <= kmax) {
+            const double w1 = 2.0 * h1 + h0;
+            const double w2 = h1 + 2.0 * h0;
+            harmonic(deriv1, deriv2, dderiv1, dderiv2, w1, w2, dv != nullptr, slope2, dslope2);
+        } else {
+            slope2 = ((2.0 + h1 + h2) * deriv1 - h1 * deriv0) / (h1 + h0);
+            dslope2 = ((2.0 + h1 + h2) * dderiv1 - h1 * dderiv0) / (h1 + h0);
+            end_point(deriv1, deriv0, dderiv1, dderiv0, dv != nullptr, slope2, dslope2);
+        }
+        const double result = y2 * sh_term / h1_3 + y1 * (h1_3 - sh_term) / h1_3 +
+                              slope2 * s_2 * sh_minus / h1_2 +
+                              slope1 * s * sh_minus * sh_minus / h1_2;
+        if (dv) {
+            const double v = s / h1;
+            deriv = slope1 * (1.0 - v) + slope2 * v;
+            dv[DIM] = deriv;
+            if (DIM > 0)
+                dv[DIM > 0 ? DIM - 1 : 0] = dy2 * sh_term / h1_3 + dy1 * (h1_3 - sh_term) / h1_3 +
+                                            dslope2 * s_2 * sh_minus / h1_2 +
+                                            dslope1 * s * sh_minus * sh_minus / h1_2;
+        }
+        return result;
+    }
+
+    WQ_NOINL static double run(const GridDev& g, const int* index, const double* loc, double& deriv,
+                               double* dv) {
+        switch (g.interp[DIM]) {
+            case WQ3D_INTERP_NEAREST:
+                return nearest(g, index, loc, deriv, dv);
+            case WQ3D_INTERP_PCHIP:
+                return pchip(g, index, loc, deriv, dv);
+            default:
+                return linear(g, index, loc, deriv, dv);
+        }
+    }
+};
+
+/* gen_grid::interpolate (gen_grid.h:83-123): edge limiting, find_index on
+ * each axis, then the recursive interpolation.  dv may be null. */
+template <int NDIM>
+WQ_HD double grid_interpolate(const GridDev& g, const double* location, double* dv) {
+    int index[NDIM];
+    double loc[NDIM];
+    for (int d = 0; d < NDIM; ++d) loc[d] = location[d];
+    for (int d = 0; d < NDIM; ++d) {
+        const AxisDev& ax = g.ax[d];
+        if (g.edge[d]) {
+            const double a = ax.x[0];
+            const double b = ax.x[ax.n - 1];
+            const double sign = (ax.inc[0] < 0) ? -1.0 : 1.0;
+            const double dd = loc[d] * sign;
+            if (dd <= a * sign) {
+                loc[d] = a;
+                index[d] = 0;
+            } else if (dd >= b * sign) {
+                loc[d] = b;
+                index[d] = ax.n - 2;
+            } else {
+                index[d] = axis_find(ax, loc[d]);
+            }
+        } else {
+            index[d] = axis_find(ax, loc[d]);
+        }
+    }
+    double dresult = 0.0;
+    return GridInterp<NDIM, NDIM - 1>::run(g, index, loc, dresult, dv);
+}
+
+#if WQ3D_WITH_GRID
+static WQ_NOINL double grid_eval(const GridDev& g, const double* location, double* dv) {
+    switch (g.ndim) {
+        case 1:
+            return grid_interpolate<1>(g, location, dv);
+        case 2:
+            return grid_interpolate<2>(g, location, dv);
+        default:
+            return grid_interpolate<3>(g, location, dv);
+    }
+}
+#endif  // WQ3D_WITH_GRID
 
 struct BoundaryDev {
     int kind;
@@ -80,11 +366,22 @@ struct OceanDev {
 /* ------------------------------------------------------------------ */
 /* sound speed: profile_{linear,munk,catenary,n2}.cc + adjust_speed     */
 /* ------------------------------------------------------------------ */
-WQ_HD void sound_speed(const ProfileDev& pr, double R, double rho,
-                       double* c, double* g_rho) {
+WQ_HD void sound_speed(const ProfileDev& pr, double R, double rho, double theta,
+                       double phi, double* c, double* g) {
     const double alt = rho - R;
-    double cc, gr;
+    double cc, gr, gt = 0.0, gp = 0.0;
     switch (pr.kind) {
+#if WQ3D_WITH_GRID
+        case WQ3D_PROFILE_GRID: { /* profile_grid.h:68-130 */
+            const double loc[3] = {rho, theta, phi};
+            double dv[3] = {0.0, 0.0, 0.0};
+            cc = grid_eval(pr.grid, loc, dv);
+            gr = dv[0];
+            if (pr.grid.ndim >= 2) gt = dv[1];
+            if (pr.grid.ndim >= 3) gp = dv[2];
+            break;
+        }
+#endif
         case WQ3D_PROFILE_LINEAR: { /* profile_linear.cc:14-40 */
             const double z = -alt;
             if (z < pr.p[2]) {
@@ -123,7 +420,9 @@ WQ_HD void sound_speed(const ProfileDev& pr, double R, double rho,
         cc = cc * rho / R;
     }
     *c = cc;
-    *g_rho = gr;
+    g[0] = gr;
+    g[1] = gt;
+    g[2] = gp;
 }
 
 /* ------------------------------------------------------------------ */
@@ -134,7 +433,45 @@ WQ_HD double boundary_height(const BoundaryDev& b, double theta, double phi) {
         return b.height * (1.0 + b.slope_a * (phi - b.loc_phi)) *
                (1.0 + b.slope_b * (theta - b.loc_theta));
     }
+#if WQ3D_WITH_GRID
+    if (b.kind == WQ3D_BOUNDARY_GRID) { /* boundary_grid.h:150-196 */
+        const double loc[2] = {theta, phi};
+        return grid_eval(b.grid, loc, nullptr);
+    }
+#endif
     return b.height;
+}
+
+/* boundary height and unit normal (boundary_model::height with a normal):
+ * flat and slope normals are constant; a grid's comes from the height
+ * gradient (boundary_grid.h:150-196) */
+WQ_HD double boundary_height_normal(const BoundaryDev& b, double theta, double phi, double* nrm) {
+#if WQ3D_WITH_GRID
+    if (b.kind == WQ3D_BOUNDARY_GRID) {
+        const double loc[2] = {theta, phi};
+        double grad[2] = {0.0, 0.0};
+        const double rho = grid_eval(b.grid, loc, grad);
+        if (b.grid.ndim == 1) {
+            const double t = -grad[0] / rho;
+            const double N = sqrt(1 + t * t);
+            nrm[0] = 1.0 / N;
+            nrm[1] = t / N;
+            nrm[2] = 0.0;
+        } else {
+            const double t = -grad[0] / rho;
+            const double p = -grad[1] / (rho * sin(theta));
+            const double N = sqrt(1 + t * t + p * p);
+            nrm[0] = 1.0 / N;
+            nrm[1] = t / N;
+            nrm[2] = p / N;
+        }
+        return rho;
+    }
+#endif
+    nrm[0] = b.normal[0];
+    nrm[1] = b.normal[1];
+    nrm[2] = b.normal[2];
+    return boundary_height(b, theta, phi);
 }
 
 /* ------------------------------------------------------------------ */

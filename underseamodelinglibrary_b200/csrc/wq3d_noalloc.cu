@@ -83,13 +83,12 @@ int staging_address(double** out) {
 __global__ void k_sound_speed_noalloc(OceanDev oc, double R, int n, double* pts) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const double rho = pts[i];
-    double c, gr;
-    sound_speed(oc.prof, R, rho, &c, &gr);
+    double c, g[3];
+    sound_speed(oc.prof, R, pts[i], pts[n + i], pts[2 * (size_t)n + i], &c, g);
     pts[3 * (size_t)n + i] = c;
-    pts[4 * (size_t)n + i] = gr;
-    pts[5 * (size_t)n + i] = 0.0;
-    pts[6 * (size_t)n + i] = 0.0;
+    pts[4 * (size_t)n + i] = g[0];
+    pts[5 * (size_t)n + i] = g[1];
+    pts[6 * (size_t)n + i] = g[2];
 }
 
 }  // namespace
@@ -113,8 +112,14 @@ extern "C" int wq3d_ocean_sound_speed_noalloc(const wq3d_ocean* ocean, double ea
     if (rc) return rc;
     const size_t bytes = n * sizeof(double);
     cudaError_t e = cudaMemcpy(pts, rho, bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && theta) e = cudaMemcpy(pts + n, theta, bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && phi) e = cudaMemcpy(pts + 2 * n, phi, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        if (theta) e = cudaMemcpy(pts + n, theta, bytes, cudaMemcpyHostToDevice);
+        else e = cudaMemset(pts + n, 0, bytes);
+    }
+    if (e == cudaSuccess) {
+        if (phi) e = cudaMemcpy(pts + 2 * n, phi, bytes, cudaMemcpyHostToDevice);
+        else e = cudaMemset(pts + 2 * n, 0, bytes);
+    }
     if (e != cudaSuccess) return noalloc_fail(WQ3D_ERR_CUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
     k_sound_speed_noalloc<<<(unsigned)((n + 127) / 128), 128>>>(oc, earth_radius, (int)n, pts);
     e = cudaGetLastError();

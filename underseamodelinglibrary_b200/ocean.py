@@ -11,7 +11,44 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from .types import earth_radius
+from .types import earth_radius, seq_linear, seq_log
+
+
+class data_grid:
+    """N-dimensional rectilinear grid (types/data_grid.h, gen_grid.h) of
+    up to three axes; data is row-major with the last axis fastest.
+    Interpolation defaults to linear with edge limiting on every axis
+    (data_grid.h:315-316)."""
+    NEAREST, LINEAR, PCHIP = _abi.INTERP_NEAREST, _abi.INTERP_LINEAR, _abi.INTERP_PCHIP
+
+    def __init__(self, axes, data):
+        self.axes = list(axes)
+        self.data = np.ascontiguousarray(np.asarray(data, dtype=np.float64).reshape(
+            [a.size() for a in self.axes]))
+        self._interp = [_abi.INTERP_LINEAR] * len(self.axes)
+        self._edge = [True] * len(self.axes)
+
+    def interp_type(self, dim, kind):
+        self._interp[dim] = int(kind)
+
+    def edge_limit(self, dim, flag):
+        self._edge[dim] = bool(flag)
+
+    def fill(self, g, keep):
+        g.ndim = len(self.axes)
+        for k, a in enumerate(self.axes):
+            x = np.ascontiguousarray(a.data, dtype=np.float64)
+            inc = np.ascontiguousarray(a.increments, dtype=np.float64)
+            keep += [x, inc]
+            g.axis[k] = _abi.as_dp(x)
+            g.axis_inc[k] = _abi.as_dp(inc)
+            g.axis_size[k] = a.size()
+            g.axis_kind[k] = (_abi.AXIS_LINEAR if isinstance(a, seq_linear)
+                              else _abi.AXIS_LOG if isinstance(a, seq_log) else _abi.AXIS_DATA)
+            g.interp[k] = self._interp[k]
+            g.edge_limit[k] = 1 if self._edge[k] else 0
+        keep.append(self.data)
+        g.data = _abi.as_dp(self.data)
 
 
 class attenuation_thorp:
@@ -99,6 +136,20 @@ class profile_n2(profile_model):
     def __init__(self, c0, g0, attmodel=None):
         super().__init__(attmodel)
         self.params = (float(c0), float(g0), 0.0, 0.0)
+
+
+class profile_grid(profile_model):
+    """profile_grid<N> (ocean/profile_grid.h:68-130): sound speed on a grid
+    over (rho[, theta[, phi]])."""
+    kind = _abi.PROFILE_GRID
+
+    def __init__(self, grid, attmodel=None):
+        super().__init__(attmodel)
+        self.grid = grid
+
+    def fill(self, d, keep=None):
+        super().fill(d)
+        self.grid.fill(d.grid, keep if keep is not None else [])
 
 
 class reflect_loss_constant:
@@ -190,6 +241,20 @@ class boundary_slope(boundary_model):
         d.lng_slope = self.lng_slope
 
 
+class boundary_grid(boundary_model):
+    """boundary_grid<N> (ocean/boundary_grid.h:40-204): boundary rho on a
+    grid over theta[, phi]; Rayleigh sand loss unless one is given."""
+    kind = _abi.BOUNDARY_GRID
+
+    def __init__(self, grid, reflect_loss=None):
+        super().__init__(reflect_loss)
+        self.grid = grid
+
+    def fill(self, d, keep=None):
+        super().fill(d)
+        self.grid.fill(d.grid, keep if keep is not None else [])
+
+
 class ocean_model:
     """ocean_model(surface, bottom, profile) (ocean/ocean_model.h:31-60)."""
 
@@ -210,11 +275,16 @@ class ocean_model:
         return self._profile
 
     def descriptor(self):
+        """The wq3d_ocean_desc; the arrays it points into stay alive as
+        long as this ocean_model does."""
         d = _abi.wq3d_ocean_desc()
         d.earth_radius = self._bottom._radius
-        self._profile.fill(d.profile)
-        self._surface.fill(d.surface)
-        self._bottom.fill(d.bottom)
+        self._keep = []
+        for model, sub in ((self._profile, d.profile), (self._surface, d.surface), (self._bottom, d.bottom)):
+            if isinstance(model, (profile_grid, boundary_grid)):
+                model.fill(sub, self._keep)
+            else:
+                model.fill(sub)
         # one construction radius serves both boundaries: build them under
         # the same wposition earth radius, as every reference caller does
         return d

@@ -16,9 +16,9 @@ import math
 import numpy as np
 
 from . import types as T
-from .ocean import (attenuation_constant, boundary_flat, boundary_slope, ocean_model,
-                    profile_linear, profile_munk, reflect_loss_constant,
-                    reflect_loss_rayleigh)
+from .ocean import (attenuation_constant, boundary_flat, boundary_grid, boundary_slope,
+                    data_grid, ocean_model, profile_grid, profile_linear, profile_munk,
+                    reflect_loss_constant, reflect_loss_rayleigh)
 from ._abi import HYBRID_GAUSSIAN
 
 
@@ -161,6 +161,91 @@ def linear_slope_rayleigh(num_de=1801, num_az=91, n_range=32, n_depth=32, time_m
     return _pack(ocean=ocean, freq=freq, pos=src, de=T.seq_rayfan(-90.0, 90.0, num_de), az=az,
                  dt=0.05, targets=tgt, time_max=time_max,
                  name="linear_slope_rayleigh_%dx%d" % (num_de, num_az))
+
+
+def _smooth(field, sigmas):
+    """Separable Gaussian smoothing (sigma in nodes per axis, reflecting
+    edges)."""
+    out = np.asarray(field, dtype=np.float64)
+    for ax, sig in enumerate(sigmas):
+        if sig <= 0:
+            continue
+        half = int(math.ceil(3.0 * sig))
+        k = np.exp(-0.5 * (np.arange(-half, half + 1) / sig) ** 2)
+        k /= k.sum()
+        pad = [(0, 0)] * out.ndim
+        pad[ax] = (half, half)
+        padded = np.pad(out, pad, mode="reflect" if out.shape[ax] > half else "edge")
+        out = np.apply_along_axis(lambda v: np.convolve(v, k, mode="valid"), ax, padded)
+    return out
+
+
+def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_lng=20,
+                  n_bathy=100, ssp_std=5.0, corr_h=50e3, corr_v=300.0, depth_min=1000.0,
+                  depth_max=5000.0):
+    """Gridded environment over span x span degrees centred on (lat0, lng0):
+
+    * profile_grid<3> on (rho, theta, phi) with n_depth nodes 0-5000 m x
+      n_lat x n_lng: the Munk profile plus a Gaussian random field of
+      ``ssp_std`` m/s with ``corr_h`` horizontal and ``corr_v`` vertical
+      correlation lengths; pchip in depth, linear across;
+    * boundary_grid<2> bottom on n_bathy x n_bathy (theta, phi) nodes:
+      Gaussian-smoothed random relief scaled to depth_min..depth_max, pchip
+      both ways, Rayleigh sand loss (the boundary_grid default).
+
+    Inputs are seeded synthetic fields (no data files)."""
+    R = T.earth_radius()
+    th0 = math.radians(90.0 - (lat0 + span / 2))
+    ph0 = math.radians(lng0 - span / 2)
+    dz = 5000.0 / (n_depth - 1)
+    rho_ax = T.seq_linear(R, -dz, n_depth)
+    th_ax = T.seq_linear(th0, math.radians(span) / (n_lat - 1), n_lat)
+    ph_ax = T.seq_linear(ph0, math.radians(span) / (n_lng - 1), n_lng)
+    z = np.arange(n_depth) * dz
+    zt = 2.0 * (z - 1300.0) / 1300.0
+    munk = 1500.0 * (1.0 + 0.00737 * (zt - 1.0 + np.exp(-zt)))
+    dx = R * math.radians(span) / (n_lat - 1)
+    noise = _smooth(rng.standard_normal((n_depth, n_lat, n_lng)),
+                    (corr_v / dz, corr_h / dx, corr_h / dx))
+    noise *= ssp_std / max(noise.std(), 1e-30)
+    ssp = data_grid([rho_ax, th_ax, ph_ax], munk[:, None, None] + noise)
+    ssp.interp_type(0, data_grid.PCHIP)
+    bt_ax = T.seq_linear(th0, math.radians(span) / (n_bathy - 1), n_bathy)
+    bp_ax = T.seq_linear(ph0, math.radians(span) / (n_bathy - 1), n_bathy)
+    relief = _smooth(rng.standard_normal((n_bathy, n_bathy)), (n_bathy / 12.0, n_bathy / 12.0))
+    relief = (relief - relief.min()) / max(relief.max() - relief.min(), 1e-30)
+    bathy = data_grid([bt_ax, bp_ax], R - (depth_min + (depth_max - depth_min) * relief))
+    bathy.interp_type(0, data_grid.PCHIP)
+    bathy.interp_type(1, data_grid.PCHIP)
+    return ocean_model(boundary_flat(), boundary_grid(bathy), profile_grid(ssp))
+
+
+def random_targets(rng, src, n, max_range=100e3, depth=(10.0, 4000.0)):
+    """n targets at uniform random bearing, range up to max_range and depth
+    in the given interval, as a 1 x n wposition."""
+    tgt = T.wposition(1, n, 0.0, 0.0, 0.0)
+    for k in range(n):
+        p = T.wposition1(src, float(rng.uniform(1e3, max_range)), float(rng.uniform(0.0, 2 * math.pi)))
+        tgt.latitude(0, k, p.latitude())
+        tgt.longitude(0, k, p.longitude())
+        tgt.altitude(0, k, -float(rng.uniform(*depth)))
+    return tgt
+
+
+def gridded_munk(seed=1, num_de=91, num_az=13, n_targets=64, time_max=30.0, src_depth=100.0,
+                 dt=0.1, freq=None, **grid_kw):
+    """One instance of the batched gridded workload: gridded_ocean() around
+    45N 45W, source ``src_depth`` m deep, tangent-spaced D/E fan x AZ 0..360
+    deg, 64 random targets at 10-4000 m depth within 100 km."""
+    T.compute_earth_radius(45.0)
+    rng = np.random.default_rng(seed)
+    ocean = gridded_ocean(rng, **grid_kw)
+    src = T.wposition1(45.0, -45.0, -float(src_depth))
+    tgt = random_targets(rng, src, n_targets)
+    az = T.seq_linear(0.0, 360.0 / (num_az - 1), num_az) if num_az > 1 else T.seq_linear(0.0, 0.0, 1)
+    return _pack(ocean=ocean, freq=freq or T.seq_log(1000.0, 1.0, 1), pos=src,
+                 de=T.seq_rayfan(-90.0, 90.0, num_de), az=az, dt=dt, targets=tgt, time_max=time_max,
+                 name="gridded_munk_%dx%d" % (num_de, num_az))
 
 
 def build_queue(sc, queue_cls, **kw):
