@@ -172,6 +172,16 @@ int wq3d_ocean_reflect_loss(const wq3d_ocean* ocean, int which, size_t n,
                             size_t nf, const double* freq, double* amplitude,
                             double* phase);
 
+/* Evaluates the profile's sea-water absorption (dB) over the distance
+ * travelled at n points for nf frequencies on the GPU: Thorp
+ * (ocean/attenuation_thorp.cc:14-36) or constant
+ * (ocean/attenuation_constant.cc:14-25).  Replaces
+ * attenuation_model::attenuation (ocean/attenuation_model.h:45-48).
+ * attenuation holds n*nf values, point-major. */
+int wq3d_ocean_attenuation(const wq3d_ocean* ocean, double earth_radius, size_t n,
+                           const double* rho, const double* distance, size_t nf,
+                           const double* freq, double* attenuation);
+
 /* Largest number of points one wq3d_ocean_sound_speed_noalloc call takes. */
 #define WQ3D_NOALLOC_MAX_POINTS 16384
 

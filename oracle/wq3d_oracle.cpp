@@ -2126,6 +2126,27 @@ int oracle_height(const wq3d_ocean_desc* od, int which, size_t n,
     return WQ3D_OK;
 }
 
+/* attenuation_model::attenuation (attenuation_thorp.cc:14-36,
+ * attenuation_constant.cc:14-25) at n points, point-major output */
+int oracle_attenuation(const wq3d_ocean_desc* od, double R, size_t n, const double* rho,
+                       const double* distance, size_t nf, const double* freq, double* atten) {
+    for (size_t k = 0; k < nf; ++k) {
+        double alpha = 0.0;
+        if (od->profile.attenuation != WQ3D_ATTEN_CONSTANT) {
+            double F2 = freq[k];
+            F2 = 1e-6 * F2 * F2;
+            alpha = 1e-3 * (3.3e-3 + F2 * (0.11 / (1.0 + F2) + 44.0 / (4100.0 + F2) + 3.0e-4)) /
+                    (1.0 - 5.88264e-6 * 1000.0);
+        }
+        for (size_t i = 0; i < n; ++i) {
+            atten[i * nf + k] = (od->profile.attenuation == WQ3D_ATTEN_CONSTANT)
+                                    ? od->profile.attenuation_coef * distance[i] * freq[k]
+                                    : distance[i] * alpha * (1.0 + 5.88264e-6 * (rho[i] - R));
+        }
+    }
+    return WQ3D_OK;
+}
+
 int oracle_reflect_loss(const wq3d_ocean_desc* od, int which, size_t n,
                         const double* grazing, size_t nf, const double* freq,
                         double* amp, double* phase) {

@@ -39,6 +39,8 @@ SIGS = {
     "oracle_height": (C.c_int, [C.POINTER(_abi.wq3d_ocean_desc), C.c_int, C.c_size_t, dp, dp, dp, dp, dp]),
     "oracle_reflect_loss": (C.c_int, [C.POINTER(_abi.wq3d_ocean_desc), C.c_int, C.c_size_t, dp,
                                       C.c_size_t, dp, dp, dp]),
+    "oracle_attenuation": (C.c_int, [C.POINTER(_abi.wq3d_ocean_desc), C.c_double, C.c_size_t, dp, dp,
+                                     C.c_size_t, dp, dp]),
     "oracle_last_error_string": (C.c_char_p, []),
 }
 
@@ -79,10 +81,27 @@ class OracleQueue:
             self._q = None
 
     def set_thresholds(self, intensity=300.0, max_bottom=999, max_surface=999, max_caustic=999,
-                       max_upper=999, max_lower=999):
-        t = _abi.wq3d_thresholds(intensity, 300.0, max_bottom, max_surface, max_caustic,
+                       max_upper=999, max_lower=999, eigenverb=300.0):
+        self._thresh = dict(intensity=intensity, max_bottom=max_bottom, max_surface=max_surface,
+                            max_caustic=max_caustic, max_upper=max_upper, max_lower=max_lower,
+                            eigenverb=eigenverb)
+        t = _abi.wq3d_thresholds(intensity, eigenverb, max_bottom, max_surface, max_caustic,
                                  max_upper, max_lower)
         _check(self._lib.oracle_queue_set_thresholds(self._q, C.byref(t)))
+
+    def _set_one(self, name, value):
+        kw = dict(getattr(self, "_thresh", {}))
+        kw[name] = value
+        self.set_thresholds(**kw)
+
+    def max_bottom(self, v):
+        self._set_one("max_bottom", int(v))
+
+    def max_surface(self, v):
+        self._set_one("max_surface", int(v))
+
+    def max_caustic(self, v):
+        self._set_one("max_caustic", int(v))
 
     def step(self, n=1):
         _check(self._lib.oracle_queue_step(self._q, int(n)))

@@ -175,6 +175,38 @@ def test_reflect_flat_parity(engine):
         assert abs(e[0] - (k + 1) * 7.450560973) < 1e-4
 
 
+def test_reflect_slope_known_answers(engine):
+    """reflection_test.cc:283-390 on the engine, stepping one step at a
+    time: bottom bounces off the 1 deg slope turn D/E by 2 deg, surface
+    bounces only flip it; the final fronts match the oracle"""
+    from test_oracle_kats import _de_of
+    sc = S.reflect_slope()
+    q = S.build_queue(sc, u.wave_queue)
+    old_de = sc["de"][0]
+    bounces = 0
+    while q.time() < sc["time_max"]:
+        q.step()
+        de = _de_of(q.curr())
+        if old_de * de < 0.0:
+            assert abs((2.0 if old_de < 0.0 else 0.0) - (de + old_de)) < 0.001
+            bounces += 1
+        old_de = de
+    assert bounces >= 4
+    o = S.build_queue(sc, OracleQueue)
+    o.run(sc["time_max"])
+    assert q.time() == o.time()
+    compare_fronts(q.curr(), o.curr(), rel=1e-9)
+
+
+def test_bounce_threshold_parity(engine):
+    """reflection_test.cc:597-661 eigenray half: bounce limits applied, and
+    the eigenrays equal the oracle's"""
+    q, o = run_pair(S.bounce_threshold())
+    eng = q.take_eigenrays()
+    assert eng and max(r.bottom for r in eng) <= 5 and max(r.surface for r in eng) <= 3
+    compare_eigenrays(eng, o.take_eigenrays())
+
+
 def test_munk_flat_full_parity(engine):
     """The 181 x 37 Munk workload, 100 targets, 600 steps, against the oracle."""
     q, o = run_pair(S.munk_flat())
@@ -276,6 +308,17 @@ def test_ocean_point_evaluations(engine):
     lib.oracle_height(C.byref(od), 1, 51, _abi.as_dp(z), _abi.as_dp(th), _abi.as_dp(ph), _abi.as_dp(ho),
                       _abi.as_dp(no))
     assert np.array_equal(h, ho)
+    for prof in (u.profile_linear(1500.0), u.profile_linear(1500.0, u.attenuation_constant(0.003))):
+        oc2 = u.ocean_model(u.boundary_flat(), u.boundary_flat(3000.0), prof)
+        rho = u.earth_radius() - np.linspace(0.0, 3000.0, 31)
+        dist = np.linspace(0.0, 500.0, 31)
+        freq = np.array([10.0, 900.0, 3000.0, 20000.0])
+        a = oc2.attenuation(rho, dist, freq)
+        ao = np.empty(31 * 4)
+        od2 = oc2.descriptor()
+        lib.oracle_attenuation(C.byref(od2), u.earth_radius(), 31, _abi.as_dp(rho), _abi.as_dp(dist), 4,
+                               _abi.as_dp(freq), _abi.as_dp(ao))
+        assert np.allclose(a.ravel(), ao, rtol=1e-14, atol=0)
     graz = np.linspace(0.0, math.pi / 2, 91)
     freq = np.array([100.0, 1000.0, 3000.0])
     for which in (0, 1):

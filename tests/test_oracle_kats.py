@@ -170,3 +170,69 @@ def test_proploss_gaussian():
     for j in range(1, sc["freq"].size()):
         for r, pl in paths.values():
             assert abs(r.intensity[j] - pl) < 2.0
+
+
+def _de_of(front):
+    """wvector1::direction (types/wvector1.cc:79-82) of ray (0, 0)"""
+    nd = [front.ndirection[k][0, 0] for k in range(3)]
+    return math.degrees(math.atan2(nd[0], math.sqrt(nd[1] * nd[1] + nd[2] * nd[2])))
+
+
+def test_reflect_slope():
+    """reflection_test.cc:283-390: at every bounce off the 1 deg slope the
+    D/E changes sign and grows by 2 deg (within 0.001); at every surface
+    bounce it only changes sign"""
+    sc = S.reflect_slope()
+    q = S.build_queue(sc, OracleQueue)
+    old_de = sc["de"][0]
+    bottoms = surfaces = 0
+    while q.time() < sc["time_max"]:
+        q.step()
+        de = _de_of(q.curr())
+        if old_de * de < 0.0:
+            if old_de < 0.0:
+                assert abs(2.0 - (de + old_de)) < 0.001
+                bottoms += 1
+            else:
+                assert abs(old_de + de) < 0.001
+                surfaces += 1
+        old_de = de
+    assert bottoms >= 2 and surfaces >= 2
+
+
+def test_bounce_threshold_eigenrays():
+    """reflection_test.cc:597-661 (eigenray half): no eigenray has more
+    bounces than max_bottom / max_surface"""
+    sc = S.bounce_threshold()
+    q = S.build_queue(sc, OracleQueue)
+    q.run(sc["time_max"])
+    rays = q.take_eigenrays()
+    assert len(rays) > 0
+    assert max(r.bottom for r in rays) <= 5 and max(r.surface for r in rays) <= 3
+    assert any(r.bottom == 5 for r in rays) or any(r.surface == 3 for r in rays)
+
+
+def test_thorp_gsm_table():
+    """ocean/test/attenuation_test.cc:61-97: Thorp over 1 km at 1000 m
+    depth within 20 % of the Generic Sonar Model table above 400 Hz"""
+    import ctypes as C
+    from underseamodelinglibrary_b200 import _abi
+    from oracle_binding import load_oracle
+    u.compute_earth_radius(45.0)
+    R = u.earth_radius()
+    freq = u.seq_log(10.0, 2.0, 14)
+    oc = u.ocean_model(u.boundary_flat(), u.boundary_flat(3000.0), u.profile_linear(1500.0))
+    od = oc.descriptor()
+    out = np.empty(freq.size())
+    f = np.ascontiguousarray(freq.data)
+    assert load_oracle().oracle_attenuation(C.byref(od), R, 1, _abi.as_dp(np.array([R - 1000.0])),
+                                            _abi.as_dp(np.array([1000.0])), freq.size(), _abi.as_dp(f),
+                                            _abi.as_dp(out)) == 0
+    gsm = [0.00006, 0.00017, 0.00047, 0.00134, 0.00379, 0.01125, 0.03615, 0.08538, 0.16469, 0.38326,
+           1.19919, 4.16885, 12.81169, 27.26378]
+    checked = 0
+    for k in range(freq.size()):
+        if freq[k] > 400.0:
+            assert abs(out[k] - gsm[k]) <= 0.2 * abs(gsm[k])
+            checked += 1
+    assert checked == 8

@@ -101,6 +101,17 @@ void setup_boundary(BoundaryDev& b, const wq3d_boundary_desc& d, double R) {
     }
 }
 
+/* attenuation_thorp.cc:14-24: the Thorp coefficient (dB/m at 1000 m
+ * depth) per frequency */
+void thorp_alpha(const double* freq, size_t nf, double* alpha) {
+    for (size_t k = 0; k < nf; ++k) {
+        double F2 = freq[k];
+        F2 = 1e-6 * F2 * F2;
+        alpha[k] = 1e-3 * (3.3e-3 + F2 * (0.11 / (1.0 + F2) + 44.0 / (4100.0 + F2) + 3.0e-4)) /
+                   (1.0 - 5.88264e-6 * 1000.0);
+    }
+}
+
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) {
@@ -557,6 +568,36 @@ int wq3d_ocean_height(const wq3d_ocean* o, int which, size_t n, const double* rh
     return WQ3D_OK;
 }
 
+int wq3d_ocean_attenuation(const wq3d_ocean* o, double earth_radius, size_t n, const double* rho,
+                           const double* distance, size_t nf, const double* freq, double* attenuation) {
+    if (!o || !rho || !distance || !freq || !attenuation) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (n == 0 || nf == 0) return WQ3D_OK;
+    std::vector<double> alpha(nf);
+    thorp_alpha(freq, nf, alpha.data());
+    std::vector<double*> d;
+    int rc = eval_points(n, d, {rho, distance});
+    double *df = nullptr, *dal = nullptr, *da = nullptr;
+    if (!rc && cudaMalloc(&df, nf * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && cudaMalloc(&dal, nf * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && cudaMalloc(&da, n * nf * sizeof(double)) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && cudaMemcpy(df, freq, nf * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    if (!rc && cudaMemcpy(dal, alpha.data(), nf * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = WQ3D_ERR_CUDA;
+    if (!rc) {
+        k_attenuation<<<(unsigned)((n + 127) / 128), 128>>>(o->dev.prof, earth_radius, (int)n, d[0], d[1],
+                                                             (int)nf, df, dal, da);
+        if (cudaGetLastError() != cudaSuccess) rc = WQ3D_ERR_CUDA;
+    }
+    if (!rc && cudaMemcpy(attenuation, da, n * nf * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = WQ3D_ERR_CUDA;
+    for (double* p : d) cudaFree(p);
+    cudaFree(df);
+    cudaFree(dal);
+    cudaFree(da);
+    if (rc) return fail(rc, "wq3d_ocean_attenuation failed");
+    return WQ3D_OK;
+}
+
 int wq3d_ocean_reflect_loss(const wq3d_ocean* o, int which, size_t n, const double* rho,
                             const double* theta, const double* phi, const double* grazing,
                             size_t nf, const double* freq, double* amplitude, double* phase) {
@@ -675,14 +716,8 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         cos_az[i] = std::cos(to_radians(az[i]));
         sin_az[i] = std::sin(to_radians(az[i]));
     }
-    /* attenuation_thorp.cc:14-36 coefficient per frequency */
     std::vector<double> alpha(nf);
-    for (size_t k = 0; k < nf; ++k) {
-        double F2 = freq[k];
-        F2 = 1e-6 * F2 * F2;
-        alpha[k] = 1e-3 * (3.3e-3 + F2 * (0.11 / (1.0 + F2) + 44.0 / (4100.0 + F2) + 3.0e-4)) /
-                   (1.0 - 5.88264e-6 * 1000.0);
-    }
+    thorp_alpha(freq.data(), nf, alpha.data());
     /* targets (wave_queue.cc:54-56, :363-369; spreading_hybrid_gaussian.cc:70-83) */
     std::vector<double> tr(nt), tt(nt), tp(nt), tsin(nt), tR2(nt), t2R(nt), tc(nt), tspread(nt * nf);
     std::vector<uint8_t> tbranch(nt);

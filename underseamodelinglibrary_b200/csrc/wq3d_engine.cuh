@@ -149,6 +149,9 @@ __global__ void k_sound_speed(OceanDev oc, double R, int n, const double* rho,
                               double* c, double* g);
 __global__ void k_height(BoundaryDev b, int n, const double* theta,
                          const double* phi, double* h, double* nrm);
+__global__ void k_attenuation(ProfileDev pr, double R, int n, const double* rho,
+                              const double* dist, int nf, const double* freq,
+                              const double* alpha, double* atten);
 __global__ void k_reflect_loss(BoundaryDev b, int n, const double* grazing,
                                int nf, const double* freq, double* amp,
                                double* ph);

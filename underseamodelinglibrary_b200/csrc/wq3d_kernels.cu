@@ -1797,6 +1797,21 @@ __global__ void k_height(BoundaryDev b, int n, const double* theta, const double
     }
 }
 
+/* attenuation_thorp.cc:29-35 with the per-frequency alpha precomputed on
+ * the host, or attenuation_constant.cc:14-25 */
+__global__ void k_attenuation(ProfileDev pr, double R, int n, const double* rho,
+                              const double* dist, int nf, const double* freq,
+                              const double* alpha, double* atten) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double alt = rho[i] - R;
+    for (int f = 0; f < nf; ++f) {
+        atten[(size_t)i * nf + f] = (pr.atten == WQ3D_ATTEN_CONSTANT)
+                                        ? pr.atten_coef * dist[i] * freq[f]
+                                        : dist[i] * alpha[f] * (1.0 + 5.88264e-6 * alt);
+    }
+}
+
 __global__ void k_reflect_loss(BoundaryDev b, int n, const double* grazing, int nf,
                                const double* freq, double* amp, double* ph) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

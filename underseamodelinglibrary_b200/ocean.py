@@ -334,6 +334,18 @@ class ocean_model:
                                               _abi.as_dp(h), _abi.as_dp(nrm)))
         return h, nrm.reshape(3, n)
 
+    def attenuation(self, rho, distance, freq):
+        """Absorption (dB) over ``distance`` metres at each point, as
+        (n, nf) (attenuation_model::attenuation)."""
+        r = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+        d = np.ascontiguousarray(np.broadcast_to(distance, r.shape), dtype=np.float64)
+        f = np.ascontiguousarray(freq, dtype=np.float64).ravel()
+        out = np.empty(r.size * f.size)
+        lib = _abi.load_engine()
+        _abi.check(lib, lib.wq3d_ocean_attenuation(self.handle(), earth_radius(), r.size, _abi.as_dp(r),
+                                                   _abi.as_dp(d), f.size, _abi.as_dp(f), _abi.as_dp(out)))
+        return out.reshape(r.size, f.size)
+
     def reflect_loss(self, which, grazing, freq):
         g = np.ascontiguousarray(grazing, dtype=np.float64).ravel()
         f = np.ascontiguousarray(freq, dtype=np.float64).ravel()

@@ -116,6 +116,31 @@ def reflect_flat():
                  targets=None, time_max=60.0)
 
 
+def reflect_slope():
+    """waveq3d/test/reflection_test.cc:283-390 -- one ray at dt 1 ms
+    between the surface and a bottom 1000 m deep at 45.1N sloping 1 deg,
+    silt Rayleigh loss."""
+    T.compute_earth_radius(45.0)
+    slope_ref = T.wposition1(45.1, -45.0, 0.0)
+    bottom = boundary_slope(slope_ref, 1000.0, math.radians(1.0), 0.0, reflect_loss_rayleigh("silt"))
+    ocean = ocean_model(boundary_flat(), bottom, profile_linear())
+    return _pack(ocean=ocean, freq=T.seq_log(10.0, 10.0, 1), pos=T.wposition1(45.0, -45.0, 0.0),
+                 de=T.seq_linear(-5.175034664, 0.0, 1), az=T.seq_linear(0.0, 0.0, 1), dt=0.001,
+                 targets=None, time_max=25.0)
+
+
+def bounce_threshold():
+    """waveq3d/test/reflection_test.cc:597-661 -- 181 x 13 fan at the
+    equator, 1000 m flat bottom, max_surface 3 and max_bottom 5."""
+    T.set_earth_radius(6371000.0)
+    ocean = ocean_model(boundary_flat(), boundary_flat(1000.0, reflect_loss_constant(0.0)),
+                        profile_linear(1500.0))
+    return _pack(ocean=ocean, freq=T.seq_log(900.0, 1.0, 1), pos=T.wposition1(0.0, 0.0, -500.0),
+                 de=T.seq_linear(-90.0, 1.0, 90.0), az=T.seq_linear(0.0, 30.0, 360.0), dt=0.1,
+                 targets=T.wposition(1, 1, 0.01, 0.0, -500.0), time_max=10.0,
+                 thresholds=dict(max_surface=3, max_bottom=5))
+
+
 def munk_flat(num_de=181, num_az=37, n_targets=10, time_max=60.0):
     """Plain FP64 workload: Munk profile, 5000 m flat bottom with 0 dB
     loss, source 1000 m at 45N 45W, 10 Hz, tangent-spaced D/E fan from -90
@@ -190,8 +215,8 @@ def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_
       ``ssp_std`` m/s with ``corr_h`` horizontal and ``corr_v`` vertical
       correlation lengths; pchip in depth, linear across;
     * boundary_grid<2> bottom on n_bathy x n_bathy (theta, phi) nodes:
-      Gaussian-smoothed random relief scaled to depth_min..depth_max, pchip
-      both ways, Rayleigh sand loss (the boundary_grid default).
+      Gaussian-smoothed random relief scaled to depth_min..depth_max,
+      linear both ways, Rayleigh sand loss (the boundary_grid default).
 
     Inputs are seeded synthetic fields (no data files)."""
     R = T.earth_radius()
@@ -215,8 +240,6 @@ def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_
     relief = _smooth(rng.standard_normal((n_bathy, n_bathy)), (n_bathy / 12.0, n_bathy / 12.0))
     relief = (relief - relief.min()) / max(relief.max() - relief.min(), 1e-30)
     bathy = data_grid([bt_ax, bp_ax], R - (depth_min + (depth_max - depth_min) * relief))
-    bathy.interp_type(0, data_grid.PCHIP)
-    bathy.interp_type(1, data_grid.PCHIP)
     return ocean_model(boundary_flat(), boundary_grid(bathy), profile_grid(ssp))
 
 
@@ -249,7 +272,11 @@ def gridded_munk(seed=1, num_de=91, num_az=13, n_targets=64, time_max=30.0, src_
 
 
 def build_queue(sc, queue_cls, **kw):
-    """Constructs ``queue_cls(ocean, freq, pos, de, az, dt, targets, type)``."""
+    """Constructs ``queue_cls(ocean, freq, pos, de, az, dt, targets, type)``
+    and applies the scenario's threshold settings."""
     T.set_earth_radius(sc["earth_radius"])
-    return queue_cls(sc["ocean"], sc["freq"], sc["pos"], sc["de"], sc["az"], sc["dt"],
-                     sc["targets"], sc["type"], **kw)
+    q = queue_cls(sc["ocean"], sc["freq"], sc["pos"], sc["de"], sc["az"], sc["dt"],
+                  sc["targets"], sc["type"], **kw)
+    for name, value in sc.get("thresholds", {}).items():
+        getattr(q, name)(value)
+    return q

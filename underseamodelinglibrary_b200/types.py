@@ -47,8 +47,12 @@ class seq_vector:
         return float(self._data[i])
 
     def increment(self, i):
-        """seq_vector::increment clamps the index (seq_vector.h:140-143)."""
-        i = max(0, min(self.size() - 1, int(i)))
+        """seq_vector::increment clamps the index to the last element
+        (seq_vector.h:140-143); its index is unsigned, so -1 clamps there
+        too."""
+        i = int(i)
+        if i < 0 or i > self.size() - 1:
+            i = self.size() - 1
         return float(self._inc[i])
 
     @property

@@ -266,6 +266,10 @@ class wave_queue:
         self._thresh.max_upper = int(v)
         self._push_thresholds()
 
+    def max_lower(self, v):
+        self._thresh.max_lower = int(v)
+        self._push_thresholds()
+
     # ---------------- listeners ----------------
     def _install_callbacks(self):
         if not self._eig_listeners and not self._refl_listeners:
