@@ -132,6 +132,19 @@ typedef struct wq3d_boundary_desc {
     wq3d_reflect_loss_desc loss;
 } wq3d_boundary_desc;
 
+/* Volume scattering layers an ocean may hold (ocean_model::add_volume,
+ * ocean/ocean_model.h:49-52). */
+#define WQ3D_MAX_VOLUME 4
+
+/* A flat volume scattering layer (ocean/volume_flat.h:32-90).  The
+ * propagator only needs its depth; thickness and the constant scattering
+ * strength are kept for the caller's reverberation model. */
+typedef struct wq3d_volume_desc {
+    double depth;              /* m below mean sea level (abs taken)      */
+    double thickness;          /* m                                       */
+    double amplitude;          /* scattering strength, dB                 */
+} wq3d_volume_desc;
+
 typedef struct wq3d_ocean_desc {
     /* value of wposition::earth_radius when the boundaries were built; the
      * reference bakes it into boundary heights at construction time
@@ -140,6 +153,8 @@ typedef struct wq3d_ocean_desc {
     wq3d_profile_desc profile;
     wq3d_boundary_desc surface;
     wq3d_boundary_desc bottom;
+    int num_volume;            /* 0..WQ3D_MAX_VOLUME layers               */
+    wq3d_volume_desc volume[WQ3D_MAX_VOLUME];
 } wq3d_ocean_desc;
 
 typedef struct wq3d_ocean wq3d_ocean;
@@ -280,6 +295,38 @@ typedef struct wq3d_reflection {
     int64_t step;
 } wq3d_reflection;
 
+/* Interfaces an eigenverb can come from (eigenverbs/eigenverb_model.h:27-32):
+ * volume layer k gives 2 + 2k (upper side) and 3 + 2k (lower side). */
+enum { WQ3D_VERB_BOTTOM = 0, WQ3D_VERB_SURFACE = 1, WQ3D_VERB_VOLUME_UPPER = 2,
+       WQ3D_VERB_VOLUME_LOWER = 3 };
+
+/* One eigenverb (eigenverbs/eigenverb_model.h:34-150): a Gaussian beam's
+ * footprint at a boundary or volume layer collision, built by
+ * wave_queue::build_eigenverb (wave_queue.cc:1063-1164).  power[]
+ * (num_freq linear values) travels beside it; frequencies are the queue's. */
+typedef struct wq3d_eigenverb {
+    double travel_time;        /* s                                        */
+    double length;             /* half-length along the beam, m            */
+    double width;              /* half-width across the beam, m            */
+    double position[3];        /* rho, theta, phi of the collision         */
+    double direction;          /* rad, clockwise from true north            */
+    double grazing;            /* rad                                      */
+    double sound_speed;        /* m/s at the collision                     */
+    double source_de;          /* rad                                      */
+    double source_az;          /* rad                                      */
+    int32_t de;                /* de_index                                 */
+    int32_t az;                /* az_index                                 */
+    int32_t surface;
+    int32_t bottom;
+    int32_t caustic;
+    int32_t upper;
+    int32_t lower;
+    int32_t interface_num;     /* WQ3D_VERB_*                               */
+    int64_t step;              /* the wave_queue::step that produced it     */
+    int32_t seq;               /* order of the ray's events in that step   */
+    int32_t pad;
+} wq3d_eigenverb;
+
 /* Listener callbacks, invoked on the calling thread inside wq3d_queue_step
  * in reference order: for every completed step, add_eigenray for each path
  * in (t1, t2, de, az) order (wave_queue.cc:361-373) and then one
@@ -292,6 +339,13 @@ typedef struct wq3d_callbacks {
                          uint64_t run_id);
     void (*check_eigenrays)(void* ctx, double time, uint64_t run_id);
     void (*reflect)(void* ctx, const wq3d_reflection* reflection);
+    /* eigenverb_listener::add_eigenverb (eigenverbs/eigenverb_listener.h:40-41);
+     * for every completed step, in the order the reference's
+     * detect_reflections loop makes them (de, az, then the ray's events),
+     * before that step's add_eigenray calls */
+    void (*add_eigenverb)(void* ctx, const wq3d_eigenverb* verb,
+                          const double* power, size_t num_freq,
+                          int interface_num);
 } wq3d_callbacks;
 
 /* Host copy of one wavefront (waveq3d/wave_front.h:152-258).  Every pointer

@@ -315,6 +315,7 @@ struct Ocean {
     Grid pgrid;
     Boundary surf, bot;
     double build_radius = 6371000.0;
+    std::vector<double> vol_rho; /* volume_flat::_rho per layer (volume_flat.h:32-37) */
 };
 
 /* profile_munk.cc:19-32, profile_linear.cc:14-40, profile_catenary.cc:14-29,
@@ -659,6 +660,10 @@ struct Queue {
     std::vector<Eig> found;
     std::vector<wq3d_reflection> refl;
     bool want_refl = false;
+    bool want_verbs = false;
+    std::vector<wq3d_eigenverb> verbs;
+    std::vector<double> verb_power;
+    int32_t ev_seq = 0;  /* events of the ray being processed this step */
     wq3d_callbacks cb{};
     void* cb_ctx = nullptr;
     uint64_t run_id = 0;
@@ -810,6 +815,12 @@ struct Queue {
         setup_boundary(oc.surf, od->surface, od->earth_radius, true);
         setup_boundary(oc.bot, od->bottom, od->earth_radius, false);
         if (oc.prof.kind == WQ3D_PROFILE_GRID) load_grid(oc.pgrid, od->profile.grid);
+        if (od->num_volume < 0 || od->num_volume > WQ3D_MAX_VOLUME) {
+            g_err = "oracle: bad number of volume layers";
+            return WQ3D_ERR_INVALID;
+        }
+        for (int k = 0; k < od->num_volume; ++k)
+            oc.vol_rho.push_back(od->earth_radius - std::abs(od->volume[k].depth));
         R = qd->earth_radius;
         nde = qd->num_de;
         naz = qd->num_az;
@@ -968,6 +979,8 @@ struct Queue {
     void detect_reflections() {
         for (size_t d = 0; d < nde; ++d) {
             for (size_t a = 0; a < naz; ++a) {
+                ev_seq = 0;
+                detect_volume_scattering(d, a);
                 if (!detect_surface(d, a)) {
                     if (!detect_bottom(d, a)) {
                         detect_vertices(d, a);
@@ -986,6 +999,7 @@ struct Queue {
             if (surface_reflection(d, a)) {
                 next->surface[i] += 1;
                 curr->surface[i] = prev->surface[i] = past->surface[i] = next->surface[i];
+                detect_volume_scattering(d, a);
                 detect_bottom(d, a);
                 return true;
             }
@@ -1003,11 +1017,95 @@ struct Queue {
             if (bottom_reflection(d, a, depth)) {
                 next->bottom[i] += 1;
                 curr->bottom[i] = prev->bottom[i] = past->bottom[i] = next->bottom[i];
+                detect_volume_scattering(d, a);
                 detect_surface(d, a);
                 return true;
             }
         }
         return false;
+    }
+
+    /* wave_queue::detect_volume_scattering (wave_queue.cc:297-345).  The
+     * collision time is measured to the ocean surface, not to the layer,
+     * as in the reference. */
+    void detect_volume_scattering(size_t d, size_t a) {
+        if (!want_verbs) return;
+        const size_t i = idx(d, a);
+        if (above_bounce(curr, i)) return;
+        for (size_t k = 0; k < oc.vol_rho.size(); ++k) {
+            const double height = oc.vol_rho[k];
+            const double d1 = height - next->pos[0][i];
+            const double d2 = height - curr->pos[0][i];
+            if (d1 * d2 >= 0) continue;
+            double c = curr->c[i];
+            const double dd = c * c * curr->nd[0][i];
+            const double time_water = (dd == 0.0) ? 0.0 : -(curr->pos[0][i] - R) / dd;
+            double position[3], ndir[3];
+            collision_location(d, a, time_water, position, ndir, &c);
+            const double grazing =
+                std::atan2(curr->nd[0][i], std::sqrt(curr->nd[1][i] * curr->nd[1][i] +
+                                                     curr->nd[2][i] * curr->nd[2][i]));
+            const int type = (d1 > 0) ? WQ3D_VERB_VOLUME_LOWER + 2 * (int)k : WQ3D_VERB_VOLUME_UPPER + 2 * (int)k;
+            build_eigenverb(d, a, time_water, grazing, c, position, ndir, type);
+        }
+    }
+
+    /* wave_queue::build_eigenverb (wave_queue.cc:1063-1164) */
+    void build_eigenverb(size_t d, size_t a, double tw, double grazing, double speed,
+                         const double* position, const double* ndir, int type) {
+        const int32_t seq = ev_seq++;
+        const size_t i = idx(d, a);
+        grazing = std::abs(grazing);
+        if (!want_verbs || above_bounce(curr, i) || time <= 0.0 || grazing < 1e-6 ||
+            (az_boundary && a == naz - 1) || std::abs(de[d]) > 89.9)
+            return;
+        /* seq_vector::increment clamps, and an index of -1 wraps to the end
+         * (seq_vector.h:140-143) */
+        auto inc = [](const std::vector<double>& v, size_t k) { return v[std::min(v.size() - 1, k)]; };
+        const double de_angle = to_radians(de[d]);
+        const double de_plus = de_angle + 0.5 * to_radians(inc(de_inc, d));
+        const double de_minus = de_angle - 0.5 * to_radians(inc(de_inc, d - 1));
+        const double az_angle = to_radians(az[a]);
+        const double az_plus = az_angle + 0.5 * to_radians(inc(az_inc, a));
+        const size_t az_index = (a == 0 && az_boundary) ? naz - 1 : a;
+        const double az_minus = az_angle - 0.5 * to_radians(inc(az_inc, az_index - 1));
+        const double area = (std::sin(de_plus) - std::sin(de_minus)) * (az_plus - az_minus);
+        const double de_delta = de_plus - de_minus;
+        const double az_delta = area / de_delta;
+        const double path_length = curr->plen[i] + curr->c[i] * tw;
+        if (path_length <= 0) return;
+        const double sin_grazing = std::sin(grazing);
+        wq3d_eigenverb v{};
+        v.length = 0.5 * path_length * de_delta / sin_grazing;
+        v.width = 0.5 * path_length * az_delta;
+        std::vector<double> power(nf);
+        bool above = false;
+        for (size_t k = 0; k < nf; ++k) {
+            power[k] = std::pow(10.0, -0.1 * curr->atten[i * nf + k]) * area / sin_grazing;
+            if (power[k] >= eigenverb_thresh) above = true;
+        }
+        if (!above) return;
+        /* wvector1::direction (wvector1.cc:79-82) */
+        v.direction = to_radians(to_degrees(std::atan2(ndir[2], -ndir[1])));
+        v.travel_time = time + tw;
+        v.grazing = grazing;
+        v.sound_speed = speed;
+        for (int k = 0; k < 3; ++k) v.position[k] = position[k];
+        v.de = (int32_t)d;
+        v.az = (int32_t)a;
+        v.source_de = to_radians(de[d]);
+        v.source_az = to_radians(az[a]);
+        v.surface = curr->surface[i];
+        v.bottom = curr->bottom[i];
+        v.caustic = curr->caustic[i];
+        v.upper = curr->upper[i];
+        v.lower = curr->lower[i];
+        v.interface_num = type;
+        v.step = (int64_t)steps;
+        v.seq = seq;
+        verbs.push_back(v);
+        verb_power.insert(verb_power.end(), power.begin(), power.end());
+        if (cb.add_eigenverb) cb.add_eigenverb(cb_ctx, &v, power.data(), nf, type);
     }
 
     /* wave_queue.cc:261-269 */
@@ -1165,6 +1263,7 @@ struct Queue {
             grazing = std::asin(-dot_full / c);
         }
         record_reflection(d, a, time_water, grazing, c, position, ndir, 0);
+        if (want_verbs) build_eigenverb(d, a, time_water, grazing, c, position, ndir, WQ3D_VERB_BOTTOM);
 
         std::vector<double> amp(nf), ph(nf);
         reflect_loss(oc.bot, freq, grazing, amp.data(), ph.data());
@@ -1197,6 +1296,7 @@ struct Queue {
                                                  curr->nd[2][i] * curr->nd[2][i]));
         if (grazing <= 0.0) return false;
         record_reflection(d, a, time_water, grazing, c, position, ndir, 1);
+        if (want_verbs) build_eigenverb(d, a, time_water, grazing, c, position, ndir, WQ3D_VERB_SURFACE);
         std::vector<double> amp(nf);
         reflect_loss(oc.surf, freq, grazing, amp.data(), nullptr);
         for (size_t k = 0; k < nf; ++k) {
@@ -2072,6 +2172,26 @@ int oracle_queue_take_eigenrays(void* qv, wq3d_eigenray* rays, double* inten,
         if (phase) std::memcpy(phase + i * nf, q->found[i].phase.data(), nf * sizeof(double));
     }
     q->found.clear();
+    return WQ3D_OK;
+}
+
+int oracle_queue_set_eigenverbs(void* qv, int on) {
+    static_cast<Queue*>(qv)->want_verbs = on != 0;
+    return WQ3D_OK;
+}
+
+/* eigenverbs made so far, in the order the listener saw them; power holds
+ * num_freq values per eigenverb */
+int oracle_queue_take_eigenverbs(void* qv, wq3d_eigenverb* out, double* power, size_t capacity,
+                                 size_t* count) {
+    Queue* q = static_cast<Queue*>(qv);
+    *count = q->verbs.size();
+    if (!out) return WQ3D_OK;
+    if (capacity < q->verbs.size()) return WQ3D_ERR_OVERFLOW;
+    std::memcpy(out, q->verbs.data(), q->verbs.size() * sizeof(wq3d_eigenverb));
+    if (power) std::memcpy(power, q->verb_power.data(), q->verb_power.size() * sizeof(double));
+    q->verbs.clear();
+    q->verb_power.clear();
     return WQ3D_OK;
 }
 

@@ -25,6 +25,9 @@ SIGS = {
     "oracle_queue_destroy": (C.c_int, [C.c_void_p]),
     "oracle_queue_set_thresholds": (C.c_int, [C.c_void_p, C.POINTER(_abi.wq3d_thresholds)]),
     "oracle_queue_set_reflections": (C.c_int, [C.c_void_p, C.c_int]),
+    "oracle_queue_set_eigenverbs": (C.c_int, [C.c_void_p, C.c_int]),
+    "oracle_queue_take_eigenverbs": (C.c_int, [C.c_void_p, C.POINTER(_abi.wq3d_eigenverb), dp, C.c_size_t,
+                                               C.POINTER(C.c_size_t)]),
     "oracle_queue_step": (C.c_int, [C.c_void_p, C.c_size_t]),
     "oracle_queue_run": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_size_t)]),
     "oracle_queue_time": (C.c_int, [C.c_void_p, dp]),
@@ -63,7 +66,7 @@ def _check(rc):
 
 class OracleQueue:
     def __init__(self, ocean, freq, pos, de, az, time_step, target_pos=None,
-                 type=_abi.HYBRID_GAUSSIAN, reflections=False):
+                 type=_abi.HYBRID_GAUSSIAN, reflections=False, eigenverbs=False):
         lib = load_oracle()
         self._lib = lib
         self._freq, self._de, self._az = freq, de, az
@@ -74,6 +77,8 @@ class OracleQueue:
         self._q = h
         if reflections:
             lib.oracle_queue_set_reflections(h, 1)
+        if eigenverbs:
+            lib.oracle_queue_set_eigenverbs(h, 1)
 
     def __del__(self):
         if getattr(self, "_q", None) is not None:
@@ -149,6 +154,22 @@ class OracleQueue:
                                                      cnt, C.byref(n)))
         return [eigenray_model.from_record(recs[i], inten[i * nf:(i + 1) * nf],
                                            phase[i * nf:(i + 1) * nf], self._freq) for i in range(cnt)]
+
+    def eigenverb_threshold(self, value):
+        self._set_one("eigenverb", abs(float(value)))
+
+    def take_eigenverbs(self):
+        """eigenverbs in the order a listener would have received them"""
+        from underseamodelinglibrary_b200.eigenverbs import eigenverb_model
+        n = C.c_size_t()
+        _check(self._lib.oracle_queue_take_eigenverbs(self._q, None, None, 0, C.byref(n)))
+        cnt = n.value
+        nf = self._freq.size()
+        recs = (_abi.wq3d_eigenverb * max(cnt, 1))()
+        power = np.empty(max(cnt, 1) * nf)
+        _check(self._lib.oracle_queue_take_eigenverbs(self._q, recs, _abi.as_dp(power), cnt, C.byref(n)))
+        return [eigenverb_model.from_record(recs[i], power[i * nf:(i + 1) * nf], self._freq)
+                for i in range(cnt)]
 
     def take_reflections(self):
         n = C.c_size_t()

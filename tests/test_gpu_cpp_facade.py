@@ -12,12 +12,27 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def test_cpp_eigenray_basic(tmp_path, engine):
+def build_cpp(tmp_path, name):
+    """compiles tests/cpp/<name>.cpp against the header and libwq3d.so"""
     lib_dir = os.path.dirname(_abi.LIB_PATH)
-    exe = str(tmp_path / "eigenray_basic_cpp")
+    exe = str(tmp_path / name)
     subprocess.check_call(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
-                           os.path.join(ROOT, "tests", "cpp", "eigenray_basic_cpp.cpp"),
+                           os.path.join(ROOT, "tests", "cpp", name + ".cpp"),
                            "-L", lib_dir, "-lwq3d", "-Wl,-rpath," + lib_dir, "-o", exe])
-    out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    return exe
+
+
+def test_cpp_eigenray_basic(tmp_path, engine):
+    out = subprocess.run([build_cpp(tmp_path, "eigenray_basic_cpp")], capture_output=True, text=True,
+                         timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.count("ray ") == 3
+
+
+def test_cpp_eigenverb_accuracy(tmp_path, engine):
+    """reverb_test.cc:216-310 through the C++ header: volume layer added
+    after construction, eigenverb listener, analytic bottom footprints"""
+    out = subprocess.run([build_cpp(tmp_path, "eigenverb_accuracy_cpp")], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "interfaces 4" in out.stdout

@@ -236,3 +236,76 @@ def test_thorp_gsm_table():
             assert abs(out[k] - gsm[k]) <= 0.2 * abs(gsm[k])
             checked += 1
     assert checked == 8
+
+
+def check_bottom_eigenverbs(sc, verbs, spacing, width_tol, direct_only):
+    """reverb_test.cc:257-309 / :389-441: downward rays along az = 0 meet
+    the bottom where the spherical-earth geometry puts them: travel time
+    within 1 ms, grazing angle within 1e-6 rad, direction = source AZ, and
+    the Gaussian footprint's length within 0.1 m and width within
+    ``width_tol``.  ``spacing(seq, index)`` gives the ray spacing used for
+    the analytic footprint."""
+    depth, c0 = sc["depth"], sc["c0"]
+    de, az = sc["de"], sc["az"]
+    checked = 0
+    for v in verbs:
+        if not (v.source_de < 0.0 and v.source_az == 0.0):
+            continue
+        if direct_only and (v.surface != 0 or v.bottom != 0):
+            continue
+        segments = v.bottom + v.surface + 1
+        R = u.earth_radius()
+        Rb = R - depth
+        p = R * math.sin(abs(v.source_de))
+        q = R * R - Rb * Rb
+        path = p - math.sqrt(p * p - q)
+        alpha = math.acos((R * R + Rb * Rb - path * path) / (2 * R * Rb))
+        grazing = abs(v.source_de) - alpha
+        path *= segments
+        time = path / c0
+        de_plus = v.source_de + 0.25 * math.radians(spacing(de, v.de_index))
+        de_minus = v.source_de - 0.25 * math.radians(spacing(de, v.de_index - 1))
+        az_plus = v.source_az + 0.25 * math.radians(spacing(az, v.az_index))
+        az_minus = v.source_az - 0.25 * math.radians(spacing(az, v.az_index - 1))
+        area = (math.sin(de_plus) - math.sin(de_minus)) * (az_plus - az_minus)
+        de_delta = de_plus - de_minus
+        az_delta = area / de_delta
+        assert abs(v.travel_time - time) < 1e-3
+        assert abs(v.grazing - grazing) < 1e-6
+        assert abs(v.direction - v.source_az) < 1e-6
+        assert abs(v.length - path * de_delta / math.sin(grazing)) < 0.1
+        assert abs(v.width - path * az_delta) < width_tol
+        checked += 1
+    return checked
+
+
+def accuracy_spacing(seq, i):
+    """reverb_test.cc:281-288 uses the constant de_spacing 5 and az_spacing 10"""
+    return 5.0 if seq.size() == 29 else 10.0
+
+
+def demo_spacing(seq, i):
+    """reverb_test.cc:406-414 uses seq_vector::increment"""
+    return seq.increment(i)
+
+
+def test_eigenverb_accuracy():
+    """reverb_test.cc:216-310"""
+    sc = S.eigenverb_accuracy()
+    q = S.build_queue(sc, OracleQueue, eigenverbs=True)
+    q.run(sc["time_max"])
+    verbs = q.take_eigenverbs()
+    bottom = [v for v in verbs if v.interface_num == u.eigenverb_model.BOTTOM]
+    assert check_bottom_eigenverbs(sc, bottom, accuracy_spacing, 0.1, False) >= 10
+    assert {v.interface_num for v in verbs} == {0, 1, 2, 3}
+
+
+def test_eigenverb_demo():
+    """reverb_test.cc:334-443: uneven (tangent) D/E spacing, bounce limits"""
+    sc = S.eigenverb_demo()
+    q = S.build_queue(sc, OracleQueue, eigenverbs=True)
+    q.run(sc["time_max"])
+    verbs = q.take_eigenverbs()
+    bottom = [v for v in verbs if v.interface_num == u.eigenverb_model.BOTTOM]
+    assert check_bottom_eigenverbs(sc, bottom, demo_spacing, 0.5, True) >= 20
+    assert all(v.surface <= 2 and v.bottom <= 2 for v in verbs)

@@ -13,10 +13,12 @@ from .types import (seq_vector, seq_linear, seq_log, seq_data, seq_rayfan,
 from .ocean import (attenuation_thorp, attenuation_constant, profile_linear,
                     profile_munk, profile_catenary, profile_n2, reflect_loss_constant,
                     reflect_loss_rayleigh, reflect_loss_eckart, boundary_flat,
-                    boundary_slope, ocean_model, data_grid, profile_grid, boundary_grid)
+                    boundary_slope, ocean_model, data_grid, profile_grid, boundary_grid,
+                    volume_flat)
 from .waveq3d import (wave_queue, eigenray_listener, reflection_listener,
                       eigenray_model)
 from .eigenrays import eigenray_collection
+from .eigenverbs import eigenverb_model, eigenverb_listener, eigenverb_collection
 
 load_engine = _abi.load_engine
 EngineError = _abi.EngineError
@@ -29,7 +31,8 @@ __all__ = [
     "profile_linear", "profile_munk", "profile_catenary", "profile_n2",
     "reflect_loss_constant", "reflect_loss_rayleigh", "reflect_loss_eckart",
     "boundary_flat", "boundary_slope", "ocean_model", "data_grid", "profile_grid",
-    "boundary_grid", "wave_queue",
+    "boundary_grid", "volume_flat", "wave_queue",
     "eigenray_listener", "reflection_listener", "eigenray_model",
-    "eigenray_collection", "load_engine", "EngineError", "LIB_PATH",
+    "eigenray_collection", "eigenverb_model", "eigenverb_listener", "eigenverb_collection",
+    "load_engine", "EngineError", "LIB_PATH",
 ]

@@ -58,9 +58,18 @@ class wq3d_boundary_desc(C.Structure):
                 ("grid", wq3d_grid_desc), ("loss", wq3d_reflect_loss_desc)]
 
 
+MAX_VOLUME = 4
+VERB_BOTTOM, VERB_SURFACE, VERB_VOLUME_UPPER, VERB_VOLUME_LOWER = 0, 1, 2, 3
+
+
+class wq3d_volume_desc(C.Structure):
+    _fields_ = [("depth", C.c_double), ("thickness", C.c_double), ("amplitude", C.c_double)]
+
+
 class wq3d_ocean_desc(C.Structure):
     _fields_ = [("earth_radius", C.c_double), ("profile", wq3d_profile_desc),
-                ("surface", wq3d_boundary_desc), ("bottom", wq3d_boundary_desc)]
+                ("surface", wq3d_boundary_desc), ("bottom", wq3d_boundary_desc),
+                ("num_volume", C.c_int), ("volume", wq3d_volume_desc * MAX_VOLUME)]
 
 
 class wq3d_queue_desc(C.Structure):
@@ -96,15 +105,26 @@ class wq3d_reflection(C.Structure):
                 ("type", C.c_int32), ("pad", C.c_int32), ("step", C.c_int64)]
 
 
+class wq3d_eigenverb(C.Structure):
+    _fields_ = [("travel_time", C.c_double), ("length", C.c_double), ("width", C.c_double),
+                ("position", C.c_double * 3), ("direction", C.c_double), ("grazing", C.c_double),
+                ("sound_speed", C.c_double), ("source_de", C.c_double), ("source_az", C.c_double),
+                ("de", C.c_int32), ("az", C.c_int32), ("surface", C.c_int32), ("bottom", C.c_int32),
+                ("caustic", C.c_int32), ("upper", C.c_int32), ("lower", C.c_int32),
+                ("interface_num", C.c_int32), ("step", C.c_int64), ("seq", C.c_int32),
+                ("pad", C.c_int32)]
+
+
 ADD_EIGENRAY = C.CFUNCTYPE(None, C.c_void_p, C.c_size_t, C.c_size_t,
                            C.POINTER(wq3d_eigenray), dp, dp, C.c_size_t, C.c_uint64)
 CHECK_EIGENRAYS = C.CFUNCTYPE(None, C.c_void_p, C.c_double, C.c_uint64)
 REFLECT = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(wq3d_reflection))
+ADD_EIGENVERB = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(wq3d_eigenverb), dp, C.c_size_t, C.c_int)
 
 
 class wq3d_callbacks(C.Structure):
     _fields_ = [("add_eigenray", ADD_EIGENRAY), ("check_eigenrays", CHECK_EIGENRAYS),
-                ("reflect", REFLECT)]
+                ("reflect", REFLECT), ("add_eigenverb", ADD_EIGENVERB)]
 
 
 class wq3d_front_view(C.Structure):

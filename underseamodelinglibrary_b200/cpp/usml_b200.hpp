@@ -3,7 +3,7 @@
  * of include/wq3d.h (header only; link with libwq3d.so).
  *
  * The classes keep the reference's names, constructor arguments and call
- * order (types/seq_*.h, types/wposition*.h, ocean/*.h, waveq3d/wave_queue.h,
+ * order (the types/seq_ and types/wposition headers, the ocean/ models, waveq3d/wave_queue.h,
  * eigenrays/eigenray_collection.h), with std::vector in place of Boost
  * uBLAS.  Engine errors become std::runtime_error / std::invalid_argument,
  * as the reference throws.
@@ -165,6 +165,8 @@ class wposition1 {
     double theta() const { return _t; }
     double phi() const { return _p; }
     void rho(double v) { _r = v; }
+    void theta(double v) { _t = v; }
+    void phi(double v) { _p = v; }
     double latitude() const { return 90.0 - to_degrees(_t); }
     double longitude() const { return to_degrees(_p); }
     double altitude() const { return _r - earth::radius(); }
@@ -325,27 +327,50 @@ class boundary_slope : public boundary_model {
     reflect_loss_model::csptr _loss;
 };
 
-/* ocean_model (ocean/ocean_model.h); the device copy is built on first use */
+/* volume_flat (ocean/volume_flat.h:32-37): a scattering layer at a
+ * constant depth */
+struct volume_model {
+    typedef std::shared_ptr<const volume_model> csptr;
+    wq3d_volume_desc d{0.0, 0.0, -300.0};
+};
+struct volume_flat : volume_model {
+    explicit volume_flat(double depth = 0.0, double thickness = 0.0, double amplitude = -300.0) {
+        d = {depth, thickness, amplitude};
+    }
+};
+
+/* ocean_model (ocean/ocean_model.h); the device copy is built on first
+ * use, so volume layers can be added after construction as in the
+ * reference */
 class ocean_model {
    public:
     typedef std::shared_ptr<const ocean_model> csptr;
     ocean_model(const boundary_model::csptr& surface, const boundary_model::csptr& bottom,
-                const profile_model::csptr& profile)
-        : _radius(types::earth::radius()) {
-        wq3d_ocean_desc d{};
-        d.earth_radius = _radius;
-        profile->fill(&d.profile);
-        surface->fill(&d.surface);
-        bottom->fill(&d.bottom);
-        wq3d_ocean* o = nullptr;
-        check(wq3d_ocean_create(&d, &o));
-        _h.reset(o, [](wq3d_ocean* p) { wq3d_ocean_destroy(p); });
+                const profile_model::csptr& profile) {
+        _d.earth_radius = types::earth::radius();
+        profile->fill(&_d.profile);
+        surface->fill(&_d.surface);
+        bottom->fill(&_d.bottom);
     }
-    const wq3d_ocean* handle() const { return _h.get(); }
+    /* ocean_model::add_volume (ocean/ocean_model.h:52) */
+    void add_volume(const volume_model::csptr& layer) {
+        if (_h) throw std::logic_error("add volume layers before the ocean is first used");
+        if (_d.num_volume >= WQ3D_MAX_VOLUME) throw std::invalid_argument("too many volume layers");
+        _d.volume[_d.num_volume++] = layer->d;
+    }
+    size_t num_volume() const { return (size_t)_d.num_volume; }
+    const wq3d_ocean* handle() const {
+        if (!_h) {
+            wq3d_ocean* o = nullptr;
+            check(wq3d_ocean_create(&_d, &o));
+            _h.reset(o, [](wq3d_ocean* p) { wq3d_ocean_destroy(p); });
+        }
+        return _h.get();
+    }
 
    private:
-    double _radius;
-    std::shared_ptr<wq3d_ocean> _h;
+    wq3d_ocean_desc _d{};
+    mutable std::shared_ptr<wq3d_ocean> _h;
 };
 
 }  // namespace ocean
@@ -429,6 +454,49 @@ class eigenray_collection : public eigenray_listener {
 
 }  // namespace eigenrays
 
+namespace eigenverbs {
+
+/* eigenverbs/eigenverb_model.h:34-150 */
+struct eigenverb_model {
+    typedef std::shared_ptr<const eigenverb_model> csptr;
+    enum interface_type { BOTTOM = WQ3D_VERB_BOTTOM, SURFACE = WQ3D_VERB_SURFACE,
+                          VOLUME_UPPER = WQ3D_VERB_VOLUME_UPPER, VOLUME_LOWER = WQ3D_VERB_VOLUME_LOWER };
+    double travel_time = 0;
+    std::vector<double> power;
+    double length = 0, width = 0;
+    types::wposition1 position;
+    double direction = 0, grazing = 0, sound_speed = 0;
+    size_t de_index = 0, az_index = 0;
+    double source_de = 0, source_az = 0;
+    int surface = 0, bottom = 0, caustic = 0, upper = 0, lower = 0;
+};
+
+/* eigenverbs/eigenverb_listener.h:23-41 */
+class eigenverb_listener {
+   public:
+    virtual void add_eigenverb(eigenverb_model::csptr verb, size_t interface_num) = 0;
+    virtual ~eigenverb_listener() {}
+};
+
+/* eigenverbs/eigenverb_collection.h: one list per interface */
+class eigenverb_collection : public eigenverb_listener {
+   public:
+    explicit eigenverb_collection(size_t num_volumes = 0) : _collection((1 + num_volumes) * 2) {}
+    size_t num_interfaces() const { return _collection.size(); }
+    size_t size(size_t interface_num) const { return _collection[interface_num].size(); }
+    const std::vector<eigenverb_model::csptr>& eigenverbs(size_t interface_num) const {
+        return _collection[interface_num];
+    }
+    void add_eigenverb(eigenverb_model::csptr verb, size_t interface_num) override {
+        _collection[interface_num].push_back(verb);
+    }
+
+   private:
+    std::vector<std::vector<eigenverb_model::csptr>> _collection;
+};
+
+}  // namespace eigenverbs
+
 namespace waveq3d {
 
 /* wave_queue (waveq3d/wave_queue.h:122-264) */
@@ -471,8 +539,11 @@ class wave_queue {
 
     void add_eigenray_listener(eigenrays::eigenray_listener* l) {
         _listeners.push_back(l);
-        wq3d_callbacks cb{&wave_queue::on_ray, &wave_queue::on_check, nullptr};
-        check(wq3d_queue_set_callbacks(_q.get(), &cb, this));
+        install();
+    }
+    void add_eigenverb_listener(eigenverbs::eigenverb_listener* l) {
+        _verb_listeners.push_back(l);
+        install();
     }
     void step() { check(wq3d_queue_step(_q.get(), 1)); }
     void run(double time_max) { check(wq3d_queue_run(_q.get(), time_max, nullptr)); }
@@ -485,8 +556,53 @@ class wave_queue {
         _th.intensity = std::abs(v);
         check(wq3d_queue_set_thresholds(_q.get(), &_th));
     }
+    void eigenverb_threshold(double v) {
+        _th.eigenverb = std::abs(v);
+        check(wq3d_queue_set_thresholds(_q.get(), &_th));
+    }
+    void max_bottom(int v) {
+        _th.max_bottom = v;
+        check(wq3d_queue_set_thresholds(_q.get(), &_th));
+    }
+    void max_surface(int v) {
+        _th.max_surface = v;
+        check(wq3d_queue_set_thresholds(_q.get(), &_th));
+    }
 
    private:
+    void install() {
+        wq3d_callbacks cb{};
+        if (!_listeners.empty()) {
+            cb.add_eigenray = &wave_queue::on_ray;
+            cb.check_eigenrays = &wave_queue::on_check;
+        }
+        if (!_verb_listeners.empty()) cb.add_eigenverb = &wave_queue::on_verb;
+        check(wq3d_queue_set_callbacks(_q.get(), &cb, this));
+    }
+    static void on_verb(void* ctx, const wq3d_eigenverb* v, const double* power, size_t nf, int interface_num) {
+        auto* self = static_cast<wave_queue*>(ctx);
+        auto verb = std::make_shared<eigenverbs::eigenverb_model>();
+        verb->travel_time = v->travel_time;
+        verb->power.assign(power, power + nf);
+        verb->length = v->length;
+        verb->width = v->width;
+        verb->position.rho(v->position[0]);
+        verb->position.theta(v->position[1]);
+        verb->position.phi(v->position[2]);
+        verb->direction = v->direction;
+        verb->grazing = v->grazing;
+        verb->sound_speed = v->sound_speed;
+        verb->de_index = (size_t)v->de;
+        verb->az_index = (size_t)v->az;
+        verb->source_de = v->source_de;
+        verb->source_az = v->source_az;
+        verb->surface = v->surface;
+        verb->bottom = v->bottom;
+        verb->caustic = v->caustic;
+        verb->upper = v->upper;
+        verb->lower = v->lower;
+        for (auto* l : self->_verb_listeners) l->add_eigenverb(verb, (size_t)interface_num);
+    }
     static void on_ray(void* ctx, size_t t1, size_t t2, const wq3d_eigenray* r, const double* inten,
                        const double* phase, size_t nf, uint64_t run) {
         auto* self = static_cast<wave_queue*>(ctx);
@@ -513,6 +629,7 @@ class wave_queue {
     types::seq_vector::csptr _freq;
     std::shared_ptr<wq3d_queue> _q;
     std::vector<eigenrays::eigenray_listener*> _listeners;
+    std::vector<eigenverbs::eigenverb_listener*> _verb_listeners;
     wq3d_thresholds _th{300.0, 300.0, 999, 999, 999, 999, 999};
 };
 

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "wq3d_engine.cuh"
@@ -236,6 +237,50 @@ struct wq3d_queue {
     std::vector<wq3d_eigenray> h_rec;
     std::vector<double> h_rinten, h_rphase;
     std::vector<wq3d_reflection> h_refl;
+    std::vector<wq3d_eigenverb> h_verb;
+    std::vector<double> h_vpower;
+
+    /* the chunk graph is rebuilt when the launch sequence changes */
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_failed = false;
+    }
+
+    bool volume_pass() const { return h.want_verbs && h.oc.nvol > 0; }
+
+    void release(void* p) {
+        if (!p) return;
+        auto it = std::find(allocs.begin(), allocs.end(), p);
+        if (it != allocs.end()) allocs.erase(it);
+        cudaFree(p);
+    }
+
+    /* Eigenverb buffers hold at least "need" records (one chunk's worth).
+     * They start at half a record per ray, step and interface and grow
+     * when a chunk fills more than half of them; a quarter of the free
+     * device memory is the limit. */
+    int ensure_verb_capacity(size_t need) {
+        if (h.verb && need <= h.cap_verb) return WQ3D_OK;
+        const size_t rec_bytes = sizeof(wq3d_eigenverb) + (size_t)h.nf * sizeof(double);
+        size_t free_b = 0, total_b = 0;
+        WQ_CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t limit = std::max<size_t>(4096, (free_b / 4) / rec_bytes);
+        const size_t cap = std::min<size_t>({std::max<size_t>(need, 4096), limit, (size_t)UINT32_MAX / 2});
+        if (h.verb && cap <= h.cap_verb) return WQ3D_OK;
+        WQ_CK(cudaStreamSynchronize(stream));
+        release(h.verb);
+        release(h.verb_power);
+        h.verb = nullptr;
+        h.verb_power = nullptr;
+        h.cap_verb = 0;
+        int rc = alloc(&h.verb, cap);
+        if (!rc) rc = alloc(&h.verb_power, cap * (size_t)h.nf);
+        if (rc) return rc;
+        h.cap_verb = (uint32_t)cap;
+        WQ_CK(cudaMemcpy(d_q, &h, sizeof(QueueDev), cudaMemcpyHostToDevice));
+        return WQ3D_OK;
+    }
 
     ~wq3d_queue() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -284,6 +329,10 @@ struct wq3d_queue {
         for (int k = 0; k < K; ++k) {
             cudaEvent_t* ev = timing ? &events[5 * k] : nullptr;
             if (ev) cudaEventRecord(ev[0], stream);
+            if (volume_pass()) {
+                k_volume<<<grd, blk, 0, stream>>>(d_q, k);
+                launches += 1;
+            }
             k_advance_fn<<<grd, blk, 0, stream>>>(d_q, k);
             if (ev) cudaEventRecord(ev[1], stream);
             launches += 1;
@@ -339,7 +388,7 @@ struct wq3d_queue {
         return WQ3D_OK;
     }
 
-    void deliver(int K, size_t nrec, size_t nrefl) {
+    void deliver(int K, size_t nrec, size_t nrefl, size_t nverb) {
         const int nf = h.nf;
         /* reference order: (step, t1, t2, de, az) for eigenrays
          * (wave_queue.cc:361-373), (step, de, az) for reflections */
@@ -361,12 +410,42 @@ struct wq3d_queue {
             if (x.az != y.az) return x.az < y.az;
             return x.pad < y.pad;
         });
-        size_t ir = 0, ie = 0;
+        /* eigenverbs: (step, de, az, seq) is the order of the reference's
+         * detect_reflections loop (wave_queue.cc:197-216) */
+        std::vector<size_t> vorder(nverb);
+        for (size_t i = 0; i < nverb; ++i) vorder[i] = i;
+        std::sort(vorder.begin(), vorder.end(), [&](size_t a, size_t b) {
+            const wq3d_eigenverb& x = h_verb[a];
+            const wq3d_eigenverb& y = h_verb[b];
+            if (x.step != y.step) return x.step < y.step;
+            if (x.de != y.de) return x.de < y.de;
+            if (x.az != y.az) return x.az < y.az;
+            return x.seq < y.seq;
+        });
+        size_t ir = 0, ie = 0, iv = 0;
         for (int k = 0; k < K; ++k) {
             const int64_t step = steps + k + 1;
-            while (ir < refl.size() && refl[ir].step == step) {
-                if (cb.reflect) cb.reflect(cb_ctx, &refl[ir]);
-                ++ir;
+            /* a reflection is announced before the eigenverb it makes, and
+             * both carry the ray's event number */
+            while ((ir < refl.size() && refl[ir].step == step) ||
+                   (iv < vorder.size() && h_verb[vorder[iv]].step == step)) {
+                const bool verb_here = iv < vorder.size() && h_verb[vorder[iv]].step == step;
+                const bool refl_here = ir < refl.size() && refl[ir].step == step;
+                bool take_refl = refl_here;
+                if (refl_here && verb_here) {
+                    const wq3d_eigenverb& v = h_verb[vorder[iv]];
+                    take_refl = !(std::make_tuple(v.de, v.az, v.seq) <
+                                  std::make_tuple(refl[ir].de, refl[ir].az, refl[ir].pad));
+                }
+                if (take_refl) {
+                    if (cb.reflect) cb.reflect(cb_ctx, &refl[ir]);
+                    ++ir;
+                } else {
+                    const size_t j = vorder[iv];
+                    if (cb.add_eigenverb)
+                        cb.add_eigenverb(cb_ctx, &h_verb[j], &h_vpower[j * nf], (size_t)nf, h_verb[j].interface_num);
+                    ++iv;
+                }
             }
             while (ie < order.size() && h_rec[order[ie]].step == step) {
                 const size_t j = order[ie];
@@ -393,17 +472,18 @@ struct wq3d_queue {
         WQ_CK(cudaMemcpyAsync(d_base, h_base, sizeof(int64_t), cudaMemcpyHostToDevice, stream));
         WQ_CK(cudaMemcpyAsync(d_times, h_times, (K + 1) * sizeof(double), cudaMemcpyHostToDevice, stream));
         WQ_CK(cudaMemsetAsync(d_counts, 0, 3 * sizeof(uint32_t), stream));
+        WQ_CK(cudaMemsetAsync(d_counts + 8, 0, sizeof(uint32_t), stream));
         if (!timing && K == chunk) {
             build_graph();
         }
         if (!timing && K == chunk && graph) {
             WQ_CK(cudaGraphLaunch(graph, stream));
-            launches += (h.nt > 0 ? 4 : 2) * (int64_t)K;
+            launches += ((h.nt > 0 ? 4 : 2) + (volume_pass() ? 1 : 0)) * (int64_t)K;
         } else {
             launch_chunk(K);
         }
         WQ_CK(cudaGetLastError());
-        WQ_CK(cudaMemcpyAsync(h_counts, d_counts, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        WQ_CK(cudaMemcpyAsync(h_counts, d_counts, 9 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         WQ_CK(cudaStreamSynchronize(stream));
         if (timing) {
             for (int k = 0; k < K; ++k) {
@@ -419,6 +499,8 @@ struct wq3d_queue {
         const uint32_t nrec = std::min(h_counts[0], h.cap_rec);
         const uint32_t nrefl = std::min(h_counts[1], h.cap_refl);
         const uint32_t err = h_counts[2];
+        const uint32_t nverb = h.want_verbs ? std::min(h_counts[8], h.cap_verb) : 0;
+        const uint32_t verbs_made = h.want_verbs ? h_counts[8] : 0;
         if (nrec > 0) {
             if (h_rec.size() < nrec) {
                 h_rec.resize(nrec);
@@ -433,11 +515,24 @@ struct wq3d_queue {
             if (h_refl.size() < nrefl) h_refl.resize(nrefl);
             WQ_CK(cudaMemcpy(h_refl.data(), h.refl, nrefl * sizeof(wq3d_reflection), cudaMemcpyDeviceToHost));
         }
-        deliver(K, nrec, nrefl);
+        if (nverb > 0) {
+            if (h_verb.size() < nverb) {
+                h_verb.resize(nverb);
+                h_vpower.resize((size_t)nverb * h.nf);
+            }
+            WQ_CK(cudaMemcpy(h_verb.data(), h.verb, nverb * sizeof(wq3d_eigenverb), cudaMemcpyDeviceToHost));
+            WQ_CK(cudaMemcpy(h_vpower.data(), h.verb_power, (size_t)nverb * h.nf * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+        }
+        deliver(K, nrec, nrefl, nverb);
+        if (verbs_made > h.cap_verb / 2 && !(err & ERR_VERB_OVERFLOW)) {
+            const int rc = ensure_verb_capacity(4 * (size_t)verbs_made);
+            if (rc) return rc;
+        }
         steps += K;
         time = h_times[K];
-        if (err & (ERR_CAND_OVERFLOW | ERR_REC_OVERFLOW | ERR_REFL_OVERFLOW))
-            return fail(WQ3D_ERR_OVERFLOW, "eigenray or reflection buffer overflow (error bits " +
+        if (err & (ERR_CAND_OVERFLOW | ERR_REC_OVERFLOW | ERR_REFL_OVERFLOW | ERR_VERB_OVERFLOW))
+            return fail(WQ3D_ERR_OVERFLOW, "eigenray, reflection or eigenverb buffer overflow (error bits " +
                                                std::to_string(err) + "); recreate the queue with a larger eigenray_capacity");
         if (err)
             return fail(WQ3D_ERR_NUMERIC, "kernel iteration bound reached (error bits " + std::to_string(err) + ")");
@@ -490,6 +585,13 @@ int wq3d_ocean_create(const wq3d_ocean_desc* d, wq3d_ocean** out) {
     p.atten_coef = d->profile.attenuation_coef;
     setup_boundary(o->dev.surf, d->surface, d->earth_radius);
     setup_boundary(o->dev.bot, d->bottom, d->earth_radius);
+    if (d->num_volume < 0 || d->num_volume > WQ3D_MAX_VOLUME) {
+        delete o;
+        return fail(WQ3D_ERR_INVALID, "num_volume must be 0.." + std::to_string(WQ3D_MAX_VOLUME));
+    }
+    /* volume_flat.h:32-37: the layer's rho under the construction radius */
+    o->dev.nvol = d->num_volume;
+    for (int k = 0; k < d->num_volume; ++k) o->dev.vol_rho[k] = d->earth_radius - std::abs(d->volume[k].depth);
     o->host = o->dev;
     int rc = WQ3D_OK;
     if (p.kind == WQ3D_PROFILE_GRID)
@@ -836,7 +938,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     if ((rc = q->alloc(&h.rec, h.cap_rec)) || (rc = q->alloc(&h.rec_inten, (size_t)h.cap_rec * nf)) ||
         (rc = q->alloc(&h.rec_phase, (size_t)h.cap_rec * nf)) || (rc = q->alloc(&h.refl, h.cap_refl)))
         return cleanup(rc);
-    if ((rc = q->alloc(&q->d_counts, 8)) || (rc = q->alloc(&q->d_base, 1)) ||
+    if ((rc = q->alloc(&q->d_counts, 16)) || (rc = q->alloc(&q->d_base, 1)) ||
         (rc = q->alloc(&q->d_times, (size_t)q->chunk + 1)))
         return cleanup(rc);
     h.n_rec = q->d_counts + 0;
@@ -846,6 +948,9 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.n_work[0] = q->d_counts + 4;
     h.n_work[1] = q->d_counts + 5;
     h.n_done = q->d_counts + 6;
+    h.n_verb = q->d_counts + 8;
+    h.want_verbs = 0;
+    h.verb_threshold = 1e-30; /* wave_thresholds.h:40 */
     {
         const size_t stride = 51 + 2 * nf;
         if ((rc = q->alloc(&h.shadow, n * stride)) || (rc = q->alloc(&h.shadow_cnt, 3 * n)) ||
@@ -861,7 +966,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     q->h_base = static_cast<int64_t*>(q->pinned);
     q->h_counts = reinterpret_cast<uint32_t*>(static_cast<char*>(q->pinned) + 64);
     q->h_times = reinterpret_cast<double*>(static_cast<char*>(q->pinned) + 128);
-    if (cudaMemset(q->d_counts, 0, 8 * sizeof(uint32_t)) != cudaSuccess)
+    if (cudaMemset(q->d_counts, 0, 16 * sizeof(uint32_t)) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
 
     if (cudaMalloc(&q->d_q, sizeof(QueueDev)) != cudaSuccess)
@@ -917,6 +1022,7 @@ int wq3d_queue_set_thresholds(wq3d_queue* q, const wq3d_thresholds* t) {
     q->h.max_caustic = t->max_caustic;
     q->h.max_upper = t->max_upper;
     q->h.max_lower = t->max_lower;
+    q->h.verb_threshold = std::pow(10.0, -0.1 * std::abs(t->eigenverb)); /* wave_thresholds.h:87-89 */
     WQ_CK(cudaMemcpy(q->d_q, &q->h, sizeof(QueueDev), cudaMemcpyHostToDevice));
     return WQ3D_OK;
 }
@@ -930,8 +1036,17 @@ int wq3d_queue_set_callbacks(wq3d_queue* q, const wq3d_callbacks* cb, void* ctx)
         q->cb = wq3d_callbacks{};
     q->cb_ctx = ctx;
     const int want = q->cb.reflect ? 1 : 0;
-    if (want != q->h.want_refl) {
+    const int want_verbs = q->cb.add_eigenverb ? 1 : 0;
+    if (want_verbs && !q->h.verb) {
+        /* eigenverb buffers, made the first time a listener asks */
+        const int rc = q->ensure_verb_capacity((size_t)q->chunk * q->h.n * (q->h.oc.nvol + 1) / 2);
+        if (rc) return rc;
+    }
+    if (want != q->h.want_refl || want_verbs != q->h.want_verbs) {
+        const bool pass = q->volume_pass();
         q->h.want_refl = want;
+        q->h.want_verbs = want_verbs;
+        if (pass != q->volume_pass()) q->drop_graph();
         WQ_CK(cudaMemcpy(q->d_q, &q->h, sizeof(QueueDev), cudaMemcpyHostToDevice));
     }
     return WQ3D_OK;

@@ -37,7 +37,8 @@ enum : uint32_t {
     ERR_CAND_OVERFLOW = 2u,      /* eigenray candidate list full               */
     ERR_REC_OVERFLOW = 4u,       /* eigenray record buffer full                */
     ERR_REFL_OVERFLOW = 8u,      /* reflection record buffer full              */
-    ERR_WALK_LIMIT = 16u         /* a Gaussian-beam walk exceeded its bound    */
+    ERR_WALK_LIMIT = 16u,        /* a Gaussian-beam walk exceeded its bound    */
+    ERR_VERB_OVERFLOW = 32u      /* eigenverb record buffer full               */
 };
 
 struct FrontPtrs {
@@ -124,6 +125,13 @@ struct QueueDev {
     uint32_t* n_refl;
     uint32_t cap_refl;
     int want_refl;
+    /* eigenverb records (only when a listener wants them) */
+    wq3d_eigenverb* verb;
+    double* verb_power;      /* [cap][nf] */
+    uint32_t* n_verb;
+    uint32_t cap_verb;
+    int want_verbs;
+    double verb_threshold;   /* linear power (wave_thresholds.h:87-89)     */
     uint32_t* err;
 };
 
@@ -141,6 +149,7 @@ WQ3D_DECLARE_STEP_KERNELS
 namespace analytic {
 WQ3D_DECLARE_STEP_KERNELS
 }
+__global__ void k_volume(const QueueDev* q, int k);
 __global__ void k_cpa(const QueueDev* q, int k);
 __global__ void k_cpa_f32(const QueueDev* q, int k);
 __global__ void k_eigenray(const QueueDev* q, int k);

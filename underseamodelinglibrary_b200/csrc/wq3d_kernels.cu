@@ -236,34 +236,135 @@ struct RayLocal {
     int surface, bottom, caustic;
 };
 
-/* collision_location (wave_queue.cc:982-1057) on the private state */
-__device__ void collision_local(const QueueDev& q, const RayLocal& L, double tw, double* pos,
-                                double* nd, double* speed) {
+/* collision_location (wave_queue.cc:982-1057) from one ray's prev, curr
+ * and next states */
+__device__ void collision_rays(const QueueDev& q, const RayS& V, const RayS& Cr, const RayS& X,
+                               double tw, double* pos, double* nd, double* speed) {
     const double dt = q.dt;
     const double time1 = 2.0 * dt;
     const double time2 = dt * dt;
     const double dtime2 = tw * tw;
-    const double drho = (L.x.c - L.v.c) / time1;
-    const double d2rho = (L.x.c + L.v.c - 2.0 * L.c.c) / time2;
-    *speed = L.c.c + drho * tw + 0.5 * d2rho * dtime2;
+    const double drho = (X.c - V.c) / time1;
+    const double d2rho = (X.c + V.c - 2.0 * Cr.c) / time2;
+    *speed = Cr.c + drho * tw + 0.5 * d2rho * dtime2;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const double v1 = (L.x.pos[k] - L.v.pos[k]) / time1;
-        const double v2 = (L.x.pos[k] + L.v.pos[k] - 2.0 * L.c.pos[k]) / time2;
-        pos[k] = L.c.pos[k] + v1 * tw + 0.5 * v2 * dtime2;
+        const double v1 = (X.pos[k] - V.pos[k]) / time1;
+        const double v2 = (X.pos[k] + V.pos[k] - 2.0 * Cr.pos[k]) / time2;
+        pos[k] = Cr.pos[k] + v1 * tw + 0.5 * v2 * dtime2;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const double v1 = (L.x.nd[k] - L.v.nd[k]) / time1;
-        const double v2 = (L.x.nd[k] + L.v.nd[k] - 2.0 * L.c.nd[k]) / time2;
-        nd[k] = L.c.nd[k] + v1 * tw + 0.5 * v2 * dtime2;
+        const double v1 = (X.nd[k] - V.nd[k]) / time1;
+        const double v2 = (X.nd[k] + V.nd[k] - 2.0 * Cr.nd[k]) / time2;
+        nd[k] = Cr.nd[k] + v1 * tw + 0.5 * v2 * dtime2;
     }
 }
 
-/* reflection_model::reflection_reinit (reflection_model.cc:248-330).
- * Keeps the reference's past.update() at :315, which leaves "temp" with
- * the derivatives of its first update.  reflection_copy copies position,
- * gradients, sound speed and step distance (reflection_model.cc:335-360). */
+/* collision_location on the private state */
+__device__ __forceinline__ void collision_local(const QueueDev& q, const RayLocal& L, double tw,
+                                                double* pos, double* nd, double* speed) {
+    collision_rays(q, L.v, L.c, L.x, tw, pos, nd, speed);
+}
+
+/* seq_vector::increment: the index clamps to the last element, and -1
+ * (an unsigned index in the reference) clamps there too */
+__device__ __forceinline__ double seq_inc(const double* inc, int n, int k) {
+    return inc[(k < 0 || k > n - 1) ? n - 1 : k];
+}
+
+/* wave_queue::build_eigenverb (wave_queue.cc:1063-1164) for ray i.  C is
+ * the stored "curr" front: its path length, attenuation and caustic /
+ * upper / lower counts are not changed by reflections.  curr_c is curr's
+ * sound speed (re-initialised by an earlier reflection of this step) and
+ * surface / bottom the counts at this point of the reflection chain. */
+__device__ void build_eigenverb(const QueueDev& q, const FrontPtrs& C, int i, int64_t step,
+                                double t_old, double tw, double grazing, double speed,
+                                const double* pos, const double* nd, int type, double curr_c,
+                                int surface, int bottom, int seq) {
+    grazing = fabs(grazing);
+    const int d = i / q.naz, a = i % q.naz;
+    if (bottom > q.max_bottom || surface > q.max_surface || C.caustic[i] > q.max_caustic ||
+        C.upper[i] > q.max_upper || C.lower[i] > q.max_lower)
+        return;
+    if (t_old <= 0.0 || grazing < 1e-6 || (q.az_boundary && a == q.naz - 1) || fabs(q.de[d]) > 89.9)
+        return;
+    /* footprint of the ray's share of the fan, half-way to its neighbours */
+    const double de_angle = deg2rad(q.de[d]);
+    const double de_plus = de_angle + 0.5 * deg2rad(seq_inc(q.de_inc, q.nde, d));
+    const double de_minus = de_angle - 0.5 * deg2rad(seq_inc(q.de_inc, q.nde, d - 1));
+    const double az_angle = deg2rad(q.az[a]);
+    const double az_plus = az_angle + 0.5 * deg2rad(seq_inc(q.az_inc, q.naz, a));
+    const int az_index = (a == 0 && q.az_boundary) ? q.naz - 1 : a;
+    const double az_minus = az_angle - 0.5 * deg2rad(seq_inc(q.az_inc, q.naz, az_index - 1));
+    const double area = (sin(de_plus) - sin(de_minus)) * (az_plus - az_minus);
+    const double de_delta = de_plus - de_minus;
+    const double az_delta = area / de_delta;
+    const double path_length = C.plen[i] + curr_c * tw;
+    if (path_length <= 0) return;
+    const double sin_grazing = sin(grazing);
+    bool above = false;
+    for (int f = 0; f < q.nf && !above; ++f)
+        above = pow(10.0, -0.1 * C.atten[(size_t)f * q.n + i]) * area / sin_grazing >= q.verb_threshold;
+    if (!above) return;
+    const uint32_t slot = atomicAdd(q.n_verb, 1u);
+    if (slot >= q.cap_verb) {
+        set_err(q, ERR_VERB_OVERFLOW);
+        return;
+    }
+    wq3d_eigenverb v;
+    v.travel_time = t_old + tw;
+    v.length = 0.5 * path_length * de_delta / sin_grazing;
+    v.width = 0.5 * path_length * az_delta;
+    for (int k = 0; k < 3; ++k) v.position[k] = pos[k];
+    /* wvector1::direction (wvector1.cc:79-82), degrees and back */
+    v.direction = deg2rad(rad2deg(atan2(nd[2], -nd[1])));
+    v.grazing = grazing;
+    v.sound_speed = speed;
+    v.source_de = deg2rad(q.de[d]);
+    v.source_az = deg2rad(q.az[a]);
+    v.de = d;
+    v.az = a;
+    v.surface = surface;
+    v.bottom = bottom;
+    v.caustic = C.caustic[i];
+    v.upper = C.upper[i];
+    v.lower = C.lower[i];
+    v.interface_num = type;
+    v.step = step;
+    v.seq = seq;
+    v.pad = 0;
+    q.verb[slot] = v;
+    for (int f = 0; f < q.nf; ++f)
+        q.verb_power[(size_t)slot * q.nf + f] =
+            pow(10.0, -0.1 * C.atten[(size_t)f * q.n + i]) * area / sin_grazing;
+}
+
+/* wave_queue::detect_volume_scattering (wave_queue.cc:297-345) with the
+ * ray's prev / curr / next states V, Cr, X.  The collision time is
+ * measured to the ocean surface, not to the layer, as in the reference. */
+__device__ void volume_scatter(const QueueDev& q, const FrontPtrs& C, int i, int64_t step,
+                               double t_old, const RayS& V, const RayS& Cr, const RayS& X,
+                               int surface, int bottom, int& seq) {
+    if (bottom > q.max_bottom || surface > q.max_surface || C.caustic[i] > q.max_caustic ||
+        C.upper[i] > q.max_upper || C.lower[i] > q.max_lower)
+        return;
+    for (int k = 0; k < q.oc.nvol; ++k) {
+        const double height = q.oc.vol_rho[k];
+        const double d1 = height - X.pos[0];
+        const double d2 = height - Cr.pos[0];
+        if (d1 * d2 >= 0) continue;
+        double c = Cr.c;
+        const double dd = c * c * Cr.nd[0];
+        const double tw = (dd == 0.0) ? 0.0 : -(Cr.pos[0] - q.R) / dd;
+        double pos[3], nd[3];
+        collision_rays(q, V, Cr, X, tw, pos, nd, &c);
+        const double grazing = atan2(Cr.nd[0], sqrt(Cr.nd[1] * Cr.nd[1] + Cr.nd[2] * Cr.nd[2]));
+        const int type = (d1 > 0) ? WQ3D_VERB_VOLUME_LOWER + 2 * k : WQ3D_VERB_VOLUME_UPPER + 2 * k;
+        build_eigenverb(q, C, i, step, t_old, tw, grazing, c, pos, nd, type, Cr.c, surface, bottom, seq++);
+    }
+}
+
 __device__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const double* pos,
                              const double* nd) {
     RayS past1, prev1, curr1, next1, temp;
@@ -334,8 +435,8 @@ __device__ void record_reflection(const QueueDev& q, int64_t step, double t_old,
 }
 
 /* reflection_model::surface_reflection (reflection_model.cc:187-243) */
-__device__ bool surface_local(const QueueDev& q, RayLocal& L, int i, int64_t step, double t_old,
-                              int seq) {
+__device__ bool surface_local(const QueueDev& q, const FrontPtrs& C, RayLocal& L, int i, int64_t step,
+                              double t_old, int& seq) {
     double c = L.c.c;
     const double d = c * c * L.c.nd[0];
     const double tw = (d == 0.0) ? 0.0 : -(L.c.pos[0] - q.R) / d;
@@ -345,6 +446,10 @@ __device__ bool surface_local(const QueueDev& q, RayLocal& L, int i, int64_t ste
     const double grazing = atan2(L.c.nd[0], sqrt(n1 * n1 + n2 * n2));
     if (grazing <= 0.0) return false;
     record_reflection(q, step, t_old, i, tw, grazing, c, pos, nd, 1, seq);
+    if (q.want_verbs)
+        build_eigenverb(q, C, i, step, t_old, tw, grazing, c, pos, nd, WQ3D_VERB_SURFACE, L.c.c, L.surface,
+                        L.bottom, seq);
+    ++seq;
     const LossDev& Lo = q.oc.surf.loss;
     double amp0 = 0.0, ph0 = 0.0;
     if (Lo.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(Lo, grazing, &amp0, &ph0);
@@ -365,8 +470,8 @@ __device__ bool surface_local(const QueueDev& q, RayLocal& L, int i, int64_t ste
 }
 
 /* reflection_model::bottom_reflection (reflection_model.cc:33-182) */
-__device__ void bottom_local(const QueueDev& q, RayLocal& L, int i, double depth, int64_t step,
-                             double t_old, int seq) {
+__device__ void bottom_local(const QueueDev& q, const FrontPtrs& C, RayLocal& L, int i, double depth,
+                             int64_t step, double t_old, int& seq) {
     const BoundaryDev& B = q.oc.bot;
     bool shallow = false;
     double position[3] = {L.c.pos[0], L.c.pos[1], L.c.pos[2]};
@@ -421,6 +526,10 @@ __device__ void bottom_local(const QueueDev& q, RayLocal& L, int i, double depth
         grazing = asin(-dot_full / c);
     }
     record_reflection(q, step, t_old, i, time_water, grazing, c, position, ndir, 0, seq);
+    if (q.want_verbs)
+        build_eigenverb(q, C, i, step, t_old, time_water, grazing, c, position, ndir, WQ3D_VERB_BOTTOM, L.c.c,
+                        L.surface, L.bottom, seq);
+    ++seq;
 
     const LossDev& Lo = B.loss;
     double amp0 = 0.0, ph0 = 0.0;
@@ -608,40 +717,43 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
                 for (int f = 0; f < q.nf; ++f) L.ph[f] -= M_PI_2;
             }
         }
+        /* the reference's detect_reflections for this ray: volume layers,
+         * then the surface / bottom chain, volume layers after each
+         * reflection (wave_queue.cc:202-256); seq orders the ray's events */
+        const bool vol = q.want_verbs && q.oc.nvol > 0;
         bool reflected = false;
         int seq = 0;
         int next_try = -1; /* 0: try bottom next, 1: try surface next */
-        if (L.x.pos[0] - q.R > 0.0 && surface_local(q, L, i, s + 1, t_old, seq)) {
-            ++seq;
+        if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
+        if (L.x.pos[0] - q.R > 0.0 && surface_local(q, *R.C, L, i, s + 1, t_old, seq)) {
             L.surface += 1;
             reflected = true;
             next_try = 0;
         } else {
             const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
             if (depth > 0.0) {
-                bottom_local(q, L, i, depth, s + 1, t_old, seq);
-                ++seq;
+                bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq);
                 L.bottom += 1;
                 reflected = true;
                 next_try = 1;
             }
         }
         if (reflected) {
+            if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
             int it = 0;
             for (; it < MAX_BOUNCE; ++it) {
                 if (next_try == 0) {
                     const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
                     if (!(depth > 0.0)) break;
-                    bottom_local(q, L, i, depth, s + 1, t_old, seq);
-                    ++seq;
+                    bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq);
                     L.bottom += 1;
                     next_try = 1;
                 } else {
-                    if (!(L.x.pos[0] - q.R > 0.0 && surface_local(q, L, i, s + 1, t_old, seq))) break;
-                    ++seq;
+                    if (!(L.x.pos[0] - q.R > 0.0 && surface_local(q, *R.C, L, i, s + 1, t_old, seq))) break;
                     L.surface += 1;
                     next_try = 0;
                 }
+                if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
             }
             if (it == MAX_BOUNCE) set_err(q, ERR_BOUNCE_LIMIT);
         }
@@ -779,6 +891,30 @@ __global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp
 }  // namespace WQ3D_KERNEL_NS
 
 #if !WQ3D_STEP_KERNELS_ONLY
+/* Volume-layer eigenverbs of the rays that do not reflect in step s
+ * (wave_queue.cc:202; k_reflect handles the reflecting ones).  Launched
+ * before k_advance of the same step, only when an eigenverb listener is
+ * installed and the ocean has volume layers. */
+__global__ void __launch_bounds__(128) k_volume(const QueueDev* __restrict__ qp, int k) {
+    const QueueDev& q = *qp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q.n) return;
+    const int64_t s = *q.d_base + k;
+    if (q.flag[s & 1][i]) return;
+    Roles R;
+    roles_at(q, s, R);
+    const double rc = R.C->pos[0][i], rx = R.X->pos[0][i];
+    bool cross = false;
+    for (int v = 0; v < q.oc.nvol; ++v) cross |= (q.oc.vol_rho[v] - rx) * (q.oc.vol_rho[v] - rc) < 0;
+    if (!cross) return;
+    RayS y0, y1, y2;
+    load_ray(*R.V, i, y0);
+    load_ray(*R.C, i, y1);
+    load_ray(*R.X, i, y2);
+    int seq = 0;
+    volume_scatter(q, *R.C, i, s + 1, q.d_times[k], y0, y1, y2, R.C->surface[i], R.C->bottom[i], seq);
+}
+
 /* ------------------------------------------------------------------ */
 /* CPA search (wave_queue.cc:351-488)                                  */
 /* ------------------------------------------------------------------ */

@@ -361,7 +361,13 @@ struct OceanDev {
     ProfileDev prof;
     BoundaryDev surf;
     BoundaryDev bot;
+    int nvol;                        /* volume scattering layers          */
+    double vol_rho[WQ3D_MAX_VOLUME]; /* volume_flat::_rho (volume_flat.h:32-37) */
 };
+
+/* to_radians / to_degrees of the reference's math_traits */
+WQ_HD double deg2rad(double t) { return t * (M_PI / 180.0); }
+WQ_HD double rad2deg(double t) { return t * (180.0 / M_PI); }
 
 /* ------------------------------------------------------------------ */
 /* sound speed: profile_{linear,munk,catenary,n2}.cc + adjust_speed     */

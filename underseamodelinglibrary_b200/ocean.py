@@ -255,6 +255,16 @@ class boundary_grid(boundary_model):
         self.grid.fill(d.grid, keep if keep is not None else [])
 
 
+class volume_flat:
+    """volume_flat(depth, thickness, amplitude) (ocean/volume_flat.h:32-37):
+    a scattering layer at a constant depth below mean sea level."""
+
+    def __init__(self, depth=0.0, thickness=0.0, amplitude=-300.0):
+        self.depth = float(depth)
+        self.thickness = float(thickness)
+        self.amplitude = float(amplitude)
+
+
 class ocean_model:
     """ocean_model(surface, bottom, profile) (ocean/ocean_model.h:31-60)."""
 
@@ -262,11 +272,27 @@ class ocean_model:
         self._surface = surface
         self._bottom = bottom
         self._profile = profile
+        self._volume = []
         self._handle = None
         self._lib = None
 
     def surface(self):
         return self._surface
+
+    def add_volume(self, layer):
+        """ocean_model::add_volume (ocean/ocean_model.h:52); layers are
+        placed under the same earth radius as the boundaries."""
+        if len(self._volume) >= _abi.MAX_VOLUME:
+            raise ValueError("at most %d volume layers" % _abi.MAX_VOLUME)
+        if self._handle is not None:
+            raise RuntimeError("add volume layers before the ocean is first used")
+        self._volume.append(layer)
+
+    def num_volume(self):
+        return len(self._volume)
+
+    def volume(self, n):
+        return self._volume[n]
 
     def bottom(self):
         return self._bottom
@@ -285,6 +311,11 @@ class ocean_model:
                 model.fill(sub, self._keep)
             else:
                 model.fill(sub)
+        d.num_volume = len(self._volume)
+        for k, layer in enumerate(self._volume):
+            d.volume[k].depth = layer.depth
+            d.volume[k].thickness = layer.thickness
+            d.volume[k].amplitude = layer.amplitude
         # one construction radius serves both boundaries: build them under
         # the same wposition earth radius, as every reference caller does
         return d

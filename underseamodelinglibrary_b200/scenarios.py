@@ -18,7 +18,7 @@ import numpy as np
 from . import types as T
 from .ocean import (attenuation_constant, boundary_flat, boundary_grid, boundary_slope,
                     data_grid, ocean_model, profile_grid, profile_linear, profile_munk,
-                    reflect_loss_constant, reflect_loss_rayleigh)
+                    reflect_loss_constant, reflect_loss_rayleigh, volume_flat)
 from ._abi import HYBRID_GAUSSIAN
 
 
@@ -139,6 +139,34 @@ def bounce_threshold():
                  de=T.seq_linear(-90.0, 1.0, 90.0), az=T.seq_linear(0.0, 30.0, 360.0), dt=0.1,
                  targets=T.wposition(1, 1, 0.01, 0.0, -500.0), time_max=10.0,
                  thresholds=dict(max_surface=3, max_bottom=5))
+
+
+def eigenverb_accuracy():
+    """waveq3d/test/reverb_test.cc:216-310 -- isovelocity 1500 m/s, 1000 m
+    sand bottom, a volume layer at 300 m (10 m thick, -40 dB), source on
+    the surface at 45N 45W, 1 kHz, D/E -80..60 step 5 x AZ -40..40 step
+    10, dt 0.1 s for 3.5 s; eigenverbs only."""
+    T.set_earth_radius(6371000.0)
+    ocean = ocean_model(boundary_flat(), boundary_flat(1000.0, reflect_loss_rayleigh("sand")),
+                        profile_linear(1500.0))
+    ocean.add_volume(volume_flat(300.0, 10.0, -40.0))
+    return _pack(ocean=ocean, freq=T.seq_log(1000.0, 10.0, 1), pos=T.wposition1(45.0, -45.0, 0.0),
+                 de=T.seq_linear(-80.0, 5.0, 60.0), az=T.seq_linear(-40.0, 10.0, 40.1), dt=0.1,
+                 targets=None, time_max=3.5, depth=1000.0, c0=1500.0)
+
+
+def eigenverb_demo():
+    """waveq3d/test/reverb_test.cc:334-443 -- isovelocity 1500 m/s without
+    absorption, 200 m sand bottom, source on the surface, 1 kHz, 181
+    tangent-spaced D/E x AZ 0..340 step 20, dt 0.1 s for 4 s, at most 2
+    surface and 2 bottom bounces."""
+    T.set_earth_radius(6371000.0)
+    ocean = ocean_model(boundary_flat(), boundary_flat(200.0, reflect_loss_rayleigh("sand")),
+                        profile_linear(1500.0, attenuation_constant(0.0)))
+    return _pack(ocean=ocean, freq=T.seq_log(1000.0, 10.0, 1), pos=T.wposition1(45.0, -45.0, 0.0),
+                 de=T.seq_rayfan(-90.0, 90.0, 181), az=T.seq_linear(0.0, 20.0, 359.0), dt=0.1,
+                 targets=None, time_max=4.0, depth=200.0, c0=1500.0,
+                 thresholds=dict(max_bottom=2, max_surface=2))
 
 
 def munk_flat(num_de=181, num_az=37, n_targets=10, time_max=60.0):

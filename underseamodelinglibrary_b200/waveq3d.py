@@ -13,6 +13,7 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
+from .eigenverbs import eigenverb_model
 from .types import earth_radius, wposition1
 
 
@@ -169,6 +170,7 @@ class wave_queue:
         self._time_step = float(time_step)
         self._eig_listeners = []
         self._refl_listeners = []
+        self._verb_listeners = []
         self._run_id = int(run_id)
         self._thresh = _abi.wq3d_thresholds(300.0, 300.0, 999, 999, 999, 999, 999)
         self._cb = None
@@ -250,6 +252,11 @@ class wave_queue:
         self._thresh.intensity = abs(float(value))
         self._push_thresholds()
 
+    def eigenverb_threshold(self, value):
+        """power threshold in dB (wave_thresholds.h:87-89)"""
+        self._thresh.eigenverb = abs(float(value))
+        self._push_thresholds()
+
     def max_bottom(self, v):
         self._thresh.max_bottom = int(v)
         self._push_thresholds()
@@ -272,7 +279,7 @@ class wave_queue:
 
     # ---------------- listeners ----------------
     def _install_callbacks(self):
-        if not self._eig_listeners and not self._refl_listeners:
+        if not self._eig_listeners and not self._refl_listeners and not self._verb_listeners:
             _abi.check(self._lib, self._lib.wq3d_queue_set_callbacks(self._q, None, None))
             self._cb = None
             return
@@ -295,10 +302,16 @@ class wave_queue:
             for l in self._refl_listeners:
                 l.reflect(r.time, r.de, r.az, r.dt, r.grazing, r.speed, pos, nd, r.type)
 
+        def verb(ctx, vp, power, nf, interface_num):
+            v = eigenverb_model.from_record(vp.contents, power[:nf], freq)
+            for l in self._verb_listeners:
+                l.add_eigenverb(v, interface_num)
+
         cb = _abi.wq3d_callbacks()
         cb.add_eigenray = _abi.ADD_EIGENRAY(add) if self._eig_listeners else _abi.ADD_EIGENRAY()
         cb.check_eigenrays = _abi.CHECK_EIGENRAYS(check) if self._eig_listeners else _abi.CHECK_EIGENRAYS()
         cb.reflect = _abi.REFLECT(reflect) if self._refl_listeners else _abi.REFLECT()
+        cb.add_eigenverb = _abi.ADD_EIGENVERB(verb) if self._verb_listeners else _abi.ADD_EIGENVERB()
         self._cb = cb
         _abi.check(self._lib, self._lib.wq3d_queue_set_callbacks(self._q, C.byref(cb), None))
 
@@ -320,6 +333,17 @@ class wave_queue:
     def remove_reflection_listener(self, listener):
         if listener in self._refl_listeners:
             self._refl_listeners.remove(listener)
+        self._install_callbacks()
+
+    def add_eigenverb_listener(self, listener):
+        """eigenverb_notifier::add_eigenverb_listener (eigenverb_notifier.h)"""
+        if listener not in self._verb_listeners:
+            self._verb_listeners.append(listener)
+        self._install_callbacks()
+
+    def remove_eigenverb_listener(self, listener):
+        if listener in self._verb_listeners:
+            self._verb_listeners.remove(listener)
         self._install_callbacks()
 
     # ---------------- propagation ----------------
