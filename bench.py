@@ -188,23 +188,32 @@ def engine_arm(args, rank, world, dist):
         return S.build_queue(sc, u.wave_queue, device=0, precision=precision)
 
     def timed_runs(precision, count):
-        """device time (ms) of ``count`` propagations, queues built first"""
+        """device time (ms) of ``count`` propagations replayed as CUDA
+        graphs, queues built first; returns (total ms, launches, eigenrays)"""
         qs = [make(precision) for _ in range(count)]
         for q in qs:
-            q.set_timing(True)
             q.timing(reset=True)
-        tot = cpa = stp = eig = 0.0
+        tot = 0.0
         launches = neig = 0
         for q in qs:
             q.run(sc["time_max"])
             tm = q.timing()
             tot += tm["total_ms"]
-            cpa += tm["cpa_ms"]
-            stp += tm["step_ms"]
-            eig += tm["eigenray_ms"]
             launches += tm["launches"]
             neig += len(q.take_eigenrays())
-        return tot, cpa, stp, eig, launches, neig
+        return tot, launches, neig
+
+    def kernel_breakdown(precision):
+        """per-kernel device ms of one propagation with CUDA events around
+        every launch (direct launches, so slower than the graph replay)"""
+        q = make(precision)
+        q.set_timing(True)
+        q.timing(reset=True)
+        q.run(sc["time_max"])
+        tm = q.timing()
+        q.take_eigenrays()
+        return {"advance": tm["advance_ms"], "reflect (side stream)": tm["reflect_ms"],
+                "cpa": tm["cpa_ms"], "eigenray": tm["eigenray_ms"], "total_with_events": tm["total_ms"]}
 
     # device-resident timing: queues built (inputs in HBM) before the timer
     for _ in range(args.warmup):
@@ -216,12 +225,16 @@ def engine_arm(args, rank, world, dist):
     clocks.start()
     if dist is not None:
         dist.barrier()
-    total_ms, cpa_ms, step_ms, eig_ms, launches, n_eig = timed_runs(_abi.FP32C, args.steps)
+    total_ms, launches, n_eig = timed_runs(_abi.FP32C, args.steps)
     if dist is not None:
         dist.barrier()
     clk = clocks.stop()
-    # the plain FP64 form on the same workload, for the FP32C:FP64 ratio
-    f64_total, f64_cpa, f64_step, f64_eig, _, f64_neig = timed_runs(_abi.FP64, 1)
+    # kernel shares from an event-timed propagation, and the plain FP64 form
+    # on the same workload for the FP32C:FP64 ratio
+    kern = kernel_breakdown(_abi.FP32C)
+    f64_total, _, f64_neig = timed_runs(_abi.FP64, 1)
+    kern64 = kernel_breakdown(_abi.FP64)
+    cpa_ms = kern["cpa"]
 
     # end to end through the public API with host buffers
     e2e_times = []
@@ -249,8 +262,7 @@ def engine_arm(args, rank, world, dist):
 
     # roofline of the CPA kernel: algorithmic FP64 operations per launch
     interior = (nde - 2) * ((naz - 1) if _wraps(sc["az"]) else (naz - 2))
-    launches_cpa = args.steps * nsteps
-    cpa_launch_s = (cpa_ms / 1000.0) / launches_cpa
+    cpa_launch_s = (cpa_ms / 1000.0) / nsteps
     flops_launch = FLOPS_PER_RAY_TARGET_STEP * interior * nt
     achieved = flops_launch / cpa_launch_s / 1e12
     peaks = measure_fma_peaks()
@@ -269,11 +281,9 @@ def engine_arm(args, rank, world, dist):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "fp64_form": {"value": ray_steps / (f64_total / 1000.0), "ms_per_step": f64_total,
-                      "kernel_ms": {"reflect+advance": f64_step, "cpa": f64_cpa, "eigenray": f64_eig},
-                      "eigenrays": f64_neig},
+                      "kernel_ms": kern64, "eigenrays": f64_neig},
         "eigenrays_per_propagation": n_eig / args.steps,
-        "kernel_ms": {"reflect+advance": step_ms / args.steps, "cpa": cpa_ms / args.steps,
-                      "eigenray": eig_ms / args.steps},
+        "kernel_ms": kern,
         "roofline": {"bound": "fp32", "achieved": achieved,
                      "peak": fp32_peak,
                      "unit": "TFLOP/s",
@@ -283,7 +293,7 @@ def engine_arm(args, rank, world, dist):
                      "peak_source": peaks["source"] + "; MEASURED_PEAKS.json has no FP32/FP64 CUDA-core figure",
                      "fp64_peak": peaks["fp64"],
                      "fp64_form_cpa_frac_of_fp64_peak": (
-                         flops_launch / (f64_cpa / 1000.0 / nsteps) / 1e12 / peaks["fp64"]) if peaks["fp64"] else None,
+                         flops_launch / (kern64["cpa"] / 1000.0 / nsteps) / 1e12 / peaks["fp64"]) if peaks["fp64"] else None,
                      "algorithmic_flops_per_launch": flops_launch},
         "roofline_hbm": hbm_roofline(interior, cpa_launch_s),
         "clocks": clk,

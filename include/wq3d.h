@@ -419,14 +419,21 @@ int wq3d_queue_take_eigenrays(wq3d_queue* q, wq3d_eigenray* rays,
  * (thread_task::abort, wavegen/wavefront_generator.cc:55-58,100-108). */
 int wq3d_queue_abort(wq3d_queue* q);
 
-/* Device time (ms, CUDA events on the queue's stream) accumulated since
- * the last reset: whole wq3d_queue_step/run calls (ms_total, including the
- * host's result handling between chunks) and, while per-kernel timing is
- * on, the step/edge, CPA and eigenray kernels; plus the number of kernel
- * launches.  No reference counterpart: benchmarking aid. */
-int wq3d_queue_timing(wq3d_queue* q, double* ms_total, double* ms_step_kernels,
-                      double* ms_cpa_kernel, double* ms_eigenray_kernel,
-                      int64_t* launches, int reset);
+/* Device time (ms, CUDA events) accumulated since the last reset. */
+typedef struct wq3d_timing {
+    double ms_total;     /* whole wq3d_queue_step/run calls on the queue's
+                            stream, host result handling between chunks
+                            included                                    */
+    double ms_advance;   /* k_advance (and k_volume), timing mode only  */
+    double ms_reflect;   /* k_reflect on its side stream, timing mode only */
+    double ms_cpa;       /* k_cpa / k_cpa_f32, timing mode only          */
+    double ms_eigenray;  /* k_eigenray, timing mode only                 */
+    int64_t launches;    /* kernel launches                              */
+} wq3d_timing;
+
+/* Reads (and optionally resets) the timing counters.  No reference
+ * counterpart: benchmarking aid. */
+int wq3d_queue_timing(wq3d_queue* q, wq3d_timing* out, int reset);
 
 /* Turns per-kernel CUDA-event timing on (direct launches, events around
  * every kernel) or off (chunks replayed as one CUDA graph, the default).

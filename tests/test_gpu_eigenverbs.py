@@ -117,6 +117,15 @@ def test_eigenverbs_gridded_ocean(engine):
     compare_verbs(eng, orc)
 
 
+def test_bounce_threshold_eigenverbs(engine):
+    """reflection_test.cc:597-661 eigenverb half on the engine, equal to
+    the oracle's"""
+    sc = S.bounce_threshold()
+    eng, orc = run_both(sc)
+    assert len(eng) > 100 and all(v.bottom <= 5 and v.surface <= 3 for v in eng)
+    compare_verbs(eng, orc)
+
+
 def test_reflection_notice_precedes_its_eigenverb(engine):
     """a listener on both streams sees each boundary eigenverb right after
     the reflection notice of the same collision (reflection_model.cc:

@@ -200,16 +200,19 @@ def test_reflect_slope():
     assert bottoms >= 2 and surfaces >= 2
 
 
-def test_bounce_threshold_eigenrays():
-    """reflection_test.cc:597-661 (eigenray half): no eigenray has more
-    bounces than max_bottom / max_surface"""
+def test_bounce_threshold():
+    """reflection_test.cc:597-661: no eigenray and no bottom or surface
+    eigenverb has more bounces than max_bottom / max_surface"""
     sc = S.bounce_threshold()
-    q = S.build_queue(sc, OracleQueue)
+    q = S.build_queue(sc, OracleQueue, eigenverbs=True)
     q.run(sc["time_max"])
     rays = q.take_eigenrays()
     assert len(rays) > 0
     assert max(r.bottom for r in rays) <= 5 and max(r.surface for r in rays) <= 3
     assert any(r.bottom == 5 for r in rays) or any(r.surface == 3 for r in rays)
+    verbs = [v for v in q.take_eigenverbs() if v.interface_num in (0, 1)]
+    assert len(verbs) > 100
+    assert all(v.bottom <= 5 and v.surface <= 3 for v in verbs)
 
 
 def test_thorp_gsm_table():

@@ -105,6 +105,11 @@ class wq3d_reflection(C.Structure):
                 ("type", C.c_int32), ("pad", C.c_int32), ("step", C.c_int64)]
 
 
+class wq3d_timing(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("ms_advance", C.c_double), ("ms_reflect", C.c_double),
+                ("ms_cpa", C.c_double), ("ms_eigenray", C.c_double), ("launches", C.c_int64)]
+
+
 class wq3d_eigenverb(C.Structure):
     _fields_ = [("travel_time", C.c_double), ("length", C.c_double), ("width", C.c_double),
                 ("position", C.c_double * 3), ("direction", C.c_double), ("grazing", C.c_double),
@@ -160,7 +165,7 @@ SIGNATURES = {
     "wq3d_queue_take_eigenrays": (C.c_int, [C.c_void_p, C.POINTER(wq3d_eigenray), dp, dp,
                                             C.c_size_t, C.POINTER(C.c_size_t)]),
     "wq3d_queue_abort": (C.c_int, [C.c_void_p]),
-    "wq3d_queue_timing": (C.c_int, [C.c_void_p, dp, dp, dp, dp, C.POINTER(C.c_int64), C.c_int]),
+    "wq3d_queue_timing": (C.c_int, [C.c_void_p, C.POINTER(wq3d_timing), C.c_int]),
     "wq3d_queue_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "wq3d_last_error_string": (C.c_char_p, []),
     "wq3d_abi_version": (C.c_int, []),

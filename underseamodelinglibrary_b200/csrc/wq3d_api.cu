@@ -227,7 +227,7 @@ struct wq3d_queue {
     std::atomic<bool> abort_flag{false};
     bool timing = false;
     std::vector<cudaEvent_t> events;
-    double ms_step = 0.0, ms_cpa = 0.0, ms_eig = 0.0, ms_total = 0.0;
+    double ms_step = 0.0, ms_cpa = 0.0, ms_eig = 0.0, ms_total = 0.0, ms_refl = 0.0;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     int64_t launches = 0;
     /* the stepping kernels' build: "gridded" when the ocean has a grid */
@@ -324,10 +324,12 @@ struct wq3d_queue {
         const dim3 blk(128);
         const dim3 grd((n + 127) / 128);
         const int rgrid = std::max(1, std::min(4 * 148, (n + 63) / 64));
+        if (timing) cudaEventRecord(events[7 * K], stream);
         k_reflect_fn<<<rgrid, 64, 0, stream>>>(d_q, 0);
+        if (timing) cudaEventRecord(events[7 * K + 1], stream);
         launches += 1;
         for (int k = 0; k < K; ++k) {
-            cudaEvent_t* ev = timing ? &events[5 * k] : nullptr;
+            cudaEvent_t* ev = timing ? &events[7 * k] : nullptr;
             if (ev) cudaEventRecord(ev[0], stream);
             if (volume_pass()) {
                 k_volume<<<grd, blk, 0, stream>>>(d_q, k);
@@ -340,7 +342,9 @@ struct wq3d_queue {
             if (more) {
                 cudaEventRecord(fork_ev[k], stream);
                 cudaStreamWaitEvent(side, fork_ev[k], 0);
+                if (ev) cudaEventRecord(ev[5], side);
                 k_reflect_fn<<<rgrid, 64, 0, side>>>(d_q, k + 1);
+                if (ev) cudaEventRecord(ev[6], side);
                 cudaEventRecord(join_ev[k], side);
                 launches += 1;
             }
@@ -486,14 +490,19 @@ struct wq3d_queue {
         WQ_CK(cudaMemcpyAsync(h_counts, d_counts, 9 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         WQ_CK(cudaStreamSynchronize(stream));
         if (timing) {
+            float r0 = 0;
+            cudaEventElapsedTime(&r0, events[7 * K], events[7 * K + 1]);
+            ms_refl += r0;
             for (int k = 0; k < K; ++k) {
-                float a = 0, b = 0, c = 0;
-                cudaEventElapsedTime(&a, events[5 * k], events[5 * k + 1]);
-                cudaEventElapsedTime(&b, events[5 * k + 2], events[5 * k + 3]);
-                cudaEventElapsedTime(&c, events[5 * k + 3], events[5 * k + 4]);
+                float a = 0, b = 0, c = 0, r = 0;
+                cudaEventElapsedTime(&a, events[7 * k], events[7 * k + 1]);
+                cudaEventElapsedTime(&b, events[7 * k + 2], events[7 * k + 3]);
+                cudaEventElapsedTime(&c, events[7 * k + 3], events[7 * k + 4]);
+                if (k + 1 < K) cudaEventElapsedTime(&r, events[7 * k + 5], events[7 * k + 6]);
                 ms_step += a;
                 ms_cpa += b;
                 ms_eig += c;
+                ms_refl += r;
             }
         }
         const uint32_t nrec = std::min(h_counts[0], h.cap_rec);
@@ -999,7 +1008,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         if (cudaEventCreateWithFlags(&q->fork_ev[k], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&q->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-    q->events.resize(5 * (size_t)q->chunk);
+    q->events.resize(7 * (size_t)q->chunk + 2);
     for (auto& ev : q->events)
         if (cudaEventCreate(&ev) != cudaSuccess) return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
     *out = q;
@@ -1170,16 +1179,18 @@ int wq3d_queue_abort(wq3d_queue* q) {
     return WQ3D_OK;
 }
 
-int wq3d_queue_timing(wq3d_queue* q, double* ms_total, double* ms_step, double* ms_cpa,
-                      double* ms_eig, int64_t* launches, int reset) {
+int wq3d_queue_timing(wq3d_queue* q, wq3d_timing* out, int reset) {
     if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
-    if (ms_total) *ms_total = q->ms_total;
-    if (ms_step) *ms_step = q->ms_step;
-    if (ms_cpa) *ms_cpa = q->ms_cpa;
-    if (ms_eig) *ms_eig = q->ms_eig;
-    if (launches) *launches = q->launches;
+    if (out) {
+        out->ms_total = q->ms_total;
+        out->ms_advance = q->ms_step;
+        out->ms_reflect = q->ms_refl;
+        out->ms_cpa = q->ms_cpa;
+        out->ms_eigenray = q->ms_eig;
+        out->launches = q->launches;
+    }
     if (reset) {
-        q->ms_step = q->ms_cpa = q->ms_eig = q->ms_total = 0.0;
+        q->ms_step = q->ms_cpa = q->ms_eig = q->ms_total = q->ms_refl = 0.0;
         q->launches = 0;
     }
     return WQ3D_OK;

@@ -380,9 +380,9 @@ class wave_queue:
         _abi.check(self._lib, self._lib.wq3d_queue_set_timing(self._q, 1 if on else 0))
 
     def timing(self, reset=False):
-        t, a, b, c = C.c_double(), C.c_double(), C.c_double(), C.c_double()
-        n = C.c_int64()
-        _abi.check(self._lib, self._lib.wq3d_queue_timing(self._q, C.byref(t), C.byref(a), C.byref(b),
-                                                          C.byref(c), C.byref(n), 1 if reset else 0))
-        return {"total_ms": t.value, "step_ms": a.value, "cpa_ms": b.value, "eigenray_ms": c.value,
-                "launches": n.value}
+        """device milliseconds since the last reset (wq3d_queue_timing): the
+        whole step/run calls, and per kernel while timing mode is on"""
+        t = _abi.wq3d_timing()
+        _abi.check(self._lib, self._lib.wq3d_queue_timing(self._q, C.byref(t), 1 if reset else 0))
+        return {"total_ms": t.ms_total, "advance_ms": t.ms_advance, "reflect_ms": t.ms_reflect,
+                "cpa_ms": t.ms_cpa, "eigenray_ms": t.ms_eigenray, "launches": t.launches}
