@@ -1053,7 +1053,19 @@ __global__ void __launch_bounds__(CPA_THREADS) k_cpa(const QueueDev* __restrict_
  * (each within 5 x 2^-53 (rho^2 + R^2), 0.05 m^2 at earth radius).  The
  * screen only rejects; every pair it does not reject is queued per warp and
  * finished in FP64 exactly as k_cpa does, 32 at a time so the lanes stay
- * converged.  Hence the eigenrays equal the FP64 form's. */
+ * converged.  Hence the eigenrays equal the FP64 form's.
+ *
+ * A block holds a patch of CPA_PATCH_DE x CPA_PATCH_AZ neighbouring rays,
+ * whose positions and directions are close, so for a given target the
+ * screen's value sum_k w_k dq_k varies little across the patch.  Before
+ * the per-ray loop, each target is tested once for the whole patch: with
+ * lo_k <= dq_k <= hi_k over the patch's rays, sum_k max(w_k lo_k, w_k hi_k)
+ * (exact products of FP32 values, summed in FP64) bounds every ray's exact
+ * value; adding the FP32 evaluation error (8 u sum W_k M_k, M_k = max
+ * |dq_k|) and the largest guard of the patch (33 u sum W_k M_k + c0), a
+ * negative bound means every ray of the patch would reject the target, so
+ * it is dropped before the loop.  Only the targets that survive for the
+ * "next" and the "prev" comparison reach the per-ray loop. */
 namespace {
 constexpr int F32_TARGETS = CPA_F32_TARGETS;
 struct TgtW {
@@ -1063,15 +1075,16 @@ struct WarpQueue {
     uint32_t e[64];
 };
 
-/* finishes queued pairs in FP64: entry = (lane of the ray << 16) | target */
+/* finishes queued pairs in FP64: entry = (thread of the ray << 16) | target */
 __device__ void cpa_finish(const QueueDev& q, const FrontPtrs& V, const FrontPtrs& C,
-                           const FrontPtrs& X, const TgtS* tile, int t0, int ray_base,
+                           const FrontPtrs& X, const TgtS* tile, int t0, int de0, int az0,
                            const uint32_t* e, int count, int lane) {
     if (lane >= count) return;
     const uint32_t v = e[lane];
     const int j = (int)(v & 0xffffu);
-    const int i = ray_base + (int)(v >> 16);
-    const int de = i / q.naz, az = i % q.naz;
+    const int th = (int)(v >> 16);
+    const int de = de0 + th / CPA_PATCH_AZ, az = az0 + th % CPA_PATCH_AZ;
+    const int i = de * q.naz + az;
     const TgtS t = tile[j];
     const double center = d2_at(C, i, t);
     if (d2_at(X, i, t) <= center) return;
@@ -1086,76 +1099,64 @@ __device__ void cpa_finish(const QueueDev& q, const FrontPtrs& V, const FrontPtr
         set_err(q, ERR_CAND_OVERFLOW);
     }
 }
+
+/* whether every ray of the patch rejects a target on one comparison */
+__device__ __forceinline__ bool patch_rejects(const TgtW& g, const float* lo, const float* hi,
+                                              const float* W, float c0) {
+    double ub = 0.0, mag = 0.0, wm = 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const double w = (double)g.w[m];
+        const double a = w * (double)lo[m], b = w * (double)hi[m];
+        ub += fmax(a, b);
+        mag += fmax(fabs(a), fabs(b));
+        wm += (double)W[m] * fmax(fabs((double)lo[m]), fabs((double)hi[m]));
+    }
+    const double u = 5.9604644775390625e-8; /* 2^-24 */
+    return ub + 1e-15 * mag + 41.0 * u * wm + 1.0001 * (double)c0 < 0.0;
+}
 }  // namespace
 
-__global__ void __launch_bounds__(CPA_THREADS) k_cpa_f32(const QueueDev* __restrict__ qp, int k) {
+__global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(const QueueDev* __restrict__ qp, int k) {
     const QueueDev& q = *qp;
     __shared__ TgtS tile[F32_TARGETS];
     __shared__ TgtW tw[F32_TARGETS];
     __shared__ float wmax[CPA_THREADS / 32][8];
+    __shared__ float red[CPA_THREADS / 32][32];
+    __shared__ float bound[32];
+    __shared__ uint16_t surv[F32_TARGETS];
+    __shared__ int nsurv;
     __shared__ WarpQueue wq[CPA_THREADS / 32];
     const int64_t s = *q.d_base + k + 1;
     const FrontPtrs& V = q.F[(s + 1) & 3];
     const FrontPtrs& C = q.F[(s + 2) & 3];
     const FrontPtrs& X = q.F[(s + 3) & 3];
-    const int t0 = blockIdx.y * F32_TARGETS;
-    const int nt_tile = min(F32_TARGETS, q.nt - t0);
-    const int ray_base = blockIdx.x * blockDim.x;
-    const int i_ref = min(ray_base, q.n - 1);
-    const double rho0 = C.cpa[0][i_ref], th0 = C.cpa[1][i_ref], ph0 = C.cpa[2][i_ref];
+    if (q.nde < 3 || q.naz < 3 || q.nt <= 0) return;
+    const int n_pa = (q.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ;
+    const int de0 = (blockIdx.x / n_pa) * CPA_PATCH_DE;
+    const int az0 = (blockIdx.x % n_pa) * CPA_PATCH_AZ;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float W[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
-        const int t = t0 + j;
-        const double R = q.tgt[0][t], T = q.tgt[1][t], P = q.tgt[2][t], S = q.tgt_sin[t];
-        tile[j] = TgtS{T, P, S, q.tgt_R2[t], q.tgt_2R[t]};
-        const double Rr = R - rho0, Xo = T - th0, Yo = P - ph0, RS = R * S;
-        TgtW g;
-        g.w[0] = 1.0f;
-        g.w[1] = (float)(-2.0 * Rr);
-        g.w[2] = (float)R;
-        g.w[3] = (float)(-2.0 * R * Xo);
-        g.w[4] = (float)(R * Xo * Xo);
-        g.w[5] = (float)RS;
-        g.w[6] = (float)(-2.0 * RS * Yo);
-        g.w[7] = (float)(RS * Yo * Yo);
-        tw[j] = g;
-#pragma unroll
-        for (int m = 0; m < 8; ++m) W[m] = fmaxf(W[m], fabsf(g.w[m]));
-    }
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) W[m] = fmaxf(W[m], __shfl_xor_sync(0xffffffffu, W[m], o));
-    }
-    if (lane == 0)
-        for (int m = 0; m < 8; ++m) wmax[w][m] = W[m];
-    __syncthreads();
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-        float v = 0.0f;
-        for (int j = 0; j < CPA_THREADS / 32; ++j) v = fmaxf(v, wmax[j][m]);
-        W[m] = v * 1.0001f;
-    }
-
-    /* this thread's ray: feature differences next-curr and prev-curr */
-    const int i = ray_base + threadIdx.x;
-    bool active = i < q.n && q.nde >= 3 && q.naz >= 3;
+    const int de = de0 + threadIdx.x / CPA_PATCH_AZ, az = az0 + threadIdx.x % CPA_PATCH_AZ;
+    bool active = de < q.nde && az < q.naz;
+    const int i = active ? de * q.naz + az : 0;
     if (active) {
-        const int de = i / q.naz, az = i % q.naz;
         const int az_start = q.az_boundary ? 0 : 1;
         active = !(de < 1 || de >= q.nde - 1 || az < az_start || az >= q.naz - 1) && !C.on_edge[i];
     }
+    if (!__syncthreads_or(active)) return;
+    /* local coordinates about the patch's middle ray */
+    const int i_ref = min(de0 + CPA_PATCH_DE / 2, q.nde - 1) * q.naz + min(az0 + CPA_PATCH_AZ / 2, q.naz - 1);
+    const double rho0 = C.cpa[0][i_ref], th0 = C.cpa[1][i_ref], ph0 = C.cpa[2][i_ref];
+
+    /* this thread's ray: feature differences next-curr and prev-curr */
     float dxc[8], dvc[8];
-    float gxc = 0.0f, gvc = 0.0f;
     {
-        const int ic = min(i, q.n - 1);
         double fq[3][8];
         const FrontPtrs* fr[3] = {&V, &C, &X};
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            const double rho = fr[m]->cpa[0][ic], sn = fr[m]->cpa[3][ic];
-            const double r = rho - rho0, x = fr[m]->cpa[1][ic] - th0, y = fr[m]->cpa[2][ic] - ph0;
+            const double rho = fr[m]->cpa[0][i], sn = fr[m]->cpa[3][i];
+            const double r = rho - rho0, x = fr[m]->cpa[1][i] - th0, y = fr[m]->cpa[2][i] - ph0;
             const double rs = rho * sn;
             fq[m][0] = r * r;
             fq[m][1] = r;
@@ -1166,50 +1167,130 @@ __global__ void __launch_bounds__(CPA_THREADS) k_cpa_f32(const QueueDev* __restr
             fq[m][6] = rs * y;
             fq[m][7] = rs;
         }
-        const float u = 5.9604645e-8f;
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
             dxc[m] = (float)(fq[2][m] - fq[1][m]);
             dvc[m] = (float)(fq[0][m] - fq[1][m]);
+        }
+    }
+    /* feature ranges over the patch's active rays: bound[0..7] / [8..15]
+     * low / high of dxc, [16..23] / [24..31] of dvc */
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        float l1 = active ? dxc[m] : INFINITY, h1 = active ? dxc[m] : -INFINITY;
+        float l2 = active ? dvc[m] : INFINITY, h2 = active ? dvc[m] : -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            l1 = fminf(l1, __shfl_xor_sync(0xffffffffu, l1, o));
+            h1 = fmaxf(h1, __shfl_xor_sync(0xffffffffu, h1, o));
+            l2 = fminf(l2, __shfl_xor_sync(0xffffffffu, l2, o));
+            h2 = fmaxf(h2, __shfl_xor_sync(0xffffffffu, h2, o));
+        }
+        if (lane == 0) {
+            red[w][m] = l1;
+            red[w][8 + m] = h1;
+            red[w][16 + m] = l2;
+            red[w][24 + m] = h2;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const bool low = (threadIdx.x & 8) == 0;
+        float v = red[0][threadIdx.x];
+        for (int j = 1; j < CPA_THREADS / 32; ++j) v = low ? fminf(v, red[j][threadIdx.x]) : fmaxf(v, red[j][threadIdx.x]);
+        bound[threadIdx.x] = v;
+    }
+
+    uint32_t* myq = wq[w].e;
+    const unsigned lt = (1u << lane) - 1u;
+    const float u = 5.9604645e-8f;
+    for (int t0 = 0; t0 < q.nt; t0 += F32_TARGETS) {
+        const int nt_tile = min(F32_TARGETS, q.nt - t0);
+        float W[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
+            const int t = t0 + j;
+            const double R = q.tgt[0][t], T = q.tgt[1][t], P = q.tgt[2][t], S = q.tgt_sin[t];
+            tile[j] = TgtS{T, P, S, q.tgt_R2[t], q.tgt_2R[t]};
+            const double Rr = R - rho0, Xo = T - th0, Yo = P - ph0, RS = R * S;
+            TgtW g;
+            g.w[0] = 1.0f;
+            g.w[1] = (float)(-2.0 * Rr);
+            g.w[2] = (float)R;
+            g.w[3] = (float)(-2.0 * R * Xo);
+            g.w[4] = (float)(R * Xo * Xo);
+            g.w[5] = (float)RS;
+            g.w[6] = (float)(-2.0 * RS * Yo);
+            g.w[7] = (float)(RS * Yo * Yo);
+            tw[j] = g;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) W[m] = fmaxf(W[m], fabsf(g.w[m]));
+        }
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) W[m] = fmaxf(W[m], __shfl_xor_sync(0xffffffffu, W[m], o));
+        }
+        if (lane == 0)
+            for (int m = 0; m < 8; ++m) wmax[w][m] = W[m];
+        if (threadIdx.x == 0) nsurv = 0;
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            float v = 0.0f;
+            for (int j = 0; j < CPA_THREADS / 32; ++j) v = fmaxf(v, wmax[j][m]);
+            W[m] = v * 1.0001f;
+        }
+        /* the guards of this tile, per ray and for the patch bound */
+        const float r0 = (float)rho0;
+        const float c0 = fmaxf(1.0f, 4.0e-15f * (r0 * r0 + W[2] * W[2]));
+        float gxc = 0.0f, gvc = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
             gxc = fmaf(W[m], fabsf(dxc[m]), gxc);
             gvc = fmaf(W[m], fabsf(dvc[m]), gvc);
         }
-        /* rounding of the reference's FP64 expression on both fronts */
-        const float r0 = (float)rho0;
-        const float c0 = fmaxf(1.0f, 4.0e-15f * (r0 * r0 + W[2] * W[2]));
         gxc = fmaf(32.0f * u, gxc, c0);
         gvc = fmaf(32.0f * u, gvc, c0);
-    }
-    uint32_t* myq = wq[w].e;
-    int qn = 0;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int j = 0; j < nt_tile; ++j) {
-        const TgtW g = tw[j];
-        float a = dxc[0];
-#pragma unroll
-        for (int m = 1; m < 8; ++m) a = fmaf(g.w[m], dxc[m], a);
-        bool want = active && !(a < -gxc);
-        if (want) {
-            float b = dvc[0];
-#pragma unroll
-            for (int m = 1; m < 8; ++m) b = fmaf(g.w[m], dvc[m], b);
-            want = !(b < -gvc);
+        /* targets that some ray of the patch may keep */
+        for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
+            const TgtW g = tw[j];
+            if (patch_rejects(g, &bound[0], &bound[8], W, c0)) continue;
+            if (patch_rejects(g, &bound[16], &bound[24], W, c0)) continue;
+            surv[atomicAdd(&nsurv, 1)] = (uint16_t)j;
         }
-        const unsigned mask = __ballot_sync(0xffffffffu, want);
-        if (mask) {
-            if (want) myq[qn + __popc(mask & lt)] = ((uint32_t)(w * 32 + lane) << 16) | (uint32_t)j;
-            qn += __popc(mask);
-            __syncwarp();
-            if (qn >= 32) {
-                cpa_finish(q, V, C, X, tile, t0, ray_base, myq, 32, lane);
+        __syncthreads();
+        const int ns = nsurv;
+        int qn = 0;
+        for (int sidx = 0; sidx < ns; ++sidx) {
+            const int j = surv[sidx];
+            const TgtW g = tw[j];
+            float a = dxc[0];
+#pragma unroll
+            for (int m = 1; m < 8; ++m) a = fmaf(g.w[m], dxc[m], a);
+            bool want = active && !(a < -gxc);
+            if (want) {
+                float b = dvc[0];
+#pragma unroll
+                for (int m = 1; m < 8; ++m) b = fmaf(g.w[m], dvc[m], b);
+                want = !(b < -gvc);
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, want);
+            if (mask) {
+                if (want) myq[qn + __popc(mask & lt)] = ((uint32_t)threadIdx.x << 16) | (uint32_t)j;
+                qn += __popc(mask);
                 __syncwarp();
-                if (lane < qn - 32) myq[lane] = myq[32 + lane];
-                __syncwarp();
-                qn -= 32;
+                if (qn >= 32) {
+                    cpa_finish(q, V, C, X, tile, t0, de0, az0, myq, 32, lane);
+                    __syncwarp();
+                    if (lane < qn - 32) myq[lane] = myq[32 + lane];
+                    __syncwarp();
+                    qn -= 32;
+                }
             }
         }
+        if (qn > 0) cpa_finish(q, V, C, X, tile, t0, de0, az0, myq, qn, lane);
+        __syncthreads();
     }
-    if (qn > 0) cpa_finish(q, V, C, X, tile, t0, ray_base, myq, qn, lane);
 }
 
 /* ------------------------------------------------------------------ */
