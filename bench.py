@@ -414,8 +414,9 @@ def main():
     if args.profile_steps:
         import underseamodelinglibrary_b200 as u
         from underseamodelinglibrary_b200 import scenarios as S
+        from underseamodelinglibrary_b200 import _abi
         sc = S.linear_slope_rayleigh()
-        q = S.build_queue(sc, u.wave_queue, device=0)
+        q = S.build_queue(sc, u.wave_queue, device=0, precision=_abi.FP32C)
         q.step(args.profile_steps)
         print("profile run: %d steps, %d eigenrays" % (q.steps(), len(q.take_eigenrays())))
         return

@@ -352,8 +352,9 @@ struct wq3d_queue {
             if (h.nt > 0) {
                 const dim3 cg((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS);
                 if (h.precision == WQ3D_FP32C)
-                    k_cpa_f32<<<((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) *
-                                    ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
+                    k_cpa_f32<<<dim3(((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) *
+                                         ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
+                                     (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS),
                                 CPA_THREADS, 0, stream>>>(d_q, k);
                 else
                     k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d_q, k);

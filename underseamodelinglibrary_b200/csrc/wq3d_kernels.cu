@@ -1076,7 +1076,7 @@ struct WarpQueue {
 };
 
 /* finishes queued pairs in FP64: entry = (thread of the ray << 16) | target */
-__device__ void cpa_finish(const QueueDev& q, const FrontPtrs& V, const FrontPtrs& C,
+__device__ __noinline__ void cpa_finish(const QueueDev& q, const FrontPtrs& V, const FrontPtrs& C,
                            const FrontPtrs& X, const TgtS* tile, int t0, int de0, int az0,
                            const uint32_t* e, int count, int lane) {
     if (lane >= count) return;
@@ -1116,6 +1116,14 @@ __device__ __forceinline__ bool patch_rejects(const TgtW& g, const float* lo, co
     return ub + 1e-15 * mag + 41.0 * u * wm + 1.0001 * (double)c0 < 0.0;
 }
 }  // namespace
+
+/* FP32 screen value sum_k w_k dq_k as two 4-term chains (any summation
+ * order stays within the guard's 8 u bound) */
+__device__ __forceinline__ float screen_dot(const TgtW& g, const float* d) {
+    float a = fmaf(g.w[3], d[3], fmaf(g.w[2], d[2], fmaf(g.w[1], d[1], d[0])));
+    float b = fmaf(g.w[7], d[7], fmaf(g.w[6], d[6], fmaf(g.w[5], d[5], g.w[4] * d[4])));
+    return a + b;
+}
 
 __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(const QueueDev* __restrict__ qp, int k) {
     const QueueDev& q = *qp;
@@ -1204,7 +1212,10 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(const QueueDev* __re
     uint32_t* myq = wq[w].e;
     const unsigned lt = (1u << lane) - 1u;
     const float u = 5.9604645e-8f;
-    for (int t0 = 0; t0 < q.nt; t0 += F32_TARGETS) {
+    /* this block's tile of targets (grid.y splits a patch's targets) */
+    {
+        const int t0 = blockIdx.y * F32_TARGETS;
+        if (t0 >= q.nt) return;
         const int nt_tile = min(F32_TARGETS, q.nt - t0);
         float W[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
@@ -1261,19 +1272,8 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(const QueueDev* __re
         __syncthreads();
         const int ns = nsurv;
         int qn = 0;
-        for (int sidx = 0; sidx < ns; ++sidx) {
-            const int j = surv[sidx];
-            const TgtW g = tw[j];
-            float a = dxc[0];
-#pragma unroll
-            for (int m = 1; m < 8; ++m) a = fmaf(g.w[m], dxc[m], a);
-            bool want = active && !(a < -gxc);
-            if (want) {
-                float b = dvc[0];
-#pragma unroll
-                for (int m = 1; m < 8; ++m) b = fmaf(g.w[m], dvc[m], b);
-                want = !(b < -gvc);
-            }
+        /* appends this lane's pair if "want"; finishes 32 at a time */
+        auto push = [&](bool want, int j) {
             const unsigned mask = __ballot_sync(0xffffffffu, want);
             if (mask) {
                 if (want) myq[qn + __popc(mask & lt)] = ((uint32_t)threadIdx.x << 16) | (uint32_t)j;
@@ -1287,9 +1287,29 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(const QueueDev* __re
                     qn -= 32;
                 }
             }
+        };
+        int sidx = 0;
+        for (; sidx + 1 < ns; sidx += 2) {
+            const int j0 = surv[sidx], j1 = surv[sidx + 1];
+            const TgtW g0 = tw[j0], g1 = tw[j1];
+            const float a0 = screen_dot(g0, dxc), a1 = screen_dot(g1, dxc);
+            bool w0 = active && !(a0 < -gxc), w1 = active && !(a1 < -gxc);
+            if (w0 || w1) {
+                const float b0 = screen_dot(g0, dvc), b1 = screen_dot(g1, dvc);
+                w0 = w0 && !(b0 < -gvc);
+                w1 = w1 && !(b1 < -gvc);
+            }
+            push(w0, j0);
+            push(w1, j1);
+        }
+        if (sidx < ns) {
+            const int j = surv[sidx];
+            const TgtW g = tw[j];
+            bool want = active && !(screen_dot(g, dxc) < -gxc);
+            if (want) want = !(screen_dot(g, dvc) < -gvc);
+            push(want, j);
         }
         if (qn > 0) cpa_finish(q, V, C, X, tile, t0, de0, az0, myq, qn, lane);
-        __syncthreads();
     }
 }
 
