@@ -278,7 +278,7 @@ __device__ __forceinline__ double seq_inc(const double* inc, int n, int k) {
  * upper / lower counts are not changed by reflections.  curr_c is curr's
  * sound speed (re-initialised by an earlier reflection of this step) and
  * surface / bottom the counts at this point of the reflection chain. */
-__device__ void build_eigenverb(const QueueDev& q, const FrontPtrs& C, int i, int64_t step,
+__device__ __noinline__ void build_eigenverb(const QueueDev& q, const FrontPtrs& C, int i, int64_t step,
                                 double t_old, double tw, double grazing, double speed,
                                 const double* pos, const double* nd, int type, double curr_c,
                                 int surface, int bottom, int seq) {
@@ -343,7 +343,7 @@ __device__ void build_eigenverb(const QueueDev& q, const FrontPtrs& C, int i, in
 /* wave_queue::detect_volume_scattering (wave_queue.cc:297-345) with the
  * ray's prev / curr / next states V, Cr, X.  The collision time is
  * measured to the ocean surface, not to the layer, as in the reference. */
-__device__ void volume_scatter(const QueueDev& q, const FrontPtrs& C, int i, int64_t step,
+__device__ __noinline__ void volume_scatter(const QueueDev& q, const FrontPtrs& C, int i, int64_t step,
                                double t_old, const RayS& V, const RayS& Cr, const RayS& X,
                                int surface, int bottom, int& seq) {
     if (bottom > q.max_bottom || surface > q.max_surface || C.caustic[i] > q.max_caustic ||
@@ -365,7 +365,9 @@ __device__ void volume_scatter(const QueueDev& q, const FrontPtrs& C, int i, int
     }
 }
 
-__device__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const double* pos,
+__device__ __noinline__ void update1_ni(const QueueDev& q, RayS& y) { update1(q, y); }
+
+__device__ __noinline__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const double* pos,
                              const double* nd) {
     RayS past1, prev1, curr1, next1, temp;
 #pragma unroll
@@ -378,30 +380,30 @@ __device__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const do
     prev1.dist = 0.0;
     curr1.dist = 0.0;
     temp.dist = 0.0;
-    update1(q, temp);
+    update1_ni(q, temp);
     rk1(-tw, temp, next1);
-    update1(q, next1);
+    update1_ni(q, next1);
     rk2(-tw, temp, next1, past1);
-    update1(q, past1);
+    update1_ni(q, past1);
     rk3(-tw, temp, next1, past1, curr1);
-    update1(q, curr1);
+    update1_ni(q, curr1);
 
     const double h = q.dt;
     rk1(-h, curr1, next1);
-    update1(q, next1);
+    update1_ni(q, next1);
     rk2(-h, curr1, next1, past1);
-    update1(q, past1);
+    update1_ni(q, past1);
     rk3(-h, curr1, next1, past1, prev1);
-    update1(q, prev1);
+    update1_ni(q, prev1);
 
     rk1(-h, prev1, next1);
-    update1(q, next1);
+    update1_ni(q, next1);
     rk2(-h, prev1, next1, temp);
     rk3(-h, prev1, next1, temp, past1);
-    update1(q, past1);
+    update1_ni(q, past1);
 
     ab3(h, past1, prev1, curr1, next1);
-    update1(q, next1);
+    update1_ni(q, next1);
     L.c = curr1;
     L.v = prev1;
     L.x = next1;
@@ -435,7 +437,7 @@ __device__ void record_reflection(const QueueDev& q, int64_t step, double t_old,
 }
 
 /* reflection_model::surface_reflection (reflection_model.cc:187-243) */
-__device__ bool surface_local(const QueueDev& q, const FrontPtrs& C, RayLocal& L, int i, int64_t step,
+__device__ __noinline__ bool surface_local(const QueueDev& q, const FrontPtrs& C, RayLocal& L, int i, int64_t step,
                               double t_old, int& seq) {
     double c = L.c.c;
     const double d = c * c * L.c.nd[0];
@@ -470,7 +472,7 @@ __device__ bool surface_local(const QueueDev& q, const FrontPtrs& C, RayLocal& L
 }
 
 /* reflection_model::bottom_reflection (reflection_model.cc:33-182) */
-__device__ void bottom_local(const QueueDev& q, const FrontPtrs& C, RayLocal& L, int i, double depth,
+__device__ __noinline__ void bottom_local(const QueueDev& q, const FrontPtrs& C, RayLocal& L, int i, double depth,
                              int64_t step, double t_old, int& seq) {
     const BoundaryDev& B = q.oc.bot;
     bool shallow = false;
