@@ -958,6 +958,8 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.n_cand = q->d_counts + 3;
     h.n_work[0] = q->d_counts + 4;
     h.n_work[1] = q->d_counts + 5;
+    h.n_work_b[0] = q->d_counts + 9;
+    h.n_work_b[1] = q->d_counts + 10;
     h.n_done = q->d_counts + 6;
     h.n_verb = q->d_counts + 8;
     h.want_verbs = 0;

@@ -105,7 +105,8 @@ struct QueueDev {
     const double* d_times;   /* time after base + k steps, k = 0..K         */
     uint8_t* flag[2];        /* reflection decision for the "next" front    */
     uint32_t* work[2];       /* rays that reflect at the start of a step     */
-    uint32_t* n_work[2];
+    uint32_t* n_work[2];     /* surface part (front of the list)             */
+    uint32_t* n_work_b[2];   /* bottom part (back of the list)               */
     uint32_t* n_done;        /* finished blocks of k_reflect              */
     double* shadow;          /* reflected prev/curr/next per worklist slot  */
     int32_t* shadow_cnt;     /* surface, bottom, caustic per slot           */

@@ -560,8 +560,8 @@ __device__ __noinline__ void bottom_local(const QueueDev& q, const FrontPtrs& C,
 }
 
 /* whether the "next" ray reflects at the start of the following step:
- * surface if above the surface and heading up (surface_reflection's
- * grazing > 0), else bottom if below the bottom (wave_queue.cc:222-256) */
+ * 1 = surface if above the surface and heading up (surface_reflection's
+ * grazing > 0), else 2 = bottom if below the bottom (wave_queue.cc:222-256) */
 __device__ __forceinline__ uint8_t reflect_decision(const QueueDev& q,
                                                     const double* xpos,
                                                     const double* cnd) {
@@ -570,7 +570,20 @@ __device__ __forceinline__ uint8_t reflect_decision(const QueueDev& q,
         if (grazing > 0.0) return 1;
     }
     const double h = boundary_height(q.oc.bot, xpos[1], xpos[2]);
-    return (h - xpos[0] > 0.0) ? 1 : 0;
+    return (h - xpos[0] > 0.0) ? 2 : 0;
+}
+
+/* appends a reflecting ray to worklist p: surface reflections fill it
+ * from the front, bottom reflections from the back, so the warps of
+ * k_reflect mostly take one path */
+__device__ __forceinline__ void work_append(const QueueDev& q, int p, uint8_t kind, int i) {
+    if (kind == 1) {
+        const uint32_t slot = atomicAdd(q.n_work[p], 1u);
+        if (slot < (uint32_t)q.n) q.work[p][slot] = (uint32_t)i;
+    } else {
+        const uint32_t slot = atomicAdd(q.n_work_b[p], 1u);
+        if (slot < (uint32_t)q.n) q.work[p][q.n - 1 - slot] = (uint32_t)i;
+    }
 }
 
 /* shadow slot of a reflecting ray: prev, curr, next (17 doubles each), the
@@ -664,10 +677,7 @@ __global__ void __launch_bounds__(128) k_startup(const QueueDev* __restrict__ qp
     }
     const uint8_t f = reflect_decision(q, x.pos, c0.nd);
     q.flag[0][i] = f;
-    if (f) {
-        const uint32_t slot = atomicAdd(q.n_work[0], 1u);
-        if (slot < (uint32_t)q.n) q.work[0][slot] = (uint32_t)i;
-    }
+    if (f) work_append(q, 0, f, i);
     (void)a;
 }
 
@@ -685,14 +695,17 @@ __global__ void __launch_bounds__(128) k_startup(const QueueDev* __restrict__ qp
 __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp, int k) {
     const QueueDev& q = *qp;
     const int64_t s = *q.d_base + k;
-    const uint32_t nwork = min(*q.n_work[s & 1], (uint32_t)q.n);
+    const uint32_t nsurf = min(*q.n_work[s & 1], (uint32_t)q.n);
+    const uint32_t nwork = nsurf + min(*q.n_work_b[s & 1], (uint32_t)q.n - nsurf);
     const uint32_t* work = q.work[s & 1];
     const double t_old = q.d_times[k];
     Roles R;
     roles_at(q, s, R);
     const uint8_t* flag_in = q.flag[s & 1];
     const size_t stride = shadow_stride(q);
-    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nwork; w += gridDim.x * blockDim.x) {
+    for (uint32_t ww = blockIdx.x * blockDim.x + threadIdx.x; ww < nwork; ww += gridDim.x * blockDim.x) {
+        /* list slot: surface part at the front, bottom part at the back */
+        const uint32_t w = ww < nsurf ? ww : (uint32_t)q.n - 1 - (ww - nsurf);
         const int i = (int)work[w];
         RayLocal L;
         load_ray(*R.V, i, L.v);
@@ -781,6 +794,7 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
         const uint32_t prev = atomicAdd(q.n_done, 1u);
         if (prev == gridDim.x - 1) {
             *q.n_work[s & 1] = 0;
+            *q.n_work_b[s & 1] = 0;
             *q.n_done = 0;
         }
     }
@@ -884,10 +898,7 @@ __global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp
     R.P->caustic[i] = R.X->caustic[i];
     const uint8_t f = reflect_decision(q, y3.pos, y2.nd);
     flag_out[i] = f;
-    if (f) {
-        const uint32_t slot = atomicAdd(q.n_work[(s + 1) & 1], 1u);
-        if (slot < (uint32_t)q.n) q.work[(s + 1) & 1][slot] = (uint32_t)i;
-    }
+    if (f) work_append(q, (int)((s + 1) & 1), f, i);
 }
 
 }  // namespace WQ3D_KERNEL_NS
