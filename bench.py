@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=64,
+                    help="instances of the batched gridded workload (0 skips it)")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="profiling mode: one queue of the workload, this many wave steps, no output")
     return ap.parse_args()
@@ -298,7 +300,36 @@ def engine_arm(args, rank, world, dist):
         "roofline_hbm": hbm_roofline(interior, cpa_launch_s),
         "clocks": clk,
     }
+    if args.batch_instances > 0:
+        out["batched"] = batched_arm(args)
     return out
+
+
+def batched_arm(args):
+    """Batched solves/s: args.batch_instances uneven instances of the
+    gridded workload (own 50x20x20 profile grid and 100x100 bathymetry
+    each, 91-1801 D/E x 1-91 AZ rays, 10-120 s, 64 targets, dt 0.05 s),
+    FP32C, run together by wq3d_batch_run.  Device time from the batch's
+    start to its last queue's end; queue building (host precompute and
+    uploads) is reported apart."""
+    import underseamodelinglibrary_b200 as u
+    from underseamodelinglibrary_b200 import scenarios as S
+    from underseamodelinglibrary_b200 import _abi
+    scs = S.batched_gridded(n_instances=args.batch_instances)
+    t0 = time.perf_counter()
+    qs = [S.build_queue(sc, u.wave_queue, precision=_abi.FP32C) for sc in scs]
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    steps, ms = u.run_batch(qs, [sc["time_max"] for sc in scs])
+    wall = time.perf_counter() - t0
+    ray_steps = sum(sc["de"].size() * sc["az"].size() * n for sc, n in zip(scs, steps))
+    n_eig = sum(len(q.take_eigenrays()) for q in qs)
+    return {"metric": "batched solves/s", "value": len(qs) / (ms / 1000.0), "unit": "solves/s",
+            "instances": len(qs), "ms_device": ms, "wall_s": wall, "build_s": t_build,
+            "ray_steps_per_s": ray_steps / (ms / 1000.0), "ray_steps": ray_steps, "eigenrays": n_eig,
+            "config": {"workload": "batched_gridded_%d" % len(qs), "form": "FP32C",
+                       "rays_total": sum(sc["de"].size() * sc["az"].size() for sc in scs),
+                       "steps_total": sum(steps)}}
 
 
 def _wraps(az):

@@ -400,6 +400,19 @@ int wq3d_queue_step(wq3d_queue* q, size_t nsteps);
  * (wavegen/wavefront_generator.cc:98-112).  *steps_done may be NULL. */
 int wq3d_queue_run(wq3d_queue* q, double time_max, size_t* steps_done);
 
+/* Runs count independent queues, each until its time() reaches
+ * time_max[i] (the reference loop of wq3d_queue_run), concurrently on one
+ * GPU: every queue's next chunk of steps is launched before any is drained,
+ * so the host delivers one queue's results while the others compute.  It
+ * replaces the reference's thread pool of wavefront_generator tasks, one
+ * wave_queue each (wavegen/wavefront_generator.cc:52-127,
+ * threads/thread_pool.cc:21-56).  Listener callbacks arrive on the calling
+ * thread, per queue in reference order.  steps_done (count values) and
+ * ms_device (device time from the batch's start to the last queue's end)
+ * may be NULL.  All queues must be on one device. */
+int wq3d_batch_run(wq3d_queue* const* queues, size_t count, const double* time_max,
+                   size_t* steps_done, double* ms_device);
+
 /* Read-only state: wave_queue::time(), source_pos(), num_de/az. */
 int wq3d_queue_time(const wq3d_queue* q, double* time);
 int wq3d_queue_source(const wq3d_queue* q, double* rho_theta_phi);

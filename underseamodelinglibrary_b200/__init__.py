@@ -16,7 +16,7 @@ from .ocean import (attenuation_thorp, attenuation_constant, profile_linear,
                     boundary_slope, ocean_model, data_grid, profile_grid, boundary_grid,
                     volume_flat)
 from .waveq3d import (wave_queue, eigenray_listener, reflection_listener,
-                      eigenray_model)
+                      eigenray_model, run_batch)
 from .eigenrays import eigenray_collection
 from .eigenverbs import eigenverb_model, eigenverb_listener, eigenverb_collection
 
@@ -31,7 +31,7 @@ __all__ = [
     "profile_linear", "profile_munk", "profile_catenary", "profile_n2",
     "reflect_loss_constant", "reflect_loss_rayleigh", "reflect_loss_eckart",
     "boundary_flat", "boundary_slope", "ocean_model", "data_grid", "profile_grid",
-    "boundary_grid", "volume_flat", "wave_queue",
+    "boundary_grid", "volume_flat", "wave_queue", "run_batch",
     "eigenray_listener", "reflection_listener", "eigenray_model",
     "eigenray_collection", "eigenverb_model", "eigenverb_listener", "eigenverb_collection",
     "load_engine", "EngineError", "LIB_PATH",

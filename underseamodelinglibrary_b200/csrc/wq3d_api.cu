@@ -471,7 +471,8 @@ struct wq3d_queue {
         }
     }
 
-    int run_chunk(int K) {
+    /* Queues chunk K's work on the stream without waiting for it. */
+    int chunk_launch(int K) {
         h_base[0] = steps;
         h_times[0] = time;
         for (int k = 0; k < K; ++k) h_times[k + 1] = h_times[k] + h.dt;
@@ -490,6 +491,11 @@ struct wq3d_queue {
         }
         WQ_CK(cudaGetLastError());
         WQ_CK(cudaMemcpyAsync(h_counts, d_counts, 9 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        return WQ3D_OK;
+    }
+
+    /* Waits for chunk K, reads its records back and delivers them. */
+    int chunk_finish(int K) {
         WQ_CK(cudaStreamSynchronize(stream));
         if (timing) {
             float r0 = 0;
@@ -548,6 +554,22 @@ struct wq3d_queue {
         if (err)
             return fail(WQ3D_ERR_NUMERIC, "kernel iteration bound reached (error bits " + std::to_string(err) + ")");
         return WQ3D_OK;
+    }
+
+    int run_chunk(int K) {
+        const int rc = chunk_launch(K);
+        return rc ? rc : chunk_finish(K);
+    }
+
+    /* steps of the reference loop "while (time() < time_max) step();" */
+    size_t steps_until(double time_max) const {
+        size_t n = 0;
+        double t = time;
+        while (t < time_max) {
+            t += h.dt;
+            ++n;
+        }
+        return n;
     }
 };
 
@@ -1090,14 +1112,71 @@ int wq3d_queue_step(wq3d_queue* q, size_t nsteps) {
 
 int wq3d_queue_run(wq3d_queue* q, double time_max, size_t* steps_done) {
     if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
-    size_t n = 0;
-    double t = q->time;
-    while (t < time_max) {
-        t += q->h.dt;
-        ++n;
-    }
+    const size_t n = q->steps_until(time_max);
     const int rc = wq3d_queue_step(q, n);
     if (steps_done) *steps_done = n;
+    return rc;
+}
+
+int wq3d_batch_run(wq3d_queue* const* queues, size_t count, const double* time_max, size_t* steps_done,
+                   double* ms_device) {
+    if (!queues || !time_max || count == 0) return fail(WQ3D_ERR_INVALID, "null argument or empty batch");
+    for (size_t i = 0; i < count; ++i) {
+        if (!queues[i]) return fail(WQ3D_ERR_INVALID, "null queue in batch");
+        if (queues[i]->device != queues[0]->device) return fail(WQ3D_ERR_INVALID, "batch queues on different devices");
+        for (size_t j = 0; j < i; ++j)
+            if (queues[j] == queues[i]) return fail(WQ3D_ERR_INVALID, "queue listed twice in batch");
+    }
+    DeviceGuard guard(queues[0]->device);
+    std::vector<size_t> left(count), K(count, 0);
+    for (size_t i = 0; i < count; ++i) {
+        left[i] = queues[i]->steps_until(time_max[i]);
+        if (steps_done) steps_done[i] = left[i];
+    }
+    /* one start event that every queue's stream waits on, so the device
+     * time of the batch is the latest queue end minus this start */
+    cudaEvent_t start = nullptr;
+    WQ_CK(cudaEventCreate(&start));
+    WQ_CK(cudaEventRecord(start, queues[0]->stream));
+    for (size_t i = 1; i < count; ++i) WQ_CK(cudaStreamWaitEvent(queues[i]->stream, start, 0));
+    int rc = WQ3D_OK;
+    bool any = true;
+    while (any && !rc) {
+        any = false;
+        /* launch every unfinished queue's next chunk, then drain them in
+         * turn: the host delivers one queue's results while the others run */
+        for (size_t i = 0; i < count && !rc; ++i) {
+            K[i] = 0;
+            if (left[i] == 0) continue;
+            if (queues[i]->abort_flag.exchange(false)) {
+                rc = fail(WQ3D_ERR_ABORTED, "aborted by caller");
+                break;
+            }
+            K[i] = std::min<size_t>(left[i], (size_t)queues[i]->chunk);
+            rc = queues[i]->chunk_launch((int)K[i]);
+            if (rc) K[i] = 0;
+        }
+        for (size_t i = 0; i < count; ++i) {
+            if (K[i] == 0) continue;
+            const int r = queues[i]->chunk_finish((int)K[i]);
+            if (r && !rc) rc = r;
+            left[i] -= K[i];
+            any = any || left[i] > 0;
+        }
+    }
+    float worst = 0.0f;
+    for (size_t i = 0; i < count; ++i) {
+        wq3d_queue* q = queues[i];
+        cudaEventRecord(q->ev_end, q->stream);
+        cudaEventSynchronize(q->ev_end);
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, start, q->ev_end) == cudaSuccess) {
+            q->ms_total += ms;
+            worst = std::max(worst, ms);
+        }
+    }
+    cudaEventDestroy(start);
+    if (ms_device) *ms_device = worst;
     return rc;
 }
 

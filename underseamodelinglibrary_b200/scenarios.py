@@ -299,6 +299,38 @@ def gridded_munk(seed=1, num_de=91, num_az=13, n_targets=64, time_max=30.0, src_
                  name="gridded_munk_%dx%d" % (num_de, num_az))
 
 
+def batched_gridded(n_instances=512, seed=20261203, num_de=(91, 1801), num_az=(1, 91),
+                    time_max=(10.0, 120.0), dt=0.05, n_targets=64):
+    """Batched workload of uneven instances: each has its own gridded_ocean()
+    (50 x 20 x 20 profile grid of Munk plus a random field, 100 x 100
+    bathymetry of 1000-5000 m), a source 10-500 m deep at 45N 45W, D/E
+    and AZ counts drawn uniformly from ``num_de`` and ``num_az`` (AZ fan
+    0..360 deg, which wraps from 3 rays up), time_max drawn from
+    ``time_max``, and 64 random targets at 10-4000 m depth within 100 km
+    (range 100 km x sqrt(U)).  Returns one scenario dict per instance."""
+    T.compute_earth_radius(45.0)
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_instances):
+        nde = int(rng.integers(num_de[0], num_de[1] + 1))
+        naz = int(rng.integers(num_az[0], num_az[1] + 1))
+        tmax = float(rng.uniform(*time_max))
+        zs = float(rng.uniform(10.0, 500.0))
+        ocean = gridded_ocean(rng)
+        src = T.wposition1(45.0, -45.0, -zs)
+        tgt = T.wposition(1, n_targets, 0.0, 0.0, 0.0)
+        for j in range(n_targets):
+            p = T.wposition1(src, float(100e3 * math.sqrt(rng.uniform())), float(rng.uniform(0.0, 2 * math.pi)))
+            tgt.latitude(0, j, p.latitude())
+            tgt.longitude(0, j, p.longitude())
+            tgt.altitude(0, j, -float(rng.uniform(10.0, 4000.0)))
+        az = T.seq_linear(0.0, 360.0 / (naz - 1), naz) if naz > 1 else T.seq_linear(0.0, 0.0, 1)
+        out.append(_pack(ocean=ocean, freq=T.seq_log(1000.0, 1.0, 1), pos=src,
+                         de=T.seq_rayfan(-90.0, 90.0, nde), az=az, dt=dt, targets=tgt, time_max=tmax,
+                         name="batched_gridded_%d_of_%d" % (k, n_instances)))
+    return out
+
+
 def build_queue(sc, queue_cls, **kw):
     """Constructs ``queue_cls(ocean, freq, pos, de, az, dt, targets, type)``
     and applies the scenario's threshold settings."""

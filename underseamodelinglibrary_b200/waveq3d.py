@@ -386,3 +386,20 @@ class wave_queue:
         _abi.check(self._lib, self._lib.wq3d_queue_timing(self._q, C.byref(t), 1 if reset else 0))
         return {"total_ms": t.ms_total, "advance_ms": t.ms_advance, "reflect_ms": t.ms_reflect,
                 "cpa_ms": t.ms_cpa, "eigenray_ms": t.ms_eigenray, "launches": t.launches}
+
+
+def run_batch(queues, time_max):
+    """Runs several wave_queues concurrently on one GPU, each until its
+    time() reaches its time_max (wq3d_batch_run; the reference runs one
+    wavefront_generator task per queue on a thread pool).  ``time_max`` is
+    one value or one per queue.  Listeners are called per queue in
+    reference order.  Returns (steps per queue, device milliseconds)."""
+    queues = list(queues)
+    n = len(queues)
+    tm = np.broadcast_to(np.asarray(time_max, dtype=np.float64), (n,)).copy()
+    handles = (C.c_void_p * n)(*[q._q for q in queues])
+    steps = (C.c_size_t * n)()
+    ms = C.c_double()
+    lib = _abi.load_engine()
+    _abi.check(lib, lib.wq3d_batch_run(handles, n, _abi.as_dp(tm), steps, C.byref(ms)))
+    return [int(x) for x in steps], ms.value
