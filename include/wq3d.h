@@ -384,6 +384,22 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* desc,
                       wq3d_queue** out);
 int wq3d_queue_destroy(wq3d_queue* q);
 
+/* Sensitivity mode (call before the first step): every eigenray also
+ * carries the exact derivatives of its transmission loss (dB, the same at
+ * every frequency) with respect to the bottom's Rayleigh parameters --
+ * density ratio, speed ratio and attenuation in dB per wavelength
+ * (reflect_loss_rayleigh.cc:68-78) -- carried along each ray as the
+ * derivative of its accumulated reflection loss.  The ray geometry does not
+ * depend on these parameters, so this is the derivative of the whole
+ * propagation.  No reference counterpart: the reference has no
+ * differentiation. */
+int wq3d_queue_enable_sensitivity(wq3d_queue* q);
+
+/* The three derivatives of each eigenray that wq3d_queue_take_eigenrays
+ * would return next, in the same order (3 values per eigenray; NaN when
+ * sensitivity mode is off).  Does not consume the eigenrays. */
+int wq3d_queue_sensitivities(const wq3d_queue* q, double* sens, size_t capacity, size_t* count);
+
 /* Replaces the wave_thresholds setters (wave_thresholds.h:54-182). */
 int wq3d_queue_set_thresholds(wq3d_queue* q, const wq3d_thresholds* t);
 

@@ -197,6 +197,7 @@ int make_grid(wq3d_ocean* o, const wq3d_grid_desc& d, int max_dims, GridDev* hg,
 struct PendingRay {
     wq3d_eigenray rec;
     std::vector<double> inten, phase;
+    double sens[3] = {0.0, 0.0, 0.0}; /* dTL / d bottom parameters */
 };
 
 struct wq3d_queue {
@@ -235,7 +236,7 @@ struct wq3d_queue {
     void (*k_reflect_fn)(const QueueDev*, int) = analytic::k_reflect;
     void (*k_advance_fn)(const QueueDev*, int) = analytic::k_advance;
     std::vector<wq3d_eigenray> h_rec;
-    std::vector<double> h_rinten, h_rphase;
+    std::vector<double> h_rinten, h_rphase, h_rsens;
     std::vector<wq3d_reflection> h_refl;
     std::vector<wq3d_eigenverb> h_verb;
     std::vector<double> h_vpower;
@@ -462,6 +463,8 @@ struct wq3d_queue {
                     PendingRay p;
                     p.rec = h_rec[j];
                     p.inten.assign(&h_rinten[j * nf], &h_rinten[j * nf] + nf);
+                    if (h.sens)
+                        for (int m = 0; m < 3; ++m) p.sens[m] = h_rsens[j * 3 + m];
                     p.phase.assign(&h_rphase[j * nf], &h_rphase[j * nf] + nf);
                     pending.push_back(std::move(p));
                 }
@@ -527,6 +530,11 @@ struct wq3d_queue {
             WQ_CK(cudaMemcpy(h_rec.data(), h.rec, nrec * sizeof(wq3d_eigenray), cudaMemcpyDeviceToHost));
             WQ_CK(cudaMemcpy(h_rinten.data(), h.rec_inten, (size_t)nrec * h.nf * sizeof(double), cudaMemcpyDeviceToHost));
             WQ_CK(cudaMemcpy(h_rphase.data(), h.rec_phase, (size_t)nrec * h.nf * sizeof(double), cudaMemcpyDeviceToHost));
+            if (h.sens) {
+                if (h_rsens.size() < (size_t)nrec * 3) h_rsens.resize((size_t)nrec * 3);
+                WQ_CK(cudaMemcpy(h_rsens.data(), h.rec_sens, (size_t)nrec * 3 * sizeof(double),
+                                 cudaMemcpyDeviceToHost));
+            }
         }
         if (nrefl > 0) {
             if (h_refl.size() < nrefl) h_refl.resize(nrefl);
@@ -1253,6 +1261,33 @@ int wq3d_queue_take_eigenrays(wq3d_queue* q, wq3d_eigenray* rays, double* inten,
         if (phase) std::memcpy(phase + i * nf, q->pending[i].phase.data(), nf * sizeof(double));
     }
     q->pending.clear();
+    return WQ3D_OK;
+}
+
+int wq3d_queue_enable_sensitivity(wq3d_queue* q) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    if (q->h.sens) return WQ3D_OK;
+    if (q->steps != 0) return fail(WQ3D_ERR_INVALID, "enable sensitivities before the first step");
+    DeviceGuard guard(q->device);
+    const size_t n = (size_t)q->h.n;
+    double* dA = nullptr;
+    int rc = q->alloc(&dA, 4 * 3 * n);
+    if (!rc) rc = q->alloc(&q->h.rec_sens, (size_t)q->h.cap_rec * 3);
+    if (rc) return rc;
+    WQ_CK(cudaMemset(dA, 0, 4 * 3 * n * sizeof(double)));
+    for (int f = 0; f < 4; ++f) q->h.F[f].dA = dA + (size_t)f * 3 * n;
+    q->h.sens = 1;
+    WQ_CK(cudaMemcpy(q->d_q, &q->h, sizeof(QueueDev), cudaMemcpyHostToDevice));
+    return WQ3D_OK;
+}
+
+int wq3d_queue_sensitivities(const wq3d_queue* q, double* sens, size_t capacity, size_t* count) {
+    if (!q || !count) return fail(WQ3D_ERR_INVALID, "null argument");
+    *count = q->pending.size();
+    if (!sens) return WQ3D_OK;
+    if (capacity < q->pending.size()) return fail(WQ3D_ERR_OVERFLOW, "capacity smaller than the pending count");
+    for (size_t i = 0; i < q->pending.size(); ++i)
+        for (int m = 0; m < 3; ++m) sens[i * 3 + m] = q->h.sens ? q->pending[i].sens[m] : NAN;
     return WQ3D_OK;
 }
 

@@ -53,6 +53,8 @@ struct FrontPtrs {
     double* atten;   /* [nf][n] */
     double* phase;   /* [nf][n] */
     double* cpa[4];  /* rho, theta, phi, sin(theta) at the last update */
+    double* dA;      /* [3][n] d attenuation / d (bottom density ratio,
+                        speed ratio, attenuation); sensitivity mode only */
     int32_t* surface;
     int32_t* bottom;
     int32_t* caustic;
@@ -121,6 +123,8 @@ struct QueueDev {
     double* rec_phase;
     uint32_t* n_rec;
     uint32_t cap_rec;
+    double* rec_sens;        /* [cap][3] dTL / d bottom parameters        */
+    int sens;                /* sensitivity mode                          */
     /* reflection records (only when a listener wants them) */
     wq3d_reflection* refl;
     uint32_t* n_refl;

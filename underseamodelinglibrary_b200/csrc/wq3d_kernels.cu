@@ -473,7 +473,7 @@ __device__ __noinline__ bool surface_local(const QueueDev& q, const FrontPtrs& C
 
 /* reflection_model::bottom_reflection (reflection_model.cc:33-182) */
 __device__ __noinline__ void bottom_local(const QueueDev& q, const FrontPtrs& C, RayLocal& L, int i, double depth,
-                             int64_t step, double t_old, int& seq) {
+                             int64_t step, double t_old, int& seq, double* dl) {
     const BoundaryDev& B = q.oc.bot;
     bool shallow = false;
     double position[3] = {L.c.pos[0], L.c.pos[1], L.c.pos[2]};
@@ -536,6 +536,11 @@ __device__ __noinline__ void bottom_local(const QueueDev& q, const FrontPtrs& C,
     const LossDev& Lo = B.loss;
     double amp0 = 0.0, ph0 = 0.0;
     if (Lo.kind != WQ3D_LOSS_ECKART) reflect_loss_scalar(Lo, grazing, &amp0, &ph0);
+    if (q.sens) {
+        double g[3];
+        reflect_loss_rayleigh_grad(Lo, grazing, g);
+        for (int j = 0; j < 3; ++j) dl[j] += g[j];
+    }
     const double w2 = Lo.p[0] * Lo.p[0];
     const double sgz = sin(grazing);
     for (int k = 0; k < q.nf; ++k) {
@@ -736,6 +741,7 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
          * then the surface / bottom chain, volume layers after each
          * reflection (wave_queue.cc:202-256); seq orders the ray's events */
         const bool vol = q.want_verbs && q.oc.nvol > 0;
+        double dl[3] = {0.0, 0.0, 0.0};
         bool reflected = false;
         int seq = 0;
         int next_try = -1; /* 0: try bottom next, 1: try surface next */
@@ -747,7 +753,7 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
         } else {
             const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
             if (depth > 0.0) {
-                bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq);
+                bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq, dl);
                 L.bottom += 1;
                 reflected = true;
                 next_try = 1;
@@ -760,7 +766,7 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
                 if (next_try == 0) {
                     const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
                     if (!(depth > 0.0)) break;
-                    bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq);
+                    bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq, dl);
                     L.bottom += 1;
                     next_try = 1;
                 } else {
@@ -780,6 +786,10 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
             sh[51 + f] = L.att[f];
             sh[51 + q.nf + f] = L.ph[f];
         }
+        /* the next front's loss tangents take this step's bottom bounces;
+         * the front is not read by the concurrent CPA work of step s-1 */
+        if (q.sens)
+            for (int j = 0; j < 3; ++j) R.X->dA[(size_t)j * q.n + i] += dl[j];
         q.shadow_cnt[3 * (size_t)w] = L.surface;
         q.shadow_cnt[3 * (size_t)w + 1] = L.bottom;
         q.shadow_cnt[3 * (size_t)w + 2] = L.caustic;
@@ -896,6 +906,8 @@ __global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp
     R.P->upper[i] = R.X->upper[i];
     R.P->lower[i] = R.X->lower[i];
     R.P->caustic[i] = R.X->caustic[i];
+    if (q.sens)
+        for (int j = 0; j < 3; ++j) R.P->dA[(size_t)j * q.n + i] = R.X->dA[(size_t)j * q.n + i];
     const uint8_t f = reflect_decision(q, y3.pos, y2.nd);
     flag_out[i] = f;
     if (f) work_append(q, (int)((s + 1) & 1), f, i);
@@ -2004,6 +2016,9 @@ __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(const QueueDev* __r
             r.step = s;
             q.rec[slot] = r;
         }
+        if (q.sens && lane < 3)
+            q.rec_sens[(size_t)slot * 3 + lane] = A0.dA[(size_t)lane * q.n + i] * (1.0 - ddt) +
+                                                  A1.dA[(size_t)lane * q.n + i] * ddt;
         if (has_lo) {
             q.rec_inten[(size_t)slot * q.nf + lane] = tl_lo;
             q.rec_phase[(size_t)slot * q.nf + lane] = C.phase[(size_t)lane * q.n + i];

@@ -554,6 +554,40 @@ WQ_HD void reflect_loss_scalar(const LossDev& L, double angle, double* amp,
     *ph = L.p[1];
 }
 
+/* Derivatives of reflect_loss_scalar's Rayleigh loss (dB) with respect
+ * to the bottom's density ratio, speed ratio and attenuation (dB per
+ * wavelength) at a fixed grazing angle.  With R = (Zb - Zw)/(Zb + Zw) and
+ * loss = -20 log10 |R|, d loss = -(20/ln 10) Re(2 Zw dZb / ((Zb + Zw)(Zb - Zw))),
+ * where Zb = cos A / (c rho_b) gives dZb/d rho_b = -Zb / rho_b and
+ * d ln Zb / d ln c = -1 / cos^2 A (sin A = sin(angle) c / c_water).  Other
+ * loss models do not depend on these parameters (zero); a Rayleigh bottom
+ * with shear is not differentiated here (NaN). */
+WQ_HD void reflect_loss_rayleigh_grad(const LossDev& L, double angle, double* d) {
+    d[0] = d[1] = d[2] = 0.0;
+    if (L.kind != WQ3D_LOSS_RAYLEIGH) return;
+    if (L.rl_shr != 0.0 || L.rl_satt != 0.0) {
+        d[0] = d[1] = d[2] = NAN;
+        return;
+    }
+    if (angle >= M_PI_2) angle = M_PI_2 - 1e-10;
+    angle = M_PI_2 - angle;
+    const double Zw = cos(angle) / (1500.0 * 1000.0);
+    cplx cosA;
+    const cplx Zb = rl_impedance(L.rl_den, L.rl_spd, L.rl_att, sin(angle), &cosA, false);
+    const cplx base = cdiv(cscale(Zb, 2.0 * Zw), cmul(cplx{Zb.re + Zw, Zb.im}, cplx{Zb.re - Zw, Zb.im}));
+    const double k = -20.0 * M_LOG10E;
+    /* density ratio p0: rho_b = 1000 p0 */
+    d[0] = k * (base.re * (-1000.0 / L.rl_den));
+    /* speed ratio p1: c = 1500 p1 (1 - i att), d ln c / d p1 = 1 / p1 */
+    const cplx g_c = cdiv(cplx{-1.0, 0.0}, cmul(cosA, cosA));
+    const cplx gv = cscale(g_c, 1500.0 / L.rl_spd);
+    d[1] = k * cmul(base, gv).re;
+    /* attenuation p2: att = p2 K, d ln c / d p2 = -i K / (1 - i att) */
+    const double K = 1.0 / (20.0 * M_LOG10E * (2.0 * M_PI));
+    const cplx dlnc = cdiv(cplx{0.0, -K}, cplx{1.0, -L.rl_att});
+    d[2] = k * cmul(base, cmul(g_c, dlnc)).re;
+}
+
 /* ------------------------------------------------------------------ */
 /* wave_front::update derivative terms (wave_front.cc:133-171)          */
 /* ------------------------------------------------------------------ */

@@ -22,7 +22,8 @@ class eigenray_model:
 
     __slots__ = ("travel_time", "intensity", "phase", "source_de", "source_az",
                  "target_de", "target_az", "surface", "bottom", "caustic", "upper",
-                 "lower", "frequencies", "step", "de_index", "az_index", "t1", "t2")
+                 "lower", "frequencies", "step", "de_index", "az_index", "t1", "t2",
+                 "d_intensity_d_bottom")
 
     @classmethod
     def from_record(cls, rec, intensity, phase, freq):
@@ -45,6 +46,7 @@ class eigenray_model:
         r.az_index = rec.az
         r.t1 = rec.t1
         r.t2 = rec.t2
+        r.d_intensity_d_bottom = None
         return r
 
 
@@ -367,6 +369,10 @@ class wave_queue:
         _abi.check(self._lib, self._lib.wq3d_queue_take_eigenrays(self._q, None, None, None, 0, C.byref(n)))
         cnt = n.value
         nf = self._freq.size()
+        sens = None
+        if getattr(self, "_sens", False):
+            sens = np.empty(max(cnt, 1) * 3)
+            _abi.check(self._lib, self._lib.wq3d_queue_sensitivities(self._q, _abi.as_dp(sens), cnt, C.byref(n)))
         recs = (_abi.wq3d_eigenray * max(cnt, 1))()
         inten = np.empty(max(cnt, 1) * nf)
         phase = np.empty(max(cnt, 1) * nf)
@@ -374,7 +380,17 @@ class wave_queue:
                                                                   _abi.as_dp(phase), cnt, C.byref(n)))
         out = [eigenray_model.from_record(recs[i], inten[i * nf:(i + 1) * nf],
                                           phase[i * nf:(i + 1) * nf], self._freq) for i in range(cnt)]
+        if sens is not None:
+            for i, r in enumerate(out):
+                r.d_intensity_d_bottom = sens[3 * i:3 * i + 3].copy()
         return out
+
+    def enable_sensitivity(self):
+        """exact d(intensity)/d(bottom density ratio, speed ratio,
+        attenuation) on every eigenray (wq3d_queue_enable_sensitivity);
+        call before the first step"""
+        _abi.check(self._lib, self._lib.wq3d_queue_enable_sensitivity(self._q))
+        self._sens = True
 
     def set_timing(self, on):
         _abi.check(self._lib, self._lib.wq3d_queue_set_timing(self._q, 1 if on else 0))
