@@ -43,6 +43,9 @@ FLOPS_PER_RAY_TARGET_STEP = 17
 # FP64 bytes the CPA kernel must read per interior ray and launch: four
 # distance2 terms (rho, theta, phi, sin theta) on three fronts plus on_edge
 BYTES_PER_RAY_CPA = 3 * 4 * 8 + 1
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_cpa_f32 launch on
+# this workload (ncu, launch 301; profiles/fp32c_step_kernels_*.md)
+NCU_TRAFFIC_CPA_F32 = 15994112 + 256
 
 
 def parse():
@@ -53,6 +56,7 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gradients", action="store_true", help="skip the gradient workload")
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched gridded workload (0 skips it)")
     ap.add_argument("--profile-steps", type=int, default=0,
@@ -290,7 +294,8 @@ def engine_arm(args, rank, world, dist):
                      "peak": fp32_peak,
                      "unit": "TFLOP/s",
                      "frac": (achieved / fp32_peak) if fp32_peak else None,
-                     "traffic": None,
+                     "traffic": NCU_TRAFFIC_CPA_F32,
+                     "traffic_unit": "bytes per launch (ncu capture)",
                      "kernel": "k_cpa_f32",
                      "peak_source": peaks["source"] + "; MEASURED_PEAKS.json has no FP32/FP64 CUDA-core figure",
                      "fp64_peak": peaks["fp64"],
@@ -302,7 +307,33 @@ def engine_arm(args, rank, world, dist):
     }
     if args.batch_instances > 0:
         out["batched"] = batched_arm(args)
+    if not args.no_gradients:
+        out["gradients"] = gradient_arm()
     return out
+
+
+def gradient_arm():
+    """Gradient cost on the differentiable workload (1801 x 91 rays, 2000
+    steps of 0.05 s, 64 receivers, 20-node profile grid, Rayleigh bottom):
+    the forward pass with bottom-parameter sensitivities, then the 40
+    perturbed propagations of the sound-speed-node differences as one
+    batch.  gradient_to_forward = (forward + gradient) / forward."""
+    from underseamodelinglibrary_b200 import adjoint as A
+    import numpy as np
+    sc = A.AdjointScenario()
+    nodes = A.munk_nodes()
+    q = sc.queue(nodes)          # warm-up of the same shapes
+    q.run(20 * sc.dt)
+    del q
+    out = A.eigenray_gradients(sc, nodes)
+    jac = out["jacobian"]
+    return {"metric": "adjoint:fwd", "value": (out["ms_forward"] + out["ms_gradient"]) / out["ms_forward"],
+            "unit": "ratio", "higher_is_better": False, "ms_forward": out["ms_forward"],
+            "ms_gradient": out["ms_gradient"], "eigenrays": len(out["eigenrays"]),
+            "gradient_rows_with_topology_change": int(np.isnan(jac[:, 0, 0]).sum()),
+            "method": "bottom parameters exact (sensitivity mode); 20 sound-speed nodes by central "
+                      "differences (h = 1e-3 c_k) run as one batch of 40 propagations",
+            "config": {"workload": "adjoint_munk_grid20_rayleigh_1801x91_2000steps_64rx"}}
 
 
 def batched_arm(args):
