@@ -309,7 +309,48 @@ def engine_arm(args, rank, world, dist):
         out["batched"] = batched_arm(args)
     if not args.no_gradients:
         out["gradients"] = gradient_arm()
+    out["std14"] = std14_arm()
     return out
+
+
+# the reference's published single-core times of its speed study
+# (studies/cmp_speed/cmp_speed_test_20221203.xlsx, WaveQ3D v3.0, Xeon
+# E3-1505M v6 @ 3.00 GHz): seconds per propagation by target count
+STD14_PUBLISHED_S = {0: 2.576, 100: 4.324, 1000: 19.445}
+
+
+def std14_arm():
+    """The reference's speed study (studies/cmp_speed/cmp_speed.cc): STD14
+    grids near Hawaii, 181 x 25 rays, 801 steps of 0.1 s, targets on a
+    100 km ring, with an eigenray_collection listener as in the study.
+    Device time of the step loop (CUDA-graph replay), FP32C and FP64, next
+    to the published single-core CPU time of the same loop."""
+    import underseamodelinglibrary_b200 as u
+    from underseamodelinglibrary_b200 import scenarios as S
+    from underseamodelinglibrary_b200 import _abi
+    rows = []
+    for nt in (0, 100, 1000):
+        sc = S.std14(num_targets=nt)
+        row = {"targets": nt, "published_cpu_s": STD14_PUBLISHED_S[nt]}
+        for name, prec in (("fp32c", _abi.FP32C), ("fp64", _abi.FP64)):
+            best = None
+            for _ in range(3):
+                q = S.build_queue(sc, u.wave_queue, precision=prec)
+                if nt:
+                    coll = u.eigenray_collection(sc["freq"], sc["pos"], sc["targets"])
+                    q.add_eigenray_listener(coll)
+                q.timing(reset=True)
+                t0 = time.perf_counter()
+                q.run(sc["time_max"])
+                wall = time.perf_counter() - t0
+                ms = q.timing()["total_ms"]
+                best = ms if best is None else min(best, ms)
+            row[name + "_ms"] = best
+            row[name + "_wall_s_last"] = wall
+        row["speedup_fp32c_vs_published_cpu"] = STD14_PUBLISHED_S[nt] / (row["fp32c_ms"] / 1000.0)
+        rows.append(row)
+    return {"workload": "std14_cmp_speed_181x25_801steps_250Hz", "rays": 181 * 25, "steps": 801,
+            "rows": rows}
 
 
 def gradient_arm():

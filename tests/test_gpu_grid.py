@@ -157,3 +157,13 @@ def test_gridded_fp32c_matches_fp64(engine):
         assert (x.step, x.t1, x.t2, x.de_index, x.az_index) == (y.step, y.t1, y.t2, y.de_index, y.az_index)
         assert x.travel_time == y.travel_time
         assert np.array_equal(x.intensity, y.intensity)
+
+
+def test_std14_parity(engine):
+    """the reference's speed-study scenario (STD14 grids near Hawaii, 100
+    targets on a 100 km ring) on the engine against the oracle for 40 s"""
+    sc = S.std14(num_targets=100, time_max=40.0)
+    q, o = run_pair(sc)
+    eng = q.take_eigenrays()
+    compare_eigenrays(eng, o.take_eigenrays())
+    compare_fronts(q.curr(), o.curr(), rel=1e-9)

@@ -331,6 +331,50 @@ def batched_gridded(n_instances=512, seed=20261203, num_de=(91, 1801), num_az=(1
     return out
 
 
+def std14_ocean():
+    """The STD14 environment of studies/cmp_speed/cmp_speed.cc:56-76: the
+    3-D sound speed grid (netcdf_profile) and 2-D bathymetry (netcdf_bathy)
+    near Hawaii over 16.2-24.6 N, 164.4-155.5 W, from the package's
+    data/std14.npz (the study's CDL dumps as float32)."""
+    import os
+    from .netcdf_cdl import netcdf_bathy, netcdf_profile
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "std14.npz"))
+    prof = {"time": d["p_time"], "depth": d["p_depth"], "lat": d["p_lat"], "lon": d["p_lon"],
+            "speed": d["p_speed"]}
+    bathy = {"lat": d["b_lat"], "lon": d["b_lon"], "depth": d["b_depth"]}
+    lat1, lat2, lng1, lng2 = 16.2, 24.6, -164.4, -155.5
+    ssp = netcdf_profile(prof, 0.0, lat1, lat2, lng1, lng2)
+    bottom = netcdf_bathy(bathy, lat1, lat2, lng1, lng2, T.earth_radius())
+    return ocean_model(boundary_flat(), boundary_grid(bottom), profile_grid(ssp))
+
+
+def std14(num_targets=100, time_max=80.0):
+    """studies/cmp_speed/cmp_speed.cc:33-114 (the reference's published
+    speed study): source 200 m deep at 19.52N 160.5W, 250 Hz, 181
+    tangent-spaced D/E x AZ 0..360 step 15 (25 rays, wrapping), dt 0.1 s
+    for 80 s, num_targets on a 100 km ring starting one bearing step from
+    north.  As in the study, the ring takes the source's altitude (the
+    100 m target depth it declares is overwritten) and the earth radius
+    keeps its default."""
+    T.set_earth_radius(6371000.0)
+    ocean = std14_ocean()
+    src = T.wposition1(19.52, -160.5, -200.0)
+    tgt = None
+    if num_targets > 0:
+        tgt = T.wposition(num_targets, 1, src.latitude(), src.longitude(), 100.0)
+        angle = 2.0 * math.pi / num_targets
+        bearing = angle
+        for n in range(num_targets):
+            spot = T.wposition1(src, 100000.0, bearing)
+            tgt.latitude(n, 0, spot.latitude())
+            tgt.longitude(n, 0, spot.longitude())
+            tgt.altitude(n, 0, spot.altitude())
+            bearing += angle
+    return _pack(ocean=ocean, freq=T.seq_linear(250.0, 1.0, 1), pos=src, de=T.seq_rayfan(-90.0, 90.0, 181),
+                 az=T.seq_linear(0.0, 15.0, 360.0), dt=0.1, targets=tgt, time_max=time_max,
+                 name="std14_%dtgt" % num_targets)
+
+
 def build_queue(sc, queue_cls, **kw):
     """Constructs ``queue_cls(ocean, freq, pos, de, az, dt, targets, type)``
     and applies the scenario's threshold settings."""
