@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-gradients", action="store_true", help="skip the gradient workload")
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched gridded workload (0 skips it)")
+    ap.add_argument("--profile-workload", default="linear_slope_rayleigh",
+                    choices=["linear_slope_rayleigh", "std14"],
+                    help="workload of --profile-steps (std14: the speed study with 100 targets)")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="profiling mode: one queue of the workload, this many wave steps, no output")
     return ap.parse_args()
@@ -518,7 +521,7 @@ def main():
         import underseamodelinglibrary_b200 as u
         from underseamodelinglibrary_b200 import scenarios as S
         from underseamodelinglibrary_b200 import _abi
-        sc = S.linear_slope_rayleigh()
+        sc = S.std14(num_targets=100) if args.profile_workload == "std14" else S.linear_slope_rayleigh()
         q = S.build_queue(sc, u.wave_queue, device=0, precision=_abi.FP32C)
         q.step(args.profile_steps)
         print("profile run: %d steps, %d eigenrays" % (q.steps(), len(q.take_eigenrays())))

@@ -172,6 +172,9 @@ int make_grid(wq3d_ocean* o, const wq3d_grid_desc& d, int max_dims, GridDev* hg,
         hg->edge[k] = d.edge_limit[k] ? 1 : 0;
     }
     if (!d.data) return fail(WQ3D_ERR_INVALID, "grid data missing");
+    hg->all_linear = 1;
+    for (int k = 0; k < d.ndim; ++k)
+        if (hg->interp[k] != WQ3D_INTERP_LINEAR) hg->all_linear = 0;
     o->store.emplace_back(d.data, d.data + total);
     hg->data = o->store.back().data();
     *dg = *hg;

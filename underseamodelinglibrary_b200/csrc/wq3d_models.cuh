@@ -64,6 +64,7 @@ struct AxisDev {
 
 struct GridDev {
     int ndim;
+    int all_linear;  /* every axis interpolates linearly: unrolled path */
     AxisDev ax[3];
     int interp[3];
     int edge[3];
@@ -321,7 +322,107 @@ WQ_HD double grid_interpolate(const GridDev& g, const double* location, double* 
     return GridInterp<NDIM, NDIM - 1>::run(g, index, loc, dresult, dv);
 }
 
+/* The all-linear case of grid_interpolate, unrolled: the same expression
+ * tree as the recursion of GridInterp (outermost over the last axis), and
+ * the same writes to the shared derivative array, so results are
+ * identical bit for bit while the evaluation stays inline in registers. */
+WQ_HD double lin1(const GridDev& g, int d, const int* index, const double* loc, double a, double b,
+                  double* u_out, double* h_out) {
+    const AxisDev& ax = g.ax[d];
+    const int k = index[d];
+    const double h = axis_inc(ax, k);
+    const double u = (loc[d] - ax.x[k]) / h;
+    *u_out = u;
+    *h_out = h;
+    return a * (1.0 - u) + b * u;
+}
+
+template <int NDIM>
+WQ_HD double grid_linear(const GridDev& g, const double* location, double* dv) {
+    int index[NDIM];
+    double loc[NDIM];
+    for (int d = 0; d < NDIM; ++d) loc[d] = location[d];
+    for (int d = 0; d < NDIM; ++d) {
+        const AxisDev& ax = g.ax[d];
+        if (g.edge[d]) {
+            const double a = ax.x[0];
+            const double b = ax.x[ax.n - 1];
+            const double sign = (ax.inc[0] < 0) ? -1.0 : 1.0;
+            const double dd = loc[d] * sign;
+            if (dd <= a * sign) {
+                loc[d] = a;
+                index[d] = 0;
+            } else if (dd >= b * sign) {
+                loc[d] = b;
+                index[d] = ax.n - 2;
+            } else {
+                index[d] = axis_find(ax, loc[d]);
+            }
+        } else {
+            index[d] = axis_find(ax, loc[d]);
+        }
+    }
+    const double* D = g.data;
+    double u, h;
+    if (NDIM == 1) {
+        const double a = D[index[0]], b = D[index[0] + 1];
+        const double r = lin1(g, 0, index, loc, a, b, &u, &h);
+        if (dv) dv[0] = (b - a) / h;
+        return r;
+    }
+    if (NDIM == 2) {
+        const size_t n1 = (size_t)g.ax[1].n;
+        const size_t o00 = (size_t)index[1] + n1 * (size_t)index[0];
+        const size_t o10 = (size_t)index[1] + n1 * (size_t)(index[0] + 1);
+        double u0, h0;
+        /* outer axis 1; inner calls over axis 0 at index[1] and index[1]+1 */
+        const double va = lin1(g, 0, index, loc, D[o00], D[o10], &u0, &h0);
+        const double da = (D[o10] - D[o00]) / h0;
+        const double vb = lin1(g, 0, index, loc, D[o00 + 1], D[o10 + 1], &u0, &h0);
+        const double db = (D[o10 + 1] - D[o00 + 1]) / h0;
+        const double r = lin1(g, 1, index, loc, va, vb, &u, &h);
+        if (dv) {
+            dv[1] = (vb - va) / h;
+            dv[0] = da * (1.0 - u) + db * u;
+        }
+        return r;
+    }
+    /* NDIM == 3: outer axis 2, then axis 1, innermost axis 0 */
+    const size_t n1 = (size_t)g.ax[1].n, n2 = (size_t)g.ax[2].n;
+    auto off = [&](int i0, int i1, int i2) { return (size_t)i2 + n2 * ((size_t)i1 + n1 * (size_t)i0); };
+    const int i0 = index[0], i1 = index[1], i2 = index[2];
+    double u0, h0, u1, h1;
+    double dv0_last = 0.0;
+    /* one axis-1 interpolation at axis-2 index j: returns value, its axis-1
+     * derivative, and the blended axis-0 derivative it leaves in dv[0] */
+    auto plane = [&](int j, double* d1, double* d0) {
+        const double a0 = D[off(i0, i1, j)], b0 = D[off(i0 + 1, i1, j)];
+        const double va = lin1(g, 0, index, loc, a0, b0, &u0, &h0);
+        const double da = (b0 - a0) / h0;
+        const double a1 = D[off(i0, i1 + 1, j)], b1 = D[off(i0 + 1, i1 + 1, j)];
+        const double vb = lin1(g, 0, index, loc, a1, b1, &u0, &h0);
+        const double db = (b1 - a1) / h0;
+        const double r = lin1(g, 1, index, loc, va, vb, &u1, &h1);
+        *d1 = (vb - va) / h1;
+        *d0 = da * (1.0 - u1) + db * u1;
+        return r;
+    };
+    double d1a, d1b, d0a;
+    const double pa = plane(i2, &d1a, &d0a);
+    const double pb = plane(i2 + 1, &d1b, &dv0_last);
+    const double r = lin1(g, 2, index, loc, pa, pb, &u, &h);
+    if (dv) {
+        dv[2] = (pb - pa) / h;
+        dv[1] = d1a * (1.0 - u) + d1b * u;
+        dv[0] = dv0_last;
+    }
+    return r;
+}
+
 #if WQ3D_WITH_GRID
+/* grid evaluation: the unrolled linear path inline, others out of line */
+WQ_HD double grid_value(const GridDev& g, const double* location, double* dv);
+
 static WQ_NOINL double grid_eval(const GridDev& g, const double* location, double* dv) {
     switch (g.ndim) {
         case 1:
@@ -331,6 +432,20 @@ static WQ_NOINL double grid_eval(const GridDev& g, const double* location, doubl
         default:
             return grid_interpolate<3>(g, location, dv);
     }
+}
+
+WQ_HD double grid_value(const GridDev& g, const double* location, double* dv) {
+    if (g.all_linear) {
+        switch (g.ndim) {
+            case 1:
+                return grid_linear<1>(g, location, dv);
+            case 2:
+                return grid_linear<2>(g, location, dv);
+            default:
+                return grid_linear<3>(g, location, dv);
+        }
+    }
+    return grid_eval(g, location, dv);
 }
 #endif  // WQ3D_WITH_GRID
 
@@ -381,7 +496,7 @@ WQ_HD void sound_speed(const ProfileDev& pr, double R, double rho, double theta,
         case WQ3D_PROFILE_GRID: { /* profile_grid.h:68-130 */
             const double loc[3] = {rho, theta, phi};
             double dv[3] = {0.0, 0.0, 0.0};
-            cc = grid_eval(pr.grid, loc, dv);
+            cc = grid_value(pr.grid, loc, dv);
             gr = dv[0];
             if (pr.grid.ndim >= 2) gt = dv[1];
             if (pr.grid.ndim >= 3) gp = dv[2];
@@ -442,7 +557,7 @@ WQ_HD double boundary_height(const BoundaryDev& b, double theta, double phi) {
 #if WQ3D_WITH_GRID
     if (b.kind == WQ3D_BOUNDARY_GRID) { /* boundary_grid.h:150-196 */
         const double loc[2] = {theta, phi};
-        return grid_eval(b.grid, loc, nullptr);
+        return grid_value(b.grid, loc, nullptr);
     }
 #endif
     return b.height;
@@ -456,7 +571,7 @@ WQ_HD double boundary_height_normal(const BoundaryDev& b, double theta, double p
     if (b.kind == WQ3D_BOUNDARY_GRID) {
         const double loc[2] = {theta, phi};
         double grad[2] = {0.0, 0.0};
-        const double rho = grid_eval(b.grid, loc, grad);
+        const double rho = grid_value(b.grid, loc, grad);
         if (b.grid.ndim == 1) {
             const double t = -grad[0] / rho;
             const double N = sqrt(1 + t * t);
