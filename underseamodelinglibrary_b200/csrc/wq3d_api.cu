@@ -209,7 +209,6 @@ struct wq3d_queue {
     cudaStream_t side = nullptr;
     std::vector<cudaEvent_t> fork_ev, join_ev;
     QueueDev h{};
-    QueueDev* d_q = nullptr;
     std::vector<void*> allocs;
     void* pinned = nullptr;
     int64_t* h_base = nullptr;
@@ -236,15 +235,17 @@ struct wq3d_queue {
     int64_t launches = 0;
     /* the stepping kernels' build: "gridded" when the ocean has a grid */
     bool gridded = false;
-    void (*k_reflect_fn)(const QueueDev*, int) = analytic::k_reflect;
-    void (*k_advance_fn)(const QueueDev*, int) = analytic::k_advance;
+    void (*k_reflect_fn)(const QueueDev, int) = analytic::k_reflect;
+    void (*k_advance_fn)(const QueueDev, int) = analytic::k_advance;
     std::vector<wq3d_eigenray> h_rec;
     std::vector<double> h_rinten, h_rphase, h_rsens;
     std::vector<wq3d_reflection> h_refl;
     std::vector<wq3d_eigenverb> h_verb;
     std::vector<double> h_vpower;
 
-    /* the chunk graph is rebuilt when the launch sequence changes */
+    /* the chunk graph holds the queue descriptor by value (kernel
+     * parameters), so it is rebuilt whenever the descriptor or the launch
+     * sequence changes */
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
@@ -282,7 +283,7 @@ struct wq3d_queue {
         if (!rc) rc = alloc(&h.verb_power, cap * (size_t)h.nf);
         if (rc) return rc;
         h.cap_verb = (uint32_t)cap;
-        WQ_CK(cudaMemcpy(d_q, &h, sizeof(QueueDev), cudaMemcpyHostToDevice));
+        drop_graph();
         return WQ3D_OK;
     }
 
@@ -295,7 +296,6 @@ struct wq3d_queue {
         if (ev_begin) cudaEventDestroy(ev_begin);
         if (ev_end) cudaEventDestroy(ev_end);
         for (void* p : allocs) cudaFree(p);
-        if (d_q) cudaFree(d_q);
         if (pinned) cudaFreeHost(pinned);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -329,17 +329,17 @@ struct wq3d_queue {
         const dim3 grd((n + 127) / 128);
         const int rgrid = std::max(1, std::min(4 * 148, (n + 63) / 64));
         if (timing) cudaEventRecord(events[7 * K], stream);
-        k_reflect_fn<<<rgrid, 64, 0, stream>>>(d_q, 0);
+        k_reflect_fn<<<rgrid, 64, 0, stream>>>(h, 0);
         if (timing) cudaEventRecord(events[7 * K + 1], stream);
         launches += 1;
         for (int k = 0; k < K; ++k) {
             cudaEvent_t* ev = timing ? &events[7 * k] : nullptr;
             if (ev) cudaEventRecord(ev[0], stream);
             if (volume_pass()) {
-                k_volume<<<grd, blk, 0, stream>>>(d_q, k);
+                k_volume<<<grd, blk, 0, stream>>>(h, k);
                 launches += 1;
             }
-            k_advance_fn<<<grd, blk, 0, stream>>>(d_q, k);
+            k_advance_fn<<<grd, blk, 0, stream>>>(h, k);
             if (ev) cudaEventRecord(ev[1], stream);
             launches += 1;
             const bool more = k + 1 < K;
@@ -347,7 +347,7 @@ struct wq3d_queue {
                 cudaEventRecord(fork_ev[k], stream);
                 cudaStreamWaitEvent(side, fork_ev[k], 0);
                 if (ev) cudaEventRecord(ev[5], side);
-                k_reflect_fn<<<rgrid, 64, 0, side>>>(d_q, k + 1);
+                k_reflect_fn<<<rgrid, 64, 0, side>>>(h, k + 1);
                 if (ev) cudaEventRecord(ev[6], side);
                 cudaEventRecord(join_ev[k], side);
                 launches += 1;
@@ -359,11 +359,11 @@ struct wq3d_queue {
                     k_cpa_f32<<<dim3(((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) *
                                          ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
                                      (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS),
-                                CPA_THREADS, 0, stream>>>(d_q, k);
+                                CPA_THREADS, 0, stream>>>(h, k);
                 else
-                    k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d_q, k);
+                    k_cpa<<<cg, CPA_THREADS, 0, stream>>>(h, k);
                 if (ev) cudaEventRecord(ev[3], stream);
-                k_eigenray<<<148, 128, 0, stream>>>(d_q, k);
+                k_eigenray<<<148, 128, 0, stream>>>(h, k);
                 launches += 2;
             } else if (ev) {
                 cudaEventRecord(ev[3], stream);
@@ -1015,25 +1015,18 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     if (cudaMemset(q->d_counts, 0, 16 * sizeof(uint32_t)) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
 
-    if (cudaMalloc(&q->d_q, sizeof(QueueDev)) != cudaSuccess)
-        return cleanup(fail(WQ3D_ERR_CUDA, "cudaMalloc failed"));
-    if (cudaMemcpy(q->d_q, &h, sizeof(QueueDev), cudaMemcpyHostToDevice) != cudaSuccess)
-        return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
-
     /* wave_queue ctor: init_wave, update, init_wavefronts */
     q->gridded = ocean->dev.prof.kind == WQ3D_PROFILE_GRID || ocean->dev.surf.kind == WQ3D_BOUNDARY_GRID ||
                  ocean->dev.bot.kind == WQ3D_BOUNDARY_GRID;
     q->k_reflect_fn = q->gridded ? gridded::k_reflect : analytic::k_reflect;
     q->k_advance_fn = q->gridded ? gridded::k_advance : analytic::k_advance;
     (q->gridded ? gridded::k_startup : analytic::k_startup)<<<(unsigned)((n + 127) / 128), 128, 0, q->stream>>>(
-        q->d_q);
+        h);
     cudaError_t e = cudaStreamSynchronize(q->stream);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return cleanup(fail(WQ3D_ERR_CUDA, std::string("start-up kernel: ") + cudaGetErrorString(e)));
     /* spreading_ray.cc:44: sound speed of ray (0,0) on the first front */
     if (cudaMemcpy(&h.init_sound_speed, h.F[2].c, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
-        return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
-    if (cudaMemcpy(q->d_q, &h, sizeof(QueueDev), cudaMemcpyHostToDevice) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
     if (cudaEventCreate(&q->ev_begin) != cudaSuccess || cudaEventCreate(&q->ev_end) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
@@ -1069,7 +1062,7 @@ int wq3d_queue_set_thresholds(wq3d_queue* q, const wq3d_thresholds* t) {
     q->h.max_upper = t->max_upper;
     q->h.max_lower = t->max_lower;
     q->h.verb_threshold = std::pow(10.0, -0.1 * std::abs(t->eigenverb)); /* wave_thresholds.h:87-89 */
-    WQ_CK(cudaMemcpy(q->d_q, &q->h, sizeof(QueueDev), cudaMemcpyHostToDevice));
+    q->drop_graph();
     return WQ3D_OK;
 }
 
@@ -1089,11 +1082,9 @@ int wq3d_queue_set_callbacks(wq3d_queue* q, const wq3d_callbacks* cb, void* ctx)
         if (rc) return rc;
     }
     if (want != q->h.want_refl || want_verbs != q->h.want_verbs) {
-        const bool pass = q->volume_pass();
         q->h.want_refl = want;
         q->h.want_verbs = want_verbs;
-        if (pass != q->volume_pass()) q->drop_graph();
-        WQ_CK(cudaMemcpy(q->d_q, &q->h, sizeof(QueueDev), cudaMemcpyHostToDevice));
+        q->drop_graph();
     }
     return WQ3D_OK;
 }
@@ -1280,7 +1271,7 @@ int wq3d_queue_enable_sensitivity(wq3d_queue* q) {
     WQ_CK(cudaMemset(dA, 0, 4 * 3 * n * sizeof(double)));
     for (int f = 0; f < 4; ++f) q->h.F[f].dA = dA + (size_t)f * 3 * n;
     q->h.sens = 1;
-    WQ_CK(cudaMemcpy(q->d_q, &q->h, sizeof(QueueDev), cudaMemcpyHostToDevice));
+    q->drop_graph();
     return WQ3D_OK;
 }
 

@@ -140,24 +140,26 @@ struct QueueDev {
     uint32_t* err;
 };
 
-/* kernels (wq3d_kernels.cu).  The ray-stepping kernels come in two
+/* kernels (wq3d_kernels.cu).  Every kernel takes the queue descriptor by
+ * value as a __grid_constant__ parameter, so its fields are read through
+ * the constant cache.  The ray-stepping kernels come in two
  * builds: "gridded" evaluates every profile and boundary kind, "analytic"
  * leaves out the gridded ones (whose out-of-line interpolation calls cost
  * the stepping kernels registers) and serves oceans without grids. */
 #define WQ3D_DECLARE_STEP_KERNELS                         \
-    __global__ void k_startup(const QueueDev* q);         \
-    __global__ void k_reflect(const QueueDev* q, int k);  \
-    __global__ void k_advance(const QueueDev* q, int k);
+    __global__ void k_startup(__grid_constant__ const QueueDev q);         \
+    __global__ void k_reflect(__grid_constant__ const QueueDev q, int k);  \
+    __global__ void k_advance(__grid_constant__ const QueueDev q, int k);
 namespace gridded {
 WQ3D_DECLARE_STEP_KERNELS
 }
 namespace analytic {
 WQ3D_DECLARE_STEP_KERNELS
 }
-__global__ void k_volume(const QueueDev* q, int k);
-__global__ void k_cpa(const QueueDev* q, int k);
-__global__ void k_cpa_f32(const QueueDev* q, int k);
-__global__ void k_eigenray(const QueueDev* q, int k);
+__global__ void k_volume(__grid_constant__ const QueueDev q, int k);
+__global__ void k_cpa(__grid_constant__ const QueueDev q, int k);
+__global__ void k_cpa_f32(__grid_constant__ const QueueDev q, int k);
+__global__ void k_eigenray(__grid_constant__ const QueueDev q, int k);
 __global__ void k_sound_speed(OceanDev oc, double R, int n, const double* rho,
                               const double* theta, const double* phi,
                               double* c, double* g);

@@ -148,6 +148,33 @@ __device__ __forceinline__ void load_ray(const FrontPtrs& f, int r, RayS& y) {
     y.dist = f.dist[r];
 }
 
+/* load_ray through the read-only data cache, for kernels that never write
+ * the arrays they read this way: the loads may then all be in flight at
+ * once instead of waiting behind stores to the caller's copy */
+__device__ __forceinline__ void load_ray_ro(const FrontPtrs& f, int r, RayS& y) {
+    double v[17];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v[k] = __ldg(f.pos[k] + r);
+        v[3 + k] = __ldg(f.pg[k] + r);
+        v[6 + k] = __ldg(f.nd[k] + r);
+        v[9 + k] = __ldg(f.ng[k] + r);
+        v[12 + k] = __ldg(f.sg[k] + r);
+    }
+    v[15] = __ldg(f.c + r);
+    v[16] = __ldg(f.dist + r);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        y.pos[k] = v[k];
+        y.pg[k] = v[3 + k];
+        y.nd[k] = v[6 + k];
+        y.ng[k] = v[9 + k];
+        y.sg[k] = v[12 + k];
+    }
+    y.c = v[15];
+    y.dist = v[16];
+}
+
 /* reflection_model::reflection_copy (reflection_model.cc:335-360); the
  * copied path_length of a fresh 1x1 front is zero, so it is left alone */
 __device__ __forceinline__ void copy_ray(const FrontPtrs& f, int r, const RayS& y) {
@@ -626,8 +653,7 @@ namespace WQ3D_KERNEL_NS {
 /* ------------------------------------------------------------------ */
 /* start-up: wave_queue ctor (wave_queue.cc:83-85) for one ray         */
 /* ------------------------------------------------------------------ */
-__global__ void __launch_bounds__(128) k_startup(const QueueDev* __restrict__ qp) {
-    const QueueDev& q = *qp;
+__global__ void __launch_bounds__(128) k_startup(__grid_constant__ const QueueDev q) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= q.n) return;
     const int d = i / q.naz, a = i % q.naz;
@@ -697,8 +723,7 @@ __global__ void __launch_bounds__(128) k_startup(const QueueDev* __restrict__ qp
  * copy of the ray.  The result goes to the ray's shadow slot; k_advance
  * commits it.  The fronts are only read here, so this kernel runs
  * concurrently with k_cpa / k_eigenray of step s-1. */
-__global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp, int k) {
-    const QueueDev& q = *qp;
+__global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev q, int k) {
     const int64_t s = *q.d_base + k;
     const uint32_t nsurf = min(*q.n_work[s & 1], (uint32_t)q.n);
     const uint32_t nwork = nsurf + min(*q.n_work_b[s & 1], (uint32_t)q.n - nsurf);
@@ -713,16 +738,25 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
         const uint32_t w = ww < nsurf ? ww : (uint32_t)q.n - 1 - (ww - nsurf);
         const int i = (int)work[w];
         RayLocal L;
-        load_ray(*R.V, i, L.v);
-        load_ray(*R.C, i, L.c);
-        load_ray(*R.X, i, L.x);
-        for (int f = 0; f < q.nf; ++f) {
-            L.att[f] = R.X->atten[(size_t)f * q.n + i];
-            L.ph[f] = R.X->phase[(size_t)f * q.n + i];
+        {
+            /* the fronts are read-only here (only X.dA is written, and it
+             * is not read this way) */
+            RayS v, c, x;
+            load_ray_ro(*R.V, i, v);
+            load_ray_ro(*R.C, i, c);
+            load_ray_ro(*R.X, i, x);
+            const int sf = __ldg(R.X->surface + i), bt = __ldg(R.X->bottom + i), cs = __ldg(R.X->caustic + i);
+            L.v = v;
+            L.c = c;
+            L.x = x;
+            L.surface = sf;
+            L.bottom = bt;
+            L.caustic = cs;
         }
-        L.surface = R.X->surface[i];
-        L.bottom = R.X->bottom[i];
-        L.caustic = R.X->caustic[i];
+        for (int f = 0; f < q.nf; ++f) {
+            L.att[f] = __ldg(R.X->atten + (size_t)f * q.n + i);
+            L.ph[f] = __ldg(R.X->phase + (size_t)f * q.n + i);
+        }
         /* detect_caustics of the neighbour below (wave_queue.cc:274-292),
          * which the reference runs before this ray reflects; that
          * neighbour is read only when it does not reflect */
@@ -815,8 +849,7 @@ __global__ void __launch_bounds__(64) k_reflect(const QueueDev* __restrict__ qp,
  * becomes "curr" (wave_front.cc:184-216; reflecting neighbours are read
  * from their shadow slots), the rotation, AB3 and update of the new front
  * (wave_queue.cc:162-183), and the reflection decision of the next step. */
-__global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp, int k) {
-    const QueueDev& q = *qp;
+__global__ void __launch_bounds__(128) k_advance(__grid_constant__ const QueueDev q, int k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) *q.n_cand = 0;
     if (i >= q.n) return;
@@ -920,8 +953,7 @@ __global__ void __launch_bounds__(128) k_advance(const QueueDev* __restrict__ qp
  * (wave_queue.cc:202; k_reflect handles the reflecting ones).  Launched
  * before k_advance of the same step, only when an eigenverb listener is
  * installed and the ocean has volume layers. */
-__global__ void __launch_bounds__(128) k_volume(const QueueDev* __restrict__ qp, int k) {
-    const QueueDev& q = *qp;
+__global__ void __launch_bounds__(128) k_volume(__grid_constant__ const QueueDev q, int k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= q.n) return;
     const int64_t s = *q.d_base + k;
@@ -1010,8 +1042,7 @@ __device__ bool is_closest(const QueueDev& q, const FrontPtrs& V, const FrontPtr
 
 }  // namespace
 
-__global__ void __launch_bounds__(CPA_THREADS) k_cpa(const QueueDev* __restrict__ qp, int k) {
-    const QueueDev& q = *qp;
+__global__ void __launch_bounds__(CPA_THREADS) k_cpa(__grid_constant__ const QueueDev q, int k) {
     __shared__ TgtS tile[CPA_TARGETS];
     const int64_t s = *q.d_base + k + 1; /* roles after this step's rotation */
     const FrontPtrs& V = q.F[(s + 1) & 3];
@@ -1150,8 +1181,7 @@ __device__ __forceinline__ float screen_dot(const TgtW& g, const float* d) {
     return a + b;
 }
 
-__global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(const QueueDev* __restrict__ qp, int k) {
-    const QueueDev& q = *qp;
+__global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(__grid_constant__ const QueueDev q, int k) {
     __shared__ TgtS tile[F32_TARGETS];
     __shared__ TgtW tw[F32_TARGETS];
     __shared__ float wmax[CPA_THREADS / 32][8];
@@ -1864,8 +1894,7 @@ __device__ void compute_offsets(const QueueDev& q, const FrontPtrs& V, const Fro
 
 constexpr int EIG_WARPS = 4;
 
-__global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(const QueueDev* __restrict__ qp, int k) {
-    const QueueDev& q = *qp;
+__global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ const QueueDev q, int k) {
     __shared__ double s_cube[EIG_WARPS][27];
     __shared__ double s_ang[EIG_WARPS][2][27];
     const int warp = threadIdx.x >> 5;
@@ -1874,7 +1903,7 @@ __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(const QueueDev* __r
     const double time = q.d_times[k + 1];
     const uint32_t ncand = min(*q.n_cand, q.cap_cand);
     WarpBuild B;
-    B.q = qp;
+    B.q = &q;
     B.pV = &q.F[(s + 1) & 3];
     B.pC = &q.F[(s + 2) & 3];
     B.pX = &q.F[(s + 3) & 3];
