@@ -401,3 +401,48 @@ def test_fp32c_matches_oracle_on_sloped_workload(engine):
     q.run(sc["time_max"])
     o.run(sc["time_max"])
     compare_eigenrays(q.take_eigenrays(), o.take_eigenrays())
+
+
+class _Log(u.eigenray_listener, u.reflection_listener):
+    """records every listener call in order"""
+
+    def __init__(self):
+        self.calls = []
+
+    def add_eigenray(self, t1, t2, ray, run_id):
+        self.calls.append(("ray", t1, t2, ray.travel_time, tuple(ray.intensity), ray.source_de, ray.source_az))
+
+    def check_eigenrays(self, time, run_id):
+        self.calls.append(("check", time))
+
+    def reflect(self, time, de, az, dt, grazing, speed, position, ndirection, type):
+        self.calls.append(("reflect", time, de, az, dt, grazing, speed,
+                           (position.rho, position.theta, position.phi), tuple(ndirection), type))
+
+
+@pytest.mark.parametrize("precision", [_abi.FP64, _abi.FP32C])
+def test_queued_chunks_match_single_chunks(engine, precision):
+    """A run of many chunks queues chunk c+1 before it delivers chunk c and
+    reflects each chunk's first step beside the previous chunk's last CPA
+    search.  Stepping one partial chunk at a time does neither, and every
+    listener call must come out the same, in the same order."""
+    sc = S.linear_slope_rayleigh(num_de=181, num_az=19, n_range=8, n_depth=8, time_max=10.0)
+    a = S.build_queue(sc, u.wave_queue, precision=precision)
+    b = S.build_queue(sc, u.wave_queue, precision=precision)
+    la, lb = _Log(), _Log()
+    for q, lg in ((a, la), (b, lb)):
+        q.add_eigenray_listener(lg)
+        q.add_reflection_listener(lg)
+    a.run(sc["time_max"])
+    n = a.steps()
+    assert n > 3 * 16
+    while b.steps() < n:
+        b.step(5)
+        b.step(2)
+    # the stepped queue may run a few steps past the run: compare the calls
+    # of the run's steps
+    checks = [i for i, c in enumerate(lb.calls) if c[0] == "check"]
+    cut = checks[n - 1] + 1
+    assert sum(1 for c in la.calls if c[0] == "reflect") > 100
+    assert sum(1 for c in la.calls if c[0] == "ray") > 10
+    assert la.calls == lb.calls[:cut]

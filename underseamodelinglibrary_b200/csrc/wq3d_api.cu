@@ -211,17 +211,43 @@ struct wq3d_queue {
     QueueDev h{};
     std::vector<void*> allocs;
     void* pinned = nullptr;
-    int64_t* h_base = nullptr;
-    double* h_times = nullptr;
-    uint32_t* h_counts = nullptr; /* n_rec, n_refl, err, n_cand */
+    /* per result set: chunk base step, chunk times, counters read back
+     * (n_rec, n_refl, err, n_cand, ..., n_verb) */
+    int64_t* h_base[2] = {nullptr, nullptr};
+    double* h_times[2] = {nullptr, nullptr};
+    uint32_t* h_counts[2] = {nullptr, nullptr};
     int64_t* d_base = nullptr;
     double* d_times = nullptr;
     uint32_t* d_counts = nullptr;
     int chunk = 16;
-    cudaGraphExec_t graph = nullptr;
-    bool graph_failed = false;
+    /* [result set][prefetches the next chunk's first reflection] */
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    bool graph_failed[2][2] = {{false, false}, {false, false}};
+    /* Result set 1: a second copy of the record buffers, so that chunk c
+     * writes set c & 1 while the host reads the other chunk's records
+     * (made by the first run of more than one chunk; set 0 lives in h). */
+    struct ResultSet {
+        wq3d_eigenray* rec = nullptr;
+        double* rec_inten = nullptr;
+        double* rec_phase = nullptr;
+        double* rec_sens = nullptr;
+        wq3d_reflection* refl = nullptr;
+        wq3d_eigenverb* verb = nullptr;
+        double* verb_power = nullptr;
+    } set1;
+    bool have_set1 = false;
+    cudaEvent_t done_ev[2] = {nullptr, nullptr}; /* a chunk's counters are on the host */
+    cudaStream_t copy = nullptr;                 /* record read-back */
+    /* delivered state (time(), steps()) and launched-through state */
     double time = 0.0;
     int64_t steps = 0;
+    double ltime = 0.0;
+    int64_t lsteps = 0;
+    /* reflection notices and eigenverbs of a step that a chunk's tail
+     * reflection made for the next chunk, delivered with that chunk */
+    std::vector<wq3d_reflection> carry_refl;
+    std::vector<wq3d_eigenverb> carry_verb;
+    std::vector<double> carry_vpower;
     double src_clamped[3] = {0, 0, 0};
     wq3d_callbacks cb{};
     void* cb_ctx = nullptr;
@@ -247,9 +273,58 @@ struct wq3d_queue {
      * parameters), so it is rebuilt whenever the descriptor or the launch
      * sequence changes */
     void drop_graph() {
-        if (graph) cudaGraphExecDestroy(graph);
-        graph = nullptr;
-        graph_failed = false;
+        for (int p = 0; p < 2; ++p)
+            for (int t = 0; t < 2; ++t) {
+                if (graph[p][t]) cudaGraphExecDestroy(graph[p][t]);
+                graph[p][t] = nullptr;
+                graph_failed[p][t] = false;
+            }
+    }
+
+    /* the descriptor that writes result set p */
+    QueueDev dev(int p) const {
+        QueueDev d = h;
+        if (p == 1) {
+            d.rec = set1.rec;
+            d.rec_inten = set1.rec_inten;
+            d.rec_phase = set1.rec_phase;
+            d.rec_sens = set1.rec_sens;
+            d.refl = set1.refl;
+            d.verb = set1.verb;
+            d.verb_power = set1.verb_power;
+        }
+        return d;
+    }
+
+    /* Result set 1, the same sizes as set 0.  Returns false (and the run
+     * stays on set 0, one chunk at a time) when the memory is not there. */
+    bool ensure_set1() {
+        if (have_set1) return true;
+        const size_t nf = (size_t)h.nf;
+        ResultSet s;
+        std::vector<void*> got;
+        auto take = [&](auto** out, size_t count) {
+            void* p = nullptr;
+            if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(**out)) != cudaSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+            got.push_back(p);
+            *out = static_cast<std::remove_reference_t<decltype(*out)>>(p);
+            return true;
+        };
+        bool ok = take(&s.rec, h.cap_rec) && take(&s.rec_inten, (size_t)h.cap_rec * nf) &&
+                  take(&s.rec_phase, (size_t)h.cap_rec * nf) && take(&s.refl, h.cap_refl) &&
+                  (!h.sens || take(&s.rec_sens, (size_t)h.cap_rec * 3)) &&
+                  (!h.verb || (take(&s.verb, h.cap_verb) && take(&s.verb_power, (size_t)h.cap_verb * nf)));
+        if (!ok) {
+            for (void* p : got) cudaFree(p);
+            return false;
+        }
+        allocs.insert(allocs.end(), got.begin(), got.end());
+        set1 = s;
+        have_set1 = true;
+        return true;
     }
 
     bool volume_pass() const { return h.want_verbs && h.oc.nvol > 0; }
@@ -261,34 +336,77 @@ struct wq3d_queue {
         cudaFree(p);
     }
 
-    /* Eigenverb buffers hold at least "need" records (one chunk's worth).
-     * They start at half a record per ray, step and interface and grow
-     * when a chunk fills more than half of them; a quarter of the free
-     * device memory is the limit. */
-    int ensure_verb_capacity(size_t need) {
-        if (h.verb && need <= h.cap_verb) return WQ3D_OK;
-        const size_t rec_bytes = sizeof(wq3d_eigenverb) + (size_t)h.nf * sizeof(double);
+    /* A record buffer's capacity for "need" records of rec_bytes each: at
+     * least 4096, at most a quarter of the free device memory. */
+    int record_capacity(size_t need, size_t rec_bytes, size_t* out) {
         size_t free_b = 0, total_b = 0;
         WQ_CK(cudaMemGetInfo(&free_b, &total_b));
         const size_t limit = std::max<size_t>(4096, (free_b / 4) / rec_bytes);
-        const size_t cap = std::min<size_t>({std::max<size_t>(need, 4096), limit, (size_t)UINT32_MAX / 2});
+        *out = std::min<size_t>({std::max<size_t>(need, 4096), limit, (size_t)UINT32_MAX / 2});
+        return WQ3D_OK;
+    }
+    template <class T>
+    int remake(T** p, size_t count) {
+        release(*p);
+        *p = nullptr;
+        return alloc(p, count);
+    }
+
+    /* Eigenverb buffers (both result sets) hold at least "need" records.
+     * They start at half a record per ray, step and interface of a chunk
+     * and grow when a chunk fills more than half of them.  Runs with no
+     * chunk in flight; drops the graphs, which hold the pointers. */
+    int ensure_verb_capacity(size_t need) {
+        if (h.verb && need <= h.cap_verb) return WQ3D_OK;
+        size_t cap = 0;
+        int rc = record_capacity(need, sizeof(wq3d_eigenverb) + (size_t)h.nf * sizeof(double), &cap);
+        if (rc) return rc;
         if (h.verb && cap <= h.cap_verb) return WQ3D_OK;
         WQ_CK(cudaStreamSynchronize(stream));
-        release(h.verb);
-        release(h.verb_power);
-        h.verb = nullptr;
-        h.verb_power = nullptr;
         h.cap_verb = 0;
-        int rc = alloc(&h.verb, cap);
-        if (!rc) rc = alloc(&h.verb_power, cap * (size_t)h.nf);
+        rc = remake(&h.verb, cap);
+        if (!rc) rc = remake(&h.verb_power, cap * (size_t)h.nf);
+        if (!rc && have_set1) rc = remake(&set1.verb, cap);
+        if (!rc && have_set1) rc = remake(&set1.verb_power, cap * (size_t)h.nf);
         if (rc) return rc;
         h.cap_verb = (uint32_t)cap;
         drop_graph();
         return WQ3D_OK;
     }
 
+    /* Reflection buffers: half a record per ray and step of a chunk when a
+     * reflection listener first asks, grown like the eigenverb buffers. */
+    int ensure_refl_capacity(size_t need) {
+        if (need <= h.cap_refl) return WQ3D_OK;
+        size_t cap = 0;
+        int rc = record_capacity(need, sizeof(wq3d_reflection), &cap);
+        if (rc) return rc;
+        if (cap <= h.cap_refl) return WQ3D_OK;
+        WQ_CK(cudaStreamSynchronize(stream));
+        h.cap_refl = 0;
+        rc = remake(&h.refl, cap);
+        if (!rc && have_set1) rc = remake(&set1.refl, cap);
+        if (rc) return rc;
+        h.cap_refl = (uint32_t)cap;
+        drop_graph();
+        return WQ3D_OK;
+    }
+
+    /* growth asked for by a chunk's counts, done when nothing is in flight */
+    size_t grow_verb = 0, grow_refl = 0;
+    int apply_growth() {
+        int rc = WQ3D_OK;
+        if (grow_verb) rc = ensure_verb_capacity(grow_verb);
+        if (!rc && grow_refl) rc = ensure_refl_capacity(grow_refl);
+        grow_verb = grow_refl = 0;
+        return rc;
+    }
+
     ~wq3d_queue() {
-        if (graph) cudaGraphExecDestroy(graph);
+        drop_graph();
+        for (auto e : done_ev)
+            if (e) cudaEventDestroy(e);
+        if (copy) cudaStreamDestroy(copy);
         for (auto e : events) cudaEventDestroy(e);
         for (auto e : fork_ev) cudaEventDestroy(e);
         for (auto e : join_ev) cudaEventDestroy(e);
@@ -319,35 +437,40 @@ struct wq3d_queue {
         return WQ3D_OK;
     }
 
-    /* One chunk of K steps.  Step k's reflections run on the side stream
-     * while step k-1's CPA search and eigenray construction run on the main
-     * stream (k_reflect only reads the fronts and writes shadow slots);
-     * k_advance(k) waits for both. */
-    int launch_chunk(int K) {
+    /* One chunk of K steps writing result set p.  Step k's reflections run
+     * on the side stream while step k-1's CPA search and eigenray
+     * construction run on the main stream (k_reflect only reads the fronts
+     * and writes shadow slots); k_advance(k) waits for both.  With "tail"
+     * the reflections of the next chunk's first step run beside this
+     * chunk's last CPA search; that chunk's own k_reflect(0) then finds an
+     * empty worklist and returns. */
+    int launch_chunk(int K, int p, bool tail) {
+        const QueueDev d = dev(p);
         const int n = h.n;
         const dim3 blk(128);
         const dim3 grd((n + 127) / 128);
         const int rgrid = std::max(1, std::min(4 * 148, (n + 63) / 64));
+        if (timing) tail = false;
         if (timing) cudaEventRecord(events[7 * K], stream);
-        k_reflect_fn<<<rgrid, 64, 0, stream>>>(h, 0);
+        k_reflect_fn<<<rgrid, 64, 0, stream>>>(d, 0);
         if (timing) cudaEventRecord(events[7 * K + 1], stream);
         launches += 1;
         for (int k = 0; k < K; ++k) {
             cudaEvent_t* ev = timing ? &events[7 * k] : nullptr;
             if (ev) cudaEventRecord(ev[0], stream);
             if (volume_pass()) {
-                k_volume<<<grd, blk, 0, stream>>>(h, k);
+                k_volume<<<grd, blk, 0, stream>>>(d, k);
                 launches += 1;
             }
-            k_advance_fn<<<grd, blk, 0, stream>>>(h, k);
+            k_advance_fn<<<grd, blk, 0, stream>>>(d, k);
             if (ev) cudaEventRecord(ev[1], stream);
             launches += 1;
-            const bool more = k + 1 < K;
+            const bool more = k + 1 < K || tail;
             if (more) {
                 cudaEventRecord(fork_ev[k], stream);
                 cudaStreamWaitEvent(side, fork_ev[k], 0);
                 if (ev) cudaEventRecord(ev[5], side);
-                k_reflect_fn<<<rgrid, 64, 0, side>>>(h, k + 1);
+                k_reflect_fn<<<rgrid, 64, 0, side>>>(d, k + 1);
                 if (ev) cudaEventRecord(ev[6], side);
                 cudaEventRecord(join_ev[k], side);
                 launches += 1;
@@ -359,11 +482,11 @@ struct wq3d_queue {
                     k_cpa_f32<<<dim3(((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) *
                                          ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
                                      (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS),
-                                CPA_THREADS, 0, stream>>>(h, k);
+                                CPA_THREADS, 0, stream>>>(d, k);
                 else
-                    k_cpa<<<cg, CPA_THREADS, 0, stream>>>(h, k);
+                    k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d, k);
                 if (ev) cudaEventRecord(ev[3], stream);
-                k_eigenray<<<148, 128, 0, stream>>>(h, k);
+                k_eigenray<<<148, 128, 0, stream>>>(d, k);
                 launches += 2;
             } else if (ev) {
                 cudaEventRecord(ev[3], stream);
@@ -374,31 +497,35 @@ struct wq3d_queue {
         return WQ3D_OK;
     }
 
-    int build_graph() {
-        if (graph || graph_failed) return WQ3D_OK;
+    int build_graph(int p, bool tail) {
+        const int t = tail ? 1 : 0;
+        if (graph[p][t] || graph_failed[p][t]) return WQ3D_OK;
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-            graph_failed = true;
+            graph_failed[p][t] = true;
             cudaGetLastError();
             return WQ3D_OK;
         }
         const bool save = timing;
         timing = false;
         const int64_t saved_launches = launches;
-        launch_chunk(chunk);
+        launch_chunk(chunk, p, tail);
         launches = saved_launches;
         timing = save;
         if (cudaStreamEndCapture(stream, &g) != cudaSuccess ||
-            cudaGraphInstantiate(&graph, g, 0) != cudaSuccess) {
-            graph_failed = true;
-            graph = nullptr;
+            cudaGraphInstantiate(&graph[p][t], g, 0) != cudaSuccess) {
+            graph_failed[p][t] = true;
+            graph[p][t] = nullptr;
             cudaGetLastError();
         }
         if (g) cudaGraphDestroy(g);
         return WQ3D_OK;
     }
 
-    void deliver(int K, size_t nrec, size_t nrefl, size_t nverb) {
+    /* Listener calls for the K steps after "steps", in the reference's
+     * order.  Reflection notices and eigenverbs of the step after the
+     * chunk (made by its tail reflection) are kept for the next chunk. */
+    void deliver(int K, size_t nrec, size_t nrefl, size_t nverb, const double* ht) {
         const int nf = h.nf;
         /* reference order: (step, t1, t2, de, az) for eigenrays
          * (wave_queue.cc:361-373), (step, de, az) for reflections */
@@ -413,7 +540,9 @@ struct wq3d_queue {
             if (x.de != y.de) return x.de < y.de;
             return x.az < y.az;
         });
-        std::vector<wq3d_reflection> refl(h_refl.begin(), h_refl.begin() + nrefl);
+        std::vector<wq3d_reflection> refl;
+        refl.swap(carry_refl);
+        refl.insert(refl.end(), h_refl.begin(), h_refl.begin() + nrefl);
         std::sort(refl.begin(), refl.end(), [](const wq3d_reflection& x, const wq3d_reflection& y) {
             if (x.step != y.step) return x.step < y.step;
             if (x.de != y.de) return x.de < y.de;
@@ -422,11 +551,17 @@ struct wq3d_queue {
         });
         /* eigenverbs: (step, de, az, seq) is the order of the reference's
          * detect_reflections loop (wave_queue.cc:197-216) */
-        std::vector<size_t> vorder(nverb);
-        for (size_t i = 0; i < nverb; ++i) vorder[i] = i;
+        std::vector<wq3d_eigenverb> verbs;
+        std::vector<double> vpower;
+        verbs.swap(carry_verb);
+        vpower.swap(carry_vpower);
+        verbs.insert(verbs.end(), h_verb.begin(), h_verb.begin() + nverb);
+        vpower.insert(vpower.end(), h_vpower.begin(), h_vpower.begin() + nverb * nf);
+        std::vector<size_t> vorder(verbs.size());
+        for (size_t i = 0; i < vorder.size(); ++i) vorder[i] = i;
         std::sort(vorder.begin(), vorder.end(), [&](size_t a, size_t b) {
-            const wq3d_eigenverb& x = h_verb[a];
-            const wq3d_eigenverb& y = h_verb[b];
+            const wq3d_eigenverb& x = verbs[a];
+            const wq3d_eigenverb& y = verbs[b];
             if (x.step != y.step) return x.step < y.step;
             if (x.de != y.de) return x.de < y.de;
             if (x.az != y.az) return x.az < y.az;
@@ -438,12 +573,12 @@ struct wq3d_queue {
             /* a reflection is announced before the eigenverb it makes, and
              * both carry the ray's event number */
             while ((ir < refl.size() && refl[ir].step == step) ||
-                   (iv < vorder.size() && h_verb[vorder[iv]].step == step)) {
-                const bool verb_here = iv < vorder.size() && h_verb[vorder[iv]].step == step;
+                   (iv < vorder.size() && verbs[vorder[iv]].step == step)) {
+                const bool verb_here = iv < vorder.size() && verbs[vorder[iv]].step == step;
                 const bool refl_here = ir < refl.size() && refl[ir].step == step;
                 bool take_refl = refl_here;
                 if (refl_here && verb_here) {
-                    const wq3d_eigenverb& v = h_verb[vorder[iv]];
+                    const wq3d_eigenverb& v = verbs[vorder[iv]];
                     take_refl = !(std::make_tuple(v.de, v.az, v.seq) <
                                   std::make_tuple(refl[ir].de, refl[ir].az, refl[ir].pad));
                 }
@@ -453,7 +588,7 @@ struct wq3d_queue {
                 } else {
                     const size_t j = vorder[iv];
                     if (cb.add_eigenverb)
-                        cb.add_eigenverb(cb_ctx, &h_verb[j], &h_vpower[j * nf], (size_t)nf, h_verb[j].interface_num);
+                        cb.add_eigenverb(cb_ctx, &verbs[j], &vpower[j * nf], (size_t)nf, verbs[j].interface_num);
                     ++iv;
                 }
             }
@@ -473,37 +608,51 @@ struct wq3d_queue {
                 }
                 ++ie;
             }
-            if (cb.check_eigenrays) cb.check_eigenrays(cb_ctx, h_times[k + 1], run_id);
+            if (cb.check_eigenrays) cb.check_eigenrays(cb_ctx, ht[k + 1], run_id);
+        }
+        carry_refl.assign(refl.begin() + ir, refl.end());
+        for (; iv < vorder.size(); ++iv) {
+            const size_t j = vorder[iv];
+            carry_verb.push_back(verbs[j]);
+            carry_vpower.insert(carry_vpower.end(), &vpower[j * nf], &vpower[j * nf] + nf);
         }
     }
 
-    /* Queues chunk K's work on the stream without waiting for it. */
-    int chunk_launch(int K) {
-        h_base[0] = steps;
-        h_times[0] = time;
-        for (int k = 0; k < K; ++k) h_times[k + 1] = h_times[k] + h.dt;
-        WQ_CK(cudaMemcpyAsync(d_base, h_base, sizeof(int64_t), cudaMemcpyHostToDevice, stream));
-        WQ_CK(cudaMemcpyAsync(d_times, h_times, (K + 1) * sizeof(double), cudaMemcpyHostToDevice, stream));
+    /* Queues chunk K's work (result set p) on the stream without waiting
+     * for it; "tail" also reflects the following chunk's first step. */
+    int chunk_launch(int K, int p, bool tail) {
+        int64_t* hb = h_base[p];
+        double* ht = h_times[p];
+        hb[0] = lsteps;
+        ht[0] = ltime;
+        for (int k = 0; k < K; ++k) ht[k + 1] = ht[k] + h.dt;
+        WQ_CK(cudaMemcpyAsync(d_base, hb, sizeof(int64_t), cudaMemcpyHostToDevice, stream));
+        WQ_CK(cudaMemcpyAsync(d_times, ht, (K + 1) * sizeof(double), cudaMemcpyHostToDevice, stream));
         WQ_CK(cudaMemsetAsync(d_counts, 0, 3 * sizeof(uint32_t), stream));
         WQ_CK(cudaMemsetAsync(d_counts + 8, 0, sizeof(uint32_t), stream));
-        if (!timing && K == chunk) {
-            build_graph();
-        }
-        if (!timing && K == chunk && graph) {
-            WQ_CK(cudaGraphLaunch(graph, stream));
-            launches += ((h.nt > 0 ? 4 : 2) + (volume_pass() ? 1 : 0)) * (int64_t)K;
+        if (timing) tail = false;
+        const int t = tail ? 1 : 0;
+        if (!timing && K == chunk) build_graph(p, tail);
+        if (!timing && K == chunk && graph[p][t]) {
+            WQ_CK(cudaGraphLaunch(graph[p][t], stream));
+            launches += ((h.nt > 0 ? 4 : 2) + (volume_pass() ? 1 : 0)) * (int64_t)K + (tail ? 1 : 0);
         } else {
-            launch_chunk(K);
+            launch_chunk(K, p, tail);
         }
         WQ_CK(cudaGetLastError());
-        WQ_CK(cudaMemcpyAsync(h_counts, d_counts, 9 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        WQ_CK(cudaMemcpyAsync(h_counts[p], d_counts, 9 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        WQ_CK(cudaEventRecord(done_ev[p], stream));
+        lsteps += K;
+        ltime = ht[K];
         return WQ3D_OK;
     }
 
-    /* Waits for chunk K, reads its records back and delivers them. */
-    int chunk_finish(int K) {
-        WQ_CK(cudaStreamSynchronize(stream));
+    /* Waits for chunk K of result set p (the oldest one in flight), reads
+     * its records back and delivers them. */
+    int chunk_finish(int K, int p) {
+        WQ_CK(cudaEventSynchronize(done_ev[p]));
         if (timing) {
+            WQ_CK(cudaStreamSynchronize(side));
             float r0 = 0;
             cudaEventElapsedTime(&r0, events[7 * K], events[7 * K + 1]);
             ms_refl += r0;
@@ -519,46 +668,48 @@ struct wq3d_queue {
                 ms_refl += r;
             }
         }
-        const uint32_t nrec = std::min(h_counts[0], h.cap_rec);
-        const uint32_t nrefl = std::min(h_counts[1], h.cap_refl);
-        const uint32_t err = h_counts[2];
-        const uint32_t nverb = h.want_verbs ? std::min(h_counts[8], h.cap_verb) : 0;
-        const uint32_t verbs_made = h.want_verbs ? h_counts[8] : 0;
+        const QueueDev d = dev(p);
+        const uint32_t* hc = h_counts[p];
+        const uint32_t nrec = std::min(hc[0], h.cap_rec);
+        const uint32_t nrefl = std::min(hc[1], h.cap_refl);
+        const uint32_t err = hc[2];
+        const uint32_t nverb = h.want_verbs ? std::min(hc[8], h.cap_verb) : 0;
+        const uint32_t verbs_made = h.want_verbs ? hc[8] : 0;
+        auto get = [&](void* dst, const void* src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, copy);
+        };
         if (nrec > 0) {
             if (h_rec.size() < nrec) {
                 h_rec.resize(nrec);
                 h_rinten.resize((size_t)nrec * h.nf);
                 h_rphase.resize((size_t)nrec * h.nf);
             }
-            WQ_CK(cudaMemcpy(h_rec.data(), h.rec, nrec * sizeof(wq3d_eigenray), cudaMemcpyDeviceToHost));
-            WQ_CK(cudaMemcpy(h_rinten.data(), h.rec_inten, (size_t)nrec * h.nf * sizeof(double), cudaMemcpyDeviceToHost));
-            WQ_CK(cudaMemcpy(h_rphase.data(), h.rec_phase, (size_t)nrec * h.nf * sizeof(double), cudaMemcpyDeviceToHost));
+            WQ_CK(get(h_rec.data(), d.rec, nrec * sizeof(wq3d_eigenray)));
+            WQ_CK(get(h_rinten.data(), d.rec_inten, (size_t)nrec * h.nf * sizeof(double)));
+            WQ_CK(get(h_rphase.data(), d.rec_phase, (size_t)nrec * h.nf * sizeof(double)));
             if (h.sens) {
                 if (h_rsens.size() < (size_t)nrec * 3) h_rsens.resize((size_t)nrec * 3);
-                WQ_CK(cudaMemcpy(h_rsens.data(), h.rec_sens, (size_t)nrec * 3 * sizeof(double),
-                                 cudaMemcpyDeviceToHost));
+                WQ_CK(get(h_rsens.data(), d.rec_sens, (size_t)nrec * 3 * sizeof(double)));
             }
         }
         if (nrefl > 0) {
             if (h_refl.size() < nrefl) h_refl.resize(nrefl);
-            WQ_CK(cudaMemcpy(h_refl.data(), h.refl, nrefl * sizeof(wq3d_reflection), cudaMemcpyDeviceToHost));
+            WQ_CK(get(h_refl.data(), d.refl, nrefl * sizeof(wq3d_reflection)));
         }
         if (nverb > 0) {
             if (h_verb.size() < nverb) {
                 h_verb.resize(nverb);
                 h_vpower.resize((size_t)nverb * h.nf);
             }
-            WQ_CK(cudaMemcpy(h_verb.data(), h.verb, nverb * sizeof(wq3d_eigenverb), cudaMemcpyDeviceToHost));
-            WQ_CK(cudaMemcpy(h_vpower.data(), h.verb_power, (size_t)nverb * h.nf * sizeof(double),
-                             cudaMemcpyDeviceToHost));
+            WQ_CK(get(h_verb.data(), d.verb, nverb * sizeof(wq3d_eigenverb)));
+            WQ_CK(get(h_vpower.data(), d.verb_power, (size_t)nverb * h.nf * sizeof(double)));
         }
-        deliver(K, nrec, nrefl, nverb);
-        if (verbs_made > h.cap_verb / 2 && !(err & ERR_VERB_OVERFLOW)) {
-            const int rc = ensure_verb_capacity(4 * (size_t)verbs_made);
-            if (rc) return rc;
-        }
+        WQ_CK(cudaStreamSynchronize(copy));
+        deliver(K, nrec, nrefl, nverb, h_times[p]);
+        if (verbs_made > h.cap_verb / 2) grow_verb = std::max(grow_verb, 4 * (size_t)verbs_made);
+        if (h.want_refl && hc[1] > h.cap_refl / 2) grow_refl = std::max(grow_refl, 4 * (size_t)hc[1]);
         steps += K;
-        time = h_times[K];
+        time = h_times[p][K];
         if (err & (ERR_CAND_OVERFLOW | ERR_REC_OVERFLOW | ERR_REFL_OVERFLOW | ERR_VERB_OVERFLOW))
             return fail(WQ3D_ERR_OVERFLOW, "eigenray, reflection or eigenverb buffer overflow (error bits " +
                                                std::to_string(err) + "); recreate the queue with a larger eigenray_capacity");
@@ -567,9 +718,51 @@ struct wq3d_queue {
         return WQ3D_OK;
     }
 
-    int run_chunk(int K) {
-        const int rc = chunk_launch(K);
-        return rc ? rc : chunk_finish(K);
+    /* nsteps steps in chunks.  Without per-kernel timing, chunk c+1 is
+     * queued before chunk c is delivered (result sets alternate), so the
+     * device does not wait for the host between chunks.  Each chunk but
+     * the last reflects the next one's first step.  A record buffer that a
+     * chunk filled past half grows once nothing is in flight.  An error or
+     * an abort stops further launches; the chunks already in flight are
+     * still delivered, and the first error is returned. */
+    int run_steps(size_t nsteps) {
+        const bool pipe = !timing && nsteps > (size_t)chunk && ensure_set1();
+        const size_t depth = pipe ? 2 : 1;
+        int K_in[2] = {0, 0}, p_in[2] = {0, 0};
+        size_t n_in = 0;
+        int next_p = 0;
+        int rc = WQ3D_OK;
+        size_t left = nsteps;
+        for (;;) {
+            if (n_in == 0 && !rc && (grow_verb || grow_refl)) rc = apply_growth();
+            while (left > 0 && !rc && n_in < depth && !grow_verb && !grow_refl) {
+                if (abort_flag.exchange(false)) {
+                    rc = fail(WQ3D_ERR_ABORTED, "aborted by caller");
+                    break;
+                }
+                const int K = (int)std::min<size_t>(left, (size_t)chunk);
+                left -= (size_t)K;
+                const int r = chunk_launch(K, next_p, left > 0);
+                if (r) {
+                    rc = r;
+                    break;
+                }
+                K_in[n_in] = K;
+                p_in[n_in] = next_p;
+                ++n_in;
+                if (pipe) next_p ^= 1;
+            }
+            if (n_in == 0) {
+                if (left > 0 && !rc && (grow_verb || grow_refl)) continue;
+                break;
+            }
+            const int r = chunk_finish(K_in[0], p_in[0]);
+            if (r && !rc) rc = r;
+            K_in[0] = K_in[1];
+            p_in[0] = p_in[1];
+            --n_in;
+        }
+        return rc;
     }
 
     /* steps of the reference loop "while (time() < time_max) step();" */
@@ -975,7 +1168,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.cap_cand = (uint32_t)(d->eigenray_capacity ? d->eigenray_capacity
                                                  : std::max<size_t>(4096, 32 * nt));
     h.cap_rec = (uint32_t)std::min<size_t>((size_t)h.cap_cand * q->chunk, (size_t)1 << 21);
-    h.cap_refl = (uint32_t)std::min<size_t>(std::max<size_t>(4096, 2 * n), (size_t)1 << 22);
+    h.cap_refl = 4096; /* grown when a reflection listener asks */
     uint32_t* cand = nullptr;
     if ((rc = q->alloc(&cand, 2 * (size_t)h.cap_cand))) return cleanup(rc);
     h.cand = cand;
@@ -1007,11 +1200,18 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.d_base = q->d_base;
     h.d_times = q->d_times;
     h.want_refl = 0;
-    if (cudaMallocHost(&q->pinned, 4096 + (q->chunk + 1) * sizeof(double)) != cudaSuccess)
-        return cleanup(fail(WQ3D_ERR_NOMEM, "cudaMallocHost failed"));
-    q->h_base = static_cast<int64_t*>(q->pinned);
-    q->h_counts = reinterpret_cast<uint32_t*>(static_cast<char*>(q->pinned) + 64);
-    q->h_times = reinterpret_cast<double*>(static_cast<char*>(q->pinned) + 128);
+    {
+        /* per result set: base step, counters, chunk times */
+        const size_t set_bytes = 128 + (((size_t)q->chunk + 1) * sizeof(double) + 63) / 64 * 64;
+        if (cudaMallocHost(&q->pinned, 2 * set_bytes) != cudaSuccess)
+            return cleanup(fail(WQ3D_ERR_NOMEM, "cudaMallocHost failed"));
+        for (int s = 0; s < 2; ++s) {
+            char* b = static_cast<char*>(q->pinned) + s * set_bytes;
+            q->h_base[s] = reinterpret_cast<int64_t*>(b);
+            q->h_counts[s] = reinterpret_cast<uint32_t*>(b + 64);
+            q->h_times[s] = reinterpret_cast<double*>(b + 128);
+        }
+    }
     if (cudaMemset(q->d_counts, 0, 16 * sizeof(uint32_t)) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
 
@@ -1030,8 +1230,12 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
     if (cudaEventCreate(&q->ev_begin) != cudaSuccess || cudaEventCreate(&q->ev_end) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-    if (cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
+    for (auto& e : q->done_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
     q->fork_ev.resize(q->chunk);
     q->join_ev.resize(q->chunk);
     for (int k = 0; k < q->chunk; ++k)
@@ -1076,6 +1280,10 @@ int wq3d_queue_set_callbacks(wq3d_queue* q, const wq3d_callbacks* cb, void* ctx)
     q->cb_ctx = ctx;
     const int want = q->cb.reflect ? 1 : 0;
     const int want_verbs = q->cb.add_eigenverb ? 1 : 0;
+    if (want) {
+        const int rc = q->ensure_refl_capacity((size_t)(q->chunk + 1) * q->h.n / 2);
+        if (rc) return rc;
+    }
     if (want_verbs && !q->h.verb) {
         /* eigenverb buffers, made the first time a listener asks */
         const int rc = q->ensure_verb_capacity((size_t)q->chunk * q->h.n * (q->h.oc.nvol + 1) / 2);
@@ -1094,17 +1302,7 @@ int wq3d_queue_step(wq3d_queue* q, size_t nsteps) {
     DeviceGuard guard(q->device);
     if (nsteps == 0) return WQ3D_OK;
     WQ_CK(cudaEventRecord(q->ev_begin, q->stream));
-    int rc = WQ3D_OK;
-    while (nsteps > 0) {
-        if (q->abort_flag.exchange(false)) {
-            rc = fail(WQ3D_ERR_ABORTED, "aborted by caller");
-            break;
-        }
-        const int K = (int)std::min<size_t>(nsteps, (size_t)q->chunk);
-        rc = q->run_chunk(K);
-        if (rc) break;
-        nsteps -= (size_t)K;
-    }
+    const int rc = q->run_steps(nsteps);
     WQ_CK(cudaEventRecord(q->ev_end, q->stream));
     WQ_CK(cudaEventSynchronize(q->ev_end));
     float ms = 0.0f;
@@ -1155,12 +1353,13 @@ int wq3d_batch_run(wq3d_queue* const* queues, size_t count, const double* time_m
                 break;
             }
             K[i] = std::min<size_t>(left[i], (size_t)queues[i]->chunk);
-            rc = queues[i]->chunk_launch((int)K[i]);
+            rc = queues[i]->chunk_launch((int)K[i], 0, left[i] > K[i]);
             if (rc) K[i] = 0;
         }
         for (size_t i = 0; i < count; ++i) {
             if (K[i] == 0) continue;
-            const int r = queues[i]->chunk_finish((int)K[i]);
+            int r = queues[i]->chunk_finish((int)K[i], 0);
+            if (!r) r = queues[i]->apply_growth();
             if (r && !rc) rc = r;
             left[i] -= K[i];
             any = any || left[i] > 0;
@@ -1267,6 +1466,7 @@ int wq3d_queue_enable_sensitivity(wq3d_queue* q) {
     double* dA = nullptr;
     int rc = q->alloc(&dA, 4 * 3 * n);
     if (!rc) rc = q->alloc(&q->h.rec_sens, (size_t)q->h.cap_rec * 3);
+    if (!rc && q->have_set1) rc = q->alloc(&q->set1.rec_sens, (size_t)q->h.cap_rec * 3);
     if (rc) return rc;
     WQ_CK(cudaMemset(dA, 0, 4 * 3 * n * sizeof(double)));
     for (int f = 0; f < 4; ++f) q->h.F[f].dA = dA + (size_t)f * 3 * n;
