@@ -849,7 +849,7 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
  * becomes "curr" (wave_front.cc:184-216; reflecting neighbours are read
  * from their shadow slots), the rotation, AB3 and update of the new front
  * (wave_queue.cc:162-183), and the reflection decision of the next step. */
-__global__ void __launch_bounds__(128) k_advance(__grid_constant__ const QueueDev q, int k) {
+__global__ void __launch_bounds__(128, 5) k_advance(__grid_constant__ const QueueDev q, int k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) *q.n_cand = 0;
     if (i >= q.n) return;
@@ -861,89 +861,175 @@ __global__ void __launch_bounds__(128) k_advance(__grid_constant__ const QueueDe
     const int naz = q.naz;
     const int d = i / naz;
     const size_t stride = shadow_stride(q);
+    /* Reads go through the read-only path: in this launch no ray reads an
+     * element that another ray writes (neighbours are read only where they
+     * do not reflect, and a reflecting ray's entries come from its shadow
+     * slot), and a ray's own updated counters and phases stay in
+     * registers, so the loads need not wait behind the stores. */
     RayS y0, y1, y2, y3;
-    if (flag_in[i]) {
+    const int max_de = q.nde - 1;
+    /* one round of loads: this ray on the three fronts and its flag, and
+     * the rows d-2 .. d+2 that detect_caustics and find_edges may read
+     * (rows clamped to the fan; a clamped row is never used) */
+    const bool refl = __ldg(flag_in + i) != 0;
+    load_ray_ro(*R.V, i, y0);
+    load_ray_ro(*R.C, i, y1);
+    load_ray_ro(*R.X, i, y2);
+    int32_t sf = __ldg(R.X->surface + i);
+    int32_t bt = __ldg(R.X->bottom + i);
+    int32_t cs = __ldg(R.X->caustic + i);
+    int32_t up = __ldg(R.X->upper + i);
+    int32_t lo = __ldg(R.X->lower + i);
+    int jrow[4];
+    jrow[0] = i + (max(d - 2, 0) - d) * naz;
+    jrow[1] = i + (max(d - 1, 0) - d) * naz;
+    jrow[2] = i + (min(d + 1, max_de) - d) * naz;
+    jrow[3] = i + (min(d + 2, max_de) - d) * naz;
+    bool fl[4];
+    double rr[4], nn[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        fl[t] = __ldg(flag_in + jrow[t]) != 0;
+        rr[t] = __ldg(R.X->pos[0] + jrow[t]);
+        nn[t] = __ldg(R.X->nd[0] + jrow[t]);
+    }
+    const double c_below = __ldg(R.C->pos[0] + jrow[1]);
+    const int32_t sf_below = __ldg(R.X->surface + jrow[1]);
+    const int32_t bt_below = __ldg(R.X->bottom + jrow[1]);
+    const double x_below = rr[1];
+    /* reflecting neighbours: their post-reflection entries */
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        if (fl[t]) {
+            const double* shj = q.shadow + (size_t)__ldg(q.shadow_slot + jrow[t]) * stride;
+            rr[t] = __ldg(shj + 34);
+            nn[t] = __ldg(shj + 34 + 6);
+        }
+    }
+    const double* sh = nullptr;
+    bool fold_hit = false, vtx_up = false, vtx_lo = false;
+    if (refl) {
         /* commit the reflected ray (reflection_copy into prev, curr, next) */
-        const int32_t w = q.shadow_slot[i];
-        const double* sh = q.shadow + (size_t)w * stride;
+        const int32_t w = __ldg(q.shadow_slot + i);
+        sh = q.shadow + (size_t)w * stride;
         ray_from(sh, y0);
         ray_from(sh + 17, y1);
         ray_from(sh + 34, y2);
         copy_ray(*R.V, i, y0);
         copy_ray(*R.C, i, y1);
         copy_ray(*R.X, i, y2);
-        for (int f = 0; f < q.nf; ++f) {
-            R.X->atten[(size_t)f * q.n + i] = sh[51 + f];
-            R.X->phase[(size_t)f * q.n + i] = sh[51 + q.nf + f];
-        }
-        const int32_t sf = q.shadow_cnt[3 * (size_t)w], bt = q.shadow_cnt[3 * (size_t)w + 1];
+        sf = __ldg(q.shadow_cnt + 3 * (size_t)w);
+        bt = __ldg(q.shadow_cnt + 3 * (size_t)w + 1);
+        cs = __ldg(q.shadow_cnt + 3 * (size_t)w + 2);
         R.V->surface[i] = R.C->surface[i] = R.X->surface[i] = sf;
         R.V->bottom[i] = R.C->bottom[i] = R.X->bottom[i] = bt;
-        R.X->caustic[i] = q.shadow_cnt[3 * (size_t)w + 2];
+        R.X->caustic[i] = cs;
     } else {
-        load_ray(*R.V, i, y0);
-        load_ray(*R.C, i, y1);
-        load_ray(*R.X, i, y2);
         /* detect_caustics of the neighbour below (wave_queue.cc:274-292) */
-        if (d >= 1 && !flag_in[i - naz]) {
-            const int j = i - naz;
-            const double A = y1.pos[0], B = R.C->pos[0][j];
-            const double Cc = y2.pos[0], D = R.X->pos[0][j];
-            const bool fold = (R.X->surface[i] == R.X->surface[j]) && (R.X->bottom[i] == R.X->bottom[j]);
+        if (d >= 1 && !fl[1]) {
+            const double A = y1.pos[0], B = c_below;
+            const double Cc = y2.pos[0], D = x_below;
+            const bool fold = (sf == sf_below) && (bt == bt_below);
             if ((Cc - D) * (A - B) < 0 && fold) {
-                R.X->caustic[i] += 1;
-                for (int f = 0; f < q.nf; ++f) R.X->phase[(size_t)f * q.n + i] -= M_PI_2;
+                fold_hit = true;
+                cs += 1;
             }
         }
         /* detect_vertices (wave_queue.cc:261-269) */
         const double L = y1.nd[0];
         const double Rn = y2.nd[0];
         if (L * Rn < 0.0 && Rn < 0.0) {
-            R.X->upper[i] += 1;
+            vtx_up = true;
+            up += 1;
         } else if (L * Rn < 0.0 && 0.0 < Rn) {
-            R.X->lower[i] += 1;
+            vtx_lo = true;
+            lo += 1;
         }
     }
-    /* find_edges on the post-reflection "next" front */
+    /* find_edges on the post-reflection "next" front (wave_front.cc:
+     * 184-216): a row is an extremum when its rho is below or above both
+     * neighbour rows */
+    bool edge;
     {
-        const int max_de = q.nde - 1;
-        auto rho_at = [&](int j) {
-            return flag_in[j] ? q.shadow[(size_t)q.shadow_slot[j] * stride + 34] : R.X->pos[0][j];
-        };
-        auto ndr_at = [&](int j) {
-            return flag_in[j] ? q.shadow[(size_t)q.shadow_slot[j] * stride + 34 + 6] : R.X->nd[0][j];
-        };
-        auto extremum = [&](int dd) -> bool {
-            if (dd < 1 || dd > max_de - 1) return false;
-            const int j = i + (dd - d) * naz;
-            const double r0 = rho_at(j), rp = rho_at(j + naz), rm = rho_at(j - naz);
+        auto ext = [](double r0, double rp, double rm) {
             return (r0 < rp && r0 < rm) || (r0 > rp && r0 > rm);
         };
-        bool edge = (d == 0) || (d == max_de) || extremum(d);
-        if (!edge && extremum(d + 1)) {
-            const double n0 = ndr_at(i + naz);
-            if (fabs(n0 - y2.nd[0]) > fabs(n0 - ndr_at(i + 2 * naz))) edge = true;
+        const double r_here = y2.pos[0], n_here = y2.nd[0];
+        const bool ext_d = d >= 1 && d <= max_de - 1 && ext(r_here, rr[2], rr[1]);
+        const bool ext_up = d + 1 >= 1 && d + 1 <= max_de - 1 && ext(rr[2], rr[3], r_here);
+        const bool ext_dn = d - 1 >= 1 && d - 1 <= max_de - 1 && ext(rr[1], r_here, rr[0]);
+        edge = (d == 0) || (d == max_de) || ext_d;
+        if (!edge && ext_up) {
+            const double n0 = nn[2];
+            if (fabs(n0 - n_here) > fabs(n0 - nn[3])) edge = true;
         }
-        if (!edge && extremum(d - 1)) {
-            const double n0 = ndr_at(i - naz);
-            if (!(fabs(n0 - ndr_at(i - 2 * naz)) > fabs(n0 - y2.nd[0]))) edge = true;
+        if (!edge && ext_dn) {
+            const double n0 = nn[1];
+            if (!(fabs(n0 - nn[0]) > fabs(n0 - n_here))) edge = true;
         }
-        R.X->on_edge[i] = edge ? 1 : 0;
     }
-    /* rotate and take the AB3 step */
+    const double plen_x = __ldg(R.X->plen + i);
+    /* rotate and take the AB3 step; wave_front::update of the new front */
     ab3(q.dt, y0, y1, y2, y3);
-    update_main(q, *R.P, i, y3, true, R.X);
-    R.P->plen[i] = y3.dist + R.X->plen[i];
-    R.P->surface[i] = R.X->surface[i];
-    R.P->bottom[i] = R.X->bottom[i];
-    R.P->upper[i] = R.X->upper[i];
-    R.P->lower[i] = R.X->lower[i];
-    R.P->caustic[i] = R.X->caustic[i];
+    profile_at(q, y3.pos, &y3.c, y3.sg);
+    double st;
+    ray_derivs(y3.c, y3.sg[0], y3.sg[1], y3.sg[2], y3.pos, y3.nd, y3.pg, y3.ng, &st);
+    const uint8_t f_next = reflect_decision(q, y3.pos, y2.nd);
+    /* stores */
+    if (fold_hit) R.X->caustic[i] = cs;
+    if (vtx_up) R.X->upper[i] = up;
+    if (vtx_lo) R.X->lower[i] = lo;
+    R.X->on_edge[i] = edge ? 1 : 0;
+    const FrontPtrs& P = *R.P;
+    copy_ray(P, i, y3);
+    P.cpa[0][i] = y3.pos[0];
+    P.cpa[1][i] = y3.pos[1];
+    P.cpa[2][i] = y3.pos[2];
+    P.cpa[3][i] = st;
+    P.plen[i] = y3.dist + plen_x;
+    P.surface[i] = sf;
+    P.bottom[i] = bt;
+    P.upper[i] = up;
+    P.lower[i] = lo;
+    P.caustic[i] = cs;
     if (q.sens)
-        for (int j = 0; j < 3; ++j) R.P->dA[(size_t)j * q.n + i] = R.X->dA[(size_t)j * q.n + i];
-    const uint8_t f = reflect_decision(q, y3.pos, y2.nd);
-    flag_out[i] = f;
-    if (f) work_append(q, (int)((s + 1) & 1), f, i);
+        for (int j = 0; j < 3; ++j) P.dA[(size_t)j * q.n + i] = __ldg(R.X->dA + (size_t)j * q.n + i);
+    /* attenuation (attenuation_thorp.cc:14-36 / attenuation_constant.cc:
+     * 14-25) added to the next front's, phase carried over; the next
+     * front's own entries take the reflection's values or the caustic's
+     * phase shift first */
+    const double alt = y3.pos[0] - q.R;
+#pragma unroll 5
+    for (int f = 0; f < q.nf; ++f) {
+        const size_t o = (size_t)f * q.n + i;
+        double ax, px;
+        if (refl) {
+            ax = __ldg(sh + 51 + f);
+            px = __ldg(sh + 51 + q.nf + f);
+            R.X->atten[o] = ax;
+            R.X->phase[o] = px;
+        } else {
+            ax = __ldg(R.X->atten + o);
+            px = __ldg(R.X->phase + o);
+            if (fold_hit) {
+                px -= M_PI_2;
+                R.X->phase[o] = px;
+            }
+        }
+        double a;
+        if (q.oc.prof.atten == WQ3D_ATTEN_CONSTANT) {
+            a = q.oc.prof.atten_coef * y3.dist * q.freq[f];
+        } else {
+            a = y3.dist * q.alpha[f] * (1.0 + 5.88264e-6 * alt);
+        }
+        a += ax;
+        double p = 0.0;
+        p += px;
+        P.atten[o] = a;
+        P.phase[o] = p;
+    }
+    flag_out[i] = f_next;
+    if (f_next) work_append(q, (int)((s + 1) & 1), f_next, i);
 }
 
 }  // namespace WQ3D_KERNEL_NS
