@@ -1465,6 +1465,8 @@ namespace {
  * a rounding-sensitive recurrence (cell distances, the running intensity
  * and its threshold test) is formed in the reference's sequential order,
  * so results equal the one-thread-per-eigenray evaluation. */
+constexpr int EIG_FG = 8; /* frequencies per pass of a walk chunk's Gaussian terms */
+
 struct WarpBuild {
     const QueueDev* q;
     const FrontPtrs* pV;
@@ -1473,6 +1475,7 @@ struct WarpBuild {
     const double* spread2;   /* [nf] for this target */
     int lane;
     double Ilo, Ihi;         /* running intensity of frequencies lane, lane+32 */
+    double (*sg)[EIG_FG + 1]; /* this warp's [cell][frequency] Gaussian terms */
 
     __device__ double fdist(const FrontPtrs& f, int d1, int a1, int d2, int a2) const {
         const int i = d1 * q->naz + a1, j = d2 * q->naz + a2;
@@ -1500,6 +1503,50 @@ struct WarpBuild {
         }
     }
     __device__ double I0() const { return __shfl_sync(0xffffffffu, Ilo, 0); }
+
+    /* The lowest frequency's running intensity over cells 0..ncell-1 (lane
+     * k holds cell k's term g0), added in cell order, and the reference's
+     * threshold test after each cell (new / old < 1.002305238).  Returns
+     * the first cell that passes it, or -1.  The sums are sequential; the
+     * divisions of the tests are not, so they run on all lanes at once. */
+    __device__ int threshold_cell(int ncell, double g0) const {
+        double i0 = I0();
+        double my_new = 1.0, my_old = 1.0;
+        for (int k = 0; k < ncell; ++k) {
+            const double old = i0;
+            i0 += __shfl_sync(0xffffffffu, g0, k);
+            if (lane == k) {
+                my_new = i0;
+                my_old = old;
+            }
+        }
+        const unsigned hit = __ballot_sync(0xffffffffu, lane < ncell && my_new / my_old < 1.002305238);
+        return hit ? __ffs(hit) - 1 : -1;
+    }
+
+    /* acc() of cells 0..ncell-1 in cell order, for every frequency: lane k
+     * computes cell k's Gaussian terms (EIG_FG frequencies per pass), then
+     * the lane that owns a frequency adds them up in cell order */
+    __device__ void acc_cells(int ncell, double cd, double cw, double nm) {
+        const int nf = q->nf;
+        for (int f0 = 0; f0 < nf; f0 += EIG_FG) {
+            const int nfg = min(EIG_FG, nf - f0);
+            if (lane < ncell)
+                for (int j = 0; j < nfg; ++j) sg[lane][j] = gauss(cd, cw, nm, f0 + j);
+            __syncwarp();
+            if (lane >= f0 && lane < f0 + nfg) {
+                double I = Ilo;
+                for (int k = 0; k < ncell; ++k) I = I + sg[k][lane - f0];
+                Ilo = I;
+            }
+            if (lane + 32 >= f0 && lane + 32 < f0 + nfg) {
+                double I = Ihi;
+                for (int k = 0; k < ncell; ++k) I = I + sg[k][lane + 32 - f0];
+                Ihi = I;
+            }
+            __syncwarp();
+        }
+    }
 
     /* spreading_hybrid_gaussian.cc:430-495 */
     __device__ double width_de(int d, int a, const double* offset) const {
@@ -1600,24 +1647,14 @@ struct WarpBuild {
         }
         /* threshold scan on the lowest frequency, in order */
         const double g0 = (lane < nend) ? gauss(my_cd, my_cw, my_nm, 0) : 0.0;
-        double i0 = I0();
-        int kstar = nend - 1;
-        for (int k = 0; k < nend; ++k) {
-            const double old = i0;
-            i0 += __shfl_sync(0xffffffffu, g0, k);
-            if (i0 / old < 1.002305238) {
-                kstar = k;
-                stop = true;
-                break;
-            }
+        int kstar = threshold_cell(nend, g0);
+        if (kstar >= 0) {
+            stop = true;
+        } else {
+            kstar = nend - 1;
         }
         /* accumulate every frequency over cells 0..kstar, in order */
-        for (int k = 0; k <= kstar; ++k) {
-            const double cd = __shfl_sync(0xffffffffu, my_cd, k);
-            const double cw = __shfl_sync(0xffffffffu, my_cw, k);
-            const double nm = __shfl_sync(0xffffffffu, my_nm, k);
-            acc(cd, cw, nm, false);
-        }
+        acc_cells(kstar + 1, my_cd, my_cw, my_nm);
         return stop;
     }
 
@@ -1786,24 +1823,10 @@ struct WarpBuild {
             }
         }
         const double g0 = (lane < ncell) ? gauss(my_cd, my_cw, my_nm, 0) : 0.0;
-        double i0 = I0();
-        int kstar = ncell - 1;
-        bool stop = false;
-        for (int k = 0; k < ncell; ++k) {
-            const double old = i0;
-            i0 += __shfl_sync(0xffffffffu, g0, k);
-            if (i0 / old < 1.002305238) {
-                kstar = k;
-                stop = true;
-                break;
-            }
-        }
-        for (int k = 0; k <= kstar; ++k) {
-            const double cd = __shfl_sync(0xffffffffu, my_cd, k);
-            const double cw = __shfl_sync(0xffffffffu, my_cw, k);
-            const double nm = __shfl_sync(0xffffffffu, my_nm, k);
-            acc(cd, cw, nm, false);
-        }
+        int kstar = threshold_cell(ncell, g0);
+        const bool stop = kstar >= 0;
+        if (!stop) kstar = ncell - 1;
+        acc_cells(kstar + 1, my_cd, my_cw, my_nm);
         if (stop) kstop = kstar;
         return stop;
     }
@@ -1983,6 +2006,7 @@ constexpr int EIG_WARPS = 4;
 __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ const QueueDev q, int k) {
     __shared__ double s_cube[EIG_WARPS][27];
     __shared__ double s_ang[EIG_WARPS][2][27];
+    __shared__ double s_g[EIG_WARPS][32][EIG_FG + 1];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t s = *q.d_base + k + 1;
@@ -1994,6 +2018,7 @@ __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ c
     B.pC = &q.F[(s + 2) & 3];
     B.pX = &q.F[(s + 3) & 3];
     B.lane = lane;
+    B.sg = s_g[warp];
     const FrontPtrs& V = *B.pV;
     const FrontPtrs& C = *B.pC;
     const FrontPtrs& X = *B.pX;
