@@ -486,7 +486,7 @@ struct wq3d_queue {
                 else
                     k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d, k);
                 if (ev) cudaEventRecord(ev[3], stream);
-                k_eigenray<<<148, 128, 0, stream>>>(d, k);
+                k_eigenray<<<EIG_BLOCKS, 128, 0, stream>>>(d, k);
                 launches += 2;
             } else if (ev) {
                 cudaEventRecord(ev[3], stream);

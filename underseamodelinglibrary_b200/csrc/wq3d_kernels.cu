@@ -1896,27 +1896,26 @@ __device__ __forceinline__ double norm2(const double* g) {
     return sqrt(t);
 }
 
-/* wave_queue::compute_offsets (wave_queue.cc:708-924) */
+/* wave_queue::compute_offsets (wave_queue.cc:708-924).  Called by a whole
+ * warp: lanes 0-8 test the 3x3 neighbours' stability at once. */
 __device__ void compute_offsets(const QueueDev& q, const FrontPtrs& V, const FrontPtrs& C,
                                 const FrontPtrs& X, int t, int de0, int az0,
                                 const double cube[3][3][3], const double* delta,
                                 double* offset, double* distance) {
-    bool unstable = false;
     const int ic = de0 * q.naz + az0;
-    const int surface = C.surface[ic], bottom = C.bottom[ic], caustic = C.caustic[ic];
-    for (int nd_ = 0; nd_ < 3 && !unstable; ++nd_) {
-        const int d = de0 + nd_ - 1;
-        for (int na = 0; na < 3 && !unstable; ++na) {
-            const int a = wrap_az(q, az0, na);
-            const int i = d * q.naz + a;
-            if (V.surface[i] != surface || C.surface[i] != surface || X.surface[i] != surface ||
-                V.bottom[i] != bottom || C.bottom[i] != bottom || X.bottom[i] != bottom ||
-                V.caustic[i] != caustic || C.caustic[i] != caustic || X.caustic[i] != caustic ||
-                V.on_edge[i]) {
-                unstable = true;
-            }
+    bool bad = false;
+    {
+        const int lane = threadIdx.x & 31;
+        if (lane < 9) {
+            const int surface = C.surface[ic], bottom = C.bottom[ic], caustic = C.caustic[ic];
+            const int i = (de0 + lane / 3 - 1) * q.naz + wrap_az(q, az0, lane % 3);
+            bad = V.surface[i] != surface || C.surface[i] != surface || X.surface[i] != surface ||
+                  V.bottom[i] != bottom || C.bottom[i] != bottom || X.bottom[i] != bottom ||
+                  V.caustic[i] != caustic || C.caustic[i] != caustic || X.caustic[i] != caustic ||
+                  V.on_edge[i];
         }
     }
+    bool unstable = __any_sync(0xffffffffu, bad);
     double center, g[3], h[3][3], inv[3][3];
     make_taylor_coeff(cube, delta, center, g, h);
     /* kept: hessian(2,1)*hessian(2,0) in the last cofactor (wave_queue.cc:762-763) */
