@@ -450,6 +450,9 @@ struct wq3d_queue {
         const dim3 blk(128);
         const dim3 grd((n + 127) / 128);
         const int rgrid = std::max(1, std::min(4 * 148, (n + 63) / 64));
+        /* eigenray candidates grow with the fan: one block per SM for small
+         * fans, up to EIG_BLOCKS */
+        const int eig_blocks = std::min(EIG_BLOCKS, std::max(148, (n + 255) / 256));
         if (timing) tail = false;
         if (timing) cudaEventRecord(events[7 * K], stream);
         k_reflect_fn<<<rgrid, 64, 0, stream>>>(d, 0);
@@ -486,7 +489,7 @@ struct wq3d_queue {
                 else
                     k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d, k);
                 if (ev) cudaEventRecord(ev[3], stream);
-                k_eigenray<<<EIG_BLOCKS, 128, 0, stream>>>(d, k);
+                k_eigenray<<<eig_blocks, 128, 0, stream>>>(d, k);
                 launches += 2;
             } else if (ev) {
                 cudaEventRecord(ev[3], stream);

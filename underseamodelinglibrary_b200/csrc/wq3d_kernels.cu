@@ -849,7 +849,15 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
  * becomes "curr" (wave_front.cc:184-216; reflecting neighbours are read
  * from their shadow slots), the rotation, AB3 and update of the new front
  * (wave_queue.cc:162-183), and the reflection decision of the next step. */
-__global__ void __launch_bounds__(128, 5) k_advance(__grid_constant__ const QueueDev q, int k) {
+/* five blocks per SM for the analytic build (96 registers, spills to L1
+ * that cost less than the lost occupancy); the gridded build calls the
+ * out-of-line grid interpolation and keeps its full register budget */
+#if WQ3D_WITH_GRID
+#define WQ_ADVANCE_BOUNDS __launch_bounds__(128)
+#else
+#define WQ_ADVANCE_BOUNDS __launch_bounds__(128, 5)
+#endif
+__global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, int k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) *q.n_cand = 0;
     if (i >= q.n) return;
@@ -1242,6 +1250,16 @@ __device__ __noinline__ void cpa_finish(const QueueDev& q, const FrontPtrs& V, c
     }
 }
 
+/* order-preserving keys of floats, for the warp's unsigned min / max
+ * reductions (non-NaN values; -0 orders below +0) */
+__device__ __forceinline__ unsigned f2key(float f) {
+    const unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key2f(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
 /* whether every ray of the patch rejects a target on one comparison */
 __device__ __forceinline__ bool patch_rejects(const TgtW& g, const float* lo, const float* hi,
                                               const float* W, float c0) {
@@ -1326,20 +1344,15 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(__grid_constant__ co
      * low / high of dxc, [16..23] / [24..31] of dvc */
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-        float l1 = active ? dxc[m] : INFINITY, h1 = active ? dxc[m] : -INFINITY;
-        float l2 = active ? dvc[m] : INFINITY, h2 = active ? dvc[m] : -INFINITY;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            l1 = fminf(l1, __shfl_xor_sync(0xffffffffu, l1, o));
-            h1 = fmaxf(h1, __shfl_xor_sync(0xffffffffu, h1, o));
-            l2 = fminf(l2, __shfl_xor_sync(0xffffffffu, l2, o));
-            h2 = fmaxf(h2, __shfl_xor_sync(0xffffffffu, h2, o));
-        }
+        const unsigned l1 = __reduce_min_sync(0xffffffffu, f2key(active ? dxc[m] : INFINITY));
+        const unsigned h1 = __reduce_max_sync(0xffffffffu, f2key(active ? dxc[m] : -INFINITY));
+        const unsigned l2 = __reduce_min_sync(0xffffffffu, f2key(active ? dvc[m] : INFINITY));
+        const unsigned h2 = __reduce_max_sync(0xffffffffu, f2key(active ? dvc[m] : -INFINITY));
         if (lane == 0) {
-            red[w][m] = l1;
-            red[w][8 + m] = h1;
-            red[w][16 + m] = l2;
-            red[w][24 + m] = h2;
+            red[w][m] = key2f(l1);
+            red[w][8 + m] = key2f(h1);
+            red[w][16 + m] = key2f(l2);
+            red[w][24 + m] = key2f(h2);
         }
     }
     __syncthreads();
@@ -1377,11 +1390,10 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(__grid_constant__ co
 #pragma unroll
             for (int m = 0; m < 8; ++m) W[m] = fmaxf(W[m], fabsf(g.w[m]));
         }
+        /* W >= 0: its bit patterns order as unsigned integers */
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) W[m] = fmaxf(W[m], __shfl_xor_sync(0xffffffffu, W[m], o));
-        }
+        for (int m = 0; m < 8; ++m)
+            W[m] = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(W[m])));
         if (lane == 0)
             for (int m = 0; m < 8; ++m) wmax[w][m] = W[m];
         if (threadIdx.x == 0) nsurv = 0;
