@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-munk-cpu", action="store_true",
+                    help="skip the oracle's full run of the Munk workload (a few seconds)")
     ap.add_argument("--no-gradients", action="store_true", help="skip the gradient workload")
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched gridded workload (0 skips it)")
@@ -313,6 +315,7 @@ def engine_arm(args, rank, world, dist):
     if not args.no_gradients:
         out["gradients"] = gradient_arm()
     out["std14"] = std14_arm()
+    out["munk_flat"] = munk_arm()
     return out
 
 
@@ -354,6 +357,32 @@ def std14_arm():
         rows.append(row)
     return {"workload": "std14_cmp_speed_181x25_801steps_250Hz", "rays": 181 * 25, "steps": 801,
             "rows": rows}
+
+
+def munk_arm():
+    """The plain FP64 workload: Munk profile, 5000 m flat bottom, source
+    1000 m, 10 Hz, 181 x 37 rays, 600 steps of 0.1 s, 100 targets at 500 m.
+    Device time of one propagation (CUDA-graph replay, best of 3), FP32C
+    and FP64; the oracle's time for the same run is in cpu_baseline."""
+    import underseamodelinglibrary_b200 as u
+    from underseamodelinglibrary_b200 import scenarios as S
+    from underseamodelinglibrary_b200 import _abi
+    sc = S.munk_flat()
+    out = {"workload": sc["name"] + "_100tgt_600steps_10Hz", "rays": sc["de"].size() * sc["az"].size()}
+    for name, prec in (("fp32c", _abi.FP32C), ("fp64", _abi.FP64)):
+        best = None
+        for _ in range(3):
+            q = S.build_queue(sc, u.wave_queue, precision=prec)
+            q.timing(reset=True)
+            q.run(sc["time_max"])
+            ms = q.timing()["total_ms"]
+            n_steps, n_eig = q.steps(), len(q.take_eigenrays())
+            best = ms if best is None else min(best, ms)
+        out[name + "_ms"] = best
+        out[name + "_ray_steps_per_s"] = out["rays"] * n_steps / (best / 1000.0)
+        out[name + "_eigenrays"] = n_eig
+    out["steps"] = n_steps
+    return out
 
 
 def gradient_arm():
@@ -463,12 +492,21 @@ def cpu_run(sc, nthreads):
 
 
 def cpu_baseline(args):
+    from underseamodelinglibrary_b200 import scenarios as S
     sc = cpu_sample_scenario(args.cpu_sample_steps)
     v, dt, n = cpu_run(sc, 1)
-    return {"value": v, "unit": "ray-steps/s", "cores": 1, "kind": "port",
-            "sample": "oracle (CPU restatement of the reference wave_queue), 1 thread: full 1801-ray "
-                      "D/E fan x every 16th AZ column (6 columns), all 1024 targets, first %d of 800 "
-                      "steps; %.1f s" % (n, dt)}
+    out = {"value": v, "unit": "ray-steps/s", "cores": 1, "kind": "port",
+           "sample": "oracle (CPU restatement of the reference wave_queue), 1 thread: full 1801-ray "
+                     "D/E fan x every 16th AZ column (6 columns), all 1024 targets, first %d of 800 "
+                     "steps; %.1f s" % (n, dt)}
+    if not args.no_munk_cpu:
+        # the whole plain FP64 Munk workload (181 x 37 rays, 600 steps, 100
+        # targets), 1 thread
+        m = S.munk_flat()
+        mv, mdt, mn = cpu_run(m, 1)
+        out["munk_flat"] = {"seconds": mdt, "ray_steps_per_s": mv, "steps": mn, "cores": 1,
+                            "kind": "port"}
+    return out
 
 
 def reference_arm(args, rank):
