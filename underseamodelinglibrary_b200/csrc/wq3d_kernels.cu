@@ -1260,20 +1260,24 @@ __device__ __forceinline__ float key2f(unsigned k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
-/* whether every ray of the patch rejects a target on one comparison */
+/* whether every ray of the patch rejects a target on one comparison.  In
+ * FP32: each product and the 8-term sums carry at most about 8u of mag
+ * (u = 2^-24), the weight sum about 9u of wm, the last three additions
+ * about 3u of mag + c0; the 14u, 43u (41u of the per-ray screen plus its
+ * own rounding) and 1.0003 factors cover them, so a rejection implies that
+ * every ray's FP32 screen rejects the pair. */
 __device__ __forceinline__ bool patch_rejects(const TgtW& g, const float* lo, const float* hi,
                                               const float* W, float c0) {
-    double ub = 0.0, mag = 0.0, wm = 0.0;
+    float ub = 0.0f, mag = 0.0f, wm = 0.0f;
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-        const double w = (double)g.w[m];
-        const double a = w * (double)lo[m], b = w * (double)hi[m];
-        ub += fmax(a, b);
-        mag += fmax(fabs(a), fabs(b));
-        wm += (double)W[m] * fmax(fabs((double)lo[m]), fabs((double)hi[m]));
+        const float a = g.w[m] * lo[m], b = g.w[m] * hi[m];
+        ub += fmaxf(a, b);
+        mag += fmaxf(fabsf(a), fabsf(b));
+        wm += W[m] * fmaxf(fabsf(lo[m]), fabsf(hi[m]));
     }
-    const double u = 5.9604644775390625e-8; /* 2^-24 */
-    return ub + 1e-15 * mag + 41.0 * u * wm + 1.0001 * (double)c0 < 0.0;
+    const float u = 5.9604645e-8f; /* 2^-24 */
+    return ub + (14.0f * u) * mag + (43.0f * u) * wm + 1.0003f * c0 < 0.0f;
 }
 }  // namespace
 
