@@ -159,8 +159,8 @@ WQ3D_DECLARE_STEP_KERNELS
 __global__ void k_volume(__grid_constant__ const QueueDev q, int k);
 __global__ void k_cpa(__grid_constant__ const QueueDev q, int k);
 __global__ void k_cpa_f32(__grid_constant__ const QueueDev q, int k);
-/* k_eigenray blocks (4 warps each, one candidate per warp at a time):
- * four per SM, so a step's candidates usually all run at once */
+/* k_eigenray blocks (4 warps each, one candidate per warp pair at a
+ * time): four per SM, so a step's candidates usually all run at once */
 constexpr int EIG_BLOCKS = 4 * 148;
 __global__ void k_eigenray(__grid_constant__ const QueueDev q, int k);
 __global__ void k_sound_speed(OceanDev oc, double R, int n, const double* rho,

@@ -1475,7 +1475,8 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(__grid_constant__ co
 /* ------------------------------------------------------------------ */
 namespace {
 
-/* One warp builds one eigenray.  Lanes share the parallel parts (the 27
+/* One warp builds one eigenray (with a second warp for the AZ walks of
+ * hybrid Gaussian spreading).  Lanes share the parallel parts (the 27
  * distance2 values, the 54 direction angles, the cell widths and Gaussian
  * terms of the beam walks, the per-frequency sums); every value that feeds
  * a rounding-sensitive recurrence (cell distances, the running intensity
@@ -2018,12 +2019,26 @@ __device__ void compute_offsets(const QueueDev& q, const FrontPtrs& V, const Fro
 
 constexpr int EIG_WARPS = 4;
 
+/* the two warps of pair p (warps 2p, 2p+1 of the block) meet here */
+__device__ __forceinline__ void pair_sync(int pair) {
+    static_assert(EIG_WARPS == 4, "two warp pairs per block: named barriers 1 and 2");
+    if (pair == 0)
+        asm volatile("bar.sync 1, 64;" ::: "memory");
+    else
+        asm volatile("bar.sync 2, 64;" ::: "memory");
+}
+
 __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ const QueueDev q, int k) {
     __shared__ double s_cube[EIG_WARPS][27];
     __shared__ double s_ang[EIG_WARPS][2][27];
     __shared__ double s_g[EIG_WARPS][32][EIG_FG + 1];
+    __shared__ double s_az[EIG_WARPS / 2][64];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    /* a warp pair per candidate: with hybrid Gaussian spreading the even
+     * warp runs the D/E walks and the odd warp the AZ walks, which are
+     * independent sums; the odd warp hands its sums over and moves on */
+    const int pair = warp >> 1, half = warp & 1;
     const int64_t s = *q.d_base + k + 1;
     const double time = q.d_times[k + 1];
     const uint32_t ncand = min(*q.n_cand, q.cap_cand);
@@ -2038,8 +2053,8 @@ __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ c
     const FrontPtrs& C = *B.pC;
     const FrontPtrs& X = *B.pX;
     double (*cube)[3][3] = reinterpret_cast<double (*)[3][3]>(s_cube[warp]);
-    const uint32_t nwarps = gridDim.x * EIG_WARPS;
-    for (uint32_t c = blockIdx.x * EIG_WARPS + warp; c < ncand; c += nwarps) {
+    const uint32_t npairs = gridDim.x * (EIG_WARPS / 2);
+    for (uint32_t c = blockIdx.x * (EIG_WARPS / 2) + pair; c < ncand; c += npairs) {
         __syncwarp();
         const int t = (int)q.cand[2 * c];
         const int i = (int)q.cand[2 * c + 1];
@@ -2076,20 +2091,36 @@ __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ c
                 }
                 no[2] = offset[2] + B.az_inc(a);
             }
-            B.Ilo = B.Ihi = 0.0;
-            B.intensity_de(de0, a, no, distance);
-            const double de_lo = B.Ilo, de_hi = B.Ihi;
-            no[2] = offset[2];
-            int d = de0;
-            if (offset[1] < 0.0 && !C.on_edge[i - q.naz]) {
-                d = de0 - 1;
-                no[1] = offset[1] + B.de_inc(d);
+            double de_lo = 0.0, de_hi = 0.0;
+            if (half == 0) {
+                B.Ilo = B.Ihi = 0.0;
+                B.intensity_de(de0, a, no, distance);
+                de_lo = B.Ilo;
+                de_hi = B.Ihi;
+            } else {
+                no[2] = offset[2];
+                int d = de0;
+                if (offset[1] < 0.0 && !C.on_edge[i - q.naz]) {
+                    d = de0 - 1;
+                    no[1] = offset[1] + B.de_inc(d);
+                }
+                B.Ilo = B.Ihi = 0.0;
+                B.intensity_az(d, az0, no, distance);
+                s_az[pair][lane] = B.Ilo;
+                s_az[pair][32 + lane] = B.Ihi;
             }
-            B.Ilo = B.Ihi = 0.0;
-            B.intensity_az(d, az0, no, distance);
-            si_lo = de_lo * B.Ilo;
-            si_hi = de_hi * B.Ihi;
+            /* both warps pass both barriers once per candidate */
+            pair_sync(pair);
+            if (half == 1) {
+                pair_sync(pair);
+                continue;
+            }
+            const double az_lo = s_az[pair][lane], az_hi = s_az[pair][32 + lane];
+            pair_sync(pair);
+            si_lo = de_lo * az_lo;
+            si_hi = de_hi * az_hi;
         } else {
+            if (half == 1) continue;
             /* spreading_ray.cc:47-133; an AZ wrap below index 0 is wrapped */
             int d = de0, a = az0;
             if (offset[1] < 0.0) --d;
