@@ -16,7 +16,7 @@ from .ocean import (attenuation_thorp, attenuation_constant, profile_linear,
                     boundary_slope, ocean_model, data_grid, profile_grid, boundary_grid,
                     volume_flat)
 from .waveq3d import (wave_queue, eigenray_listener, reflection_listener,
-                      eigenray_model, run_batch)
+                      eigenray_model, eigenray_list, run_batch)
 from .eigenrays import eigenray_collection
 from .eigenverbs import eigenverb_model, eigenverb_listener, eigenverb_collection
 
@@ -32,7 +32,7 @@ __all__ = [
     "reflect_loss_constant", "reflect_loss_rayleigh", "reflect_loss_eckart",
     "boundary_flat", "boundary_slope", "ocean_model", "data_grid", "profile_grid",
     "boundary_grid", "volume_flat", "wave_queue", "run_batch",
-    "eigenray_listener", "reflection_listener", "eigenray_model",
+    "eigenray_listener", "reflection_listener", "eigenray_model", "eigenray_list",
     "eigenray_collection", "eigenverb_model", "eigenverb_listener", "eigenverb_collection",
     "load_engine", "EngineError", "LIB_PATH",
 ]

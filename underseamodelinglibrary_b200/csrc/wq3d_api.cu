@@ -1248,6 +1248,12 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     q->events.resize(7 * (size_t)q->chunk + 2);
     for (auto& ev : q->events)
         if (cudaEventCreate(&ev) != cudaSuccess) return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+    /* set-up a run would otherwise do on its first chunks: the second
+     * result set and the chunk graphs (rebuilt later only if callbacks,
+     * thresholds or sensitivities change the descriptor) */
+    q->ensure_set1();
+    for (int p = 0; p < (q->have_set1 ? 2 : 1); ++p)
+        for (int t = 0; t < 2; ++t) q->build_graph(p, t != 0);
     *out = q;
     return WQ3D_OK;
 }

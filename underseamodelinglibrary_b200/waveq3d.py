@@ -9,6 +9,7 @@ libwq3d.so on the GPU; this module only marshals arguments and dispatches
 listener callbacks in the reference's order.
 """
 import ctypes as C
+from collections.abc import Sequence
 
 import numpy as np
 
@@ -48,6 +49,62 @@ class eigenray_model:
         r.t2 = rec.t2
         r.d_intensity_d_bottom = None
         return r
+
+
+class eigenray_list(Sequence):
+    """The eigenrays of one ``take_eigenrays`` call.  The records are held
+    as numpy arrays (one copy out of the engine); an ``eigenray_model`` is
+    made when an element is read, so a caller that only wants the arrays
+    (``arrays()``) or the count pays no per-ray Python cost."""
+
+    __slots__ = ("_rec", "_inten", "_phase", "_sens", "_freq")
+
+    def __init__(self, rec, inten, phase, sens, freq):
+        self._rec = rec
+        self._inten = inten
+        self._phase = phase
+        self._sens = sens
+        self._freq = freq
+
+    def __len__(self):
+        return len(self._rec)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[j] for j in range(*i.indices(len(self)))]
+        n = len(self._rec)
+        i = int(i)
+        if i < 0:
+            i += n
+        if not 0 <= i < n:
+            raise IndexError("eigenray index out of range")
+        (t, sde, saz, tde, taz, sf, bt, cs, up, lo, t1, t2, de, az, _pad, step) = self._rec[i].item()
+        r = eigenray_model()
+        r.travel_time = t
+        r.intensity = self._inten[i].copy()
+        r.phase = self._phase[i].copy()
+        r.source_de, r.source_az, r.target_de, r.target_az = sde, saz, tde, taz
+        r.surface, r.bottom, r.caustic, r.upper, r.lower = sf, bt, cs, up, lo
+        r.frequencies = self._freq
+        r.step, r.de_index, r.az_index, r.t1, r.t2 = step, de, az, t1, t2
+        r.d_intensity_d_bottom = None if self._sens is None else self._sens[i].copy()
+        return r
+
+    def __iter__(self):
+        for i in range(len(self._rec)):
+            yield self[i]
+
+    def arrays(self):
+        """All eigenrays as columns: the record fields (travel time as
+        "time", CPA bracket as "step", "de", "az"), intensity and phase
+        [n, frequencies] and, with sensitivities on, d_intensity_d_bottom
+        [n, 3]."""
+        out = {name: self._rec[name] for name in self._rec.dtype.names if name != "pad"}
+        out["intensity"] = self._inten
+        out["phase"] = self._phase
+        if self._sens is not None:
+            out["d_intensity_d_bottom"] = self._sens
+        return out
 
 
 class eigenray_listener:
@@ -364,7 +421,8 @@ class wave_queue:
 
     def take_eigenrays(self):
         """Eigenrays found since the last call (when no eigenray listener is
-        registered), as a structured numpy array plus intensity and phase."""
+        registered), in the reference's delivery order, as an eigenray_list
+        (a sequence of eigenray_model)."""
         n = C.c_size_t()
         _abi.check(self._lib, self._lib.wq3d_queue_take_eigenrays(self._q, None, None, None, 0, C.byref(n)))
         cnt = n.value
@@ -378,12 +436,9 @@ class wave_queue:
         phase = np.empty(max(cnt, 1) * nf)
         _abi.check(self._lib, self._lib.wq3d_queue_take_eigenrays(self._q, recs, _abi.as_dp(inten),
                                                                   _abi.as_dp(phase), cnt, C.byref(n)))
-        out = [eigenray_model.from_record(recs[i], inten[i * nf:(i + 1) * nf],
-                                          phase[i * nf:(i + 1) * nf], self._freq) for i in range(cnt)]
-        if sens is not None:
-            for i, r in enumerate(out):
-                r.d_intensity_d_bottom = sens[3 * i:3 * i + 3].copy()
-        return out
+        rec = np.ctypeslib.as_array(recs)[:cnt].copy()
+        return eigenray_list(rec, inten[:cnt * nf].reshape(cnt, nf), phase[:cnt * nf].reshape(cnt, nf),
+                             None if sens is None else sens[:cnt * 3].reshape(cnt, 3), self._freq)
 
     def enable_sensitivity(self):
         """exact d(intensity)/d(bottom density ratio, speed ratio,
