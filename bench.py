@@ -45,7 +45,7 @@ FLOPS_PER_RAY_TARGET_STEP = 17
 BYTES_PER_RAY_CPA = 3 * 4 * 8 + 1
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_cpa_f32 launch on
 # this workload (ncu, launch 301; profiles/fp32c_step_kernels_*.md)
-NCU_TRAFFIC_CPA_F32 = 15993344 + 0
+NCU_TRAFFIC_CPA_F32 = 15986688 + 0
 
 
 def parse():
