@@ -179,6 +179,17 @@ def measure_fma_peaks():
 
 
 # ---------------------------------------------------------------- engine arm
+def max_over_ranks(values, dist):
+    """Each value's maximum over the ranks (every rank calls this once, in
+    the same place); the values themselves with a single process."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def engine_arm(args, rank, world, dist):
     import underseamodelinglibrary_b200 as u
     from underseamodelinglibrary_b200 import scenarios as S
@@ -261,13 +272,7 @@ def engine_arm(args, rank, world, dist):
         h2d = 8 * (nf + 2 * nde + 2 * naz + 3 * nt) + 8 * 3
         d2h = len(rays) * (96 + 16 * nf)
 
-    total_s = total_ms / 1000.0
-    e2e_s = sum(e2e_times)
-    if dist is not None:
-        import torch
-        tt = torch.tensor([total_s, e2e_s], dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_s, e2e_s = float(tt[0]), float(tt[1])
+    total_s, e2e_s = max_over_ranks([total_ms / 1000.0, sum(e2e_times)], dist)
     value = world * args.steps * ray_steps / total_s
     e2e = world * args.steps * ray_steps / e2e_s
 
