@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reverb", action="store_true",
+                    help="skip the reverberation-scale sample (3601 x 181 rays, 4096 targets)")
     ap.add_argument("--no-munk-cpu", action="store_true",
                     help="skip the oracle's full run of the Munk workload (a few seconds)")
     ap.add_argument("--no-gradients", action="store_true", help="skip the gradient workload")
@@ -321,6 +323,8 @@ def engine_arm(args, rank, world, dist):
         out["gradients"] = gradient_arm()
     out["std14"] = std14_arm()
     out["munk_flat"] = munk_arm()
+    if not args.no_reverb:
+        out["reverb_scale_sample"] = reverb_arm()
     return out
 
 
@@ -388,6 +392,33 @@ def munk_arm():
         out[name + "_eigenrays"] = n_eig
     out["steps"] = n_steps
     return out
+
+
+def reverb_arm():
+    """A bounded sample of the reverberation-scale workload: one of its 16
+    source depths (100 m), 3601 x 181 rays, 4096 targets, 32 frequencies,
+    the first 10 s (200 steps) of 180 s, eigenverbs off.  Device time of the
+    propagation (CUDA-graph replay); the eigenrays are read back after it."""
+    import underseamodelinglibrary_b200 as u
+    from underseamodelinglibrary_b200 import scenarios as S
+    from underseamodelinglibrary_b200 import _abi
+    try:
+        sc = S.reverb_scale(time_max=10.0)
+        rays = sc["de"].size() * sc["az"].size()
+        t0 = time.perf_counter()
+        q = S.build_queue(sc, u.wave_queue, precision=_abi.FP32C, eigenray_capacity=1 << 19)
+        t_build = time.perf_counter() - t0
+        q.timing(reset=True)
+        q.run(sc["time_max"])
+        ms = q.timing()["total_ms"]
+        n_steps = q.steps()
+        n_eig = len(q.take_eigenrays())
+        del q
+        return {"workload": sc["name"], "sample": "1 of 16 source depths, first 10 s of 180 s, eigenverbs off",
+                "rays": rays, "steps": n_steps, "ms_device": ms, "ray_steps_per_s": rays * n_steps / (ms / 1000.0),
+                "eigenrays": n_eig, "build_s": t_build, "form": "FP32C"}
+    except Exception as e:  # a failure here must not hide the headline line
+        return {"error": "%s: %s" % (type(e).__name__, e)}
 
 
 def gradient_arm():

@@ -18,7 +18,7 @@ import numpy as np
 from . import types as T
 from .ocean import (attenuation_constant, boundary_flat, boundary_grid, boundary_slope,
                     data_grid, ocean_model, profile_grid, profile_linear, profile_munk,
-                    reflect_loss_constant, reflect_loss_rayleigh, volume_flat)
+                    reflect_loss_constant, reflect_loss_eckart, reflect_loss_rayleigh, volume_flat)
 from ._abi import HYBRID_GAUSSIAN
 
 
@@ -235,7 +235,7 @@ def _smooth(field, sigmas):
 
 def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_lng=20,
                   n_bathy=100, ssp_std=5.0, corr_h=50e3, corr_v=300.0, depth_min=1000.0,
-                  depth_max=5000.0):
+                  depth_max=5000.0, surface=None):
     """Gridded environment over span x span degrees centred on (lat0, lng0):
 
     * profile_grid<3> on (rho, theta, phi) with n_depth nodes 0-5000 m x
@@ -244,7 +244,8 @@ def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_
       correlation lengths; pchip in depth, linear across;
     * boundary_grid<2> bottom on n_bathy x n_bathy (theta, phi) nodes:
       Gaussian-smoothed random relief scaled to depth_min..depth_max,
-      linear both ways, Rayleigh sand loss (the boundary_grid default).
+      linear both ways, Rayleigh sand loss (the boundary_grid default);
+    * ``surface``: the ocean surface (default boundary_flat()).
 
     Inputs are seeded synthetic fields (no data files)."""
     R = T.earth_radius()
@@ -268,7 +269,8 @@ def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_
     relief = _smooth(rng.standard_normal((n_bathy, n_bathy)), (n_bathy / 12.0, n_bathy / 12.0))
     relief = (relief - relief.min()) / max(relief.max() - relief.min(), 1e-30)
     bathy = data_grid([bt_ax, bp_ax], R - (depth_min + (depth_max - depth_min) * relief))
-    return ocean_model(boundary_flat(), boundary_grid(bathy), profile_grid(ssp))
+    return ocean_model(surface if surface is not None else boundary_flat(), boundary_grid(bathy),
+                       profile_grid(ssp))
 
 
 def random_targets(rng, src, n, max_range=100e3, depth=(10.0, 4000.0)):
@@ -297,6 +299,26 @@ def gridded_munk(seed=1, num_de=91, num_az=13, n_targets=64, time_max=30.0, src_
     return _pack(ocean=ocean, freq=freq or T.seq_log(1000.0, 1.0, 1), pos=src,
                  de=T.seq_rayfan(-90.0, 90.0, num_de), az=az, dt=dt, targets=tgt, time_max=time_max,
                  name="gridded_munk_%dx%d" % (num_de, num_az))
+
+
+def reverb_scale(source_depth=100.0, num_de=3601, num_az=181, n_targets=4096, time_max=180.0,
+                 seed=20261203):
+    """Reverberation-scale workload for one source depth: gridded_ocean()
+    (random profile grid and bathymetry) with Eckart surface loss at 10 m/s
+    wind, source ``source_depth`` m deep at 45N 45W, 32 log-spaced
+    frequencies 100 Hz - 10 kHz with Thorp attenuation, tangent-spaced D/E
+    fan x AZ 0..360 deg in 2 deg steps, dt 0.05 s, 4096 random targets
+    (10-4000 m deep within 100 km)."""
+    T.compute_earth_radius(45.0)
+    rng = np.random.default_rng(seed)
+    ocean = gridded_ocean(rng, surface=boundary_flat(0.0, reflect_loss_eckart(10.0)))
+    src = T.wposition1(45.0, -45.0, -float(source_depth))
+    tgt = random_targets(rng, src, n_targets)
+    freq = T.seq_log(100.0, 100.0 ** (1.0 / 31.0), 32)
+    az = T.seq_linear(0.0, 360.0 / (num_az - 1), num_az)
+    return _pack(ocean=ocean, freq=freq, pos=src, de=T.seq_rayfan(-90.0, 90.0, num_de), az=az, dt=0.05,
+                 targets=tgt, time_max=time_max,
+                 name="reverb_scale_%dx%d_%dtgt_32f" % (num_de, num_az, n_targets))
 
 
 def batched_gridded(n_instances=512, seed=20261203, num_de=(91, 1801), num_az=(1, 91),
