@@ -1266,18 +1266,43 @@ __device__ __forceinline__ float key2f(unsigned k) {
  * about 3u of mag + c0; the 14u, 43u (41u of the per-ray screen plus its
  * own rounding) and 1.0003 factors cover them, so a rejection implies that
  * every ray's FP32 screen rejects the pair. */
-__device__ __forceinline__ bool patch_rejects(const TgtW& g, const float* lo, const float* hi,
-                                              const float* W, float c0) {
-    float ub = 0.0f, mag = 0.0f, wm = 0.0f;
+struct PatchGuard {
+    float M[8]; /* max(|lo_k|, |hi_k|) of the patch's feature ranges      */
+    float K;    /* 43u * sum_k W_k M_k (W: the tile's largest weights)     */
+    float Cc;   /* 1.0003 c0                                               */
+};
+
+/* the parts of the bound that are the same for every target of the tile */
+__device__ __forceinline__ PatchGuard patch_guard(const float* lo, const float* hi, const float* W, float c0) {
+    PatchGuard p;
+    float wm = 0.0f;
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-        const float a = g.w[m] * lo[m], b = g.w[m] * hi[m];
-        ub += fmaxf(a, b);
-        mag += fmaxf(fabsf(a), fabsf(b));
-        wm += W[m] * fmaxf(fabsf(lo[m]), fabsf(hi[m]));
+        p.M[m] = fmaxf(fabsf(lo[m]), fabsf(hi[m]));
+        wm += W[m] * p.M[m];
     }
     const float u = 5.9604645e-8f; /* 2^-24 */
-    return ub + (14.0f * u) * mag + (43.0f * u) * wm + 1.0003f * c0 < 0.0f;
+    p.K = (43.0f * u) * wm;
+    p.Cc = 1.0003f * c0;
+    return p;
+}
+
+/* The sum above with one product per term: rounding is monotone, so
+ * max(fl(w lo), fl(w hi)) is fl(w hi) for w >= 0 and fl(w lo) otherwise,
+ * and max(|fl(w lo)|, |fl(w hi)|) is fl(|w| max(|lo|, |hi|)); the
+ * additions keep their order, so the decisions are those of the full
+ * form. */
+__device__ __forceinline__ bool patch_rejects(const TgtW& g, const float* lo, const float* hi,
+                                              const PatchGuard& p) {
+    float ub = 0.0f, mag = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const float w = g.w[m];
+        ub += w * (w >= 0.0f ? hi[m] : lo[m]);
+        mag += fabsf(w) * p.M[m];
+    }
+    const float u = 5.9604645e-8f; /* 2^-24 */
+    return ub + (14.0f * u) * mag + p.K + p.Cc < 0.0f;
 }
 }  // namespace
 
@@ -1420,10 +1445,12 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(__grid_constant__ co
         gxc = fmaf(32.0f * u, gxc, c0);
         gvc = fmaf(32.0f * u, gvc, c0);
         /* targets that some ray of the patch may keep */
+        const PatchGuard px = patch_guard(&bound[0], &bound[8], W, c0);
+        const PatchGuard pv = patch_guard(&bound[16], &bound[24], W, c0);
         for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
             const TgtW g = tw[j];
-            if (patch_rejects(g, &bound[0], &bound[8], W, c0)) continue;
-            if (patch_rejects(g, &bound[16], &bound[24], W, c0)) continue;
+            if (patch_rejects(g, &bound[0], &bound[8], px)) continue;
+            if (patch_rejects(g, &bound[16], &bound[24], pv)) continue;
             surv[atomicAdd(&nsurv, 1)] = (uint16_t)j;
         }
         __syncthreads();
