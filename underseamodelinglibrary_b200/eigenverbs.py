@@ -77,3 +77,39 @@ class eigenverb_collection(eigenverb_listener):
 
     def add_eigenverb(self, verb, interface_num):
         self._collection[interface_num].append(verb)
+
+    #: size of the search area of find_eigenverbs, in footprint lengths and
+    #: widths (eigenverb_collection.cc:32)
+    search_scale = 1.5
+
+    def find_eigenverbs(self, bounding_verb, interface_num):
+        """eigenverb_collection::find_eigenverbs (eigenverb_collection.cc:
+        60-93): the eigenverbs of one interface whose centres lie strictly
+        inside the quadrilateral, in (latitude, longitude), whose corners are
+        search_scale x length ahead of and behind the bounding eigenverb
+        along its direction and search_scale x width to either side.  The
+        reference queries an R-tree; the corners are convex, so this tests
+        each centre against the four edges at once (in insertion order)."""
+        from .types import wposition1
+        verbs = self._collection[interface_num]
+        if not verbs:
+            return []
+        pos = wposition1()
+        pos.rho, pos.theta, pos.phi = bounding_verb.position
+        d, s = bounding_verb.direction, self.search_scale
+        corners = [wposition1(pos, s * bounding_verb.length, d),
+                   wposition1(pos, s * bounding_verb.width, d + np.pi / 2),
+                   wposition1(pos, s * bounding_verb.length, d + np.pi),
+                   wposition1(pos, s * bounding_verb.width, d + np.pi + np.pi / 2)]
+        cx = np.array([c.latitude() for c in corners])
+        cy = np.array([c.longitude() for c in corners])
+        th = np.array([v.position[1] for v in verbs])
+        ph = np.array([v.position[2] for v in verbs])
+        x = 90.0 - np.degrees(th)
+        y = np.degrees(ph)
+        cross = np.empty((4, len(verbs)))
+        for k in range(4):
+            x1, y1, x2, y2 = cx[k], cy[k], cx[(k + 1) % 4], cy[(k + 1) % 4]
+            cross[k] = (x2 - x1) * (y - y1) - (y2 - y1) * (x - x1)
+        inside = np.all(cross > 0.0, axis=0) | np.all(cross < 0.0, axis=0)
+        return [verbs[i] for i in np.nonzero(inside)[0]]
