@@ -8,8 +8,10 @@ averages of time and angles (eigenray_collection.cc:105-191).
 import cmath
 import math
 
-from .types import to_degrees, to_radians
-from .waveq3d import eigenray_listener
+import numpy as np
+
+from .types import to_degrees, to_radians, wposition1
+from .waveq3d import eigenray_listener, eigenray_model
 
 
 class eigenray_total:
@@ -50,6 +52,19 @@ class eigenray_collection(eigenray_listener):
 
     def eigenrays(self, t1, t2):
         return list(self._rays[t1][t2])
+
+    def dead_reckon(self, t1, t2, source_new, target_new, profile):
+        """eigenray_collection::dead_reckon (eigenray_collection.cc:361-368):
+        the eigenrays of target (t1, t2) moved to a new source position, then
+        to a new target position, by dead_reckon_one.  ``profile`` is the
+        ocean_model (or profile_model) whose sound speed and attenuation are
+        used."""
+        rays = dead_reckon_one(self._rays[t1][t2], self._source, source_new, profile)
+        old_target = wposition1()
+        old_target.rho = float(self._targets.rho[t1, t2])
+        old_target.theta = float(self._targets.theta[t1, t2])
+        old_target.phi = float(self._targets.phi[t1, t2])
+        return dead_reckon_one(rays, old_target, target_new, profile)
 
     def initial_time(self, t1, t2):
         return self._initial[t1][t2]
@@ -102,3 +117,60 @@ class eigenray_collection(eigenray_listener):
                 tot.surface, tot.bottom, tot.caustic = surface, bottom, caustic
                 tot.upper, tot.lower = upper, lower
                 self._total[t1][t2] = tot
+
+
+def _evaluator(profile):
+    """an object with sound_speed / attenuation point evaluations"""
+    if hasattr(profile, "sound_speed") and hasattr(profile, "attenuation") and hasattr(profile, "handle"):
+        return profile
+    from .ocean import boundary_flat, ocean_model
+    return ocean_model(boundary_flat(), boundary_flat(1.0e4), profile)
+
+
+def dead_reckon_one(eigenrays, oldpos, newpos, profile):
+    """eigenray_collection::dead_reckon_one (eigenray_collection.cc:373-446):
+    adjusts eigenrays for a small move of one sensor.  The move, in the local
+    tangent plane at the old position, is projected on each ray's launch
+    direction (source D/E and AZ, also for a moving target, as the reference
+    does); travel time changes by that range over the sound speed at the old
+    position, and intensity by the change of 20 log10(r) plus attenuation
+    over r (r = travel time x sound speed).  A move of less than 1 mm returns
+    the eigenrays unchanged."""
+    dr_rho = newpos.rho - oldpos.rho
+    dr_th = (newpos.theta - oldpos.theta) * oldpos.rho
+    dr_ph = (newpos.phi - oldpos.phi) * (oldpos.rho * math.sin(oldpos.theta))
+    if dr_rho * dr_rho + dr_th * dr_th + dr_ph * dr_ph < 1e-6:
+        return list(eigenrays)
+    rays = list(eigenrays)
+    if not rays:
+        return []
+    ev = _evaluator(profile)
+    c, _ = ev.sound_speed([oldpos.rho], [oldpos.theta], [oldpos.phi])
+    sound_speed = float(c[0])
+    freq = rays[0].frequencies
+    fv = np.array([freq(k) for k in range(freq.size())], dtype=np.float64)
+    r1 = np.empty(len(rays))
+    r2 = np.empty(len(rays))
+    out = []
+    for n, ray in enumerate(rays):
+        de = to_radians(ray.source_de)
+        az = to_radians(ray.source_az)
+        cos_de, sin_de = math.cos(de), math.sin(de)
+        cos_az, sin_az = math.cos(az), math.sin(az)
+        dr = dr_rho * sin_de + dr_th * (-cos_de * cos_az) + dr_ph * (cos_de * sin_az)
+        new = eigenray_model()
+        for name in eigenray_model.__slots__:
+            setattr(new, name, getattr(ray, name, None))
+        new.travel_time = ray.travel_time + dr / sound_speed
+        r1[n] = ray.travel_time * sound_speed
+        r2[n] = r1[n] + dr
+        out.append(new)
+    rho = np.full(len(rays), oldpos.rho)
+    a1 = ev.attenuation(rho, r1, fv)
+    a2 = ev.attenuation(rho, r2, fv)
+    for n, (ray, new) in enumerate(zip(rays, out)):
+        inten = np.array(ray.intensity, dtype=np.float64)
+        offset = inten - 20.0 * np.log10(r1[n]) - a1[n]
+        new.intensity = 20.0 * np.log10(r2[n]) + a2[n] + offset
+        new.phase = np.array(ray.phase, dtype=np.float64)
+    return out
