@@ -18,6 +18,7 @@ from .ocean import (attenuation_thorp, attenuation_constant, profile_linear,
 from .waveq3d import (wave_queue, eigenray_listener, reflection_listener,
                       eigenray_model, eigenray_list, run_batch)
 from .eigenrays import eigenray_collection
+from .wavegen import run_wavefront_generators, wavefront_generator
 from .eigenverbs import eigenverb_model, eigenverb_listener, eigenverb_collection
 
 load_engine = _abi.load_engine
@@ -33,6 +34,7 @@ __all__ = [
     "boundary_flat", "boundary_slope", "ocean_model", "data_grid", "profile_grid",
     "boundary_grid", "volume_flat", "wave_queue", "run_batch",
     "eigenray_listener", "reflection_listener", "eigenray_model", "eigenray_list",
+    "wavefront_generator", "run_wavefront_generators",
     "eigenray_collection", "eigenverb_model", "eigenverb_listener", "eigenverb_collection",
     "load_engine", "EngineError", "LIB_PATH",
 ]
