@@ -73,49 +73,62 @@ class eigenray_collection(eigenray_listener):
         return self._total[t1][t2]
 
     def sum_eigenrays(self):
+        """eigenray_collection::sum_eigenrays (eigenray_collection.cc:
+        105-191), one target at a time with numpy.  Every sum runs in the
+        reference's order (frequency, then eigenray) as a sequential
+        cumulative sum: the phasor of each frequency, and the weights
+        a^2 = 10^(-I/10) with the weighted travel time, D/E and the unit
+        vectors of AZ.  The strongest path (first largest weight) gives the
+        counts."""
         nf = self._freq.size()
+        fv = np.array([self._freq[f] for f in range(nf)], dtype=np.float64)
+        two_pi = 2.0 * math.pi
         for t1 in range(self.size1()):
             for t2 in range(self.size2()):
                 rays = self._rays[t1][t2]
                 tot = eigenray_total()
-                tot.intensity = [0.0] * nf
-                tot.phase = [0.0] * nf
-                time = source_de = saz_x = saz_y = target_de = taz_x = taz_y = 0.0
-                surface = bottom = caustic = upper = lower = -1
-                wgt = 0.0
-                max_a = 0.0
-                for f in range(nf):
-                    phasor = complex(0.0, 0.0)
-                    for ray in rays:
-                        a = math.pow(10.0, ray.intensity[f] / -20.0)
-                        if self._coherent:
-                            p = 2.0 * math.pi * self._freq[f] * ray.travel_time + ray.phase[f]
-                            p = math.fmod(p, 2.0 * math.pi)
-                            phasor += complex(a * math.cos(p), a * math.sin(p))
-                        else:
-                            phasor += a
-                        a *= a
-                        wgt += a
-                        time += a * ray.travel_time
-                        source_de += a * ray.source_de
-                        saz_x += a * math.sin(to_radians(ray.source_az))
-                        saz_y += a * math.cos(to_radians(ray.source_az))
-                        target_de += a * ray.target_de
-                        taz_x += a * math.sin(to_radians(ray.target_az))
-                        taz_y += a * math.cos(to_radians(ray.target_az))
-                        if a > max_a:
-                            max_a = a
-                            surface, bottom, caustic = ray.surface, ray.bottom, ray.caustic
-                            upper, lower = ray.upper, ray.lower
-                    tot.intensity[f] = -20.0 * math.log10(max(1e-15, abs(phasor)))
-                    tot.phase[f] = cmath.phase(phasor)
-                tot.travel_time = time / wgt if wgt else float("nan")
-                tot.source_de = source_de / wgt if wgt else float("nan")
-                tot.source_az = 90.0 - to_degrees(math.atan2(saz_y, saz_x))
-                tot.target_de = target_de / wgt if wgt else float("nan")
-                tot.target_az = 90.0 - to_degrees(math.atan2(taz_y, taz_x))
-                tot.surface, tot.bottom, tot.caustic = surface, bottom, caustic
-                tot.upper, tot.lower = upper, lower
+                n = len(rays)
+                if n == 0:
+                    tot.intensity = [-20.0 * math.log10(1e-15)] * nf
+                    tot.phase = [0.0] * nf
+                    tot.travel_time = tot.source_de = tot.target_de = float("nan")
+                    tot.source_az = tot.target_az = 90.0 - to_degrees(math.atan2(0.0, 0.0))
+                    tot.surface = tot.bottom = tot.caustic = tot.upper = tot.lower = -1
+                    self._total[t1][t2] = tot
+                    continue
+                amp = np.power(10.0, np.array([r.intensity for r in rays], dtype=np.float64).T / -20.0)
+                if self._coherent:
+                    tt = np.array([r.travel_time for r in rays], dtype=np.float64)
+                    ph = np.array([r.phase for r in rays], dtype=np.float64).T
+                    p = np.fmod(two_pi * fv[:, None] * tt[None, :] + ph, two_pi)
+                    re = np.cumsum(amp * np.cos(p), axis=1)[:, -1]
+                    im = np.cumsum(amp * np.sin(p), axis=1)[:, -1]
+                else:
+                    re = np.cumsum(amp, axis=1)[:, -1]
+                    im = np.zeros(nf)
+                tot.intensity = [float(x) for x in -20.0 * np.log10(np.maximum(1e-15, np.hypot(re, im)))]
+                tot.phase = [float(x) for x in np.arctan2(im, re)]
+                w = (amp * amp).ravel()  # (frequency, eigenray) order
+                wgt = float(np.cumsum(w)[-1])
+
+                def wsum(v):
+                    return float(np.cumsum(w * np.tile(np.asarray(v, dtype=np.float64), nf))[-1])
+
+                saz = np.radians([r.source_az for r in rays])
+                taz = np.radians([r.target_az for r in rays])
+                nan = float("nan")
+                tot.travel_time = wsum([r.travel_time for r in rays]) / wgt if wgt else nan
+                tot.source_de = wsum([r.source_de for r in rays]) / wgt if wgt else nan
+                tot.source_az = 90.0 - to_degrees(math.atan2(wsum(np.cos(saz)), wsum(np.sin(saz))))
+                tot.target_de = wsum([r.target_de for r in rays]) / wgt if wgt else nan
+                tot.target_az = 90.0 - to_degrees(math.atan2(wsum(np.cos(taz)), wsum(np.sin(taz))))
+                j = int(np.argmax(w))
+                if w[j] > 0.0:
+                    best = rays[j % n]
+                    tot.surface, tot.bottom, tot.caustic = best.surface, best.bottom, best.caustic
+                    tot.upper, tot.lower = best.upper, best.lower
+                else:
+                    tot.surface = tot.bottom = tot.caustic = tot.upper = tot.lower = -1
                 self._total[t1][t2] = tot
 
 
