@@ -920,11 +920,14 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
         /* commit the reflected ray (reflection_copy into prev, curr, next) */
         const int32_t w = __ldg(q.shadow_slot + i);
         sh = q.shadow + (size_t)w * stride;
+        /* one state at a time: its stores may alias the later loads as
+         * far as the compiler knows, so loading all three first would keep
+         * 51 values live */
         ray_from(sh, y0);
-        ray_from(sh + 17, y1);
-        ray_from(sh + 34, y2);
         copy_ray(*R.V, i, y0);
+        ray_from(sh + 17, y1);
         copy_ray(*R.C, i, y1);
+        ray_from(sh + 34, y2);
         copy_ray(*R.X, i, y2);
         sf = __ldg(q.shadow_cnt + 3 * (size_t)w);
         bt = __ldg(q.shadow_cnt + 3 * (size_t)w + 1);
