@@ -446,3 +446,17 @@ def test_queued_chunks_match_single_chunks(engine, precision):
     assert sum(1 for c in la.calls if c[0] == "reflect") > 100
     assert sum(1 for c in la.calls if c[0] == "ray") > 10
     assert la.calls == lb.calls[:cut]
+
+
+def test_reverb_scale_reduced_parity(engine):
+    """The reverberation-scale environment (gridded random ocean, Eckart
+    surface loss at 10 m/s, 32 frequencies 100 Hz - 10 kHz) on a reduced
+    fan and target set, FP32C engine against the oracle."""
+    sc = S.reverb_scale(num_de=181, num_az=19, n_targets=32, time_max=5.0)
+    q = S.build_queue(sc, u.wave_queue, precision=_abi.FP32C)
+    o = S.build_queue(sc, OracleQueue)
+    q.run(sc["time_max"])
+    o.run(sc["time_max"])
+    eng = q.take_eigenrays()
+    assert len(eng) > 10 and len(eng[0].intensity) == 32
+    compare_eigenrays(eng, o.take_eigenrays())
