@@ -135,6 +135,8 @@ __device__ __forceinline__ void ab3(double h, const RayS& y0, const RayS& y1,
     }
 }
 
+#if !WQ3D_STEP_KERNELS_ONLY
+/* one ray's state (k_volume) */
 __device__ __forceinline__ void load_ray(const FrontPtrs& f, int r, RayS& y) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -147,6 +149,7 @@ __device__ __forceinline__ void load_ray(const FrontPtrs& f, int r, RayS& y) {
     y.c = f.c[r];
     y.dist = f.dist[r];
 }
+#endif
 
 /* load_ray through the read-only data cache, for kernels that never write
  * the arrays they read this way: the loads may then all be in flight at
