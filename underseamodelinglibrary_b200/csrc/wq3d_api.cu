@@ -197,10 +197,18 @@ int make_grid(wq3d_ocean* o, const wq3d_grid_desc& d, int max_dims, GridDev* hg,
 
 }  // namespace
 
-struct PendingRay {
-    wq3d_eigenray rec;
-    std::vector<double> inten, phase;
-    double sens[3] = {0.0, 0.0, 0.0}; /* dTL / d bottom parameters */
+/* eigenrays kept for wq3d_queue_take_eigenrays (no listener), as flat
+ * arrays: nf intensities and phases and 3 bottom sensitivities per ray */
+struct PendingRays {
+    std::vector<wq3d_eigenray> rec;
+    std::vector<double> inten, phase, sens;
+    size_t size() const { return rec.size(); }
+    void clear() {
+        rec.clear();
+        inten.clear();
+        phase.clear();
+        sens.clear();
+    }
 };
 
 struct wq3d_queue {
@@ -252,7 +260,7 @@ struct wq3d_queue {
     wq3d_callbacks cb{};
     void* cb_ctx = nullptr;
     uint64_t run_id = 0;
-    std::vector<PendingRay> pending;
+    PendingRays pending;
     std::atomic<bool> abort_flag{false};
     bool timing = false;
     std::vector<cudaEvent_t> events;
@@ -601,13 +609,10 @@ struct wq3d_queue {
                     cb.add_eigenray(cb_ctx, (size_t)h_rec[j].t1, (size_t)h_rec[j].t2, &h_rec[j],
                                     &h_rinten[j * nf], &h_rphase[j * nf], (size_t)nf, run_id);
                 } else {
-                    PendingRay p;
-                    p.rec = h_rec[j];
-                    p.inten.assign(&h_rinten[j * nf], &h_rinten[j * nf] + nf);
-                    if (h.sens)
-                        for (int m = 0; m < 3; ++m) p.sens[m] = h_rsens[j * 3 + m];
-                    p.phase.assign(&h_rphase[j * nf], &h_rphase[j * nf] + nf);
-                    pending.push_back(std::move(p));
+                    pending.rec.push_back(h_rec[j]);
+                    pending.inten.insert(pending.inten.end(), &h_rinten[j * nf], &h_rinten[j * nf] + nf);
+                    pending.phase.insert(pending.phase.end(), &h_rphase[j * nf], &h_rphase[j * nf] + nf);
+                    for (int m = 0; m < 3; ++m) pending.sens.push_back(h.sens ? h_rsens[j * 3 + m] : 0.0);
                 }
                 ++ie;
             }
@@ -1457,10 +1462,11 @@ int wq3d_queue_take_eigenrays(wq3d_queue* q, wq3d_eigenray* rays, double* inten,
     if (!rays) return WQ3D_OK;
     if (capacity < q->pending.size()) return fail(WQ3D_ERR_OVERFLOW, "capacity smaller than the pending count");
     const size_t nf = q->h.nf;
-    for (size_t i = 0; i < q->pending.size(); ++i) {
-        rays[i] = q->pending[i].rec;
-        if (inten) std::memcpy(inten + i * nf, q->pending[i].inten.data(), nf * sizeof(double));
-        if (phase) std::memcpy(phase + i * nf, q->pending[i].phase.data(), nf * sizeof(double));
+    const size_t n = q->pending.size();
+    if (n > 0) {
+        std::memcpy(rays, q->pending.rec.data(), n * sizeof(wq3d_eigenray));
+        if (inten) std::memcpy(inten, q->pending.inten.data(), n * nf * sizeof(double));
+        if (phase) std::memcpy(phase, q->pending.phase.data(), n * nf * sizeof(double));
     }
     q->pending.clear();
     return WQ3D_OK;
@@ -1490,7 +1496,7 @@ int wq3d_queue_sensitivities(const wq3d_queue* q, double* sens, size_t capacity,
     if (!sens) return WQ3D_OK;
     if (capacity < q->pending.size()) return fail(WQ3D_ERR_OVERFLOW, "capacity smaller than the pending count");
     for (size_t i = 0; i < q->pending.size(); ++i)
-        for (int m = 0; m < 3; ++m) sens[i * 3 + m] = q->h.sens ? q->pending[i].sens[m] : NAN;
+        for (int m = 0; m < 3; ++m) sens[i * 3 + m] = q->h.sens ? q->pending.sens[i * 3 + m] : NAN;
     return WQ3D_OK;
 }
 
