@@ -415,7 +415,8 @@ struct wq3d_queue {
         for (auto e : done_ev)
             if (e) cudaEventDestroy(e);
         if (copy) cudaStreamDestroy(copy);
-        for (auto e : events) cudaEventDestroy(e);
+        for (auto e : events)
+            if (e) cudaEventDestroy(e);
         for (auto e : fork_ev) cudaEventDestroy(e);
         for (auto e : join_ev) cudaEventDestroy(e);
         if (side) cudaStreamDestroy(side);
@@ -1250,15 +1251,13 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         if (cudaEventCreateWithFlags(&q->fork_ev[k], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&q->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-    q->events.resize(7 * (size_t)q->chunk + 2);
-    for (auto& ev : q->events)
-        if (cudaEventCreate(&ev) != cudaSuccess) return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
     /* set-up a run would otherwise do on its first chunks: the second
-     * result set and the chunk graphs (rebuilt later only if callbacks,
-     * thresholds or sensitivities change the descriptor) */
+     * result set and the graphs of the chunks that reflect the next
+     * chunk's first step (rebuilt later only if callbacks, thresholds or
+     * sensitivities change the descriptor); the graphs of a run's last
+     * full chunk are built when first used */
     q->ensure_set1();
-    for (int p = 0; p < (q->have_set1 ? 2 : 1); ++p)
-        for (int t = 0; t < 2; ++t) q->build_graph(p, t != 0);
+    for (int p = 0; p < (q->have_set1 ? 2 : 1); ++p) q->build_graph(p, true);
     *out = q;
     return WQ3D_OK;
 }
@@ -1527,6 +1526,15 @@ int wq3d_queue_timing(wq3d_queue* q, wq3d_timing* out, int reset) {
  * the chunk graph while on). */
 int wq3d_queue_set_timing(wq3d_queue* q, int on) {
     if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    if (on && q->events.empty()) {
+        DeviceGuard guard(q->device);
+        q->events.resize(7 * (size_t)q->chunk + 2);
+        for (auto& ev : q->events)
+            if (cudaEventCreate(&ev) != cudaSuccess) {
+                ev = nullptr;
+                return fail(WQ3D_ERR_CUDA, "cudaEventCreate failed");
+            }
+    }
     q->timing = on != 0;
     return WQ3D_OK;
 }
