@@ -36,3 +36,11 @@ def test_cpp_eigenverb_accuracy(tmp_path, engine):
                          timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "interfaces 4" in out.stdout
+
+
+def test_cpp_run_batch(tmp_path, engine):
+    """wave_queue::run_batch through the C++ header: two sources batched,
+    each equal to its solo run bit for bit"""
+    out = subprocess.run([build_cpp(tmp_path, "batch_cpp")], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "batch equals solo" in out.stdout

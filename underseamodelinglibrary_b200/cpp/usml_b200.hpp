@@ -547,6 +547,23 @@ class wave_queue {
     }
     void step() { check(wq3d_queue_step(_q.get(), 1)); }
     void run(double time_max) { check(wq3d_queue_run(_q.get(), time_max, nullptr)); }
+    /** thread_task::abort: the run stops before its next chunk of steps */
+    void abort() { check(wq3d_queue_abort(_q.get())); }
+    /**
+     * Runs several queues together on one GPU, each until its time()
+     * reaches its time_max (wq3d_batch_run), where the reference runs one
+     * wavefront_generator task per queue on a thread pool.  Listeners are
+     * called per queue in the reference's order.  Returns the device
+     * milliseconds of the batch.
+     */
+    static double run_batch(const std::vector<wave_queue*>& queues, const std::vector<double>& time_max) {
+        if (queues.size() != time_max.size()) throw std::invalid_argument("one time_max per queue");
+        std::vector<wq3d_queue*> handles;
+        for (auto* q : queues) handles.push_back(q->_q.get());
+        double ms = 0.0;
+        check(wq3d_batch_run(handles.data(), handles.size(), time_max.data(), nullptr, &ms));
+        return ms;
+    }
     double time() const {
         double t = 0.0;
         check(wq3d_queue_time(_q.get(), &t));
