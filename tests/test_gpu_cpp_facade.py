@@ -44,3 +44,29 @@ def test_cpp_run_batch(tmp_path, engine):
     out = subprocess.run([build_cpp(tmp_path, "batch_cpp")], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "batch equals solo" in out.stdout
+
+
+def test_cpp_reflection_listener(tmp_path, engine):
+    """reflection_test.cc:168-280 through the C++ header: a
+    reflection_listener hears every bounce, the same as the oracle's, and a
+    removed listener hears no more; the queue's accessors read back"""
+    import math
+    import re
+
+    from oracle_binding import OracleQueue
+    from underseamodelinglibrary_b200 import scenarios as S
+
+    out = subprocess.run([build_cpp(tmp_path, "reflect_cpp")], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "reflections ok" in out.stdout
+    got = [(int(m[0]), float(m[1]), float(m[2]))
+           for m in re.findall(r"type (\d+) time ([-\d.]+) grazing ([-\d.]+)", out.stdout)]
+    sc = S.reflect_flat()
+    o = S.build_queue(sc, OracleQueue, reflections=True)
+    o.run(sc["time_max"])
+    ref = o.take_reflections()
+    assert len(got) == len(ref) >= 7
+    for (t, time, graz), r in zip(got, ref):
+        assert t == r.type
+        assert abs(time - r.time) < 2e-9
+        assert abs(graz - math.degrees(r.grazing)) < 2e-6

@@ -10,6 +10,7 @@
  */
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <memory>
@@ -173,6 +174,22 @@ class wposition1 {
     void latitude(double v) { _t = to_radians(90.0 - v); }
     void longitude(double v) { _p = to_radians(v); }
     void altitude(double v) { _r = v + earth::radius(); }
+
+   private:
+    double _r = 0, _t = 0, _p = 0;
+};
+
+/* wvector1 (types/wvector1.h): one vector in spherical earth coordinates */
+class wvector1 {
+   public:
+    wvector1() {}
+    wvector1(double rho, double theta, double phi) : _r(rho), _t(theta), _p(phi) {}
+    double rho() const { return _r; }
+    double theta() const { return _t; }
+    double phi() const { return _p; }
+    void rho(double v) { _r = v; }
+    void theta(double v) { _t = v; }
+    void phi(double v) { _p = v; }
 
    private:
     double _r = 0, _t = 0, _p = 0;
@@ -499,6 +516,16 @@ class eigenverb_collection : public eigenverb_listener {
 
 namespace waveq3d {
 
+/* reflection_listener (waveq3d/reflection_listener.h:46-49): one call per
+ * boundary collision; type 0 is the bottom, 1 the surface */
+class reflection_listener {
+   public:
+    virtual ~reflection_listener() {}
+    virtual void reflect(double time, size_t de, size_t az, double dt, double grazing, double speed,
+                         const types::wposition1& position, const types::wvector1& ndirection,
+                         size_t type) = 0;
+};
+
 /* wave_queue (waveq3d/wave_queue.h:122-264) */
 class wave_queue {
    public:
@@ -508,7 +535,7 @@ class wave_queue {
                const types::wposition1& pos, const types::seq_vector::csptr& de,
                const types::seq_vector::csptr& az, double time_step, const types::wposition* targets = nullptr,
                spreading_type type = HYBRID_GAUSSIAN, int precision = WQ3D_FP32C)
-        : _ocean(ocean), _freq(freq) {
+        : _ocean(ocean), _freq(freq), _time_step(time_step), _num_de(de->size()), _num_az(az->size()) {
         wq3d_queue_desc d{};
         d.freq = freq->data().data();
         d.num_freq = freq->size();
@@ -545,6 +572,13 @@ class wave_queue {
         _verb_listeners.push_back(l);
         install();
     }
+    void add_reflection_listener(reflection_listener* l) {
+        _refl_listeners.push_back(l);
+        install();
+    }
+    void remove_eigenray_listener(eigenrays::eigenray_listener* l) { drop(_listeners, l); }
+    void remove_eigenverb_listener(eigenverbs::eigenverb_listener* l) { drop(_verb_listeners, l); }
+    void remove_reflection_listener(reflection_listener* l) { drop(_refl_listeners, l); }
     void step() { check(wq3d_queue_step(_q.get(), 1)); }
     void run(double time_max) { check(wq3d_queue_run(_q.get(), time_max, nullptr)); }
     /** thread_task::abort: the run stops before its next chunk of steps */
@@ -569,6 +603,24 @@ class wave_queue {
         check(wq3d_queue_time(_q.get(), &t));
         return t;
     }
+    double time_step() const { return _time_step; }
+    size_t num_de() const { return _num_de; }
+    size_t num_az() const { return _num_az; }
+    /** steps taken since the queue was made (AB3 and start-up alike) */
+    int64_t steps() const {
+        int64_t n = 0;
+        check(wq3d_queue_steps(_q.get(), &n));
+        return n;
+    }
+    types::wposition1 source_pos() const {
+        double s[3];
+        check(wq3d_queue_source(_q.get(), s));
+        types::wposition1 p;
+        p.rho(s[0]);
+        p.theta(s[1]);
+        p.phi(s[2]);
+        return p;
+    }
     void intensity_threshold(double v) {
         _th.intensity = std::abs(v);
         check(wq3d_queue_set_thresholds(_q.get(), &_th));
@@ -585,8 +637,25 @@ class wave_queue {
         _th.max_surface = v;
         check(wq3d_queue_set_thresholds(_q.get(), &_th));
     }
+    void max_caustic(int v) {
+        _th.max_caustic = v;
+        check(wq3d_queue_set_thresholds(_q.get(), &_th));
+    }
+    void max_upper(int v) {
+        _th.max_upper = v;
+        check(wq3d_queue_set_thresholds(_q.get(), &_th));
+    }
+    void max_lower(int v) {
+        _th.max_lower = v;
+        check(wq3d_queue_set_thresholds(_q.get(), &_th));
+    }
 
    private:
+    template <class L>
+    void drop(std::vector<L*>& v, L* l) {
+        v.erase(std::remove(v.begin(), v.end(), l), v.end());
+        install();
+    }
     void install() {
         wq3d_callbacks cb{};
         if (!_listeners.empty()) {
@@ -594,7 +663,19 @@ class wave_queue {
             cb.check_eigenrays = &wave_queue::on_check;
         }
         if (!_verb_listeners.empty()) cb.add_eigenverb = &wave_queue::on_verb;
+        if (!_refl_listeners.empty()) cb.reflect = &wave_queue::on_reflect;
         check(wq3d_queue_set_callbacks(_q.get(), &cb, this));
+    }
+    static void on_reflect(void* ctx, const wq3d_reflection* r) {
+        auto* self = static_cast<wave_queue*>(ctx);
+        types::wposition1 pos;
+        pos.rho(r->position[0]);
+        pos.theta(r->position[1]);
+        pos.phi(r->position[2]);
+        const types::wvector1 nd(r->ndirection[0], r->ndirection[1], r->ndirection[2]);
+        for (auto* l : self->_refl_listeners)
+            l->reflect(r->time, (size_t)r->de, (size_t)r->az, r->dt, r->grazing, r->speed, pos, nd,
+                       (size_t)r->type);
     }
     static void on_verb(void* ctx, const wq3d_eigenverb* v, const double* power, size_t nf, int interface_num) {
         auto* self = static_cast<wave_queue*>(ctx);
@@ -647,6 +728,9 @@ class wave_queue {
     std::shared_ptr<wq3d_queue> _q;
     std::vector<eigenrays::eigenray_listener*> _listeners;
     std::vector<eigenverbs::eigenverb_listener*> _verb_listeners;
+    std::vector<reflection_listener*> _refl_listeners;
+    double _time_step;
+    size_t _num_de, _num_az;
     wq3d_thresholds _th{300.0, 300.0, 999, 999, 999, 999, 999};
 };
 
