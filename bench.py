@@ -325,6 +325,7 @@ def engine_arm(args, rank, world, dist):
     out["munk_flat"] = munk_arm()
     if not args.no_reverb:
         out["reverb_scale_sample"] = reverb_arm()
+    out["biverbs"] = biverb_arm()
     return out
 
 
@@ -417,6 +418,73 @@ def reverb_arm():
         return {"workload": sc["name"], "sample": "1 of 16 source depths, first 10 s of 180 s, eigenverbs off",
                 "rays": rays, "steps": n_steps, "ms_device": ms, "ray_steps_per_s": rays * n_steps / (ms / 1000.0),
                 "eigenrays": n_eig, "build_s": t_build, "form": "FP32C"}
+    except Exception as e:  # a failure here must not hide the headline line
+        return {"error": "%s: %s" % (type(e).__name__, e)}
+
+
+BIVERB_WORKLOAD = "biverbs_bistatic_footprints_57600x57600_2freq"
+
+
+def biverb_inputs():
+    """Bistatic footprints in the shape of the reference's biverb test
+    (biverbs_test.cc:41-77): a source at (0, 0) and a receiver 1.1 km away
+    on the surface of 500 m deep isovelocity water, D/E -85..-5.5 deg in
+    0.5 deg steps x AZ 0..359 deg in 1 deg steps (57,600 eigenverbs each),
+    2 frequencies, -30 dB constant bottom scattering."""
+    import numpy as np
+    from underseamodelinglibrary_b200 import scenarios as S
+    from underseamodelinglibrary_b200 import types as T
+    T.set_earth_radius(6371000.0)
+    de = np.arange(-85.0, -5.0, 0.5)
+    az = np.arange(0.0, 360.0, 1.0)
+    src = S.analytic_footprints(0.0, 0.0, 500.0, de, az, 2)
+    rcv = S.analytic_footprints(0.007, 0.007, 500.0, de, az, 2)
+    return src, rcv, np.array([1000.0, 2000.0])
+
+
+def biverb_call(lib, fn, src, rcv, freq, num_rcv=None, out=None, out_power=None, capacity=0):
+    import ctypes as C
+    from underseamodelinglibrary_b200 import _abi
+    from underseamodelinglibrary_b200.ocean import scattering_constant
+    dp = C.POINTER(C.c_double)
+    (s, sp), (r, rp) = src, rcv
+    ns, nr = sp.shape[0], rp.shape[0] if num_rcv is None else num_rcv
+    count = C.c_size_t()
+    desc = scattering_constant(-30.0).desc()
+    rc = getattr(lib, fn)(s, sp.ctypes.data_as(dp), ns, r, rp.ctypes.data_as(dp), nr,
+                          freq.ctypes.data_as(dp), freq.size, C.byref(desc), 6371000.0, 1.5, 1e-20,
+                          out, out_power.ctypes.data_as(dp) if out_power is not None else None,
+                          capacity, C.byref(count))
+    if rc != 0:
+        raise _abi.EngineError(rc, "biverbs")
+    return count.value
+
+
+def biverb_arm():
+    """wq3d_biverbs on the bistatic footprint workload, end to end through
+    the C ABI: host eigenverbs in, host biverbs out, device buffers made and
+    freed inside every call.  The first call counts, and sizes the output;
+    then 3 timed calls (wall clock)."""
+    import numpy as np
+    from underseamodelinglibrary_b200 import _abi
+    try:
+        lib = _abi.load_engine()
+        src, rcv, freq = biverb_inputs()
+        n = biverb_call(lib, "wq3d_biverbs", src, rcv, freq)
+        out = (_abi.wq3d_biverb * n)()
+        power = np.zeros((n, freq.size))
+        biverb_call(lib, "wq3d_biverbs", src, rcv, freq, out=out, out_power=power, capacity=n)
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            biverb_call(lib, "wq3d_biverbs", src, rcv, freq, out=out, out_power=power, capacity=n)
+            times.append(time.perf_counter() - t0)
+        t = min(times)
+        pairs = src[1].shape[0] * rcv[1].shape[0]
+        return {"workload": BIVERB_WORKLOAD, "source_eigenverbs": src[1].shape[0],
+                "receiver_eigenverbs": rcv[1].shape[0], "pairs": pairs, "biverbs": n,
+                "ms_e2e": t * 1000.0, "pairs_per_s": pairs / t, "biverbs_per_s": n / t,
+                "timing": "wall clock of the whole C-ABI call, best of 3 (host buffers in and out)"}
     except Exception as e:  # a failure here must not hide the headline line
         return {"error": "%s: %s" % (type(e).__name__, e)}
 
@@ -542,6 +610,18 @@ def cpu_baseline(args):
         mv, mdt, mn = cpu_run(m, 1)
         out["munk_flat"] = {"seconds": mdt, "ray_steps_per_s": mv, "steps": mn, "cores": 1,
                             "kind": "port"}
+    # the biverb workload's first 4000 receiver eigenverbs against all
+    # 57,600 source eigenverbs, 1 thread
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_binding import load_oracle
+    src, rcv, freq = biverb_inputs()
+    k = 4000
+    t0 = time.perf_counter()
+    nb = biverb_call(load_oracle(), "oracle_biverbs", src, rcv, freq, num_rcv=k)
+    dt_b = time.perf_counter() - t0
+    out["biverbs"] = {"pairs_per_s": src[1].shape[0] * k / dt_b, "seconds": dt_b, "biverbs": nb,
+                      "cores": 1, "kind": "port",
+                      "sample": "first %d of %d receiver eigenverbs x all source eigenverbs" % (k, rcv[1].shape[0])}
     return out
 
 

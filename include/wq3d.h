@@ -470,6 +470,62 @@ int wq3d_queue_timing(wq3d_queue* q, wq3d_timing* out, int reset);
 int wq3d_queue_set_timing(wq3d_queue* q, int on);
 
 /* ------------------------------------------------------------------ */
+/* bistatic eigenverbs (biverbs/)                                      */
+/* ------------------------------------------------------------------ */
+
+/* Scattering strength models of one interface
+ * (ocean/scattering_{constant,lambert,chapman}.h), chosen per interface the
+ * way ocean_model::scattering does (ocean/ocean_model.h:88-112). */
+enum {
+    WQ3D_SCATTER_CONSTANT = 0, /* p = strength in dB (scattering_constant.h) */
+    WQ3D_SCATTER_LAMBERT = 1,  /* p = bss in dB: 10^(bss/10) |sin a sin b|
+                                  (scattering_lambert.h)                  */
+    WQ3D_SCATTER_CHAPMAN = 2   /* p = wind speed, m/s (scattering_chapman.h) */
+};
+typedef struct wq3d_scattering_desc {
+    int32_t kind;
+    int32_t pad;
+    double p;
+} wq3d_scattering_desc;
+
+/* One bistatic eigenverb (biverbs/biverb_model.h): the overlap of a
+ * source eigenverb and a receiver eigenverb on one interface.  The power
+ * for each frequency is returned beside it. */
+typedef struct wq3d_biverb {
+    double travel_time;        /* source + receiver travel time, s        */
+    double duration;           /* s                                       */
+    double source_de;          /* rad                                     */
+    double source_az;
+    double receiver_de;
+    double receiver_az;
+    int32_t de_index;          /* the receiver eigenverb's                */
+    int32_t az_index;
+    int32_t source_surface, source_bottom, source_caustic, source_upper, source_lower;
+    int32_t receiver_surface, receiver_bottom, receiver_caustic, receiver_upper, receiver_lower;
+    int32_t source;            /* index of the source eigenverb           */
+    int32_t receiver;          /* index of the receiver eigenverb         */
+} wq3d_biverb;
+
+/* The biverbs of one interface (biverb_generator::run,
+ * biverbs/biverb_generator.cc:50-72, with biverb_collection::add_biverb,
+ * biverbs/biverb_collection.cc:44-172).  For every receiver eigenverb, the
+ * source eigenverbs whose centres lie strictly inside its search
+ * quadrilateral (eigenverb_collection::find_eigenverbs,
+ * eigenverbs/eigenverb_collection.cc:60-93, corners search_scale x length
+ * and width away) are overlapped with it; pairs whose largest power over
+ * frequency is below power_threshold are dropped.  Results come back in
+ * (receiver, source) index order, at most `capacity` of them; *count is the
+ * number that exist (with out == NULL only *count is computed).  Arrays are
+ * host memory: src_power is num_src x num_freq, rcv_power num_rcv x
+ * num_freq, out_power capacity x num_freq.  A count above capacity
+ * returns WQ3D_ERR_OVERFLOW after filling the first `capacity`. */
+int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, size_t num_src,
+                 const wq3d_eigenverb* rcv, const double* rcv_power, size_t num_rcv,
+                 const double* freq, size_t num_freq, const wq3d_scattering_desc* scattering,
+                 double earth_radius, double search_scale, double power_threshold,
+                 wq3d_biverb* out, double* out_power, size_t capacity, size_t* count);
+
+/* ------------------------------------------------------------------ */
 /* misc                                                                */
 /* ------------------------------------------------------------------ */
 const char* wq3d_last_error_string(void);

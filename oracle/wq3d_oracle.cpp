@@ -17,6 +17,9 @@
  *   waveq3d/spreading_hybrid_gaussian.cc, waveq3d/spreading_ray.cc
  *   ocean/profile_*.cc, boundary_{flat,slope}.cc, reflect_loss_*.{h,cc},
  *   attenuation_{thorp,constant}.cc, types/wvector1.cc
+ *   biverbs/biverb_generator.cc, biverbs/biverb_collection.cc,
+ *   eigenverbs/eigenverb_collection.cc (find_eigenverbs),
+ *   ocean/scattering_{constant,lambert,chapman}.h, types/wposition1.cc
  * Each function cites the file:line it follows.  Reference quirks are kept
  * on purpose (they are listed where they occur).
  *
@@ -2276,6 +2279,224 @@ int oracle_reflect_loss(const wq3d_ocean_desc* od, int which, size_t n,
     for (size_t i = 0; i < n; ++i)
         reflect_loss(b, fv, grazing[i], amp + i * nf, phase ? phase + i * nf : nullptr);
     return WQ3D_OK;
+}
+
+}  // extern "C"
+
+/* ------------------------------------------------------------------ */
+/* bistatic eigenverbs                                                 */
+/* ------------------------------------------------------------------ */
+namespace {
+
+double bv_to_degrees(double t) { return t * (180.0 / M_PI); }
+double bv_to_radians(double t) { return t * (M_PI / 180.0); }
+
+/* wposition1 with the reference's getters and setters (types/wposition1.h) */
+struct BvPos {
+    double rho, theta, phi, R0;
+    double latitude() const { return 90.0 - bv_to_degrees(theta); }
+    double longitude() const { return bv_to_degrees(phi); }
+    double altitude() const { return rho - R0; }
+    void latitude(double v) { theta = bv_to_radians(90.0 - v); }
+    void longitude(double v) { phi = bv_to_radians(v); }
+    void altitude(double v) { rho = v + R0; }
+};
+
+/* wposition1(location, range, bearing) (types/wposition1.cc:23-37) */
+BvPos bv_move(const BvPos& location, double range, double bearing) {
+    const double lat1 = bv_to_radians(location.latitude());
+    const double lng1 = bv_to_radians(location.longitude());
+    const double R = location.R0 + location.altitude();
+    range /= R;
+    const double lat2 = std::asin(std::sin(lat1) * std::cos(range) + std::cos(lat1) * std::sin(range) * std::cos(bearing));
+    const double lng2 = lng1 + std::atan2(std::sin(bearing) * std::sin(range) * std::cos(lat1),
+                                          std::cos(range) - std::sin(lat1) * std::sin(lat2));
+    BvPos p = location;
+    p.latitude(bv_to_degrees(lat2));
+    p.longitude(bv_to_degrees(lng2));
+    p.altitude(location.altitude());
+    return p;
+}
+
+/* wposition1::gc_range (types/wposition1.cc:57-92) */
+double bv_gc_range(const BvPos& self, const BvPos& location, double* bearing) {
+    const double lat1 = bv_to_radians(self.latitude());
+    const double lng1 = bv_to_radians(self.longitude());
+    const double R = self.R0 + self.altitude();
+    const double lat2 = bv_to_radians(location.latitude());
+    const double lng2 = bv_to_radians(location.longitude());
+    double hav1at = std::sin(0.5 * (lat1 - lat2));
+    hav1at *= hav1at;
+    double havlng = std::sin(0.5 * (lng1 - lng2));
+    havlng *= havlng;
+    const double range = 2.0 * std::asin(std::sqrt(hav1at + std::cos(lat1) * std::cos(lat2) * havlng));
+    if (std::abs(range) < 1e-6 || std::abs(lat1) < 1e-10) {
+        *bearing = (lat1 > 0) ? M_PI : 0.0;
+    } else {
+        *bearing = std::atan2(std::sin(lng1 - lng2) * std::cos(lat2),
+                              std::cos(lat1) * std::sin(lat2) - std::sin(lat1) * std::cos(lat2) * std::cos(lng1 - lng2));
+        *bearing = std::fmod(2.0 * M_PI - *bearing, 2.0 * M_PI);
+    }
+    return range * R;
+}
+
+BvPos bv_pos(const wq3d_eigenverb& v, double R0) { return BvPos{v.position[0], v.position[1], v.position[2], R0}; }
+
+/* eigenverb_collection::find_eigenverbs (eigenverb_collection.cc:60-93):
+ * the search quadrilateral A-B-C-D of a bounding eigenverb, as (latitude,
+ * longitude) corners */
+struct BvQuad {
+    double x[4], y[4];
+};
+
+BvQuad bv_quad(const wq3d_eigenverb& bounding, double R0, double search_scale) {
+    const BvPos pos = bv_pos(bounding, R0);
+    const double d = bounding.direction;
+    const BvPos c[4] = {bv_move(pos, search_scale * bounding.length, d),
+                        bv_move(pos, search_scale * bounding.width, d + M_PI_2),
+                        bv_move(pos, search_scale * bounding.length, d + M_PI),
+                        bv_move(pos, search_scale * bounding.width, d + M_PI + M_PI_2)};
+    BvQuad q;
+    for (int k = 0; k < 4; ++k) {
+        q.x[k] = c[k].latitude();
+        q.y[k] = c[k].longitude();
+    }
+    return q;
+}
+
+/* a centre strictly inside the quadrilateral (bgi::within); the sources
+ * are tested in index order */
+bool bv_found(const BvQuad& q, const wq3d_eigenverb& v, double R0) {
+    const BvPos p = bv_pos(v, R0);
+    const double x = p.latitude(), y = p.longitude();
+    int pos_n = 0, neg_n = 0;
+    for (int k = 0; k < 4; ++k) {
+        const int k2 = (k + 1) % 4;
+        const double cr = (q.x[k2] - q.x[k]) * (y - q.y[k]) - (q.y[k2] - q.y[k]) * (x - q.x[k]);
+        pos_n += cr > 0.0;
+        neg_n += cr < 0.0;
+    }
+    return pos_n == 4 || neg_n == 4;
+}
+
+/* ocean/scattering_{constant,lambert,chapman}.h, single-point forms */
+void bv_scattering(const wq3d_scattering_desc& m, const std::vector<double>& freq, double de_incident,
+                   double de_scattered, std::vector<double>& amp) {
+    amp.assign(freq.size(), 0.0);
+    if (m.kind == WQ3D_SCATTER_CONSTANT) {
+        const double a = std::pow(10.0, m.p / 10.0);
+        for (auto& v : amp) v = a;
+    } else if (m.kind == WQ3D_SCATTER_LAMBERT) {
+        const double coeff = std::pow(10.0, m.p / 10.0);
+        for (auto& v : amp) v = std::abs(coeff * std::sin(de_incident) * std::sin(de_scattered));
+    } else {
+        const double grazing = 0.5 * (de_incident + de_scattered) * 180.0 / M_PI;
+        const double speed = m.p * 1.94384449;
+        for (size_t f = 0; f < freq.size(); ++f) {
+            const double beta = 158.0 * std::pow(speed * std::pow(freq[f], 1.0 / 3.0), -0.58);
+            const double a = 2.6 - 42.4 * std::log10(beta) + 3.3 * beta * std::log10(grazing / 30.0 + 1e-6);
+            amp[f] = std::pow(10.0, a / 10.0);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+/* biverb_generator::run for one interface (biverb_generator.cc:50-72)
+ * with biverb_collection::add_biverb (biverb_collection.cc:44-172);
+ * records in (receiver, source) order, as wq3d_biverbs returns them */
+int oracle_biverbs(const wq3d_eigenverb* src, const double* src_power, size_t num_src,
+                   const wq3d_eigenverb* rcv, const double* rcv_power, size_t num_rcv,
+                   const double* freq, size_t num_freq, const wq3d_scattering_desc* scattering,
+                   double earth_radius, double search_scale, double power_threshold,
+                   wq3d_biverb* out, double* out_power, size_t capacity, size_t* count) {
+    const std::vector<double> fv(freq, freq + num_freq);
+    std::vector<double> scatter, power(num_freq);
+    size_t n = 0;
+    for (size_t ri = 0; ri < num_rcv; ++ri) {
+        const wq3d_eigenverb& r = rcv[ri];
+        const BvQuad quad = bv_quad(r, earth_radius, search_scale);
+        for (size_t si = 0; si < num_src; ++si) {
+            const wq3d_eigenverb& s = src[si];
+            if (!bv_found(quad, s, earth_radius)) continue;
+            bv_scattering(*scattering, fv, s.grazing, r.grazing, scatter);
+
+            double bearing;
+            const double range = bv_gc_range(bv_pos(r, earth_radius), bv_pos(s, earth_radius), &bearing);
+            if (range < 1e-6) bearing = 0;
+            bearing -= r.direction;
+            const double ys = range * std::cos(bearing);
+            const double ys2 = ys * ys;
+            const double xs = range * std::sin(bearing);
+            const double xs2 = xs * xs;
+
+            const double alpha = s.direction - r.direction;
+            const double cos2alpha = std::cos(2.0 * alpha);
+            const double sin2alpha = std::sin(2.0 * alpha);
+            const double src_length2 = s.length * s.length;
+            const double src_width2 = s.width * s.width;
+            const double src_sum = src_length2 + src_width2;
+            const double src_diff = src_length2 - src_width2;
+            const double src_prod = src_length2 * src_width2;
+            const double rcv_length2 = r.length * r.length;
+            const double rcv_width2 = r.width * r.width;
+            const double rcv_sum = rcv_length2 + rcv_width2;
+            const double rcv_diff = rcv_length2 - rcv_width2;
+            const double rcv_prod = rcv_length2 * rcv_width2;
+
+            double det_sr = 0.5 * (2.0 * (src_prod + rcv_prod) + (src_sum * rcv_sum) - (src_diff * rcv_diff) * cos2alpha);
+            for (size_t f = 0; f < num_freq; ++f)
+                power[f] = 0.25 * 0.5 * src_power[si * num_freq + f] * rcv_power[ri * num_freq + f] * scatter[f];
+            const double new_prod = src_diff * cos2alpha;
+            const double kappa = -0.25 *
+                                 (xs2 * (src_sum + new_prod + 2.0 * rcv_length2) +
+                                  ys2 * (src_sum - new_prod + 2.0 * rcv_width2) -
+                                  2.0 * std::sqrt(xs2 * ys2) * src_diff * sin2alpha) /
+                                 det_sr;
+            const double overlap_scale = std::exp(kappa) / std::sqrt(det_sr);
+            double pmax = 0.0;
+            for (size_t f = 0; f < num_freq; ++f) {
+                power[f] *= overlap_scale;
+                pmax = std::max(pmax, std::abs(power[f]));
+            }
+            det_sr = det_sr / (src_prod * rcv_prod);
+            const double sigma = 0.5 *
+                                 ((1.0 / src_width2 + 1.0 / src_length2) +
+                                  (1.0 / src_width2 - 1.0 / src_length2) * cos2alpha + 2.0 / rcv_width2) /
+                                 det_sr;
+            const double factor = std::cos(r.grazing) / r.sound_speed;
+            if (!(pmax >= power_threshold)) continue;
+            if (out && n < capacity) {
+                wq3d_biverb& v = out[n];
+                v.travel_time = s.travel_time + r.travel_time;
+                v.duration = 0.5 * factor * std::sqrt(sigma);
+                v.source_de = s.source_de;
+                v.source_az = s.source_az;
+                v.receiver_de = r.source_de;
+                v.receiver_az = r.source_az;
+                v.de_index = r.de;
+                v.az_index = r.az;
+                v.source_surface = s.surface;
+                v.source_bottom = s.bottom;
+                v.source_caustic = s.caustic;
+                v.source_upper = s.upper;
+                v.source_lower = s.lower;
+                v.receiver_surface = r.surface;
+                v.receiver_bottom = r.bottom;
+                v.receiver_caustic = r.caustic;
+                v.receiver_upper = r.upper;
+                v.receiver_lower = r.lower;
+                v.source = (int32_t)si;
+                v.receiver = (int32_t)ri;
+                for (size_t f = 0; f < num_freq; ++f) out_power[n * num_freq + f] = power[f];
+            }
+            ++n;
+        }
+    }
+    *count = n;
+    return (out && n > capacity) ? WQ3D_ERR_OVERFLOW : WQ3D_OK;
 }
 
 }  // extern "C"

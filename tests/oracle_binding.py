@@ -44,6 +44,7 @@ SIGS = {
                                       C.c_size_t, dp, dp, dp]),
     "oracle_attenuation": (C.c_int, [C.POINTER(_abi.wq3d_ocean_desc), C.c_double, C.c_size_t, dp, dp,
                                      C.c_size_t, dp, dp]),
+    "oracle_biverbs": _abi.SIGNATURES["wq3d_biverbs"],
     "oracle_last_error_string": (C.c_char_p, []),
 }
 

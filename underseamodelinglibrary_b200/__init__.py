@@ -14,12 +14,13 @@ from .ocean import (attenuation_thorp, attenuation_constant, profile_linear,
                     profile_munk, profile_catenary, profile_n2, reflect_loss_constant,
                     reflect_loss_rayleigh, reflect_loss_eckart, boundary_flat,
                     boundary_slope, ocean_model, data_grid, profile_grid, boundary_grid,
-                    volume_flat)
+                    volume_flat, scattering_constant, scattering_lambert, scattering_chapman)
 from .waveq3d import (wave_queue, eigenray_listener, reflection_listener,
                       eigenray_model, eigenray_list, run_batch)
 from .eigenrays import eigenray_collection
 from .wavegen import run_wavefront_generators, wavefront_generator
 from .eigenverbs import eigenverb_model, eigenverb_listener, eigenverb_collection
+from .biverbs import biverb_model, biverb_collection, biverb_generator
 
 load_engine = _abi.load_engine
 EngineError = _abi.EngineError
@@ -32,9 +33,11 @@ __all__ = [
     "profile_linear", "profile_munk", "profile_catenary", "profile_n2",
     "reflect_loss_constant", "reflect_loss_rayleigh", "reflect_loss_eckart",
     "boundary_flat", "boundary_slope", "ocean_model", "data_grid", "profile_grid",
-    "boundary_grid", "volume_flat", "wave_queue", "run_batch",
+    "boundary_grid", "volume_flat", "scattering_constant", "scattering_lambert",
+    "scattering_chapman", "wave_queue", "run_batch",
     "eigenray_listener", "reflection_listener", "eigenray_model", "eigenray_list",
     "wavefront_generator", "run_wavefront_generators",
     "eigenray_collection", "eigenverb_model", "eigenverb_listener", "eigenverb_collection",
+    "biverb_model", "biverb_collection", "biverb_generator",
     "load_engine", "EngineError", "LIB_PATH",
 ]

@@ -120,6 +120,26 @@ class wq3d_eigenverb(C.Structure):
                 ("pad", C.c_int32)]
 
 
+SCATTER_CONSTANT, SCATTER_LAMBERT, SCATTER_CHAPMAN = 0, 1, 2
+
+
+class wq3d_scattering_desc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("pad", C.c_int32), ("p", C.c_double)]
+
+
+class wq3d_biverb(C.Structure):
+    _fields_ = [("travel_time", C.c_double), ("duration", C.c_double),
+                ("source_de", C.c_double), ("source_az", C.c_double),
+                ("receiver_de", C.c_double), ("receiver_az", C.c_double),
+                ("de_index", C.c_int32), ("az_index", C.c_int32),
+                ("source_surface", C.c_int32), ("source_bottom", C.c_int32),
+                ("source_caustic", C.c_int32), ("source_upper", C.c_int32),
+                ("source_lower", C.c_int32), ("receiver_surface", C.c_int32),
+                ("receiver_bottom", C.c_int32), ("receiver_caustic", C.c_int32),
+                ("receiver_upper", C.c_int32), ("receiver_lower", C.c_int32),
+                ("source", C.c_int32), ("receiver", C.c_int32)]
+
+
 ADD_EIGENRAY = C.CFUNCTYPE(None, C.c_void_p, C.c_size_t, C.c_size_t,
                            C.POINTER(wq3d_eigenray), dp, dp, C.c_size_t, C.c_uint64)
 CHECK_EIGENRAYS = C.CFUNCTYPE(None, C.c_void_p, C.c_double, C.c_uint64)
@@ -170,6 +190,10 @@ SIGNATURES = {
     "wq3d_queue_abort": (C.c_int, [C.c_void_p]),
     "wq3d_queue_timing": (C.c_int, [C.c_void_p, C.POINTER(wq3d_timing), C.c_int]),
     "wq3d_queue_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "wq3d_biverbs": (C.c_int, [C.POINTER(wq3d_eigenverb), dp, C.c_size_t, C.POINTER(wq3d_eigenverb), dp,
+                               C.c_size_t, dp, C.c_size_t, C.POINTER(wq3d_scattering_desc), C.c_double,
+                               C.c_double, C.c_double, C.POINTER(wq3d_biverb), dp, C.c_size_t,
+                               C.POINTER(C.c_size_t)]),
     "wq3d_last_error_string": (C.c_char_p, []),
     "wq3d_abi_version": (C.c_int, []),
     "wq3d_device_count": (C.c_int, [C.POINTER(C.c_int)]),

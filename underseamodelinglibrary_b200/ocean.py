@@ -186,15 +186,65 @@ class reflect_loss_eckart:
         self.params = (float(wind_speed), 0.0, 0.0, 0.0, 0.0)
 
 
+class scattering_model:
+    """Scattering strength of an interface (ocean/scattering_model.h),
+    evaluated on the GPU by the bistatic eigenverb kernels."""
+    kind = None
+
+    def __init__(self, p):
+        self.p = float(p)
+
+    def desc(self):
+        d = _abi.wq3d_scattering_desc()
+        d.kind = self.kind
+        d.p = self.p
+        return d
+
+
+class scattering_constant(scattering_model):
+    """scattering_constant(amplitude=-300) (ocean/scattering_constant.h):
+    the same strength, in dB, at every angle and frequency."""
+    kind = _abi.SCATTER_CONSTANT
+
+    def __init__(self, amplitude=-300.0):
+        super().__init__(amplitude)
+
+
+class scattering_lambert(scattering_model):
+    """scattering_lambert(bss=-27) (ocean/scattering_lambert.h):
+    10^(bss/10) |sin(de_incident) sin(de_scattered)|."""
+    kind = _abi.SCATTER_LAMBERT
+
+    def __init__(self, bss=-27.0):
+        super().__init__(bss)
+
+
+class scattering_chapman(scattering_model):
+    """scattering_chapman(wind_speed) (ocean/scattering_chapman.h): the
+    Chapman-Harris surface scattering strength for a wind speed in m/s."""
+    kind = _abi.SCATTER_CHAPMAN
+
+    def __init__(self, wind_speed):
+        super().__init__(wind_speed)
+
+
 class boundary_model:
     kind = None
 
-    def __init__(self, reflect_loss=None):
+    def __init__(self, reflect_loss=None, scattering=None):
         self._loss = reflect_loss
+        self._scattering = scattering if scattering is not None else scattering_constant()
         self._radius = earth_radius()
 
     def reflect_loss(self, model):
         self._loss = model
+
+    def scattering(self, model=None):
+        """boundary_model::scattering: the interface's scattering strength
+        model (scattering_constant(-300 dB) unless one is given)"""
+        if model is None:
+            return self._scattering
+        self._scattering = model
 
     def fill(self, d):
         d.kind = self.kind
@@ -207,11 +257,12 @@ class boundary_model:
 
 
 class boundary_flat(boundary_model):
-    """boundary_flat(depth=0, reflect_loss) (boundary_flat.cc:19-31)."""
+    """boundary_flat(depth=0, reflect_loss, scattering) (boundary_flat.cc:
+    19-31)."""
     kind = _abi.BOUNDARY_FLAT
 
-    def __init__(self, depth=0.0, reflect_loss=None):
-        super().__init__(reflect_loss)
+    def __init__(self, depth=0.0, reflect_loss=None, scattering=None):
+        super().__init__(reflect_loss, scattering)
         self.depth = float(depth)
 
     def fill(self, d):
@@ -225,8 +276,8 @@ class boundary_slope(boundary_model):
     caller's location; this copies it."""
     kind = _abi.BOUNDARY_SLOPE
 
-    def __init__(self, location, depth, lat_slope, lng_slope=0.0, reflect_loss=None):
-        super().__init__(reflect_loss)
+    def __init__(self, location, depth, lat_slope, lng_slope=0.0, reflect_loss=None, scattering=None):
+        super().__init__(reflect_loss, scattering)
         self.location = (location.rho, location.theta, location.phi)
         self.depth = float(depth)
         self.lat_slope = float(lat_slope)
@@ -246,8 +297,8 @@ class boundary_grid(boundary_model):
     grid over theta[, phi]; Rayleigh sand loss unless one is given."""
     kind = _abi.BOUNDARY_GRID
 
-    def __init__(self, grid, reflect_loss=None):
-        super().__init__(reflect_loss)
+    def __init__(self, grid, reflect_loss=None, scattering=None):
+        super().__init__(reflect_loss, scattering)
         self.grid = grid
 
     def fill(self, d, keep=None):
@@ -256,13 +307,22 @@ class boundary_grid(boundary_model):
 
 
 class volume_flat:
-    """volume_flat(depth, thickness, amplitude) (ocean/volume_flat.h:32-37):
-    a scattering layer at a constant depth below mean sea level."""
+    """volume_flat(depth, thickness, amplitude) (ocean/volume_flat.h:32-37)
+    or volume_flat(depth, thickness, scattering) (volume_flat.h:47-50): a
+    scattering layer at a constant depth below mean sea level."""
 
     def __init__(self, depth=0.0, thickness=0.0, amplitude=-300.0):
         self.depth = float(depth)
         self.thickness = float(thickness)
-        self.amplitude = float(amplitude)
+        if isinstance(amplitude, scattering_model):
+            self._scattering = amplitude
+            self.amplitude = amplitude.p if amplitude.kind == _abi.SCATTER_CONSTANT else -300.0
+        else:
+            self.amplitude = float(amplitude)
+            self._scattering = scattering_constant(self.amplitude)
+
+    def scattering(self):
+        return self._scattering
 
 
 class ocean_model:
@@ -290,6 +350,16 @@ class ocean_model:
 
     def num_volume(self):
         return len(self._volume)
+
+    def scattering_model(self, interface):
+        """the scattering strength model of an interface, chosen as
+        ocean_model::scattering does (ocean/ocean_model.h:88-112): 0 bottom,
+        1 surface, 2 + 2k and 3 + 2k the two sides of volume layer k"""
+        if interface == 0:
+            return self._bottom.scattering()
+        if interface == 1:
+            return self._surface.scattering()
+        return self._volume[(int(interface) - 2) // 2].scattering()
 
     def volume(self, n):
         return self._volume[n]

@@ -406,3 +406,49 @@ def build_queue(sc, queue_cls, **kw):
     for name, value in sc.get("thresholds", {}).items():
         getattr(q, name)(value)
     return q
+
+
+def analytic_footprints(sensor_lat, sensor_lng, depth, de_values, az_values, num_freq):
+    """Bottom eigenverbs of a sensor on the surface of isovelocity 1500 m/s
+    water, in the shape of the reference's biverb test footprints
+    (biverbs/test/biverbs_test.cc:41-77): for every (D/E, AZ) in degrees a
+    footprint where the ray meets a flat bottom `depth` metres down, sized
+    by the fan spacing, with power length x width / slant range^2 at every
+    frequency.  Returns (wq3d_eigenverb array, power (n, num_freq)), built
+    with numpy for large fans."""
+    from . import _abi
+    de = np.asarray(de_values, dtype=np.float64)
+    az = np.asarray(az_values, dtype=np.float64)
+    de_spacing = float(de[1] - de[0]) if de.size > 1 else 1.0
+    az_spacing = float(az[1] - az[0]) if az.size > 1 else 1.0
+    DE, AZ = np.meshgrid(de, az)            # AZ-major, as the reference's loops
+    DE, AZ = DE.ravel(), AZ.ravel()
+    n = DE.size
+    de_rad, az_rad = np.radians(DE), np.radians(AZ)
+    grazing = np.abs(de_rad)
+    slant = depth / np.sin(grazing)
+    horz = depth / np.tan(grazing)
+    length = 0.5 * slant * math.radians(de_spacing) / np.sin(grazing)
+    width = 0.5 * slant * math.radians(az_spacing) * np.cos(grazing)
+    R = T.earth_radius()
+    lat1, lng1 = math.radians(sensor_lat), math.radians(sensor_lng)
+    rng = horz / R
+    lat2 = np.arcsin(math.sin(lat1) * np.cos(rng) + math.cos(lat1) * np.sin(rng) * np.cos(az_rad))
+    lng2 = lng1 + np.arctan2(np.sin(az_rad) * np.sin(rng) * math.cos(lat1),
+                             np.cos(rng) - math.sin(lat1) * np.sin(lat2))
+    recs = (_abi.wq3d_eigenverb * max(n, 1))()
+    a = np.ctypeslib.as_array(recs)[:n]
+    a["travel_time"] = slant / 1500.0
+    a["length"] = length
+    a["width"] = width
+    pos = np.stack([np.full(n, R - depth), np.pi / 2 - lat2, lng2], axis=1)
+    a["position"] = pos
+    a["direction"] = az_rad
+    a["grazing"] = grazing
+    a["sound_speed"] = 1500.0
+    a["source_de"] = de_rad
+    a["source_az"] = az_rad
+    a["de"] = np.round((90.0 + DE) / de_spacing - 1.0).astype(np.int32)
+    a["az"] = np.round(AZ / az_spacing).astype(np.int32)
+    power = np.repeat((length * width / (slant * slant))[:, None], num_freq, axis=1)
+    return recs, np.ascontiguousarray(power)
