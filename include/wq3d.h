@@ -518,7 +518,9 @@ typedef struct wq3d_biverb {
  * number that exist (with out == NULL only *count is computed).  Arrays are
  * host memory: src_power is num_src x num_freq, rcv_power num_rcv x
  * num_freq, out_power capacity x num_freq.  A count above capacity
- * returns WQ3D_ERR_OVERFLOW after filling the first `capacity`. */
+ * returns WQ3D_ERR_OVERFLOW after filling the first `capacity`.  Runs on the
+ * current device; its device buffers stay allocated for the next call on
+ * that device (they only grow), and calls on one device are serialised. */
 int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, size_t num_src,
                  const wq3d_eigenverb* rcv, const double* rcv_power, size_t num_rcv,
                  const double* freq, size_t num_freq, const wq3d_scattering_desc* scattering,

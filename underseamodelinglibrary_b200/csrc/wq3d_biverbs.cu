@@ -10,16 +10,20 @@
  * adds the Gaussian overlap to a collection
  * (biverbs/biverb_collection.cc:44-172).
  *
- * Here every (receiver, source) pair is tested on the GPU.  One warp owns
- * one receiver: its search quadrilateral and bounding box are computed
- * once (k_biverb_boxes), the source centres stream through shared memory
- * in tiles that all eight warps of a block share, a bounding-box test
- * rejects most pairs before the four edge tests, and only pairs inside the
- * quadrilateral evaluate the overlap.  Two passes keep the output order
- * fixed without atomics: the first counts each receiver's surviving pairs,
- * the host turns the counts into offsets, and the second writes every
- * pair at its receiver's offset plus its rank among the warp's hits
- * (ballot + popc), in source index order.
+ * Here every (receiver, source) pair is screened on the GPU.  One warp
+ * owns one receiver: its search quadrilateral and bounding box are
+ * computed once (k_biverb_boxes).  The sources are cut into groups of 32
+ * consecutive ones with a bounding box each (k_biverb_groups); the warp
+ * tests 32 group boxes at once against its receiver's box, one per lane,
+ * and visits only the groups that may hold a hit, each lane taking one
+ * source.  A bounding-box test rejects most of their pairs before the four
+ * edge tests, and only pairs inside the quadrilateral evaluate the
+ * overlap.  No shared memory and no block barrier are involved, so warps
+ * run independently.
+ * Two passes keep the output order fixed without atomics: the first counts
+ * each receiver's surviving pairs, the host turns the counts into offsets,
+ * and the second writes every pair at its receiver's offset plus its rank
+ * among the warp's hits (ballot + popc), in source index order.
  *
  * The work is FP64 scalar arithmetic on records that are read once per
  * tile; the pair tests are compute-bound on the FP64 pipe, not on HBM.
@@ -27,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <mutex>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -38,7 +43,6 @@ extern "C" void wq3d_internal_set_error(const char* msg);
 namespace {
 
 constexpr int BV_WARPS = 8;    /* receivers per block, one warp each   */
-constexpr int BV_TILE = 512;   /* source centres staged per tile      */
 constexpr int BV_BOX = 12;     /* doubles per receiver box            */
 
 int bv_fail(int code, const std::string& msg) {
@@ -76,6 +80,7 @@ struct BvArgs {
     const wq3d_eigenverb* rcv;
     const double* rcv_pow;
     const double* box;      /* BV_BOX doubles per receiver */
+    const double* groups;   /* per group of 32 sources: latitude min, max, longitude min, max */
     int nr;
     int nf;
     int kind;
@@ -111,6 +116,32 @@ __global__ void k_biverb_boxes(const BvArgs a, double search_scale, double* box,
         sx[i] = 90.0 - bv_deg(a.src[i].position[1]);
         sy[i] = bv_deg(a.src[i].position[2]);
     }
+}
+
+/* the bounding box (latitude min, max, longitude min, max) of each group
+ * of 32 consecutive source centres, one warp per group */
+__global__ void __launch_bounds__(256) k_biverb_groups(const double* sx, const double* sy, int ns, double* groups) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = {INFINITY, -INFINITY, INFINITY, -INFINITY};
+    if (i < ns) {
+        v[0] = v[1] = sx[i];
+        v[2] = v[3] = sy[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        v[0] = fmin(v[0], __shfl_xor_sync(0xffffffffu, v[0], o));
+        v[1] = fmax(v[1], __shfl_xor_sync(0xffffffffu, v[1], o));
+        v[2] = fmin(v[2], __shfl_xor_sync(0xffffffffu, v[2], o));
+        v[3] = fmax(v[3], __shfl_xor_sync(0xffffffffu, v[3], o));
+    }
+    const int g = i >> 5;
+    if ((threadIdx.x & 31) == 0 && (g << 5) < ns)
+        for (int k = 0; k < 4; ++k) groups[4 * (size_t)g + k] = v[k];
+}
+
+/* a box (latitude min, max, longitude min, max) that holds no point
+ * strictly inside the receiver box b[8..11] */
+__device__ __forceinline__ bool bv_misses(const double* box, const double* b) {
+    return box[1] <= b[8] || box[0] >= b[9] || box[3] <= b[10] || box[2] >= b[11];
 }
 
 /* strictly inside the quadrilateral: all four edge cross products have
@@ -218,45 +249,41 @@ __device__ __forceinline__ double bv_power(const BvArgs& a, int si, int ri, int 
 
 template <bool WRITE>
 __global__ void __launch_bounds__(BV_WARPS * 32) k_biverb_pairs(const BvArgs a) {
-    __shared__ double s_x[BV_TILE];
-    __shared__ double s_y[BV_TILE];
-    const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int ri = blockIdx.x * BV_WARPS + warp;
-    const bool live = ri < a.nr;
+    const int ri = blockIdx.x * BV_WARPS + (threadIdx.x >> 5);
+    if (ri >= a.nr) return;  /* a whole warp: no block barrier follows */
     double b[BV_BOX];
 #pragma unroll
-    for (int k = 0; k < BV_BOX; ++k) b[k] = live ? a.box[(size_t)ri * BV_BOX + k] : 0.0;
-    const long long base = (WRITE && live) ? a.offs[ri] : 0;
+    for (int k = 0; k < BV_BOX; ++k) b[k] = a.box[(size_t)ri * BV_BOX + k];
+    const long long base = WRITE ? a.offs[ri] : 0;
     const unsigned below = (1u << lane) - 1u;
+    const int ngroups = (a.ns + 31) >> 5;
     long long n = 0;
-    for (int t0 = 0; t0 < a.ns; t0 += BV_TILE) {
-        const int m = min(BV_TILE, a.ns - t0);
-        __syncthreads();
-        for (int i = threadIdx.x; i < m; i += blockDim.x) {
-            s_x[i] = a.sx[t0 + i];
-            s_y[i] = a.sy[t0 + i];
-        }
-        __syncthreads();
-        if (!live) continue;
-        const int rounds = (m + 31) >> 5;
-        for (int q = 0; q < rounds; ++q) {
-            const int j = (q << 5) + lane;
+    /* a centre strictly inside the quadrilateral lies strictly inside the
+     * receiver's bounding box: each lane tests one group box, and the warp
+     * visits the groups that may hold a hit in increasing order */
+    for (int g0 = 0; g0 < ngroups; g0 += 32) {
+        const int gl = g0 + lane;
+        const bool need = gl < ngroups && !bv_misses(a.groups + 4 * (size_t)gl, b);
+        unsigned todo = __ballot_sync(0xffffffffu, need);
+        while (todo) {
+            const int g = g0 + __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int si = (g << 5) + lane;
             bool hit = false;
             BvOverlap o{0.0, 0.0};
-            if (j < m && bv_inside(b, s_x[j], s_y[j])) {
-                const wq3d_eigenverb& s = a.src[t0 + j];
+            if (si < a.ns && bv_inside(b, a.sx[si], a.sy[si])) {
+                const wq3d_eigenverb& s = a.src[si];
                 const wq3d_eigenverb& r = a.rcv[ri];
                 o = bv_overlap(s, r, a.R0);
                 double pmax = 0.0;
-                for (int f = 0; f < a.nf; ++f) pmax = fmax(pmax, fabs(bv_power(a, t0 + j, ri, f, o.scale, s.grazing, r.grazing)));
+                for (int f = 0; f < a.nf; ++f) pmax = fmax(pmax, fabs(bv_power(a, si, ri, f, o.scale, s.grazing, r.grazing)));
                 hit = pmax >= a.threshold;
             }
             const unsigned bal = __ballot_sync(0xffffffffu, hit);
             if (WRITE && hit) {
                 const long long k = base + n + __popc(bal & below);
                 if (k < a.cap) {
-                    const int si = t0 + j;
                     const wq3d_eigenverb& s = a.src[si];
                     const wq3d_eigenverb& r = a.rcv[ri];
                     wq3d_biverb v;
@@ -288,31 +315,43 @@ __global__ void __launch_bounds__(BV_WARPS * 32) k_biverb_pairs(const BvArgs a) 
             n += __popc(bal);
         }
     }
-    if (!WRITE && live && lane == 0) a.counts[ri] = n;
+    if (!WRITE && lane == 0) a.counts[ri] = n;
 }
 
-/* device buffers freed on every exit path */
-struct BvBuffers {
-    std::vector<void*> ptrs;
-    ~BvBuffers() {
-        for (void* p : ptrs) cudaFree(p);
-    }
+/* Device buffers and a stream kept per device from one call to the next,
+ * so that a call allocates nothing once the buffers are large enough
+ * (they only grow, by a quarter more than asked).  The mutex serialises
+ * calls on one device.  The buffers live until the process exits. */
+constexpr int BV_MAX_DEVICES = 64;
+enum { BV_SRC, BV_RCV, BV_SPOW, BV_RPOW, BV_SX, BV_SY, BV_BOXES, BV_GROUPS_BUF, BV_COUNTS, BV_CHAP,
+       BV_OFFS, BV_OUT, BV_OPOW, BV_NBUF };
+
+struct BvWorkspace {
+    std::mutex m;
+    cudaStream_t s = nullptr;
+    void* p[BV_NBUF] = {};
+    size_t cap[BV_NBUF] = {};
     template <class T>
-    cudaError_t alloc(T** p, size_t n) {
-        void* v = nullptr;
-        const cudaError_t e = cudaMalloc(&v, n ? n * sizeof(T) : 1);
-        if (e == cudaSuccess) ptrs.push_back(v);
-        *p = static_cast<T*>(v);
-        return e;
+    cudaError_t get(int k, T** out, size_t n) {
+        const size_t bytes = (n ? n : 1) * sizeof(T);
+        if (bytes > cap[k]) {
+            if (p[k]) cudaFree(p[k]);
+            p[k] = nullptr;
+            cap[k] = 0;
+            const size_t want = bytes + bytes / 4;
+            const cudaError_t e = cudaMalloc(&p[k], want);
+            if (e != cudaSuccess) {
+                p[k] = nullptr;
+                return e;
+            }
+            cap[k] = want;
+        }
+        *out = static_cast<T*>(p[k]);
+        return cudaSuccess;
     }
 };
 
-struct BvStream {
-    cudaStream_t s = nullptr;
-    ~BvStream() {
-        if (s) cudaStreamDestroy(s);
-    }
-};
+BvWorkspace g_bv[BV_MAX_DEVICES];
 
 }  // namespace
 
@@ -358,27 +397,32 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
         a.coef = std::pow(10.0, scattering->p / 10.0);
     }
 
-    BvBuffers buf;
-    BvStream st;
-    BV_CK(cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking));
+    int dev = 0;
+    BV_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= BV_MAX_DEVICES) return bv_fail(WQ3D_ERR_CUDA, "device index out of range");
+    BvWorkspace& ws = g_bv[dev];
+    std::lock_guard<std::mutex> lock(ws.m);
+    if (!ws.s) BV_CK(cudaStreamCreateWithFlags(&ws.s, cudaStreamNonBlocking));
     wq3d_eigenverb *d_src, *d_rcv;
-    double *d_spow, *d_rpow, *d_sx, *d_sy, *d_box, *d_chap = nullptr;
+    double *d_spow, *d_rpow, *d_sx, *d_sy, *d_box, *d_groups, *d_chap = nullptr;
     long long* d_counts;
-    BV_CK(buf.alloc(&d_src, num_src));
-    BV_CK(buf.alloc(&d_rcv, num_rcv));
-    BV_CK(buf.alloc(&d_spow, num_src * num_freq));
-    BV_CK(buf.alloc(&d_rpow, num_rcv * num_freq));
-    BV_CK(buf.alloc(&d_sx, num_src));
-    BV_CK(buf.alloc(&d_sy, num_src));
-    BV_CK(buf.alloc(&d_box, num_rcv * BV_BOX));
-    BV_CK(buf.alloc(&d_counts, num_rcv));
-    if (!chap.empty()) BV_CK(buf.alloc(&d_chap, chap.size()));
-    BV_CK(cudaMemcpyAsync(d_src, src, num_src * sizeof(wq3d_eigenverb), cudaMemcpyHostToDevice, st.s));
-    BV_CK(cudaMemcpyAsync(d_rcv, rcv, num_rcv * sizeof(wq3d_eigenverb), cudaMemcpyHostToDevice, st.s));
-    BV_CK(cudaMemcpyAsync(d_spow, src_power, num_src * num_freq * sizeof(double), cudaMemcpyHostToDevice, st.s));
-    BV_CK(cudaMemcpyAsync(d_rpow, rcv_power, num_rcv * num_freq * sizeof(double), cudaMemcpyHostToDevice, st.s));
+    BV_CK(ws.get(BV_SRC, &d_src, num_src));
+    BV_CK(ws.get(BV_RCV, &d_rcv, num_rcv));
+    BV_CK(ws.get(BV_SPOW, &d_spow, num_src * num_freq));
+    BV_CK(ws.get(BV_RPOW, &d_rpow, num_rcv * num_freq));
+    BV_CK(ws.get(BV_SX, &d_sx, num_src));
+    BV_CK(ws.get(BV_SY, &d_sy, num_src));
+    BV_CK(ws.get(BV_BOXES, &d_box, num_rcv * BV_BOX));
+    const size_t num_groups = (num_src + 31) / 32;
+    BV_CK(ws.get(BV_GROUPS_BUF, &d_groups, num_groups * 4));
+    BV_CK(ws.get(BV_COUNTS, &d_counts, num_rcv));
+    if (!chap.empty()) BV_CK(ws.get(BV_CHAP, &d_chap, chap.size()));
+    BV_CK(cudaMemcpyAsync(d_src, src, num_src * sizeof(wq3d_eigenverb), cudaMemcpyHostToDevice, ws.s));
+    BV_CK(cudaMemcpyAsync(d_rcv, rcv, num_rcv * sizeof(wq3d_eigenverb), cudaMemcpyHostToDevice, ws.s));
+    BV_CK(cudaMemcpyAsync(d_spow, src_power, num_src * num_freq * sizeof(double), cudaMemcpyHostToDevice, ws.s));
+    BV_CK(cudaMemcpyAsync(d_rpow, rcv_power, num_rcv * num_freq * sizeof(double), cudaMemcpyHostToDevice, ws.s));
     if (d_chap)
-        BV_CK(cudaMemcpyAsync(d_chap, chap.data(), chap.size() * sizeof(double), cudaMemcpyHostToDevice, st.s));
+        BV_CK(cudaMemcpyAsync(d_chap, chap.data(), chap.size() * sizeof(double), cudaMemcpyHostToDevice, ws.s));
 
     a.src = d_src;
     a.src_pow = d_spow;
@@ -388,6 +432,7 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     a.rcv = d_rcv;
     a.rcv_pow = d_rpow;
     a.box = d_box;
+    a.groups = d_groups;
     a.nr = (int)num_rcv;
     a.nf = (int)num_freq;
     a.chap = d_chap;
@@ -396,14 +441,16 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     a.counts = d_counts;
 
     const size_t nmax = num_src > num_rcv ? num_src : num_rcv;
-    k_biverb_boxes<<<(unsigned)((nmax + 127) / 128), 128, 0, st.s>>>(a, search_scale, d_box, d_sx, d_sy);
+    k_biverb_boxes<<<(unsigned)((nmax + 127) / 128), 128, 0, ws.s>>>(a, search_scale, d_box, d_sx, d_sy);
+    BV_CK(cudaGetLastError());
+    k_biverb_groups<<<(unsigned)((num_src + 255) / 256), 256, 0, ws.s>>>(d_sx, d_sy, (int)num_src, d_groups);
     BV_CK(cudaGetLastError());
     const unsigned blocks = (unsigned)((num_rcv + BV_WARPS - 1) / BV_WARPS);
-    k_biverb_pairs<false><<<blocks, BV_WARPS * 32, 0, st.s>>>(a);
+    k_biverb_pairs<false><<<blocks, BV_WARPS * 32, 0, ws.s>>>(a);
     BV_CK(cudaGetLastError());
     std::vector<long long> counts(num_rcv);
-    BV_CK(cudaMemcpyAsync(counts.data(), d_counts, num_rcv * sizeof(long long), cudaMemcpyDeviceToHost, st.s));
-    BV_CK(cudaStreamSynchronize(st.s));
+    BV_CK(cudaMemcpyAsync(counts.data(), d_counts, num_rcv * sizeof(long long), cudaMemcpyDeviceToHost, ws.s));
+    BV_CK(cudaStreamSynchronize(ws.s));
     std::vector<long long> offs(num_rcv);
     long long total = 0;
     for (size_t i = 0; i < num_rcv; ++i) {
@@ -419,19 +466,19 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     long long* d_offs;
     wq3d_biverb* d_out;
     double* d_opow;
-    BV_CK(buf.alloc(&d_offs, num_rcv));
-    BV_CK(buf.alloc(&d_out, nout));
-    BV_CK(buf.alloc(&d_opow, nout * num_freq));
-    BV_CK(cudaMemcpyAsync(d_offs, offs.data(), num_rcv * sizeof(long long), cudaMemcpyHostToDevice, st.s));
+    BV_CK(ws.get(BV_OFFS, &d_offs, num_rcv));
+    BV_CK(ws.get(BV_OUT, &d_out, nout));
+    BV_CK(ws.get(BV_OPOW, &d_opow, nout * num_freq));
+    BV_CK(cudaMemcpyAsync(d_offs, offs.data(), num_rcv * sizeof(long long), cudaMemcpyHostToDevice, ws.s));
     a.offs = d_offs;
     a.out = d_out;
     a.out_pow = d_opow;
     a.cap = (long long)nout;
-    k_biverb_pairs<true><<<blocks, BV_WARPS * 32, 0, st.s>>>(a);
+    k_biverb_pairs<true><<<blocks, BV_WARPS * 32, 0, ws.s>>>(a);
     BV_CK(cudaGetLastError());
-    BV_CK(cudaMemcpyAsync(out, d_out, nout * sizeof(wq3d_biverb), cudaMemcpyDeviceToHost, st.s));
-    BV_CK(cudaMemcpyAsync(out_power, d_opow, nout * num_freq * sizeof(double), cudaMemcpyDeviceToHost, st.s));
-    BV_CK(cudaStreamSynchronize(st.s));
+    BV_CK(cudaMemcpyAsync(out, d_out, nout * sizeof(wq3d_biverb), cudaMemcpyDeviceToHost, ws.s));
+    BV_CK(cudaMemcpyAsync(out_power, d_opow, nout * num_freq * sizeof(double), cudaMemcpyDeviceToHost, ws.s));
+    BV_CK(cudaStreamSynchronize(ws.s));
     if ((size_t)total > capacity) return bv_fail(WQ3D_ERR_OVERFLOW, "biverb capacity too small");
     return WQ3D_OK;
 }
