@@ -10,7 +10,8 @@ from underseamodelinglibrary_b200 import _abi
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-@pytest.mark.parametrize("name", ["eigenray_basic_cpp", "eigenverb_accuracy_cpp", "batch_cpp", "reflect_cpp"])
+@pytest.mark.parametrize("name", ["eigenray_basic_cpp", "eigenverb_accuracy_cpp", "batch_cpp", "reflect_cpp",
+                                  "biverbs_cpp"])
 def test_cpp_program_builds(tmp_path, name):
     if not os.path.exists(_abi.LIB_PATH):
         pytest.skip("libwq3d.so not built")

@@ -70,3 +70,12 @@ def test_cpp_reflection_listener(tmp_path, engine):
         assert t == r.type
         assert abs(time - r.time) < 2e-9
         assert abs(graz - math.degrees(r.grazing)) < 2e-6
+
+
+def test_cpp_biverb_generator(tmp_path, engine):
+    """biverbs_test.cc:41-158 through the C++ header: biverb_generator over
+    the 80 analytic footprints, 109 biverbs ordered by travel time, every
+    footprint overlapping itself"""
+    out = subprocess.run([build_cpp(tmp_path, "biverbs_cpp")], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "biverbs ok" in out.stdout and "biverbs 109" in out.stdout

@@ -162,6 +162,20 @@ class wposition1 {
         longitude(lng);
         altitude(alt);
     }
+    /* great circle range (m) and bearing (rad) from a point
+     * (types/wposition1.cc:23-37) */
+    wposition1(const wposition1& location, double range, double bearing) {
+        const double lat1 = to_radians(location.latitude());
+        const double lng1 = to_radians(location.longitude());
+        const double R = earth::radius() + location.altitude();
+        range /= R;
+        const double lat2 = std::asin(std::sin(lat1) * std::cos(range) + std::cos(lat1) * std::sin(range) * std::cos(bearing));
+        const double lng2 = lng1 + std::atan2(std::sin(bearing) * std::sin(range) * std::cos(lat1),
+                                              std::cos(range) - std::sin(lat1) * std::sin(lat2));
+        latitude(to_degrees(lat2));
+        longitude(to_degrees(lng2));
+        altitude(location.altitude());
+    }
     double rho() const { return _r; }
     double theta() const { return _t; }
     double phi() const { return _p; }
@@ -300,17 +314,41 @@ struct reflect_loss_rayleigh : reflect_loss_model {
     }
 };
 
+/* scattering strength models (ocean/scattering_{constant,lambert,chapman}.h),
+ * evaluated on the GPU by wq3d_biverbs */
+struct scattering_model {
+    typedef std::shared_ptr<const scattering_model> csptr;
+    wq3d_scattering_desc d{WQ3D_SCATTER_CONSTANT, 0, -300.0};
+};
+struct scattering_constant : scattering_model {
+    explicit scattering_constant(double amplitude = -300.0) { d = {WQ3D_SCATTER_CONSTANT, 0, amplitude}; }
+};
+struct scattering_lambert : scattering_model {
+    explicit scattering_lambert(double bss = -27.0) { d = {WQ3D_SCATTER_LAMBERT, 0, bss}; }
+};
+struct scattering_chapman : scattering_model {
+    explicit scattering_chapman(double wind_speed) { d = {WQ3D_SCATTER_CHAPMAN, 0, wind_speed}; }
+};
+
 class boundary_model {
    public:
     typedef std::shared_ptr<const boundary_model> csptr;
+    explicit boundary_model(const scattering_model::csptr& scattering = nullptr)
+        : _scattering(scattering ? scattering : std::make_shared<scattering_constant>()) {}
     virtual void fill(wq3d_boundary_desc* d) const = 0;
     virtual ~boundary_model() {}
+    /** boundary_model::scattering: scattering_constant(-300 dB) unless given */
+    const scattering_model::csptr& scattering() const { return _scattering; }
+
+   private:
+    scattering_model::csptr _scattering;
 };
 
 class boundary_flat : public boundary_model {
    public:
-    explicit boundary_flat(double depth = 0.0, const reflect_loss_model::csptr& loss = nullptr)
-        : _depth(depth), _loss(loss) {}
+    explicit boundary_flat(double depth = 0.0, const reflect_loss_model::csptr& loss = nullptr,
+                           const scattering_model::csptr& scattering = nullptr)
+        : boundary_model(scattering), _depth(depth), _loss(loss) {}
     void fill(wq3d_boundary_desc* d) const override {
         d->kind = WQ3D_BOUNDARY_FLAT;
         d->depth = _depth;
@@ -325,8 +363,9 @@ class boundary_flat : public boundary_model {
 class boundary_slope : public boundary_model {
    public:
     boundary_slope(const types::wposition1& loc, double depth, double lat_slope, double lng_slope = 0.0,
-                   const reflect_loss_model::csptr& loss = nullptr)
-        : _loc(loc), _depth(depth), _lat(lat_slope), _lng(lng_slope), _loss(loss) {}
+                   const reflect_loss_model::csptr& loss = nullptr,
+                   const scattering_model::csptr& scattering = nullptr)
+        : boundary_model(scattering), _loc(loc), _depth(depth), _lat(lat_slope), _lng(lng_slope), _loss(loss) {}
     void fill(wq3d_boundary_desc* d) const override {
         d->kind = WQ3D_BOUNDARY_SLOPE;
         d->depth = _depth;
@@ -349,10 +388,17 @@ class boundary_slope : public boundary_model {
 struct volume_model {
     typedef std::shared_ptr<const volume_model> csptr;
     wq3d_volume_desc d{0.0, 0.0, -300.0};
+    scattering_model::csptr scattering = std::make_shared<scattering_constant>();
 };
 struct volume_flat : volume_model {
     explicit volume_flat(double depth = 0.0, double thickness = 0.0, double amplitude = -300.0) {
         d = {depth, thickness, amplitude};
+        scattering = std::make_shared<scattering_constant>(amplitude);
+    }
+    /* volume_flat(depth, thickness, scattering) (volume_flat.h:47-50) */
+    volume_flat(double depth, double thickness, const scattering_model::csptr& model) {
+        d = {depth, thickness, model->d.kind == WQ3D_SCATTER_CONSTANT ? model->d.p : -300.0};
+        scattering = model;
     }
 };
 
@@ -363,7 +409,8 @@ class ocean_model {
    public:
     typedef std::shared_ptr<const ocean_model> csptr;
     ocean_model(const boundary_model::csptr& surface, const boundary_model::csptr& bottom,
-                const profile_model::csptr& profile) {
+                const profile_model::csptr& profile)
+        : _surface(surface), _bottom(bottom) {
         _d.earth_radius = types::earth::radius();
         profile->fill(&_d.profile);
         surface->fill(&_d.surface);
@@ -374,8 +421,16 @@ class ocean_model {
         if (_h) throw std::logic_error("add volume layers before the ocean is first used");
         if (_d.num_volume >= WQ3D_MAX_VOLUME) throw std::invalid_argument("too many volume layers");
         _d.volume[_d.num_volume++] = layer->d;
+        _volume.push_back(layer);
     }
     size_t num_volume() const { return (size_t)_d.num_volume; }
+    /** the scattering model of an interface, as ocean_model::scattering
+     * picks it (ocean/ocean_model.h:88-112) */
+    const scattering_model::csptr& scattering_model_of(size_t interface) const {
+        if (interface == 0) return _bottom->scattering();
+        if (interface == 1) return _surface->scattering();
+        return _volume.at((interface - 2) / 2)->scattering;
+    }
     const wq3d_ocean* handle() const {
         if (!_h) {
             wq3d_ocean* o = nullptr;
@@ -386,6 +441,8 @@ class ocean_model {
     }
 
    private:
+    boundary_model::csptr _surface, _bottom;
+    std::vector<volume_model::csptr> _volume;
     wq3d_ocean_desc _d{};
     mutable std::shared_ptr<wq3d_ocean> _h;
 };
@@ -498,6 +555,9 @@ class eigenverb_listener {
 /* eigenverbs/eigenverb_collection.h: one list per interface */
 class eigenverb_collection : public eigenverb_listener {
    public:
+    /** size of the biverb search area, in footprint lengths and widths
+     * (eigenverb_collection.cc:32) */
+    static inline double search_scale = 1.5;
     explicit eigenverb_collection(size_t num_volumes = 0) : _collection((1 + num_volumes) * 2) {}
     size_t num_interfaces() const { return _collection.size(); }
     size_t size(size_t interface_num) const { return _collection[interface_num].size(); }
@@ -513,6 +573,160 @@ class eigenverb_collection : public eigenverb_listener {
 };
 
 }  // namespace eigenverbs
+
+namespace biverbs {
+
+/* biverbs/biverb_model.h:24-104, plus the indices of the source and
+ * receiver eigenverbs it overlaps */
+struct biverb_model {
+    typedef std::shared_ptr<const biverb_model> csptr;
+    double travel_time = 0;
+    std::vector<double> power;
+    double duration = 0;
+    size_t de_index = 0, az_index = 0;
+    double source_de = 0, source_az = 0, receiver_de = 0, receiver_az = 0;
+    int source_surface = 0, source_bottom = 0, source_caustic = 0, source_upper = 0, source_lower = 0;
+    int receiver_surface = 0, receiver_bottom = 0, receiver_caustic = 0, receiver_upper = 0, receiver_lower = 0;
+    size_t source_index = 0, receiver_index = 0;
+};
+
+/* biverbs/biverb_collection.h: one list per interface, ordered by travel
+ * time; equal travel times keep the order they were added in (the
+ * reference's multimap) */
+class biverb_collection {
+   public:
+    typedef std::shared_ptr<const biverb_collection> csptr;
+    /** biverb_collection.cc:28 */
+    static inline double power_threshold = 1e-20;
+    explicit biverb_collection(size_t num_volumes = 0) : _collection((1 + num_volumes) * 2) {}
+    size_t num_interfaces() const { return _collection.size(); }
+    size_t size(size_t interface_num) const { return _collection[interface_num].size(); }
+    const std::vector<biverb_model::csptr>& biverbs(size_t interface_num) const { return _collection[interface_num]; }
+    void add_biverbs(const std::vector<biverb_model::csptr>& list, size_t interface_num) {
+        auto& c = _collection[interface_num];
+        c.insert(c.end(), list.begin(), list.end());
+        std::stable_sort(c.begin(), c.end(), [](const biverb_model::csptr& a, const biverb_model::csptr& b) {
+            return a->travel_time < b->travel_time;
+        });
+    }
+
+   private:
+    std::vector<std::vector<biverb_model::csptr>> _collection;
+};
+
+/* biverb_generator (biverbs/biverb_generator.cc:26-82): one wq3d_biverbs
+ * call per interface; the ocean and frequencies, process-wide singletons
+ * in the reference, are arguments */
+class biverb_generator {
+   public:
+    biverb_generator(const ocean::ocean_model::csptr& ocean,
+                     const std::shared_ptr<const eigenverbs::eigenverb_collection>& src,
+                     const std::shared_ptr<const eigenverbs::eigenverb_collection>& rcv,
+                     const types::seq_vector::csptr& freq)
+        : _ocean(ocean), _src(src), _rcv(rcv), _freq(freq) {}
+    void abort() { _abort = true; }
+    bool done() const { return _done; }
+    const biverb_collection::csptr& collection() const { return _collection; }
+
+    void run() {
+        if (_abort) return;
+        auto coll = std::make_shared<biverb_collection>(_ocean->num_volume());
+        const size_t nf = _freq->size();
+        for (size_t interface = 0; interface < _rcv->num_interfaces(); ++interface) {
+            if (interface >= _src->num_interfaces()) break;
+            const auto& sv = _src->eigenverbs(interface);
+            const auto& rv = _rcv->eigenverbs(interface);
+            if (sv.empty() || rv.empty()) continue;
+            std::vector<wq3d_eigenverb> s, r;
+            std::vector<double> sp, rp;
+            pack(sv, nf, &s, &sp);
+            pack(rv, nf, &r, &rp);
+            const wq3d_scattering_desc sc = _ocean->scattering_model_of(interface)->d;
+            size_t n = 0;
+            call(s, sp, r, rp, sc, nullptr, nullptr, 0, &n);
+            std::vector<wq3d_biverb> out(n);
+            std::vector<double> power(n * nf);
+            call(s, sp, r, rp, sc, out.data(), power.data(), n, &n);
+            std::vector<biverb_model::csptr> list;
+            list.reserve(n);
+            for (size_t k = 0; k < n; ++k) list.push_back(to_model(out[k], &power[k * nf], nf));
+            coll->add_biverbs(list, interface);
+            if (_abort) return;
+        }
+        _collection = coll;
+        _done = true;
+    }
+
+   private:
+    static void pack(const std::vector<eigenverbs::eigenverb_model::csptr>& verbs, size_t nf,
+                     std::vector<wq3d_eigenverb>* recs, std::vector<double>* power) {
+        recs->assign(verbs.size(), wq3d_eigenverb{});
+        power->assign(verbs.size() * nf, 0.0);
+        for (size_t i = 0; i < verbs.size(); ++i) {
+            const auto& v = *verbs[i];
+            wq3d_eigenverb& e = (*recs)[i];
+            e.travel_time = v.travel_time;
+            e.length = v.length;
+            e.width = v.width;
+            e.position[0] = v.position.rho();
+            e.position[1] = v.position.theta();
+            e.position[2] = v.position.phi();
+            e.direction = v.direction;
+            e.grazing = v.grazing;
+            e.sound_speed = v.sound_speed;
+            e.source_de = v.source_de;
+            e.source_az = v.source_az;
+            e.de = (int32_t)v.de_index;
+            e.az = (int32_t)v.az_index;
+            e.surface = v.surface;
+            e.bottom = v.bottom;
+            e.caustic = v.caustic;
+            e.upper = v.upper;
+            e.lower = v.lower;
+            for (size_t f = 0; f < nf; ++f) (*power)[i * nf + f] = v.power.size() == nf ? v.power[f] : v.power.at(0);
+        }
+    }
+    void call(const std::vector<wq3d_eigenverb>& s, const std::vector<double>& sp,
+              const std::vector<wq3d_eigenverb>& r, const std::vector<double>& rp, const wq3d_scattering_desc& sc,
+              wq3d_biverb* out, double* power, size_t capacity, size_t* n) const {
+        check(wq3d_biverbs(s.data(), sp.data(), s.size(), r.data(), rp.data(), r.size(), _freq->data().data(),
+                           _freq->size(), &sc, types::earth::radius(), eigenverbs::eigenverb_collection::search_scale,
+                           biverb_collection::power_threshold, out, power, capacity, n));
+    }
+    static biverb_model::csptr to_model(const wq3d_biverb& b, const double* power, size_t nf) {
+        auto m = std::make_shared<biverb_model>();
+        m->travel_time = b.travel_time;
+        m->power.assign(power, power + nf);
+        m->duration = b.duration;
+        m->de_index = (size_t)b.de_index;
+        m->az_index = (size_t)b.az_index;
+        m->source_de = b.source_de;
+        m->source_az = b.source_az;
+        m->receiver_de = b.receiver_de;
+        m->receiver_az = b.receiver_az;
+        m->source_surface = b.source_surface;
+        m->source_bottom = b.source_bottom;
+        m->source_caustic = b.source_caustic;
+        m->source_upper = b.source_upper;
+        m->source_lower = b.source_lower;
+        m->receiver_surface = b.receiver_surface;
+        m->receiver_bottom = b.receiver_bottom;
+        m->receiver_caustic = b.receiver_caustic;
+        m->receiver_upper = b.receiver_upper;
+        m->receiver_lower = b.receiver_lower;
+        m->source_index = (size_t)b.source;
+        m->receiver_index = (size_t)b.receiver;
+        return m;
+    }
+
+    ocean::ocean_model::csptr _ocean;
+    std::shared_ptr<const eigenverbs::eigenverb_collection> _src, _rcv;
+    types::seq_vector::csptr _freq;
+    biverb_collection::csptr _collection;
+    bool _abort = false, _done = false;
+};
+
+}  // namespace biverbs
 
 namespace waveq3d {
 
