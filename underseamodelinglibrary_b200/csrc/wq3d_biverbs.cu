@@ -247,8 +247,10 @@ __device__ __forceinline__ double bv_power(const BvArgs& a, int si, int ri, int 
     return p * scale;
 }
 
+/* three blocks per SM (80 registers): the group scan is latency-bound, and
+ * the extra warps hide more of it than the rare overlap code loses */
 template <bool WRITE>
-__global__ void __launch_bounds__(BV_WARPS * 32) k_biverb_pairs(const BvArgs a) {
+__global__ void __launch_bounds__(BV_WARPS * 32, 3) k_biverb_pairs(const BvArgs a) {
     const int lane = threadIdx.x & 31;
     const int ri = blockIdx.x * BV_WARPS + (threadIdx.x >> 5);
     if (ri >= a.nr) return;  /* a whole warp: no block barrier follows */
