@@ -34,7 +34,8 @@ def test_library_exports_every_declared_symbol():
 
 STRUCTS = ["wq3d_grid_desc", "wq3d_profile_desc", "wq3d_reflect_loss_desc", "wq3d_boundary_desc",
            "wq3d_ocean_desc", "wq3d_queue_desc", "wq3d_thresholds", "wq3d_eigenray",
-           "wq3d_reflection", "wq3d_callbacks", "wq3d_front_view"]
+           "wq3d_reflection", "wq3d_callbacks", "wq3d_front_view", "wq3d_eigenverb",
+           "wq3d_scattering_desc", "wq3d_biverb", "wq3d_timing"]
 
 
 def test_struct_layouts_match_header():

@@ -163,3 +163,37 @@ def test_scattering_model_per_interface():
     assert ocean.scattering_model(2).p == -40.0 and ocean.scattering_model(3).p == -40.0
     assert ocean.scattering_model(4).kind == u.scattering_chapman(1).kind
     assert ocean.scattering_model(5).p == 5.0
+
+
+def test_abi_argument_checks_without_gpu():
+    """wq3d_biverbs checks its arguments before it touches the device:
+    bad ones return WQ3D_ERR_INVALID with a message, and an empty side
+    returns no biverbs"""
+    import ctypes as C
+    from underseamodelinglibrary_b200 import _abi
+    lib = _abi.load_engine()
+    verbs, freq = kat_eigenverbs()
+    s, sp = B.pack_eigenverbs(verbs, 1)
+    f = np.array([3000.0])
+    dp = C.POINTER(C.c_double)
+    count = C.c_size_t(99)
+    desc = u.scattering_constant(-30.0).desc()
+
+    def call(ns=80, nr=80, fp=f.ctypes.data_as(dp), nf=1, sc=C.byref(desc), R=6371000.0, scale=1.5,
+             cnt=C.byref(count)):
+        return lib.wq3d_biverbs(s, sp.ctypes.data_as(dp), ns, s, sp.ctypes.data_as(dp), nr, fp, nf, sc, R,
+                                scale, 1e-20, None, None, 0, cnt)
+
+    assert call(cnt=None) == _abi.WQ3D_ERR_INVALID
+    assert call(sc=None) == _abi.WQ3D_ERR_INVALID
+    assert call(nf=0) == _abi.WQ3D_ERR_INVALID
+    assert call(R=0.0) == _abi.WQ3D_ERR_INVALID
+    assert call(scale=-1.0) == _abi.WQ3D_ERR_INVALID
+    bad = u.scattering_constant(0.0).desc()
+    bad.kind = 3
+    assert call(sc=C.byref(bad)) == _abi.WQ3D_ERR_INVALID
+    assert b"scattering" in lib.wq3d_last_error_string()
+    assert call(ns=0) == _abi.WQ3D_OK and count.value == 0
+    count.value = 99
+    assert call(nr=0) == _abi.WQ3D_OK and count.value == 0
+
