@@ -12,6 +12,7 @@ one ``wq3d_biverbs`` call per interface; the collection keeps each
 interface's biverbs ordered by travel time, as the reference's multimap
 does."""
 import ctypes as C
+from collections.abc import Sequence
 
 import numpy as np
 
@@ -23,35 +24,38 @@ def _freq_array(frequencies):
     return np.ascontiguousarray(np.asarray(f, dtype=np.float64).ravel())
 
 
+_VERB_FIELDS = ("travel_time", "length", "width", "direction", "grazing", "sound_speed", "source_de",
+                "source_az")
+_VERB_INTS = (("de", "de_index"), ("az", "az_index"), ("surface", "surface"), ("bottom", "bottom"),
+              ("caustic", "caustic"), ("upper", "upper"), ("lower", "lower"))
+
+
 def pack_eigenverbs(verbs, num_freq):
-    """eigenverb_model list -> (wq3d_eigenverb array, power (n, num_freq))"""
+    """eigenverb_model list -> (wq3d_eigenverb array, power (n, num_freq)),
+    filled a column at a time"""
     n = len(verbs)
     recs = (_abi.wq3d_eigenverb * max(n, 1))()
     power = np.zeros((n, num_freq))
-    for i, v in enumerate(verbs):
-        r = recs[i]
-        r.travel_time = v.travel_time
-        r.length = v.length
-        r.width = v.width
-        r.position[0], r.position[1], r.position[2] = v.position
-        r.direction = v.direction
-        r.grazing = v.grazing
-        r.sound_speed = v.sound_speed
-        r.source_de = v.source_de
-        r.source_az = v.source_az
-        r.de = int(v.de_index)
-        r.az = int(v.az_index)
-        r.surface, r.bottom, r.caustic = int(v.surface), int(v.bottom), int(v.caustic)
-        r.upper, r.lower = int(v.upper), int(v.lower)
-        power[i] = np.broadcast_to(np.asarray(v.power, dtype=np.float64), (num_freq,))
+    if n == 0:
+        return recs, power
+    a = np.ctypeslib.as_array(recs)[:n]
+    for f in _VERB_FIELDS:
+        a[f] = [getattr(v, f) for v in verbs]
+    for f, attr in _VERB_INTS:
+        a[f] = [int(getattr(v, attr)) for v in verbs]
+    a["position"] = [v.position for v in verbs]
+    p = [np.asarray(v.power, dtype=np.float64) for v in verbs]
+    power[:] = np.stack([np.broadcast_to(x, (num_freq,)) for x in p])
     return recs, power
 
 
 def compute_biverbs(src_verbs, rcv_verbs, frequencies, scattering, search_scale=1.5,
                     power_threshold=1e-20, lib=None, fn="wq3d_biverbs"):
     """The biverbs of one interface, in (receiver, source) order: returns
-    (wq3d_biverb array, power (n, num_freq)).  ``scattering`` is an
-    ocean scattering model (scattering_constant, _lambert, _chapman)."""
+    (records, power (n, num_freq)).  The records are a numpy record array
+    over the library's wq3d_biverb layout (fields read as attributes:
+    ``recs[k].travel_time``).  ``scattering`` is an ocean scattering model
+    (scattering_constant, _lambert, _chapman)."""
     lib = lib or _abi.load_engine()
     freq = _freq_array(frequencies)
     nf = freq.size
@@ -78,7 +82,8 @@ def compute_biverbs(src_verbs, rcv_verbs, frequencies, scattering, search_scale=
         msg = lib.wq3d_last_error_string() if hasattr(lib, "wq3d_last_error_string") else b""
         raise _abi.EngineError(rc, msg.decode() if msg else "")
     n = count.value
-    return out[:n], power[:n]
+    recs = np.ctypeslib.as_array(out)[:n].copy().view(np.recarray)
+    return recs, power[:n].copy()
 
 
 def _earth():
@@ -98,6 +103,7 @@ class biverb_model:
 
     @classmethod
     def from_record(cls, rec, power, frequencies):
+        """from a wq3d_biverb record (ctypes or numpy record)"""
         b = cls()
         b.travel_time = rec.travel_time
         b.frequencies = frequencies
@@ -116,6 +122,44 @@ class biverb_model:
         return b
 
 
+class biverb_list(Sequence):
+    """The biverbs of one interface over record arrays: a biverb_model is
+    made when an element is read, so a caller that wants the arrays
+    (``arrays()``) or the count pays no per-biverb Python cost."""
+
+    __slots__ = ("_rec", "_power", "_freq")
+
+    def __init__(self, rec, power, frequencies):
+        self._rec = rec
+        self._power = power
+        self._freq = frequencies
+
+    def __len__(self):
+        return len(self._rec)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[j] for j in range(*i.indices(len(self)))]
+        n = len(self._rec)
+        i = int(i)
+        if i < 0:
+            i += n
+        if not 0 <= i < n:
+            raise IndexError("biverb index out of range")
+        return biverb_model.from_record(self._rec[i], self._power[i], self._freq)
+
+    def __iter__(self):
+        for i in range(len(self._rec)):
+            yield self[i]
+
+    def __eq__(self, other):
+        return list(self) == list(other) if isinstance(other, (list, biverb_list)) else NotImplemented
+
+    def arrays(self):
+        """(records as a numpy record array, power (n, num_freq))"""
+        return self._rec, self._power
+
+
 class biverb_collection:
     """biverb_collection(num_volumes) (biverbs/biverb_collection.h:36-119):
     one list per interface, ordered by travel time; biverbs of equal
@@ -126,16 +170,26 @@ class biverb_collection:
     power_threshold = 1e-20
 
     def __init__(self, num_volumes=0):
-        self._collection = [[] for _ in range((1 + int(num_volumes)) * 2)]
+        n = (1 + int(num_volumes)) * 2
+        self._collection = [[] for _ in range(n)]
+        self._records = [None] * n      # (records, power, frequencies) per interface
 
     def num_interfaces(self):
         return len(self._collection)
 
     def size(self, interface_num):
-        return len(self._collection[interface_num])
+        r = self._records[interface_num]
+        return len(self._collection[interface_num]) + (0 if r is None else len(r[0]))
 
     def biverbs(self, interface_num):
-        return list(self._collection[interface_num])
+        r = self._records[interface_num]
+        if r is None:
+            return list(self._collection[interface_num])
+        if not self._collection[interface_num]:
+            return biverb_list(*r)
+        merged = list(biverb_list(*r)) + self._collection[interface_num]
+        merged.sort(key=lambda b: b.travel_time)
+        return merged
 
     def add_biverbs(self, biverbs, interface_num):
         """inserts, as the reference's multimap insert does: after every
@@ -143,6 +197,16 @@ class biverb_collection:
         merged = self._collection[interface_num] + list(biverbs)
         merged.sort(key=lambda b: b.travel_time)
         self._collection[interface_num] = merged
+
+    def add_records(self, records, power, frequencies, interface_num):
+        """the records of one wq3d_biverbs call, kept as arrays; inserted as
+        add_biverbs does (a stable sort by travel time)"""
+        old = self._records[interface_num]
+        if old is not None:
+            records = np.concatenate([old[0], records]).view(np.recarray)
+            power = np.concatenate([old[1], power])
+        order = np.argsort(records.travel_time, kind="stable")
+        self._records[interface_num] = (records[order], power[order], frequencies)
 
 
 class biverb_generator:
@@ -184,8 +248,7 @@ class biverb_generator:
                                               self.ocean.scattering_model(interface),
                                               search_scale=src.search_scale,
                                               power_threshold=biverb_collection.power_threshold)
-                coll.add_biverbs([biverb_model.from_record(recs[k], power[k], self.frequencies)
-                                  for k in range(len(recs))], interface)
+                coll.add_records(recs, power, self.frequencies, interface)
             if self._abort:
                 return
         self._collection = coll
