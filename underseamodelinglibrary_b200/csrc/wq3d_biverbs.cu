@@ -25,8 +25,9 @@
  * and the second writes every pair at its receiver's offset plus its rank
  * among the warp's hits (ballot + popc), in source index order.
  *
- * The work is FP64 scalar arithmetic on records that are read once per
- * tile; the pair tests are compute-bound on the FP64 pipe, not on HBM.
+ * The inputs are read from HBM once and the group boxes stay in L1, so the
+ * passes are bound by the latency of the group scan and of the FP64
+ * compares, not by HBM or the FP64 pipe.
  */
 #include <cuda_runtime.h>
 
