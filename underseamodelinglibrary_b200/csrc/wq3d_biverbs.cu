@@ -21,9 +21,11 @@
  * overlap.  No shared memory and no block barrier are involved, so warps
  * run independently.
  * Two passes keep the output order fixed without atomics: the first counts
- * each receiver's surviving pairs, the host turns the counts into offsets,
- * and the second writes every pair at its receiver's offset plus its rank
- * among the warp's hits (ballot + popc), in source index order.
+ * each receiver's surviving pairs and keeps the sources of its first 256,
+ * the host turns the counts into offsets, and the second writes every pair
+ * at its receiver's offset plus its rank among the warp's hits (ballot +
+ * popc), in source index order: from the kept sources when they are all
+ * of them, else by scanning again.
  *
  * The inputs are read from HBM once and the group boxes stay in L1, so the
  * passes are bound by the latency of the group scan and of the FP64
@@ -45,6 +47,7 @@ namespace {
 
 constexpr int BV_WARPS = 8;    /* receivers per block, one warp each   */
 constexpr int BV_BOX = 12;     /* doubles per receiver box            */
+constexpr int BV_HITS = 256;   /* hit sources the count pass keeps per receiver */
 
 int bv_fail(int code, const std::string& msg) {
     wq3d_internal_set_error(msg.c_str());
@@ -89,7 +92,8 @@ struct BvArgs {
     const double* chap;     /* Chapman: 2.6 - 42.4 log10(beta), 3.3 beta */
     double R0;
     double threshold;
-    long long* counts;      /* pass 1 */
+    long long* counts;      /* pass 1 writes, pass 2 reads */
+    int* hits;              /* BV_HITS source indices per receiver */
     const long long* offs;  /* pass 2 */
     wq3d_biverb* out;
     double* out_pow;
@@ -248,6 +252,36 @@ __device__ __forceinline__ double bv_power(const BvArgs& a, int si, int ri, int 
     return p * scale;
 }
 
+/* writes the biverb of source si and receiver ri at output slot k */
+__device__ __noinline__ void bv_write(const BvArgs& a, int si, int ri, const BvOverlap& o, long long k) {
+    const wq3d_eigenverb& s = a.src[si];
+    const wq3d_eigenverb& r = a.rcv[ri];
+    wq3d_biverb v;
+    v.travel_time = s.travel_time + r.travel_time;
+    v.duration = o.duration;
+    v.source_de = s.source_de;
+    v.source_az = s.source_az;
+    v.receiver_de = r.source_de;
+    v.receiver_az = r.source_az;
+    v.de_index = r.de;
+    v.az_index = r.az;
+    v.source_surface = s.surface;
+    v.source_bottom = s.bottom;
+    v.source_caustic = s.caustic;
+    v.source_upper = s.upper;
+    v.source_lower = s.lower;
+    v.receiver_surface = r.surface;
+    v.receiver_bottom = r.bottom;
+    v.receiver_caustic = r.caustic;
+    v.receiver_upper = r.upper;
+    v.receiver_lower = r.lower;
+    v.source = si;
+    v.receiver = ri;
+    a.out[k] = v;
+    for (int f = 0; f < a.nf; ++f)
+        a.out_pow[(size_t)k * a.nf + f] = bv_power(a, si, ri, f, o.scale, s.grazing, r.grazing);
+}
+
 /* three blocks per SM (80 registers): the group scan is latency-bound, and
  * the extra warps hide more of it than the rare overlap code loses */
 template <bool WRITE>
@@ -259,6 +293,18 @@ __global__ void __launch_bounds__(BV_WARPS * 32, 3) k_biverb_pairs(const BvArgs 
 #pragma unroll
     for (int k = 0; k < BV_BOX; ++k) b[k] = a.box[(size_t)ri * BV_BOX + k];
     const long long base = WRITE ? a.offs[ri] : 0;
+    if (WRITE) {
+        /* the count pass stored the sources of up to BV_HITS hits, in
+         * source order: write those without scanning again */
+        const long long cnt = a.counts[ri];
+        if (cnt <= BV_HITS) {
+            for (int k = lane; k < cnt; k += 32) {
+                const int si = a.hits[(size_t)ri * BV_HITS + k];
+                if (base + k < a.cap) bv_write(a, si, ri, bv_overlap(a.src[si], a.rcv[ri], a.R0), base + k);
+            }
+            return;
+        }
+    }
     const unsigned below = (1u << lane) - 1u;
     const int ngroups = (a.ns + 31) >> 5;
     long long n = 0;
@@ -284,35 +330,12 @@ __global__ void __launch_bounds__(BV_WARPS * 32, 3) k_biverb_pairs(const BvArgs 
                 hit = pmax >= a.threshold;
             }
             const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if (WRITE && hit) {
-                const long long k = base + n + __popc(bal & below);
-                if (k < a.cap) {
-                    const wq3d_eigenverb& s = a.src[si];
-                    const wq3d_eigenverb& r = a.rcv[ri];
-                    wq3d_biverb v;
-                    v.travel_time = s.travel_time + r.travel_time;
-                    v.duration = o.duration;
-                    v.source_de = s.source_de;
-                    v.source_az = s.source_az;
-                    v.receiver_de = r.source_de;
-                    v.receiver_az = r.source_az;
-                    v.de_index = r.de;
-                    v.az_index = r.az;
-                    v.source_surface = s.surface;
-                    v.source_bottom = s.bottom;
-                    v.source_caustic = s.caustic;
-                    v.source_upper = s.upper;
-                    v.source_lower = s.lower;
-                    v.receiver_surface = r.surface;
-                    v.receiver_bottom = r.bottom;
-                    v.receiver_caustic = r.caustic;
-                    v.receiver_upper = r.upper;
-                    v.receiver_lower = r.lower;
-                    v.source = si;
-                    v.receiver = ri;
-                    a.out[k] = v;
-                    for (int f = 0; f < a.nf; ++f)
-                        a.out_pow[(size_t)k * a.nf + f] = bv_power(a, si, ri, f, o.scale, s.grazing, r.grazing);
+            if (hit) {
+                const long long k = n + __popc(bal & below);
+                if (WRITE) {
+                    if (base + k < a.cap) bv_write(a, si, ri, o, base + k);
+                } else if (k < BV_HITS) {
+                    a.hits[(size_t)ri * BV_HITS + k] = si;
                 }
             }
             n += __popc(bal);
@@ -327,7 +350,7 @@ __global__ void __launch_bounds__(BV_WARPS * 32, 3) k_biverb_pairs(const BvArgs 
  * calls on one device.  The buffers live until the process exits. */
 constexpr int BV_MAX_DEVICES = 64;
 enum { BV_SRC, BV_RCV, BV_SPOW, BV_RPOW, BV_SX, BV_SY, BV_BOXES, BV_GROUPS_BUF, BV_COUNTS, BV_CHAP,
-       BV_OFFS, BV_OUT, BV_OPOW, BV_NBUF };
+       BV_OFFS, BV_OUT, BV_OPOW, BV_HITS_BUF, BV_NBUF };
 
 struct BvWorkspace {
     std::mutex m;
@@ -409,6 +432,7 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     wq3d_eigenverb *d_src, *d_rcv;
     double *d_spow, *d_rpow, *d_sx, *d_sy, *d_box, *d_groups, *d_chap = nullptr;
     long long* d_counts;
+    int* d_hits;
     BV_CK(ws.get(BV_SRC, &d_src, num_src));
     BV_CK(ws.get(BV_RCV, &d_rcv, num_rcv));
     BV_CK(ws.get(BV_SPOW, &d_spow, num_src * num_freq));
@@ -419,6 +443,7 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     const size_t num_groups = (num_src + 31) / 32;
     BV_CK(ws.get(BV_GROUPS_BUF, &d_groups, num_groups * 4));
     BV_CK(ws.get(BV_COUNTS, &d_counts, num_rcv));
+    BV_CK(ws.get(BV_HITS_BUF, &d_hits, num_rcv * BV_HITS));
     if (!chap.empty()) BV_CK(ws.get(BV_CHAP, &d_chap, chap.size()));
     BV_CK(cudaMemcpyAsync(d_src, src, num_src * sizeof(wq3d_eigenverb), cudaMemcpyHostToDevice, ws.s));
     BV_CK(cudaMemcpyAsync(d_rcv, rcv, num_rcv * sizeof(wq3d_eigenverb), cudaMemcpyHostToDevice, ws.s));
@@ -442,6 +467,7 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     a.R0 = earth_radius;
     a.threshold = power_threshold;
     a.counts = d_counts;
+    a.hits = d_hits;
 
     const size_t nmax = num_src > num_rcv ? num_src : num_rcv;
     k_biverb_boxes<<<(unsigned)((nmax + 127) / 128), 128, 0, ws.s>>>(a, search_scale, d_box, d_sx, d_sy);
