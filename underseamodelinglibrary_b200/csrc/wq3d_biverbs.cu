@@ -13,10 +13,11 @@
  * Here every (receiver, source) pair is screened on the GPU.  One warp
  * owns one receiver: its search quadrilateral and bounding box are
  * computed once (k_biverb_boxes).  The sources are cut into groups of 32
- * consecutive ones with a bounding box each (k_biverb_groups); the warp
- * tests 32 group boxes at once against its receiver's box, one per lane,
- * and visits only the groups that may hold a hit, each lane taking one
- * source.  A bounding-box test rejects most of their pairs before the four
+ * consecutive ones with a bounding box each (k_biverb_groups), and the
+ * groups into runs of 32 with a box each (k_biverb_supers); the warp tests
+ * 32 run boxes at once against its receiver's box, one per lane, then the
+ * group boxes of each run that may hold a hit, and visits only the groups
+ * that may hold a hit, each lane taking one source.  A bounding-box test rejects most of their pairs before the four
  * edge tests, and only pairs inside the quadrilateral evaluate the
  * overlap.  No shared memory and no block barrier are involved, so warps
  * run independently.
@@ -85,6 +86,7 @@ struct BvArgs {
     const double* rcv_pow;
     const double* box;      /* BV_BOX doubles per receiver */
     const double* groups;   /* per group of 32 sources: latitude min, max, longitude min, max */
+    const double* supers;   /* the same per 32 groups */
     int nr;
     int nf;
     int kind;
@@ -141,6 +143,23 @@ __global__ void __launch_bounds__(256) k_biverb_groups(const double* sx, const d
     const int g = i >> 5;
     if ((threadIdx.x & 31) == 0 && (g << 5) < ns)
         for (int k = 0; k < 4; ++k) groups[4 * (size_t)g + k] = v[k];
+}
+
+/* the bounding box of each run of 32 group boxes, one warp per run */
+__global__ void __launch_bounds__(256) k_biverb_supers(const double* groups, int ngroups, double* supers) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = {INFINITY, -INFINITY, INFINITY, -INFINITY};
+    if (i < ngroups)
+        for (int k = 0; k < 4; ++k) v[k] = groups[4 * (size_t)i + k];
+    for (int o = 16; o > 0; o >>= 1) {
+        v[0] = fmin(v[0], __shfl_xor_sync(0xffffffffu, v[0], o));
+        v[1] = fmax(v[1], __shfl_xor_sync(0xffffffffu, v[1], o));
+        v[2] = fmin(v[2], __shfl_xor_sync(0xffffffffu, v[2], o));
+        v[3] = fmax(v[3], __shfl_xor_sync(0xffffffffu, v[3], o));
+    }
+    const int h = i >> 5;
+    if ((threadIdx.x & 31) == 0 && (h << 5) < ngroups)
+        for (int k = 0; k < 4; ++k) supers[4 * (size_t)h + k] = v[k];
 }
 
 /* a box (latitude min, max, longitude min, max) that holds no point
@@ -309,36 +328,45 @@ __global__ void __launch_bounds__(BV_WARPS * 32, 3) k_biverb_pairs(const BvArgs 
     const int ngroups = (a.ns + 31) >> 5;
     long long n = 0;
     /* a centre strictly inside the quadrilateral lies strictly inside the
-     * receiver's bounding box: each lane tests one group box, and the warp
-     * visits the groups that may hold a hit in increasing order */
-    for (int g0 = 0; g0 < ngroups; g0 += 32) {
-        const int gl = g0 + lane;
-        const bool need = gl < ngroups && !bv_misses(a.groups + 4 * (size_t)gl, b);
-        unsigned todo = __ballot_sync(0xffffffffu, need);
-        while (todo) {
-            const int g = g0 + __ffs(todo) - 1;
-            todo &= todo - 1;
-            const int si = (g << 5) + lane;
-            bool hit = false;
-            BvOverlap o{0.0, 0.0};
-            if (si < a.ns && bv_inside(b, a.sx[si], a.sy[si])) {
-                const wq3d_eigenverb& s = a.src[si];
-                const wq3d_eigenverb& r = a.rcv[ri];
-                o = bv_overlap(s, r, a.R0);
-                double pmax = 0.0;
-                for (int f = 0; f < a.nf; ++f) pmax = fmax(pmax, fabs(bv_power(a, si, ri, f, o.scale, s.grazing, r.grazing)));
-                hit = pmax >= a.threshold;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if (hit) {
-                const long long k = n + __popc(bal & below);
-                if (WRITE) {
-                    if (base + k < a.cap) bv_write(a, si, ri, o, base + k);
-                } else if (k < BV_HITS) {
-                    a.hits[(size_t)ri * BV_HITS + k] = si;
+     * receiver's bounding box: each lane tests one box of 32 groups, then,
+     * inside each that may hold a hit, one group box, and the warp visits
+     * the groups that may hold a hit in increasing order */
+    const int nsupers = (ngroups + 31) >> 5;
+    for (int h0 = 0; h0 < nsupers; h0 += 32) {
+        const int hl = h0 + lane;
+        const bool hneed = hl < nsupers && !bv_misses(a.supers + 4 * (size_t)hl, b);
+        unsigned htodo = __ballot_sync(0xffffffffu, hneed);
+        while (htodo) {
+            const int g0 = (h0 + __ffs(htodo) - 1) << 5;
+            htodo &= htodo - 1;
+            const int gl = g0 + lane;
+            const bool need = gl < ngroups && !bv_misses(a.groups + 4 * (size_t)gl, b);
+            unsigned todo = __ballot_sync(0xffffffffu, need);
+            while (todo) {
+                const int g = g0 + __ffs(todo) - 1;
+                todo &= todo - 1;
+                const int si = (g << 5) + lane;
+                bool hit = false;
+                BvOverlap o{0.0, 0.0};
+                if (si < a.ns && bv_inside(b, a.sx[si], a.sy[si])) {
+                    const wq3d_eigenverb& s = a.src[si];
+                    const wq3d_eigenverb& r = a.rcv[ri];
+                    o = bv_overlap(s, r, a.R0);
+                    double pmax = 0.0;
+                    for (int f = 0; f < a.nf; ++f) pmax = fmax(pmax, fabs(bv_power(a, si, ri, f, o.scale, s.grazing, r.grazing)));
+                    hit = pmax >= a.threshold;
                 }
+                const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                if (hit) {
+                    const long long k = n + __popc(bal & below);
+                    if (WRITE) {
+                        if (base + k < a.cap) bv_write(a, si, ri, o, base + k);
+                    } else if (k < BV_HITS) {
+                        a.hits[(size_t)ri * BV_HITS + k] = si;
+                    }
+                }
+                n += __popc(bal);
             }
-            n += __popc(bal);
         }
     }
     if (!WRITE && lane == 0) a.counts[ri] = n;
@@ -350,7 +378,7 @@ __global__ void __launch_bounds__(BV_WARPS * 32, 3) k_biverb_pairs(const BvArgs 
  * calls on one device.  The buffers live until the process exits. */
 constexpr int BV_MAX_DEVICES = 64;
 enum { BV_SRC, BV_RCV, BV_SPOW, BV_RPOW, BV_SX, BV_SY, BV_BOXES, BV_GROUPS_BUF, BV_COUNTS, BV_CHAP,
-       BV_OFFS, BV_OUT, BV_OPOW, BV_HITS_BUF, BV_NBUF };
+       BV_OFFS, BV_OUT, BV_OPOW, BV_HITS_BUF, BV_SUPERS_BUF, BV_NBUF };
 
 struct BvWorkspace {
     std::mutex m;
@@ -442,6 +470,9 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     BV_CK(ws.get(BV_BOXES, &d_box, num_rcv * BV_BOX));
     const size_t num_groups = (num_src + 31) / 32;
     BV_CK(ws.get(BV_GROUPS_BUF, &d_groups, num_groups * 4));
+    const size_t num_supers = (num_groups + 31) / 32;
+    double* d_supers;
+    BV_CK(ws.get(BV_SUPERS_BUF, &d_supers, num_supers * 4));
     BV_CK(ws.get(BV_COUNTS, &d_counts, num_rcv));
     BV_CK(ws.get(BV_HITS_BUF, &d_hits, num_rcv * BV_HITS));
     if (!chap.empty()) BV_CK(ws.get(BV_CHAP, &d_chap, chap.size()));
@@ -461,6 +492,7 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     a.rcv_pow = d_rpow;
     a.box = d_box;
     a.groups = d_groups;
+    a.supers = d_supers;
     a.nr = (int)num_rcv;
     a.nf = (int)num_freq;
     a.chap = d_chap;
@@ -473,6 +505,8 @@ extern "C" int wq3d_biverbs(const wq3d_eigenverb* src, const double* src_power, 
     k_biverb_boxes<<<(unsigned)((nmax + 127) / 128), 128, 0, ws.s>>>(a, search_scale, d_box, d_sx, d_sy);
     BV_CK(cudaGetLastError());
     k_biverb_groups<<<(unsigned)((num_src + 255) / 256), 256, 0, ws.s>>>(d_sx, d_sy, (int)num_src, d_groups);
+    BV_CK(cudaGetLastError());
+    k_biverb_supers<<<(unsigned)((num_groups + 255) / 256), 256, 0, ws.s>>>(d_groups, (int)num_groups, d_supers);
     BV_CK(cudaGetLastError());
     const unsigned blocks = (unsigned)((num_rcv + BV_WARPS - 1) / BV_WARPS);
     k_biverb_pairs<false><<<blocks, BV_WARPS * 32, 0, ws.s>>>(a);
