@@ -197,3 +197,45 @@ def test_abi_argument_checks_without_gpu():
     count.value = 99
     assert call(nr=0) == _abi.WQ3D_OK and count.value == 0
 
+
+
+def test_record_collection_and_lazy_list():
+    """add_records keeps the multimap order across calls (stable by travel
+    time, earlier calls first among equals); biverb_list reads a
+    biverb_model per element and hands out the arrays"""
+    from underseamodelinglibrary_b200 import _abi
+    freq = u.seq_linear(3000.0, 1.0, 1)
+
+    def recs(times, tags):
+        a = np.zeros(len(times), dtype=np.ctypeslib.as_array((_abi.wq3d_biverb * 1)()).dtype).view(np.recarray)
+        a.travel_time = times
+        a.source = tags
+        return a, np.array(times, dtype=np.float64)[:, None] * 10.0
+
+    c = B.biverb_collection(0)
+    c.add_records(*recs([2.0, 1.0, 2.0], [0, 1, 2]), freq, 0)
+    c.add_records(*recs([2.0, 0.5], [3, 4]), freq, 0)
+    lst = c.biverbs(0)
+    assert isinstance(lst, B.biverb_list) and len(lst) == c.size(0) == 5
+    assert [b.source_index for b in lst] == [4, 1, 0, 2, 3]
+    assert lst[-1].power[0] == 20.0 and lst[0].frequencies is freq
+    rec, power = lst.arrays()
+    assert list(rec.source) == [4, 1, 0, 2, 3] and power.shape == (5, 1)
+    with pytest.raises(IndexError):
+        lst[5]
+    assert c.biverbs(1) == [] and c.size(1) == 0
+
+
+def test_generator_aborted_before_run_does_nothing():
+    """thread_task::abort before execution (biverb_generator.cc:40-45): no
+    device work, no collection, no notification"""
+    verbs, freq = kat_eigenverbs()
+    coll = u.eigenverb_collection(0)
+    for v in verbs:
+        coll.add_eigenverb(v, 0)
+    heard = []
+    ocean = u.ocean_model(u.boundary_flat(), u.boundary_flat(1000.0), u.profile_linear())
+    gen = B.biverb_generator(ocean, coll, coll, freq, listener=heard.append)
+    gen.abort()
+    gen.run()
+    assert not gen.done() and gen.collection() is None and heard == []
