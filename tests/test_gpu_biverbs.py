@@ -163,3 +163,46 @@ def test_generator_on_propagated_eigenverbs(engine):
             np.testing.assert_allclose(b.power, power[k], rtol=REL_POWER, atol=0.0)
         total += len(got)
     assert total > 1000
+
+
+def test_high_latitude_across_the_date_line(engine):
+    """footprints of a sensor at 60N, 179.99E whose fan spans longitude
+    180 (the centres run from 179.92 to 180.06 deg, not wrapped): engine
+    and oracle agree pair for pair (search area 3 footprint lengths and
+    widths, so neighbours overlap).  Longitudes are compared as stored, so
+    a receiver fan built from the same place written as -180.01 deg finds
+    nothing on either side"""
+    from underseamodelinglibrary_b200 import scenarios as S
+    from underseamodelinglibrary_b200.eigenverbs import eigenverb_model
+    u.set_earth_radius(6371000.0)
+    de = np.arange(-80.0, -10.0, 2.0)
+    az = np.arange(0.0, 360.0, 6.0)
+    freq = np.array([2000.0])
+    model = u.scattering_lambert(-27.0)
+
+    def verbs(lat, lng):
+        recs, power = S.analytic_footprints(lat, lng, 800.0, de, az, 1)
+        a = np.ctypeslib.as_array(recs)
+        out = []
+        for k in range(len(power)):
+            rec = a[k]
+            v = eigenverb_model()
+            v.travel_time, v.length, v.width = rec["travel_time"], rec["length"], rec["width"]
+            v.position = tuple(rec["position"])
+            v.direction, v.grazing, v.sound_speed = rec["direction"], rec["grazing"], rec["sound_speed"]
+            v.source_de, v.source_az = rec["source_de"], rec["source_az"]
+            v.de_index, v.az_index = int(rec["de"]), int(rec["az"])
+            v.surface = v.bottom = v.caustic = v.upper = v.lower = 0
+            v.power = power[k]
+            out.append(v)
+        return out
+
+    fan = verbs(60.0, 179.99)
+    lng = np.degrees(np.array([v.position[2] for v in fan]))
+    assert lng.min() < 180.0 < lng.max()
+    eng, orc = both(fan, fan, freq, model, search_scale=3.0)
+    assert len(eng[0]) > 3 * len(fan)
+    compare(eng, orc)
+    other = verbs(60.0, -180.01)
+    eng, orc = both(fan, other, freq, model, search_scale=3.0)
+    assert len(eng[0]) == len(orc[0]) == 0
