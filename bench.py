@@ -54,7 +54,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--cpu-sample-steps", type=int, default=40)
+    ap.add_argument("--cpu-sample-steps", type=int, default=240,
+                    help="wave steps of the CPU samples (240 of 801: eigenrays to targets out to "
+                         "about 15 km are built inside the sample)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reverb", action="store_true",
                     help="skip the reverberation-scale sample (3601 x 181 rays, 4096 targets)")
@@ -284,7 +286,11 @@ def engine_arm(args, rank, world, dist):
     flops_launch = FLOPS_PER_RAY_TARGET_STEP * interior * nt
     achieved = flops_launch / cpa_launch_s / 1e12
     peaks = measure_fma_peaks()
-    fp32_peak = peaks["fp32"]
+    # the FP32 peak from the clock: 148 SMs x 128 FP32 lanes x 2 flops per
+    # FMA x the median SM clock sampled during the timed region
+    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    fp64_peak_clock = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
     out = {
         "metric": METRIC, "value": value, "unit": "ray-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -309,10 +315,14 @@ def engine_arm(args, rank, world, dist):
                      "traffic": NCU_TRAFFIC_CPA_F32,
                      "traffic_unit": "bytes per launch (ncu capture)",
                      "kernel": "k_cpa_f32",
-                     "peak_source": peaks["source"] + "; MEASURED_PEAKS.json has no FP32/FP64 CUDA-core figure",
-                     "fp64_peak": peaks["fp64"],
+                     "peak_source": "clock-derived: 148 SMs x 128 FP32 lanes x 2 x median SM clock %.0f MHz "
+                                    "(MEASURED_PEAKS.json has no FP32/FP64 CUDA-core figure)" % sm_mhz,
+                     "fp32_fma_loop_tflops": peaks["fp32"],
+                     "frac_of_fma_loop": (achieved / peaks["fp32"]) if peaks["fp32"] else None,
+                     "fp64_peak": fp64_peak_clock,
+                     "fp64_fma_loop_tflops": peaks["fp64"],
                      "fp64_form_cpa_frac_of_fp64_peak": (
-                         flops_launch / (kern64["cpa"] / 1000.0 / nsteps) / 1e12 / peaks["fp64"]) if peaks["fp64"] else None,
+                         flops_launch / (kern64["cpa"] / 1000.0 / nsteps) / 1e12 / fp64_peak_clock),
                      "algorithmic_flops_per_launch": flops_launch},
         "roofline_hbm": hbm_roofline(interior, cpa_launch_s),
         "clocks": clk,
@@ -492,9 +502,11 @@ def biverb_arm():
 def gradient_arm():
     """Gradient cost on the differentiable workload (1801 x 91 rays, 2000
     steps of 0.05 s, 64 receivers, 20-node profile grid, Rayleigh bottom):
-    the forward pass with bottom-parameter sensitivities, then the 40
-    perturbed propagations of the sound-speed-node differences as one
-    batch.  gradient_to_forward = (forward + gradient) / forward."""
+    the forward pass recorded for the adjoint (checkpoints every 50 steps,
+    each eigenray's partials, bottom sensitivities), then one reverse sweep
+    for the weighted sum of every eigenray's TL and travel time.
+    value = sweep / recorded forward; vs_plain_forward = (sweep + recording
+    overhead) / the forward without recording."""
     from underseamodelinglibrary_b200 import adjoint as A
     import numpy as np
     sc = A.AdjointScenario()
@@ -502,14 +514,26 @@ def gradient_arm():
     q = sc.queue(nodes)          # warm-up of the same shapes
     q.run(20 * sc.dt)
     del q
-    out = A.eigenray_gradients(sc, nodes)
-    jac = out["jacobian"]
-    return {"metric": "adjoint:fwd", "value": (out["ms_forward"] + out["ms_gradient"]) / out["ms_forward"],
-            "unit": "ratio", "higher_is_better": False, "ms_forward": out["ms_forward"],
-            "ms_gradient": out["ms_gradient"], "eigenrays": len(out["eigenrays"]),
-            "gradient_rows_with_topology_change": int(np.isnan(jac[:, 0, 0]).sum()),
-            "method": "bottom parameters exact (sensitivity mode); 20 sound-speed nodes by central "
-                      "differences (h = 1e-3 c_k) run as one batch of 40 propagations",
+    q = sc.queue(nodes)
+    q.timing(reset=True)
+    q.run(sc.time_max)
+    ms_plain = q.timing()["total_ms"]
+    del q
+    prop = A.Propagation(sc, nodes, checkpoint=50)
+    n = len(prop.eigenrays)
+    rng = np.random.default_rng(20261203)
+    w_tl, w_t = rng.normal(size=n), rng.normal(size=n)
+    prop.vjp(w_tl, w_t)          # first sweep makes the workspace
+    g, gb, ms_adj = prop.vjp(w_tl, w_t)
+    return {"metric": "adjoint:fwd", "value": ms_adj / prop.ms_forward, "unit": "ratio",
+            "higher_is_better": False, "ms_forward_recorded": prop.ms_forward, "ms_forward_plain": ms_plain,
+            "ms_adjoint": ms_adj,
+            "vs_plain_forward": (ms_adj + prop.ms_forward - ms_plain) / ms_plain,
+            "eigenrays": n, "checkpoint_interval": 50,
+            "gradient_norm": float(np.linalg.norm(g)),
+            "method": "reverse sweep: checkpoints every 50 steps, recompute per interval, adjoint of AB3, "
+                      "reflections and start-up with dual-number step Jacobians; eigenray partials recorded "
+                      "in the forward; bottom parameters exact (sensitivity mode)",
             "config": {"workload": "adjoint_munk_grid20_rayleigh_1801x91_2000steps_64rx"}}
 
 
@@ -629,7 +653,7 @@ def reference_arm(args, rank):
     if rank != 0:
         return None
     ncores = os.cpu_count() or 1
-    sc = cpu_sample_scenario(max(4, args.cpu_sample_steps // 4))
+    sc = cpu_sample_scenario(args.cpu_sample_steps)
     for _ in range(args.warmup if args.warmup < 1 else 1):
         cpu_run(cpu_sample_scenario(2), ncores)
     vals = []

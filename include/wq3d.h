@@ -16,7 +16,16 @@
  * exactly as the reference seq_vector fans hold them.
  *
  * Device memory is owned by the library.  Host arrays passed in are copied
- * during the call; the caller keeps ownership of them.
+ * during the call; the caller keeps ownership of them.  An ocean lives on
+ * the device that was current when it was created; evaluating it with
+ * another device current, or building a queue for another device from it,
+ * returns WQ3D_ERR_INVALID.
+ *
+ * The library keeps per-device state between calls (the staging array's
+ * address of wq3d_ocean_sound_speed_noalloc, the bistatic eigenverb
+ * workspace).  cudaDeviceReset destroys the device objects behind that
+ * state: do not call into the library after a cudaDeviceReset in the same
+ * process.
  */
 #ifndef WQ3D_H
 #define WQ3D_H
@@ -384,6 +393,17 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* desc,
                       wq3d_queue** out);
 int wq3d_queue_destroy(wq3d_queue* q);
 
+/* Cache of destroyed queues.  wq3d_queue_destroy keeps up to max_queues
+ * queues (2 by default; the oldest is freed first) whose buffers still have
+ * their creation sizes (no eigenverb listener, reflection buffer not grown,
+ * no sensitivity or adjoint mode), and wq3d_queue_create re-initialises one
+ * of the same device, fan, frequency, target and eigenray-capacity shape
+ * instead of allocating: a create-run-destroy loop then allocates and
+ * instantiates its graphs once.  Results are those of a fresh queue.
+ * max_queues = 0 frees the cached queues and turns the cache off.  The
+ * reference has no counterpart (each wave_queue owns its fronts). */
+int wq3d_set_queue_cache(size_t max_queues);
+
 /* Sensitivity mode (call before the first step): every eigenray also
  * carries the exact derivatives of its transmission loss (dB, the same at
  * every frequency) with respect to the bottom's Rayleigh parameters --
@@ -394,6 +414,38 @@ int wq3d_queue_destroy(wq3d_queue* q);
  * propagation.  No reference counterpart: the reference has no
  * differentiation. */
 int wq3d_queue_enable_sensitivity(wq3d_queue* q);
+
+/* Adjoint recording (call before the first step): while the queue runs,
+ * every ray's state is kept every checkpoint_interval steps (max_steps
+ * bounds the run) and every eigenray record (at most max_eigenrays; 0 for
+ * 65536) gets the partial derivatives of its first-frequency TL and its
+ * travel time with respect to the fronts it was built from.
+ * wq3d_queue_adjoint then runs the reverse sweep.  Supported oceans: a
+ * profile_grid<1> linear in depth (its nodes, at most 64 and more than a
+ * step's reach apart, are the parameters), flat or sloped boundaries with
+ * constant, fluid Rayleigh (no shear) or Eckart loss, no volume layers;
+ * hybrid Gaussian spreading; targets required.  Other oceans return
+ * WQ3D_ERR_UNSUPPORTED.  No reference counterpart: the reference has no
+ * differentiation. */
+int wq3d_queue_enable_adjoint(wq3d_queue* q, int checkpoint_interval, size_t max_steps,
+                              size_t max_eigenrays);
+
+/* The reverse sweep at the forward pass's eigenray topology.  For weights
+ * w_tl[k] and w_time[k] of the eigenrays rays[k] (records as
+ * wq3d_queue_take_eigenrays returned them), grad[j] receives
+ *   sum_k w_tl[k] dTL_k / dc_j + w_time[k] dT_k / dc_j
+ * for the num_nodes nodes c_j of the profile grid (TL of the first
+ * frequency, dB; travel time, s; c_j in m/s).  From each checkpoint, last
+ * first, the states of the rays that reach a weighted eigenray are
+ * recomputed, the eigenrays' partials are taken to them, and the sweep runs
+ * back to the previous checkpoint; the start-up (init_wave and the RK3
+ * start, wave_queue.cc:114-150) closes it.  ms (may be NULL) receives the
+ * sweep's device time.  A record the forward did not see returns
+ * WQ3D_ERR_INVALID; an eigenray whose beam walk outran the recorded cells,
+ * or a step that reached nodes beyond its window, returns
+ * WQ3D_ERR_NUMERIC.  No reference counterpart. */
+int wq3d_queue_adjoint(wq3d_queue* q, const wq3d_eigenray* rays, const double* w_tl,
+                       const double* w_time, size_t n, double* grad, size_t num_nodes, double* ms);
 
 /* The three derivatives of each eigenray that wq3d_queue_take_eigenrays
  * would return next, in the same order (3 values per eigenray; NaN when

@@ -225,6 +225,107 @@ def test_linear_slope_rayleigh_reduced_parity(engine):
     compare_fronts(q.curr(), o.curr(), rel=1e-9)
 
 
+def test_linear_slope_rayleigh_full_fan_parity(engine):
+    """The sloped Rayleigh workload at full D/E width against the oracle:
+    all 1801 D/E rays x all 1024 targets x 5 frequencies on six AZ columns
+    (every 16th column of the 91-ray fan: 0, 64, ..., 320 deg), 12 s (240
+    steps).  Both the plain FP64 form and the FP32-screened form must
+    reproduce the oracle's eigenrays."""
+    sc = S.linear_slope_rayleigh()
+    sc["az"] = u.seq_linear(0.0, 64.0, 6)
+    sc["time_max"] = 12.0
+    o = S.build_queue(sc, OracleQueue)
+    o.run(sc["time_max"])
+    orc = o.take_eigenrays()
+    assert len(orc) > 2000
+    for precision in (_abi.FP64, _abi.FP32C):
+        q = S.build_queue(sc, u.wave_queue, precision=precision)
+        q.run(sc["time_max"])
+        assert q.time() == o.time()
+        compare_eigenrays(q.take_eigenrays(), orc)
+
+
+def test_reflect_loss_reference_values(engine):
+    """The engine's loss models at the reference's known answers: the
+    Rayleigh limestone preset at normal incidence and 1 kHz, 3.672875 dB
+    within 4e-4 percent (ocean/test/reflect_loss_test.cc:254-278), and the
+    Eckart surface loss at 10 deg against Jones et al. figures 2-5 within 1
+    percent (:312-373)."""
+    u.compute_earth_radius(45.0)
+    oc = u.ocean_model(u.boundary_flat(), u.boundary_flat(1000.0, u.reflect_loss_rayleigh("limestone")),
+                       u.profile_linear())
+    a, _ = oc.reflect_loss(1, np.array([math.pi / 2]), np.array([1000.0]))
+    assert abs(float(a.ravel()[0]) - 3.672875) <= 4e-4 / 100.0 * 3.672875
+    for wind, freq, expect in ((4.6, 3150.0, 1.15), (4.6, 5000.0, 2.90), (14.4, 1000.0, 11.15),
+                               (14.4, 5000.0, 278.76)):
+        oc = u.ocean_model(u.boundary_flat(0.0, u.reflect_loss_eckart(wind)), u.boundary_flat(1000.0),
+                           u.profile_linear())
+        a, _ = oc.reflect_loss(0, np.array([math.radians(10.0)]), np.array([freq]))
+        assert abs(float(a.ravel()[0]) - expect) <= 0.01 * expect, (wind, freq, a)
+
+
+def test_nan_profile_node_reports_numeric(engine):
+    """A NaN sound-speed node given to wq3d_ocean_create reaches the rays
+    that cross its depth interval; the per-step finiteness check in the
+    advance kernel turns that into WQ3D_ERR_NUMERIC (no fault, no trap),
+    and a healthy queue runs afterwards in the same process."""
+    u.compute_earth_radius(45.0)
+    R = u.earth_radius()
+    depth = np.linspace(0.0, 5000.0, 10)
+    nodes = 1500.0 + 0.0163 * depth
+    nodes[3] = np.nan
+    ax = u.seq_linear(R, -5000.0 / 9.0, 10)
+    freq, de, az = u.seq_log(1000.0, 1.0, 1), u.seq_rayfan(-90.0, 90.0, 31), u.seq_linear(0.0, 30.0, 7)
+    pos = u.wposition1(45.0, -45.0, -1000.0)
+    bad = u.ocean_model(u.boundary_flat(), u.boundary_flat(5000.0),
+                        u.profile_grid(u.data_grid([ax], nodes)))
+    q = u.wave_queue(bad, freq, pos, de, az, 0.1)
+    with pytest.raises(u.EngineError) as ei:
+        q.run(5.0)
+    assert ei.value.code == _abi.WQ3D_ERR_NUMERIC
+    assert "NaN or Inf" in str(ei.value)
+    nodes[3] = 1500.0 + 0.0163 * depth[3]
+    good = u.ocean_model(u.boundary_flat(), u.boundary_flat(5000.0),
+                         u.profile_grid(u.data_grid([ax], nodes)))
+    q = u.wave_queue(good, freq, pos, de, az, 0.1)
+    q.run(5.0)
+    assert q.time() >= 5.0
+
+
+def test_cached_queue_matches_fresh(engine):
+    """Queues re-initialised from the cache of destroyed queues compute
+    what fresh queues compute, bit for bit: the same inputs twice, then
+    another source depth and ocean on the same shapes."""
+    def run(sc):
+        q = S.build_queue(sc, u.wave_queue)
+        q.run(sc["time_max"])
+        rays = q.take_eigenrays()
+        front = q.curr()
+        rt = (np.array(front.rho, copy=True), np.array(front.theta, copy=True))
+        del q
+        return rays.arrays(), rt
+
+    sc1 = S.linear_slope_rayleigh(num_de=181, num_az=19, n_range=8, n_depth=8, time_max=6.0)
+    sc2 = S.linear_slope_rayleigh(num_de=181, num_az=19, n_range=8, n_depth=8, time_max=6.0)
+    sc2["pos"] = u.wposition1(45.0, -45.0, -120.0)
+    sc2["ocean"] = u.ocean_model(u.boundary_flat(), u.boundary_flat(3000.0, u.reflect_loss_rayleigh(1.5, 1.1, 0.5)),
+                                 u.profile_linear(1500.0, 0.0163))
+    try:
+        engine.wq3d_set_queue_cache(0)
+        fresh1, f1 = run(sc1)
+        fresh2, f2 = run(sc2)
+        engine.wq3d_set_queue_cache(2)
+        outs = [run(sc1), run(sc1), run(sc2), run(sc1)]
+    finally:
+        engine.wq3d_set_queue_cache(2)
+    for (got, front), (want, wf) in zip(outs, [(fresh1, f1), (fresh1, f1), (fresh2, f2), (fresh1, f1)]):
+        assert set(got) == set(want)
+        for k in want:
+            assert np.array_equal(got[k], want[k]), k
+        assert np.array_equal(front[0], wf[0]) and np.array_equal(front[1], wf[1])
+    assert len(fresh1["time"]) > 50 and len(fresh2["time"]) > 50
+
+
 def test_listener_order_and_collection(engine):
     """add_eigenray arrives in (step, t1, t2, de, az) order, check_eigenrays
     once per step; eigenray_collection sums them"""

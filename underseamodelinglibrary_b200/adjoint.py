@@ -3,21 +3,26 @@ with respect to a piecewise-linear sound-speed profile (profile_grid<1>
 nodes) and the Rayleigh bottom parameters, at the forward pass's frozen
 eigenray topology.
 
+* d TL / d c_j and d T / d c_j (profile nodes): the engine's reverse sweep
+  (wq3d_queue_enable_adjoint / wq3d_queue_adjoint).  The forward pass keeps
+  every ray's state every K steps and each eigenray's partial derivatives
+  with respect to the fronts it was built from; the sweep recomputes each
+  checkpoint interval and runs the adjoint of the AB3 steps, the reflection
+  chains and the start-up back through it.  One sweep gives one weighted
+  sum of the rows (a vector-Jacobian product); a row of the Jacobian is a
+  sweep with one unit weight.
 * d TL / d bottom (density ratio, speed ratio, attenuation in dB per
   wavelength): exact, from the GPU's sensitivity mode
   (wq3d_queue_enable_sensitivity).  The reflection loss does not move the
-  rays, so the derivative of each ray's accumulated loss is the whole
-  derivative; travel time does not depend on these parameters.
-* d TL / d c_k and d T / d c_k: central differences of the FP64 GPU form
-  with step h = rel_step * c_k, all 2 x nodes perturbed propagations run
-  together by wq3d_batch_run.  An eigenray whose (step, target, D/E, AZ)
-  bracket is not found in both perturbed runs gets NaN rows.  This is a
-  numerical derivative of the discrete model, not an adjoint sweep.
+  rays, so each ray's accumulated loss derivative is the whole derivative;
+  travel time does not depend on these parameters.
+* ``finite_differences`` keeps the batched central differences of the FP64
+  GPU form (2 x nodes perturbed propagations run together), the check the
+  adjoint is held to.
 
-``eigenray_gradients`` returns the Jacobian; ``EigenrayTLTime`` wraps it as
-a torch.autograd.Function whose forward gives (TL at each frequency's
-first entry, travel time) per eigenray and whose backward applies the
-Jacobian's transpose.
+``EigenrayTLTime`` is a torch.autograd.Function over these: forward gives
+(TL at the first frequency, travel time) per eigenray, backward is one
+reverse sweep.
 """
 import math
 
@@ -53,6 +58,7 @@ class AdjointScenario:
         self.earth_radius = T.earth_radius()
         self.num_de, self.num_az = num_de, num_az
         self.dt = dt
+        self.n_steps = n_steps
         self.time_max = (n_steps - 0.5) * dt
         self.freq = T.seq_log(freq, 1.0, 1)
         self.depth = depth
@@ -88,47 +94,80 @@ def _key(r):
     return (r.step, r.t1, r.t2, r.de_index, r.az_index)
 
 
-def eigenray_gradients(sc, nodes, rel_step=1e-3, ssp=True):
-    """Forward propagation plus gradients.  Returns a dict with
-    ``eigenrays`` (eigenray_model list, reference order), ``values`` (n x 2:
-    TL of the first frequency, travel time), ``jacobian`` (n x 2 x
-    (nodes + 3)), ``ms_forward`` and ``ms_gradient`` (device ms)."""
+class Propagation:
+    """One forward pass recorded for the reverse sweep: ``eigenrays``,
+    ``values`` (n x 2: TL of the first frequency, travel time),
+    ``d_bottom`` (n x 3, exact TL derivatives with respect to the bottom
+    parameters) and ``ms_forward`` (device ms).  ``vjp`` and ``rows`` run
+    reverse sweeps on it."""
+
+    def __init__(self, sc, nodes, checkpoint=50, precision=_abi.FP64, max_eigenrays=0):
+        self.nodes = np.asarray(nodes, dtype=np.float64)
+        q = sc.queue(self.nodes, precision=precision)
+        q.enable_sensitivity()
+        q.enable_adjoint(checkpoint, sc.n_steps + 16, max_eigenrays)
+        q.timing(reset=True)
+        q.run(sc.time_max)
+        self.ms_forward = q.timing()["total_ms"]
+        self.queue = q
+        self.eigenrays = q.take_eigenrays()
+        cols = self.eigenrays.arrays()
+        n = len(self.eigenrays)
+        self.values = np.stack([cols["intensity"][:, 0], cols["time"]], axis=1) if n else np.zeros((0, 2))
+        self.d_bottom = cols.get("d_intensity_d_bottom", np.zeros((n, 3)))
+
+    def vjp(self, w_tl, w_time):
+        """(d/d nodes, d/d bottom, device ms) of sum_k w_tl[k] TL_k +
+        w_time[k] T_k: one reverse sweep."""
+        w_tl = np.asarray(w_tl, dtype=np.float64)
+        w_time = np.asarray(w_time, dtype=np.float64)
+        g, ms = self.queue.adjoint(self.eigenrays, w_tl, w_time, self.nodes.size)
+        gb = w_tl @ self.d_bottom if len(w_tl) else np.zeros(3)
+        return g, gb, ms
+
+    def rows(self, indices):
+        """Jacobian rows (len(indices) x 2 x (nodes + 3)) of the chosen
+        eigenrays: two unit-weight sweeps per eigenray."""
+        n = len(self.eigenrays)
+        out = np.zeros((len(indices), 2, self.nodes.size + 3))
+        for r, i in enumerate(indices):
+            w = np.zeros(n)
+            w[i] = 1.0
+            out[r, 0, :self.nodes.size], _ = self.queue.adjoint(self.eigenrays, w, np.zeros(n), self.nodes.size)
+            out[r, 1, :self.nodes.size], _ = self.queue.adjoint(self.eigenrays, np.zeros(n), w, self.nodes.size)
+            out[r, 0, self.nodes.size:] = self.d_bottom[i]
+        return out
+
+
+def finite_differences(sc, nodes, rel_step=1e-3):
+    """Central differences of the FP64 GPU form for every eigenray and
+    node: (eigenrays, jacobian n x 2 x nodes, device ms).  An eigenray whose
+    (step, target, D/E, AZ) bracket is not found in both perturbed runs
+    gets NaN."""
     nodes = np.asarray(nodes, dtype=np.float64)
-    nk = nodes.size
     q = sc.queue(nodes)
-    q.enable_sensitivity()
-    q.timing(reset=True)
     q.run(sc.time_max)
-    ms_fwd = q.timing()["total_ms"]
     rays = q.take_eigenrays()
-    n = len(rays)
-    values = np.array([[r.intensity[0], r.travel_time] for r in rays]).reshape(n, 2)
-    jac = np.zeros((n, 2, nk + 3))
-    for i, r in enumerate(rays):
-        jac[i, 0, nk:] = r.d_intensity_d_bottom
-    ms_grad = 0.0
-    if ssp and n > 0:
-        qs, hs = [], []
-        for k in range(nk):
-            h = rel_step * abs(nodes[k])
-            hs.append(h)
-            for sgn in (1.0, -1.0):
-                c = nodes.copy()
-                c[k] += sgn * h
-                qs.append(sc.queue(c))
-        _, ms_grad = run_batch(qs, sc.time_max)
-        index = {_key(r): i for i, r in enumerate(rays)}
-        for k in range(nk):
-            plus = {_key(r): r for r in qs[2 * k].take_eigenrays()}
-            minus = {_key(r): r for r in qs[2 * k + 1].take_eigenrays()}
-            for kk, i in index.items():
-                if kk in plus and kk in minus:
-                    jac[i, 0, k] = (plus[kk].intensity[0] - minus[kk].intensity[0]) / (2 * hs[k])
-                    jac[i, 1, k] = (plus[kk].travel_time - minus[kk].travel_time) / (2 * hs[k])
-                else:
-                    jac[i, :, k] = np.nan
-    return {"eigenrays": rays, "values": values, "jacobian": jac, "ms_forward": ms_fwd,
-            "ms_gradient": ms_grad}
+    nk = nodes.size
+    qs, hs = [], []
+    for k in range(nk):
+        h = rel_step * abs(nodes[k])
+        hs.append(h)
+        for sgn in (1.0, -1.0):
+            c = nodes.copy()
+            c[k] += sgn * h
+            qs.append(sc.queue(c))
+    _, ms = run_batch(qs, sc.time_max)
+    jac = np.full((len(rays), 2, nk), np.nan)
+    index = {_key(r): i for i, r in enumerate(rays)}
+    for k in range(nk):
+        plus = {_key(r): r for r in qs[2 * k].take_eigenrays()}
+        minus = {_key(r): r for r in qs[2 * k + 1].take_eigenrays()}
+        for kk, i in index.items():
+            if kk in plus and kk in minus:
+                jac[i, 0, k] = (plus[kk].intensity[0] - minus[kk].intensity[0]) / (2 * hs[k])
+                jac[i, 1, k] = (plus[kk].travel_time - minus[kk].travel_time) / (2 * hs[k])
+    return rays, jac, ms
 
 
 def _torch_function():
@@ -136,25 +175,24 @@ def _torch_function():
 
     class EigenrayTLTime(torch.autograd.Function):
         """forward(nodes[k], bottom[3], scenario) -> (n, 2) tensor of
-        (TL, travel time) per eigenray; backward applies the Jacobian of
-        eigenray_gradients (NaN rows, for eigenrays whose topology changes
-        under the perturbation, contribute zero)."""
+        (TL, travel time) per eigenray; backward is one reverse sweep of the
+        engine's adjoint (and the exact bottom sensitivities)."""
 
         @staticmethod
         def forward(ctx, nodes, bottom, sc):
             b = tuple(float(x) for x in bottom.detach().cpu().numpy())
             if b != sc.bottom:
                 sc.bottom = b
-            out = eigenray_gradients(sc, nodes.detach().cpu().numpy())
-            ctx.save_for_backward(torch.as_tensor(np.nan_to_num(out["jacobian"]), dtype=nodes.dtype))
-            ctx.nk = nodes.numel()
-            return torch.as_tensor(out["values"], dtype=nodes.dtype)
+            prop = Propagation(sc, nodes.detach().cpu().numpy())
+            ctx.prop = prop
+            ctx.dtype = nodes.dtype
+            return torch.as_tensor(prop.values, dtype=nodes.dtype)
 
         @staticmethod
         def backward(ctx, grad_out):
-            (jac,) = ctx.saved_tensors
-            g = torch.einsum("ij,ijk->k", grad_out.to(jac.dtype), jac)
-            return g[:ctx.nk], g[ctx.nk:], None
+            g = grad_out.detach().cpu().numpy().astype(np.float64)
+            gn, gb, _ = ctx.prop.vjp(g[:, 0], g[:, 1])
+            return torch.as_tensor(gn, dtype=ctx.dtype), torch.as_tensor(gb, dtype=ctx.dtype), None
 
     return EigenrayTLTime
 

@@ -21,7 +21,7 @@ OBJECTS = [(f, f, []) for f in SOURCES] + [
     ("wq3d_kernels_analytic.cu", "wq3d_kernels.cu",
      ["-DWQ3D_WITH_GRID=0", "-DWQ3D_KERNEL_NS=analytic", "-DWQ3D_STEP_KERNELS_ONLY=1"]),
 ]
-HEADERS = ["wq3d_engine.cuh", "wq3d_models.cuh"]
+HEADERS = ["wq3d_engine.cuh", "wq3d_models.cuh", "wq3d_dual.cuh", "wq3d_adjoint.cuh"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "--fmad=false", "-lineinfo",

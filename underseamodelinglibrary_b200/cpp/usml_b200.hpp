@@ -39,6 +39,9 @@ inline double to_degrees(double t) { return t * (180.0 / M_PI); }
 class seq_vector {
    public:
     typedef std::shared_ptr<const seq_vector> csptr;
+    /** the axis search the engine uses for this sequence (find_index of
+     * seq_linear.h:89-94, seq_log.h:88-94 or seq_data.cc:15-36) */
+    virtual int axis_kind() const { return WQ3D_AXIS_DATA; }
     size_t size() const { return _data.size(); }
     double operator()(size_t i) const { return _data[i]; }
     double increment(size_t i) const {
@@ -55,6 +58,7 @@ class seq_vector {
 
 class seq_linear : public seq_vector {
    public:
+    int axis_kind() const override { return WQ3D_AXIS_LINEAR; }
     seq_linear(double first, double increment, int size) { init(first, increment, (size_t)size); }
     seq_linear(double first, double increment, double last) {
         const size_t n = (increment == 0.0)
@@ -77,6 +81,7 @@ class seq_linear : public seq_vector {
 
 class seq_log : public seq_vector {
    public:
+    int axis_kind() const override { return WQ3D_AXIS_LOG; }
     seq_log(double first, double increment, int size) { init(first, increment, (size_t)size); }
     seq_log(double first, double increment, double last) {
         const size_t n = (increment == 1.0)
@@ -138,6 +143,53 @@ class seq_rayfan : public seq_data {
         for (size_t n = 0; n < size; ++n) v[n] = center + std::tan(a0 + scale * (double)n) * spread;
         init(v);
     }
+};
+
+/* data_grid<N> (types/data_grid.h, gen_grid.h:83-520): values on up to
+ * three axes, row-major with the last axis fastest; linear interpolation
+ * with edge limiting on every axis unless set otherwise
+ * (data_grid.h:315-316) */
+class data_grid {
+   public:
+    typedef std::shared_ptr<const data_grid> csptr;
+    data_grid(const std::vector<seq_vector::csptr>& axes, const std::vector<double>& data)
+        : _axes(axes), _data(data) {
+        if (axes.empty() || axes.size() > 3) throw std::invalid_argument("data_grid takes 1 to 3 axes");
+        size_t n = 1;
+        for (const auto& a : axes) n *= a->size();
+        if (n != data.size()) throw std::invalid_argument("data_grid: data size does not match the axes");
+        for (size_t d = 0; d < 3; ++d) {
+            _interp[d] = WQ3D_INTERP_LINEAR;
+            _edge[d] = 1;
+        }
+    }
+    size_t dim() const { return _axes.size(); }
+    const seq_vector::csptr& axis(size_t d) const { return _axes.at(d); }
+    /** data_grid::interp_type (data_grid.h:137-145): WQ3D_INTERP_* */
+    void interp_type(size_t d, int kind) { _interp[d] = kind; }
+    int interp_type(size_t d) const { return _interp[d]; }
+    /** data_grid::edge_limit (data_grid.h:159-166) */
+    void edge_limit(size_t d, bool on) { _edge[d] = on ? 1 : 0; }
+    const std::vector<double>& data() const { return _data; }
+    /** the engine's description; the pointers stay valid while this grid lives */
+    void fill(wq3d_grid_desc* g) const {
+        g->ndim = (int)_axes.size();
+        for (size_t d = 0; d < _axes.size(); ++d) {
+            g->axis[d] = _axes[d]->data().data();
+            g->axis_inc[d] = _axes[d]->increments().data();
+            g->axis_size[d] = _axes[d]->size();
+            g->axis_kind[d] = _axes[d]->axis_kind();
+            g->interp[d] = _interp[d];
+            g->edge_limit[d] = _edge[d];
+        }
+        g->data = _data.data();
+    }
+
+   private:
+    std::vector<seq_vector::csptr> _axes;
+    std::vector<double> _data;
+    int _interp[3];
+    int _edge[3];
 };
 
 /* wposition::earth_radius and compute_earth_radius (types/wposition.cc) */
@@ -217,6 +269,13 @@ class wposition {
     size_t size2() const { return _n2; }
     wposition1& at(size_t r, size_t c) { return _v[r * _n2 + c]; }
     const wposition1& at(size_t r, size_t c) const { return _v[r * _n2 + c]; }
+    /* element accessors of types/wposition.h */
+    double latitude(size_t r, size_t c) const { return at(r, c).latitude(); }
+    double longitude(size_t r, size_t c) const { return at(r, c).longitude(); }
+    double altitude(size_t r, size_t c) const { return at(r, c).altitude(); }
+    void latitude(size_t r, size_t c, double v) { at(r, c).latitude(v); }
+    void longitude(size_t r, size_t c, double v) { at(r, c).longitude(v); }
+    void altitude(size_t r, size_t c, double v) { at(r, c).altitude(v); }
     std::vector<double> packed() const {
         const size_t n = _v.size();
         std::vector<double> out(3 * n);
@@ -261,7 +320,9 @@ class profile_model {
         d->flat_earth = _flat ? 1 : 0;
         d->attenuation = _atten ? _atten->kind : WQ3D_ATTEN_THORP;
         d->attenuation_coef = _atten ? _atten->coef : 0.0;
+        fill_grid(d);
     }
+    virtual void fill_grid(wq3d_profile_desc*) const {}
     virtual ~profile_model() {}
 
    protected:
@@ -301,6 +362,39 @@ struct profile_munk : profile_model {
     }
 };
 
+/* profile_catenary (ocean/profile_catenary.cc:14-29): c = c1 cosh((z - z1) / g1) */
+struct profile_catenary : profile_model {
+    profile_catenary(double c1, double g1, double z1, const attenuation_model::csptr& a = nullptr)
+        : profile_model(a) {
+        _kind = WQ3D_PROFILE_CATENARY;
+        _p[0] = c1;
+        _p[1] = g1;
+        _p[2] = z1;
+    }
+};
+
+/* profile_n2 (ocean/profile_n2.cc:14-24): the n^2 linear profile */
+struct profile_n2 : profile_model {
+    profile_n2(double c0, double g0, const attenuation_model::csptr& a = nullptr) : profile_model(a) {
+        _kind = WQ3D_PROFILE_N2;
+        _p[0] = c0;
+        _p[1] = g0;
+    }
+};
+
+/* profile_grid<N> (ocean/profile_grid.h:68-130): sound speed on a grid over
+ * (rho[, theta[, phi]]) */
+struct profile_grid : profile_model {
+    explicit profile_grid(const types::data_grid::csptr& grid, const attenuation_model::csptr& a = nullptr)
+        : profile_model(a), _grid(grid) {
+        _kind = WQ3D_PROFILE_GRID;
+    }
+    void fill_grid(wq3d_profile_desc* d) const { _grid->fill(&d->grid); }
+
+   private:
+    types::data_grid::csptr _grid;
+};
+
 struct reflect_loss_model {
     typedef std::shared_ptr<const reflect_loss_model> csptr;
     wq3d_reflect_loss_desc d{WQ3D_LOSS_DEFAULT, {0, 0, 0, 0, 0}};
@@ -312,6 +406,12 @@ struct reflect_loss_rayleigh : reflect_loss_model {
     reflect_loss_rayleigh(double density, double speed, double att = 0.0, double shear = 0.0, double satt = 0.0) {
         d = {WQ3D_LOSS_RAYLEIGH, {density, speed, att, shear, satt}};
     }
+};
+
+/* reflect_loss_eckart (ocean/reflect_loss_eckart.h:76-85): rough-surface
+ * loss from the wind speed (m/s) */
+struct reflect_loss_eckart : reflect_loss_model {
+    explicit reflect_loss_eckart(double wind_speed) { d = {WQ3D_LOSS_ECKART, {wind_speed, 0, 0, 0, 0}}; }
 };
 
 /* scattering strength models (ocean/scattering_{constant,lambert,chapman}.h),
@@ -383,6 +483,25 @@ class boundary_slope : public boundary_model {
     reflect_loss_model::csptr _loss;
 };
 
+/* boundary_grid<N> (ocean/boundary_grid.h:40-204): boundary rho on a grid
+ * over theta[, phi]; the Rayleigh sand loss unless one is given
+ * (boundary_grid.h:56-59) */
+class boundary_grid : public boundary_model {
+   public:
+    explicit boundary_grid(const types::data_grid::csptr& grid, const reflect_loss_model::csptr& loss = nullptr,
+                           const scattering_model::csptr& scattering = nullptr)
+        : boundary_model(scattering), _grid(grid), _loss(loss) {}
+    void fill(wq3d_boundary_desc* d) const override {
+        d->kind = WQ3D_BOUNDARY_GRID;
+        _grid->fill(&d->grid);
+        d->loss = _loss ? _loss->d : wq3d_reflect_loss_desc{WQ3D_LOSS_DEFAULT, {0, 0, 0, 0, 0}};
+    }
+
+   private:
+    types::data_grid::csptr _grid;
+    reflect_loss_model::csptr _loss;
+};
+
 /* volume_flat (ocean/volume_flat.h:32-37): a scattering layer at a
  * constant depth */
 struct volume_model {
@@ -410,7 +529,7 @@ class ocean_model {
     typedef std::shared_ptr<const ocean_model> csptr;
     ocean_model(const boundary_model::csptr& surface, const boundary_model::csptr& bottom,
                 const profile_model::csptr& profile)
-        : _surface(surface), _bottom(bottom) {
+        : _surface(surface), _bottom(bottom), _profile(profile) {
         _d.earth_radius = types::earth::radius();
         profile->fill(&_d.profile);
         surface->fill(&_d.surface);
@@ -442,6 +561,7 @@ class ocean_model {
 
    private:
     boundary_model::csptr _surface, _bottom;
+    profile_model::csptr _profile;
     std::vector<volume_model::csptr> _volume;
     wq3d_ocean_desc _d{};
     mutable std::shared_ptr<wq3d_ocean> _h;
@@ -740,6 +860,19 @@ class reflection_listener {
                          size_t type) = 0;
 };
 
+/* Host copy of one wavefront (waveq3d/wave_front.h:152-258), the data
+ * the reference's wave_queue::curr()/next()/prev()/past() expose; arrays are
+ * num_de x num_az row-major (de, az), attenuation and phase with the
+ * frequency fastest. */
+struct wave_front {
+    size_t num_de = 0, num_az = 0, num_freq = 0;
+    std::vector<double> rho, theta, phi, sound_speed, distance, path_length, attenuation, phase;
+    std::vector<double> ndir[3], pos_grad[3], ndir_grad[3], sound_grad[3];
+    std::vector<int32_t> surface, bottom, caustic, upper, lower;
+    std::vector<uint8_t> on_edge;
+    size_t index(size_t de, size_t az) const { return de * num_az + az; }
+};
+
 /* wave_queue (waveq3d/wave_queue.h:122-264) */
 class wave_queue {
    public:
@@ -818,6 +951,12 @@ class wave_queue {
         return t;
     }
     double time_step() const { return _time_step; }
+    /** wave_queue::past()/prev()/curr()/next() (wave_queue.h:179-216), as
+     * host copies of the fronts */
+    wave_front past() const { return front(WQ3D_FRONT_PAST); }
+    wave_front prev() const { return front(WQ3D_FRONT_PREV); }
+    wave_front curr() const { return front(WQ3D_FRONT_CURR); }
+    wave_front next() const { return front(WQ3D_FRONT_NEXT); }
     size_t num_de() const { return _num_de; }
     size_t num_az() const { return _num_az; }
     /** steps taken since the queue was made (AB3 and start-up alike) */
@@ -865,6 +1004,43 @@ class wave_queue {
     }
 
    private:
+    wave_front front(int which) const {
+        wave_front f;
+        f.num_de = _num_de;
+        f.num_az = _num_az;
+        f.num_freq = _freq->size();
+        const size_t n = _num_de * _num_az, nf = f.num_freq;
+        for (auto* v : {&f.rho, &f.theta, &f.phi, &f.sound_speed, &f.distance, &f.path_length}) v->resize(n);
+        for (int k = 0; k < 3; ++k)
+            for (auto* v : {&f.ndir[k], &f.pos_grad[k], &f.ndir_grad[k], &f.sound_grad[k]}) v->resize(n);
+        f.attenuation.resize(n * nf);
+        f.phase.resize(n * nf);
+        for (auto* v : {&f.surface, &f.bottom, &f.caustic, &f.upper, &f.lower}) v->resize(n);
+        f.on_edge.resize(n);
+        wq3d_front_view view{};
+        view.rho = f.rho.data();
+        view.theta = f.theta.data();
+        view.phi = f.phi.data();
+        for (int k = 0; k < 3; ++k) {
+            view.ndir[k] = f.ndir[k].data();
+            view.pos_grad[k] = f.pos_grad[k].data();
+            view.ndir_grad[k] = f.ndir_grad[k].data();
+            view.sound_grad[k] = f.sound_grad[k].data();
+        }
+        view.sound_speed = f.sound_speed.data();
+        view.distance = f.distance.data();
+        view.path_length = f.path_length.data();
+        view.attenuation = f.attenuation.data();
+        view.phase = f.phase.data();
+        view.surface = f.surface.data();
+        view.bottom = f.bottom.data();
+        view.caustic = f.caustic.data();
+        view.upper = f.upper.data();
+        view.lower = f.lower.data();
+        view.on_edge = f.on_edge.data();
+        check(wq3d_queue_get_front(_q.get(), which, &view));
+        return f;
+    }
     template <class L>
     void drop(std::vector<L*>& v, L* l) {
         v.erase(std::remove(v.begin(), v.end(), l), v.end());

@@ -14,7 +14,9 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -132,6 +134,7 @@ struct wq3d_ocean {
     OceanDev dev;   /* device pointers, passed to kernels        */
     OceanDev host;  /* host pointers, for host-side evaluations  */
     double build_radius;
+    int device = 0;  /* the device holding dmem: where the ocean can be used */
     std::vector<std::vector<double>> store;  /* host copies of grid arrays */
     std::vector<void*> dmem;                 /* device copies             */
     ~wq3d_ocean() {
@@ -271,6 +274,24 @@ struct wq3d_queue {
     bool gridded = false;
     void (*k_reflect_fn)(const QueueDev, int) = analytic::k_reflect;
     void (*k_advance_fn)(const QueueDev, int) = analytic::k_advance;
+    /* set while wq3d_queue_create re-initialises a queue taken from the
+     * cache of destroyed queues: uploads then copy into the buffers the
+     * queue already has */
+    bool reuse = false;
+    char* ring = nullptr;   /* the wavefront ring's allocation */
+    size_t ring_bytes = 0;
+    /* adjoint workspace (wq3d_queue_adjoint), made on first use */
+    struct AdjWork {
+        double* seg = nullptr;
+        uint32_t* chain = nullptr;
+        double* seed = nullptr;
+        double* lam = nullptr;
+        int64_t* last = nullptr;
+        double* grad = nullptr;
+        double* w = nullptr;
+        uint32_t* err = nullptr;
+        size_t w_cap = 0;
+    } adjw;
     std::vector<wq3d_eigenray> h_rec;
     std::vector<double> h_rinten, h_rphase, h_rsens;
     std::vector<wq3d_reflection> h_refl;
@@ -439,8 +460,12 @@ struct wq3d_queue {
     template <class T>
     int upload(const T** out, const std::vector<T>& v) {
         T* p = nullptr;
-        int rc = alloc(&p, v.size());
-        if (rc) return rc;
+        if (reuse && *out) {
+            p = const_cast<T*>(*out); /* same size: the cache key fixes every length */
+        } else {
+            int rc = alloc(&p, v.size());
+            if (rc) return rc;
+        }
         if (!v.empty()) WQ_CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
         *out = p;
         return WQ3D_OK;
@@ -470,6 +495,10 @@ struct wq3d_queue {
         for (int k = 0; k < K; ++k) {
             cudaEvent_t* ev = timing ? &events[7 * k] : nullptr;
             if (ev) cudaEventRecord(ev[0], stream);
+            if (h.adj) {
+                k_adj_checkpoint<<<grd, blk, 0, stream>>>(d, k);
+                launches += 1;
+            }
             if (volume_pass()) {
                 k_volume<<<grd, blk, 0, stream>>>(d, k);
                 launches += 1;
@@ -500,6 +529,11 @@ struct wq3d_queue {
                 if (ev) cudaEventRecord(ev[3], stream);
                 k_eigenray<<<eig_blocks, 128, 0, stream>>>(d, k);
                 launches += 2;
+                if (h.adj) {
+                    k_eigenray_jac<<<4 * 148, 64, 0, stream>>>(d, k);
+                    k_adj_mark<<<1, 1, 0, stream>>>(d);
+                    launches += 2;
+                }
             } else if (ev) {
                 cudaEventRecord(ev[3], stream);
             }
@@ -639,12 +673,14 @@ struct wq3d_queue {
         WQ_CK(cudaMemcpyAsync(d_times, ht, (K + 1) * sizeof(double), cudaMemcpyHostToDevice, stream));
         WQ_CK(cudaMemsetAsync(d_counts, 0, 3 * sizeof(uint32_t), stream));
         WQ_CK(cudaMemsetAsync(d_counts + 8, 0, sizeof(uint32_t), stream));
+        if (h.adj) WQ_CK(cudaMemsetAsync(d_counts + 11, 0, sizeof(uint32_t), stream));
         if (timing) tail = false;
         const int t = tail ? 1 : 0;
         if (!timing && K == chunk) build_graph(p, tail);
         if (!timing && K == chunk && graph[p][t]) {
             WQ_CK(cudaGraphLaunch(graph[p][t], stream));
-            launches += ((h.nt > 0 ? 4 : 2) + (volume_pass() ? 1 : 0)) * (int64_t)K + (tail ? 1 : 0);
+            launches += ((h.nt > 0 ? 4 : 2) + (volume_pass() ? 1 : 0) + (h.adj ? (h.nt > 0 ? 3 : 1) : 0)) *
+                            (int64_t)K + (tail ? 1 : 0);
         } else {
             launch_chunk(K, p, tail);
         }
@@ -722,6 +758,12 @@ struct wq3d_queue {
         if (err & (ERR_CAND_OVERFLOW | ERR_REC_OVERFLOW | ERR_REFL_OVERFLOW | ERR_VERB_OVERFLOW))
             return fail(WQ3D_ERR_OVERFLOW, "eigenray, reflection or eigenverb buffer overflow (error bits " +
                                                std::to_string(err) + "); recreate the queue with a larger eigenray_capacity");
+        if (err & ERR_ADJ_OVERFLOW)
+            return fail(WQ3D_ERR_OVERFLOW, "adjoint checkpoint or eigenray record buffer full (error bits " +
+                                               std::to_string(err) + "); enable the adjoint with larger limits");
+        if (err & ERR_NONFINITE)
+            return fail(WQ3D_ERR_NUMERIC, "a ray's position or direction became NaN or Inf (error bits " +
+                                              std::to_string(err) + "); check the ocean's profile and boundaries");
         if (err)
             return fail(WQ3D_ERR_NUMERIC, "kernel iteration bound reached (error bits " + std::to_string(err) + ")");
         return WQ3D_OK;
@@ -793,8 +835,26 @@ const char* wq3d_last_error_string(void) { return g_err.c_str(); }
 /* Internal hooks for the other source files of the library. */
 void wq3d_internal_set_error(const char* msg) { g_err = msg ? msg : ""; }
 
+/* An ocean's device arrays live on the device that was current when it
+ * was created; using them with another device current would hand kernels
+ * pointers into a different GPU's memory. */
+static int ocean_device_check(const wq3d_ocean* o, int device) {
+    if (device != o->device)
+        return fail(WQ3D_ERR_INVALID, "the ocean was created on device " + std::to_string(o->device) +
+                                          " and cannot be used on device " + std::to_string(device));
+    return WQ3D_OK;
+}
+
+static int ocean_on_current_device(const wq3d_ocean* o) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(WQ3D_ERR_CUDA, "cudaGetDevice failed");
+    return ocean_device_check(o, dev);
+}
+
 int wq3d_internal_ocean_model(const wq3d_ocean* ocean, OceanDev* out) {
-    if (!ocean || !out) return WQ3D_ERR_INVALID;
+    if (!ocean || !out) return fail(WQ3D_ERR_INVALID, "null argument");
+    const int rc = ocean_on_current_device(ocean);
+    if (rc) return rc;
     *out = ocean->dev;
     return WQ3D_OK;
 }
@@ -819,7 +879,10 @@ int wq3d_ocean_create(const wq3d_ocean_desc* d, wq3d_ocean** out) {
     for (const wq3d_boundary_desc* b : {&d->surface, &d->bottom})
         if (b->kind < WQ3D_BOUNDARY_FLAT || b->kind > WQ3D_BOUNDARY_GRID)
             return fail(WQ3D_ERR_UNSUPPORTED, "boundary kind not supported by this build");
+    int cur_dev = 0;
+    if (cudaGetDevice(&cur_dev) != cudaSuccess) return fail(WQ3D_ERR_CUDA, "no CUDA device is available");
     wq3d_ocean* o = new wq3d_ocean();
+    o->device = cur_dev;
     std::memset(&o->dev, 0, sizeof(o->dev));
     ProfileDev& p = o->dev.prof;
     p.kind = d->profile.kind;
@@ -867,7 +930,10 @@ static int eval_points(size_t n, std::vector<double*>& dev_in, const std::vector
         double* p = nullptr;
         WQ_CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(double)));
         dev_in.push_back(p);
-        if (host_in[k]) WQ_CK(cudaMemcpy(p, host_in[k], n * sizeof(double), cudaMemcpyHostToDevice));
+        if (host_in[k])
+            WQ_CK(cudaMemcpy(p, host_in[k], n * sizeof(double), cudaMemcpyHostToDevice));
+        else
+            WQ_CK(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(double)));
     }
     return WQ3D_OK;
 }
@@ -875,6 +941,7 @@ static int eval_points(size_t n, std::vector<double*>& dev_in, const std::vector
 int wq3d_ocean_sound_speed(const wq3d_ocean* o, double R, size_t n, const double* rho,
                            const double* theta, const double* phi, double* speed, double* grad) {
     if (!o || !rho || !speed) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (ocean_on_current_device(o)) return WQ3D_ERR_INVALID;
     std::vector<double*> d;
     int rc = eval_points(n, d, {rho, theta, phi});
     double *dc = nullptr, *dg = nullptr;
@@ -896,6 +963,7 @@ int wq3d_ocean_sound_speed(const wq3d_ocean* o, double R, size_t n, const double
 int wq3d_ocean_height(const wq3d_ocean* o, int which, size_t n, const double* rho,
                       const double* theta, const double* phi, double* height, double* normal) {
     if (!o || !theta || !phi || !height) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (ocean_on_current_device(o)) return WQ3D_ERR_INVALID;
     (void)rho;
     std::vector<double*> d;
     int rc = eval_points(n, d, {theta, phi});
@@ -919,6 +987,7 @@ int wq3d_ocean_height(const wq3d_ocean* o, int which, size_t n, const double* rh
 int wq3d_ocean_attenuation(const wq3d_ocean* o, double earth_radius, size_t n, const double* rho,
                            const double* distance, size_t nf, const double* freq, double* attenuation) {
     if (!o || !rho || !distance || !freq || !attenuation) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (ocean_on_current_device(o)) return WQ3D_ERR_INVALID;
     if (n == 0 || nf == 0) return WQ3D_OK;
     std::vector<double> alpha(nf);
     thorp_alpha(freq, nf, alpha.data());
@@ -950,6 +1019,7 @@ int wq3d_ocean_reflect_loss(const wq3d_ocean* o, int which, size_t n, const doub
                             const double* theta, const double* phi, const double* grazing,
                             size_t nf, const double* freq, double* amplitude, double* phase) {
     if (!o || !grazing || !freq || !amplitude) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (ocean_on_current_device(o)) return WQ3D_ERR_INVALID;
     (void)rho;
     (void)theta;
     (void)phi;
@@ -976,6 +1046,58 @@ int wq3d_ocean_reflect_loss(const wq3d_ocean* o, int which, size_t n, const doub
     return WQ3D_OK;
 }
 
+/* Destroyed queues kept for reuse.  A propagation loop that creates a
+ * queue, runs it and destroys it spends most of its host time allocating
+ * and freeing device buffers, instantiating CUDA graphs and freeing them
+ * again; wq3d_queue_destroy instead parks a queue whose buffers have their
+ * creation sizes, and wq3d_queue_create takes one of the same shape (device,
+ * fan, frequencies, targets, eigenray capacity), uploads the new inputs into
+ * its buffers and runs the start-up.  The chunk graphs are kept when the
+ * new queue's descriptor equals the old one.  A reused queue computes what
+ * a fresh one would, bit for bit. */
+namespace {
+std::mutex g_cache_mu;
+std::vector<wq3d_queue*>* g_cache = new std::vector<wq3d_queue*>();
+size_t g_cache_max = 2;
+
+bool cacheable(const wq3d_queue* q) {
+    const QueueDev& h = q->h;
+    return !h.sens && !h.adj && !h.verb && !q->set1.verb && h.cap_refl == 4096 && q->stream;
+}
+
+wq3d_queue* cache_take(int device, size_t nde, size_t naz, size_t nf, size_t nt1, size_t nt2, uint32_t cap_cand) {
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    for (size_t k = 0; k < g_cache->size(); ++k) {
+        wq3d_queue* q = (*g_cache)[k];
+        const QueueDev& h = q->h;
+        if (q->device == device && (size_t)h.nde == nde && (size_t)h.naz == naz && (size_t)h.nf == nf &&
+            (size_t)h.nt1 == (h.nt ? nt1 : 0) && (size_t)h.nt2 == (h.nt ? nt2 : 1) && h.cap_cand == cap_cand &&
+            ((h.nt == 0) == (nt1 * nt2 == 0))) {
+            g_cache->erase(g_cache->begin() + k);
+            return q;
+        }
+    }
+    return nullptr;
+}
+}  // namespace
+
+int wq3d_set_queue_cache(size_t max_queues) {
+    std::vector<wq3d_queue*> drop;
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        g_cache_max = max_queues;
+        while (g_cache->size() > g_cache_max) {
+            drop.push_back(g_cache->front());
+            g_cache->erase(g_cache->begin());
+        }
+    }
+    for (wq3d_queue* q : drop) {
+        DeviceGuard guard(q->device);
+        delete q;
+    }
+    return WQ3D_OK;
+}
+
 int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_queue** out) {
     if (!ocean || !d || !out) return fail(WQ3D_ERR_INVALID, "null argument");
     if (d->num_de < 1 || d->num_az < 1 || !d->de || !d->az || !d->de_inc || !d->az_inc)
@@ -994,13 +1116,39 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(WQ3D_ERR_CUDA, "no CUDA device is available");
     if (d->device < 0 || d->device >= ndev) return fail(WQ3D_ERR_INVALID, "device ordinal out of range");
+    if (ocean_device_check(ocean, d->device)) return WQ3D_ERR_INVALID;
     DeviceGuard guard(d->device);
 
-    wq3d_queue* q = new wq3d_queue();
+    const uint32_t cap_cand = (uint32_t)(d->eigenray_capacity ? d->eigenray_capacity
+                                                              : std::max<size_t>(4096, 32 * nt));
+    wq3d_queue* q = cache_take(d->device, d->num_de, d->num_az, d->num_freq, d->num_targets1, d->num_targets2,
+                               cap_cand);
+    const bool reuse = q != nullptr;
+    QueueDev old_h{};
+    if (reuse) {
+        /* the run state of a fresh queue; the device buffers stay */
+        old_h = q->h;
+        q->reuse = true;
+        q->time = q->ltime = 0.0;
+        q->steps = q->lsteps = 0;
+        q->carry_refl.clear();
+        q->carry_verb.clear();
+        q->carry_vpower.clear();
+        q->cb = wq3d_callbacks{};
+        q->cb_ctx = nullptr;
+        q->pending = PendingRays{};
+        q->abort_flag = false;
+        q->timing = false;
+        q->ms_step = q->ms_cpa = q->ms_eig = q->ms_total = q->ms_refl = 0.0;
+        q->launches = 0;
+        q->grow_verb = q->grow_refl = 0;
+    } else {
+        q = new wq3d_queue();
+    }
     q->device = d->device;
     q->run_id = d->run_id;
     QueueDev& h = q->h;
-    std::memset(&h, 0, sizeof(h));
+    if (!reuse) std::memset(&h, 0, sizeof(h));
     h.oc = ocean->dev;
     h.nde = (int)d->num_de;
     h.naz = (int)d->num_az;
@@ -1023,7 +1171,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         return rc;
     };
     int rc = 0;
-    if (cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (!reuse && cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
 
     /* host-side inputs */
@@ -1136,8 +1284,10 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         const size_t ibytes = al(n * sizeof(int32_t));
         const size_t bbytes = al(n);
         const size_t per_front = nd_arrays * dbytes + 5 * ibytes + bbytes;
-        char* base = nullptr;
-        if ((rc = q->alloc(&base, 4 * per_front + 2 * bbytes))) return cleanup(rc);
+        char* base = reuse ? q->ring : nullptr;
+        if (!reuse && (rc = q->alloc(&base, 4 * per_front + 2 * bbytes))) return cleanup(rc);
+        q->ring = base;
+        q->ring_bytes = 4 * per_front + 2 * bbytes;
         if (cudaMemset(base, 0, 4 * per_front + 2 * bbytes) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
         char* p = base;
@@ -1178,15 +1328,17 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
                                                  : std::max<size_t>(4096, 32 * nt));
     h.cap_rec = (uint32_t)std::min<size_t>((size_t)h.cap_cand * q->chunk, (size_t)1 << 21);
     h.cap_refl = 4096; /* grown when a reflection listener asks */
-    uint32_t* cand = nullptr;
-    if ((rc = q->alloc(&cand, 2 * (size_t)h.cap_cand))) return cleanup(rc);
-    h.cand = cand;
-    if ((rc = q->alloc(&h.rec, h.cap_rec)) || (rc = q->alloc(&h.rec_inten, (size_t)h.cap_rec * nf)) ||
-        (rc = q->alloc(&h.rec_phase, (size_t)h.cap_rec * nf)) || (rc = q->alloc(&h.refl, h.cap_refl)))
-        return cleanup(rc);
-    if ((rc = q->alloc(&q->d_counts, 16)) || (rc = q->alloc(&q->d_base, 1)) ||
-        (rc = q->alloc(&q->d_times, (size_t)q->chunk + 1)))
-        return cleanup(rc);
+    if (!reuse) {
+        uint32_t* cand = nullptr;
+        if ((rc = q->alloc(&cand, 2 * (size_t)h.cap_cand))) return cleanup(rc);
+        h.cand = cand;
+        if ((rc = q->alloc(&h.rec, h.cap_rec)) || (rc = q->alloc(&h.rec_inten, (size_t)h.cap_rec * nf)) ||
+            (rc = q->alloc(&h.rec_phase, (size_t)h.cap_rec * nf)) || (rc = q->alloc(&h.refl, h.cap_refl)))
+            return cleanup(rc);
+        if ((rc = q->alloc(&q->d_counts, 16)) || (rc = q->alloc(&q->d_base, 1)) ||
+            (rc = q->alloc(&q->d_times, (size_t)q->chunk + 1)))
+            return cleanup(rc);
+    }
     h.n_rec = q->d_counts + 0;
     h.n_refl = q->d_counts + 1;
     h.err = q->d_counts + 2;
@@ -1199,20 +1351,20 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.n_verb = q->d_counts + 8;
     h.want_verbs = 0;
     h.verb_threshold = 1e-30; /* wave_thresholds.h:40 */
-    {
+    if (!reuse) {
         const size_t stride = 51 + 2 * nf;
         if ((rc = q->alloc(&h.shadow, n * stride)) || (rc = q->alloc(&h.shadow_cnt, 3 * n)) ||
             (rc = q->alloc(&h.shadow_slot, n)))
             return cleanup(rc);
+        if ((rc = q->alloc(&h.work[0], n)) || (rc = q->alloc(&h.work[1], n))) return cleanup(rc);
     }
-    if ((rc = q->alloc(&h.work[0], n)) || (rc = q->alloc(&h.work[1], n))) return cleanup(rc);
     h.d_base = q->d_base;
     h.d_times = q->d_times;
     h.want_refl = 0;
     {
         /* per result set: base step, counters, chunk times */
         const size_t set_bytes = 128 + (((size_t)q->chunk + 1) * sizeof(double) + 63) / 64 * 64;
-        if (cudaMallocHost(&q->pinned, 2 * set_bytes) != cudaSuccess)
+        if (!reuse && cudaMallocHost(&q->pinned, 2 * set_bytes) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_NOMEM, "cudaMallocHost failed"));
         for (int s = 0; s < 2; ++s) {
             char* b = static_cast<char*>(q->pinned) + s * set_bytes;
@@ -1237,20 +1389,25 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     /* spreading_ray.cc:44: sound speed of ray (0,0) on the first front */
     if (cudaMemcpy(&h.init_sound_speed, h.F[2].c, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemcpy failed"));
-    if (cudaEventCreate(&q->ev_begin) != cudaSuccess || cudaEventCreate(&q->ev_end) != cudaSuccess)
-        return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-    if (cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess)
-        return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
-    for (auto& e : q->done_ev)
-        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+    if (!reuse) {
+        if (cudaEventCreate(&q->ev_begin) != cudaSuccess || cudaEventCreate(&q->ev_end) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-    q->fork_ev.resize(q->chunk);
-    q->join_ev.resize(q->chunk);
-    for (int k = 0; k < q->chunk; ++k)
-        if (cudaEventCreateWithFlags(&q->fork_ev[k], cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&q->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
-            return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+        if (cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess)
+            return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
+        for (auto& e : q->done_ev)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+                return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+        q->fork_ev.resize(q->chunk);
+        q->join_ev.resize(q->chunk);
+        for (int k = 0; k < q->chunk; ++k)
+            if (cudaEventCreateWithFlags(&q->fork_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&q->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
+                return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+    }
+    /* the chunk graphs hold the descriptor by value */
+    if (reuse && std::memcmp(&old_h, &h, sizeof(h)) != 0) q->drop_graph();
+    q->reuse = false;
     /* set-up a run would otherwise do on its first chunks: the second
      * result set and the graphs of the chunks that reflect the next
      * chunk's first step (rebuilt later only if callbacks, thresholds or
@@ -1265,6 +1422,29 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
 int wq3d_queue_destroy(wq3d_queue* q) {
     if (!q) return WQ3D_OK;
     DeviceGuard guard(q->device);
+    if (cacheable(q) && cudaStreamSynchronize(q->stream) == cudaSuccess &&
+        cudaStreamSynchronize(q->side) == cudaSuccess && cudaStreamSynchronize(q->copy) == cudaSuccess) {
+        wq3d_queue* drop = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(g_cache_mu);
+            if (g_cache_max > 0) {
+                q->pending = PendingRays{};
+                g_cache->push_back(q);
+                q = nullptr;
+                if (g_cache->size() > g_cache_max) {
+                    drop = g_cache->front();
+                    g_cache->erase(g_cache->begin());
+                }
+            }
+        }
+        if (!q) {
+            if (drop) {
+                DeviceGuard g2(drop->device);
+                delete drop;
+            }
+            return WQ3D_OK;
+        }
+    }
     delete q;
     return WQ3D_OK;
 }
@@ -1486,6 +1666,223 @@ int wq3d_queue_enable_sensitivity(wq3d_queue* q) {
     for (int f = 0; f < 4; ++f) q->h.F[f].dA = dA + (size_t)f * 3 * n;
     q->h.sens = 1;
     q->drop_graph();
+    return WQ3D_OK;
+}
+
+int wq3d_queue_enable_adjoint(wq3d_queue* q, int checkpoint_interval, size_t max_steps,
+                              size_t max_eigenrays) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    if (q->h.adj) return fail(WQ3D_ERR_INVALID, "adjoint recording is already on");
+    if (q->steps != 0 || q->lsteps != 0) return fail(WQ3D_ERR_INVALID, "enable the adjoint before the first step");
+    if (checkpoint_interval < 1 || max_steps < 1) return fail(WQ3D_ERR_INVALID, "checkpoint interval and steps must be positive");
+    const QueueDev& h = q->h;
+    const ProfileDev& pr = h.oc.prof;
+    if (pr.kind != WQ3D_PROFILE_GRID || pr.grid.ndim != 1 || pr.grid.interp[0] != WQ3D_INTERP_LINEAR)
+        return fail(WQ3D_ERR_UNSUPPORTED, "the adjoint needs a profile_grid<1> with linear interpolation");
+    if (pr.grid.ax[0].n < 2 || pr.grid.ax[0].n > ADJ_MAX_NODES)
+        return fail(WQ3D_ERR_UNSUPPORTED, "the adjoint's profile has 2 to " + std::to_string(ADJ_MAX_NODES) + " nodes");
+    for (const BoundaryDev* b : {&h.oc.surf, &h.oc.bot}) {
+        if (b->kind != WQ3D_BOUNDARY_FLAT && b->kind != WQ3D_BOUNDARY_SLOPE)
+            return fail(WQ3D_ERR_UNSUPPORTED, "the adjoint needs flat or sloped boundaries");
+        if (b->loss.kind == WQ3D_LOSS_RAYLEIGH && (b->loss.rl_shr != 0.0 || b->loss.rl_satt != 0.0))
+            return fail(WQ3D_ERR_UNSUPPORTED, "the adjoint's Rayleigh loss has no shear");
+    }
+    if (h.oc.nvol > 0) return fail(WQ3D_ERR_UNSUPPORTED, "the adjoint does not take volume layers");
+    if (h.spreading != WQ3D_HYBRID_GAUSSIAN) return fail(WQ3D_ERR_UNSUPPORTED, "the adjoint needs hybrid Gaussian spreading");
+    if (h.nt < 1) return fail(WQ3D_ERR_INVALID, "the adjoint needs targets");
+    DeviceGuard guard(q->device);
+    const size_t n = (size_t)h.n;
+    const int nckpt = (int)(max_steps / (size_t)checkpoint_interval + 1);
+    const size_t cap = max_eigenrays ? max_eigenrays : 65536;
+    if (cap > UINT32_MAX / 2) return fail(WQ3D_ERR_INVALID, "max_eigenrays too large");
+    double* ck = nullptr;
+    AdjRec* rec = nullptr;
+    int rc = q->alloc(&ck, (size_t)nckpt * ADJ_S * n);
+    if (!rc) rc = q->alloc(&rec, cap);
+    if (rc) return rc;
+    WQ_CK(cudaMemset(q->d_counts + 11, 0, 2 * sizeof(uint32_t)));
+    q->h.adj = 1;
+    q->h.adj_K = checkpoint_interval;
+    q->h.adj_nckpt = nckpt;
+    q->h.adj_ckpt = ck;
+    q->h.adj_rec = rec;
+    q->h.adj_cap = (uint32_t)cap;
+    q->h.adj_mark = q->d_counts + 11;
+    q->h.adj_n = q->d_counts + 12;
+    q->drop_graph();
+    return WQ3D_OK;
+}
+
+int wq3d_queue_adjoint(wq3d_queue* q, const wq3d_eigenray* rays, const double* w_tl, const double* w_time,
+                       size_t n_rays, double* grad, size_t num_nodes, double* ms) {
+    if (!q || !grad) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (n_rays && (!rays || !w_tl || !w_time)) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (!q->h.adj) return fail(WQ3D_ERR_INVALID, "adjoint recording is off (wq3d_queue_enable_adjoint)");
+    const QueueDev& h = q->h;
+    const int nodes = h.oc.prof.grid.ax[0].n;
+    if (num_nodes != (size_t)nodes)
+        return fail(WQ3D_ERR_INVALID, "the profile has " + std::to_string(nodes) + " nodes");
+    for (int j = 0; j < nodes; ++j) grad[j] = 0.0;
+    if (ms) *ms = 0.0;
+    const int64_t m_end = q->steps;
+    if (m_end < 1 || n_rays == 0) return WQ3D_OK;
+    DeviceGuard guard(q->device);
+    WQ_CK(cudaStreamSynchronize(q->stream));
+    const size_t n = (size_t)h.n;
+    const int K = h.adj_K;
+    /* the records' keys, flags and spread partials, strided out of AdjRec */
+    uint32_t nrec = 0;
+    WQ_CK(cudaMemcpy(&nrec, h.adj_n, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    nrec = std::min(nrec, h.adj_cap);
+    std::vector<int64_t> kstep(nrec);
+    std::vector<int32_t> kti(2 * (size_t)nrec), kflags(nrec);
+    std::vector<double> kds2(nrec);
+    if (nrec > 0) {
+        const size_t pitch = sizeof(AdjRec);
+        WQ_CK(cudaMemcpy2D(kstep.data(), sizeof(int64_t), (const char*)h.adj_rec + offsetof(AdjRec, step), pitch,
+                           sizeof(int64_t), nrec, cudaMemcpyDeviceToHost));
+        WQ_CK(cudaMemcpy2D(kti.data(), 2 * sizeof(int32_t), (const char*)h.adj_rec + offsetof(AdjRec, t), pitch,
+                           2 * sizeof(int32_t), nrec, cudaMemcpyDeviceToHost));
+        WQ_CK(cudaMemcpy2D(kflags.data(), sizeof(int32_t), (const char*)h.adj_rec + offsetof(AdjRec, flags), pitch,
+                           sizeof(int32_t), nrec, cudaMemcpyDeviceToHost));
+        WQ_CK(cudaMemcpy2D(kds2.data(), sizeof(double), (const char*)h.adj_rec + offsetof(AdjRec, dTL_ds2), pitch,
+                           sizeof(double), nrec, cudaMemcpyDeviceToHost));
+    }
+    /* weights per record, matched on (step, target, ray) */
+    std::vector<size_t> order(nrec);
+    for (size_t r = 0; r < nrec; ++r) order[r] = r;
+    auto key = [&](size_t r) { return std::make_tuple(kstep[r], kti[2 * r], kti[2 * r + 1]); };
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return key(a) < key(b); });
+    std::vector<double> w(2 * (size_t)nrec, 0.0);
+    std::vector<double> gs2((size_t)h.nt, 0.0);
+    for (size_t k = 0; k < n_rays; ++k) {
+        const wq3d_eigenray& e = rays[k];
+        const auto want = std::make_tuple((int64_t)e.step, (int32_t)(e.t1 * h.nt2 + e.t2), (int32_t)(e.de * h.naz + e.az));
+        auto it = std::lower_bound(order.begin(), order.end(), want,
+                                   [&](size_t r, const std::tuple<int64_t, int32_t, int32_t>& v) { return key(r) < v; });
+        if (it == order.end() || key(*it) != want)
+            return fail(WQ3D_ERR_INVALID, "eigenray " + std::to_string(k) + " was not recorded by this queue's adjoint");
+        const size_t r = *it;
+        if ((w_tl[k] != 0.0 || w_time[k] != 0.0) && !(kflags[r] & ADJ_VALID))
+            return fail(WQ3D_ERR_NUMERIC, "eigenray " + std::to_string(k) + ": its beam walk outran the " +
+                                              std::to_string(ADJ_MAX_CELLS) + " recorded cells");
+        w[r] += w_tl[k];
+        w[nrec + r] += w_time[k];
+        gs2[kti[2 * r]] += w_tl[k] * kds2[r];
+    }
+    /* workspace */
+    auto& W = q->adjw;
+    int rc = WQ3D_OK;
+    if (!W.seg) {
+        if ((rc = q->alloc(&W.seg, (size_t)(K + 1) * ADJ_S * n)) || (rc = q->alloc(&W.chain, (size_t)(K + 1) * n)) ||
+            (rc = q->alloc(&W.seed, (size_t)(K + 1) * ADJ_L * n)) || (rc = q->alloc(&W.lam, (size_t)ADJ_L * n)) ||
+            (rc = q->alloc(&W.last, n)) || (rc = q->alloc(&W.grad, ADJ_MAX_NODES)) || (rc = q->alloc(&W.err, 1)))
+            return rc;
+    }
+    if (W.w_cap < 2 * (size_t)nrec) {
+        q->release(W.w);
+        W.w = nullptr;
+        if ((rc = q->alloc(&W.w, std::max<size_t>(2 * (size_t)nrec, 2)))) return rc;
+        W.w_cap = std::max<size_t>(2 * (size_t)nrec, 2);
+    }
+    cudaStream_t st = q->stream;
+    cudaEvent_t e0 = q->ev_begin, e1 = q->ev_end;
+    if (!e0) WQ_CK(cudaEventCreate(&q->ev_begin));
+    if (!e1) WQ_CK(cudaEventCreate(&q->ev_end));
+    e0 = q->ev_begin;
+    e1 = q->ev_end;
+    double alpha0 = 0.0;
+    WQ_CK(cudaMemcpy(&alpha0, h.alpha, sizeof(double), cudaMemcpyDeviceToHost));
+    WQ_CK(cudaEventRecord(e0, st));
+    if (nrec > 0) WQ_CK(cudaMemcpyAsync(W.w, w.data(), 2 * (size_t)nrec * sizeof(double), cudaMemcpyHostToDevice, st));
+    WQ_CK(cudaMemsetAsync(W.last, 0, n * sizeof(int64_t), st));
+    WQ_CK(cudaMemsetAsync(W.lam, 0, (size_t)ADJ_L * n * sizeof(double), st));
+    WQ_CK(cudaMemsetAsync(W.grad, 0, ADJ_MAX_NODES * sizeof(double), st));
+    WQ_CK(cudaMemsetAsync(W.err, 0, sizeof(uint32_t), st));
+    AdjSweep a{};
+    a.m_end = m_end;
+    a.nrec = (int)nrec;
+    a.w_tl = W.w;
+    a.w_t = W.w + nrec;
+    a.seg = W.seg;
+    a.chain = W.chain;
+    a.seed = W.seed;
+    a.lam = W.lam;
+    a.last = W.last;
+    a.grad = W.grad;
+    a.nodes = nodes;
+    a.alpha0 = alpha0;
+    a.err = W.err;
+    /* the recompute retraces the forward without notices or sensitivities */
+    QueueDev qa = q->dev(0);
+    qa.want_refl = 0;
+    qa.want_verbs = 0;
+    qa.sens = 0;
+    const unsigned rb = (unsigned)((nrec + 127) / 128);
+    const unsigned gb = (unsigned)((n + 127) / 128);
+    if (nrec > 0) k_adj_touch<<<rb, 128, 0, st>>>(a, qa);
+    /* checkpoints exist for the states the forward advanced from */
+    const int64_t c_last = std::min<int64_t>((m_end - 1) / K, (int64_t)h.adj_nckpt - 1);
+    for (int64_t c = c_last; c >= 0; --c) {
+        a.m0 = c * K;
+        a.m1 = (c == c_last) ? m_end + 1 : (c + 1) * K;
+        if (a.m1 - a.m0 > K + 1) return fail(WQ3D_ERR_OVERFLOW, "the run went past the adjoint's max_steps");
+        a.ckpt = (int)c;
+        WQ_CK(cudaMemsetAsync(W.seed, 0, (size_t)(a.m1 - a.m0) * ADJ_L * n * sizeof(double), st));
+        k_adj_recompute<<<gb, 128, 0, st>>>(a, qa);
+        if (nrec > 0) k_adj_expand<<<rb, 128, 0, st>>>(a, qa);
+        k_adj_reverse<<<gb, 128, 0, st>>>(a, qa);
+    }
+    k_adj_startup<<<gb, 128, 0, st>>>(a, qa);
+    WQ_CK(cudaGetLastError());
+    WQ_CK(cudaEventRecord(e1, st));
+    std::vector<double> g(nodes);
+    uint32_t err = 0;
+    WQ_CK(cudaMemcpyAsync(g.data(), W.grad, nodes * sizeof(double), cudaMemcpyDeviceToHost, st));
+    WQ_CK(cudaMemcpyAsync(&err, W.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    WQ_CK(cudaStreamSynchronize(st));
+    if (ms) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        *ms = t;
+    }
+    if (err & ADJ_ERR_WINDOW)
+        return fail(WQ3D_ERR_NUMERIC, "adjoint: a step reached profile nodes beyond its window (nodes closer "
+                                      "than a step's reach)");
+    if (err & ADJ_ERR_CHAIN) return fail(WQ3D_ERR_NUMERIC, "adjoint: more than 8 reflections in one step");
+    if (err & ADJ_ERR_TOPOLOGY)
+        return fail(WQ3D_ERR_NUMERIC, "adjoint: a reflection chain's re-evaluation took another branch");
+    /* the beam spread s2 = (2 pi c_target / f)^2 of the first frequency
+     * through the target's sound speed (d s2 / d c = 2 s2 / c), which is
+     * linear in the two nodes around the target's depth */
+    std::vector<double> ax((size_t)nodes), trho((size_t)h.nt), tc((size_t)h.nt), ts2((size_t)h.nt);
+    WQ_CK(cudaMemcpy(ax.data(), h.oc.prof.grid.ax[0].x, nodes * sizeof(double), cudaMemcpyDeviceToHost));
+    WQ_CK(cudaMemcpy(trho.data(), h.tgt[0], h.nt * sizeof(double), cudaMemcpyDeviceToHost));
+    WQ_CK(cudaMemcpy(tc.data(), h.tgt_c, h.nt * sizeof(double), cudaMemcpyDeviceToHost));
+    WQ_CK(cudaMemcpy2D(ts2.data(), sizeof(double), h.tgt_spread2, (size_t)h.nf * sizeof(double), sizeof(double),
+                       (size_t)h.nt, cudaMemcpyDeviceToHost));
+    const double sign = (ax[1] < ax[0]) ? -1.0 : 1.0;
+    for (int t = 0; t < h.nt; ++t) {
+        if (gs2[t] == 0.0 || tc[t] == 0.0) continue;
+        const double gc = gs2[t] * 2.0 * ts2[t] / tc[t];
+        const double r = trho[t];
+        int k = 0;
+        double u = 0.0;
+        if (r * sign <= ax[0] * sign) {
+            k = 0;
+            u = 0.0;
+        } else if (r * sign >= ax[nodes - 1] * sign) {
+            k = nodes - 2;
+            u = 1.0;
+        } else {
+            while (k < nodes - 2 && r * sign >= ax[k + 1] * sign) ++k;
+            u = (r - ax[k]) / (ax[k + 1] - ax[k]);
+        }
+        const double fe = h.oc.prof.flat_earth ? r / h.R : 1.0;
+        g[k] += gc * (1.0 - u) * fe;
+        g[k + 1] += gc * u * fe;
+    }
+    for (int j = 0; j < nodes; ++j) grad[j] = g[j];
     return WQ3D_OK;
 }
 

@@ -38,8 +38,39 @@ enum : uint32_t {
     ERR_REC_OVERFLOW = 4u,       /* eigenray record buffer full                */
     ERR_REFL_OVERFLOW = 8u,      /* reflection record buffer full              */
     ERR_WALK_LIMIT = 16u,        /* a Gaussian-beam walk exceeded its bound    */
-    ERR_VERB_OVERFLOW = 32u      /* eigenverb record buffer full               */
+    ERR_VERB_OVERFLOW = 32u,     /* eigenverb record buffer full               */
+    ERR_NONFINITE = 64u,         /* a ray's new position or direction is NaN/Inf */
+    ERR_ADJ_OVERFLOW = 128u      /* adjoint checkpoint or record buffer full    */
 };
+
+/* Per-eigenray partial derivatives recorded for the adjoint (one per
+ * eigenray record while adjoint recording is on).  TL is the first
+ * frequency's.  The cube values are the 27 target distance2 values that
+ * build_eigenray reads on the prev / curr / next fronts; cells are the
+ * beam-walk cells whose widths the hybrid Gaussian sum used. */
+constexpr int ADJ_MAX_CELLS = 256;
+struct AdjRec {
+    int64_t step;          /* eigenray step (its fronts are that step's)  */
+    int32_t t;             /* target index                                 */
+    int32_t i;             /* ray index de * num_az + az                   */
+    int32_t ncell;
+    int32_t flags;         /* ADJ_VALID, ADJ_CELL_OVERFLOW                 */
+    int32_t a_de;          /* AZ column of the D/E walk                    */
+    int32_t d_az;          /* D/E row of the AZ walk                       */
+    int32_t role_a0;       /* fronts (0 prev, 1 curr, 2 next) holding the  */
+    int32_t role_a1;       /* two attenuations interpolated in time        */
+    double no_de[3];       /* offsets the D/E walk's widths use            */
+    double no_az[3];       /* offsets the AZ walk's widths use             */
+    double dT[27];         /* d travel time / d cube value                 */
+    double dTL[27];        /* d TL / d cube value                          */
+    double dTL_da0, dTL_da1;
+    double dTL_ds2;        /* d TL / d (2 pi c_target / f)^2               */
+    int16_t cell_d[ADJ_MAX_CELLS];
+    int16_t cell_a[ADJ_MAX_CELLS];
+    uint8_t cell_kind[ADJ_MAX_CELLS]; /* 0 width_de, 1 width_az */
+    double cell_g[ADJ_MAX_CELLS];     /* d TL / d cell width   */
+};
+enum : int32_t { ADJ_VALID = 1, ADJ_CELL_OVERFLOW = 2 };
 
 struct FrontPtrs {
     double* pos[3];
@@ -138,6 +169,15 @@ struct QueueDev {
     int want_verbs;
     double verb_threshold;   /* linear power (wave_thresholds.h:87-89)     */
     uint32_t* err;
+    /* adjoint recording (wq3d_queue_enable_adjoint) */
+    int adj;                 /* record checkpoints and eigenray partials   */
+    int adj_K;               /* checkpoint interval (steps)                 */
+    int adj_nckpt;           /* checkpoint slots                            */
+    double* adj_ckpt;        /* [slot][18][n]: pos, ndir of prev/curr/next  */
+    AdjRec* adj_rec;
+    uint32_t* adj_n;         /* AdjRec entries written                      */
+    uint32_t adj_cap;
+    uint32_t* adj_mark;      /* eigenray records of the chunk processed     */
 };
 
 /* kernels (wq3d_kernels.cu).  Every kernel takes the queue descriptor by
@@ -174,6 +214,49 @@ __global__ void k_attenuation(ProfileDev pr, double R, int n, const double* rho,
 __global__ void k_reflect_loss(BoundaryDev b, int n, const double* grazing,
                                int nf, const double* freq, double* amp,
                                double* ph);
+/* adjoint recording (wq3d_adjoint.cuh) */
+__global__ void k_adj_checkpoint(__grid_constant__ const QueueDev q, int k);
+__global__ void k_eigenray_jac(__grid_constant__ const QueueDev q, int k);
+__global__ void k_adj_mark(__grid_constant__ const QueueDev q);
+
+/* adjoint sweep (wq3d_adjoint.cuh) */
+constexpr int ADJ_S = 18;         /* state doubles per ray                   */
+constexpr int ADJ_L = 21;         /* adjoint doubles: state + 3 attenuations */
+constexpr int ADJ_W = 6;          /* profile nodes one step's Jacobian covers */
+constexpr int ADJ_NB = 8;         /* dual directions per pass                */
+constexpr int ADJ_MAX_NODES = 64; /* profile nodes the gradient can have     */
+
+/* adjoint error bits (AdjSweep::err) */
+enum : uint32_t {
+    ADJ_ERR_WINDOW = 1u,   /* a step reached profile nodes beyond its window */
+    ADJ_ERR_CHAIN = 2u,    /* more than 8 reflections in one step            */
+    ADJ_ERR_TOPOLOGY = 4u  /* the dual re-evaluation took another branch     */
+};
+
+struct AdjSweep {
+    int64_t m0, m1;        /* segment of states [m0, m1)                 */
+    int64_t m_end;         /* the last state of the run                  */
+    int ckpt;              /* checkpoint slot of m0                      */
+    int nrec;              /* AdjRec entries                              */
+    const double* w_tl;    /* per AdjRec: weight of TL                    */
+    const double* w_t;     /* per AdjRec: weight of travel time           */
+    double* seg;           /* [K+1][18][n] states of the segment          */
+    uint32_t* chain;       /* [K+1][n] reflection chain of each step       */
+    double* seed;          /* [K+1][21][n]                                */
+    double* lam;           /* [21][n] lambda at the segment's end          */
+    int64_t* last;         /* [n] last seeded state, -1 for none            */
+    double* grad;          /* [nodes] d L / d node                         */
+    int nodes;
+    double alpha0;         /* absorption per metre factor, frequency 0     */
+    uint32_t* err;
+};
+
+__global__ void k_adj_touch(AdjSweep a, __grid_constant__ const QueueDev q);
+__global__ void k_adj_recompute(AdjSweep a, __grid_constant__ const QueueDev q);
+__global__ void k_adj_expand(AdjSweep a, __grid_constant__ const QueueDev q);
+__global__ void k_adj_reverse(AdjSweep a, __grid_constant__ const QueueDev q);
+__global__ void k_adj_startup(AdjSweep a, __grid_constant__ const QueueDev q);
+
 
 constexpr int CPA_THREADS = 128;     /* rays per CPA block            */
 constexpr int CPA_TARGETS = 64;      /* targets per FP64 CPA block    */

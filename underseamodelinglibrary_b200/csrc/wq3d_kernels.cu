@@ -989,6 +989,9 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     double st;
     ray_derivs(y3.c, y3.sg[0], y3.sg[1], y3.sg[2], y3.pos, y3.nd, y3.pg, y3.ng, &st);
     const uint8_t f_next = reflect_decision(q, y3.pos, y2.nd);
+    /* the per-step finiteness check: a NaN or Inf in the environment (a
+     * bad profile node, a zero sound speed) reaches the new front here */
+    if (!isfinite(y3.pos[0] + y3.pos[1] + y3.pos[2] + y3.nd[0] + y3.nd[1] + y3.nd[2])) set_err(q, ERR_NONFINITE);
     /* stores */
     if (fold_hit) R.X->caustic[i] = cs;
     if (vtx_up) R.X->upper[i] = up;
@@ -2320,3 +2323,9 @@ __global__ void k_reflect_loss(BoundaryDev b, int n, const double* grazing, int 
 #endif  // !WQ3D_STEP_KERNELS_ONLY
 
 }  // namespace wq3d
+
+#if WQ3D_WITH_GRID && !WQ3D_STEP_KERNELS_ONLY
+/* the adjoint's kernels reuse the step functions above */
+#define WQ3D_ADJOINT_IMPL 1
+#include "wq3d_adjoint.cuh"
+#endif

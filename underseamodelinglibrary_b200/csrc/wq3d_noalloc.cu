@@ -106,7 +106,8 @@ extern "C" int wq3d_ocean_sound_speed_noalloc(const wq3d_ocean* ocean, double ea
                                                   std::to_string(WQ3D_NOALLOC_MAX_POINTS));
     if (n == 0) return WQ3D_OK;
     OceanDev oc;
-    if (wq3d_internal_ocean_model(ocean, &oc) != WQ3D_OK) return noalloc_fail(WQ3D_ERR_INVALID, "bad ocean");
+    const int orc = wq3d_internal_ocean_model(ocean, &oc); /* also checks the ocean's device */
+    if (orc != WQ3D_OK) return orc;
     double* pts = nullptr;
     int rc = staging_address(&pts);
     if (rc) return rc;

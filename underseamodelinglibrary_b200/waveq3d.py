@@ -94,6 +94,11 @@ class eigenray_list(Sequence):
         for i in range(len(self._rec)):
             yield self[i]
 
+    @property
+    def records(self):
+        """the engine's wq3d_eigenray records (numpy structured array)"""
+        return self._rec
+
     def arrays(self):
         """All eigenrays as columns: the record fields (travel time as
         "time", CPA bracket as "step", "de", "az"), intensity and phase
@@ -446,6 +451,31 @@ class wave_queue:
         call before the first step"""
         _abi.check(self._lib, self._lib.wq3d_queue_enable_sensitivity(self._q))
         self._sens = True
+
+    def enable_adjoint(self, checkpoint_interval=50, max_steps=100000, max_eigenrays=0):
+        """Records what the reverse sweep needs (wq3d_queue_enable_adjoint):
+        ray states every ``checkpoint_interval`` steps and each eigenray's
+        partial derivatives; call before the first step."""
+        _abi.check(self._lib, self._lib.wq3d_queue_enable_adjoint(self._q, int(checkpoint_interval),
+                                                                  int(max_steps), int(max_eigenrays)))
+
+    def adjoint(self, rays, w_tl, w_time, num_nodes):
+        """The reverse sweep (wq3d_queue_adjoint): sum_k w_tl[k] dTL_k/dc +
+        w_time[k] dT_k/dc over the profile grid's nodes c, for the
+        eigenrays ``rays`` (an eigenray_list this queue returned).  Returns
+        (gradient, device milliseconds)."""
+        rec = np.ascontiguousarray(rays.records if hasattr(rays, "records") else rays)
+        n = rec.shape[0]
+        wt = np.ascontiguousarray(w_tl, dtype=np.float64).reshape(-1)
+        wtt = np.ascontiguousarray(w_time, dtype=np.float64).reshape(-1)
+        if wt.size != n or wtt.size != n:
+            raise ValueError("one TL weight and one travel-time weight per eigenray")
+        grad = np.zeros(int(num_nodes))
+        ms = C.c_double()
+        _abi.check(self._lib, self._lib.wq3d_queue_adjoint(
+            self._q, rec.ctypes.data_as(C.c_void_p), _abi.as_dp(wt), _abi.as_dp(wtt), n,
+            _abi.as_dp(grad), grad.size, C.byref(ms)))
+        return grad, ms.value
 
     def set_timing(self, on):
         _abi.check(self._lib, self._lib.wq3d_queue_set_timing(self._q, 1 if on else 0))
