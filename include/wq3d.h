@@ -447,6 +447,43 @@ int wq3d_queue_enable_adjoint(wq3d_queue* q, int checkpoint_interval, size_t max
 int wq3d_queue_adjoint(wq3d_queue* q, const wq3d_eigenray* rays, const double* w_tl,
                        const double* w_time, size_t n, double* grad, size_t num_nodes, double* ms);
 
+/* The reverse sweep for one ray's state instead of eigenrays: grad[j]
+ * receives d x / d c_j for component `component` of ray `ray`'s state
+ * after step `step` (0-17: position rho, theta, phi then normalised
+ * direction of the prev, curr and next fronts as that step's eigenray
+ * search reads them; 18-20: their first-frequency attenuation).  Checks
+ * the sweep's propagation part against differences of the fronts
+ * (wq3d_queue_get_front).  No reference counterpart. */
+int wq3d_queue_adjoint_state(wq3d_queue* q, int ray, int64_t step, int component, double* grad,
+                             size_t num_nodes);
+
+/* Eigenverb counting sink: with on != 0 the queue builds eigenverbs as
+ * for an eigenverb listener (wave_queue.cc:1063-1164), reads them back per
+ * chunk and counts them per interface instead of calling add_eigenverb;
+ * counts (2 + 2 * WQ3D_MAX_VOLUME entries, indexed by interface number)
+ * accumulate until the queue is destroyed.  For callers that measure or
+ * subsample the eigenverb stream without a callback per eigenverb.  No
+ * reference counterpart (the reference always calls its listeners). */
+int wq3d_queue_count_eigenverbs(wq3d_queue* q, int on);
+int wq3d_queue_eigenverb_counts(const wq3d_queue* q, uint64_t* counts);
+
+/* eigenray_collection::sum_eigenrays (eigenrays/eigenray_collection.cc:
+ * 105-191) on the GPU: for every target of a num_targets1 x num_targets2
+ * grid, the coherent (or, with coherent = 0, incoherent) phasor sum of its
+ * eigenrays per frequency, and their power-weighted travel time, D/E
+ * angles and AZ angles; the counts are the strongest path's.  rays[k]
+ * (intensity and phase: n x nf, frequency fastest) names its target in
+ * t1, t2; a target's eigenrays are summed in the order they appear, as the
+ * reference's per-target lists hold them.  total (num_targets1 x
+ * num_targets2 records, de, az and step set to -1), total_intensity and
+ * total_phase (targets x nf) receive the sums; a target without eigenrays
+ * gets 300 dB, NaN time and angles, and counts of -1, as in the
+ * reference. */
+int wq3d_sum_eigenrays(const wq3d_eigenray* rays, const double* intensity, const double* phase,
+                       size_t n, const double* freq, size_t nf, size_t num_targets1,
+                       size_t num_targets2, int coherent, wq3d_eigenray* total,
+                       double* total_intensity, double* total_phase);
+
 /* The three derivatives of each eigenray that wq3d_queue_take_eigenrays
  * would return next, in the same order (3 values per eigenray; NaN when
  * sensitivity mode is off).  Does not consume the eigenrays. */

@@ -1,15 +1,19 @@
-"""eigenray_collection.sum_eigenrays (numpy, sequential sums) against a
-scalar restatement of eigenray_collection.cc:105-191, on random eigenray
-sets: equal within 1e-12 relative (the two use different sin / cos / pow
-implementations, which may differ in the last place)."""
+"""eigenray_collection.sum_eigenrays (the GPU's wq3d_sum_eigenrays,
+sequential sums per target) against a scalar restatement of
+eigenray_collection.cc:105-191, on random eigenray sets: equal within
+1e-11 relative (CUDA's and the host's pow / sin / cos / log10 / atan2 may
+differ in the last place)."""
 import cmath
 import math
 
 import numpy as np
+import pytest
 
 from underseamodelinglibrary_b200 import types as T
 from underseamodelinglibrary_b200.eigenrays import eigenray_collection
 from underseamodelinglibrary_b200.waveq3d import eigenray_model
+
+pytestmark = pytest.mark.gpu
 
 
 def scalar_sum(rays, freq, coherent=True):
@@ -60,7 +64,7 @@ def _ray(rng, nf):
     return r
 
 
-def test_vectorised_sum_matches_scalar_restatement():
+def test_gpu_sum_matches_scalar_restatement(engine):
     T.compute_earth_radius(45.0)
     freq = T.seq_log(100.0, 2.0, 5)
     fv = [freq[f] for f in range(freq.size())]
@@ -75,14 +79,14 @@ def test_vectorised_sum_matches_scalar_restatement():
         coll.sum_eigenrays()
         for k, rays in enumerate(sets):
             got, ref = coll.total(0, k), scalar_sum(rays, fv, coherent)
-            assert np.allclose(got.intensity, ref["intensity"], rtol=1e-12, atol=0)
+            assert np.allclose(got.intensity, ref["intensity"], rtol=1e-11, atol=0)
             assert np.allclose(got.phase, ref["phase"], rtol=1e-9, atol=1e-12)
             for f in ("travel_time", "source_de", "source_az", "target_de", "target_az"):
-                assert math.isclose(getattr(got, f), ref[f], rel_tol=1e-12, abs_tol=1e-12), f
+                assert math.isclose(getattr(got, f), ref[f], rel_tol=1e-11, abs_tol=1e-11), f
             assert (got.surface, got.bottom, got.caustic, got.upper, got.lower) == ref["counts"]
 
 
-def test_empty_target_total():
+def test_empty_target_total(engine):
     T.compute_earth_radius(45.0)
     freq = T.seq_log(100.0, 2.0, 2)
     coll = eigenray_collection(freq, T.wposition1(45.0, -45.0, -50.0), T.wposition(1, 1, 45.0, -45.0, -10.0))

@@ -173,6 +173,11 @@ SIGNATURES = {
     "wq3d_queue_sensitivities": (C.c_int, [C.c_void_p, dp, C.c_size_t, C.POINTER(C.c_size_t)]),
     "wq3d_queue_enable_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_size_t]),
     "wq3d_set_queue_cache": (C.c_int, [C.c_size_t]),
+    "wq3d_queue_adjoint_state": (C.c_int, [C.c_void_p, C.c_int, C.c_int64, C.c_int, dp, C.c_size_t]),
+    "wq3d_queue_count_eigenverbs": (C.c_int, [C.c_void_p, C.c_int]),
+    "wq3d_queue_eigenverb_counts": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "wq3d_sum_eigenrays": (C.c_int, [C.c_void_p, dp, dp, C.c_size_t, dp, C.c_size_t, C.c_size_t, C.c_size_t,
+                                     C.c_int, C.c_void_p, dp, dp]),
     "wq3d_queue_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, dp, dp, C.c_size_t, dp, C.c_size_t, dp]),
     "wq3d_batch_run": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t, dp, C.POINTER(C.c_size_t), dp]),
     "wq3d_ocean_attenuation": (C.c_int, [C.c_void_p, C.c_double, C.c_size_t, dp, dp, C.c_size_t, dp, dp]),

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwq3d.so")
-SOURCES = ["wq3d_api.cu", "wq3d_kernels.cu", "wq3d_noalloc.cu", "wq3d_biverbs.cu"]
+SOURCES = ["wq3d_api.cu", "wq3d_kernels.cu", "wq3d_noalloc.cu", "wq3d_biverbs.cu", "wq3d_sum.cu"]
 # (object name, source, extra flags): wq3d_kernels.cu is compiled a second
 # time for the ray-stepping kernels of oceans without gridded models
 OBJECTS = [(f, f, []) for f in SOURCES] + [

@@ -599,42 +599,49 @@ class eigenray_collection : public eigenray_listener {
     }
     const std::vector<eigenray_model::csptr>& eigenrays(size_t t1, size_t t2) const { return _rays[t1 * _n2 + t2]; }
     const eigenray_model& total(size_t t1, size_t t2) const { return _total[t1 * _n2 + t2]; }
+    /** eigenray_collection::sum_eigenrays (eigenray_collection.cc:105-191)
+     * on the GPU (wq3d_sum_eigenrays) */
     void sum_eigenrays() {
-        const double TWO_PI = 2.0 * M_PI;
-        for (size_t t = 0; t < _rays.size(); ++t) {
-            eigenray_model& tot = _total[t];
-            const size_t nf = _freq->size();
-            tot.intensity.assign(nf, 0.0);
-            tot.phase.assign(nf, 0.0);
-            double time = 0, wgt = 0, sde = 0, tde = 0, max_a = 0;
-            for (size_t f = 0; f < nf; ++f) {
-                std::complex<double> ph(0.0, 0.0);
-                for (const auto& r : _rays[t]) {
-                    double a = std::pow(10.0, r->intensity[f] / -20.0);
-                    if (_coherent) {
-                        double p = std::fmod(TWO_PI * (*_freq)(f) * r->travel_time + r->phase[f], TWO_PI);
-                        ph += std::complex<double>(a * std::cos(p), a * std::sin(p));
-                    } else {
-                        ph += a;
-                    }
-                    a *= a;
-                    wgt += a;
-                    time += a * r->travel_time;
-                    sde += a * r->source_de;
-                    tde += a * r->target_de;
-                    if (a > max_a) {
-                        max_a = a;
-                        tot.surface = r->surface;
-                        tot.bottom = r->bottom;
-                        tot.caustic = r->caustic;
-                    }
-                }
-                tot.intensity[f] = -20.0 * std::log10(std::max(1e-15, std::abs(ph)));
-                tot.phase[f] = std::arg(ph);
+        const size_t nf = _freq->size();
+        std::vector<wq3d_eigenray> rec;
+        std::vector<double> inten, phase;
+        for (size_t t = 0; t < _rays.size(); ++t)
+            for (const auto& r : _rays[t]) {
+                wq3d_eigenray e{};
+                e.time = r->travel_time;
+                e.source_de = r->source_de;
+                e.source_az = r->source_az;
+                e.target_de = r->target_de;
+                e.target_az = r->target_az;
+                e.surface = r->surface;
+                e.bottom = r->bottom;
+                e.caustic = r->caustic;
+                e.upper = r->upper;
+                e.lower = r->lower;
+                e.t1 = (int32_t)(t / _n2);
+                e.t2 = (int32_t)(t % _n2);
+                rec.push_back(e);
+                inten.insert(inten.end(), r->intensity.begin(), r->intensity.end());
+                phase.insert(phase.end(), r->phase.begin(), r->phase.end());
             }
-            tot.travel_time = time / wgt;
-            tot.source_de = sde / wgt;
-            tot.target_de = tde / wgt;
+        std::vector<wq3d_eigenray> tot(_rays.size());
+        std::vector<double> ti(_rays.size() * nf), tp(_rays.size() * nf);
+        check(wq3d_sum_eigenrays(rec.data(), inten.data(), phase.data(), rec.size(), _freq->data().data(), nf,
+                                 _n1, _n2, _coherent ? 1 : 0, tot.data(), ti.data(), tp.data()));
+        for (size_t t = 0; t < _rays.size(); ++t) {
+            eigenray_model& o = _total[t];
+            o.travel_time = tot[t].time;
+            o.source_de = tot[t].source_de;
+            o.source_az = tot[t].source_az;
+            o.target_de = tot[t].target_de;
+            o.target_az = tot[t].target_az;
+            o.surface = tot[t].surface;
+            o.bottom = tot[t].bottom;
+            o.caustic = tot[t].caustic;
+            o.upper = tot[t].upper;
+            o.lower = tot[t].lower;
+            o.intensity.assign(ti.begin() + t * nf, ti.begin() + (t + 1) * nf);
+            o.phase.assign(tp.begin() + t * nf, tp.begin() + (t + 1) * nf);
         }
     }
 

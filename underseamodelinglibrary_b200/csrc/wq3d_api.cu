@@ -218,7 +218,10 @@ struct wq3d_queue {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;
+    cudaStream_t eig = nullptr; /* k_commit and the eigenray construction */
     std::vector<cudaEvent_t> fork_ev, join_ev;
+    std::vector<cudaEvent_t> adv_ev, com_ev, cpa_ev; /* per step of a chunk */
+    cudaEvent_t eig_end = nullptr;
     QueueDev h{};
     std::vector<void*> allocs;
     void* pinned = nullptr;
@@ -274,6 +277,9 @@ struct wq3d_queue {
     bool gridded = false;
     void (*k_reflect_fn)(const QueueDev, int) = analytic::k_reflect;
     void (*k_advance_fn)(const QueueDev, int) = analytic::k_advance;
+    /* eigenverb counting sink (wq3d_queue_count_eigenverbs) */
+    bool count_verbs = false;
+    uint64_t verb_counts[2 + 2 * WQ3D_MAX_VOLUME] = {0};
     /* set while wq3d_queue_create re-initialises a queue taken from the
      * cache of destroyed queues: uploads then copy into the buffers the
      * queue already has */
@@ -440,6 +446,10 @@ struct wq3d_queue {
             if (e) cudaEventDestroy(e);
         for (auto e : fork_ev) cudaEventDestroy(e);
         for (auto e : join_ev) cudaEventDestroy(e);
+        for (auto* v : {&adv_ev, &com_ev, &cpa_ev})
+            for (auto e : *v) cudaEventDestroy(e);
+        if (eig_end) cudaEventDestroy(eig_end);
+        if (eig) cudaStreamDestroy(eig);
         if (side) cudaStreamDestroy(side);
         if (ev_begin) cudaEventDestroy(ev_begin);
         if (ev_end) cudaEventDestroy(ev_end);
@@ -488,6 +498,12 @@ struct wq3d_queue {
          * fans, up to EIG_BLOCKS */
         const int eig_blocks = std::min(EIG_BLOCKS, std::max(148, (n + 255) / 256));
         if (timing) tail = false;
+        /* Without per-kernel timing, step k's commit and eigenray
+         * construction run on their own stream beside step k+1's advance and
+         * CPA search: step k+1's k_commit (which rewrites the fronts step k's
+         * eigenrays read) waits for them in stream order, and step k+2's
+         * reflections wait for that commit. */
+        const bool ovl = !timing;
         if (timing) cudaEventRecord(events[7 * K], stream);
         k_reflect_fn<<<rgrid, 64, 0, stream>>>(d, 0);
         if (timing) cudaEventRecord(events[7 * K + 1], stream);
@@ -504,12 +520,24 @@ struct wq3d_queue {
                 launches += 1;
             }
             k_advance_fn<<<grd, blk, 0, stream>>>(d, k);
+            launches += 2;
+            if (ovl) {
+                cudaEventRecord(adv_ev[k], stream);
+                cudaStreamWaitEvent(eig, adv_ev[k], 0);
+                k_commit<<<grd, blk, 0, eig>>>(d, k);
+                cudaEventRecord(com_ev[k], eig);
+            } else {
+                k_commit<<<grd, blk, 0, stream>>>(d, k);
+            }
             if (ev) cudaEventRecord(ev[1], stream);
-            launches += 1;
             const bool more = k + 1 < K || tail;
             if (more) {
-                cudaEventRecord(fork_ev[k], stream);
-                cudaStreamWaitEvent(side, fork_ev[k], 0);
+                if (ovl) {
+                    cudaStreamWaitEvent(side, com_ev[k], 0);
+                } else {
+                    cudaEventRecord(fork_ev[k], stream);
+                    cudaStreamWaitEvent(side, fork_ev[k], 0);
+                }
                 if (ev) cudaEventRecord(ev[5], side);
                 k_reflect_fn<<<rgrid, 64, 0, side>>>(d, k + 1);
                 if (ev) cudaEventRecord(ev[6], side);
@@ -527,11 +555,17 @@ struct wq3d_queue {
                 else
                     k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d, k);
                 if (ev) cudaEventRecord(ev[3], stream);
-                k_eigenray<<<eig_blocks, 128, 0, stream>>>(d, k);
+                cudaStream_t es = stream;
+                if (ovl) {
+                    cudaEventRecord(cpa_ev[k], stream);
+                    cudaStreamWaitEvent(eig, cpa_ev[k], 0);
+                    es = eig;
+                }
+                k_eigenray<<<eig_blocks, 128, 0, es>>>(d, k);
                 launches += 2;
                 if (h.adj) {
-                    k_eigenray_jac<<<4 * 148, 64, 0, stream>>>(d, k);
-                    k_adj_mark<<<1, 1, 0, stream>>>(d);
+                    k_eigenray_jac<<<4 * 148, 64, 0, es>>>(d, k);
+                    k_adj_mark<<<1, 1, 0, es>>>(d);
                     launches += 2;
                 }
             } else if (ev) {
@@ -539,6 +573,10 @@ struct wq3d_queue {
             }
             if (ev) cudaEventRecord(ev[4], stream);
             if (more) cudaStreamWaitEvent(stream, join_ev[k], 0);
+        }
+        if (ovl) {
+            cudaEventRecord(eig_end, eig);
+            cudaStreamWaitEvent(stream, eig_end, 0);
         }
         return WQ3D_OK;
     }
@@ -633,8 +671,12 @@ struct wq3d_queue {
                     ++ir;
                 } else {
                     const size_t j = vorder[iv];
-                    if (cb.add_eigenverb)
+                    if (count_verbs) {
+                        const int in = verbs[j].interface_num;
+                        if (in >= 0 && in < 2 + 2 * WQ3D_MAX_VOLUME) ++verb_counts[in];
+                    } else if (cb.add_eigenverb) {
                         cb.add_eigenverb(cb_ctx, &verbs[j], &vpower[j * nf], (size_t)nf, verbs[j].interface_num);
+                    }
                     ++iv;
                 }
             }
@@ -679,7 +721,7 @@ struct wq3d_queue {
         if (!timing && K == chunk) build_graph(p, tail);
         if (!timing && K == chunk && graph[p][t]) {
             WQ_CK(cudaGraphLaunch(graph[p][t], stream));
-            launches += ((h.nt > 0 ? 4 : 2) + (volume_pass() ? 1 : 0) + (h.adj ? (h.nt > 0 ? 3 : 1) : 0)) *
+            launches += ((h.nt > 0 ? 5 : 3) + (volume_pass() ? 1 : 0) + (h.adj ? (h.nt > 0 ? 3 : 1) : 0)) *
                             (int64_t)K + (tail ? 1 : 0);
         } else {
             launch_chunk(K, p, tail);
@@ -1142,6 +1184,8 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         q->ms_step = q->ms_cpa = q->ms_eig = q->ms_total = q->ms_refl = 0.0;
         q->launches = 0;
         q->grow_verb = q->grow_refl = 0;
+        q->count_verbs = false;
+        for (auto& c : q->verb_counts) c = 0;
     } else {
         q = new wq3d_queue();
     }
@@ -1357,6 +1401,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
             (rc = q->alloc(&h.shadow_slot, n)))
             return cleanup(rc);
         if ((rc = q->alloc(&h.work[0], n)) || (rc = q->alloc(&h.work[1], n))) return cleanup(rc);
+        if ((rc = q->alloc(&h.commit_flag, n))) return cleanup(rc);
     }
     h.d_base = q->d_base;
     h.d_times = q->d_times;
@@ -1393,17 +1438,20 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         if (cudaEventCreate(&q->ev_begin) != cudaSuccess || cudaEventCreate(&q->ev_end) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
         if (cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&q->eig, cudaStreamNonBlocking) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
+        if (cudaEventCreateWithFlags(&q->eig_end, cudaEventDisableTiming) != cudaSuccess)
+            return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
         for (auto& e : q->done_ev)
             if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
                 return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-        q->fork_ev.resize(q->chunk);
-        q->join_ev.resize(q->chunk);
-        for (int k = 0; k < q->chunk; ++k)
-            if (cudaEventCreateWithFlags(&q->fork_ev[k], cudaEventDisableTiming) != cudaSuccess ||
-                cudaEventCreateWithFlags(&q->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
-                return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+        for (auto* v : {&q->fork_ev, &q->join_ev, &q->adv_ev, &q->com_ev, &q->cpa_ev}) {
+            v->resize(q->chunk);
+            for (int k = 0; k < q->chunk; ++k)
+                if (cudaEventCreateWithFlags(&(*v)[k], cudaEventDisableTiming) != cudaSuccess)
+                    return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
+        }
     }
     /* the chunk graphs hold the descriptor by value */
     if (reuse && std::memcmp(&old_h, &h, sizeof(h)) != 0) q->drop_graph();
@@ -1423,7 +1471,8 @@ int wq3d_queue_destroy(wq3d_queue* q) {
     if (!q) return WQ3D_OK;
     DeviceGuard guard(q->device);
     if (cacheable(q) && cudaStreamSynchronize(q->stream) == cudaSuccess &&
-        cudaStreamSynchronize(q->side) == cudaSuccess && cudaStreamSynchronize(q->copy) == cudaSuccess) {
+        cudaStreamSynchronize(q->side) == cudaSuccess && cudaStreamSynchronize(q->eig) == cudaSuccess &&
+        cudaStreamSynchronize(q->copy) == cudaSuccess) {
         wq3d_queue* drop = nullptr;
         {
             std::lock_guard<std::mutex> lock(g_cache_mu);
@@ -1463,6 +1512,8 @@ int wq3d_queue_set_thresholds(wq3d_queue* q, const wq3d_thresholds* t) {
     return WQ3D_OK;
 }
 
+static int apply_listener_wants(wq3d_queue* q);
+
 int wq3d_queue_set_callbacks(wq3d_queue* q, const wq3d_callbacks* cb, void* ctx) {
     if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
     DeviceGuard guard(q->device);
@@ -1471,15 +1522,20 @@ int wq3d_queue_set_callbacks(wq3d_queue* q, const wq3d_callbacks* cb, void* ctx)
     else
         q->cb = wq3d_callbacks{};
     q->cb_ctx = ctx;
+    return apply_listener_wants(q);
+}
+
+/* record buffers and descriptor flags for the notices someone will take */
+static int apply_listener_wants(wq3d_queue* q) {
     const int want = q->cb.reflect ? 1 : 0;
-    const int want_verbs = q->cb.add_eigenverb ? 1 : 0;
+    const int want_verbs = (q->cb.add_eigenverb || q->count_verbs) ? 1 : 0;
     if (want) {
         const int rc = q->ensure_refl_capacity((size_t)(q->chunk + 1) * q->h.n / 2);
         if (rc) return rc;
     }
     if (want_verbs && !q->h.verb) {
         /* eigenverb buffers, made the first time a listener asks */
-        const int rc = q->ensure_verb_capacity((size_t)q->chunk * q->h.n * (q->h.oc.nvol + 1) / 2);
+        const int rc = q->ensure_verb_capacity((size_t)q->chunk * q->h.n * (q->h.oc.nvol + 1) / 32);
         if (rc) return rc;
     }
     if (want != q->h.want_refl || want_verbs != q->h.want_verbs) {
@@ -1487,6 +1543,19 @@ int wq3d_queue_set_callbacks(wq3d_queue* q, const wq3d_callbacks* cb, void* ctx)
         q->h.want_verbs = want_verbs;
         q->drop_graph();
     }
+    return WQ3D_OK;
+}
+
+int wq3d_queue_count_eigenverbs(wq3d_queue* q, int on) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    DeviceGuard guard(q->device);
+    q->count_verbs = on != 0;
+    return apply_listener_wants(q);
+}
+
+int wq3d_queue_eigenverb_counts(const wq3d_queue* q, uint64_t* counts) {
+    if (!q || !counts) return fail(WQ3D_ERR_INVALID, "null argument");
+    for (int k = 0; k < 2 + 2 * WQ3D_MAX_VOLUME; ++k) counts[k] = q->verb_counts[k];
     return WQ3D_OK;
 }
 
@@ -1713,8 +1782,34 @@ int wq3d_queue_enable_adjoint(wq3d_queue* q, int checkpoint_interval, size_t max
     return WQ3D_OK;
 }
 
+namespace {
+/* one unit seed on one ray's state component (wq3d_queue_adjoint_state) */
+struct AdjUnitSeed {
+    int ray;
+    int64_t step;
+    int comp;
+};
+}  // namespace
+
+static int adjoint_sweep(wq3d_queue* q, const wq3d_eigenray* rays, const double* w_tl, const double* w_time,
+                         size_t n_rays, double* grad, size_t num_nodes, double* ms, const AdjUnitSeed* xs);
+
 int wq3d_queue_adjoint(wq3d_queue* q, const wq3d_eigenray* rays, const double* w_tl, const double* w_time,
                        size_t n_rays, double* grad, size_t num_nodes, double* ms) {
+    return adjoint_sweep(q, rays, w_tl, w_time, n_rays, grad, num_nodes, ms, nullptr);
+}
+
+int wq3d_queue_adjoint_state(wq3d_queue* q, int ray, int64_t step, int component, double* grad,
+                             size_t num_nodes) {
+    if (!q || !grad) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (ray < 0 || ray >= q->h.n || component < 0 || component >= ADJ_L || step < 0 || step > q->steps)
+        return fail(WQ3D_ERR_INVALID, "ray, step or state component out of range");
+    const AdjUnitSeed xs{ray, step, component};
+    return adjoint_sweep(q, nullptr, nullptr, nullptr, 0, grad, num_nodes, nullptr, &xs);
+}
+
+static int adjoint_sweep(wq3d_queue* q, const wq3d_eigenray* rays, const double* w_tl, const double* w_time,
+                         size_t n_rays, double* grad, size_t num_nodes, double* ms, const AdjUnitSeed* xs) {
     if (!q || !grad) return fail(WQ3D_ERR_INVALID, "null argument");
     if (n_rays && (!rays || !w_tl || !w_time)) return fail(WQ3D_ERR_INVALID, "null argument");
     if (!q->h.adj) return fail(WQ3D_ERR_INVALID, "adjoint recording is off (wq3d_queue_enable_adjoint)");
@@ -1725,7 +1820,7 @@ int wq3d_queue_adjoint(wq3d_queue* q, const wq3d_eigenray* rays, const double* w
     for (int j = 0; j < nodes; ++j) grad[j] = 0.0;
     if (ms) *ms = 0.0;
     const int64_t m_end = q->steps;
-    if (m_end < 1 || n_rays == 0) return WQ3D_OK;
+    if (m_end < 1 || (n_rays == 0 && !xs)) return WQ3D_OK;
     DeviceGuard guard(q->device);
     WQ_CK(cudaStreamSynchronize(q->stream));
     const size_t n = (size_t)h.n;
@@ -1796,6 +1891,10 @@ int wq3d_queue_adjoint(wq3d_queue* q, const wq3d_eigenray* rays, const double* w
     WQ_CK(cudaEventRecord(e0, st));
     if (nrec > 0) WQ_CK(cudaMemcpyAsync(W.w, w.data(), 2 * (size_t)nrec * sizeof(double), cudaMemcpyHostToDevice, st));
     WQ_CK(cudaMemsetAsync(W.last, 0, n * sizeof(int64_t), st));
+    if (xs) {
+        const int64_t biased = xs->step + 1;
+        WQ_CK(cudaMemcpyAsync(W.last + xs->ray, &biased, sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    }
     WQ_CK(cudaMemsetAsync(W.lam, 0, (size_t)ADJ_L * n * sizeof(double), st));
     WQ_CK(cudaMemsetAsync(W.grad, 0, ADJ_MAX_NODES * sizeof(double), st));
     WQ_CK(cudaMemsetAsync(W.err, 0, sizeof(uint32_t), st));
@@ -1829,6 +1928,11 @@ int wq3d_queue_adjoint(wq3d_queue* q, const wq3d_eigenray* rays, const double* w
         if (a.m1 - a.m0 > K + 1) return fail(WQ3D_ERR_OVERFLOW, "the run went past the adjoint's max_steps");
         a.ckpt = (int)c;
         WQ_CK(cudaMemsetAsync(W.seed, 0, (size_t)(a.m1 - a.m0) * ADJ_L * n * sizeof(double), st));
+        if (xs && xs->step >= a.m0 && xs->step < a.m1) {
+            const double one = 1.0;
+            WQ_CK(cudaMemcpyAsync(W.seed + ((size_t)(xs->step - a.m0) * ADJ_L + xs->comp) * n + xs->ray, &one,
+                                  sizeof(double), cudaMemcpyHostToDevice, st));
+        }
         k_adj_recompute<<<gb, 128, 0, st>>>(a, qa);
         if (nrec > 0) k_adj_expand<<<rb, 128, 0, st>>>(a, qa);
         k_adj_reverse<<<gb, 128, 0, st>>>(a, qa);

@@ -43,6 +43,9 @@ enum : uint32_t {
     ERR_ADJ_OVERFLOW = 128u      /* adjoint checkpoint or record buffer full    */
 };
 
+/* k_advance's decisions for k_commit (QueueDev::commit_flag) */
+enum : uint8_t { COMMIT_REFLECT = 1, COMMIT_FOLD = 2, COMMIT_UPPER = 4, COMMIT_LOWER = 8 };
+
 /* Per-eigenray partial derivatives recorded for the adjoint (one per
  * eigenray record while adjoint recording is on).  TL is the first
  * frequency's.  The cube values are the 27 target distance2 values that
@@ -144,6 +147,7 @@ struct QueueDev {
     double* shadow;          /* reflected prev/curr/next per worklist slot  */
     int32_t* shadow_cnt;     /* surface, bottom, caustic per slot           */
     int32_t* shadow_slot;    /* worklist slot of each reflecting ray        */
+    uint8_t* commit_flag;    /* per ray: COMMIT_* bits k_advance leaves for k_commit */
     /* eigenray candidates of the current step */
     uint32_t* cand;          /* packed: target index, ray index              */
     uint32_t* n_cand;
@@ -197,6 +201,7 @@ namespace analytic {
 WQ3D_DECLARE_STEP_KERNELS
 }
 __global__ void k_volume(__grid_constant__ const QueueDev q, int k);
+__global__ void k_commit(__grid_constant__ const QueueDev q, int k);
 __global__ void k_cpa(__grid_constant__ const QueueDev q, int k);
 __global__ void k_cpa_f32(__grid_constant__ const QueueDev q, int k);
 /* k_eigenray blocks (4 warps each, one candidate per warp pair at a

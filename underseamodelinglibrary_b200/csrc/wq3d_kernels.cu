@@ -921,23 +921,17 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     bool fold_hit = false, vtx_up = false, vtx_lo = false;
     if (refl) {
         /* commit the reflected ray (reflection_copy into prev, curr, next) */
+        /* the reflected ray's states come from its shadow slot; k_commit
+         * writes them into the prev, curr and next fronts once the previous
+         * step's eigenray construction no longer reads those fronts */
         const int32_t w = __ldg(q.shadow_slot + i);
         sh = q.shadow + (size_t)w * stride;
-        /* one state at a time: its stores may alias the later loads as
-         * far as the compiler knows, so loading all three first would keep
-         * 51 values live */
         ray_from(sh, y0);
-        copy_ray(*R.V, i, y0);
         ray_from(sh + 17, y1);
-        copy_ray(*R.C, i, y1);
         ray_from(sh + 34, y2);
-        copy_ray(*R.X, i, y2);
         sf = __ldg(q.shadow_cnt + 3 * (size_t)w);
         bt = __ldg(q.shadow_cnt + 3 * (size_t)w + 1);
         cs = __ldg(q.shadow_cnt + 3 * (size_t)w + 2);
-        R.V->surface[i] = R.C->surface[i] = R.X->surface[i] = sf;
-        R.V->bottom[i] = R.C->bottom[i] = R.X->bottom[i] = bt;
-        R.X->caustic[i] = cs;
     } else {
         /* detect_caustics of the neighbour below (wave_queue.cc:274-292) */
         if (d >= 1 && !fl[1]) {
@@ -992,10 +986,11 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     /* the per-step finiteness check: a NaN or Inf in the environment (a
      * bad profile node, a zero sound speed) reaches the new front here */
     if (!isfinite(y3.pos[0] + y3.pos[1] + y3.pos[2] + y3.nd[0] + y3.nd[1] + y3.nd[2])) set_err(q, ERR_NONFINITE);
-    /* stores */
-    if (fold_hit) R.X->caustic[i] = cs;
-    if (vtx_up) R.X->upper[i] = up;
-    if (vtx_lo) R.X->lower[i] = lo;
+    /* stores: the new front, the next front's edge flag (not read by the
+     * previous step's eigenray construction) and what k_commit changes on
+     * the prev / curr / next fronts */
+    q.commit_flag[i] = (uint8_t)((refl ? COMMIT_REFLECT : 0) | (fold_hit ? COMMIT_FOLD : 0) |
+                                 (vtx_up ? COMMIT_UPPER : 0) | (vtx_lo ? COMMIT_LOWER : 0));
     R.X->on_edge[i] = edge ? 1 : 0;
     const FrontPtrs& P = *R.P;
     copy_ray(P, i, y3);
@@ -1023,15 +1018,10 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
         if (refl) {
             ax = __ldg(sh + 51 + f);
             px = __ldg(sh + 51 + q.nf + f);
-            R.X->atten[o] = ax;
-            R.X->phase[o] = px;
         } else {
             ax = __ldg(R.X->atten + o);
             px = __ldg(R.X->phase + o);
-            if (fold_hit) {
-                px -= M_PI_2;
-                R.X->phase[o] = px;
-            }
+            if (fold_hit) px -= M_PI_2;
         }
         double a;
         if (q.oc.prof.atten == WQ3D_ATTEN_CONSTANT) {
@@ -1052,6 +1042,48 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
 }  // namespace WQ3D_KERNEL_NS
 
 #if !WQ3D_STEP_KERNELS_ONLY
+/* What k_advance of step s decided for the prev / curr / next fronts, done
+ * after the eigenray construction of step s-1 has read them: a reflected
+ * ray's three states, counts and next-front losses from its shadow slot
+ * (reflection_model::reflection_copy, reflection_model.cc:335-360), and for
+ * the other rays the caustic hand-off (count, and phase - pi/2 on every
+ * frequency, wave_queue.cc:274-292) and the vertex counts (:261-269). */
+__global__ void __launch_bounds__(128) k_commit(__grid_constant__ const QueueDev q, int k) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q.n) return;
+    const uint8_t b = q.commit_flag[i];
+    if (!b) return;
+    const int64_t s = *q.d_base + k;
+    Roles R;
+    roles_at(q, s, R);
+    if (b & COMMIT_REFLECT) {
+        const int32_t w = q.shadow_slot[i];
+        const double* sh = q.shadow + (size_t)w * shadow_stride(q);
+        RayS y;
+        ray_from(sh, y);
+        copy_ray(*R.V, i, y);
+        ray_from(sh + 17, y);
+        copy_ray(*R.C, i, y);
+        ray_from(sh + 34, y);
+        copy_ray(*R.X, i, y);
+        const int32_t sf = q.shadow_cnt[3 * (size_t)w], bt = q.shadow_cnt[3 * (size_t)w + 1];
+        R.V->surface[i] = R.C->surface[i] = R.X->surface[i] = sf;
+        R.V->bottom[i] = R.C->bottom[i] = R.X->bottom[i] = bt;
+        R.X->caustic[i] = q.shadow_cnt[3 * (size_t)w + 2];
+        for (int f = 0; f < q.nf; ++f) {
+            R.X->atten[(size_t)f * q.n + i] = sh[51 + f];
+            R.X->phase[(size_t)f * q.n + i] = sh[51 + q.nf + f];
+        }
+        return;
+    }
+    if (b & COMMIT_FOLD) {
+        R.X->caustic[i] += 1;
+        for (int f = 0; f < q.nf; ++f) R.X->phase[(size_t)f * q.n + i] -= M_PI_2;
+    }
+    if (b & COMMIT_UPPER) R.X->upper[i] += 1;
+    if (b & COMMIT_LOWER) R.X->lower[i] += 1;
+}
+
 /* Volume-layer eigenverbs of the rays that do not reflect in step s
  * (wave_queue.cc:202; k_reflect handles the reflecting ones).  Launched
  * before k_advance of the same step, only when an eigenverb listener is

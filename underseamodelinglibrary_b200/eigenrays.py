@@ -5,7 +5,6 @@ per target (eigenray_collection.cc:90-100) and ``sum_eigenrays`` forms the
 coherent (or incoherent) phasor sum per frequency with power-weighted
 averages of time and angles (eigenray_collection.cc:105-191).
 """
-import cmath
 import math
 
 import numpy as np
@@ -74,62 +73,45 @@ class eigenray_collection(eigenray_listener):
 
     def sum_eigenrays(self):
         """eigenray_collection::sum_eigenrays (eigenray_collection.cc:
-        105-191), one target at a time with numpy.  Every sum runs in the
-        reference's order (frequency, then eigenray) as a sequential
-        cumulative sum: the phasor of each frequency, and the weights
-        a^2 = 10^(-I/10) with the weighted travel time, D/E and the unit
-        vectors of AZ.  The strongest path (first largest weight) gives the
-        counts."""
+        105-191) on the GPU (wq3d_sum_eigenrays): per target, the coherent
+        (or incoherent) phasor sum of its eigenrays at each frequency, in
+        the order they were added, and the power-weighted travel time, D/E
+        and AZ; the strongest path gives the counts."""
+        import ctypes as C
+
+        from . import _abi
+        lib = _abi.load_engine()
         nf = self._freq.size()
-        fv = np.array([self._freq[f] for f in range(nf)], dtype=np.float64)
-        two_pi = 2.0 * math.pi
-        for t1 in range(self.size1()):
-            for t2 in range(self.size2()):
-                rays = self._rays[t1][t2]
-                tot = eigenray_total()
-                n = len(rays)
-                if n == 0:
-                    tot.intensity = [-20.0 * math.log10(1e-15)] * nf
-                    tot.phase = [0.0] * nf
-                    tot.travel_time = tot.source_de = tot.target_de = float("nan")
-                    tot.source_az = tot.target_az = 90.0 - to_degrees(math.atan2(0.0, 0.0))
-                    tot.surface = tot.bottom = tot.caustic = tot.upper = tot.lower = -1
-                    self._total[t1][t2] = tot
-                    continue
-                amp = np.power(10.0, np.array([r.intensity for r in rays], dtype=np.float64).T / -20.0)
-                if self._coherent:
-                    tt = np.array([r.travel_time for r in rays], dtype=np.float64)
-                    ph = np.array([r.phase for r in rays], dtype=np.float64).T
-                    p = np.fmod(two_pi * fv[:, None] * tt[None, :] + ph, two_pi)
-                    re = np.cumsum(amp * np.cos(p), axis=1)[:, -1]
-                    im = np.cumsum(amp * np.sin(p), axis=1)[:, -1]
-                else:
-                    re = np.cumsum(amp, axis=1)[:, -1]
-                    im = np.zeros(nf)
-                tot.intensity = [float(x) for x in -20.0 * np.log10(np.maximum(1e-15, np.hypot(re, im)))]
-                tot.phase = [float(x) for x in np.arctan2(im, re)]
-                w = (amp * amp).ravel()  # (frequency, eigenray) order
-                wgt = float(np.cumsum(w)[-1])
-
-                def wsum(v):
-                    return float(np.cumsum(w * np.tile(np.asarray(v, dtype=np.float64), nf))[-1])
-
-                saz = np.radians([r.source_az for r in rays])
-                taz = np.radians([r.target_az for r in rays])
-                nan = float("nan")
-                tot.travel_time = wsum([r.travel_time for r in rays]) / wgt if wgt else nan
-                tot.source_de = wsum([r.source_de for r in rays]) / wgt if wgt else nan
-                tot.source_az = 90.0 - to_degrees(math.atan2(wsum(np.cos(saz)), wsum(np.sin(saz))))
-                tot.target_de = wsum([r.target_de for r in rays]) / wgt if wgt else nan
-                tot.target_az = 90.0 - to_degrees(math.atan2(wsum(np.cos(taz)), wsum(np.sin(taz))))
-                j = int(np.argmax(w))
-                if w[j] > 0.0:
-                    best = rays[j % n]
-                    tot.surface, tot.bottom, tot.caustic = best.surface, best.bottom, best.caustic
-                    tot.upper, tot.lower = best.upper, best.lower
-                else:
-                    tot.surface = tot.bottom = tot.caustic = tot.upper = tot.lower = -1
-                self._total[t1][t2] = tot
+        n1, n2 = self.size1(), self.size2()
+        fv = np.ascontiguousarray([self._freq[f] for f in range(nf)], dtype=np.float64)
+        rays = [(t1, t2, r) for t1 in range(n1) for t2 in range(n2) for r in self._rays[t1][t2]]
+        n = len(rays)
+        rec = (_abi.wq3d_eigenray * max(n, 1))()
+        inten = np.zeros((max(n, 1), nf))
+        phase = np.zeros((max(n, 1), nf))
+        for k, (t1, t2, r) in enumerate(rays):
+            e = rec[k]
+            e.time, e.source_de, e.source_az = r.travel_time, r.source_de, r.source_az
+            e.target_de, e.target_az = r.target_de, r.target_az
+            e.surface, e.bottom, e.caustic, e.upper, e.lower = r.surface, r.bottom, r.caustic, r.upper, r.lower
+            e.t1, e.t2 = t1, t2
+            inten[k] = r.intensity
+            phase[k] = r.phase
+        tot = (_abi.wq3d_eigenray * (n1 * n2))()
+        ti = np.empty((n1 * n2, nf))
+        tp = np.empty((n1 * n2, nf))
+        _abi.check(lib, lib.wq3d_sum_eigenrays(C.cast(rec, C.c_void_p), _abi.as_dp(inten), _abi.as_dp(phase), n,
+                                               _abi.as_dp(fv), nf, n1, n2, 1 if self._coherent else 0,
+                                               C.cast(tot, C.c_void_p), _abi.as_dp(ti), _abi.as_dp(tp)))
+        for t in range(n1 * n2):
+            o = tot[t]
+            out = eigenray_total()
+            out.travel_time, out.source_de, out.source_az = o.time, o.source_de, o.source_az
+            out.target_de, out.target_az = o.target_de, o.target_az
+            out.surface, out.bottom, out.caustic, out.upper, out.lower = o.surface, o.bottom, o.caustic, o.upper, o.lower
+            out.intensity = [float(x) for x in ti[t]]
+            out.phase = [float(x) for x in tp[t]]
+            self._total[t // n2][t % n2] = out
 
 
 def _evaluator(profile):

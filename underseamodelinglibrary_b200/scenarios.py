@@ -235,7 +235,7 @@ def _smooth(field, sigmas):
 
 def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_lng=20,
                   n_bathy=100, ssp_std=5.0, corr_h=50e3, corr_v=300.0, depth_min=1000.0,
-                  depth_max=5000.0, surface=None):
+                  depth_max=5000.0, surface=None, bottom_loss=None):
     """Gridded environment over span x span degrees centred on (lat0, lng0):
 
     * profile_grid<3> on (rho, theta, phi) with n_depth nodes 0-5000 m x
@@ -245,7 +245,9 @@ def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_
     * boundary_grid<2> bottom on n_bathy x n_bathy (theta, phi) nodes:
       Gaussian-smoothed random relief scaled to depth_min..depth_max,
       linear both ways, Rayleigh sand loss (the boundary_grid default);
-    * ``surface``: the ocean surface (default boundary_flat()).
+    * ``surface``: the ocean surface (default boundary_flat());
+    * ``bottom_loss``: the bathymetry's reflection loss (default Rayleigh
+      sand, the boundary_grid default).
 
     Inputs are seeded synthetic fields (no data files)."""
     R = T.earth_radius()
@@ -269,7 +271,7 @@ def gridded_ocean(rng, lat0=45.0, lng0=-45.0, span=2.0, n_depth=50, n_lat=20, n_
     relief = _smooth(rng.standard_normal((n_bathy, n_bathy)), (n_bathy / 12.0, n_bathy / 12.0))
     relief = (relief - relief.min()) / max(relief.max() - relief.min(), 1e-30)
     bathy = data_grid([bt_ax, bp_ax], R - (depth_min + (depth_max - depth_min) * relief))
-    return ocean_model(surface if surface is not None else boundary_flat(), boundary_grid(bathy),
+    return ocean_model(surface if surface is not None else boundary_flat(), boundary_grid(bathy, bottom_loss),
                        profile_grid(ssp))
 
 
@@ -302,16 +304,17 @@ def gridded_munk(seed=1, num_de=91, num_az=13, n_targets=64, time_max=30.0, src_
 
 
 def reverb_scale(source_depth=100.0, num_de=3601, num_az=181, n_targets=4096, time_max=180.0,
-                 seed=20261203):
+                 seed=20261203, bottom_loss=None):
     """Reverberation-scale workload for one source depth: gridded_ocean()
     (random profile grid and bathymetry) with Eckart surface loss at 10 m/s
     wind, source ``source_depth`` m deep at 45N 45W, 32 log-spaced
     frequencies 100 Hz - 10 kHz with Thorp attenuation, tangent-spaced D/E
     fan x AZ 0..360 deg in 2 deg steps, dt 0.05 s, 4096 random targets
-    (10-4000 m deep within 100 km)."""
+    (10-4000 m deep within 100 km).  ``bottom_loss``: the bathymetry's
+    reflection loss (default Rayleigh sand)."""
     T.compute_earth_radius(45.0)
     rng = np.random.default_rng(seed)
-    ocean = gridded_ocean(rng, surface=boundary_flat(0.0, reflect_loss_eckart(10.0)))
+    ocean = gridded_ocean(rng, surface=boundary_flat(0.0, reflect_loss_eckart(10.0)), bottom_loss=bottom_loss)
     src = T.wposition1(45.0, -45.0, -float(source_depth))
     tgt = random_targets(rng, src, n_targets)
     freq = T.seq_log(100.0, 100.0 ** (1.0 / 31.0), 32)

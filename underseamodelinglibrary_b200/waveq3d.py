@@ -477,6 +477,27 @@ class wave_queue:
             _abi.as_dp(grad), grad.size, C.byref(ms)))
         return grad, ms.value
 
+    def adjoint_state(self, ray, step, component, num_nodes):
+        """d (component of ray's state after step) / d profile nodes
+        (wq3d_queue_adjoint_state): the reverse sweep seeded on one state
+        value; components 0-17 are rho, theta, phi and the normalised
+        direction of the prev, curr and next fronts"""
+        grad = np.zeros(int(num_nodes))
+        _abi.check(self._lib, self._lib.wq3d_queue_adjoint_state(self._q, int(ray), int(step), int(component),
+                                                                 _abi.as_dp(grad), grad.size))
+        return grad
+
+    def count_eigenverbs(self, on=True):
+        """builds eigenverbs and counts them per interface instead of
+        delivering them (wq3d_queue_count_eigenverbs)"""
+        _abi.check(self._lib, self._lib.wq3d_queue_count_eigenverbs(self._q, 1 if on else 0))
+
+    def eigenverb_counts(self):
+        """eigenverbs counted per interface number since counting began"""
+        out = (C.c_uint64 * (2 + 2 * _abi.MAX_VOLUME))()
+        _abi.check(self._lib, self._lib.wq3d_queue_eigenverb_counts(self._q, out))
+        return [int(x) for x in out]
+
     def set_timing(self, on):
         _abi.check(self._lib, self._lib.wq3d_queue_set_timing(self._q, 1 if on else 0))
 
