@@ -226,7 +226,9 @@ struct wq3d_queue {
     std::vector<void*> allocs;
     void* pinned = nullptr;
     /* per result set: chunk base step, chunk times, counters read back
-     * (n_rec, n_refl, err, n_cand, ..., n_verb) */
+     * (n_rec, n_refl, err, -, work lists, n_done, -, n_verb); d_counts also
+     * holds the bottom work lists (9, 10), the adjoint's mark and entry
+     * count (11, 12) and the two candidate counts (13, 14) */
     int64_t* h_base[2] = {nullptr, nullptr};
     double* h_times[2] = {nullptr, nullptr};
     uint32_t* h_counts[2] = {nullptr, nullptr};
@@ -806,6 +808,9 @@ struct wq3d_queue {
         if (err & ERR_NONFINITE)
             return fail(WQ3D_ERR_NUMERIC, "a ray's position or direction became NaN or Inf (error bits " +
                                               std::to_string(err) + "); check the ocean's profile and boundaries");
+        if (err & ERR_BAD_CANDIDATE)
+            return fail(WQ3D_ERR_CUDA, "internal error: an eigenray candidate named a ray or target outside "
+                                       "the fan (error bits " + std::to_string(err) + ")");
         if (err)
             return fail(WQ3D_ERR_NUMERIC, "kernel iteration bound reached (error bits " + std::to_string(err) + ")");
         return WQ3D_OK;
@@ -1374,7 +1379,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.cap_refl = 4096; /* grown when a reflection listener asks */
     if (!reuse) {
         uint32_t* cand = nullptr;
-        if ((rc = q->alloc(&cand, 2 * (size_t)h.cap_cand))) return cleanup(rc);
+        if ((rc = q->alloc(&cand, 4 * (size_t)h.cap_cand))) return cleanup(rc);
         h.cand = cand;
         if ((rc = q->alloc(&h.rec, h.cap_rec)) || (rc = q->alloc(&h.rec_inten, (size_t)h.cap_rec * nf)) ||
             (rc = q->alloc(&h.rec_phase, (size_t)h.cap_rec * nf)) || (rc = q->alloc(&h.refl, h.cap_refl)))
@@ -1386,7 +1391,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.n_rec = q->d_counts + 0;
     h.n_refl = q->d_counts + 1;
     h.err = q->d_counts + 2;
-    h.n_cand = q->d_counts + 3;
+    h.n_cand = q->d_counts + 13; /* two lists: 13, 14 */
     h.n_work[0] = q->d_counts + 4;
     h.n_work[1] = q->d_counts + 5;
     h.n_work_b[0] = q->d_counts + 9;
@@ -1396,7 +1401,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.want_verbs = 0;
     h.verb_threshold = 1e-30; /* wave_thresholds.h:40 */
     if (!reuse) {
-        const size_t stride = 51 + 2 * nf;
+        const size_t stride = 54 + 2 * nf;
         if ((rc = q->alloc(&h.shadow, n * stride)) || (rc = q->alloc(&h.shadow_cnt, 3 * n)) ||
             (rc = q->alloc(&h.shadow_slot, n)))
             return cleanup(rc);

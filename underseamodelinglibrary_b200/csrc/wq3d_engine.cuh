@@ -40,7 +40,8 @@ enum : uint32_t {
     ERR_WALK_LIMIT = 16u,        /* a Gaussian-beam walk exceeded its bound    */
     ERR_VERB_OVERFLOW = 32u,     /* eigenverb record buffer full               */
     ERR_NONFINITE = 64u,         /* a ray's new position or direction is NaN/Inf */
-    ERR_ADJ_OVERFLOW = 128u      /* adjoint checkpoint or record buffer full    */
+    ERR_ADJ_OVERFLOW = 128u,     /* adjoint checkpoint or record buffer full    */
+    ERR_BAD_CANDIDATE = 256u     /* a candidate names a ray or target outside the fan (skipped) */
 };
 
 /* k_advance's decisions for k_commit (QueueDev::commit_flag) */
@@ -148,9 +149,11 @@ struct QueueDev {
     int32_t* shadow_cnt;     /* surface, bottom, caustic per slot           */
     int32_t* shadow_slot;    /* worklist slot of each reflecting ray        */
     uint8_t* commit_flag;    /* per ray: COMMIT_* bits k_advance leaves for k_commit */
-    /* eigenray candidates of the current step */
-    uint32_t* cand;          /* packed: target index, ray index              */
-    uint32_t* n_cand;
+    /* eigenray candidates: two lists by step parity (cand_list), so the
+     * next step's advance and CPA search fill one while this step's
+     * eigenray construction, on its own stream, reads the other */
+    uint32_t* cand;          /* [2][cap_cand] packed: target, ray index      */
+    uint32_t* n_cand;        /* [2] counts                                   */
     uint32_t cap_cand;
     /* eigenray records of the chunk */
     wq3d_eigenray* rec;
@@ -183,6 +186,13 @@ struct QueueDev {
     uint32_t adj_cap;
     uint32_t* adj_mark;      /* eigenray records of the chunk processed     */
 };
+
+/* The candidate list of the step whose rotated roles start at s (the "s"
+ * of the CPA and eigenray kernels, one more than the advance's).  Step k's
+ * eigenray construction reads list (s+1)&1 while step k+1 clears and fills
+ * the other; step k+2's advance clears this one only after step k+1's
+ * commit, which follows step k's eigenray construction on its stream. */
+__device__ __forceinline__ int cand_list(int64_t s) { return (int)((s + 1) & 1); }
 
 /* kernels (wq3d_kernels.cu).  Every kernel takes the queue descriptor by
  * value as a __grid_constant__ parameter, so its fields are read through

@@ -622,8 +622,9 @@ __device__ __forceinline__ void work_append(const QueueDev& q, int p, uint8_t ki
 }
 
 /* shadow slot of a reflecting ray: prev, curr, next (17 doubles each), the
- * next front's attenuation and phase (nf each); counts in shadow_cnt */
-__device__ __forceinline__ size_t shadow_stride(const QueueDev& q) { return 51 + 2 * (size_t)q.nf; }
+ * next front's attenuation and phase (nf each), and the three loss
+ * tangents its bottom bounces add; counts in shadow_cnt */
+__device__ __forceinline__ size_t shadow_stride(const QueueDev& q) { return 54 + 2 * (size_t)q.nf; }
 
 __device__ __forceinline__ void ray_to(double* dst, const RayS& y) {
     for (int k = 0; k < 3; ++k) {
@@ -742,8 +743,7 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
         const int i = (int)work[w];
         RayLocal L;
         {
-            /* the fronts are read-only here (only X.dA is written, and it
-             * is not read this way) */
+            /* the fronts are read-only here */
             RayS v, c, x;
             load_ray_ro(*R.V, i, v);
             load_ray_ro(*R.C, i, c);
@@ -823,10 +823,11 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
             sh[51 + f] = L.att[f];
             sh[51 + q.nf + f] = L.ph[f];
         }
-        /* the next front's loss tangents take this step's bottom bounces;
-         * the front is not read by the concurrent CPA work of step s-1 */
+        /* the next front's loss tangents take this step's bottom bounces
+         * when k_commit applies the slot; the previous step's eigenray
+         * construction may still be reading them */
         if (q.sens)
-            for (int j = 0; j < 3; ++j) R.X->dA[(size_t)j * q.n + i] += dl[j];
+            for (int j = 0; j < 3; ++j) sh[51 + 2 * q.nf + j] = dl[j];
         q.shadow_cnt[3 * (size_t)w] = L.surface;
         q.shadow_cnt[3 * (size_t)w + 1] = L.bottom;
         q.shadow_cnt[3 * (size_t)w + 2] = L.caustic;
@@ -862,9 +863,9 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
 #endif
 __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, int k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *q.n_cand = 0;
-    if (i >= q.n) return;
     const int64_t s = *q.d_base + k;
+    if (blockIdx.x == 0 && threadIdx.x == 0) q.n_cand[cand_list(s + 1)] = 0;
+    if (i >= q.n) return;
     Roles R;
     roles_at(q, s, R);
     const uint8_t* flag_in = q.flag[s & 1];
@@ -1005,7 +1006,8 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     P.lower[i] = lo;
     P.caustic[i] = cs;
     if (q.sens)
-        for (int j = 0; j < 3; ++j) P.dA[(size_t)j * q.n + i] = __ldg(R.X->dA + (size_t)j * q.n + i);
+        for (int j = 0; j < 3; ++j)
+            P.dA[(size_t)j * q.n + i] = __ldg(R.X->dA + (size_t)j * q.n + i) + (refl ? __ldg(sh + 51 + 2 * q.nf + j) : 0.0);
     /* attenuation (attenuation_thorp.cc:14-36 / attenuation_constant.cc:
      * 14-25) added to the next front's, phase carried over; the next
      * front's own entries take the reflection's values or the caustic's
@@ -1074,6 +1076,8 @@ __global__ void __launch_bounds__(128) k_commit(__grid_constant__ const QueueDev
             R.X->atten[(size_t)f * q.n + i] = sh[51 + f];
             R.X->phase[(size_t)f * q.n + i] = sh[51 + q.nf + f];
         }
+        if (q.sens)
+            for (int j = 0; j < 3; ++j) R.X->dA[(size_t)j * q.n + i] += sh[51 + 2 * q.nf + j];
         return;
     }
     if (b & COMMIT_FOLD) {
@@ -1120,6 +1124,19 @@ __device__ __forceinline__ double d2_at(const FrontPtrs& f, int i, const TgtS& t
     const double rho = f.cpa[0][i];
     return target_distance2(rho, rho * rho, f.cpa[1][i], f.cpa[2][i], f.cpa[3][i],
                             t.th, t.ph, t.sn, t.R2, t.twoR);
+}
+
+/* appends (target, ray) to the candidate list of the step at s */
+__device__ __forceinline__ void cand_push(const QueueDev& q, int64_t s, uint32_t t, uint32_t i) {
+    const int l = cand_list(s);
+    const uint32_t slot = atomicAdd(q.n_cand + l, 1u);
+    if (slot < q.cap_cand) {
+        uint32_t* c = q.cand + (size_t)l * 2 * q.cap_cand;
+        c[2 * slot] = t;
+        c[2 * slot + 1] = i;
+    } else {
+        set_err(q, ERR_CAND_OVERFLOW);
+    }
 }
 
 __device__ __forceinline__ int wrap_az(const QueueDev& q, int az, int na) {
@@ -1212,13 +1229,7 @@ __global__ void __launch_bounds__(CPA_THREADS) k_cpa(__grid_constant__ const Que
         if (dp < center) continue;
         double cube[3][3][3];
         if (!is_closest(q, V, C, X, t, q.de_branch[t0 + j] != 0, de, az, center, cube)) continue;
-        const uint32_t slot = atomicAdd(q.n_cand, 1u);
-        if (slot < q.cap_cand) {
-            q.cand[2 * slot] = (uint32_t)(t0 + j);
-            q.cand[2 * slot + 1] = (uint32_t)i;
-        } else {
-            set_err(q, ERR_CAND_OVERFLOW);
-        }
+        cand_push(q, s, (uint32_t)(t0 + j), (uint32_t)i);
     }
 }
 
@@ -1267,7 +1278,7 @@ struct WarpQueue {
 };
 
 /* finishes queued pairs in FP64: entry = (thread of the ray << 16) | target */
-__device__ __noinline__ void cpa_finish(const QueueDev& q, const FrontPtrs& V, const FrontPtrs& C,
+__device__ __noinline__ void cpa_finish(const QueueDev& q, int64_t s, const FrontPtrs& V, const FrontPtrs& C,
                            const FrontPtrs& X, const TgtS* tile, int t0, int de0, int az0,
                            const uint32_t* e, int count, int lane) {
     if (lane >= count) return;
@@ -1282,13 +1293,7 @@ __device__ __noinline__ void cpa_finish(const QueueDev& q, const FrontPtrs& V, c
     if (d2_at(V, i, t) < center) return;
     double cube[3][3][3];
     if (!is_closest(q, V, C, X, t, q.de_branch[t0 + j] != 0, de, az, center, cube)) return;
-    const uint32_t slot = atomicAdd(q.n_cand, 1u);
-    if (slot < q.cap_cand) {
-        q.cand[2 * slot] = (uint32_t)(t0 + j);
-        q.cand[2 * slot + 1] = (uint32_t)i;
-    } else {
-        set_err(q, ERR_CAND_OVERFLOW);
-    }
+    cand_push(q, s, (uint32_t)(t0 + j), (uint32_t)i);
 }
 
 /* order-preserving keys of floats, for the warp's unsigned min / max
@@ -1505,7 +1510,7 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(__grid_constant__ co
                 qn += __popc(mask);
                 __syncwarp();
                 if (qn >= 32) {
-                    cpa_finish(q, V, C, X, tile, t0, de0, az0, myq, 32, lane);
+                    cpa_finish(q, s, V, C, X, tile, t0, de0, az0, myq, 32, lane);
                     __syncwarp();
                     if (lane < qn - 32) myq[lane] = myq[32 + lane];
                     __syncwarp();
@@ -1534,7 +1539,7 @@ __global__ void __launch_bounds__(CPA_THREADS, 4) k_cpa_f32(__grid_constant__ co
             if (want) want = !(screen_dot(g, dvc) < -gvc);
             push(want, j);
         }
-        if (qn > 0) cpa_finish(q, V, C, X, tile, t0, de0, az0, myq, qn, lane);
+        if (qn > 0) cpa_finish(q, s, V, C, X, tile, t0, de0, az0, myq, qn, lane);
     }
 }
 
@@ -2109,7 +2114,9 @@ __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ c
     const int pair = warp >> 1, half = warp & 1;
     const int64_t s = *q.d_base + k + 1;
     const double time = q.d_times[k + 1];
-    const uint32_t ncand = min(*q.n_cand, q.cap_cand);
+    const int list = cand_list(s);
+    const uint32_t ncand = min(q.n_cand[list], q.cap_cand);
+    const uint32_t* cand = q.cand + (size_t)list * 2 * q.cap_cand;
     WarpBuild B;
     B.q = &q;
     B.pV = &q.F[(s + 1) & 3];
@@ -2124,8 +2131,14 @@ __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ c
     const uint32_t npairs = gridDim.x * (EIG_WARPS / 2);
     for (uint32_t c = blockIdx.x * (EIG_WARPS / 2) + pair; c < ncand; c += npairs) {
         __syncwarp();
-        const int t = (int)q.cand[2 * c];
-        const int i = (int)q.cand[2 * c + 1];
+        const uint32_t tu = cand[2 * c], iu = cand[2 * c + 1];
+        /* the CPA kernels only queue interior rays and real targets */
+        if (tu >= (uint32_t)q.nt || iu >= (uint32_t)q.n || iu / q.naz < 1 || iu / q.naz > (uint32_t)q.nde - 2) {
+            if (lane == 0) set_err(q, ERR_BAD_CANDIDATE);
+            continue;
+        }
+        const int t = (int)tu;
+        const int i = (int)iu;
         const int de0 = i / q.naz, az0 = i % q.naz;
         /* above_bounce_threshold (wave_thresholds.h:192-199) */
         if (C.bottom[i] > q.max_bottom || C.surface[i] > q.max_surface ||
