@@ -105,7 +105,7 @@ def _write_grid(fh, grid):
 def test_cpp_std14_gridded(tmp_path, engine):
     """The reference's speed study (studies/cmp_speed/cmp_speed.cc:33-114)
     through the C++ header: STD14 profile_grid and boundary_grid built from
-    data_grid objects, 20 targets on the 100 km ring, 40 s; every eigenray
+    data_grid objects, 20 targets on the 100 km ring, 80 s; every eigenray
     equals the oracle's (per target, in order: travel time within 1 us, TL
     within 0.1 dB, angles within 0.01 deg, counts equal), and curr() reads
     the front back."""
@@ -114,7 +114,7 @@ def test_cpp_std14_gridded(tmp_path, engine):
     import numpy as np
     from oracle_binding import OracleQueue
     from underseamodelinglibrary_b200 import scenarios as S
-    sc = S.std14(num_targets=20, time_max=40.0)
+    sc = S.std14(num_targets=20, time_max=80.0)
     ocean = sc["ocean"]
     path = str(tmp_path / "std14.bin")
     with open(path, "wb") as fh:
@@ -140,7 +140,7 @@ def test_cpp_std14_gridded(tmp_path, engine):
     for r in o.take_eigenrays():
         want.setdefault(r.t1, []).append([r.travel_time, r.intensity[0], r.source_de, r.source_az,
                                           r.target_de, r.target_az, r.surface, r.bottom, r.caustic])
-    assert sum(len(v) for v in want.values()) > 20
+    assert sum(len(v) for v in want.values()) > 200
     assert set(got) == set(want)
     for t in want:
         assert len(got[t]) == len(want[t]), t

@@ -1540,7 +1540,7 @@ static int apply_listener_wants(wq3d_queue* q) {
     }
     if (want_verbs && !q->h.verb) {
         /* eigenverb buffers, made the first time a listener asks */
-        const int rc = q->ensure_verb_capacity((size_t)q->chunk * q->h.n * (q->h.oc.nvol + 1) / 32);
+        const int rc = q->ensure_verb_capacity((size_t)q->chunk * q->h.n * (q->h.oc.nvol + 1) / 2);
         if (rc) return rc;
     }
     if (want != q->h.want_refl || want_verbs != q->h.want_verbs) {
