@@ -41,6 +41,28 @@
 #include <string>
 #include <vector>
 
+#ifndef ORACLE_OPCOUNT
+/* the Rayleigh loss's complex arithmetic and the C-ABI arrays (plain
+ * double also in the op-counting build, opcount.cpp) */
+typedef double oracle_plain_double;
+#endif
+/* the op-counting build (opcount.cpp) attributes the operations of a
+ * scope to a phase of the step: 1 target distances, 2 CPA search, 3
+ * eigenray construction (everything else is 0, the ray step itself) */
+#ifdef ORACLE_OPCOUNT
+#define ORACLE_PHASE(p) wq3d_opcount::Phase oracle_phase_scope_(p)
+#else
+#define ORACLE_PHASE(p)
+#endif
+/* C-ABI double arrays seen as the oracle's scalar type and back (casts
+ * that change nothing except in the op-counting build) */
+template <class T>
+inline const double* abi_in(const T* p) { return reinterpret_cast<const double*>(p); }
+template <class T>
+inline oracle_plain_double* abi_out(T* p) { return reinterpret_cast<oracle_plain_double*>(p); }
+template <class T>
+inline const oracle_plain_double* abi_out(const T* p) { return reinterpret_cast<const oracle_plain_double*>(p); }
+
 namespace {
 
 const double PI = M_PI;
@@ -325,7 +347,7 @@ struct Ocean {
  * profile_n2.cc:14-24, with profile_model::adjust_speed (profile_model.cc:14-26) */
 void sound_speed(const Ocean& oc, double R, double rho, double theta,
                  double phi, double* c, double* g) {
-    const double* p = oc.prof.p;
+    const double* p = abi_in(oc.prof.p);
     const double alt = rho - R;
     double gr = 0.0, gt = 0.0, gp = 0.0;
     double cc = 0.0;
@@ -438,7 +460,7 @@ void reflect_loss(const Boundary& b, const std::vector<double>& freq,
     const size_t nf = freq.size();
     switch (b.loss.kind) {
         case WQ3D_LOSS_RAYLEIGH: {
-            typedef std::complex<double> cd;
+            typedef std::complex<oracle_plain_double> cd;
             const double dw = 1000.0, sw = 1500.0;
             if (angle >= M_PI_2) angle = M_PI_2 - 1e-10;
             angle = M_PI_2 - angle;
@@ -707,6 +729,7 @@ struct Queue {
 
     /* wave_front::compute_target_distance (wave_front.cc:222-236) */
     void compute_target_distance(Front& f) {
+        ORACLE_PHASE(1);
         for (size_t t = 0; t < nt; ++t) {
             const double R2 = tgt[0][t], TH = tgt[1][t], PH = tgt[2][t];
             const double S = tgt_sin[t];
@@ -1042,7 +1065,7 @@ struct Queue {
             if (d1 * d2 >= 0) continue;
             double c = curr->c[i];
             const double dd = c * c * curr->nd[0][i];
-            const double time_water = (dd == 0.0) ? 0.0 : -(curr->pos[0][i] - R) / dd;
+            const double time_water = (dd == 0.0) ? double(0.0) : -(curr->pos[0][i] - R) / dd;
             double position[3], ndir[3];
             collision_location(d, a, time_water, position, ndir, &c);
             const double grazing =
@@ -1108,7 +1131,7 @@ struct Queue {
         v.seq = seq;
         verbs.push_back(v);
         verb_power.insert(verb_power.end(), power.begin(), power.end());
-        if (cb.add_eigenverb) cb.add_eigenverb(cb_ctx, &v, power.data(), nf, type);
+        if (cb.add_eigenverb) cb.add_eigenverb(cb_ctx, &v, abi_out(power.data()), nf, type);
     }
 
     /* wave_queue.cc:261-269 */
@@ -1238,7 +1261,7 @@ struct Queue {
         double max_dot = -std::max(MIN_REFLECT, (height_water + depth) * nrm[0]);
         if (dot_full >= max_dot) dot_full = max_dot;
         const double dot_water = -height_water * nrm[0];
-        const double time_water = std::max(0.0, dot_water / dot_full);
+        const double time_water = std::max<double>(0.0, dot_water / dot_full);
 
         collision_location(d, a, time_water, position, ndir, &c);
         height(oc.bot, position[0], position[1], position[2], &bottom_rho, nrm);
@@ -1291,7 +1314,7 @@ struct Queue {
         const size_t i = idx(d, a);
         double c = curr->c[i];
         const double dd = c * c * curr->nd[0][i];
-        const double time_water = (dd == 0.0) ? 0.0 : -(curr->pos[0][i] - R) / dd;
+        const double time_water = (dd == 0.0) ? double(0.0) : -(curr->pos[0][i] - R) / dd;
         double position[3], ndir[3];
         collision_location(d, a, time_water, position, ndir, &c);
         const double grazing =
@@ -1375,6 +1398,7 @@ struct Queue {
     /* wave_queue.cc:351-404 */
     void detect_eigenrays() {
         if (!has_targets) return;
+        ORACLE_PHASE(2);
         double cube[3][3][3];
         const size_t az_start = az_boundary ? 0 : 1;
         for (size_t t1 = 0; t1 < nt1; ++t1) {
@@ -1547,12 +1571,12 @@ struct Queue {
         make_taylor_coeff(cube, delta, center, g, h);
         /* quirk kept: hessian(2,1)*hessian(2,0) (wave_queue.cc:762-763) */
         double determinant =
-            std::max(1e-6, h[0][0] * (h[1][1] * h[2][2] - h[1][2] * h[2][1]) +
+            std::max<double>(1e-6, h[0][0] * (h[1][1] * h[2][2] - h[1][2] * h[2][1]) +
                                h[0][1] * (h[1][2] * h[2][0] - h[1][0] * h[2][2]) +
                                h[0][2] * (h[1][0] * h[2][1] - h[2][1] * h[2][0]));
         unstable = unstable || determinant < norm2(g);
         for (int k = 0; k < 3; ++k) {
-            const double hh = std::max(1e-10, h[k][k]);
+            const double hh = std::max<double>(1e-10, h[k][k]);
             offset[k] = -g[k] / hh;
             if (std::abs(offset[k] / delta[k]) > 0.5) {
                 unstable = true;
@@ -1595,7 +1619,7 @@ struct Queue {
         }
         for (int k = 0; k < 3; ++k) {
             distance[k] = -g[k] * offset[k] - 0.5 * h[k][k] * offset[k] * offset[k];
-            distance[k] = std::sqrt(std::max(0.0, distance[k]));
+            distance[k] = std::sqrt(std::max<double>(0.0, distance[k]));
             if (offset[k] < 0.0) distance[k] *= -1.0;
         }
         if (unstable) {
@@ -1966,6 +1990,7 @@ struct Queue {
 
     /* wave_queue.cc:495-702 */
     void build_eigenray(size_t t1, size_t t2, size_t de0, size_t az0, double cube[3][3][3]) {
+        ORACLE_PHASE(3);
         const size_t ic = idx(de0, az0);
         const size_t t = t1 * nt2 + t2;
         if (above_bounce(curr, ic)) return;
@@ -2002,7 +2027,7 @@ struct Queue {
         for (size_t k = 0; k < nf; ++k)
             if (std::isnan(si[k])) return;
         e.inten.assign(nf, 0.0);
-        for (size_t k = 0; k < nf; ++k) e.inten[k] = -10.0 * std::log10(std::max(si[k], 1e-30));
+        for (size_t k = 0; k < nf; ++k) e.inten[k] = -10.0 * std::log10(std::max<double>(si[k], 1e-30));
         double ddt = offset[0] / dt;
         if (ddt >= 0.0) {
             for (size_t k = 0; k < nf; ++k)
@@ -2051,7 +2076,7 @@ struct Queue {
         for (const Eig& e : found) {
             if (e.rec.step != steps) continue;
             cb.add_eigenray(cb_ctx, (size_t)e.rec.t1, (size_t)e.rec.t2, &e.rec,
-                            e.inten.data(), e.phase.data(), nf, run_id);
+                            abi_out(e.inten.data()), abi_out(e.phase.data()), nf, run_id);
         }
     }
 };
@@ -2131,7 +2156,7 @@ int oracle_queue_get_front(void* qv, int which, const wq3d_front_view* v) {
                      : which == WQ3D_FRONT_CURR ? q->curr
                                                 : q->next;
     const size_t n = q->n, nf = q->nf;
-    auto cp = [n](double* dst, const std::vector<double>& src) {
+    auto cp = [n](oracle_plain_double* dst, const std::vector<double>& src) {
         if (dst) std::memcpy(dst, src.data(), n * sizeof(double));
     };
     auto cpi = [n](int32_t* dst, const std::vector<int>& src) {

@@ -48,16 +48,25 @@ SIGS = {
     "oracle_last_error_string": (C.c_char_p, []),
 }
 
-_lib = None
+ORACLE_OPCOUNT_LIB = os.path.join(ORACLE_DIR, "liboracle_opcount.so")
+_libs = {}
 
 
-def load_oracle():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(ORACLE_LIB):
-            subprocess.check_call(["make", "-s", "-C", ORACLE_DIR])
-        _lib = _abi.bind(C.CDLL(ORACLE_LIB), SIGS)
-    return _lib
+def load_oracle(opcount=False):
+    """the oracle library, or with opcount its operation-counting build
+    (oracle/opcount.cpp), which adds oracle_opcount_read / _reset"""
+    path = ORACLE_OPCOUNT_LIB if opcount else ORACLE_LIB
+    if path not in _libs:
+        if opcount or not os.path.exists(path):
+            subprocess.check_call(["make", "-s", "-C", ORACLE_DIR] + (["opcount"] if opcount else []))
+        lib = _abi.bind(C.CDLL(path), SIGS)
+        if opcount:
+            lib.oracle_opcount_read.restype = C.c_int
+            lib.oracle_opcount_read.argtypes = [C.POINTER(C.c_uint64)]
+            lib.oracle_opcount_reset.restype = C.c_int
+            lib.oracle_opcount_reset.argtypes = []
+        _libs[path] = lib
+    return _libs[path]
 
 
 def _check(rc):
@@ -67,8 +76,8 @@ def _check(rc):
 
 class OracleQueue:
     def __init__(self, ocean, freq, pos, de, az, time_step, target_pos=None,
-                 type=_abi.HYBRID_GAUSSIAN, reflections=False, eigenverbs=False):
-        lib = load_oracle()
+                 type=_abi.HYBRID_GAUSSIAN, reflections=False, eigenverbs=False, opcount=False):
+        lib = load_oracle(opcount)
         self._lib = lib
         self._freq, self._de, self._az = freq, de, az
         d, self._keep = make_queue_desc(freq, pos, de, az, time_step, target_pos, type)
