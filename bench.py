@@ -554,8 +554,10 @@ def gradient_arm():
     the forward pass recorded for the adjoint (checkpoints every 50 steps,
     each eigenray's partials, bottom sensitivities), then one reverse sweep
     for the weighted sum of every eigenray's TL and travel time.
-    value = sweep / recorded forward; vs_plain_forward = (sweep + recording
-    overhead) / the forward without recording."""
+    value = what the gradient adds to a plain forward pass (the recording's
+    overhead plus the sweep) / that forward pass; sweep_vs_plain_forward is
+    the sweep alone.  All three times are device time in the engine's
+    normal mode (chunk graphs, streams overlapped)."""
     from underseamodelinglibrary_b200 import adjoint as A
     import numpy as np
     sc = A.AdjointScenario()
@@ -574,10 +576,11 @@ def gradient_arm():
     w_tl, w_t = rng.normal(size=n), rng.normal(size=n)
     prop.vjp(w_tl, w_t)          # first sweep makes the workspace
     g, gb, ms_adj = prop.vjp(w_tl, w_t)
-    return {"metric": "adjoint:fwd", "value": ms_adj / prop.ms_forward, "unit": "ratio",
+    return {"metric": "adjoint:fwd", "value": (ms_adj + prop.ms_forward - ms_plain) / ms_plain, "unit": "ratio",
             "higher_is_better": False, "ms_forward_recorded": prop.ms_forward, "ms_forward_plain": ms_plain,
             "ms_adjoint": ms_adj,
-            "vs_plain_forward": (ms_adj + prop.ms_forward - ms_plain) / ms_plain,
+            "sweep_vs_plain_forward": ms_adj / ms_plain,
+            "recording_overhead_vs_plain_forward": (prop.ms_forward - ms_plain) / ms_plain,
             "eigenrays": n, "checkpoint_interval": 50,
             "gradient_norm": float(np.linalg.norm(g)),
             "method": "reverse sweep: checkpoints every 50 steps, recompute per interval, adjoint of AB3, "

@@ -4,18 +4,31 @@ restatement of the reference): the engine's reverse sweep for the
 sound-speed nodes, the exact bottom-parameter derivatives of the
 sensitivity mode, and the torch.autograd.Function wrapper.
 
-Tolerance: 1e-3 of the difference quotient, as the differentiation
-contract states, plus an absolute floor of 1e-6 dB or 1e-9 s per m/s for
-derivatives the difference step cannot resolve."""
+Difference steps.  A step of 1e-3 of a node's sound speed (1.5 m/s) is
+outside the linear range of many rays: near the sound-channel axis the
+difference quotient at that step is tens of percent away from its limit,
+and about a third of the eigenrays change their (step, target, D/E, AZ)
+bracket under it.  The oracle's differences are therefore taken at two
+steps, 1e-4 and 1e-5 of c_k; a (eigenray, node) pair is checked where both
+brackets hold and the two quotients agree within 2e-3 (the derivative is
+resolved), and there the adjoint must agree with one of them within 1e-3,
+the differentiation contract's tolerance, plus an absolute floor of 1e-6
+dB or 1e-9 s per m/s."""
+import os
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 import pytest
 
 from underseamodelinglibrary_b200 import adjoint as A
-from oracle_binding import OracleQueue
+from oracle_binding import OracleQueue, load_oracle
 
 pytestmark = pytest.mark.gpu
 
 REL = 1e-3
+AGREE = 2e-3
+H1, H2 = 1e-4, 1e-5
+FLOORS = (1e-6, 1e-9)
 
 
 def small():
@@ -38,16 +51,36 @@ def prop():
 
 @pytest.fixture(scope="module")
 def oracle_fd(prop):
-    """central differences of the oracle, step 1e-3 c_k, for every node"""
+    """the oracle's eigenrays with node k moved by +-h c_k, for both steps
+    (the runs go to a thread pool: the oracle's calls release the GIL)"""
     sc, nodes, _ = prop
-    out = []
-    for k in range(nodes.size):
-        h = 1e-3 * abs(nodes[k])
-        cp, cm = nodes.copy(), nodes.copy()
-        cp[k] += h
-        cm[k] -= h
-        out.append((h, oracle_rays(sc, cp), oracle_rays(sc, cm)))
-    return out
+    load_oracle()
+    jobs = [(k, hr, sgn) for k in range(nodes.size) for hr in (H1, H2) for sgn in (1, -1)]
+
+    def run(job):
+        k, hr, sgn = job
+        c = nodes.copy()
+        c[k] += sgn * hr * abs(nodes[k])
+        return job, oracle_rays(sc, c)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(32, os.cpu_count() or 1))) as ex:
+        return dict(ex.map(run, jobs))
+
+
+def differences(res, nodes, key, k, hr):
+    """(d TL, d T) / d c_k of one eigenray at step hr, or None when its
+    bracket does not hold under both moves"""
+    h = hr * abs(nodes[k])
+    p, m = res[(k, hr, 1)], res[(k, hr, -1)]
+    if key not in p or key not in m:
+        return None
+    return ((p[key].intensity[0] - m[key].intensity[0]) / (2 * h),
+            (p[key].travel_time - m[key].travel_time) / (2 * h))
+
+
+def resolved(a, b, j):
+    return a is not None and b is not None and \
+        abs(a[j] - b[j]) <= AGREE * max(abs(a[j]), abs(b[j])) + FLOORS[j]
 
 
 def test_bottom_derivatives_match_oracle_differences(prop):
@@ -77,48 +110,54 @@ def test_bottom_derivatives_match_oracle_differences(prop):
 
 def test_adjoint_rows_match_oracle_differences(prop, oracle_fd):
     """Jacobian rows from unit-weight reverse sweeps against the oracle's
-    central differences, node by node, on eigenrays whose (step, target,
-    D/E, AZ) bracket holds under both perturbations."""
+    central differences, node by node, wherever the differences resolve
+    the derivative"""
     sc, nodes, p = prop
     rays = p.eigenrays
     rng = np.random.default_rng(7)
-    idx = sorted(rng.choice(len(rays), size=min(12, len(rays)), replace=False))
+    idx = sorted(rng.choice(len(rays), size=min(16, len(rays)), replace=False))
     rows = p.rows(idx)
-    checked = 0
+    checked = total = 0
     for r_i, i in enumerate(idx):
         key = A._key(rays[i])
-        for k, (h, plus, minus) in enumerate(oracle_fd):
-            if key not in plus or key not in minus:
-                continue
-            fd_tl = (plus[key].intensity[0] - minus[key].intensity[0]) / (2 * h)
-            fd_t = (plus[key].travel_time - minus[key].travel_time) / (2 * h)
-            assert abs(rows[r_i, 0, k] - fd_tl) <= REL * abs(fd_tl) + 1e-6, (key, k, rows[r_i, 0, k], fd_tl)
-            assert abs(rows[r_i, 1, k] - fd_t) <= REL * abs(fd_t) + 1e-9, (key, k, rows[r_i, 1, k], fd_t)
-            checked += 1
-    assert checked > 100
+        for k in range(nodes.size):
+            a = differences(oracle_fd, nodes, key, k, H1)
+            b = differences(oracle_fd, nodes, key, k, H2)
+            for j in (0, 1):
+                total += 1
+                if not resolved(a, b, j):
+                    continue
+                g = rows[r_i, j, k]
+                err = min(abs(g - a[j]), abs(g - b[j]))
+                assert err <= REL * max(abs(a[j]), abs(b[j])) + FLOORS[j], (key, k, j, g, a[j], b[j])
+                checked += 1
+    assert checked >= 0.6 * total, (checked, total)
 
 
 def test_vjp_matches_weighted_oracle_differences(prop, oracle_fd):
-    """one reverse sweep with weights on every eigenray equals the same
-    weighted sum of the oracle's differences (eigenrays whose topology
-    changes under a perturbation carry no weight)"""
+    """one reverse sweep with weights on every eigenray whose derivatives
+    the differences resolve for all nodes equals the same weighted sum of
+    the oracle's differences (to 1e-3 of the sum of the terms' sizes)"""
     sc, nodes, p = prop
     rays = p.eigenrays
     keys = [A._key(r) for r in rays]
-    stable = np.array([all(k in plus and k in minus for _, plus, minus in oracle_fd) for k in keys])
-    assert stable.sum() > 0.5 * len(rays)
+    fd = [[(differences(oracle_fd, nodes, key, k, H1), differences(oracle_fd, nodes, key, k, H2))
+           for k in range(nodes.size)] for key in keys]
+    stable = np.array([all(resolved(a, b, j) for a, b in row for j in (0, 1)) for row in fd])
+    assert stable.sum() >= 0.2 * len(rays), (stable.sum(), len(rays))
     rng = np.random.default_rng(11)
     w_tl = rng.normal(size=len(rays)) * stable
     w_t = rng.normal(size=len(rays)) * stable * 1000.0
     g, gb, ms = p.vjp(w_tl, w_t)
     assert ms > 0.0
-    for k, (h, plus, minus) in enumerate(oracle_fd):
-        fd = 0.0
-        for i, key in enumerate(keys):
-            if stable[i]:
-                fd += w_tl[i] * (plus[key].intensity[0] - minus[key].intensity[0]) / (2 * h)
-                fd += w_t[i] * (plus[key].travel_time - minus[key].travel_time) / (2 * h)
-        assert abs(g[k] - fd) <= REL * abs(fd) + 1e-5, (k, g[k], fd)
+    for k in range(nodes.size):
+        s1 = s2 = scale = 0.0
+        for i in np.nonzero(stable)[0]:
+            a, b = fd[i][k]
+            s1 += w_tl[i] * a[0] + w_t[i] * a[1]
+            s2 += w_tl[i] * b[0] + w_t[i] * b[1]
+            scale += abs(w_tl[i] * a[0]) + abs(w_t[i] * a[1])
+        assert min(abs(g[k] - s1), abs(g[k] - s2)) <= REL * scale + 1e-5, (k, g[k], s1, s2, scale)
     assert np.allclose(gb, w_tl @ p.d_bottom, rtol=1e-12, atol=0)
 
 

@@ -133,7 +133,7 @@ def test_cpp_std14_gridded(tmp_path, engine):
     for line in out.stdout.splitlines():
         f = line.split()
         if f[0] == "ray":
-            got.setdefault(int(f[1]), []).append([float(x) for x in f[2:7]] + [int(x) for x in f[7:10]])
+            got.setdefault(int(f[1]), []).append([float(x) for x in f[2:8]] + [int(x) for x in f[8:11]])
     o = S.build_queue(sc, OracleQueue)
     o.run(sc["time_max"])
     want = {}

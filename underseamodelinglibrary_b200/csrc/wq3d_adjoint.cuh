@@ -1045,7 +1045,9 @@ struct Walker {
 
 /* S_s of every ray when s is a multiple of the checkpoint interval;
  * launched before k_advance of step s (k_reflect of that step only writes
- * shadow slots, so the fronts hold S_s) */
+ * shadow slots, so the fronts hold S_s, except the prev and curr states of
+ * rays that reflected at step s-1 while step s-1's commit is pending: those
+ * come from that step's slots) */
 __global__ void __launch_bounds__(128) k_adj_checkpoint(__grid_constant__ const QueueDev q, int k) {
     const int64_t s = *q.d_base + k;
     if (s % q.adj_K != 0) return;
@@ -1059,11 +1061,14 @@ __global__ void __launch_bounds__(128) k_adj_checkpoint(__grid_constant__ const 
     Roles R;
     roles_at(q, s, R);
     double* base = q.adj_ckpt + (size_t)slot * ADJ_S * q.n;
+    const double* sp = prev_step_slot(q, s, i);
     const FrontPtrs* F[3] = {R.V, R.C, R.X};
     for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c) {
-            base[(size_t)(r * 6 + c) * q.n + i] = F[r]->pos[c][i];
-            base[(size_t)(r * 6 + 3 + c) * q.n + i] = F[r]->nd[c][i];
+            /* slot layout: pos at +0, nd at +6 of each 17-double state */
+            const bool from_slot = sp && r < 2;
+            base[(size_t)(r * 6 + c) * q.n + i] = from_slot ? sp[17 * (r + 1) + c] : F[r]->pos[c][i];
+            base[(size_t)(r * 6 + 3 + c) * q.n + i] = from_slot ? sp[17 * (r + 1) + 6 + c] : F[r]->nd[c][i];
         }
 }
 

@@ -483,13 +483,21 @@ struct wq3d_queue {
         return WQ3D_OK;
     }
 
-    /* One chunk of K steps writing result set p.  Step k's reflections run
-     * on the side stream while step k-1's CPA search and eigenray
-     * construction run on the main stream (k_reflect only reads the fronts
-     * and writes shadow slots); k_advance(k) waits for both.  With "tail"
-     * the reflections of the next chunk's first step run beside this
-     * chunk's last CPA search; that chunk's own k_reflect(0) then finds an
-     * empty worklist and returns. */
+    /* One chunk of K steps writing result set p, on three streams:
+     *   main  k_advance(k), k_cpa(k); k_advance(k+1) waits for k_reflect(k+1)
+     *   side  k_reflect(k+1), right after k_advance(k), beside k_cpa(k)
+     *   eig   k_commit(k), k_eigenray(k) (after k_cpa(k)), and the adjoint's
+     *         eigenray partials
+     * Step k+1 reads the rays that reflected at step k from step k's shadow
+     * slots, so neither k_reflect(k+1) nor k_advance(k+1) waits for
+     * k_commit(k).  k_reflect(k+1) writes the slot set of step k-1 and so
+     * waits for k_commit(k-1); with eigenverbs it also waits for
+     * k_commit(k), since an eigenverb reads the curr front's losses and
+     * counts.  With "tail" the reflections of the next chunk's first step
+     * run beside this chunk's last CPA search; that chunk's own k_reflect(0)
+     * then finds an empty worklist and returns.  With per-kernel timing the
+     * steps run one launch after another, except k_reflect(k+1) beside
+     * k_cpa(k) and k_eigenray(k). */
     int launch_chunk(int K, int p, bool tail) {
         const QueueDev d = dev(p);
         const int n = h.n;
@@ -500,11 +508,6 @@ struct wq3d_queue {
          * fans, up to EIG_BLOCKS */
         const int eig_blocks = std::min(EIG_BLOCKS, std::max(148, (n + 255) / 256));
         if (timing) tail = false;
-        /* Without per-kernel timing, step k's commit and eigenray
-         * construction run on their own stream beside step k+1's advance and
-         * CPA search: step k+1's k_commit (which rewrites the fronts step k's
-         * eigenrays read) waits for them in stream order, and step k+2's
-         * reflections wait for that commit. */
         const bool ovl = !timing;
         if (timing) cudaEventRecord(events[7 * K], stream);
         k_reflect_fn<<<rgrid, 64, 0, stream>>>(d, 0);
@@ -535,7 +538,9 @@ struct wq3d_queue {
             const bool more = k + 1 < K || tail;
             if (more) {
                 if (ovl) {
-                    cudaStreamWaitEvent(side, com_ev[k], 0);
+                    cudaStreamWaitEvent(side, adv_ev[k], 0);
+                    if (k >= 1) cudaStreamWaitEvent(side, com_ev[k - 1], 0);
+                    if (h.want_verbs) cudaStreamWaitEvent(side, com_ev[k], 0);
                 } else {
                     cudaEventRecord(fork_ev[k], stream);
                     cudaStreamWaitEvent(side, fork_ev[k], 0);
@@ -1402,12 +1407,16 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.verb_threshold = 1e-30; /* wave_thresholds.h:40 */
     if (!reuse) {
         const size_t stride = 54 + 2 * nf;
-        if ((rc = q->alloc(&h.shadow, n * stride)) || (rc = q->alloc(&h.shadow_cnt, 3 * n)) ||
-            (rc = q->alloc(&h.shadow_slot, n)))
-            return cleanup(rc);
+        for (int p = 0; p < 2; ++p)
+            if ((rc = q->alloc(&h.shadow[p], n * stride)) || (rc = q->alloc(&h.shadow_cnt[p], 3 * n)) ||
+                (rc = q->alloc(&h.shadow_slot[p], n)) || (rc = q->alloc(&h.commit_flag[p], n)))
+                return cleanup(rc);
         if ((rc = q->alloc(&h.work[0], n)) || (rc = q->alloc(&h.work[1], n))) return cleanup(rc);
-        if ((rc = q->alloc(&h.commit_flag, n))) return cleanup(rc);
     }
+    /* no ray reflected in the step before the first */
+    for (int p = 0; p < 2; ++p)
+        if (cudaMemset(h.commit_flag[p], 0, n) != cudaSuccess)
+            return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
     h.d_base = q->d_base;
     h.d_times = q->d_times;
     h.want_refl = 0;
@@ -1442,7 +1451,11 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     if (!reuse) {
         if (cudaEventCreate(&q->ev_begin) != cudaSuccess || cudaEventCreate(&q->ev_end) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-        if (cudaStreamCreateWithFlags(&q->side, cudaStreamNonBlocking) != cudaSuccess ||
+        /* the reflections are the longest chain of a step (one thread per
+         * reflecting ray): their blocks go first when SMs free up */
+        int prio_low = 0, prio_high = 0;
+        if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) prio_high = 0;
+        if (cudaStreamCreateWithPriority(&q->side, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->eig, cudaStreamNonBlocking) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));

@@ -145,10 +145,12 @@ struct QueueDev {
     uint32_t* n_work[2];     /* surface part (front of the list)             */
     uint32_t* n_work_b[2];   /* bottom part (back of the list)               */
     uint32_t* n_done;        /* finished blocks of k_reflect              */
-    double* shadow;          /* reflected prev/curr/next per worklist slot  */
-    int32_t* shadow_cnt;     /* surface, bottom, caustic per slot           */
-    int32_t* shadow_slot;    /* worklist slot of each reflecting ray        */
-    uint8_t* commit_flag;    /* per ray: COMMIT_* bits k_advance leaves for k_commit */
+    /* reflections of step s, in set s & 1 (two sets, so that step s+1 can
+     * read step s's slots while k_commit of step s has not yet run) */
+    double* shadow[2];       /* reflected prev/curr/next per worklist slot  */
+    int32_t* shadow_cnt[2];  /* surface, bottom, caustic per slot           */
+    int32_t* shadow_slot[2]; /* worklist slot of each reflecting ray        */
+    uint8_t* commit_flag[2]; /* per ray: COMMIT_* bits k_advance leaves for k_commit */
     /* eigenray candidates: two lists by step parity (cand_list), so the
      * next step's advance and CPA search fill one while this step's
      * eigenray construction, on its own stream, reads the other */

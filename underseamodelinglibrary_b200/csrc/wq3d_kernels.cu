@@ -1,7 +1,7 @@
 /*
  * wq3d_kernels.cu -- FP64 WaveQ3D propagation kernels for sm_100a.
  *
- * One step of wave_queue::step() (waveq3d/wave_queue.cc:155-192) is four
+ * One step of wave_queue::step() (waveq3d/wave_queue.cc:155-192) is five
  * launches:
  *   k_reflect   one thread per ray on the worklist of rays that reflect in
  *               this step: caustic hand-off from the D/E neighbour and the
@@ -9,10 +9,13 @@
  *               re-initialisation, on a private copy of the ray written to
  *               its shadow slot.  It only reads the fronts, so it runs on a
  *               side stream beside the previous step's k_cpa / k_eigenray.
- *   k_advance   one thread per ray: commits shadow slots, caustic hand-off
- *               and vertices of the other rays, wave_front::find_edges,
- *               the queue rotation, the AB3 step and wave_front::update of
- *               the new front, and the next step's reflection worklist.
+ *   k_advance   one thread per ray: caustic hand-off and vertices,
+ *               wave_front::find_edges (reflecting rays read from their
+ *               shadow slots), the queue rotation, the AB3 step and
+ *               wave_front::update of the new front, and the next step's
+ *               reflection worklist.
+ *   k_commit    writes the reflected rays' slots and the caustic and vertex
+ *               counts into the fronts, on the eigenray stream.
  *   k_cpa       rays x targets: closest-point-of-approach test
  *               (detect_eigenrays + is_closest_ray) with distance2
  *               recomputed from per-front terms; k_cpa_f32 is its FP32
@@ -650,6 +653,42 @@ __device__ __forceinline__ void ray_from(const double* src, RayS& y) {
     y.dist = src[16];
 }
 
+/* A ray that reflected at step s-1 keeps its post-reflection states in
+ * that step's shadow slot until k_commit of step s-1, which runs on its
+ * own stream behind the eigenray construction of step s-2, has written
+ * them into the fronts.  At step s those are its prev state (the slot's
+ * curr, at +17) and its curr state (the slot's next, at +34), with the
+ * slot's counts.  Returns the slot, or null when the ray did not reflect
+ * at step s-1 and the fronts hold its states. */
+__device__ __forceinline__ const double* prev_step_slot(const QueueDev& q, int64_t s, int i,
+                                                        const int32_t** cnt = nullptr) {
+    const int p = (int)((s + 1) & 1); /* the set of step s-1 */
+    if (!(__ldg(q.commit_flag[p] + i) & COMMIT_REFLECT)) return nullptr;
+    const int32_t w = __ldg(q.shadow_slot[p] + i);
+    if (cnt) *cnt = q.shadow_cnt[p] + 3 * (size_t)w;
+    return q.shadow[p] + (size_t)w * shadow_stride(q);
+}
+
+/* the prev and curr states of ray i at step s (fronts V and C, or the
+ * previous step's shadow slot) */
+__device__ __forceinline__ void load_prev_curr(const QueueDev& q, int64_t s, const Roles& R, int i,
+                                               RayS& v, RayS& c) {
+    const double* sp = prev_step_slot(q, s, i);
+    if (sp) {
+        ray_from(sp + 17, v);
+        ray_from(sp + 34, c);
+    } else {
+        load_ray_ro(*R.V, i, v);
+        load_ray_ro(*R.C, i, c);
+    }
+}
+
+/* rho of ray j on the curr front at step s */
+__device__ __forceinline__ double curr_rho(const QueueDev& q, int64_t s, const Roles& R, int j) {
+    const double* sp = prev_step_slot(q, s, j);
+    return sp ? __ldg(sp + 34) : __ldg(R.C->pos[0] + j);
+}
+
 }  // namespace
 
 namespace WQ3D_KERNEL_NS {
@@ -737,6 +776,7 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
     roles_at(q, s, R);
     const uint8_t* flag_in = q.flag[s & 1];
     const size_t stride = shadow_stride(q);
+    const int set = (int)(s & 1);
     for (uint32_t ww = blockIdx.x * blockDim.x + threadIdx.x; ww < nwork; ww += gridDim.x * blockDim.x) {
         /* list slot: surface part at the front, bottom part at the back */
         const uint32_t w = ww < nsurf ? ww : (uint32_t)q.n - 1 - (ww - nsurf);
@@ -745,8 +785,7 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
         {
             /* the fronts are read-only here */
             RayS v, c, x;
-            load_ray_ro(*R.V, i, v);
-            load_ray_ro(*R.C, i, c);
+            load_prev_curr(q, s, R, i, v, c);
             load_ray_ro(*R.X, i, x);
             const int sf = __ldg(R.X->surface + i), bt = __ldg(R.X->bottom + i), cs = __ldg(R.X->caustic + i);
             L.v = v;
@@ -766,7 +805,7 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
         const int d = i / q.naz;
         if (d >= 1 && !flag_in[i - q.naz]) {
             const int j = i - q.naz;
-            const double A = L.c.pos[0], B = R.C->pos[0][j];
+            const double A = L.c.pos[0], B = curr_rho(q, s, R, j);
             const double Cc = L.x.pos[0], D = R.X->pos[0][j];
             const bool fold = (L.surface == R.X->surface[j]) && (L.bottom == R.X->bottom[j]);
             if ((Cc - D) * (A - B) < 0 && fold) {
@@ -815,7 +854,7 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
             }
             if (it == MAX_BOUNCE) set_err(q, ERR_BOUNCE_LIMIT);
         }
-        double* sh = q.shadow + (size_t)w * stride;
+        double* sh = q.shadow[set] + (size_t)w * stride;
         ray_to(sh, L.v);
         ray_to(sh + 17, L.c);
         ray_to(sh + 34, L.x);
@@ -828,10 +867,10 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
          * construction may still be reading them */
         if (q.sens)
             for (int j = 0; j < 3; ++j) sh[51 + 2 * q.nf + j] = dl[j];
-        q.shadow_cnt[3 * (size_t)w] = L.surface;
-        q.shadow_cnt[3 * (size_t)w + 1] = L.bottom;
-        q.shadow_cnt[3 * (size_t)w + 2] = L.caustic;
-        q.shadow_slot[i] = (int32_t)w;
+        q.shadow_cnt[set][3 * (size_t)w] = L.surface;
+        q.shadow_cnt[set][3 * (size_t)w + 1] = L.bottom;
+        q.shadow_cnt[set][3 * (size_t)w + 2] = L.caustic;
+        q.shadow_slot[set][i] = (int32_t)w;
     }
     /* the last block to finish empties this step's worklist, which the
      * advance of step s+1 refills (every block has read the count by then;
@@ -884,8 +923,8 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
      * the rows d-2 .. d+2 that detect_caustics and find_edges may read
      * (rows clamped to the fan; a clamped row is never used) */
     const bool refl = __ldg(flag_in + i) != 0;
-    load_ray_ro(*R.V, i, y0);
-    load_ray_ro(*R.C, i, y1);
+    const int set = (int)(s & 1);
+    if (!refl) load_prev_curr(q, s, R, i, y0, y1);
     load_ray_ro(*R.X, i, y2);
     int32_t sf = __ldg(R.X->surface + i);
     int32_t bt = __ldg(R.X->bottom + i);
@@ -905,7 +944,7 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
         rr[t] = __ldg(R.X->pos[0] + jrow[t]);
         nn[t] = __ldg(R.X->nd[0] + jrow[t]);
     }
-    const double c_below = __ldg(R.C->pos[0] + jrow[1]);
+    const double c_below = curr_rho(q, s, R, jrow[1]);
     const int32_t sf_below = __ldg(R.X->surface + jrow[1]);
     const int32_t bt_below = __ldg(R.X->bottom + jrow[1]);
     const double x_below = rr[1];
@@ -913,7 +952,7 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
         if (fl[t]) {
-            const double* shj = q.shadow + (size_t)__ldg(q.shadow_slot + jrow[t]) * stride;
+            const double* shj = q.shadow[set] + (size_t)__ldg(q.shadow_slot[set] + jrow[t]) * stride;
             rr[t] = __ldg(shj + 34);
             nn[t] = __ldg(shj + 34 + 6);
         }
@@ -921,18 +960,17 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     const double* sh = nullptr;
     bool fold_hit = false, vtx_up = false, vtx_lo = false;
     if (refl) {
-        /* commit the reflected ray (reflection_copy into prev, curr, next) */
         /* the reflected ray's states come from its shadow slot; k_commit
-         * writes them into the prev, curr and next fronts once the previous
+         * writes them into the curr and next fronts once the previous
          * step's eigenray construction no longer reads those fronts */
-        const int32_t w = __ldg(q.shadow_slot + i);
-        sh = q.shadow + (size_t)w * stride;
+        const int32_t w = __ldg(q.shadow_slot[set] + i);
+        sh = q.shadow[set] + (size_t)w * stride;
         ray_from(sh, y0);
         ray_from(sh + 17, y1);
         ray_from(sh + 34, y2);
-        sf = __ldg(q.shadow_cnt + 3 * (size_t)w);
-        bt = __ldg(q.shadow_cnt + 3 * (size_t)w + 1);
-        cs = __ldg(q.shadow_cnt + 3 * (size_t)w + 2);
+        sf = __ldg(q.shadow_cnt[set] + 3 * (size_t)w);
+        bt = __ldg(q.shadow_cnt[set] + 3 * (size_t)w + 1);
+        cs = __ldg(q.shadow_cnt[set] + 3 * (size_t)w + 2);
     } else {
         /* detect_caustics of the neighbour below (wave_queue.cc:274-292) */
         if (d >= 1 && !fl[1]) {
@@ -990,7 +1028,7 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     /* stores: the new front, the next front's edge flag (not read by the
      * previous step's eigenray construction) and what k_commit changes on
      * the prev / curr / next fronts */
-    q.commit_flag[i] = (uint8_t)((refl ? COMMIT_REFLECT : 0) | (fold_hit ? COMMIT_FOLD : 0) |
+    q.commit_flag[set][i] = (uint8_t)((refl ? COMMIT_REFLECT : 0) | (fold_hit ? COMMIT_FOLD : 0) |
                                  (vtx_up ? COMMIT_UPPER : 0) | (vtx_lo ? COMMIT_LOWER : 0));
     R.X->on_edge[i] = edge ? 1 : 0;
     const FrontPtrs& P = *R.P;
@@ -1044,34 +1082,40 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
 }  // namespace WQ3D_KERNEL_NS
 
 #if !WQ3D_STEP_KERNELS_ONLY
-/* What k_advance of step s decided for the prev / curr / next fronts, done
- * after the eigenray construction of step s-1 has read them: a reflected
- * ray's three states, counts and next-front losses from its shadow slot
+/* What k_advance of step s decided for the curr / next fronts, done after
+ * the eigenray construction of step s-1 has read them: a reflected ray's
+ * states, counts and next-front losses from its shadow slot
  * (reflection_model::reflection_copy, reflection_model.cc:335-360), and for
  * the other rays the caustic hand-off (count, and phase - pi/2 on every
- * frequency, wave_queue.cc:274-292) and the vertex counts (:261-269). */
+ * frequency, wave_queue.cc:274-292) and the vertex counts (:261-269).
+ * Until it has run, step s+1 reads a reflected ray's states from the slot
+ * (prev_step_slot); the eigenray construction of step s, the eigenverbs of
+ * step s+1 and the commit of step s+2 (which reuses this step's slot set)
+ * wait for it. */
 __global__ void __launch_bounds__(128) k_commit(__grid_constant__ const QueueDev q, int k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= q.n) return;
-    const uint8_t b = q.commit_flag[i];
-    if (!b) return;
     const int64_t s = *q.d_base + k;
+    const int set = (int)(s & 1);
+    const uint8_t b = q.commit_flag[set][i];
+    if (!b) return;
     Roles R;
     roles_at(q, s, R);
     if (b & COMMIT_REFLECT) {
-        const int32_t w = q.shadow_slot[i];
-        const double* sh = q.shadow + (size_t)w * shadow_stride(q);
+        /* the reflected prev state is only used by this step's AB3, which
+         * took it from the slot; the prev front becomes this step's new
+         * front */
+        const int32_t w = q.shadow_slot[set][i];
+        const double* sh = q.shadow[set] + (size_t)w * shadow_stride(q);
+        const int32_t* cnt = q.shadow_cnt[set] + 3 * (size_t)w;
         RayS y;
-        ray_from(sh, y);
-        copy_ray(*R.V, i, y);
         ray_from(sh + 17, y);
         copy_ray(*R.C, i, y);
         ray_from(sh + 34, y);
         copy_ray(*R.X, i, y);
-        const int32_t sf = q.shadow_cnt[3 * (size_t)w], bt = q.shadow_cnt[3 * (size_t)w + 1];
-        R.V->surface[i] = R.C->surface[i] = R.X->surface[i] = sf;
-        R.V->bottom[i] = R.C->bottom[i] = R.X->bottom[i] = bt;
-        R.X->caustic[i] = q.shadow_cnt[3 * (size_t)w + 2];
+        R.C->surface[i] = R.X->surface[i] = cnt[0];
+        R.C->bottom[i] = R.X->bottom[i] = cnt[1];
+        R.X->caustic[i] = cnt[2];
         for (int f = 0; f < q.nf; ++f) {
             R.X->atten[(size_t)f * q.n + i] = sh[51 + f];
             R.X->phase[(size_t)f * q.n + i] = sh[51 + q.nf + f];
