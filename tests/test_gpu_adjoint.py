@@ -8,12 +8,13 @@ Difference steps.  A step of 1e-3 of a node's sound speed (1.5 m/s) is
 outside the linear range of many rays: near the sound-channel axis the
 difference quotient at that step is tens of percent away from its limit,
 and about a third of the eigenrays change their (step, target, D/E, AZ)
-bracket under it.  The oracle's differences are therefore taken at two
-steps, 1e-4 and 1e-5 of c_k; a (eigenray, node) pair is checked where both
-brackets hold and the two quotients agree within 2e-3 (the derivative is
-resolved), and there the adjoint must agree with one of them within 1e-3,
-the differentiation contract's tolerance, plus an absolute floor of 1e-6
-dB or 1e-9 s per m/s."""
+bracket under it.  The oracle's differences are therefore taken at 1e-4
+and 5e-5 of c_k and extrapolated (Richardson: (4 D(h/2) - D(h)) / 3).  An
+(eigenray, node) pair is checked where its bracket holds at both steps and
+the two quotients agree within 2e-3 (the step resolves the derivative);
+there the adjoint must agree with the extrapolation within 1e-3, the
+differentiation contract's tolerance, plus an absolute floor of 1e-6 dB
+or 1e-9 s per m/s."""
 import os
 from concurrent.futures import ThreadPoolExecutor
 
@@ -27,7 +28,7 @@ pytestmark = pytest.mark.gpu
 
 REL = 1e-3
 AGREE = 2e-3
-H1, H2 = 1e-4, 1e-5
+H1, H2 = 1e-4, 5e-5
 FLOORS = (1e-6, 1e-9)
 
 
@@ -83,6 +84,11 @@ def resolved(a, b, j):
         abs(a[j] - b[j]) <= AGREE * max(abs(a[j]), abs(b[j])) + FLOORS[j]
 
 
+def extrapolated(a, b):
+    """Richardson's extrapolation of central differences at h and h/2"""
+    return (4.0 * b - a) / 3.0
+
+
 def test_bottom_derivatives_match_oracle_differences(prop):
     sc, nodes, p = prop
     rays = p.eigenrays
@@ -110,8 +116,8 @@ def test_bottom_derivatives_match_oracle_differences(prop):
 
 def test_adjoint_rows_match_oracle_differences(prop, oracle_fd):
     """Jacobian rows from unit-weight reverse sweeps against the oracle's
-    central differences, node by node, wherever the differences resolve
-    the derivative"""
+    extrapolated central differences, node by node, wherever the steps
+    resolve the derivative"""
     sc, nodes, p = prop
     rays = p.eigenrays
     rng = np.random.default_rng(7)
@@ -127,29 +133,31 @@ def test_adjoint_rows_match_oracle_differences(prop, oracle_fd):
                 total += 1
                 if not resolved(a, b, j):
                     continue
+                want = extrapolated(a[j], b[j])
                 g = rows[r_i, j, k]
-                err = min(abs(g - a[j]), abs(g - b[j]))
-                assert err <= REL * max(abs(a[j]), abs(b[j])) + FLOORS[j], (key, k, j, g, a[j], b[j])
+                assert abs(g - want) <= REL * abs(want) + FLOORS[j], (key, k, j, g, want, a[j], b[j])
                 checked += 1
     assert checked >= 0.6 * total, (checked, total)
 
 
 def test_vjp_matches_weighted_oracle_differences(prop, oracle_fd):
-    """one reverse sweep with weights on every eigenray whose derivatives
-    the differences resolve for all nodes equals the same weighted sum of
-    the oracle's differences (to 1e-3 of the sum of the terms' sizes)"""
+    """one reverse sweep with random weights on every eigenray whose
+    bracket holds under all the moves equals the difference quotient of the
+    same weighted sum (extrapolated), node by node, wherever the steps
+    resolve it (to 1e-3 of the sum of the terms' sizes)"""
     sc, nodes, p = prop
     rays = p.eigenrays
     keys = [A._key(r) for r in rays]
     fd = [[(differences(oracle_fd, nodes, key, k, H1), differences(oracle_fd, nodes, key, k, H2))
            for k in range(nodes.size)] for key in keys]
-    stable = np.array([all(resolved(a, b, j) for a, b in row for j in (0, 1)) for row in fd])
-    assert stable.sum() >= 0.2 * len(rays), (stable.sum(), len(rays))
+    stable = np.array([all(a is not None and b is not None for a, b in row) for row in fd])
+    assert stable.sum() >= 0.5 * len(rays), (stable.sum(), len(rays))
     rng = np.random.default_rng(11)
     w_tl = rng.normal(size=len(rays)) * stable
     w_t = rng.normal(size=len(rays)) * stable * 1000.0
     g, gb, ms = p.vjp(w_tl, w_t)
     assert ms > 0.0
+    checked = 0
     for k in range(nodes.size):
         s1 = s2 = scale = 0.0
         for i in np.nonzero(stable)[0]:
@@ -157,7 +165,12 @@ def test_vjp_matches_weighted_oracle_differences(prop, oracle_fd):
             s1 += w_tl[i] * a[0] + w_t[i] * a[1]
             s2 += w_tl[i] * b[0] + w_t[i] * b[1]
             scale += abs(w_tl[i] * a[0]) + abs(w_t[i] * a[1])
-        assert min(abs(g[k] - s1), abs(g[k] - s2)) <= REL * scale + 1e-5, (k, g[k], s1, s2, scale)
+        if abs(s1 - s2) > AGREE * scale + 1e-5:
+            continue
+        want = extrapolated(s1, s2)
+        assert abs(g[k] - want) <= REL * scale + 1e-5, (k, g[k], want, s1, s2, scale)
+        checked += 1
+    assert checked >= 0.5 * nodes.size, checked
     assert np.allclose(gb, w_tl @ p.d_bottom, rtol=1e-12, atol=0)
 
 

@@ -220,7 +220,7 @@ struct wq3d_queue {
     cudaStream_t side = nullptr;
     cudaStream_t eig = nullptr; /* k_commit and the eigenray construction */
     std::vector<cudaEvent_t> fork_ev, join_ev;
-    std::vector<cudaEvent_t> adv_ev, com_ev, cpa_ev; /* per step of a chunk */
+    std::vector<cudaEvent_t> adv_ev, com_ev, cpa_ev, eig_ev; /* per step of a chunk */
     cudaEvent_t eig_end = nullptr;
     QueueDev h{};
     std::vector<void*> allocs;
@@ -448,7 +448,7 @@ struct wq3d_queue {
             if (e) cudaEventDestroy(e);
         for (auto e : fork_ev) cudaEventDestroy(e);
         for (auto e : join_ev) cudaEventDestroy(e);
-        for (auto* v : {&adv_ev, &com_ev, &cpa_ev})
+        for (auto* v : {&adv_ev, &com_ev, &cpa_ev, &eig_ev})
             for (auto e : *v) cudaEventDestroy(e);
         if (eig_end) cudaEventDestroy(eig_end);
         if (eig) cudaStreamDestroy(eig);
@@ -490,9 +490,11 @@ struct wq3d_queue {
      *         eigenray partials
      * Step k+1 reads the rays that reflected at step k from step k's shadow
      * slots, so neither k_reflect(k+1) nor k_advance(k+1) waits for
-     * k_commit(k).  k_reflect(k+1) writes the slot set of step k-1 and so
-     * waits for k_commit(k-1); with eigenverbs it also waits for
-     * k_commit(k), since an eigenverb reads the curr front's losses and
+     * k_commit(k).  k_reflect(k+1) writes the slot set of step k-1, and
+     * k_advance(k+1) clears the candidate list of step k-1, so k_reflect(k+1)
+     * waits for step k-1's work on the eigenray stream (its commit,
+     * eigenray construction and partials); with eigenverbs it also waits
+     * for k_commit(k), since an eigenverb reads the curr front's losses and
      * counts.  With "tail" the reflections of the next chunk's first step
      * run beside this chunk's last CPA search; that chunk's own k_reflect(0)
      * then finds an empty worklist and returns.  With per-kernel timing the
@@ -539,7 +541,7 @@ struct wq3d_queue {
             if (more) {
                 if (ovl) {
                     cudaStreamWaitEvent(side, adv_ev[k], 0);
-                    if (k >= 1) cudaStreamWaitEvent(side, com_ev[k - 1], 0);
+                    if (k >= 1) cudaStreamWaitEvent(side, eig_ev[k - 1], 0);
                     if (h.want_verbs) cudaStreamWaitEvent(side, com_ev[k], 0);
                 } else {
                     cudaEventRecord(fork_ev[k], stream);
@@ -578,6 +580,8 @@ struct wq3d_queue {
             } else if (ev) {
                 cudaEventRecord(ev[3], stream);
             }
+            /* the end of step k's work on the eigenray stream */
+            if (ovl) cudaEventRecord(eig_ev[k], eig);
             if (ev) cudaEventRecord(ev[4], stream);
             if (more) cudaStreamWaitEvent(stream, join_ev[k], 0);
         }
@@ -1464,7 +1468,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         for (auto& e : q->done_ev)
             if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
                 return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-        for (auto* v : {&q->fork_ev, &q->join_ev, &q->adv_ev, &q->com_ev, &q->cpa_ev}) {
+        for (auto* v : {&q->fork_ev, &q->join_ev, &q->adv_ev, &q->com_ev, &q->cpa_ev, &q->eig_ev}) {
             v->resize(q->chunk);
             for (int k = 0; k < q->chunk; ++k)
                 if (cudaEventCreateWithFlags(&(*v)[k], cudaEventDisableTiming) != cudaSuccess)
