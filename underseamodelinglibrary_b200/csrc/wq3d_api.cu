@@ -219,6 +219,8 @@ struct wq3d_queue {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;
     cudaStream_t eig = nullptr; /* k_commit and the eigenray construction */
+    cudaStream_t adv = nullptr; /* k_advance, checkpoints, volume eigenverbs */
+    cudaEvent_t start_ev = nullptr;
     std::vector<cudaEvent_t> fork_ev, join_ev;
     std::vector<cudaEvent_t> adv_ev, com_ev, cpa_ev, eig_ev; /* per step of a chunk */
     cudaEvent_t eig_end = nullptr;
@@ -239,6 +241,7 @@ struct wq3d_queue {
     /* [result set][prefetches the next chunk's first reflection] */
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     bool graph_failed[2][2] = {{false, false}, {false, false}};
+    int64_t graph_launches[2][2] = {{0, 0}, {0, 0}}; /* kernels in each graph */
     /* Result set 1: a second copy of the record buffers, so that chunk c
      * writes set c & 1 while the host reads the other chunk's records
      * (made by the first run of more than one chunk; set 0 lives in h). */
@@ -278,7 +281,7 @@ struct wq3d_queue {
     /* the stepping kernels' build: "gridded" when the ocean has a grid */
     bool gridded = false;
     void (*k_reflect_fn)(const QueueDev, int) = analytic::k_reflect;
-    void (*k_advance_fn)(const QueueDev, int) = analytic::k_advance;
+    void (*k_advance_fn)(const QueueDev, int, int) = analytic::k_advance;
     /* eigenverb counting sink (wq3d_queue_count_eigenverbs) */
     bool count_verbs = false;
     uint64_t verb_counts[2 + 2 * WQ3D_MAX_VOLUME] = {0};
@@ -451,6 +454,8 @@ struct wq3d_queue {
         for (auto* v : {&adv_ev, &com_ev, &cpa_ev, &eig_ev})
             for (auto e : *v) cudaEventDestroy(e);
         if (eig_end) cudaEventDestroy(eig_end);
+        if (start_ev) cudaEventDestroy(start_ev);
+        if (adv) cudaStreamDestroy(adv);
         if (eig) cudaStreamDestroy(eig);
         if (side) cudaStreamDestroy(side);
         if (ev_begin) cudaEventDestroy(ev_begin);
@@ -483,23 +488,30 @@ struct wq3d_queue {
         return WQ3D_OK;
     }
 
-    /* One chunk of K steps writing result set p, on three streams:
-     *   main  k_advance(k), k_cpa(k); k_advance(k+1) waits for k_reflect(k+1)
-     *   side  k_reflect(k+1), right after k_advance(k), beside k_cpa(k)
-     *   eig   k_commit(k), k_eigenray(k) (after k_cpa(k)), and the adjoint's
-     *         eigenray partials
+    /* One chunk of K steps writing result set p.  Without per-kernel
+     * timing it runs on four streams:
+     *   adv   k_advance(k+1) in two launches: the rays whose step needs no
+     *         reflection of step k+1 (ADVANCE_FREE) right after step k's
+     *         advance, beside k_reflect(k+1) and k_cpa(k); the others
+     *         (ADVANCE_BOUND) once k_reflect(k+1) is done.  The adjoint's
+     *         checkpoint and the volume eigenverbs of a step run here
+     *         before its advance.
+     *   side  k_reflect(k+1) (high priority), after step k's advance
+     *   main  k_cpa(k), after step k's advance
+     *   eig   k_commit(k) after step k's advance, k_eigenray(k) after
+     *         k_cpa(k), and the adjoint's eigenray partials
      * Step k+1 reads the rays that reflected at step k from step k's shadow
-     * slots, so neither k_reflect(k+1) nor k_advance(k+1) waits for
-     * k_commit(k).  k_reflect(k+1) writes the slot set of step k-1, and
-     * k_advance(k+1) clears the candidate list of step k-1, so k_reflect(k+1)
-     * waits for step k-1's work on the eigenray stream (its commit,
-     * eigenray construction and partials); with eigenverbs it also waits
-     * for k_commit(k), since an eigenverb reads the curr front's losses and
-     * counts.  With "tail" the reflections of the next chunk's first step
-     * run beside this chunk's last CPA search; that chunk's own k_reflect(0)
-     * then finds an empty worklist and returns.  With per-kernel timing the
-     * steps run one launch after another, except k_reflect(k+1) beside
-     * k_cpa(k) and k_eigenray(k). */
+     * slots, so nothing on the adv or side stream waits for k_commit(k)
+     * (except with eigenverbs: an eigenverb reads the curr front's losses
+     * and counts).  Step k+1's advance overwrites the front, commit flags
+     * and candidate list that step k-1 used, and k_reflect(k+1) its slot
+     * set, so both wait for step k-1's eigenray-stream work.  The first
+     * step of a chunk advances every ray in one launch.  With "tail" the
+     * reflections of the next chunk's first step run beside this chunk's
+     * last CPA search; that chunk's own k_reflect(0) then finds an empty
+     * worklist and returns.
+     * With per-kernel timing the steps run one launch after another on the
+     * main stream, except k_reflect(k+1) beside k_cpa(k) and k_eigenray(k). */
     int launch_chunk(int K, int p, bool tail) {
         const QueueDev d = dev(p);
         const int n = h.n;
@@ -510,85 +522,125 @@ struct wq3d_queue {
          * fans, up to EIG_BLOCKS */
         const int eig_blocks = std::min(EIG_BLOCKS, std::max(148, (n + 255) / 256));
         if (timing) tail = false;
-        const bool ovl = !timing;
+        auto cpa_launch = [&](int k, cudaStream_t st) {
+            if (h.precision == WQ3D_FP32C)
+                k_cpa_f32<<<dim3(((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) *
+                                     ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
+                                 (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS),
+                            CPA_THREADS, 0, st>>>(d, k);
+            else
+                k_cpa<<<dim3((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS),
+                        CPA_THREADS, 0, st>>>(d, k);
+        };
+        auto eig_launch = [&](int k, cudaStream_t st) {
+            k_eigenray<<<eig_blocks, 128, 0, st>>>(d, k);
+            launches += 1;
+            if (h.adj) {
+                k_eigenray_jac<<<4 * 148, 64, 0, st>>>(d, k);
+                k_adj_mark<<<1, 1, 0, st>>>(d);
+                launches += 2;
+            }
+        };
         if (timing) cudaEventRecord(events[7 * K], stream);
         k_reflect_fn<<<rgrid, 64, 0, stream>>>(d, 0);
         if (timing) cudaEventRecord(events[7 * K + 1], stream);
         launches += 1;
+        if (timing) {
+            for (int k = 0; k < K; ++k) {
+                cudaEvent_t* ev = &events[7 * k];
+                cudaEventRecord(ev[0], stream);
+                if (h.adj) {
+                    k_adj_checkpoint<<<grd, blk, 0, stream>>>(d, k);
+                    launches += 1;
+                }
+                if (volume_pass()) {
+                    k_volume<<<grd, blk, 0, stream>>>(d, k);
+                    launches += 1;
+                }
+                k_advance_fn<<<grd, blk, 0, stream>>>(d, k, ADVANCE_ALL);
+                k_commit<<<grd, blk, 0, stream>>>(d, k);
+                launches += 2;
+                cudaEventRecord(ev[1], stream);
+                if (k + 1 < K) {
+                    cudaEventRecord(fork_ev[k], stream);
+                    cudaStreamWaitEvent(side, fork_ev[k], 0);
+                    cudaEventRecord(ev[5], side);
+                    k_reflect_fn<<<rgrid, 64, 0, side>>>(d, k + 1);
+                    cudaEventRecord(ev[6], side);
+                    cudaEventRecord(join_ev[k], side);
+                    launches += 1;
+                }
+                cudaEventRecord(ev[2], stream);
+                if (h.nt > 0) {
+                    cpa_launch(k, stream);
+                    launches += 1;
+                    cudaEventRecord(ev[3], stream);
+                    eig_launch(k, stream);
+                } else {
+                    cudaEventRecord(ev[3], stream);
+                }
+                cudaEventRecord(ev[4], stream);
+                if (k + 1 < K) cudaStreamWaitEvent(stream, join_ev[k], 0);
+            }
+            return WQ3D_OK;
+        }
+        cudaEventRecord(start_ev, stream);
+        cudaStreamWaitEvent(adv, start_ev, 0);
         for (int k = 0; k < K; ++k) {
-            cudaEvent_t* ev = timing ? &events[7 * k] : nullptr;
-            if (ev) cudaEventRecord(ev[0], stream);
+            /* adv: step k's checkpoint, volume eigenverbs and advance */
             if (h.adj) {
-                k_adj_checkpoint<<<grd, blk, 0, stream>>>(d, k);
+                k_adj_checkpoint<<<grd, blk, 0, adv>>>(d, k);
                 launches += 1;
             }
             if (volume_pass()) {
-                k_volume<<<grd, blk, 0, stream>>>(d, k);
+                if (k >= 1) cudaStreamWaitEvent(adv, com_ev[k - 1], 0);
+                k_volume<<<grd, blk, 0, adv>>>(d, k);
                 launches += 1;
             }
-            k_advance_fn<<<grd, blk, 0, stream>>>(d, k);
-            launches += 2;
-            if (ovl) {
-                cudaEventRecord(adv_ev[k], stream);
-                cudaStreamWaitEvent(eig, adv_ev[k], 0);
-                k_commit<<<grd, blk, 0, eig>>>(d, k);
-                cudaEventRecord(com_ev[k], eig);
+            if (k == 0) {
+                k_advance_fn<<<grd, blk, 0, adv>>>(d, 0, ADVANCE_ALL);
             } else {
-                k_commit<<<grd, blk, 0, stream>>>(d, k);
+                cudaStreamWaitEvent(adv, join_ev[k - 1], 0);
+                k_advance_fn<<<grd, blk, 0, adv>>>(d, k, ADVANCE_BOUND);
             }
-            if (ev) cudaEventRecord(ev[1], stream);
+            launches += 1;
+            cudaEventRecord(adv_ev[k], adv);
+            /* eig: step k's commit */
+            cudaStreamWaitEvent(eig, adv_ev[k], 0);
+            k_commit<<<grd, blk, 0, eig>>>(d, k);
+            launches += 1;
+            cudaEventRecord(com_ev[k], eig);
             const bool more = k + 1 < K || tail;
             if (more) {
-                if (ovl) {
-                    cudaStreamWaitEvent(side, adv_ev[k], 0);
-                    if (k >= 1) cudaStreamWaitEvent(side, eig_ev[k - 1], 0);
-                    if (h.want_verbs) cudaStreamWaitEvent(side, com_ev[k], 0);
-                } else {
-                    cudaEventRecord(fork_ev[k], stream);
-                    cudaStreamWaitEvent(side, fork_ev[k], 0);
-                }
-                if (ev) cudaEventRecord(ev[5], side);
+                /* side: step k+1's reflections */
+                cudaStreamWaitEvent(side, adv_ev[k], 0);
+                if (k >= 1) cudaStreamWaitEvent(side, eig_ev[k - 1], 0);
+                if (h.want_verbs) cudaStreamWaitEvent(side, com_ev[k], 0);
                 k_reflect_fn<<<rgrid, 64, 0, side>>>(d, k + 1);
-                if (ev) cudaEventRecord(ev[6], side);
                 cudaEventRecord(join_ev[k], side);
                 launches += 1;
             }
-            if (ev) cudaEventRecord(ev[2], stream);
-            if (h.nt > 0) {
-                const dim3 cg((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS);
-                if (h.precision == WQ3D_FP32C)
-                    k_cpa_f32<<<dim3(((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) *
-                                         ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
-                                     (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS),
-                                CPA_THREADS, 0, stream>>>(d, k);
-                else
-                    k_cpa<<<cg, CPA_THREADS, 0, stream>>>(d, k);
-                if (ev) cudaEventRecord(ev[3], stream);
-                cudaStream_t es = stream;
-                if (ovl) {
-                    cudaEventRecord(cpa_ev[k], stream);
-                    cudaStreamWaitEvent(eig, cpa_ev[k], 0);
-                    es = eig;
-                }
-                k_eigenray<<<eig_blocks, 128, 0, es>>>(d, k);
-                launches += 2;
-                if (h.adj) {
-                    k_eigenray_jac<<<4 * 148, 64, 0, es>>>(d, k);
-                    k_adj_mark<<<1, 1, 0, es>>>(d);
-                    launches += 2;
-                }
-            } else if (ev) {
-                cudaEventRecord(ev[3], stream);
+            if (k + 1 < K) {
+                /* adv: the rays of step k+1 that need none of its reflections */
+                if (k >= 1) cudaStreamWaitEvent(adv, eig_ev[k - 1], 0);
+                k_advance_fn<<<grd, blk, 0, adv>>>(d, k + 1, ADVANCE_FREE);
+                launches += 1;
             }
-            /* the end of step k's work on the eigenray stream */
-            if (ovl) cudaEventRecord(eig_ev[k], eig);
-            if (ev) cudaEventRecord(ev[4], stream);
-            if (more) cudaStreamWaitEvent(stream, join_ev[k], 0);
+            /* main: step k's CPA search; eig: its eigenray construction */
+            cudaStreamWaitEvent(stream, adv_ev[k], 0);
+            if (h.nt > 0) {
+                cpa_launch(k, stream);
+                launches += 1;
+                cudaEventRecord(cpa_ev[k], stream);
+                cudaStreamWaitEvent(eig, cpa_ev[k], 0);
+                eig_launch(k, eig);
+            }
+            cudaEventRecord(eig_ev[k], eig);
         }
-        if (ovl) {
-            cudaEventRecord(eig_end, eig);
-            cudaStreamWaitEvent(stream, eig_end, 0);
-        }
+        /* every stream joins the main stream */
+        cudaEventRecord(eig_end, eig);
+        cudaStreamWaitEvent(stream, eig_end, 0);
+        if (tail) cudaStreamWaitEvent(stream, join_ev[K - 1], 0);
         return WQ3D_OK;
     }
 
@@ -605,6 +657,7 @@ struct wq3d_queue {
         timing = false;
         const int64_t saved_launches = launches;
         launch_chunk(chunk, p, tail);
+        graph_launches[p][t] = launches - saved_launches;
         launches = saved_launches;
         timing = save;
         if (cudaStreamEndCapture(stream, &g) != cudaSuccess ||
@@ -732,8 +785,7 @@ struct wq3d_queue {
         if (!timing && K == chunk) build_graph(p, tail);
         if (!timing && K == chunk && graph[p][t]) {
             WQ_CK(cudaGraphLaunch(graph[p][t], stream));
-            launches += ((h.nt > 0 ? 5 : 3) + (volume_pass() ? 1 : 0) + (h.adj ? (h.nt > 0 ? 3 : 1) : 0)) *
-                            (int64_t)K + (tail ? 1 : 0);
+            launches += graph_launches[p][t];
         } else {
             launch_chunk(K, p, tail);
         }
@@ -1461,9 +1513,11 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) prio_high = 0;
         if (cudaStreamCreateWithPriority(&q->side, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->eig, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&q->adv, cudaStreamNonBlocking) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
-        if (cudaEventCreateWithFlags(&q->eig_end, cudaEventDisableTiming) != cudaSuccess)
+        if (cudaEventCreateWithFlags(&q->eig_end, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&q->start_ev, cudaEventDisableTiming) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
         for (auto& e : q->done_ev)
             if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
@@ -1494,7 +1548,7 @@ int wq3d_queue_destroy(wq3d_queue* q) {
     DeviceGuard guard(q->device);
     if (cacheable(q) && cudaStreamSynchronize(q->stream) == cudaSuccess &&
         cudaStreamSynchronize(q->side) == cudaSuccess && cudaStreamSynchronize(q->eig) == cudaSuccess &&
-        cudaStreamSynchronize(q->copy) == cudaSuccess) {
+        cudaStreamSynchronize(q->adv) == cudaSuccess && cudaStreamSynchronize(q->copy) == cudaSuccess) {
         wq3d_queue* drop = nullptr;
         {
             std::lock_guard<std::mutex> lock(g_cache_mu);

@@ -398,8 +398,10 @@ __device__ __noinline__ void volume_scatter(const QueueDev& q, const FrontPtrs& 
     }
 }
 
-__device__ __noinline__ void update1_ni(const QueueDev& q, RayS& y) { update1(q, y); }
-
+/* reflection_model::reflection_reinit on the private state.  The ten
+ * updates are inlined so that the five temporary rays stay in registers
+ * (out of line, each update round-tripped a ray through local memory on
+ * the reflection chain's critical path). */
 __device__ __noinline__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const double* pos,
                              const double* nd) {
     RayS past1, prev1, curr1, next1, temp;
@@ -413,30 +415,30 @@ __device__ __noinline__ void reinit_local(const QueueDev& q, RayLocal& L, double
     prev1.dist = 0.0;
     curr1.dist = 0.0;
     temp.dist = 0.0;
-    update1_ni(q, temp);
+    update1(q, temp);
     rk1(-tw, temp, next1);
-    update1_ni(q, next1);
+    update1(q, next1);
     rk2(-tw, temp, next1, past1);
-    update1_ni(q, past1);
+    update1(q, past1);
     rk3(-tw, temp, next1, past1, curr1);
-    update1_ni(q, curr1);
+    update1(q, curr1);
 
     const double h = q.dt;
     rk1(-h, curr1, next1);
-    update1_ni(q, next1);
+    update1(q, next1);
     rk2(-h, curr1, next1, past1);
-    update1_ni(q, past1);
+    update1(q, past1);
     rk3(-h, curr1, next1, past1, prev1);
-    update1_ni(q, prev1);
+    update1(q, prev1);
 
     rk1(-h, prev1, next1);
-    update1_ni(q, next1);
+    update1(q, next1);
     rk2(-h, prev1, next1, temp);
     rk3(-h, prev1, next1, temp, past1);
-    update1_ni(q, past1);
+    update1(q, past1);
 
     ab3(h, past1, prev1, curr1, next1);
-    update1_ni(q, next1);
+    update1(q, next1);
     L.c = curr1;
     L.v = prev1;
     L.x = next1;
@@ -900,10 +902,14 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
 #else
 #define WQ_ADVANCE_BOUNDS __launch_bounds__(128, 5)
 #endif
-__global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, int k) {
+/* phase: ADVANCE_ALL every ray; ADVANCE_FREE the rays whose step needs
+ * none of this step's reflections (neither the ray nor a D/E neighbour
+ * within two rows reflects), which may run beside k_reflect; ADVANCE_BOUND
+ * the others, after k_reflect */
+__global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, int k, int phase) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t s = *q.d_base + k;
-    if (blockIdx.x == 0 && threadIdx.x == 0) q.n_cand[cand_list(s + 1)] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && phase != ADVANCE_BOUND) q.n_cand[cand_list(s + 1)] = 0;
     if (i >= q.n) return;
     Roles R;
     roles_at(q, s, R);
@@ -912,17 +918,29 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     const int naz = q.naz;
     const int d = i / naz;
     const size_t stride = shadow_stride(q);
+    const int max_de = q.nde - 1;
+    int jrow[4];
+    jrow[0] = i + (max(d - 2, 0) - d) * naz;
+    jrow[1] = i + (max(d - 1, 0) - d) * naz;
+    jrow[2] = i + (min(d + 1, max_de) - d) * naz;
+    jrow[3] = i + (min(d + 2, max_de) - d) * naz;
+    const bool refl = __ldg(flag_in + i) != 0;
+    bool fl[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) fl[t] = __ldg(flag_in + jrow[t]) != 0;
+    if (phase != ADVANCE_ALL) {
+        const bool bound = refl || fl[0] || fl[1] || fl[2] || fl[3];
+        if (bound != (phase == ADVANCE_BOUND)) return;
+    }
     /* Reads go through the read-only path: in this launch no ray reads an
      * element that another ray writes (neighbours are read only where they
      * do not reflect, and a reflecting ray's entries come from its shadow
      * slot), and a ray's own updated counters and phases stay in
      * registers, so the loads need not wait behind the stores. */
     RayS y0, y1, y2, y3;
-    const int max_de = q.nde - 1;
-    /* one round of loads: this ray on the three fronts and its flag, and
-     * the rows d-2 .. d+2 that detect_caustics and find_edges may read
-     * (rows clamped to the fan; a clamped row is never used) */
-    const bool refl = __ldg(flag_in + i) != 0;
+    /* one round of loads: this ray on the three fronts, and the rows
+     * d-2 .. d+2 that detect_caustics and find_edges may read (rows
+     * clamped to the fan; a clamped row is never used) */
     const int set = (int)(s & 1);
     if (!refl) load_prev_curr(q, s, R, i, y0, y1);
     load_ray_ro(*R.X, i, y2);
@@ -931,16 +949,9 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     int32_t cs = __ldg(R.X->caustic + i);
     int32_t up = __ldg(R.X->upper + i);
     int32_t lo = __ldg(R.X->lower + i);
-    int jrow[4];
-    jrow[0] = i + (max(d - 2, 0) - d) * naz;
-    jrow[1] = i + (max(d - 1, 0) - d) * naz;
-    jrow[2] = i + (min(d + 1, max_de) - d) * naz;
-    jrow[3] = i + (min(d + 2, max_de) - d) * naz;
-    bool fl[4];
     double rr[4], nn[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-        fl[t] = __ldg(flag_in + jrow[t]) != 0;
         rr[t] = __ldg(R.X->pos[0] + jrow[t]);
         nn[t] = __ldg(R.X->nd[0] + jrow[t]);
     }
