@@ -219,8 +219,6 @@ struct wq3d_queue {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;
     cudaStream_t eig = nullptr; /* k_commit and the eigenray construction */
-    cudaStream_t adv = nullptr; /* k_advance, checkpoints, volume eigenverbs */
-    cudaEvent_t start_ev = nullptr;
     std::vector<cudaEvent_t> fork_ev, join_ev;
     std::vector<cudaEvent_t> adv_ev, com_ev, cpa_ev, eig_ev; /* per step of a chunk */
     cudaEvent_t eig_end = nullptr;
@@ -281,7 +279,7 @@ struct wq3d_queue {
     /* the stepping kernels' build: "gridded" when the ocean has a grid */
     bool gridded = false;
     void (*k_reflect_fn)(const QueueDev, int) = analytic::k_reflect;
-    void (*k_advance_fn)(const QueueDev, int, int) = analytic::k_advance;
+    void (*k_advance_fn)(const QueueDev, int) = analytic::k_advance;
     /* eigenverb counting sink (wq3d_queue_count_eigenverbs) */
     bool count_verbs = false;
     uint64_t verb_counts[2 + 2 * WQ3D_MAX_VOLUME] = {0};
@@ -454,8 +452,6 @@ struct wq3d_queue {
         for (auto* v : {&adv_ev, &com_ev, &cpa_ev, &eig_ev})
             for (auto e : *v) cudaEventDestroy(e);
         if (eig_end) cudaEventDestroy(eig_end);
-        if (start_ev) cudaEventDestroy(start_ev);
-        if (adv) cudaStreamDestroy(adv);
         if (eig) cudaStreamDestroy(eig);
         if (side) cudaStreamDestroy(side);
         if (ev_begin) cudaEventDestroy(ev_begin);
@@ -489,29 +485,29 @@ struct wq3d_queue {
     }
 
     /* One chunk of K steps writing result set p.  Without per-kernel
-     * timing it runs on four streams:
-     *   adv   k_advance(k+1) in two launches: the rays whose step needs no
-     *         reflection of step k+1 (ADVANCE_FREE) right after step k's
-     *         advance, beside k_reflect(k+1) and k_cpa(k); the others
-     *         (ADVANCE_BOUND) once k_reflect(k+1) is done.  The adjoint's
-     *         checkpoint and the volume eigenverbs of a step run here
-     *         before its advance.
-     *   side  k_reflect(k+1) (high priority), after step k's advance
-     *   main  k_cpa(k), after step k's advance
-     *   eig   k_commit(k) after step k's advance, k_eigenray(k) after
-     *         k_cpa(k), and the adjoint's eigenray partials
+     * timing it runs on three streams:
+     *   main  k_advance(k) (after k_reflect(k)), then k_cpa(k); the adjoint's
+     *         checkpoint and the volume eigenverbs of a step run before its
+     *         advance
+     *   side  k_reflect(k+1) (high priority), right after k_advance(k),
+     *         beside k_cpa(k)
+     *   eig   k_commit(k) after k_advance(k), k_eigenray(k) after k_cpa(k),
+     *         and the adjoint's eigenray partials
      * Step k+1 reads the rays that reflected at step k from step k's shadow
-     * slots, so nothing on the adv or side stream waits for k_commit(k)
-     * (except with eigenverbs: an eigenverb reads the curr front's losses
-     * and counts).  Step k+1's advance overwrites the front, commit flags
-     * and candidate list that step k-1 used, and k_reflect(k+1) its slot
-     * set, so both wait for step k-1's eigenray-stream work.  The first
-     * step of a chunk advances every ray in one launch.  With "tail" the
-     * reflections of the next chunk's first step run beside this chunk's
-     * last CPA search; that chunk's own k_reflect(0) then finds an empty
-     * worklist and returns.
+     * slots, so neither k_reflect(k+1) nor k_advance(k+1) waits for
+     * k_commit(k) (except with eigenverbs: an eigenverb reads the curr
+     * front's losses and counts, so k_reflect(k+1) then waits for it).
+     * k_advance(k+1) overwrites the commit flags and candidate list of step
+     * k-1, and k_reflect(k+1) its slot set, so k_reflect(k+1) waits for step
+     * k-1's whole eigenray-stream work.  With "tail" the reflections of the
+     * next chunk's first step run beside this chunk's last CPA search; that
+     * chunk's own k_reflect(0) then finds an empty worklist and returns.
      * With per-kernel timing the steps run one launch after another on the
-     * main stream, except k_reflect(k+1) beside k_cpa(k) and k_eigenray(k). */
+     * main stream, except k_reflect(k+1) beside k_cpa(k) and k_eigenray(k).
+     * (An advance split into the rays that need none of the step's
+     * reflections, run beside k_reflect and k_cpa, and the rest was slower:
+     * 149.5 against 131.9 ms per propagation of the sloped workload, the
+     * memory-bound advance taking SM time from the CPA search.) */
     int launch_chunk(int K, int p, bool tail) {
         const QueueDev d = dev(p);
         const int n = h.n;
@@ -557,7 +553,7 @@ struct wq3d_queue {
                     k_volume<<<grd, blk, 0, stream>>>(d, k);
                     launches += 1;
                 }
-                k_advance_fn<<<grd, blk, 0, stream>>>(d, k, ADVANCE_ALL);
+                k_advance_fn<<<grd, blk, 0, stream>>>(d, k);
                 k_commit<<<grd, blk, 0, stream>>>(d, k);
                 launches += 2;
                 cudaEventRecord(ev[1], stream);
@@ -584,27 +580,19 @@ struct wq3d_queue {
             }
             return WQ3D_OK;
         }
-        cudaEventRecord(start_ev, stream);
-        cudaStreamWaitEvent(adv, start_ev, 0);
         for (int k = 0; k < K; ++k) {
-            /* adv: step k's checkpoint, volume eigenverbs and advance */
+            /* main: step k's checkpoint, volume eigenverbs and advance */
             if (h.adj) {
-                k_adj_checkpoint<<<grd, blk, 0, adv>>>(d, k);
+                k_adj_checkpoint<<<grd, blk, 0, stream>>>(d, k);
                 launches += 1;
             }
             if (volume_pass()) {
-                if (k >= 1) cudaStreamWaitEvent(adv, com_ev[k - 1], 0);
-                k_volume<<<grd, blk, 0, adv>>>(d, k);
+                k_volume<<<grd, blk, 0, stream>>>(d, k);
                 launches += 1;
             }
-            if (k == 0) {
-                k_advance_fn<<<grd, blk, 0, adv>>>(d, 0, ADVANCE_ALL);
-            } else {
-                cudaStreamWaitEvent(adv, join_ev[k - 1], 0);
-                k_advance_fn<<<grd, blk, 0, adv>>>(d, k, ADVANCE_BOUND);
-            }
+            k_advance_fn<<<grd, blk, 0, stream>>>(d, k);
             launches += 1;
-            cudaEventRecord(adv_ev[k], adv);
+            cudaEventRecord(adv_ev[k], stream);
             /* eig: step k's commit */
             cudaStreamWaitEvent(eig, adv_ev[k], 0);
             k_commit<<<grd, blk, 0, eig>>>(d, k);
@@ -620,14 +608,7 @@ struct wq3d_queue {
                 cudaEventRecord(join_ev[k], side);
                 launches += 1;
             }
-            if (k + 1 < K) {
-                /* adv: the rays of step k+1 that need none of its reflections */
-                if (k >= 1) cudaStreamWaitEvent(adv, eig_ev[k - 1], 0);
-                k_advance_fn<<<grd, blk, 0, adv>>>(d, k + 1, ADVANCE_FREE);
-                launches += 1;
-            }
             /* main: step k's CPA search; eig: its eigenray construction */
-            cudaStreamWaitEvent(stream, adv_ev[k], 0);
             if (h.nt > 0) {
                 cpa_launch(k, stream);
                 launches += 1;
@@ -636,11 +617,11 @@ struct wq3d_queue {
                 eig_launch(k, eig);
             }
             cudaEventRecord(eig_ev[k], eig);
+            if (more) cudaStreamWaitEvent(stream, join_ev[k], 0);
         }
-        /* every stream joins the main stream */
+        /* the eigenray stream joins the main stream */
         cudaEventRecord(eig_end, eig);
         cudaStreamWaitEvent(stream, eig_end, 0);
-        if (tail) cudaStreamWaitEvent(stream, join_ev[K - 1], 0);
         return WQ3D_OK;
     }
 
@@ -1513,11 +1494,9 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) prio_high = 0;
         if (cudaStreamCreateWithPriority(&q->side, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->eig, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaStreamCreateWithFlags(&q->adv, cudaStreamNonBlocking) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
-        if (cudaEventCreateWithFlags(&q->eig_end, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&q->start_ev, cudaEventDisableTiming) != cudaSuccess)
+        if (cudaEventCreateWithFlags(&q->eig_end, cudaEventDisableTiming) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
         for (auto& e : q->done_ev)
             if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
@@ -1548,7 +1527,7 @@ int wq3d_queue_destroy(wq3d_queue* q) {
     DeviceGuard guard(q->device);
     if (cacheable(q) && cudaStreamSynchronize(q->stream) == cudaSuccess &&
         cudaStreamSynchronize(q->side) == cudaSuccess && cudaStreamSynchronize(q->eig) == cudaSuccess &&
-        cudaStreamSynchronize(q->adv) == cudaSuccess && cudaStreamSynchronize(q->copy) == cudaSuccess) {
+        cudaStreamSynchronize(q->copy) == cudaSuccess) {
         wq3d_queue* drop = nullptr;
         {
             std::lock_guard<std::mutex> lock(g_cache_mu);

@@ -44,9 +44,6 @@ enum : uint32_t {
     ERR_BAD_CANDIDATE = 256u     /* a candidate names a ray or target outside the fan (skipped) */
 };
 
-/* which rays a k_advance launch takes (its "phase" argument) */
-enum : int { ADVANCE_ALL = 0, ADVANCE_FREE = 1, ADVANCE_BOUND = 2 };
-
 /* k_advance's decisions for k_commit (QueueDev::commit_flag) */
 enum : uint8_t { COMMIT_REFLECT = 1, COMMIT_FOLD = 2, COMMIT_UPPER = 4, COMMIT_LOWER = 8 };
 
@@ -208,7 +205,7 @@ __device__ __forceinline__ int cand_list(int64_t s) { return (int)((s + 1) & 1);
 #define WQ3D_DECLARE_STEP_KERNELS                         \
     __global__ void k_startup(__grid_constant__ const QueueDev q);         \
     __global__ void k_reflect(__grid_constant__ const QueueDev q, int k);  \
-    __global__ void k_advance(__grid_constant__ const QueueDev q, int k, int phase);
+    __global__ void k_advance(__grid_constant__ const QueueDev q, int k);
 namespace gridded {
 WQ3D_DECLARE_STEP_KERNELS
 }

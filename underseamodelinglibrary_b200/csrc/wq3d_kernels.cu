@@ -398,10 +398,19 @@ __device__ __noinline__ void volume_scatter(const QueueDev& q, const FrontPtrs& 
     }
 }
 
-/* reflection_model::reflection_reinit on the private state.  The ten
- * updates are inlined so that the five temporary rays stay in registers
- * (out of line, each update round-tripped a ray through local memory on
- * the reflection chain's critical path). */
+/* The updates of the re-initialisation.  The analytic build inlines them
+ * so that the five temporary rays stay in registers (out of line, each
+ * update round-tripped a ray through local memory on the reflection
+ * chain's critical path); in the gridded build the grid interpolation's
+ * calls would then push the chain into register spills, so it keeps them
+ * out of line. */
+#if WQ3D_WITH_GRID
+__device__ __noinline__ void reinit_update(const QueueDev& q, RayS& y) { update1(q, y); }
+#else
+__device__ __forceinline__ void reinit_update(const QueueDev& q, RayS& y) { update1(q, y); }
+#endif
+
+/* reflection_model::reflection_reinit on the private state */
 __device__ __noinline__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const double* pos,
                              const double* nd) {
     RayS past1, prev1, curr1, next1, temp;
@@ -415,30 +424,30 @@ __device__ __noinline__ void reinit_local(const QueueDev& q, RayLocal& L, double
     prev1.dist = 0.0;
     curr1.dist = 0.0;
     temp.dist = 0.0;
-    update1(q, temp);
+    reinit_update(q, temp);
     rk1(-tw, temp, next1);
-    update1(q, next1);
+    reinit_update(q, next1);
     rk2(-tw, temp, next1, past1);
-    update1(q, past1);
+    reinit_update(q, past1);
     rk3(-tw, temp, next1, past1, curr1);
-    update1(q, curr1);
+    reinit_update(q, curr1);
 
     const double h = q.dt;
     rk1(-h, curr1, next1);
-    update1(q, next1);
+    reinit_update(q, next1);
     rk2(-h, curr1, next1, past1);
-    update1(q, past1);
+    reinit_update(q, past1);
     rk3(-h, curr1, next1, past1, prev1);
-    update1(q, prev1);
+    reinit_update(q, prev1);
 
     rk1(-h, prev1, next1);
-    update1(q, next1);
+    reinit_update(q, next1);
     rk2(-h, prev1, next1, temp);
     rk3(-h, prev1, next1, temp, past1);
-    update1(q, past1);
+    reinit_update(q, past1);
 
     ab3(h, past1, prev1, curr1, next1);
-    update1(q, next1);
+    reinit_update(q, next1);
     L.c = curr1;
     L.v = prev1;
     L.x = next1;
@@ -902,14 +911,10 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
 #else
 #define WQ_ADVANCE_BOUNDS __launch_bounds__(128, 5)
 #endif
-/* phase: ADVANCE_ALL every ray; ADVANCE_FREE the rays whose step needs
- * none of this step's reflections (neither the ray nor a D/E neighbour
- * within two rows reflects), which may run beside k_reflect; ADVANCE_BOUND
- * the others, after k_reflect */
-__global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, int k, int phase) {
+__global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, int k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t s = *q.d_base + k;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && phase != ADVANCE_BOUND) q.n_cand[cand_list(s + 1)] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) q.n_cand[cand_list(s + 1)] = 0;
     if (i >= q.n) return;
     Roles R;
     roles_at(q, s, R);
@@ -928,10 +933,6 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     bool fl[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) fl[t] = __ldg(flag_in + jrow[t]) != 0;
-    if (phase != ADVANCE_ALL) {
-        const bool bound = refl || fl[0] || fl[1] || fl[2] || fl[3];
-        if (bound != (phase == ADVANCE_BOUND)) return;
-    }
     /* Reads go through the read-only path: in this launch no ray reads an
      * element that another ray writes (neighbours are read only where they
      * do not reflect, and a reflecting ray's entries come from its shadow
@@ -1424,6 +1425,7 @@ __global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ co
     __shared__ uint16_t surv[F32_TARGETS];
     __shared__ int nsurv;
     __shared__ WarpQueue wq[CPA_THREADS / 32];
+    __shared__ uint16_t wsurv[CPA_THREADS / 32][F32_TARGETS];
     const int64_t s = *q.d_base + k + 1;
     const FrontPtrs& V = q.F[(s + 1) & 3];
     const FrontPtrs& C = q.F[(s + 2) & 3];
@@ -1555,7 +1557,30 @@ __global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ co
             surv[atomicAdd(&nsurv, 1)] = (uint16_t)j;
         }
         __syncthreads();
-        const int ns = nsurv;
+        /* the warp's own patch (4 D/E rows x 8 AZ columns, its ranges in
+         * red[w]) drops more of the block's targets with the same test */
+        int ns = 0;
+        {
+            const PatchGuard wx = patch_guard(&red[w][0], &red[w][8], W, c0);
+            const PatchGuard wv = patch_guard(&red[w][16], &red[w][24], W, c0);
+            const int nb = nsurv;
+            for (int j0 = 0; j0 < nb; j0 += 32) {
+                const int jj = j0 + lane;
+                bool keep = false;
+                int tj = 0;
+                if (jj < nb) {
+                    tj = surv[jj];
+                    const TgtW g = tw[tj];
+                    keep = !patch_rejects(g, &red[w][0], &red[w][8], wx) &&
+                           !patch_rejects(g, &red[w][16], &red[w][24], wv);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) wsurv[w][ns + __popc(m & lt)] = (uint16_t)tj;
+                ns += __popc(m);
+            }
+            __syncwarp();
+        }
+        const uint16_t* surv_w = wsurv[w];
         int qn = 0;
         /* appends this lane's pair if "want"; finishes 32 at a time */
         auto push = [&](bool want, int j) {
@@ -1575,7 +1600,7 @@ __global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ co
         };
         int sidx = 0;
         for (; sidx + 1 < ns; sidx += 2) {
-            const int j0 = surv[sidx], j1 = surv[sidx + 1];
+            const int j0 = surv_w[sidx], j1 = surv_w[sidx + 1];
             const TgtW g0 = tw[j0], g1 = tw[j1];
             const float a0 = screen_dot(g0, dxc), a1 = screen_dot(g1, dxc);
             bool w0 = active && !(a0 < -gxc), w1 = active && !(a1 < -gxc);
@@ -1588,7 +1613,7 @@ __global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ co
             push(w1, j1);
         }
         if (sidx < ns) {
-            const int j = surv[sidx];
+            const int j = surv_w[sidx];
             const TgtW g = tw[j];
             bool want = active && !(screen_dot(g, dxc) < -gxc);
             if (want) want = !(screen_dot(g, dvc) < -gvc);
