@@ -1090,9 +1090,9 @@ __global__ void __launch_bounds__(32 * JAC_WARPS) k_eigenray_jac(__grid_constant
     const double time = q.d_times[k + 1];
     const uint32_t lo = *q.adj_mark;
     const uint32_t hi = min(*q.n_rec, q.cap_rec);
-    const FrontPtrs& V = q.F[(s + 1) & 3];
-    const FrontPtrs& C = q.F[(s + 2) & 3];
-    const FrontPtrs& X = q.F[(s + 3) & 3];
+    const FrontPtrs& V = q.F[ring_slot(s + 1)];
+    const FrontPtrs& C = q.F[ring_slot(s + 2)];
+    const FrontPtrs& X = q.F[ring_slot(s + 3)];
     for (uint32_t r = lo + blockIdx.x * JAC_WARPS + warp; r < hi; r += gridDim.x * JAC_WARPS) {
         __syncwarp();
         const wq3d_eigenray rec = q.rec[r];

@@ -220,7 +220,7 @@ struct wq3d_queue {
     cudaStream_t side = nullptr;
     cudaStream_t eig = nullptr; /* k_commit and the eigenray construction */
     std::vector<cudaEvent_t> fork_ev, join_ev;
-    std::vector<cudaEvent_t> adv_ev, com_ev, cpa_ev, eig_ev; /* per step of a chunk */
+    std::vector<cudaEvent_t> adv_ev, com_ev, cpa_ev; /* per step of a chunk */
     cudaEvent_t eig_end = nullptr;
     QueueDev h{};
     std::vector<void*> allocs;
@@ -228,7 +228,7 @@ struct wq3d_queue {
     /* per result set: chunk base step, chunk times, counters read back
      * (n_rec, n_refl, err, -, work lists, n_done, -, n_verb); d_counts also
      * holds the bottom work lists (9, 10), the adjoint's mark and entry
-     * count (11, 12) and the two candidate counts (13, 14) */
+     * count (11, 12) and the three candidate counts (13-15) */
     int64_t* h_base[2] = {nullptr, nullptr};
     double* h_times[2] = {nullptr, nullptr};
     uint32_t* h_counts[2] = {nullptr, nullptr};
@@ -449,7 +449,7 @@ struct wq3d_queue {
             if (e) cudaEventDestroy(e);
         for (auto e : fork_ev) cudaEventDestroy(e);
         for (auto e : join_ev) cudaEventDestroy(e);
-        for (auto* v : {&adv_ev, &com_ev, &cpa_ev, &eig_ev})
+        for (auto* v : {&adv_ev, &com_ev, &cpa_ev})
             for (auto e : *v) cudaEventDestroy(e);
         if (eig_end) cudaEventDestroy(eig_end);
         if (eig) cudaStreamDestroy(eig);
@@ -497,9 +497,11 @@ struct wq3d_queue {
      * slots, so neither k_reflect(k+1) nor k_advance(k+1) waits for
      * k_commit(k) (except with eigenverbs: an eigenverb reads the curr
      * front's losses and counts, so k_reflect(k+1) then waits for it).
-     * k_advance(k+1) overwrites the commit flags and candidate list of step
-     * k-1, and k_reflect(k+1) its slot set, so k_reflect(k+1) waits for step
-     * k-1's whole eigenray-stream work.  With "tail" the reflections of the
+     * k_reflect(k+1) reuses step k-1's slot set and k_advance(k+1) its
+     * commit flags, so k_reflect(k+1) waits for k_commit(k-1); that also
+     * orders k_advance(k+1) after step k-2's eigenray construction, whose
+     * prev front and candidate list it overwrites (five ring slots, three
+     * candidate lists).  With "tail" the reflections of the
      * next chunk's first step run beside this chunk's last CPA search; that
      * chunk's own k_reflect(0) then finds an empty worklist and returns.
      * With per-kernel timing the steps run one launch after another on the
@@ -602,7 +604,7 @@ struct wq3d_queue {
             if (more) {
                 /* side: step k+1's reflections */
                 cudaStreamWaitEvent(side, adv_ev[k], 0);
-                if (k >= 1) cudaStreamWaitEvent(side, eig_ev[k - 1], 0);
+                if (k >= 1) cudaStreamWaitEvent(side, com_ev[k - 1], 0);
                 if (h.want_verbs) cudaStreamWaitEvent(side, com_ev[k], 0);
                 k_reflect_fn<<<rgrid, 64, 0, side>>>(d, k + 1);
                 cudaEventRecord(join_ev[k], side);
@@ -616,7 +618,6 @@ struct wq3d_queue {
                 cudaStreamWaitEvent(eig, cpa_ev[k], 0);
                 eig_launch(k, eig);
             }
-            cudaEventRecord(eig_ev[k], eig);
             if (more) cudaStreamWaitEvent(stream, join_ev[k], 0);
         }
         /* the eigenray stream joins the main stream */
@@ -1376,10 +1377,10 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         const size_t bbytes = al(n);
         const size_t per_front = nd_arrays * dbytes + 5 * ibytes + bbytes;
         char* base = reuse ? q->ring : nullptr;
-        if (!reuse && (rc = q->alloc(&base, 4 * per_front + 2 * bbytes))) return cleanup(rc);
+        if (!reuse && (rc = q->alloc(&base, RING * per_front + 2 * bbytes))) return cleanup(rc);
         q->ring = base;
-        q->ring_bytes = 4 * per_front + 2 * bbytes;
-        if (cudaMemset(base, 0, 4 * per_front + 2 * bbytes) != cudaSuccess)
+        q->ring_bytes = RING * per_front + 2 * bbytes;
+        if (cudaMemset(base, 0, RING * per_front + 2 * bbytes) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
         char* p = base;
         auto dtake = [&](size_t count) {
@@ -1387,7 +1388,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
             p += al(count * sizeof(double));
             return r;
         };
-        for (int f = 0; f < 4; ++f) {
+        for (int f = 0; f < RING; ++f) {
             FrontPtrs& F = h.F[f];
             for (int k = 0; k < 3; ++k) {
                 F.pos[k] = dtake(n);
@@ -1421,7 +1422,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.cap_refl = 4096; /* grown when a reflection listener asks */
     if (!reuse) {
         uint32_t* cand = nullptr;
-        if ((rc = q->alloc(&cand, 4 * (size_t)h.cap_cand))) return cleanup(rc);
+        if ((rc = q->alloc(&cand, 2 * CAND_LISTS * (size_t)h.cap_cand))) return cleanup(rc);
         h.cand = cand;
         if ((rc = q->alloc(&h.rec, h.cap_rec)) || (rc = q->alloc(&h.rec_inten, (size_t)h.cap_rec * nf)) ||
             (rc = q->alloc(&h.rec_phase, (size_t)h.cap_rec * nf)) || (rc = q->alloc(&h.refl, h.cap_refl)))
@@ -1433,7 +1434,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.n_rec = q->d_counts + 0;
     h.n_refl = q->d_counts + 1;
     h.err = q->d_counts + 2;
-    h.n_cand = q->d_counts + 13; /* two lists: 13, 14 */
+    h.n_cand = q->d_counts + 13; /* three lists: 13, 14, 15 */
     h.n_work[0] = q->d_counts + 4;
     h.n_work[1] = q->d_counts + 5;
     h.n_work_b[0] = q->d_counts + 9;
@@ -1501,7 +1502,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         for (auto& e : q->done_ev)
             if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
                 return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
-        for (auto* v : {&q->fork_ev, &q->join_ev, &q->adv_ev, &q->com_ev, &q->cpa_ev, &q->eig_ev}) {
+        for (auto* v : {&q->fork_ev, &q->join_ev, &q->adv_ev, &q->com_ev, &q->cpa_ev}) {
             v->resize(q->chunk);
             for (int k = 0; k < q->chunk; ++k)
                 if (cudaEventCreateWithFlags(&(*v)[k], cudaEventDisableTiming) != cudaSuccess)
@@ -1719,7 +1720,7 @@ int wq3d_queue_steps(const wq3d_queue* q, int64_t* steps) {
 int wq3d_queue_get_front(wq3d_queue* q, int which, const wq3d_front_view* v) {
     if (!q || !v || which < 0 || which > 3) return fail(WQ3D_ERR_INVALID, "bad argument");
     DeviceGuard guard(q->device);
-    const FrontPtrs& F = q->h.F[(q->steps + which) & 3];
+    const FrontPtrs& F = q->h.F[(q->steps + which) % RING];
     const size_t n = q->h.n, nf = q->h.nf;
     auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
         if (!dst) return WQ3D_OK;
@@ -1782,12 +1783,12 @@ int wq3d_queue_enable_sensitivity(wq3d_queue* q) {
     DeviceGuard guard(q->device);
     const size_t n = (size_t)q->h.n;
     double* dA = nullptr;
-    int rc = q->alloc(&dA, 4 * 3 * n);
+    int rc = q->alloc(&dA, RING * 3 * n);
     if (!rc) rc = q->alloc(&q->h.rec_sens, (size_t)q->h.cap_rec * 3);
     if (!rc && q->have_set1) rc = q->alloc(&q->set1.rec_sens, (size_t)q->h.cap_rec * 3);
     if (rc) return rc;
-    WQ_CK(cudaMemset(dA, 0, 4 * 3 * n * sizeof(double)));
-    for (int f = 0; f < 4; ++f) q->h.F[f].dA = dA + (size_t)f * 3 * n;
+    WQ_CK(cudaMemset(dA, 0, RING * 3 * n * sizeof(double)));
+    for (int f = 0; f < RING; ++f) q->h.F[f].dA = dA + (size_t)f * 3 * n;
     q->h.sens = 1;
     q->drop_graph();
     return WQ3D_OK;

@@ -2,14 +2,18 @@
  * wq3d_engine.cuh -- device-side layout of one wave queue and the kernel
  * entry points of the FP64 propagation engine.
  *
- * HBM layout: four wavefronts in a ring (the reference's past/prev/curr/next
- * circular queue, waveq3d/wave_queue.h:350).  Every per-ray field is its
- * own contiguous array of N = num_de * num_az values in (de, az) row-major
- * order, so one thread per ray reads and writes fully coalesced.  Per
- * frequency fields are frequency-major ([f][N]).  A ring role is selected by
- * the step number: at the start of step s the roles are past = F[s&3],
- * prev = F[(s+1)&3], curr = F[(s+2)&3], next = F[(s+3)&3], which is the
- * reference's pointer rotation (wave_queue.cc:162-167) without copying.
+ * HBM layout: wavefronts in a ring of RING slots (the reference's
+ * past/prev/curr/next circular queue, waveq3d/wave_queue.h:350, plus one
+ * slot).  Every per-ray field is its own contiguous array of N = num_de *
+ * num_az values in (de, az) row-major order, so one thread per ray reads
+ * and writes fully coalesced.  Per frequency fields are frequency-major
+ * ([f][N]).  A ring role is selected by the step number: at the start of
+ * step s the roles are past = F[s % RING], prev = F[(s+1) % RING], curr =
+ * F[(s+2) % RING], next = F[(s+3) % RING], and step s writes its new front
+ * into F[(s+4) % RING]: the reference's pointer rotation
+ * (wave_queue.cc:162-167) without copying.  The fifth slot lets step s+1
+ * write its new front while step s-1's eigenray construction, on its own
+ * stream, still reads that step's prev / curr / next fronts.
  *
  * Instead of the reference's num_targets x N distance2 matrices per front
  * (wave_front.h:258), each front keeps the four terms that
@@ -28,6 +32,8 @@
 namespace wq3d {
 
 constexpr int MAX_FREQ = 64;     /* frequencies per queue                */
+constexpr int RING = 5;          /* wavefront slots                      */
+constexpr int CAND_LISTS = 3;    /* eigenray candidate lists             */
 constexpr int MAX_AZ = 4096;     /* AZ fan size (duplicate bit mask)     */
 constexpr int MAX_BOUNCE = 64;   /* reflections of one ray in one step   */
 
@@ -99,7 +105,7 @@ struct FrontPtrs {
 };
 
 struct QueueDev {
-    FrontPtrs F[4];
+    FrontPtrs F[RING];
     OceanDev oc;
     int nde, naz, nf, n;
     int nt, nt1, nt2;
@@ -151,11 +157,11 @@ struct QueueDev {
     int32_t* shadow_cnt[2];  /* surface, bottom, caustic per slot           */
     int32_t* shadow_slot[2]; /* worklist slot of each reflecting ray        */
     uint8_t* commit_flag[2]; /* per ray: COMMIT_* bits k_advance leaves for k_commit */
-    /* eigenray candidates: two lists by step parity (cand_list), so the
-     * next step's advance and CPA search fill one while this step's
-     * eigenray construction, on its own stream, reads the other */
-    uint32_t* cand;          /* [2][cap_cand] packed: target, ray index      */
-    uint32_t* n_cand;        /* [2] counts                                   */
+    /* eigenray candidates: CAND_LISTS lists by step (cand_list), so the
+     * next steps' advance and CPA search fill others while this step's
+     * eigenray construction, on its own stream, reads its list */
+    uint32_t* cand;          /* [CAND_LISTS][cap_cand] packed: target, ray   */
+    uint32_t* n_cand;        /* [CAND_LISTS] counts                          */
     uint32_t cap_cand;
     /* eigenray records of the chunk */
     wq3d_eigenray* rec;
@@ -189,12 +195,15 @@ struct QueueDev {
     uint32_t* adj_mark;      /* eigenray records of the chunk processed     */
 };
 
+/* the ring slot of step-relative index s (s >= 0) */
+__device__ __forceinline__ int ring_slot(int64_t s) { return (int)(s % RING); }
+
 /* The candidate list of the step whose rotated roles start at s (the "s"
  * of the CPA and eigenray kernels, one more than the advance's).  Step k's
- * eigenray construction reads list (s+1)&1 while step k+1 clears and fills
- * the other; step k+2's advance clears this one only after step k+1's
+ * eigenray construction reads its list while steps k+1 and k+2 fill the
+ * others; step k+3's advance clears it again only after step k+2's
  * commit, which follows step k's eigenray construction on its stream. */
-__device__ __forceinline__ int cand_list(int64_t s) { return (int)((s + 1) & 1); }
+__device__ __forceinline__ int cand_list(int64_t s) { return (int)((s + 2) % CAND_LISTS); }
 
 /* kernels (wq3d_kernels.cu).  Every kernel takes the queue descriptor by
  * value as a __grid_constant__ parameter, so its fields are read through

@@ -67,10 +67,10 @@ struct Roles {
 
 __device__ __forceinline__ void roles_at(const QueueDev& q, int64_t s,
                                          Roles& r) {
-    r.P = &q.F[s & 3];
-    r.V = &q.F[(s + 1) & 3];
-    r.C = &q.F[(s + 2) & 3];
-    r.X = &q.F[(s + 3) & 3];
+    r.P = &q.F[ring_slot(s + 4)];
+    r.V = &q.F[ring_slot(s + 1)];
+    r.C = &q.F[ring_slot(s + 2)];
+    r.X = &q.F[ring_slot(s + 3)];
 }
 
 __device__ __forceinline__ void set_err(const QueueDev& q, uint32_t bit) {
@@ -398,17 +398,11 @@ __device__ __noinline__ void volume_scatter(const QueueDev& q, const FrontPtrs& 
     }
 }
 
-/* The updates of the re-initialisation.  The analytic build inlines them
- * so that the five temporary rays stay in registers (out of line, each
- * update round-tripped a ray through local memory on the reflection
- * chain's critical path); in the gridded build the grid interpolation's
- * calls would then push the chain into register spills, so it keeps them
- * out of line. */
-#if WQ3D_WITH_GRID
+/* The updates of the re-initialisation, out of line: inlined, they keep
+ * the temporary rays in registers, but the larger code made k_reflect
+ * wait on instruction fetch (90.6 instead of 58.4 us per launch on the
+ * sloped workload, ncu: "no instruction" stalls 2.9 -> 10.1 per issue). */
 __device__ __noinline__ void reinit_update(const QueueDev& q, RayS& y) { update1(q, y); }
-#else
-__device__ __forceinline__ void reinit_update(const QueueDev& q, RayS& y) { update1(q, y); }
-#endif
 
 /* reflection_model::reflection_reinit on the private state */
 __device__ __noinline__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const double* pos,
@@ -751,7 +745,7 @@ __global__ void __launch_bounds__(128) k_startup(__grid_constant__ const QueueDe
     curr.plen[i] = 0.0;
     prev.plen[i] = 0.0;
     past.plen[i] = 0.0;
-    for (int f = 0; f < 4; ++f) {
+    for (int f = 0; f < RING; ++f) {
         const FrontPtrs& F = q.F[f];
         F.surface[i] = 0;
         F.bottom[i] = 0;
@@ -1253,9 +1247,9 @@ __device__ bool is_closest(const QueueDev& q, const FrontPtrs& V, const FrontPtr
 __global__ void __launch_bounds__(CPA_THREADS) k_cpa(__grid_constant__ const QueueDev q, int k) {
     __shared__ TgtS tile[CPA_TARGETS];
     const int64_t s = *q.d_base + k + 1; /* roles after this step's rotation */
-    const FrontPtrs& V = q.F[(s + 1) & 3];
-    const FrontPtrs& C = q.F[(s + 2) & 3];
-    const FrontPtrs& X = q.F[(s + 3) & 3];
+    const FrontPtrs& V = q.F[ring_slot(s + 1)];
+    const FrontPtrs& C = q.F[ring_slot(s + 2)];
+    const FrontPtrs& X = q.F[ring_slot(s + 3)];
     const int t0 = blockIdx.y * CPA_TARGETS;
     const int nt_tile = min(CPA_TARGETS, q.nt - t0);
     for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
@@ -1425,11 +1419,10 @@ __global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ co
     __shared__ uint16_t surv[F32_TARGETS];
     __shared__ int nsurv;
     __shared__ WarpQueue wq[CPA_THREADS / 32];
-    __shared__ uint16_t wsurv[CPA_THREADS / 32][F32_TARGETS];
     const int64_t s = *q.d_base + k + 1;
-    const FrontPtrs& V = q.F[(s + 1) & 3];
-    const FrontPtrs& C = q.F[(s + 2) & 3];
-    const FrontPtrs& X = q.F[(s + 3) & 3];
+    const FrontPtrs& V = q.F[ring_slot(s + 1)];
+    const FrontPtrs& C = q.F[ring_slot(s + 2)];
+    const FrontPtrs& X = q.F[ring_slot(s + 3)];
     if (q.nde < 3 || q.naz < 3 || q.nt <= 0) return;
     const int n_pa = (q.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ;
     const int de0 = (blockIdx.x / n_pa) * CPA_PATCH_DE;
@@ -1557,30 +1550,7 @@ __global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ co
             surv[atomicAdd(&nsurv, 1)] = (uint16_t)j;
         }
         __syncthreads();
-        /* the warp's own patch (4 D/E rows x 8 AZ columns, its ranges in
-         * red[w]) drops more of the block's targets with the same test */
-        int ns = 0;
-        {
-            const PatchGuard wx = patch_guard(&red[w][0], &red[w][8], W, c0);
-            const PatchGuard wv = patch_guard(&red[w][16], &red[w][24], W, c0);
-            const int nb = nsurv;
-            for (int j0 = 0; j0 < nb; j0 += 32) {
-                const int jj = j0 + lane;
-                bool keep = false;
-                int tj = 0;
-                if (jj < nb) {
-                    tj = surv[jj];
-                    const TgtW g = tw[tj];
-                    keep = !patch_rejects(g, &red[w][0], &red[w][8], wx) &&
-                           !patch_rejects(g, &red[w][16], &red[w][24], wv);
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (keep) wsurv[w][ns + __popc(m & lt)] = (uint16_t)tj;
-                ns += __popc(m);
-            }
-            __syncwarp();
-        }
-        const uint16_t* surv_w = wsurv[w];
+        const int ns = nsurv;
         int qn = 0;
         /* appends this lane's pair if "want"; finishes 32 at a time */
         auto push = [&](bool want, int j) {
@@ -1600,7 +1570,7 @@ __global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ co
         };
         int sidx = 0;
         for (; sidx + 1 < ns; sidx += 2) {
-            const int j0 = surv_w[sidx], j1 = surv_w[sidx + 1];
+            const int j0 = surv[sidx], j1 = surv[sidx + 1];
             const TgtW g0 = tw[j0], g1 = tw[j1];
             const float a0 = screen_dot(g0, dxc), a1 = screen_dot(g1, dxc);
             bool w0 = active && !(a0 < -gxc), w1 = active && !(a1 < -gxc);
@@ -1613,7 +1583,7 @@ __global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ co
             push(w1, j1);
         }
         if (sidx < ns) {
-            const int j = surv_w[sidx];
+            const int j = surv[sidx];
             const TgtW g = tw[j];
             bool want = active && !(screen_dot(g, dxc) < -gxc);
             if (want) want = !(screen_dot(g, dvc) < -gvc);
@@ -2199,9 +2169,9 @@ __global__ void __launch_bounds__(32 * EIG_WARPS) k_eigenray(__grid_constant__ c
     const uint32_t* cand = q.cand + (size_t)list * 2 * q.cap_cand;
     WarpBuild B;
     B.q = &q;
-    B.pV = &q.F[(s + 1) & 3];
-    B.pC = &q.F[(s + 2) & 3];
-    B.pX = &q.F[(s + 3) & 3];
+    B.pV = &q.F[ring_slot(s + 1)];
+    B.pC = &q.F[ring_slot(s + 2)];
+    B.pX = &q.F[ring_slot(s + 3)];
     B.lane = lane;
     B.sg = s_g[warp];
     const FrontPtrs& V = *B.pV;
