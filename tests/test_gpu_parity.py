@@ -97,7 +97,11 @@ def test_classic_ray_parity(engine):
     compare_eigenrays(q.take_eigenrays(), o.take_eigenrays())
 
 
-def compare_fronts(a, b, rel=1e-11):
+def compare_fronts(a, b, rel=1e-11, edges=True):
+    """every field of two front views; edges=False leaves out on_edge,
+    which for the next front is only computed at the start of the following
+    step (find_edges in detect_reflections, wave_queue.cc:197-216), so
+    after a step both hold flags left from an earlier step"""
     for name in ("rho", "theta", "phi", "sound_speed", "distance", "path_length"):
         x, y = getattr(a, name), getattr(b, name)
         scale = np.maximum(np.abs(y), 1e-300)
@@ -107,7 +111,7 @@ def compare_fronts(a, b, rel=1e-11):
     for k in range(3):
         x, y = a.ndirection[k], b.ndirection[k]
         assert np.max(np.abs(x - y)) <= rel * max(np.max(np.abs(y)), 1e-12), ("ndir", k)
-    for name in ("surface", "bottom", "caustic", "upper", "lower", "on_edge"):
+    for name in ("surface", "bottom", "caustic", "upper", "lower") + (("on_edge",) if edges else ()):
         assert np.array_equal(getattr(a, name), getattr(b, name)), name
     assert np.allclose(a.attenuation, b.attenuation, rtol=1e-9, atol=1e-12)
     assert np.allclose(a.phase, b.phase, rtol=0, atol=1e-9)
@@ -118,7 +122,7 @@ def test_munk_refraction_fronts(engine):
     sc = S.refraction_munk_range()
     q, o = run_pair(sc)
     for w in ("past", "prev", "curr", "next"):
-        compare_fronts(getattr(q, w)(), getattr(o, w)())
+        compare_fronts(getattr(q, w)(), getattr(o, w)(), edges=w != "next")
 
 
 def test_munk_refraction_known_answers(engine):

@@ -219,6 +219,8 @@ struct wq3d_queue {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;
     cudaStream_t eig = nullptr; /* k_commit and the eigenray construction */
+    cudaStream_t adv = nullptr; /* k_advance, checkpoints, volume eigenverbs */
+    cudaEvent_t start_ev = nullptr;
     std::vector<cudaEvent_t> fork_ev, join_ev;
     std::vector<cudaEvent_t> adv_ev, com_ev, cpa_ev; /* per step of a chunk */
     cudaEvent_t eig_end = nullptr;
@@ -452,6 +454,8 @@ struct wq3d_queue {
         for (auto* v : {&adv_ev, &com_ev, &cpa_ev})
             for (auto e : *v) cudaEventDestroy(e);
         if (eig_end) cudaEventDestroy(eig_end);
+        if (start_ev) cudaEventDestroy(start_ev);
+        if (adv) cudaStreamDestroy(adv);
         if (eig) cudaStreamDestroy(eig);
         if (side) cudaStreamDestroy(side);
         if (ev_begin) cudaEventDestroy(ev_begin);
@@ -485,10 +489,10 @@ struct wq3d_queue {
     }
 
     /* One chunk of K steps writing result set p.  Without per-kernel
-     * timing it runs on three streams:
-     *   main  k_advance(k) (after k_reflect(k)), then k_cpa(k); the adjoint's
-     *         checkpoint and the volume eigenverbs of a step run before its
-     *         advance
+     * timing it runs on four streams:
+     *   adv   k_advance(k) after k_reflect(k); the adjoint's checkpoint and
+     *         the volume eigenverbs of a step run before its advance
+     *   main  k_cpa(k) after k_advance(k), beside k_advance(k+1)
      *   side  k_reflect(k+1) (high priority), right after k_advance(k),
      *         beside k_cpa(k)
      *   eig   k_commit(k) after k_advance(k), k_eigenray(k) after k_cpa(k),
@@ -582,19 +586,23 @@ struct wq3d_queue {
             }
             return WQ3D_OK;
         }
+        cudaEventRecord(start_ev, stream);
+        cudaStreamWaitEvent(adv, start_ev, 0);
         for (int k = 0; k < K; ++k) {
-            /* main: step k's checkpoint, volume eigenverbs and advance */
+            /* adv: step k's checkpoint, volume eigenverbs and advance, after
+             * its reflections */
+            if (k >= 1) cudaStreamWaitEvent(adv, join_ev[k - 1], 0);
             if (h.adj) {
-                k_adj_checkpoint<<<grd, blk, 0, stream>>>(d, k);
+                k_adj_checkpoint<<<grd, blk, 0, adv>>>(d, k);
                 launches += 1;
             }
             if (volume_pass()) {
-                k_volume<<<grd, blk, 0, stream>>>(d, k);
+                k_volume<<<grd, blk, 0, adv>>>(d, k);
                 launches += 1;
             }
-            k_advance_fn<<<grd, blk, 0, stream>>>(d, k);
+            k_advance_fn<<<grd, blk, 0, adv>>>(d, k);
             launches += 1;
-            cudaEventRecord(adv_ev[k], stream);
+            cudaEventRecord(adv_ev[k], adv);
             /* eig: step k's commit */
             cudaStreamWaitEvent(eig, adv_ev[k], 0);
             k_commit<<<grd, blk, 0, eig>>>(d, k);
@@ -610,7 +618,9 @@ struct wq3d_queue {
                 cudaEventRecord(join_ev[k], side);
                 launches += 1;
             }
-            /* main: step k's CPA search; eig: its eigenray construction */
+            /* main: step k's CPA search (beside step k+1's advance);
+             * eig: its eigenray construction */
+            cudaStreamWaitEvent(stream, adv_ev[k], 0);
             if (h.nt > 0) {
                 cpa_launch(k, stream);
                 launches += 1;
@@ -618,11 +628,11 @@ struct wq3d_queue {
                 cudaStreamWaitEvent(eig, cpa_ev[k], 0);
                 eig_launch(k, eig);
             }
-            if (more) cudaStreamWaitEvent(stream, join_ev[k], 0);
         }
-        /* the eigenray stream joins the main stream */
+        /* every stream joins the main stream */
         cudaEventRecord(eig_end, eig);
         cudaStreamWaitEvent(stream, eig_end, 0);
+        if (tail) cudaStreamWaitEvent(stream, join_ev[K - 1], 0);
         return WQ3D_OK;
     }
 
@@ -1495,9 +1505,11 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) prio_high = 0;
         if (cudaStreamCreateWithPriority(&q->side, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->eig, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&q->adv, cudaStreamNonBlocking) != cudaSuccess ||
             cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaStreamCreate failed"));
-        if (cudaEventCreateWithFlags(&q->eig_end, cudaEventDisableTiming) != cudaSuccess)
+        if (cudaEventCreateWithFlags(&q->eig_end, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&q->start_ev, cudaEventDisableTiming) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaEventCreate failed"));
         for (auto& e : q->done_ev)
             if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
@@ -1528,7 +1540,7 @@ int wq3d_queue_destroy(wq3d_queue* q) {
     DeviceGuard guard(q->device);
     if (cacheable(q) && cudaStreamSynchronize(q->stream) == cudaSuccess &&
         cudaStreamSynchronize(q->side) == cudaSuccess && cudaStreamSynchronize(q->eig) == cudaSuccess &&
-        cudaStreamSynchronize(q->copy) == cudaSuccess) {
+        cudaStreamSynchronize(q->adv) == cudaSuccess && cudaStreamSynchronize(q->copy) == cudaSuccess) {
         wq3d_queue* drop = nullptr;
         {
             std::lock_guard<std::mutex> lock(g_cache_mu);

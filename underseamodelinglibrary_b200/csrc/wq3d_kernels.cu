@@ -1088,8 +1088,8 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
 }  // namespace WQ3D_KERNEL_NS
 
 #if !WQ3D_STEP_KERNELS_ONLY
-/* What k_advance of step s decided for the curr / next fronts, done after
- * the eigenray construction of step s-1 has read them: a reflected ray's
+/* What k_advance of step s decided for the prev / curr / next fronts, done
+ * after the eigenray construction of step s-1 has read them: a reflected ray's
  * states, counts and next-front losses from its shadow slot
  * (reflection_model::reflection_copy, reflection_model.cc:335-360), and for
  * the other rays the caustic hand-off (count, and phase - pi/2 on every
@@ -1108,19 +1108,21 @@ __global__ void __launch_bounds__(128) k_commit(__grid_constant__ const QueueDev
     Roles R;
     roles_at(q, s, R);
     if (b & COMMIT_REFLECT) {
-        /* the reflected prev state is only used by this step's AB3, which
-         * took it from the slot; the prev front becomes this step's new
-         * front */
+        /* the prev front is read by no later kernel (this step's AB3 took
+         * the reflected prev state from the slot) but is the "past" front
+         * a caller may look at after the step */
         const int32_t w = q.shadow_slot[set][i];
         const double* sh = q.shadow[set] + (size_t)w * shadow_stride(q);
         const int32_t* cnt = q.shadow_cnt[set] + 3 * (size_t)w;
         RayS y;
+        ray_from(sh, y);
+        copy_ray(*R.V, i, y);
         ray_from(sh + 17, y);
         copy_ray(*R.C, i, y);
         ray_from(sh + 34, y);
         copy_ray(*R.X, i, y);
-        R.C->surface[i] = R.X->surface[i] = cnt[0];
-        R.C->bottom[i] = R.X->bottom[i] = cnt[1];
+        R.V->surface[i] = R.C->surface[i] = R.X->surface[i] = cnt[0];
+        R.V->bottom[i] = R.C->bottom[i] = R.X->bottom[i] = cnt[1];
         R.X->caustic[i] = cnt[2];
         for (int f = 0; f < q.nf; ++f) {
             R.X->atten[(size_t)f * q.n + i] = sh[51 + f];
