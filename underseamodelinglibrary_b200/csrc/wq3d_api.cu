@@ -1390,7 +1390,12 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         if (!reuse && (rc = q->alloc(&base, RING * per_front + 2 * bbytes))) return cleanup(rc);
         q->ring = base;
         q->ring_bytes = RING * per_front + 2 * bbytes;
-        if (cudaMemset(base, 0, RING * per_front + 2 * bbytes) != cudaSuccess)
+        /* only the reflection flags need zeros: the start-up writes every
+         * field of the first four fronts and the counters and edge flags of
+         * all five, and the first step writes the fifth before it is read
+         * (zeroing the whole ring cost the 512-queue batch seconds of its
+         * build) */
+        if (cudaMemset(base + RING * per_front, 0, 2 * bbytes) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
         char* p = base;
         auto dtake = [&](size_t count) {
