@@ -820,8 +820,9 @@ constexpr int JAC_WARPS = 2;
 struct WalkCells {
     double w[ADJ_MAX_CELLS];
     double nm[ADJ_MAX_CELLS];
-    double cd[ADJ_MAX_CELLS];
-    double cw[ADJ_MAX_CELLS];
+    double cd[ADJ_MAX_CELLS];  /* cell distance, then d G / d distance   */
+    double cw[ADJ_MAX_CELLS];  /* cell width, then d G / d width         */
+    double p2[ADJ_MAX_CELLS];  /* d G / d spread2                        */
     int16_t d[ADJ_MAX_CELLS];
     int16_t a[ADJ_MAX_CELLS];
     uint8_t kind[ADJ_MAX_CELLS]; /* 0 width_de, 1 width_az */
@@ -834,30 +835,18 @@ struct Run {
     double sign;
 };
 
+/* The pieces of one eigenray's beam walks (spreading_hybrid_gaussian.cc:
+ * 124-425) the adjoint needs: the first frequency's Gaussian term and the
+ * cell widths.  WarpWalker runs the walks with them. */
 struct Walker {
     const QueueDev* q;
     FrontAcc A;
     WalkCells* wc;
-    int n;            /* cells recorded */
-    bool overflow;
     double s2;        /* spread2 of the first frequency */
 
     __device__ double gauss(double d, double w, double nm) const {
         const double bw = s2 + 2.0 * 2.0 * w * w;
         return ::exp((-0.5 * d * d) / bw) / ::sqrt(bw) * nm;
-    }
-    __device__ int add(int kind, int d, int a, double w, double nm, bool virt) {
-        if (n >= ADJ_MAX_CELLS) {
-            overflow = true;
-            return ADJ_MAX_CELLS - 1;
-        }
-        wc->w[n] = w;
-        wc->nm[n] = nm;
-        wc->d[n] = (int16_t)d;
-        wc->a[n] = (int16_t)a;
-        wc->kind[n] = (uint8_t)kind;
-        wc->virt[n] = virt ? 1 : 0;
-        return n++;
     }
     __device__ double wde(int d, int a, const double* no) {
         double g[3] = {0.0, 0.0, 0.0};
@@ -867,56 +856,170 @@ struct Walker {
         double g[3] = {0.0, 0.0, 0.0};
         return width_az_vjp(*q, A, d, a, no, 0.0, g, NoSink());
     }
+};
+
+/* One eigenray's beam walks (intensity_de / intensity_az,
+ * spreading_hybrid_gaussian.cc:124-425, first frequency) on a whole warp,
+ * as k_eigenray's WarpBuild runs them: the widths of up to 32 cells are
+ * formed on the lanes at once, then the cell distances, the running
+ * intensity and its threshold test follow in cell order (shuffles), so the
+ * cells kept and every sum are those of the forward construction.  Cells
+ * go to wc in walk order, each lane writing its own.  All lanes call every
+ * member with the same arguments. */
+struct WarpWalker {
+    Walker W;
+    int lane;
+    int n;
+    bool overflow;
+
+    __device__ double sh(double v, int k) const { return __shfl_sync(0xffffffffu, v, k); }
+
+    /* ncell prepared cells (lane j: width w_j, norm nm_j, virtual v_j) of a
+     * run with sign s.  Advances cell_dist / cell_width and I in cell
+     * order, records the cells up to the stop and returns whether the walk
+     * stops here (threshold, a virtual cell or a full record).  "kstop" is
+     * the cell (in this chunk) the threshold stopped on, or -1. */
+    __device__ bool run(int ncell, int kind, int d_j, int a_j, double w_j, double nm_j, bool v_j,
+                        double sign, double& cell_dist, double& cell_width, double& I, int& kstop) {
+        kstop = -1;
+        double my_cd = 0.0, my_cw = 0.0;
+        int nend = ncell;
+        bool stop = false;
+        for (int k = 0; k < ncell; ++k) {
+            const bool v = __shfl_sync(0xffffffffu, v_j, k);
+            const double wk = sh(w_j, k);
+            if (sign > 0.0) {
+                cell_dist += cell_width;
+                if (v) {
+                    cell_dist += cell_width;
+                } else {
+                    cell_width = wk;
+                    cell_dist += cell_width;
+                }
+            } else {
+                cell_dist -= cell_width;
+                if (v) {
+                    cell_dist -= cell_width;
+                } else {
+                    cell_width = wk;
+                    cell_dist -= cell_width;
+                }
+            }
+            if (lane == k) {
+                my_cd = cell_dist;
+                my_cw = cell_width;
+            }
+            if (v) {
+                nend = k + 1;
+                stop = true;
+                break;
+            }
+        }
+        /* room in the record: a full record stops the walk (its eigenray is
+         * then flagged and carries no gradient) */
+        if (n + nend > ADJ_MAX_CELLS) {
+            nend = ADJ_MAX_CELLS - n;
+            overflow = true;
+            stop = true;
+        }
+        const double g = (lane < nend) ? W.gauss(my_cd, my_cw, nm_j) : 0.0;
+        int kstar = nend - 1;
+        for (int k = 0; k < nend; ++k) {
+            const double old = I;
+            I = I + sh(g, k);
+            if (I / old < 1.002305238) {
+                kstar = k;
+                kstop = k;
+                stop = true;
+                break;
+            }
+        }
+        if (lane <= kstar && lane < nend) {
+            const int c = n + lane;
+            W.wc->w[c] = w_j;
+            W.wc->nm[c] = nm_j;
+            W.wc->cd[c] = my_cd;
+            W.wc->cw[c] = my_cw;
+            W.wc->d[c] = (int16_t)d_j;
+            W.wc->a[c] = (int16_t)a_j;
+            W.wc->kind[c] = (uint8_t)kind;
+            W.wc->virt[c] = v_j ? 1 : 0;
+        }
+        n += (nend > 0) ? kstar + 1 : 0;
+        return stop;
+    }
+
+    /* the start cells of a walk (center and lower neighbour) */
+    __device__ void start(int kind, int dc, int ac, double wcv, double nmc, int dl, int al, double wlv, double nml) {
+        if (n + 2 > ADJ_MAX_CELLS) {
+            overflow = true;
+            return;
+        }
+        if (lane == 0) {
+            W.wc->w[n] = wcv;
+            W.wc->nm[n] = nmc;
+            W.wc->d[n] = (int16_t)dc;
+            W.wc->a[n] = (int16_t)ac;
+            W.wc->kind[n] = (uint8_t)kind;
+            W.wc->virt[n] = 0;
+            W.wc->w[n + 1] = wlv;
+            W.wc->nm[n + 1] = nml;
+            W.wc->d[n + 1] = (int16_t)dl;
+            W.wc->a[n + 1] = (int16_t)al;
+            W.wc->kind[n + 1] = (uint8_t)kind;
+            W.wc->virt[n + 1] = 0;
+        }
+        n += 2;
+    }
 
     /* intensity_de (spreading_hybrid_gaussian.cc:124-258) */
     __device__ double walk_de(int de0, int a, const double* no, double L, Run* runs) {
-        const QueueDev& Q = *q;
-        const FrontPtrs& C = *A.F[1];
-        const int i_c = add(0, de0, a, wde(de0, a, no), Q.norm_de[de0], false);
-        const int i_l = add(0, de0 - 1, a, wde(de0 - 1, a, no), Q.norm_de[de0 - 1], false);
-        const double wcv = wc->w[i_c], wlv = wc->w[i_l];
-        double I = gauss(L - wcv, wcv, wc->nm[i_c]);
-        I = I + gauss(L + wlv, wlv, wc->nm[i_l]);
+        const QueueDev& Q = *W.q;
+        const FrontPtrs& C = *W.A.F[1];
+        double wcv = 0.0, wlv = 0.0;
+        if (lane == 0) wcv = W.wde(de0, a, no);
+        if (lane == 1) wlv = W.wde(de0 - 1, a, no);
+        wcv = sh(wcv, 0);
+        wlv = sh(wlv, 1);
+        const int i_c = n, i_l = n + 1;
+        start(0, de0, a, wcv, Q.norm_de[de0], de0 - 1, a, wlv, Q.norm_de[de0 - 1]);
+        double I = W.gauss(L - wcv, wcv, Q.norm_de[de0]);
+        I = I + W.gauss(L + wlv, wlv, Q.norm_de[de0 - 1]);
         runs[0] = Run{i_l, n, n, 1.0};
         runs[1] = Run{i_c, n, n, -1.0};
         if (I < 1e-10) return I;
         double cell_width = wlv, cell_dist = L + wlv;
-        for (int d = de0 - 2; d >= 0; --d) {
-            const bool virt = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
-            const double w = virt ? 0.0 : wde(d, a, no);
-            const int k = add(0, d, a, w, virt ? Q.norm_de[d + 1] : Q.norm_de[d], virt);
-            cell_dist += cell_width;
-            if (virt) {
-                cell_dist += cell_width;
-            } else {
-                cell_width = w;
-                cell_dist += cell_width;
+        int kst;
+        for (int d0 = de0 - 2; d0 >= 0; d0 -= 32) {
+            const int d = d0 - lane;
+            const int ncell = min(32, d0 + 1);
+            bool virt = false;
+            double w = 0.0, nm = 0.0;
+            if (lane < ncell) {
+                virt = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
+                if (!virt) w = W.wde(d, a, no);
+                nm = virt ? Q.norm_de[d + 1] : Q.norm_de[d];
             }
-            const double g = gauss(cell_dist, cell_width, wc->nm[k]);
-            const double old = I;
-            I = I + g;
-            if (I / old < 1.002305238 || virt || overflow) break;
+            if (run(ncell, 0, d, a, w, nm, virt, 1.0, cell_dist, cell_width, I, kst)) break;
         }
         runs[0].e = n;
         runs[1].b = runs[1].e = n;
         cell_width = wcv;
         cell_dist = L - wcv;
         const int size = Q.nde - 1;
-        for (int d = de0 + 1; d < size; ++d) {
-            const bool virt = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
-            const double w = virt ? 0.0 : wde(d, a, no);
-            const int k = add(0, d, a, w, virt ? Q.norm_de[d - 1] : Q.norm_de[d], virt);
-            cell_dist -= cell_width;
-            if (virt) {
-                cell_dist -= cell_width;
-            } else {
-                cell_width = w;
-                cell_dist -= cell_width;
+        if (!overflow) {
+            for (int d0 = de0 + 1; d0 < size; d0 += 32) {
+                const int d = d0 + lane;
+                const int ncell = min(32, size - d0);
+                bool virt = false;
+                double w = 0.0, nm = 0.0;
+                if (lane < ncell) {
+                    virt = C.on_edge[(d + 1) * Q.naz + a] && C.on_edge[d * Q.naz + a];
+                    if (!virt) w = W.wde(d, a, no);
+                    nm = virt ? Q.norm_de[d - 1] : Q.norm_de[d];
+                }
+                if (run(ncell, 0, d, a, w, nm, virt, -1.0, cell_dist, cell_width, I, kst)) break;
             }
-            const double g = gauss(cell_dist, cell_width, wc->nm[k]);
-            const double old = I;
-            I = I + g;
-            if (I / old < 1.002305238 || virt || overflow) break;
         }
         runs[1].e = n;
         return I;
@@ -924,115 +1027,139 @@ struct Walker {
 
     /* intensity_az (spreading_hybrid_gaussian.cc:264-425) */
     __device__ double walk_az(int d, int az0, const double* no, double L, Run* runs) {
-        const QueueDev& Q = *q;
-        const FrontPtrs& C = *A.F[1];
+        const QueueDev& Q = *W.q;
+        const FrontPtrs& C = *W.A.F[1];
         const int max_de = Q.nde - 2;
         const int max_az = Q.naz - 1;
         const int az_lower = Q.az_boundary ? az0 : 0;
         const int az_upper = Q.az_boundary ? az0 : max_az - 1;
         auto norm = [&](int aa) { return (d >= max_de) ? Q.norm_az[1 * Q.naz + aa] : Q.norm_az[d * Q.naz + aa]; };
         const int a1 = (az0 < 1) ? max_az - 1 : az0 - 1;
-        const int i_c = add(1, d, az0, waz(d, az0, no), norm(az0), false);
-        const int i_l = add(1, d, a1, waz(d, a1, no), norm(a1), false);
-        const double wcv = wc->w[i_c], wlv = wc->w[i_l];
-        double I = gauss(L - wcv, wcv, wc->nm[i_c]);
-        I = I + gauss(L + wlv, wlv, wc->nm[i_l]);
+        double wcv = 0.0, wlv = 0.0;
+        if (lane == 0) wcv = W.waz(d, az0, no);
+        if (lane == 1) wlv = W.waz(d, a1, no);
+        wcv = sh(wcv, 0);
+        wlv = sh(wlv, 1);
+        const int i_c = n, i_l = n + 1;
+        start(1, d, az0, wcv, norm(az0), d, a1, wlv, norm(a1));
+        double I = W.gauss(L - wcv, wcv, norm(az0));
+        I = I + W.gauss(L + wlv, wlv, norm(a1));
         runs[0] = Run{i_l, n, n, 1.0};
         runs[1] = Run{i_c, n, n, -1.0};
         if (I < 1e-10) return I;
-        const int start = (a1 < 1) ? max_az - 1 : a1 - 1;
+        const int start_a = (a1 < 1) ? max_az - 1 : a1 - 1;
         double cell_width = wlv, cell_dist = L + wlv;
         int marked = -1;
-        for (int k = 0; k < max_az; ++k) {
-            int a = start - k;
+        bool done = false;
+        for (int k0 = 0; !done && k0 < max_az; k0 += 32) {
+            const int kk = k0 + lane;
+            int a = start_a - kk;
             a = ((a % max_az) + max_az) % max_az;
-            if (a == az_lower) break;
-            if (a == az0 || a == a1) break;
-            if (C.on_edge[d * Q.naz + a]) {
-                marked = k;
-                break;
+            int kind = 0; /* 0 process, 1 loop end (not marked), 2 marked stop */
+            if (kk >= max_az || a == az_lower) {
+                kind = 1;
+            } else if (a == az0 || a == a1) {
+                kind = 1;
+            } else if (C.on_edge[d * Q.naz + a]) {
+                kind = 2;
             }
-            const double w = waz(d, a, no);
-            const int c = add(1, d, a, w, norm(a), false);
-            cell_dist += cell_width;
-            cell_width = w;
-            cell_dist += cell_width;
-            const double g = gauss(cell_dist, cell_width, wc->nm[c]);
-            const double old = I;
-            I = I + g;
-            marked = k;
-            if (I / old < 1.002305238 || overflow) break;
+            const unsigned stopmask = __ballot_sync(0xffffffffu, kind != 0);
+            int first = 32, fk = 0;
+            if (stopmask) {
+                first = __ffs(stopmask) - 1;
+                fk = __shfl_sync(0xffffffffu, kind, first);
+            }
+            const int ncell = first;
+            double w = 0.0, nm = 0.0;
+            if (lane < ncell) {
+                w = W.waz(d, a, no);
+                nm = norm(a);
+            }
+            int kst = -1;
+            const bool brk = (ncell > 0) && run(ncell, 1, d, a, w, nm, false, 1.0, cell_dist, cell_width, I, kst);
+            if (brk) {
+                marked = (kst >= 0) ? k0 + kst : k0 + ncell - 1;
+                done = true;
+            } else {
+                if (ncell > 0) marked = k0 + ncell - 1;
+                if (stopmask) {
+                    done = true;
+                    if (fk == 2) marked = k0 + first;
+                }
+            }
         }
         runs[0].e = n;
         runs[1].b = runs[1].e = n;
         cell_width = wcv;
         cell_dist = L - wcv;
-        for (int k = 0; k < max_az; ++k) {
-            const int a = (az0 + 1 + k) % max_az;
-            const int off = ((start - a) % max_az + max_az) % max_az;
+        done = overflow;
+        for (int k0 = 0; !done && k0 < max_az; k0 += 32) {
+            const int kk = k0 + lane;
+            const int a = (az0 + 1 + kk) % max_az;
+            int kind = 0;
+            const int off = ((start_a - a) % max_az + max_az) % max_az;
             const bool dup = (a == az0) || (a == a1) || (marked >= 0 && off <= marked);
-            if (a == az_upper || dup || C.on_edge[d * Q.naz + a]) break;
-            const double w = waz(d, a, no);
-            const int c = add(1, d, a, w, norm(a), false);
-            cell_dist -= cell_width;
-            cell_width = w;
-            cell_dist -= cell_width;
-            const double g = gauss(cell_dist, cell_width, wc->nm[c]);
-            const double old = I;
-            I = I + g;
-            if (I / old < 1.002305238 || overflow) break;
+            if (kk >= max_az || a == az_upper || dup || C.on_edge[d * Q.naz + a]) kind = 1;
+            const unsigned stopmask = __ballot_sync(0xffffffffu, kind != 0);
+            int ncell = 32;
+            if (stopmask) {
+                ncell = __ffs(stopmask) - 1;
+                done = true;
+            }
+            double w = 0.0, nm = 0.0;
+            if (lane < ncell) {
+                w = W.waz(d, a, no);
+                nm = norm(a);
+            }
+            int kst = -1;
+            if (ncell > 0 && run(ncell, 1, d, a, w, nm, false, -1.0, cell_dist, cell_width, I, kst)) done = true;
         }
         runs[1].e = n;
         return I;
     }
 
     /* reverse of one run: dI/d (cell widths) into gwid, dI/dL returned,
-     * dI/d spread2 added to gs2; gI = dTL/dI */
-    __device__ double reverse_run(const Run& r, double L, double gI, double* gwid, double& gs2) const {
-        double Acd = 0.0, Acw_next = 0.0;
+     * dI/d spread2 added to gs2, for gI = dTL/dI.  The Gaussian's partials
+     * of every cell are formed on the lanes, then the adjoint recurrence
+     * runs in cell order on lane 0 (gwid, gs2 and the returned value are
+     * lane 0's) */
+    __device__ double reverse_run(const Run& r, double L, double gI, double* gwid, double& gs2) {
+        WalkCells* wc = W.wc;
         const double s = r.sign;
-        /* the G partials at (cd, cw, nm) */
-        auto partials = [&](double cd, double cw, double nm, double& gcd, double& gcw) {
-            const double bw = s2 + 2.0 * 2.0 * cw * cw;
-            const double G = ::exp((-0.5 * cd * cd) / bw) / ::sqrt(bw) * nm;
+        for (int k = r.b + lane; k < r.e; k += 32) {
+            const double cd = wc->cd[k], cw = wc->cw[k];
+            const double bw = W.s2 + 2.0 * 2.0 * cw * cw;
+            const double G = ::exp((-0.5 * cd * cd) / bw) / ::sqrt(bw) * wc->nm[k];
             const double gbw = G * (0.5 * cd * cd / (bw * bw) - 0.5 / bw);
-            gcd = gI * (-G * cd / bw);
-            gcw = gI * gbw * 8.0 * cw;
-            gs2 += gI * gbw;
-        };
-        /* forward values of the run: cd_k, cw_k */
-        double cw0 = wc->w[r.s0], cd0 = L + s * cw0;
-        {
-            double cw = cw0, cd = cd0;
-            for (int k = r.b; k < r.e; ++k) {
-                cd += s * cw;
+            wc->cd[k] = -G * cd / bw;
+            wc->cw[k] = gbw * 8.0 * cw;
+            wc->p2[k] = gbw;
+        }
+        __syncwarp();
+        double Acd = 0.0;
+        if (lane == 0) {
+            double Acw_next = 0.0;
+            for (int k = r.e - 1; k >= r.b; --k) {
+                Acd = gI * wc->cd[k] + Acd;
+                const double Acw = gI * wc->cw[k] + Acw_next;
+                gs2 += gI * wc->p2[k];
                 if (wc->virt[k]) {
-                    cd += s * cw;
+                    Acw_next = Acw + 2.0 * s * Acd;
                 } else {
-                    cw = wc->w[k];
-                    cd += s * cw;
+                    gwid[k] += Acw + s * Acd;
+                    Acw_next = s * Acd;
                 }
-                wc->cd[k] = cd;
-                wc->cw[k] = cw;
             }
+            const double cw0 = wc->w[r.s0], cd0 = L + s * cw0;
+            const double bw = W.s2 + 2.0 * 2.0 * cw0 * cw0;
+            const double G = ::exp((-0.5 * cd0 * cd0) / bw) / ::sqrt(bw) * wc->nm[r.s0];
+            const double gbw = G * (0.5 * cd0 * cd0 / (bw * bw) - 0.5 / bw);
+            Acd = gI * (-G * cd0 / bw) + Acd;
+            const double Acw = gI * gbw * 8.0 * cw0 + Acw_next;
+            gs2 += gI * gbw;
+            gwid[r.s0] += Acw + s * Acd;
         }
-        for (int k = r.e - 1; k >= r.b; --k) {
-            double gcd, gcw;
-            partials(wc->cd[k], wc->cw[k], wc->nm[k], gcd, gcw);
-            Acd = gcd + Acd;
-            const double Acw = gcw + Acw_next;
-            if (wc->virt[k]) {
-                Acw_next = Acw + 2.0 * s * Acd;
-            } else {
-                gwid[k] += Acw + s * Acd;
-                Acw_next = s * Acd;
-            }
-        }
-        double gcd, gcw;
-        partials(cd0, cw0, wc->nm[r.s0], gcd, gcw);
-        Acd = gcd + Acd;
-        const double Acw = gcw + Acw_next;
-        gwid[r.s0] += Acw + s * Acd;
+        __syncwarp();
         return Acd;
     }
 };
@@ -1136,7 +1263,7 @@ __global__ void __launch_bounds__(32 * JAC_WARPS) k_eigenray_jac(__grid_constant
                 dth[3 + m] = dd[m].d[0];
             }
         }
-        /* lane 0: the walks forward and in reverse */
+        /* the walks forward and in reverse, on the whole warp */
         AdjRec* out = nullptr;
         uint32_t slot = 0;
         if (lane == 0) {
@@ -1146,37 +1273,46 @@ __global__ void __launch_bounds__(32 * JAC_WARPS) k_eigenray_jac(__grid_constant
         slot = __shfl_sync(0xffffffffu, slot, 0);
         if (slot >= q.adj_cap) continue;
         out = q.adj_rec + slot;
-        if (lane == 0) {
-            Walker W;
-            W.q = &q;
-            W.A.F[0] = &V;
-            W.A.F[1] = &C;
-            W.A.F[2] = &X;
-            W.wc = &s_cells[warp];
-            W.n = 0;
-            W.overflow = false;
-            W.s2 = q.tgt_spread2[(size_t)t * q.nf];
-            /* spreading_hybrid_gaussian.cc:65-119 */
-            int a = az0;
-            double no_de[3] = {off[0], off[1], off[2]};
-            if (off[2] < 0.0) {
-                if (az0 > 0) {
-                    a = az0 - 1;
-                } else if (q.az_boundary) {
-                    a = q.naz - 2;
-                }
-                no_de[2] = off[2] + q.az_inc[min(max(a, 0), q.naz - 1)];
+        WarpWalker WW;
+        WW.W.q = &q;
+        WW.W.A.F[0] = &V;
+        WW.W.A.F[1] = &C;
+        WW.W.A.F[2] = &X;
+        WW.W.wc = &s_cells[warp];
+        WW.W.s2 = q.tgt_spread2[(size_t)t * q.nf];
+        WW.lane = lane;
+        WW.n = 0;
+        WW.overflow = false;
+        /* spreading_hybrid_gaussian.cc:65-119 */
+        int a = az0;
+        double no_de[3] = {off[0], off[1], off[2]};
+        if (off[2] < 0.0) {
+            if (az0 > 0) {
+                a = az0 - 1;
+            } else if (q.az_boundary) {
+                a = q.naz - 2;
             }
-            double no_az[3] = {off[0], off[1], off[2]};
-            int d = de0;
-            if (off[1] < 0.0 && !C.on_edge[i - q.naz]) {
-                d = de0 - 1;
-                no_az[1] = off[1] + q.de_inc[min(max(d, 0), q.nde - 1)];
-            }
-            Run rde[2], raz[2];
-            const double Ide = W.walk_de(de0, a, no_de, dist[1], rde);
-            const int n_de = W.n;
-            const double Iaz = W.walk_az(d, az0, no_az, dist[2], raz);
+            no_de[2] = off[2] + q.az_inc[min(max(a, 0), q.naz - 1)];
+        }
+        double no_az[3] = {off[0], off[1], off[2]};
+        int d = de0;
+        if (off[1] < 0.0 && !C.on_edge[i - q.naz]) {
+            d = de0 - 1;
+            no_az[1] = off[1] + q.de_inc[min(max(d, 0), q.nde - 1)];
+        }
+        Run rde[2], raz[2];
+        const double Ide = WW.walk_de(de0, a, no_de, dist[1], rde);
+        const int n_de = WW.n;
+        const double Iaz = WW.overflow ? 0.0 : WW.walk_az(d, az0, no_az, dist[2], raz);
+        __syncwarp();
+        const bool ovf = WW.overflow;
+        const int ncells = min(WW.n, ADJ_MAX_CELLS);
+        double* gw = s_gw[warp];
+        for (int c = lane; c < ncells; c += 32) gw[c] = 0.0;
+        __syncwarp();
+        double gs2 = 0.0, gL_de = 0.0, gL_az = 0.0;
+        double g_no_de[3] = {0.0, 0.0, 0.0}, g_no_az[3] = {0.0, 0.0, 0.0};
+        if (!ovf) {
             const double si = Ide * Iaz;
             double gI_de = 0.0, gI_az = 0.0;
             if (si > 1e-30) {
@@ -1184,22 +1320,44 @@ __global__ void __launch_bounds__(32 * JAC_WARPS) k_eigenray_jac(__grid_constant
                 gI_de = gsi * Iaz;
                 gI_az = gsi * Ide;
             }
-            double* gw = s_gw[warp];
-            for (int c = 0; c < W.n; ++c) gw[c] = 0.0;
-            double gs2 = 0.0;
-            const double gL_de = W.reverse_run(rde[0], dist[1], gI_de, gw, gs2) +
-                                 W.reverse_run(rde[1], dist[1], gI_de, gw, gs2);
-            const double gL_az = W.reverse_run(raz[0], dist[2], gI_az, gw, gs2) +
-                                 W.reverse_run(raz[1], dist[2], gI_az, gw, gs2);
-            /* width derivatives with respect to the offsets they blend with */
-            double g_no_de[3] = {0.0, 0.0, 0.0}, g_no_az[3] = {0.0, 0.0, 0.0};
-            for (int c = 0; c < W.n; ++c) {
-                if (W.wc->virt[c] || gw[c] == 0.0) continue;
+            gL_de = WW.reverse_run(rde[0], dist[1], gI_de, gw, gs2);
+            gL_de = gL_de + WW.reverse_run(rde[1], dist[1], gI_de, gw, gs2);
+            gL_az = WW.reverse_run(raz[0], dist[2], gI_az, gw, gs2);
+            gL_az = gL_az + WW.reverse_run(raz[1], dist[2], gI_az, gw, gs2);
+            /* width derivatives with respect to the offsets they blend
+             * with, one cell per lane */
+            for (int c = lane; c < ncells; c += 32) {
+                if (WW.W.wc->virt[c] || gw[c] == 0.0) continue;
                 if (c < n_de)
-                    width_de_vjp(q, W.A, W.wc->d[c], W.wc->a[c], no_de, gw[c], g_no_de, NoSink());
+                    width_de_vjp(q, WW.W.A, WW.W.wc->d[c], WW.W.wc->a[c], no_de, gw[c], g_no_de, NoSink());
                 else
-                    width_az_vjp(q, W.A, W.wc->d[c], W.wc->a[c], no_az, gw[c], g_no_az, NoSink());
+                    width_az_vjp(q, WW.W.A, WW.W.wc->d[c], WW.W.wc->a[c], no_az, gw[c], g_no_az, NoSink());
             }
+            for (int m = 0; m < 3; ++m)
+                for (int o = 16; o > 0; o >>= 1) {
+                    g_no_de[m] += __shfl_xor_sync(0xffffffffu, g_no_de[m], o);
+                    g_no_az[m] += __shfl_xor_sync(0xffffffffu, g_no_az[m], o);
+                }
+        }
+        /* the cells the walks used, in walk order */
+        int nc = 0;
+        {
+            const unsigned lt = (1u << lane) - 1u;
+            for (int c0 = 0; c0 < ncells; c0 += 32) {
+                const int c = c0 + lane;
+                const bool keep = !ovf && c < ncells && !WW.W.wc->virt[c] && gw[c] != 0.0;
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int o = nc + __popc(m & lt);
+                    out->cell_d[o] = WW.W.wc->d[c];
+                    out->cell_a[o] = WW.W.wc->a[c];
+                    out->cell_kind[o] = WW.W.wc->kind[c];
+                    out->cell_g[o] = gw[c];
+                }
+                nc += __popc(m);
+            }
+        }
+        if (lane == 0) {
             /* attenuation interpolated in time (build_eigenray) */
             double ddt = off[0] / q.dt;
             const int ra0 = (ddt >= 0.0) ? 1 : 0, ra1 = (ddt >= 0.0) ? 2 : 1;
@@ -1216,18 +1374,8 @@ __global__ void __launch_bounds__(32 * JAC_WARPS) k_eigenray_jac(__grid_constant
             out->step = s;
             out->t = t;
             out->i = i;
-            out->ncell = 0;
-            int nc = 0;
-            for (int c = 0; c < W.n; ++c) {
-                if (W.wc->virt[c] || gw[c] == 0.0) continue;
-                out->cell_d[nc] = W.wc->d[c];
-                out->cell_a[nc] = W.wc->a[c];
-                out->cell_kind[nc] = W.wc->kind[c];
-                out->cell_g[nc] = gw[c];
-                ++nc;
-            }
             out->ncell = nc;
-            out->flags = W.overflow ? ADJ_CELL_OVERFLOW : ADJ_VALID;
+            out->flags = ovf ? ADJ_CELL_OVERFLOW : ADJ_VALID;
             out->a_de = a;
             out->d_az = d;
             out->role_a0 = ra0;
