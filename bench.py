@@ -261,6 +261,15 @@ def engine_arm(args, rank, world, dist):
     f64_total, _, f64_neig = timed_runs(_abi.FP64, 1)
     kern64 = kernel_breakdown(_abi.FP64)
     cpa_ms = kern["cpa"]
+    # the FP32 propagation form: speed, and its eigenrays against the FP64
+    # form's on the same workload
+    f32_total, _, f32_neig = timed_runs(_abi.FP32, 1)
+    from underseamodelinglibrary_b200.eigenrays import form_errors
+    q64, q32 = make(_abi.FP64), make(_abi.FP32)
+    q64.run(sc["time_max"])
+    q32.run(sc["time_max"])
+    f32_err = form_errors(q32.take_eigenrays(), q64.take_eigenrays())
+    del q64, q32
 
     # end to end through the public API with host buffers
     e2e_times = []
@@ -299,13 +308,18 @@ def engine_arm(args, rank, world, dist):
         "config": {"workload": WORKLOAD, "rays": nde * naz, "num_de": nde, "num_az": naz,
                    "targets": nt, "frequencies": sc["freq"].size(), "wave_steps": nsteps,
                    "form": "FP32C (FP32-screened CPA, FP64 state)", "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "working set (4 fronts, %.0f MB) exceeds L2" % (nde * naz * 4 * 30 * 8 / 1e6)},
+                   "l2": "working set (5 fronts, %.0f MB) exceeds L2" % (nde * naz * 5 * 32 * 8 / 1e6)},
         "eigenrays_per_s": world * n_eig / total_s,
         "e2e": {"value": e2e, "unit": "ray-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "fp64_form": {"value": ray_steps / (f64_total / 1000.0), "ms_per_step": f64_total,
                       "kernel_ms": kern64, "eigenrays": f64_neig},
+        "fp32_form": {"value": ray_steps / (f32_total / 1000.0), "ms_per_step": f32_total,
+                      "vs_fp64_form": f64_total / f32_total, "eigenrays": f32_neig,
+                      "form": "FP32 sound speed, gradient and ray derivatives at the altitude offset; "
+                              "FP64 state, travel time, distance terms and CPA fit; FP32-screened CPA",
+                      "errors_vs_fp64_form": f32_err},
         "eigenrays_per_propagation": n_eig / args.steps,
         "kernel_ms": kern,
         "roofline": {"bound": "fp32", "achieved": achieved,

@@ -231,7 +231,16 @@ int wq3d_ocean_sound_speed_noalloc(const wq3d_ocean* ocean, double earth_radius,
 /* ------------------------------------------------------------------ */
 
 enum { WQ3D_CLASSIC_RAY = 0, WQ3D_HYBRID_GAUSSIAN = 1 }; /* wave_queue.h:90 */
-enum { WQ3D_FP64 = 0, WQ3D_FP32C = 1 };                   /* arithmetic form */
+/* Arithmetic form.  WQ3D_FP64: the reference's FP64 arithmetic throughout.
+ * WQ3D_FP32C: the same, with the CPA search's comparisons screened in FP32
+ * and finished in FP64 where the screen cannot decide (the eigenrays equal
+ * the FP64 form's bit for bit).  WQ3D_FP32: additionally the sound speed,
+ * its gradient and the ray derivatives of every wave_front::update
+ * (wave_front.cc:125-178) in FP32, at the altitude offset rho - R, while
+ * positions, directions, travel time, the distance terms and the CPA
+ * Taylor fit stay FP64; its error against the FP64 form is measured, not
+ * zero.  The adjoint is refused for WQ3D_FP32. */
+enum { WQ3D_FP64 = 0, WQ3D_FP32C = 1, WQ3D_FP32 = 2 };
 
 typedef struct wq3d_queue_desc {
     const double* freq;        /* frequencies (Hz), seq_vector freq       */
@@ -250,7 +259,7 @@ typedef struct wq3d_queue_desc {
     size_t num_targets1;
     size_t num_targets2;
     int spreading;             /* WQ3D_CLASSIC_RAY or WQ3D_HYBRID_GAUSSIAN */
-    int precision;             /* WQ3D_FP64 or WQ3D_FP32C                  */
+    int precision;             /* WQ3D_FP64, WQ3D_FP32C or WQ3D_FP32       */
     double earth_radius;       /* wposition::earth_radius while propagating */
     size_t eigenray_capacity;  /* device records kept per step chunk; 0 = default */
     int device;                /* CUDA device ordinal                     */

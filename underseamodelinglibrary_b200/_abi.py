@@ -27,7 +27,7 @@ BOUNDARY_FLAT, BOUNDARY_SLOPE, BOUNDARY_GRID = 0, 1, 2
 LOSS_DEFAULT, LOSS_CONSTANT, LOSS_RAYLEIGH, LOSS_ECKART = -1, 0, 1, 2
 INTERP_NEAREST, INTERP_LINEAR, INTERP_PCHIP = -1, 0, 1
 CLASSIC_RAY, HYBRID_GAUSSIAN = 0, 1
-FP64, FP32C = 0, 1
+FP64, FP32C, FP32 = 0, 1, 2
 FRONT_PAST, FRONT_PREV, FRONT_CURR, FRONT_NEXT = 0, 1, 2, 3
 
 dp = C.POINTER(C.c_double)

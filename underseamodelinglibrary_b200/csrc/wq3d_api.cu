@@ -525,7 +525,7 @@ struct wq3d_queue {
         const int eig_blocks = std::min(EIG_BLOCKS, std::max(148, (n + 255) / 256));
         if (timing) tail = false;
         auto cpa_launch = [&](int k, cudaStream_t st) {
-            if (h.precision == WQ3D_FP32C)
+            if (h.precision != WQ3D_FP64)
                 k_cpa_f32<<<dim3(((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) *
                                      ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
                                  (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS),
@@ -1206,8 +1206,8 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     if (d->num_freq > (size_t)MAX_FREQ) return fail(WQ3D_ERR_UNSUPPORTED, "more than 64 frequencies");
     if (d->num_az > (size_t)MAX_AZ) return fail(WQ3D_ERR_UNSUPPORTED, "more than 4096 AZ angles");
     if (!(d->time_step > 0.0)) return fail(WQ3D_ERR_INVALID, "time_step must be positive");
-    if (d->precision != WQ3D_FP64 && d->precision != WQ3D_FP32C)
-        return fail(WQ3D_ERR_INVALID, "precision must be WQ3D_FP64 or WQ3D_FP32C");
+    if (d->precision != WQ3D_FP64 && d->precision != WQ3D_FP32C && d->precision != WQ3D_FP32)
+        return fail(WQ3D_ERR_INVALID, "precision must be WQ3D_FP64, WQ3D_FP32C or WQ3D_FP32");
     const size_t n = d->num_de * d->num_az;
     if (n > (size_t)0x7fffffff) return fail(WQ3D_ERR_INVALID, "ray fan too large");
     const size_t nt = (d->targets && d->num_targets1 * d->num_targets2 > 0)
@@ -1818,6 +1818,8 @@ int wq3d_queue_enable_adjoint(wq3d_queue* q, int checkpoint_interval, size_t max
     if (q->steps != 0 || q->lsteps != 0) return fail(WQ3D_ERR_INVALID, "enable the adjoint before the first step");
     if (checkpoint_interval < 1 || max_steps < 1) return fail(WQ3D_ERR_INVALID, "checkpoint interval and steps must be positive");
     const QueueDev& h = q->h;
+    if (h.precision == WQ3D_FP32)
+        return fail(WQ3D_ERR_UNSUPPORTED, "the adjoint retraces FP64 steps: use WQ3D_FP64 or WQ3D_FP32C");
     const ProfileDev& pr = h.oc.prof;
     if (pr.kind != WQ3D_PROFILE_GRID || pr.grid.ndim != 1 || pr.grid.interp[0] != WQ3D_INTERP_LINEAR)
         return fail(WQ3D_ERR_UNSUPPORTED, "the adjoint needs a profile_grid<1> with linear interpolation");

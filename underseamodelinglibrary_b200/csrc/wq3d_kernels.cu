@@ -90,6 +90,17 @@ __device__ __forceinline__ void update1(const QueueDev& q, RayS& y) {
     ray_derivs(y.c, y.sg[0], y.sg[1], y.sg[2], y.pos, y.nd, y.pg, y.ng, &st);
 }
 
+/* wave_front::update of the FP32 propagation form (no distance terms) */
+__device__ __forceinline__ void update1_f32(const QueueDev& q, RayS& y) {
+    float c, g[3];
+    sound_speed_f32(q.oc.prof, q.R, y.pos[0], y.pos[1], y.pos[2], &c, g);
+    y.c = (double)c;
+    y.sg[0] = (double)g[0];
+    y.sg[1] = (double)g[1];
+    y.sg[2] = (double)g[2];
+    ray_derivs_f32(c, g, y.pos, y.nd, y.pg, y.ng);
+}
+
 /* ode_integ.cc:20-126 */
 __device__ __forceinline__ void rk1(double h, const RayS& y0, RayS& y1) {
 #pragma unroll
@@ -402,7 +413,12 @@ __device__ __noinline__ void volume_scatter(const QueueDev& q, const FrontPtrs& 
  * the temporary rays in registers, but the larger code made k_reflect
  * wait on instruction fetch (90.6 instead of 58.4 us per launch on the
  * sloped workload, ncu: "no instruction" stalls 2.9 -> 10.1 per issue). */
-__device__ __noinline__ void reinit_update(const QueueDev& q, RayS& y) { update1(q, y); }
+__device__ __noinline__ void reinit_update(const QueueDev& q, RayS& y) {
+    if (q.precision == WQ3D_FP32)
+        update1_f32(q, y);
+    else
+        update1(q, y);
+}
 
 /* reflection_model::reflection_reinit on the private state */
 __device__ __noinline__ void reinit_local(const QueueDev& q, RayLocal& L, double tw, const double* pos,
@@ -1022,11 +1038,17 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
         }
     }
     const double plen_x = __ldg(R.X->plen + i);
-    /* rotate and take the AB3 step; wave_front::update of the new front */
+    /* rotate and take the AB3 step; wave_front::update of the new front
+     * (the distance terms' sin(theta) is FP64 in every form) */
     ab3(q.dt, y0, y1, y2, y3);
-    profile_at(q, y3.pos, &y3.c, y3.sg);
     double st;
-    ray_derivs(y3.c, y3.sg[0], y3.sg[1], y3.sg[2], y3.pos, y3.nd, y3.pg, y3.ng, &st);
+    if (q.precision == WQ3D_FP32) {
+        update1_f32(q, y3);
+        st = sin(y3.pos[1]);
+    } else {
+        profile_at(q, y3.pos, &y3.c, y3.sg);
+        ray_derivs(y3.c, y3.sg[0], y3.sg[1], y3.sg[2], y3.pos, y3.nd, y3.pg, y3.ng, &st);
+    }
     const uint8_t f_next = reflect_decision(q, y3.pos, y2.nd);
     /* the per-step finiteness check: a NaN or Inf in the environment (a
      * bad profile node, a zero sound speed) reaches the new front here */

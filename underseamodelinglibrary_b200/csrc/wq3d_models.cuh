@@ -725,6 +725,94 @@ WQ_HD void ray_derivs(double c, double sg_r, double sg_t, double sg_p,
     *sin_out = st;
 }
 
+/* ------------------------------------------------------------------ */
+/* the FP32 propagation form (WQ3D_FP32): sound speed, gradient and ray  */
+/* derivatives of wave_front::update in single precision                */
+/* ------------------------------------------------------------------ */
+/* The analytic profiles at the altitude offset alt = rho - R (formed in
+ * FP64, then rounded: 0.5 mm at 5 km), in single precision; a gridded
+ * profile is interpolated in FP64 and rounded. */
+WQ_HD void sound_speed_f32(const ProfileDev& pr, double R, double rho, double theta, double phi, float* c,
+                           float* g) {
+    const float alt = (float)(rho - R);
+    float cc, gr, gt = 0.0f, gp = 0.0f;
+    switch (pr.kind) {
+#if WQ3D_WITH_GRID
+        case WQ3D_PROFILE_GRID: {
+            double c64, g64[3];
+            sound_speed(pr, R, rho, theta, phi, &c64, g64);
+            *c = (float)c64;
+            g[0] = (float)g64[0];
+            g[1] = (float)g64[1];
+            g[2] = (float)g64[2];
+            return;
+        }
+#endif
+        case WQ3D_PROFILE_LINEAR: {
+            const float z = -alt;
+            if (z < (float)pr.p[2]) {
+                cc = (float)pr.p[0] + (float)pr.p[1] * z;
+                gr = -(float)pr.p[1];
+            } else {
+                cc = (float)(pr.p[0] + pr.p[1] * pr.p[2]) + (float)pr.p[3] * (z - (float)pr.p[2]);
+                gr = -(float)pr.p[3];
+            }
+            break;
+        }
+        case WQ3D_PROFILE_MUNK: {
+            const float z = 2.0f * (-alt - (float)pr.p[0]) / (float)pr.p[1];
+            const float e = expf(-z);
+            cc = (((z - 1.0f) + e) * (float)pr.p[3] + 1.0f) * (float)pr.p[2];
+            gr = (1.0f - e) * (float)pr.munk_k;
+            break;
+        }
+        case WQ3D_PROFILE_CATENARY: {
+            const float x = (alt + (float)pr.p[2]) / (-(float)pr.p[1]);
+            cc = (float)pr.p[0] * coshf(x);
+            gr = -sinhf(x) * (float)(pr.p[0] / pr.p[1]);
+            break;
+        }
+        case WQ3D_PROFILE_N2: {
+            const float f = (float)pr.n2_factor;
+            cc = (float)pr.p[0] / sqrtf(1.0f - alt * f);
+            gr = cc * cc * cc * f / (float)(2.0 * pr.p[0] * pr.p[0]);
+            break;
+        }
+        default:
+            cc = 1500.0f;
+            gr = 0.0f;
+    }
+    if (pr.flat_earth) {
+        gr = gr * (float)(rho / R) + cc / (float)R;
+        cc = cc * (float)(rho / R);
+    }
+    *c = cc;
+    g[0] = gr;
+    g[1] = gt;
+    g[2] = gp;
+}
+
+/* ray_derivs in single precision (rho enters only as 1/rho factors, so its
+ * rounding is relative) */
+WQ_HD void ray_derivs_f32(float c, const float* sg, const double* pos, const double* nd, double* pg, double* ng) {
+    const float rho = (float)pos[0];
+    const float dcc_r = sg[0] / c;
+    const float dcc_t = sg[1] / c;
+    const float dcc_p = sg[2] / c;
+    const float th = (float)pos[1];
+    const float st = sinf(th);
+    const float ct = cosf(th) / st;
+    const float n0 = (float)nd[0], n1 = (float)nd[1], n2 = (float)nd[2];
+    const float c2 = c * c;
+    const float c2r = c2 / rho;
+    pg[0] = (double)(c2 * n0);
+    pg[1] = (double)(c2r * n1);
+    pg[2] = (double)((c2r / st) * n2);
+    ng[0] = (double)(c2r * (n1 * n1 + n2 * n2) - dcc_r);
+    ng[1] = (double)((-c2r) * (n0 * n1 - (n2 * n2) * ct) - dcc_t / rho);
+    ng[2] = (double)((-c2r) * (n2 * (n0 + n1 * ct)) - dcc_p / (rho * st));
+}
+
 /* wave_front::compute_target_distance for one (ray, target) pair
  * (wave_front.cc:222-236).  rho2 = rho*rho, two_R = 2*target rho,
  * R2 = target rho squared: the same values the reference forms. */

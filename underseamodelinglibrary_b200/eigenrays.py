@@ -169,3 +169,38 @@ def dead_reckon_one(eigenrays, oldpos, newpos, profile):
         new.intensity = 20.0 * np.log10(r2[n]) + a2[n] + offset
         new.phase = np.array(ray.phase, dtype=np.float64)
     return out
+
+
+def form_errors(test, ref):
+    """Differences between two eigenray sets of the same propagation (two
+    arithmetic forms, or the engine and the oracle), matched on the CPA
+    bracket (step, t1, t2, D/E index, AZ index): the counts found in one set
+    only, and for the matched eigenrays the largest and 99th-percentile
+    absolute differences of travel time (s), intensity (dB, every
+    frequency), source D/E and AZ and target D/E and AZ (deg).  ``test`` and
+    ``ref`` are eigenray_lists (take_eigenrays)."""
+    def table(rays):
+        a = rays.arrays()
+        keys = list(zip(a["step"].tolist(), a["t1"].tolist(), a["t2"].tolist(), a["de"].tolist(),
+                        a["az"].tolist()))
+        return a, {k: i for i, k in enumerate(keys)}
+    at, it = table(test)
+    ar, ir = table(ref)
+    common = sorted(set(it) & set(ir))
+    out = {"matched": len(common), "only_test": len(it) - len(common), "only_ref": len(ir) - len(common)}
+    if not common:
+        return out
+    jt = np.array([it[k] for k in common])
+    jr = np.array([ir[k] for k in common])
+    cols = {"travel_time_s": ("time", 1.0), "intensity_db": ("intensity", 1.0),
+            "source_de_deg": ("source_de", 1.0), "source_az_deg": ("source_az", 1.0),
+            "target_de_deg": ("target_de", 1.0), "target_az_deg": ("target_az", 1.0)}
+    for name, (col, _) in cols.items():
+        d = np.abs(np.asarray(at[col])[jt] - np.asarray(ar[col])[jr])
+        if name.endswith("az_deg"):
+            d = np.minimum(d, 360.0 - d)
+        d = d.ravel()
+        out[name] = {"max": float(d.max()), "p99": float(np.percentile(d, 99))}
+    counts = ("surface", "bottom", "caustic", "upper", "lower")
+    out["counts_differ"] = int(sum(np.count_nonzero(np.asarray(at[c])[jt] != np.asarray(ar[c])[jr]) for c in counts))
+    return out
