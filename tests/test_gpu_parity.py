@@ -565,3 +565,40 @@ def test_reverb_scale_reduced_parity(engine):
     eng = q.take_eigenrays()
     assert len(eng) > 10 and len(eng[0].intensity) == 32
     compare_eigenrays(eng, o.take_eigenrays())
+
+
+@pytest.mark.parametrize("builder,t_max", [
+    (lambda: S.munk_flat(), 5e-6),
+    (lambda: S.linear_slope_rayleigh(num_de=181, num_az=19, n_range=8, n_depth=8, time_max=10.0), 1e-6),
+    (lambda: S.eigenray_basic(), 1e-7),
+])
+def test_fp32_form_error_envelope(engine, builder, t_max):
+    """The FP32 propagation form (sound speed, gradient and ray derivatives
+    in single precision) against the FP64 form: the same eigenrays and
+    counts, TL within 0.1 dB, angles within 1e-3 deg, travel time within
+    the form's measured drift (the rounding of c in FP32, about 8e-8
+    relative, accumulates along the path: 3 us after the Munk workload's
+    60 s, 0.7 us after the sloped workload's 10 s)."""
+    from underseamodelinglibrary_b200.eigenrays import form_errors
+    sc = builder()
+    a = S.build_queue(sc, u.wave_queue, precision=_abi.FP64)
+    b = S.build_queue(sc, u.wave_queue, precision=_abi.FP32)
+    a.run(sc["time_max"])
+    b.run(sc["time_max"])
+    ra, rb = a.take_eigenrays(), b.take_eigenrays()
+    assert len(ra) > 0
+    e = form_errors(rb, ra)
+    assert e["only_test"] == 0 and e["only_ref"] == 0 and e["counts_differ"] == 0, e
+    assert e["travel_time_s"]["max"] <= t_max, e
+    assert e["intensity_db"]["max"] <= 0.1, e
+    for k in ("source_de_deg", "source_az_deg", "target_de_deg", "target_az_deg"):
+        assert e[k]["max"] <= 1e-3, (k, e)
+
+
+def test_fp32_form_refuses_the_adjoint(engine):
+    from underseamodelinglibrary_b200 import adjoint as A
+    sc = A.AdjointScenario(num_de=31, num_az=7, n_steps=20, n_targets=4, max_range=5e3)
+    q = sc.queue(A.munk_nodes(), precision=_abi.FP32)
+    with pytest.raises(u.EngineError) as ei:
+        q.enable_adjoint(10, 40)
+    assert ei.value.code == _abi.WQ3D_ERR_UNSUPPORTED
