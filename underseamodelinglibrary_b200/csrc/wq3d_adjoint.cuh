@@ -1640,6 +1640,115 @@ __device__ __noinline__ uint32_t step_vjp_pass(const QueueDev& q, const AdjSweep
     return err;
 }
 
+/* lambda contribution of Phi_m for a step without reflections, front by
+ * front.  Without a reflection chain, Phi_m passes the curr and next
+ * states through and forms the new front from the three fronts'
+ * derivatives (AB3): each front's (pg, ng) depends only on its own six
+ * state values and the two profile nodes around its depth, so one dual
+ * pass of eight directions per front gives its block of the Jacobian, and
+ * AB3, the step length and the absorption increment are transposed by
+ * hand.  Equal to step_vjp_pass's three passes over all 24 inputs. */
+__device__ __noinline__ uint32_t step_vjp_blocked(const QueueDev& q, const AdjSweep& a, const double* S,
+                                                  const ParamWin& pw, const double* lam1, double* lam0,
+                                                  double* gnode) {
+    using D = Dual<8>;
+    const double h = q.dt;
+    const double A2 = 23.0 / 12.0, A1 = 16.0 / 12.0, A0 = 5.0 / 12.0;
+    const double coef[3] = {h * A0, -h * A1, h * A2}; /* V, C, X */
+    uint32_t err = 0;
+    /* the three fronts' derivatives (values) and Jacobian blocks */
+    double pg[3][3], ng[3][3];
+    double J[3][6][8]; /* [front][pg0..2, ng0..2][pos0..2, nd0..2, node k, node k+1] */
+    int knode[3];
+    for (int r = 0; r < 3; ++r) {
+        bool ok = true;
+        RayT<D> Y;
+        for (int c = 0; c < 3; ++c) {
+            Y.pos[c] = D::var(S[r * 6 + c], c);
+            Y.nd[c] = D::var(S[r * 6 + 3 + c], 3 + c);
+        }
+        Y.dist = D(0.0);
+        ParamWin pr;
+        pr.k0 = ssp_interval(q, S[r * 6]);
+        pr.w = 2;
+        pr.base = 6;
+        knode[r] = pr.k0;
+        update_t(q, Y, pr, ok);
+        if (!ok) err |= ADJ_ERR_WINDOW;
+        for (int k = 0; k < 3; ++k) {
+            pg[r][k] = Y.pg[k].v;
+            ng[r][k] = Y.ng[k].v;
+            for (int j = 0; j < 8; ++j) {
+                J[r][k][j] = Y.pg[k].d[j];
+                J[r][3 + k][j] = Y.ng[k].d[j];
+            }
+        }
+    }
+    /* AB3 step values (ab3_t): d_k and the step length */
+    double d[3];
+    for (int k = 0; k < 3; ++k) d[k] = h * (A2 * pg[2][k] - A1 * pg[1][k] + A0 * pg[0][k]);
+    const double rx = S[12], tx = S[13];
+    const double sx = ::sin(tx), cx = ::cos(tx);
+    const double b = rx * d[1];
+    const double cc = rx * (sx * d[2]);
+    const double dist = ::sqrt(d[0] * d[0] + b * b + cc * cc);
+    /* the absorption increment of the first frequency */
+    const double l_inc = lam1[20];
+    double l_dist = 0.0, l_y3r = 0.0;
+    if (q.oc.prof.atten == WQ3D_ATTEN_CONSTANT) {
+        l_dist = l_inc * (q.oc.prof.atten_coef * q.freq[0]);
+    } else {
+        const double y3r = S[12] + d[0];
+        l_dist = l_inc * (a.alpha0 * (1.0 + 5.88264e-6 * (y3r - q.R)));
+        l_y3r = l_inc * (dist * a.alpha0 * 5.88264e-6);
+    }
+    /* curr and next pass through; the new front's position and direction
+     * add to the next front's */
+    for (int c = 0; c < 6; ++c) {
+        lam0[6 + c] += lam1[c];
+        lam0[12 + c] += lam1[6 + c];
+    }
+    double L3p[3] = {lam1[12] + l_y3r, lam1[13], lam1[14]};
+    for (int k = 0; k < 3; ++k) {
+        lam0[12 + k] += L3p[k];
+        lam0[15 + k] += lam1[15 + k];
+    }
+    /* through the step length: d dist / d (d, rho_X, theta_X) */
+    double ld[3] = {L3p[0], L3p[1], L3p[2]};
+    if (dist > 0.0 && l_dist != 0.0) {
+        const double gdist = l_dist / dist;
+        ld[0] += gdist * d[0];
+        ld[1] += gdist * (b * rx);
+        ld[2] += gdist * (cc * rx * sx);
+        lam0[12] += gdist * (b * d[1] + cc * sx * d[2]);
+        lam0[13] += gdist * (cc * rx * cx * d[2]);
+    }
+    /* through AB3 into each front's derivatives, then its block */
+    for (int r = 0; r < 3; ++r) {
+        double lo[6];
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = coef[r] * ld[k];
+            lo[3 + k] = coef[r] * lam1[15 + k];
+        }
+        for (int j = 0; j < 6; ++j) {
+            double g = 0.0;
+            for (int o = 0; o < 6; ++o) g += lo[o] * J[r][o][j];
+            lam0[r * 6 + j] += g;
+        }
+        for (int t = 0; t < 2; ++t) {
+            double g = 0.0;
+            for (int o = 0; o < 6; ++o) g += lo[o] * J[r][o][6 + t];
+            const int w = knode[r] + t - pw.k0;
+            if (w < 0 || w >= pw.w) {
+                if (g != 0.0) err |= ADJ_ERR_WINDOW;
+            } else {
+                gnode[w] += g;
+            }
+        }
+    }
+    return err;
+}
+
 /* init_wave and the RK3 start-up of one ray (k_startup) on dual node
  * values: lambda_0 . d S_0 / d nodes into gnode */
 __device__ __noinline__ uint32_t startup_vjp(const QueueDev& q, const AdjSweep& a, int i, ParamWin pw,
@@ -1729,8 +1838,12 @@ __global__ void __launch_bounds__(128) k_adj_reverse(AdjSweep a, __grid_constant
                 double lam0[ADJ_S], gnode[ADJ_W];
                 for (int c = 0; c < ADJ_S; ++c) lam0[c] = 0.0;
                 for (int c = 0; c < ADJ_W; ++c) gnode[c] = 0.0;
-                for (int off = 0; off < ADJ_S + pw.w; off += ADJ_NB)
-                    err |= step_vjp_pass<ADJ_NB>(q, a, S, code, pw, off, lam, lam0, gnode);
+                if (code == 0) {
+                    err |= step_vjp_blocked(q, a, S, pw, lam, lam0, gnode);
+                } else {
+                    for (int off = 0; off < ADJ_S + pw.w; off += ADJ_NB)
+                        err |= step_vjp_pass<ADJ_NB>(q, a, S, code, pw, off, lam, lam0, gnode);
+                }
                 for (int c = 0; c < pw.w; ++c) gacc[pw.k0 + c] += gnode[c];
                 const double la_v = lam[18], la_c = lam[19], la_x = lam[20];
                 for (int c = 0; c < ADJ_S; ++c) lam[c] = lam0[c];
