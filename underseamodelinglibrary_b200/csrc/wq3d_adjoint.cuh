@@ -1657,7 +1657,7 @@ __device__ __noinline__ uint32_t step_vjp_blocked(const QueueDev& q, const AdjSw
     const double coef[3] = {h * A0, -h * A1, h * A2}; /* V, C, X */
     uint32_t err = 0;
     /* the three fronts' derivatives (values) and Jacobian blocks */
-    double pg[3][3], ng[3][3];
+    double pg[3][3];
     double J[3][6][8]; /* [front][pg0..2, ng0..2][pos0..2, nd0..2, node k, node k+1] */
     int knode[3];
     for (int r = 0; r < 3; ++r) {
@@ -1677,7 +1677,6 @@ __device__ __noinline__ uint32_t step_vjp_blocked(const QueueDev& q, const AdjSw
         if (!ok) err |= ADJ_ERR_WINDOW;
         for (int k = 0; k < 3; ++k) {
             pg[r][k] = Y.pg[k].v;
-            ng[r][k] = Y.ng[k].v;
             for (int j = 0; j < 8; ++j) {
                 J[r][k][j] = Y.pg[k].d[j];
                 J[r][3 + k][j] = Y.ng[k].d[j];
