@@ -66,8 +66,10 @@ def parse():
     ap.add_argument("--batch-instances", type=int, default=512,
                     help="instances of the batched gridded workload (0 skips it)")
     ap.add_argument("--profile-workload", default="linear_slope_rayleigh",
-                    choices=["linear_slope_rayleigh", "std14"],
-                    help="workload of --profile-steps (std14: the speed study with 100 targets)")
+                    choices=["linear_slope_rayleigh", "std14", "gridded"],
+                    help="workload of --profile-steps (std14: the speed study with 100 targets; "
+                         "gridded: one 1801 x 45 ray instance of the batched gridded workload's "
+                         "environment, 64 targets, dt 0.05 s)")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="profiling mode: one queue of the workload, this many wave steps, no output")
     return ap.parse_args()
@@ -773,7 +775,12 @@ def main():
         import underseamodelinglibrary_b200 as u
         from underseamodelinglibrary_b200 import scenarios as S
         from underseamodelinglibrary_b200 import _abi
-        sc = S.std14(num_targets=100) if args.profile_workload == "std14" else S.linear_slope_rayleigh()
+        if args.profile_workload == "std14":
+            sc = S.std14(num_targets=100)
+        elif args.profile_workload == "gridded":
+            sc = S.gridded_munk(seed=1, num_de=1801, num_az=45, n_targets=64, time_max=60.0, dt=0.05)
+        else:
+            sc = S.linear_slope_rayleigh()
         q = S.build_queue(sc, u.wave_queue, device=0, precision=_abi.FP32C)
         q.step(args.profile_steps)
         print("profile run: %d steps, %d eigenrays" % (q.steps(), len(q.take_eigenrays())))

@@ -178,6 +178,9 @@ int make_grid(wq3d_ocean* o, const wq3d_grid_desc& d, int max_dims, GridDev* hg,
     hg->all_linear = 1;
     for (int k = 0; k < d.ndim; ++k)
         if (hg->interp[k] != WQ3D_INTERP_LINEAR) hg->all_linear = 0;
+    hg->pchip0 = hg->interp[0] == WQ3D_INTERP_PCHIP;
+    for (int k = 1; k < d.ndim; ++k)
+        if (hg->interp[k] != WQ3D_INTERP_LINEAR) hg->pchip0 = 0;
     o->store.emplace_back(d.data, d.data + total);
     hg->data = o->store.back().data();
     *dg = *hg;

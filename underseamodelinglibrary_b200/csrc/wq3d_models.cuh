@@ -65,6 +65,7 @@ struct AxisDev {
 struct GridDev {
     int ndim;
     int all_linear;  /* every axis interpolates linearly: unrolled path */
+    int pchip0;      /* pchip on axis 0, linear on the others: unrolled path */
     AxisDev ax[3];
     int interp[3];
     int edge[3];
@@ -419,8 +420,171 @@ WQ_HD double grid_linear(const GridDev& g, const double* location, double* dv) {
     return r;
 }
 
+/* pchip along axis 0 with every other axis linear (a profile grid's
+ * usual form: pchip in depth, linear across), unrolled like grid_linear.
+ * At axis 0 the recursion's corner values carry no derivative of their
+ * own, so gen_grid.h's pchip (gen_grid.h:350-500) reduces to the value
+ * and its axis-0 slope below; the spacing and offset terms depend only on
+ * the axis-0 index and are computed once for every corner.  All corner
+ * loads are issued before any arithmetic; the recursion instead fetched
+ * them one out-of-line call at a time. */
+struct Pchip0 {
+    double h0, h1, h2, h1_2, h1_3, s, s_2, sh_minus, sh_term, v;
+    bool lo_in;  /* k >= 1: a row below the cell */
+    bool hi_in;  /* k <= n - 3: a row above the cell's upper row */
+};
+
+WQ_HD void pchip0_setup(const AxisDev& ax, int k, double x, Pchip0& P) {
+    P.lo_in = k >= 1;
+    P.hi_in = k <= ax.n - 3;
+    P.h0 = axis_inc(ax, (long)k - 1);
+    P.h1 = axis_inc(ax, k);
+    P.h2 = axis_inc(ax, (long)k + 1);
+    P.h1_2 = P.h1 * P.h1;
+    P.h1_3 = P.h1_2 * P.h1;
+    P.s = x - ax.x[k];
+    P.s_2 = P.s * P.s;
+    const double s_3 = P.s_2 * P.s;
+    P.sh_minus = P.s - P.h1;
+    P.sh_term = 3.0 * P.h1 * P.s_2 - 2.0 * s_3;
+    P.v = P.s / P.h1;
+}
+
+/* one corner: rows k-1 .. k+2 of axis 0 (y0 / y3 already replaced by
+ * y1 / y2 outside the axis); *deriv takes the axis-0 slope when want */
+WQ_HD double pchip0_corner(const Pchip0& P, double y0, double y1, double y2, double y3, bool want,
+                           double* deriv) {
+    const double deriv0 = (y1 - y0) / P.h0;
+    const double deriv1 = (y2 - y1) / P.h1;
+    const double deriv2 = (y3 - y2) / P.h2;
+    double slope1 = 0.0;
+    if (P.lo_in) {
+        const double w0 = 2.0 * P.h1 + P.h0;
+        const double w1 = P.h1 + 2.0 * P.h0;
+        if (deriv0 * deriv1 > 0.0) slope1 = (w0 + w1) / (w0 / deriv0 + w1 / deriv1);
+    } else {
+        slope1 = ((2.0 + P.h1 + P.h2) * deriv1 - P.h1 * deriv2) / (P.h1 + P.h2);
+        if (slope1 * deriv1 < 0.0) {
+            slope1 = 0.0;
+        } else if ((deriv1 * deriv2 < 0.0) && (fabs(slope1) > fabs(3.0 * deriv2))) {
+            slope1 = 3.0 * deriv2;
+        }
+    }
+    double slope2 = 0.0;
+    if (P.hi_in) {
+        const double w1 = 2.0 * P.h1 + P.h0;
+        const double w2 = P.h1 + 2.0 * P.h0;
+        if (deriv1 * deriv2 > 0.0) slope2 = (w1 + w2) / (w1 / deriv1 + w2 / deriv2);
+    } else {
+        slope2 = ((2.0 + P.h1 + P.h2) * deriv1 - P.h1 * deriv0) / (P.h1 + P.h0);
+        if (slope2 * deriv1 < 0.0) {
+            slope2 = 0.0;
+        } else if ((deriv1 * deriv0 < 0.0) && (fabs(slope2) > fabs(3.0 * deriv0))) {
+            slope2 = 3.0 * deriv0;
+        }
+    }
+    const double result = y2 * P.sh_term / P.h1_3 + y1 * (P.h1_3 - P.sh_term) / P.h1_3 +
+                          slope2 * P.s_2 * P.sh_minus / P.h1_2 +
+                          slope1 * P.s * P.sh_minus * P.sh_minus / P.h1_2;
+    if (want) *deriv = slope1 * (1.0 - P.v) + slope2 * P.v;
+    return result;
+}
+
+/* edge limiting and find_index on every axis (gen_grid.h:83-110) */
+template <int NDIM>
+WQ_HD void grid_locate(const GridDev& g, const double* location, int* index, double* loc) {
+    for (int d = 0; d < NDIM; ++d) loc[d] = location[d];
+    for (int d = 0; d < NDIM; ++d) {
+        const AxisDev& ax = g.ax[d];
+        if (g.edge[d]) {
+            const double a = ax.x[0];
+            const double b = ax.x[ax.n - 1];
+            const double sign = (ax.inc[0] < 0) ? -1.0 : 1.0;
+            const double dd = loc[d] * sign;
+            if (dd <= a * sign) {
+                loc[d] = a;
+                index[d] = 0;
+            } else if (dd >= b * sign) {
+                loc[d] = b;
+                index[d] = ax.n - 2;
+            } else {
+                index[d] = axis_find(ax, loc[d]);
+            }
+        } else {
+            index[d] = axis_find(ax, loc[d]);
+        }
+    }
+}
+
+template <int NDIM>
+WQ_HD double grid_pchip0(const GridDev& g, const double* location, double* dv) {
+    int index[NDIM];
+    double loc[NDIM];
+    grid_locate<NDIM>(g, location, index, loc);
+    const double* D = g.data;
+    const AxisDev& a0 = g.ax[0];
+    const int k = index[0];
+    Pchip0 P;
+    pchip0_setup(a0, k, loc[0], P);
+    const int km = k >= 1 ? k - 1 : k;
+    const int kp = k + 2 <= a0.n - 1 ? k + 2 : k + 1;
+    const bool want = dv != nullptr;
+    /* rows km, k, k+1, kp of axis 0 at axis-0 stride st, from offset o */
+    auto corner = [&](size_t o, size_t st, double* d0) {
+        double y0 = D[o + st * (size_t)km], y1 = D[o + st * (size_t)k];
+        double y2 = D[o + st * (size_t)(k + 1)], y3 = D[o + st * (size_t)kp];
+        if (!P.lo_in) y0 = y1;
+        if (!P.hi_in) y3 = y2;
+        return pchip0_corner(P, y0, y1, y2, y3, want, d0);
+    };
+    double u, h;
+    if (NDIM == 1) {
+        double d0 = 0.0;
+        const double r = corner(0, 1, &d0);
+        if (dv) dv[0] = d0;
+        return r;
+    }
+    if (NDIM == 2) {
+        const size_t n1 = (size_t)g.ax[1].n;
+        double da = 0.0, db = 0.0;
+        const double a = corner((size_t)index[1], n1, &da);
+        const double b = corner((size_t)index[1] + 1, n1, &db);
+        const double r = lin1(g, 1, index, loc, a, b, &u, &h);
+        if (dv) {
+            dv[1] = (b - a) / h;
+            dv[0] = da * (1.0 - u) + db * u;
+        }
+        return r;
+    }
+    /* NDIM == 3: outer axis 2, then axis 1, innermost axis 0 (pchip) */
+    const size_t n1 = (size_t)g.ax[1].n, n2 = (size_t)g.ax[2].n;
+    const size_t st = n1 * n2;
+    const int i1 = index[1], i2 = index[2];
+    double u1, h1;
+    auto plane = [&](int j, double* d1, double* d0) {
+        double da = 0.0, db = 0.0;
+        const double va = corner((size_t)j + n2 * (size_t)i1, st, &da);
+        const double vb = corner((size_t)j + n2 * (size_t)(i1 + 1), st, &db);
+        const double r = lin1(g, 1, index, loc, va, vb, &u1, &h1);
+        *d1 = (vb - va) / h1;
+        *d0 = da * (1.0 - u1) + db * u1;
+        return r;
+    };
+    double d1a, d1b, d0a, d0b;
+    const double pa = plane(i2, &d1a, &d0a);
+    const double pb = plane(i2 + 1, &d1b, &d0b);
+    const double r = lin1(g, 2, index, loc, pa, pb, &u, &h);
+    if (dv) {
+        dv[2] = (pb - pa) / h;
+        dv[1] = d1a * (1.0 - u) + d1b * u;
+        dv[0] = d0b;
+    }
+    return r;
+}
+
 #if WQ3D_WITH_GRID
-/* grid evaluation: the unrolled linear path inline, others out of line */
+/* grid evaluation: the unrolled linear and pchip-in-axis-0 paths inline,
+ * others out of line */
 WQ_HD double grid_value(const GridDev& g, const double* location, double* dv);
 
 static WQ_NOINL double grid_eval(const GridDev& g, const double* location, double* dv) {
@@ -443,6 +607,16 @@ WQ_HD double grid_value(const GridDev& g, const double* location, double* dv) {
                 return grid_linear<2>(g, location, dv);
             default:
                 return grid_linear<3>(g, location, dv);
+        }
+    }
+    if (g.pchip0) {
+        switch (g.ndim) {
+            case 1:
+                return grid_pchip0<1>(g, location, dv);
+            case 2:
+                return grid_pchip0<2>(g, location, dv);
+            default:
+                return grid_pchip0<3>(g, location, dv);
         }
     }
     return grid_eval(g, location, dv);
