@@ -567,6 +567,36 @@ int wq3d_queue_timing(wq3d_queue* q, wq3d_timing* out, int reset);
  * No reference counterpart: benchmarking aid. */
 int wq3d_queue_set_timing(wq3d_queue* q, int on);
 
+/* Where the reflections of a step run (results are identical bit for bit):
+ *   WQ3D_REFLECT_SIDE    k_reflect, a separate launch on a high-priority
+ *                        stream over a compact list of the reflecting rays;
+ *                        the next step's advance waits for it.  Best when
+ *                        the fan fills the GPU: reflecting rays take few
+ *                        blocks.
+ *   WQ3D_REFLECT_INLINE  the advance of step s reflects step s+1's rays as
+ *                        soon as it has written their next front, so a step
+ *                        costs the longer of the advance and the longest
+ *                        reflection chain instead of their sum.  Best for
+ *                        small fans, whose steps are bound by that chain.
+ *                        (Eigenverb listeners and volume layers always use
+ *                        the side stream.)
+ *   WQ3D_REFLECT_AUTO    (default) a queue run alone follows a plan per
+ *                        queue shape and per 128-step bucket of the run
+ *                        (which schedule wins changes as the fan spreads):
+ *                        the first queue of a shape tries both schedules
+ *                        on one chunk of each bucket, every later chunk and
+ *                        queue of that shape takes the faster and refines
+ *                        its timing.  Queues run by wq3d_batch_run use the
+ *                        side stream.
+ * No reference counterpart (the reference reflects inside its step). */
+enum { WQ3D_REFLECT_AUTO = 0, WQ3D_REFLECT_SIDE = 1, WQ3D_REFLECT_INLINE = 2 };
+int wq3d_queue_set_reflect_schedule(wq3d_queue* q, int schedule);
+
+/* The schedule of the queue's last chunk (WQ3D_REFLECT_SIDE or
+ * WQ3D_REFLECT_INLINE), the one set, or WQ3D_REFLECT_AUTO before any run
+ * under the tuned schedule. */
+int wq3d_queue_reflect_schedule(const wq3d_queue* q, int* schedule);
+
 /* ------------------------------------------------------------------ */
 /* bistatic eigenverbs (biverbs/)                                      */
 /* ------------------------------------------------------------------ */

@@ -28,6 +28,7 @@ LOSS_DEFAULT, LOSS_CONSTANT, LOSS_RAYLEIGH, LOSS_ECKART = -1, 0, 1, 2
 INTERP_NEAREST, INTERP_LINEAR, INTERP_PCHIP = -1, 0, 1
 CLASSIC_RAY, HYBRID_GAUSSIAN = 0, 1
 FP64, FP32C, FP32 = 0, 1, 2
+REFLECT_AUTO, REFLECT_SIDE, REFLECT_INLINE = 0, 1, 2
 FRONT_PAST, FRONT_PREV, FRONT_CURR, FRONT_NEXT = 0, 1, 2, 3
 
 dp = C.POINTER(C.c_double)
@@ -198,6 +199,8 @@ SIGNATURES = {
     "wq3d_queue_abort": (C.c_int, [C.c_void_p]),
     "wq3d_queue_timing": (C.c_int, [C.c_void_p, C.POINTER(wq3d_timing), C.c_int]),
     "wq3d_queue_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "wq3d_queue_set_reflect_schedule": (C.c_int, [C.c_void_p, C.c_int]),
+    "wq3d_queue_reflect_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "wq3d_biverbs": (C.c_int, [C.POINTER(wq3d_eigenverb), dp, C.c_size_t, C.POINTER(wq3d_eigenverb), dp,
                                C.c_size_t, dp, C.c_size_t, C.POINTER(wq3d_scattering_desc), C.c_double,
                                C.c_double, C.c_double, C.POINTER(wq3d_biverb), dp, C.c_size_t,

@@ -203,6 +203,69 @@ int make_grid(wq3d_ocean* o, const wq3d_grid_desc& d, int max_dims, GridDev* hg,
 
 }  // namespace
 
+/* The reflection-schedule plan learnt per queue shape (fan, targets,
+ * frequencies, kernel build, precision, chunk length, sensitivities,
+ * adjoint), shared by every queue of the process.  A run is cut into
+ * buckets of TUNE_BUCKET steps, since which schedule wins changes as the
+ * fan spreads and meets the boundaries; per bucket and schedule the plan
+ * keeps the device time of the full chunks measured there.  A bucket's
+ * first two chunks try each schedule once; after that the faster one runs
+ * and its chunks keep refining the mean. */
+constexpr int TUNE_BUCKET = 128;
+struct TunePlan {
+    std::string key;
+    std::vector<double> ms[2];
+    std::vector<int> cnt[2];
+    std::vector<int> pend[2]; /* chunks chosen but not yet measured */
+};
+std::mutex g_tune_mu;
+std::vector<TunePlan> g_plans;
+
+TunePlan& tune_plan(const std::string& key, size_t bucket) {
+    TunePlan* e = nullptr;
+    for (auto& t : g_plans)
+        if (t.key == key) e = &t;
+    if (!e) {
+        g_plans.emplace_back();
+        e = &g_plans.back();
+        e->key = key;
+    }
+    for (int m = 0; m < 2; ++m)
+        if (e->ms[m].size() <= bucket) {
+            e->ms[m].resize(bucket + 1, 0.0);
+            e->cnt[m].resize(bucket + 1, 0);
+            e->pend[m].resize(bucket + 1, 0);
+        }
+    return *e;
+}
+
+/* the schedule of a full chunk in this bucket: 1 inline, 0 side */
+int tune_choose(const std::string& key, size_t bucket) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    TunePlan& t = tune_plan(key, bucket);
+    int m;
+    if (t.cnt[1][bucket] + t.pend[1][bucket] == 0)
+        m = 1;
+    else if (t.cnt[0][bucket] + t.pend[0][bucket] == 0)
+        m = 0;
+    else if (t.cnt[0][bucket] == 0 || t.cnt[1][bucket] == 0)
+        m = t.cnt[0][bucket] == 0 ? 1 : 0; /* the measured one until both are */
+    else
+        m = t.ms[1][bucket] / t.cnt[1][bucket] < t.ms[0][bucket] / t.cnt[0][bucket] ? 1 : 0;
+    t.pend[m][bucket] += 1;
+    return m;
+}
+
+void tune_record(const std::string& key, size_t bucket, int m, bool ok, double ms) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    TunePlan& t = tune_plan(key, bucket);
+    if (t.pend[m][bucket] > 0) t.pend[m][bucket] -= 1;
+    if (ok) {
+        t.ms[m][bucket] += ms;
+        t.cnt[m][bucket] += 1;
+    }
+}
+
 /* eigenrays kept for wq3d_queue_take_eigenrays (no listener), as flat
  * arrays: nf intensities and phases and 3 bottom sensitivities per ray */
 struct PendingRays {
@@ -233,7 +296,8 @@ struct wq3d_queue {
     /* per result set: chunk base step, chunk times, counters read back
      * (n_rec, n_refl, err, -, work lists, n_done, -, n_verb); d_counts also
      * holds the bottom work lists (9, 10), the adjoint's mark and entry
-     * count (11, 12) and the three candidate counts (13-15) */
+     * count (11, 12), the three candidate counts (13-15) and the three
+     * shadow sets' inline slot counts (16-18) */
     int64_t* h_base[2] = {nullptr, nullptr};
     double* h_times[2] = {nullptr, nullptr};
     uint32_t* h_counts[2] = {nullptr, nullptr};
@@ -241,10 +305,23 @@ struct wq3d_queue {
     double* d_times = nullptr;
     uint32_t* d_counts = nullptr;
     int chunk = 16;
-    /* [result set][prefetches the next chunk's first reflection] */
-    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    bool graph_failed[2][2] = {{false, false}, {false, false}};
-    int64_t graph_launches[2][2] = {{0, 0}, {0, 0}}; /* kernels in each graph */
+    /* [result set][prefetches the next chunk's first reflection][inline
+     * reflections] */
+    cudaGraphExec_t graph[2][2][2] = {};
+    bool graph_failed[2][2][2] = {};
+    int64_t graph_launches[2][2][2] = {}; /* kernels in each graph */
+    /* Reflection schedule (wq3d_queue_set_reflect_schedule).  Under
+     * WQ3D_REFLECT_AUTO a queue run alone follows its shape's plan
+     * (tune_choose) for every full chunk but a run's first, and times the
+     * chunk to refine the plan.  Both schedules give the same results bit
+     * for bit. */
+    int refl_sched = WQ3D_REFLECT_AUTO;
+    int last_inl = -1;             /* schedule of the last chunk launched */
+    bool in_batch = false;         /* queues of a batch use the side stream */
+    bool chunk_trial[2] = {false, false}; /* per result set: the chunk in flight is timed */
+    int chunk_inl[2] = {0, 0};            /* its schedule */
+    size_t chunk_bucket[2] = {0, 0};      /* and its bucket */
+    cudaEvent_t tune_ev[2][2] = {};
     /* Result set 1: a second copy of the record buffers, so that chunk c
      * writes set c & 1 while the host reads the other chunk's records
      * (made by the first run of more than one chunk; set 0 lives in h). */
@@ -285,6 +362,7 @@ struct wq3d_queue {
     bool gridded = false;
     void (*k_reflect_fn)(const QueueDev, int) = analytic::k_reflect;
     void (*k_advance_fn)(const QueueDev, int) = analytic::k_advance;
+    void (*k_advance_inline_fn)(const QueueDev, int) = analytic::k_advance_inline;
     /* eigenverb counting sink (wq3d_queue_count_eigenverbs) */
     bool count_verbs = false;
     uint64_t verb_counts[2 + 2 * WQ3D_MAX_VOLUME] = {0};
@@ -317,11 +395,12 @@ struct wq3d_queue {
      * sequence changes */
     void drop_graph() {
         for (int p = 0; p < 2; ++p)
-            for (int t = 0; t < 2; ++t) {
-                if (graph[p][t]) cudaGraphExecDestroy(graph[p][t]);
-                graph[p][t] = nullptr;
-                graph_failed[p][t] = false;
-            }
+            for (int t = 0; t < 2; ++t)
+                for (int m = 0; m < 2; ++m) {
+                    if (graph[p][t][m]) cudaGraphExecDestroy(graph[p][t][m]);
+                    graph[p][t][m] = nullptr;
+                    graph_failed[p][t][m] = false;
+                }
     }
 
     /* the descriptor that writes result set p */
@@ -449,6 +528,9 @@ struct wq3d_queue {
         drop_graph();
         for (auto e : done_ev)
             if (e) cudaEventDestroy(e);
+        for (auto& pe : tune_ev)
+            for (auto e : pe)
+                if (e) cudaEventDestroy(e);
         if (copy) cudaStreamDestroy(copy);
         for (auto e : events)
             if (e) cudaEventDestroy(e);
@@ -511,13 +593,19 @@ struct wq3d_queue {
      * candidate lists).  With "tail" the reflections of the
      * next chunk's first step run beside this chunk's last CPA search; that
      * chunk's own k_reflect(0) then finds an empty worklist and returns.
+     * Without eigenverbs (which read the committed curr front) there is no
+     * side stream: k_advance(k) runs step k+1's reflection chains for its
+     * own rays as soon as it has written their next front, so a step costs
+     * the longer of the advance and the longest reflection chain instead of
+     * their sum.  Those chains fill the shadow set of step k+1, the set
+     * step k-2 used, so k_advance(k) waits for k_commit(k-2).
      * With per-kernel timing the steps run one launch after another on the
      * main stream, except k_reflect(k+1) beside k_cpa(k) and k_eigenray(k).
      * (An advance split into the rays that need none of the step's
      * reflections, run beside k_reflect and k_cpa, and the rest was slower:
      * 149.5 against 131.9 ms per propagation of the sloped workload, the
      * memory-bound advance taking SM time from the CPA search.) */
-    int launch_chunk(int K, int p, bool tail) {
+    int launch_chunk(int K, int p, bool tail, bool inl_wanted) {
         const QueueDev d = dev(p);
         const int n = h.n;
         const dim3 blk(128);
@@ -591,10 +679,20 @@ struct wq3d_queue {
         }
         cudaEventRecord(start_ev, stream);
         cudaStreamWaitEvent(adv, start_ev, 0);
+        /* inline schedule: k_advance(k) reflects step k+1's rays itself
+         * (into the third shadow set) once their next front is written;
+         * nothing else in that reflection waits for step k's commit unless
+         * it makes eigenverbs */
+        const bool inl = inl_wanted && !h.want_verbs && !volume_pass();
         for (int k = 0; k < K; ++k) {
+            const bool more = k + 1 < K || tail;
             /* adv: step k's checkpoint, volume eigenverbs and advance, after
-             * its reflections */
-            if (k >= 1) cudaStreamWaitEvent(adv, join_ev[k - 1], 0);
+             * its reflections; an inline advance also after step k-2's
+             * commit (it refills that step's shadow set, and so follows step
+             * k-3's eigenray construction, whose prev front and candidate
+             * list it overwrites) */
+            if (!inl && k >= 1) cudaStreamWaitEvent(adv, join_ev[k - 1], 0);
+            if (inl && k >= 2) cudaStreamWaitEvent(adv, com_ev[k - 2], 0);
             if (h.adj) {
                 k_adj_checkpoint<<<grd, blk, 0, adv>>>(d, k);
                 launches += 1;
@@ -603,7 +701,7 @@ struct wq3d_queue {
                 k_volume<<<grd, blk, 0, adv>>>(d, k);
                 launches += 1;
             }
-            k_advance_fn<<<grd, blk, 0, adv>>>(d, k);
+            (inl && more ? k_advance_inline_fn : k_advance_fn)<<<grd, blk, 0, adv>>>(d, k);
             launches += 1;
             cudaEventRecord(adv_ev[k], adv);
             /* eig: step k's commit */
@@ -611,8 +709,7 @@ struct wq3d_queue {
             k_commit<<<grd, blk, 0, eig>>>(d, k);
             launches += 1;
             cudaEventRecord(com_ev[k], eig);
-            const bool more = k + 1 < K || tail;
-            if (more) {
+            if (more && !inl) {
                 /* side: step k+1's reflections */
                 cudaStreamWaitEvent(side, adv_ev[k], 0);
                 if (k >= 1) cudaStreamWaitEvent(side, com_ev[k - 1], 0);
@@ -635,30 +732,38 @@ struct wq3d_queue {
         /* every stream joins the main stream */
         cudaEventRecord(eig_end, eig);
         cudaStreamWaitEvent(stream, eig_end, 0);
-        if (tail) cudaStreamWaitEvent(stream, join_ev[K - 1], 0);
+        if (tail && !inl) cudaStreamWaitEvent(stream, join_ev[K - 1], 0);
+        cudaStreamWaitEvent(stream, adv_ev[K - 1], 0);
         return WQ3D_OK;
     }
 
-    int build_graph(int p, bool tail) {
-        const int t = tail ? 1 : 0;
-        if (graph[p][t] || graph_failed[p][t]) return WQ3D_OK;
+    /* the shape a tuned reflection schedule applies to */
+    std::string tune_key() const {
+        return std::to_string(h.nde) + "x" + std::to_string(h.naz) + " t" + std::to_string(h.nt) + " f" +
+               std::to_string(h.nf) + (gridded ? " g" : " a") + " p" + std::to_string(h.precision) + " c" +
+               std::to_string(chunk) + " s" + std::to_string(h.sens) + " j" + std::to_string(h.adj ? 1 : 0);
+    }
+
+    int build_graph(int p, bool tail, bool inl) {
+        const int t = tail ? 1 : 0, m = inl ? 1 : 0;
+        if (graph[p][t][m] || graph_failed[p][t][m]) return WQ3D_OK;
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-            graph_failed[p][t] = true;
+            graph_failed[p][t][m] = true;
             cudaGetLastError();
             return WQ3D_OK;
         }
         const bool save = timing;
         timing = false;
         const int64_t saved_launches = launches;
-        launch_chunk(chunk, p, tail);
-        graph_launches[p][t] = launches - saved_launches;
+        launch_chunk(chunk, p, tail, inl);
+        graph_launches[p][t][m] = launches - saved_launches;
         launches = saved_launches;
         timing = save;
         if (cudaStreamEndCapture(stream, &g) != cudaSuccess ||
-            cudaGraphInstantiate(&graph[p][t], g, 0) != cudaSuccess) {
-            graph_failed[p][t] = true;
-            graph[p][t] = nullptr;
+            cudaGraphInstantiate(&graph[p][t][m], g, 0) != cudaSuccess) {
+            graph_failed[p][t][m] = true;
+            graph[p][t][m] = nullptr;
             cudaGetLastError();
         }
         if (g) cudaGraphDestroy(g);
@@ -777,13 +882,43 @@ struct wq3d_queue {
         if (h.adj) WQ_CK(cudaMemsetAsync(d_counts + 11, 0, sizeof(uint32_t), stream));
         if (timing) tail = false;
         const int t = tail ? 1 : 0;
-        if (!timing && K == chunk) build_graph(p, tail);
-        if (!timing && K == chunk && graph[p][t]) {
-            WQ_CK(cudaGraphLaunch(graph[p][t], stream));
-            launches += graph_launches[p][t];
-        } else {
-            launch_chunk(K, p, tail);
+        /* the reflection schedule of this chunk, from the plan when tuned */
+        const bool can_inline = !timing && !h.want_verbs && !volume_pass();
+        bool inl = false, trial = false;
+        size_t bucket = 0;
+        if (can_inline) {
+            if (refl_sched == WQ3D_REFLECT_INLINE) {
+                inl = true;
+            } else if (refl_sched == WQ3D_REFLECT_AUTO && !in_batch && K == chunk && lsteps > 0) {
+                /* not a run's first chunk, whose start-up reflections are
+                 * not typical */
+                bucket = (size_t)(lsteps / TUNE_BUCKET);
+                inl = tune_choose(tune_key(), bucket) != 0;
+                trial = true;
+            } else if (refl_sched == WQ3D_REFLECT_AUTO && !in_batch) {
+                inl = last_inl > 0;
+            }
         }
+        last_inl = inl ? 1 : 0;
+        const int m = inl ? 1 : 0;
+        chunk_trial[p] = trial;
+        chunk_inl[p] = m;
+        chunk_bucket[p] = bucket;
+        if (!timing && K == chunk) build_graph(p, tail, inl);
+        /* a trial times the chunk's device work only: its start is marked
+         * after any graph building on the host */
+        if (trial) {
+            for (int e = 0; e < 2; ++e)
+                if (!tune_ev[p][e]) WQ_CK(cudaEventCreate(&tune_ev[p][e]));
+            WQ_CK(cudaEventRecord(tune_ev[p][0], stream));
+        }
+        if (!timing && K == chunk && graph[p][t][m]) {
+            WQ_CK(cudaGraphLaunch(graph[p][t][m], stream));
+            launches += graph_launches[p][t][m];
+        } else {
+            launch_chunk(K, p, tail, inl);
+        }
+        if (trial) WQ_CK(cudaEventRecord(tune_ev[p][1], stream));
         WQ_CK(cudaGetLastError());
         WQ_CK(cudaMemcpyAsync(h_counts[p], d_counts, 9 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         WQ_CK(cudaEventRecord(done_ev[p], stream));
@@ -796,6 +931,12 @@ struct wq3d_queue {
      * its records back and delivers them. */
     int chunk_finish(int K, int p) {
         WQ_CK(cudaEventSynchronize(done_ev[p]));
+        if (chunk_trial[p]) {
+            chunk_trial[p] = false;
+            float ms = 0.0f;
+            const bool ok = cudaEventElapsedTime(&ms, tune_ev[p][0], tune_ev[p][1]) == cudaSuccess;
+            tune_record(tune_key(), chunk_bucket[p], chunk_inl[p], ok, ms);
+        }
         if (timing) {
             WQ_CK(cudaStreamSynchronize(side));
             float r0 = 0;
@@ -867,6 +1008,9 @@ struct wq3d_queue {
         if (err & ERR_BAD_CANDIDATE)
             return fail(WQ3D_ERR_CUDA, "internal error: an eigenray candidate named a ray or target outside "
                                        "the fan (error bits " + std::to_string(err) + ")");
+        if (err & ERR_SLOT_OVERFLOW)
+            return fail(WQ3D_ERR_CUDA, "internal error: more reflecting rays in a step than rays (error bits " +
+                                           std::to_string(err) + ")");
         if (err)
             return fail(WQ3D_ERR_NUMERIC, "kernel iteration bound reached (error bits " + std::to_string(err) + ")");
         return WQ3D_OK;
@@ -1247,6 +1391,10 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         q->grow_verb = q->grow_refl = 0;
         q->count_verbs = false;
         for (auto& c : q->verb_counts) c = 0;
+        q->refl_sched = WQ3D_REFLECT_AUTO;
+        q->last_inl = -1;
+        q->in_batch = false;
+        q->chunk_trial[0] = q->chunk_trial[1] = false;
     } else {
         q = new wq3d_queue();
     }
@@ -1445,7 +1593,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
         if ((rc = q->alloc(&h.rec, h.cap_rec)) || (rc = q->alloc(&h.rec_inten, (size_t)h.cap_rec * nf)) ||
             (rc = q->alloc(&h.rec_phase, (size_t)h.cap_rec * nf)) || (rc = q->alloc(&h.refl, h.cap_refl)))
             return cleanup(rc);
-        if ((rc = q->alloc(&q->d_counts, 16)) || (rc = q->alloc(&q->d_base, 1)) ||
+        if ((rc = q->alloc(&q->d_counts, 20)) || (rc = q->alloc(&q->d_base, 1)) ||
             (rc = q->alloc(&q->d_times, (size_t)q->chunk + 1)))
             return cleanup(rc);
     }
@@ -1459,18 +1607,19 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     h.n_work_b[1] = q->d_counts + 10;
     h.n_done = q->d_counts + 6;
     h.n_verb = q->d_counts + 8;
+    h.n_slot = q->d_counts + 16; /* one per shadow set: 16, 17, 18 */
     h.want_verbs = 0;
     h.verb_threshold = 1e-30; /* wave_thresholds.h:40 */
     if (!reuse) {
-        const size_t stride = 54 + 2 * nf;
-        for (int p = 0; p < 2; ++p)
+        const size_t stride = 54 + 3 * nf;
+        for (int p = 0; p < SHADOW_SETS; ++p)
             if ((rc = q->alloc(&h.shadow[p], n * stride)) || (rc = q->alloc(&h.shadow_cnt[p], 3 * n)) ||
                 (rc = q->alloc(&h.shadow_slot[p], n)) || (rc = q->alloc(&h.commit_flag[p], n)))
                 return cleanup(rc);
         if ((rc = q->alloc(&h.work[0], n)) || (rc = q->alloc(&h.work[1], n))) return cleanup(rc);
     }
     /* no ray reflected in the step before the first */
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < SHADOW_SETS; ++p)
         if (cudaMemset(h.commit_flag[p], 0, n) != cudaSuccess)
             return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
     h.d_base = q->d_base;
@@ -1488,7 +1637,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
             q->h_times[s] = reinterpret_cast<double*>(b + 128);
         }
     }
-    if (cudaMemset(q->d_counts, 0, 16 * sizeof(uint32_t)) != cudaSuccess)
+    if (cudaMemset(q->d_counts, 0, 20 * sizeof(uint32_t)) != cudaSuccess)
         return cleanup(fail(WQ3D_ERR_CUDA, "cudaMemset failed"));
 
     /* wave_queue ctor: init_wave, update, init_wavefronts */
@@ -1496,6 +1645,7 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
                  ocean->dev.bot.kind == WQ3D_BOUNDARY_GRID;
     q->k_reflect_fn = q->gridded ? gridded::k_reflect : analytic::k_reflect;
     q->k_advance_fn = q->gridded ? gridded::k_advance : analytic::k_advance;
+    q->k_advance_inline_fn = q->gridded ? gridded::k_advance_inline : analytic::k_advance_inline;
     (q->gridded ? gridded::k_startup : analytic::k_startup)<<<(unsigned)((n + 127) / 128), 128, 0, q->stream>>>(
         h);
     cudaError_t e = cudaStreamSynchronize(q->stream);
@@ -1533,12 +1683,13 @@ int wq3d_queue_create(const wq3d_ocean* ocean, const wq3d_queue_desc* d, wq3d_qu
     if (reuse && std::memcmp(&old_h, &h, sizeof(h)) != 0) q->drop_graph();
     q->reuse = false;
     /* set-up a run would otherwise do on its first chunks: the second
-     * result set and the graphs of the chunks that reflect the next
-     * chunk's first step (rebuilt later only if callbacks, thresholds or
-     * sensitivities change the descriptor); the graphs of a run's last
-     * full chunk are built when first used */
+     * result set and the side-stream graphs of the chunks that reflect
+     * the next chunk's first step (rebuilt later only if callbacks,
+     * thresholds or sensitivities change the descriptor); the graphs of a
+     * run's last full chunk and of the inline schedule are built when
+     * first used */
     q->ensure_set1();
-    for (int p = 0; p < (q->have_set1 ? 2 : 1); ++p) q->build_graph(p, true);
+    for (int p = 0; p < (q->have_set1 ? 2 : 1); ++p) q->build_graph(p, true, false);
     *out = q;
     return WQ3D_OK;
 }
@@ -1666,6 +1817,18 @@ int wq3d_batch_run(wq3d_queue* const* queues, size_t count, const double* time_m
             if (queues[j] == queues[i]) return fail(WQ3D_ERR_INVALID, "queue listed twice in batch");
     }
     DeviceGuard guard(queues[0]->device);
+    /* queues sharing the GPU keep their reflecting rays in compact
+     * k_reflect launches (under WQ3D_REFLECT_AUTO) */
+    struct BatchMark {
+        wq3d_queue* const* qs;
+        size_t n;
+        BatchMark(wq3d_queue* const* q, size_t c) : qs(q), n(c) {
+            for (size_t i = 0; i < n; ++i) qs[i]->in_batch = n > 1;
+        }
+        ~BatchMark() {
+            for (size_t i = 0; i < n; ++i) qs[i]->in_batch = false;
+        }
+    } mark(queues, count);
     std::vector<size_t> left(count), K(count, 0);
     for (size_t i = 0; i < count; ++i) {
         left[i] = queues[i]->steps_until(time_max[i]);
@@ -2115,6 +2278,25 @@ int wq3d_queue_set_timing(wq3d_queue* q, int on) {
             }
     }
     q->timing = on != 0;
+    return WQ3D_OK;
+}
+
+int wq3d_queue_set_reflect_schedule(wq3d_queue* q, int schedule) {
+    if (!q) return fail(WQ3D_ERR_INVALID, "null queue");
+    if (schedule < WQ3D_REFLECT_AUTO || schedule > WQ3D_REFLECT_INLINE)
+        return fail(WQ3D_ERR_INVALID, "unknown reflection schedule");
+    q->refl_sched = schedule;
+    return WQ3D_OK;
+}
+
+int wq3d_queue_reflect_schedule(const wq3d_queue* q, int* schedule) {
+    if (!q || !schedule) return fail(WQ3D_ERR_INVALID, "null argument");
+    if (q->refl_sched != WQ3D_REFLECT_AUTO)
+        *schedule = q->refl_sched;
+    else if (q->last_inl >= 0)
+        *schedule = q->last_inl ? WQ3D_REFLECT_INLINE : WQ3D_REFLECT_SIDE;
+    else
+        *schedule = WQ3D_REFLECT_AUTO;
     return WQ3D_OK;
 }
 

@@ -34,6 +34,7 @@ namespace wq3d {
 constexpr int MAX_FREQ = 64;     /* frequencies per queue                */
 constexpr int RING = 5;          /* wavefront slots                      */
 constexpr int CAND_LISTS = 3;    /* eigenray candidate lists             */
+constexpr int SHADOW_SETS = 3;   /* reflection shadow slot sets          */
 constexpr int MAX_AZ = 4096;     /* AZ fan size (duplicate bit mask)     */
 constexpr int MAX_BOUNCE = 64;   /* reflections of one ray in one step   */
 
@@ -47,7 +48,8 @@ enum : uint32_t {
     ERR_VERB_OVERFLOW = 32u,     /* eigenverb record buffer full               */
     ERR_NONFINITE = 64u,         /* a ray's new position or direction is NaN/Inf */
     ERR_ADJ_OVERFLOW = 128u,     /* adjoint checkpoint or record buffer full    */
-    ERR_BAD_CANDIDATE = 256u     /* a candidate names a ray or target outside the fan (skipped) */
+    ERR_BAD_CANDIDATE = 256u,    /* a candidate names a ray or target outside the fan (skipped) */
+    ERR_SLOT_OVERFLOW = 512u     /* more inline reflections in a step than rays (skipped) */
 };
 
 /* k_advance's decisions for k_commit (QueueDev::commit_flag) */
@@ -151,12 +153,15 @@ struct QueueDev {
     uint32_t* n_work[2];     /* surface part (front of the list)             */
     uint32_t* n_work_b[2];   /* bottom part (back of the list)               */
     uint32_t* n_done;        /* finished blocks of k_reflect              */
-    /* reflections of step s, in set s & 1 (two sets, so that step s+1 can
-     * read step s's slots while k_commit of step s has not yet run) */
-    double* shadow[2];       /* reflected prev/curr/next per worklist slot  */
-    int32_t* shadow_cnt[2];  /* surface, bottom, caustic per slot           */
-    int32_t* shadow_slot[2]; /* worklist slot of each reflecting ray        */
-    uint8_t* commit_flag[2]; /* per ray: COMMIT_* bits k_advance leaves for k_commit */
+    /* reflections of step s, in set shadow_set(s): step s+1 reads step s's
+     * slots while k_commit of step s has not yet run, and an advance that
+     * reflects the following step's rays itself fills a third set while
+     * it reads the two before */
+    double* shadow[SHADOW_SETS];       /* reflected prev/curr/next per slot */
+    int32_t* shadow_cnt[SHADOW_SETS];  /* surface, bottom, caustic per slot */
+    int32_t* shadow_slot[SHADOW_SETS]; /* slot of each reflecting ray       */
+    uint8_t* commit_flag[SHADOW_SETS]; /* per ray: COMMIT_* bits k_advance leaves for k_commit */
+    uint32_t* n_slot;        /* [SHADOW_SETS] slots taken by inline reflections */
     /* eigenray candidates: CAND_LISTS lists by step (cand_list), so the
      * next steps' advance and CPA search fill others while this step's
      * eigenray construction, on its own stream, reads its list */
@@ -198,6 +203,9 @@ struct QueueDev {
 /* the ring slot of step-relative index s (s >= 0) */
 __device__ __forceinline__ int ring_slot(int64_t s) { return (int)(s % RING); }
 
+/* the shadow slot set of the reflections at the start of step s (s >= 0) */
+__device__ __forceinline__ int shadow_set(int64_t s) { return (int)(s % SHADOW_SETS); }
+
 /* The candidate list of the step whose rotated roles start at s (the "s"
  * of the CPA and eigenray kernels, one more than the advance's).  Step k's
  * eigenray construction reads its list while steps k+1 and k+2 fill the
@@ -214,7 +222,8 @@ __device__ __forceinline__ int cand_list(int64_t s) { return (int)((s + 2) % CAN
 #define WQ3D_DECLARE_STEP_KERNELS                         \
     __global__ void k_startup(__grid_constant__ const QueueDev q);         \
     __global__ void k_reflect(__grid_constant__ const QueueDev q, int k);  \
-    __global__ void k_advance(__grid_constant__ const QueueDev q, int k);
+    __global__ void k_advance(__grid_constant__ const QueueDev q, int k);         \
+    __global__ void k_advance_inline(__grid_constant__ const QueueDev q, int k);
 namespace gridded {
 WQ3D_DECLARE_STEP_KERNELS
 }

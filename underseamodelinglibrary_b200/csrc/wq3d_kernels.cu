@@ -277,6 +277,7 @@ struct RayLocal {
     RayS v, c, x;
     double att[MAX_FREQ];
     double ph[MAX_FREQ];
+    double phf[MAX_FREQ];  /* the phases had the caustic hand-off shifted them first */
     int surface, bottom, caustic;
 };
 
@@ -519,6 +520,7 @@ __device__ __noinline__ bool surface_local(const QueueDev& q, const FrontPtrs& C
         }
         L.att[k] += a;
         L.ph[k] -= M_PI;
+        L.phf[k] -= M_PI;
     }
     nd[0] = -nd[0];
     reinit_local(q, L, tw, pos, nd);
@@ -606,6 +608,7 @@ __device__ __noinline__ void bottom_local(const QueueDev& q, const FrontPtrs& C,
         }
         L.att[k] += a;
         L.ph[k] += p;
+        L.phf[k] += p;
     }
     dot_full *= 2.0;
     ndir[0] = ndir[0] - dot_full * nrm[0];
@@ -648,7 +651,12 @@ __device__ __forceinline__ void work_append(const QueueDev& q, int p, uint8_t ki
 /* shadow slot of a reflecting ray: prev, curr, next (17 doubles each), the
  * next front's attenuation and phase (nf each), and the three loss
  * tangents its bottom bounces add; counts in shadow_cnt */
-__device__ __forceinline__ size_t shadow_stride(const QueueDev& q) { return 54 + 2 * (size_t)q.nf; }
+/* a shadow slot: prev, curr and next states (17 doubles each), the next
+ * front's attenuation and phase (nf each), the three loss tangents of the
+ * step's bottom bounces, and the phases again as they are when the caustic
+ * hand-off of the neighbour below shifted them by -pi/2 before the
+ * reflection (nf) */
+__device__ __forceinline__ size_t shadow_stride(const QueueDev& q) { return 54 + 3 * (size_t)q.nf; }
 
 __device__ __forceinline__ void ray_to(double* dst, const RayS& y) {
     for (int k = 0; k < 3; ++k) {
@@ -683,7 +691,7 @@ __device__ __forceinline__ void ray_from(const double* src, RayS& y) {
  * at step s-1 and the fronts hold its states. */
 __device__ __forceinline__ const double* prev_step_slot(const QueueDev& q, int64_t s, int i,
                                                         const int32_t** cnt = nullptr) {
-    const int p = (int)((s + 1) & 1); /* the set of step s-1 */
+    const int p = shadow_set(s + SHADOW_SETS - 1); /* the set of step s-1 */
     if (!(__ldg(q.commit_flag[p] + i) & COMMIT_REFLECT)) return nullptr;
     const int32_t w = __ldg(q.shadow_slot[p] + i);
     if (cnt) *cnt = q.shadow_cnt[p] + 3 * (size_t)w;
@@ -781,12 +789,95 @@ __global__ void __launch_bounds__(128) k_startup(__grid_constant__ const QueueDe
 /* then every ray advances                                             */
 /* ------------------------------------------------------------------ */
 
-/* Reflecting rays of step s (listed by the launch that produced the
- * "next" front): caustic hand-off from the D/E neighbour below, then the
- * surface/bottom reflection chain (wave_queue.cc:197-256) on a private
- * copy of the ray.  The result goes to the ray's shadow slot; k_advance
- * commits it.  The fronts are only read here, so this kernel runs
- * concurrently with k_cpa / k_eigenray of step s-1. */
+/* The reflection chain of ray i at the start of step s (wave_queue.cc:
+ * 197-256) on L: the ray's prev, curr and next states, counts and next-front
+ * losses before the step's reflections.  The result goes to slot w of set
+ * shadow_set(s); k_advance of step s takes it from there.  The caustic
+ * hand-off from the D/E neighbour below (wave_queue.cc:274-292), which the
+ * reference runs before the ray reflects, is decided by k_advance of step
+ * s, when that neighbour's next front is complete; the slot carries the
+ * phases both without and with its -pi/2 shift. */
+__device__ __forceinline__ void reflect_chain_body(const QueueDev& q, int64_t s, int i, uint32_t w,
+                                                   RayLocal& L, double t_old) {
+    Roles R;
+    roles_at(q, s, R);
+    for (int f = 0; f < q.nf; ++f) L.phf[f] = L.ph[f] - M_PI_2;
+    /* the reference's detect_reflections for this ray: volume layers,
+     * then the surface / bottom chain, volume layers after each
+     * reflection (wave_queue.cc:202-256); seq orders the ray's events */
+    const bool vol = q.want_verbs && q.oc.nvol > 0;
+    double dl[3] = {0.0, 0.0, 0.0};
+    bool reflected = false;
+    int seq = 0;
+    int next_try = -1; /* 0: try bottom next, 1: try surface next */
+    if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
+    if (L.x.pos[0] - q.R > 0.0 && surface_local(q, *R.C, L, i, s + 1, t_old, seq)) {
+        L.surface += 1;
+        reflected = true;
+        next_try = 0;
+    } else {
+        const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
+        if (depth > 0.0) {
+            bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq, dl);
+            L.bottom += 1;
+            reflected = true;
+            next_try = 1;
+        }
+    }
+    if (reflected) {
+        if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
+        int it = 0;
+        for (; it < MAX_BOUNCE; ++it) {
+            if (next_try == 0) {
+                const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
+                if (!(depth > 0.0)) break;
+                bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq, dl);
+                L.bottom += 1;
+                next_try = 1;
+            } else {
+                if (!(L.x.pos[0] - q.R > 0.0 && surface_local(q, *R.C, L, i, s + 1, t_old, seq))) break;
+                L.surface += 1;
+                next_try = 0;
+            }
+            if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
+        }
+        if (it == MAX_BOUNCE) set_err(q, ERR_BOUNCE_LIMIT);
+    }
+    const int set = shadow_set(s);
+    const size_t stride = shadow_stride(q);
+    double* sh = q.shadow[set] + (size_t)w * stride;
+    ray_to(sh, L.v);
+    ray_to(sh + 17, L.c);
+    ray_to(sh + 34, L.x);
+    for (int f = 0; f < q.nf; ++f) {
+        sh[51 + f] = L.att[f];
+        sh[51 + q.nf + f] = L.ph[f];
+        sh[54 + 2 * q.nf + f] = L.phf[f];
+    }
+    /* the next front's loss tangents take this step's bottom bounces
+     * when k_commit applies the slot; the previous step's eigenray
+     * construction may still be reading them */
+    if (q.sens)
+        for (int j = 0; j < 3; ++j) sh[51 + 2 * q.nf + j] = dl[j];
+    q.shadow_cnt[set][3 * (size_t)w] = L.surface;
+    q.shadow_cnt[set][3 * (size_t)w + 1] = L.bottom;
+    q.shadow_cnt[set][3 * (size_t)w + 2] = L.caustic;
+    q.shadow_slot[set][i] = (int32_t)w;
+}
+
+/* out of line for the inline schedule's advance, whose other rays need
+ * none of its registers */
+__device__ __noinline__ void reflect_chain(const QueueDev& q, int64_t s, int i, uint32_t w, RayLocal& L,
+                                           double t_old) {
+    reflect_chain_body(q, s, i, w, L, t_old);
+}
+
+/* Reflecting rays of step s listed by the launch that produced the "next"
+ * front: the reflection chain on a private copy of each ray.  The fronts
+ * are only read here, so this kernel runs concurrently with k_cpa /
+ * k_eigenray of step s-1.  (k_advance reflects the following step's rays
+ * itself where nothing in between needs the committed fronts; this kernel
+ * then finds an empty list.) */
 __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev q, int k) {
     const int64_t s = *q.d_base + k;
     const uint32_t nsurf = min(*q.n_work[s & 1], (uint32_t)q.n);
@@ -795,9 +886,6 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
     const double t_old = q.d_times[k];
     Roles R;
     roles_at(q, s, R);
-    const uint8_t* flag_in = q.flag[s & 1];
-    const size_t stride = shadow_stride(q);
-    const int set = (int)(s & 1);
     for (uint32_t ww = blockIdx.x * blockDim.x + threadIdx.x; ww < nwork; ww += gridDim.x * blockDim.x) {
         /* list slot: surface part at the front, bottom part at the back */
         const uint32_t w = ww < nsurf ? ww : (uint32_t)q.n - 1 - (ww - nsurf);
@@ -808,90 +896,18 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
             RayS v, c, x;
             load_prev_curr(q, s, R, i, v, c);
             load_ray_ro(*R.X, i, x);
-            const int sf = __ldg(R.X->surface + i), bt = __ldg(R.X->bottom + i), cs = __ldg(R.X->caustic + i);
             L.v = v;
             L.c = c;
             L.x = x;
-            L.surface = sf;
-            L.bottom = bt;
-            L.caustic = cs;
+            L.surface = __ldg(R.X->surface + i);
+            L.bottom = __ldg(R.X->bottom + i);
+            L.caustic = __ldg(R.X->caustic + i);
         }
         for (int f = 0; f < q.nf; ++f) {
             L.att[f] = __ldg(R.X->atten + (size_t)f * q.n + i);
             L.ph[f] = __ldg(R.X->phase + (size_t)f * q.n + i);
         }
-        /* detect_caustics of the neighbour below (wave_queue.cc:274-292),
-         * which the reference runs before this ray reflects; that
-         * neighbour is read only when it does not reflect */
-        const int d = i / q.naz;
-        if (d >= 1 && !flag_in[i - q.naz]) {
-            const int j = i - q.naz;
-            const double A = L.c.pos[0], B = curr_rho(q, s, R, j);
-            const double Cc = L.x.pos[0], D = R.X->pos[0][j];
-            const bool fold = (L.surface == R.X->surface[j]) && (L.bottom == R.X->bottom[j]);
-            if ((Cc - D) * (A - B) < 0 && fold) {
-                L.caustic += 1;
-                for (int f = 0; f < q.nf; ++f) L.ph[f] -= M_PI_2;
-            }
-        }
-        /* the reference's detect_reflections for this ray: volume layers,
-         * then the surface / bottom chain, volume layers after each
-         * reflection (wave_queue.cc:202-256); seq orders the ray's events */
-        const bool vol = q.want_verbs && q.oc.nvol > 0;
-        double dl[3] = {0.0, 0.0, 0.0};
-        bool reflected = false;
-        int seq = 0;
-        int next_try = -1; /* 0: try bottom next, 1: try surface next */
-        if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
-        if (L.x.pos[0] - q.R > 0.0 && surface_local(q, *R.C, L, i, s + 1, t_old, seq)) {
-            L.surface += 1;
-            reflected = true;
-            next_try = 0;
-        } else {
-            const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
-            if (depth > 0.0) {
-                bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq, dl);
-                L.bottom += 1;
-                reflected = true;
-                next_try = 1;
-            }
-        }
-        if (reflected) {
-            if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
-            int it = 0;
-            for (; it < MAX_BOUNCE; ++it) {
-                if (next_try == 0) {
-                    const double depth = boundary_height(q.oc.bot, L.x.pos[1], L.x.pos[2]) - L.x.pos[0];
-                    if (!(depth > 0.0)) break;
-                    bottom_local(q, *R.C, L, i, depth, s + 1, t_old, seq, dl);
-                    L.bottom += 1;
-                    next_try = 1;
-                } else {
-                    if (!(L.x.pos[0] - q.R > 0.0 && surface_local(q, *R.C, L, i, s + 1, t_old, seq))) break;
-                    L.surface += 1;
-                    next_try = 0;
-                }
-                if (vol) volume_scatter(q, *R.C, i, s + 1, t_old, L.v, L.c, L.x, L.surface, L.bottom, seq);
-            }
-            if (it == MAX_BOUNCE) set_err(q, ERR_BOUNCE_LIMIT);
-        }
-        double* sh = q.shadow[set] + (size_t)w * stride;
-        ray_to(sh, L.v);
-        ray_to(sh + 17, L.c);
-        ray_to(sh + 34, L.x);
-        for (int f = 0; f < q.nf; ++f) {
-            sh[51 + f] = L.att[f];
-            sh[51 + q.nf + f] = L.ph[f];
-        }
-        /* the next front's loss tangents take this step's bottom bounces
-         * when k_commit applies the slot; the previous step's eigenray
-         * construction may still be reading them */
-        if (q.sens)
-            for (int j = 0; j < 3; ++j) sh[51 + 2 * q.nf + j] = dl[j];
-        q.shadow_cnt[set][3 * (size_t)w] = L.surface;
-        q.shadow_cnt[set][3 * (size_t)w + 1] = L.bottom;
-        q.shadow_cnt[set][3 * (size_t)w + 2] = L.caustic;
-        q.shadow_slot[set][i] = (int32_t)w;
+        reflect_chain_body(q, s, i, w, L, t_old);
     }
     /* the last block to finish empties this step's worklist, which the
      * advance of step s+1 refills (every block has read the count by then;
@@ -921,10 +937,15 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
 #else
 #define WQ_ADVANCE_BOUNDS __launch_bounds__(128, 5)
 #endif
-__global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, int k) {
+template <bool INLINE>
+__device__ __forceinline__ void advance_body(const QueueDev& q, int k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t s = *q.d_base + k;
-    if (blockIdx.x == 0 && threadIdx.x == 0) q.n_cand[cand_list(s + 1)] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        q.n_cand[cand_list(s + 1)] = 0;
+        /* the slot count the next step's inline reflections start from */
+        q.n_slot[shadow_set(s + 2)] = 0;
+    }
     if (i >= q.n) return;
     Roles R;
     roles_at(q, s, R);
@@ -952,7 +973,7 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
     /* one round of loads: this ray on the three fronts, and the rows
      * d-2 .. d+2 that detect_caustics and find_edges may read (rows
      * clamped to the fan; a clamped row is never used) */
-    const int set = (int)(s & 1);
+    const int set = shadow_set(s);
     if (!refl) load_prev_curr(q, s, R, i, y0, y1);
     load_ray_ro(*R.X, i, y2);
     int32_t sf = __ldg(R.X->surface + i);
@@ -993,6 +1014,18 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
         sf = __ldg(q.shadow_cnt[set] + 3 * (size_t)w);
         bt = __ldg(q.shadow_cnt[set] + 3 * (size_t)w + 1);
         cs = __ldg(q.shadow_cnt[set] + 3 * (size_t)w + 2);
+        /* detect_caustics of the neighbour below on this ray's states
+         * before its reflection (wave_queue.cc:274-292: the reference runs
+         * it first); the fronts still hold them until k_commit */
+        if (d >= 1 && !fl[1]) {
+            const double A = curr_rho(q, s, R, i), B = c_below;
+            const double Cc = __ldg(R.X->pos[0] + i), D = x_below;
+            const bool fold = (__ldg(R.X->surface + i) == sf_below) && (__ldg(R.X->bottom + i) == bt_below);
+            if ((Cc - D) * (A - B) < 0 && fold) {
+                fold_hit = true;
+                cs += 1;
+            }
+        }
     } else {
         /* detect_caustics of the neighbour below (wave_queue.cc:274-292) */
         if (d >= 1 && !fl[1]) {
@@ -1085,7 +1118,7 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
         double ax, px;
         if (refl) {
             ax = __ldg(sh + 51 + f);
-            px = __ldg(sh + 51 + q.nf + f);
+            px = __ldg(sh + (fold_hit ? 54 + 2 * q.nf : 51 + q.nf) + f);
         } else {
             ax = __ldg(R.X->atten + o);
             px = __ldg(R.X->phase + o);
@@ -1104,7 +1137,52 @@ __global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, 
         P.phase[o] = p;
     }
     flag_out[i] = f_next;
-    if (f_next) work_append(q, (int)((s + 1) & 1), f_next, i);
+    if (!f_next) return;
+    if (!INLINE) {
+        work_append(q, (int)((s + 1) & 1), f_next, i);
+        return;
+    }
+    /* the reflections of step s+1 right here: this ray's prev and curr
+     * states at step s+1 are its curr and next at step s, its next the
+     * front just written (read back by this thread) */
+    RayLocal L;
+    if (refl) {
+        ray_from(sh + 17, L.v);
+        ray_from(sh + 34, L.c);
+    } else {
+        const double* sp = prev_step_slot(q, s, i);
+        if (sp)
+            ray_from(sp + 34, L.v);
+        else
+            load_ray_ro(*R.C, i, L.v);
+        load_ray_ro(*R.X, i, L.c);
+    }
+    L.x = y3;
+    L.surface = sf;
+    L.bottom = bt;
+    L.caustic = cs;
+    for (int f = 0; f < q.nf; ++f) {
+        L.att[f] = P.atten[(size_t)f * q.n + i];
+        L.ph[f] = P.phase[(size_t)f * q.n + i];
+    }
+    const uint32_t w = atomicAdd(q.n_slot + shadow_set(s + 1), 1u);
+    if (w >= (uint32_t)q.n) {
+        set_err(q, ERR_SLOT_OVERFLOW);
+        return;
+    }
+    reflect_chain(q, s + 1, i, w, L, q.d_times[k + 1]);
+}
+
+/* the side schedule: the reflecting rays of step s+1 go to the worklist
+ * of k_reflect */
+__global__ void WQ_ADVANCE_BOUNDS k_advance(__grid_constant__ const QueueDev q, int k) {
+    advance_body<false>(q, k);
+}
+
+/* the inline schedule: each thread runs step s+1's reflection chain of
+ * its ray itself */
+__global__ void WQ_ADVANCE_BOUNDS k_advance_inline(__grid_constant__ const QueueDev q, int k) {
+    advance_body<true>(q, k);
 }
 
 }  // namespace WQ3D_KERNEL_NS
@@ -1124,7 +1202,7 @@ __global__ void __launch_bounds__(128) k_commit(__grid_constant__ const QueueDev
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= q.n) return;
     const int64_t s = *q.d_base + k;
-    const int set = (int)(s & 1);
+    const int set = shadow_set(s);
     const uint8_t b = q.commit_flag[set][i];
     if (!b) return;
     Roles R;
@@ -1145,10 +1223,13 @@ __global__ void __launch_bounds__(128) k_commit(__grid_constant__ const QueueDev
         copy_ray(*R.X, i, y);
         R.V->surface[i] = R.C->surface[i] = R.X->surface[i] = cnt[0];
         R.V->bottom[i] = R.C->bottom[i] = R.X->bottom[i] = cnt[1];
-        R.X->caustic[i] = cnt[2];
+        /* with the caustic hand-off k_advance found before the reflection */
+        const bool fold = (b & COMMIT_FOLD) != 0;
+        R.X->caustic[i] = cnt[2] + (fold ? 1 : 0);
+        const double* ph = sh + (fold ? 54 + 2 * q.nf : 51 + q.nf);
         for (int f = 0; f < q.nf; ++f) {
             R.X->atten[(size_t)f * q.n + i] = sh[51 + f];
-            R.X->phase[(size_t)f * q.n + i] = sh[51 + q.nf + f];
+            R.X->phase[(size_t)f * q.n + i] = ph[f];
         }
         if (q.sens)
             for (int j = 0; j < 3; ++j) R.X->dA[(size_t)j * q.n + i] += sh[51 + 2 * q.nf + j];

@@ -501,6 +501,19 @@ class wave_queue:
     def set_timing(self, on):
         _abi.check(self._lib, self._lib.wq3d_queue_set_timing(self._q, 1 if on else 0))
 
+    def set_reflect_schedule(self, schedule):
+        """where a step's reflections run (wq3d_queue_set_reflect_schedule):
+        _abi.REFLECT_AUTO (tuned), REFLECT_SIDE or REFLECT_INLINE; the
+        results do not depend on it"""
+        _abi.check(self._lib, self._lib.wq3d_queue_set_reflect_schedule(self._q, int(schedule)))
+
+    def reflect_schedule(self):
+        """the schedule in use: REFLECT_SIDE, REFLECT_INLINE, or
+        REFLECT_AUTO while still tuning"""
+        v = C.c_int()
+        _abi.check(self._lib, self._lib.wq3d_queue_reflect_schedule(self._q, C.byref(v)))
+        return v.value
+
     def timing(self, reset=False):
         """device milliseconds since the last reset (wq3d_queue_timing): the
         whole step/run calls, and per kernel while timing mode is on"""
