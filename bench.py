@@ -70,6 +70,8 @@ def parse():
                     help="workload of --profile-steps (std14: the speed study with 100 targets; "
                          "gridded: one 1801 x 45 ray instance of the batched gridded workload's "
                          "environment, 64 targets, dt 0.05 s)")
+    ap.add_argument("--profile-schedule", default="auto", choices=["auto", "side", "inline"],
+                    help="reflection schedule of the --profile-steps queue")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="profiling mode: one queue of the workload, this many wave steps, no output")
     return ap.parse_args()
@@ -782,6 +784,8 @@ def main():
         else:
             sc = S.linear_slope_rayleigh()
         q = S.build_queue(sc, u.wave_queue, device=0, precision=_abi.FP32C)
+        q.set_reflect_schedule({"auto": _abi.REFLECT_AUTO, "side": _abi.REFLECT_SIDE,
+                                "inline": _abi.REFLECT_INLINE}[args.profile_schedule])
         q.step(args.profile_steps)
         print("profile run: %d steps, %d eigenrays" % (q.steps(), len(q.take_eigenrays())))
         return

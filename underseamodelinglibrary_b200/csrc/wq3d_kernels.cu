@@ -1515,7 +1515,7 @@ __device__ __forceinline__ float screen_dot(const TgtW& g, const float* d) {
     return a + b;
 }
 
-__global__ void __launch_bounds__(CPA_THREADS, 5) k_cpa_f32(__grid_constant__ const QueueDev q, int k) {
+__global__ void __launch_bounds__(CPA_THREADS, 3) k_cpa_f32(__grid_constant__ const QueueDev q, int k) {
     __shared__ TgtS tile[F32_TARGETS];
     __shared__ TgtW tw[F32_TARGETS];
     __shared__ float wmax[CPA_THREADS / 32][8];
