@@ -616,14 +616,12 @@ struct wq3d_queue {
         const int eig_blocks = std::min(EIG_BLOCKS, std::max(148, (n + 255) / 256));
         if (timing) tail = false;
         auto cpa_launch = [&](int k, cudaStream_t st) {
+            const dim3 cgrid(((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) * ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
+                             (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS);
             if (h.precision != WQ3D_FP64)
-                k_cpa_f32<<<dim3(((h.nde + CPA_PATCH_DE - 1) / CPA_PATCH_DE) *
-                                     ((h.naz + CPA_PATCH_AZ - 1) / CPA_PATCH_AZ),
-                                 (h.nt + CPA_F32_TARGETS - 1) / CPA_F32_TARGETS),
-                            CPA_THREADS, 0, st>>>(d, k);
+                k_cpa_f32<<<cgrid, CPA_THREADS, 0, st>>>(d, k);
             else
-                k_cpa<<<dim3((n + CPA_THREADS - 1) / CPA_THREADS, (h.nt + CPA_TARGETS - 1) / CPA_TARGETS),
-                        CPA_THREADS, 0, st>>>(d, k);
+                k_cpa<<<cgrid, CPA_THREADS, 0, st>>>(d, k);
         };
         auto eig_launch = [&](int k, cudaStream_t st) {
             k_eigenray<<<eig_blocks, 128, 0, st>>>(d, k);

@@ -294,7 +294,6 @@ __global__ void k_adj_startup(AdjSweep a, __grid_constant__ const QueueDev q);
 
 
 constexpr int CPA_THREADS = 128;     /* rays per CPA block            */
-constexpr int CPA_TARGETS = 64;      /* targets per FP64 CPA block    */
 constexpr int CPA_F32_TARGETS = 256; /* targets per FP32C CPA tile    */
 constexpr int CPA_PATCH_AZ = 8;      /* FP32C CPA block: 16 D/E x 8 AZ rays */
 constexpr int CPA_PATCH_DE = CPA_THREADS / CPA_PATCH_AZ;

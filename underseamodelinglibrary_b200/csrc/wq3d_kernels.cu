@@ -2,24 +2,28 @@
  * wq3d_kernels.cu -- FP64 WaveQ3D propagation kernels for sm_100a.
  *
  * One step of wave_queue::step() (waveq3d/wave_queue.cc:155-192) is five
- * launches:
+ * launches (four under the inline reflection schedule):
  *   k_reflect   one thread per ray on the worklist of rays that reflect in
- *               this step: caustic hand-off from the D/E neighbour and the
- *               surface/bottom reflection chain with the RK3
- *               re-initialisation, on a private copy of the ray written to
- *               its shadow slot.  It only reads the fronts, so it runs on a
- *               side stream beside the previous step's k_cpa / k_eigenray.
- *   k_advance   one thread per ray: caustic hand-off and vertices,
+ *               this step: the surface/bottom reflection chain with the RK3
+ *               re-initialisation (reflect_chain), on a private copy of the
+ *               ray written to its shadow slot.  It only reads the fronts,
+ *               so it runs on a side stream beside the previous step's
+ *               k_cpa / k_eigenray.
+ *   k_advance   one thread per ray: caustic hand-off (for a reflecting ray
+ *               on its states before the reflection) and vertices,
  *               wave_front::find_edges (reflecting rays read from their
  *               shadow slots), the queue rotation, the AB3 step and
  *               wave_front::update of the new front, and the next step's
- *               reflection worklist.
+ *               reflection worklist; k_advance_inline runs the next step's
+ *               reflection chains itself instead.
  *   k_commit    writes the reflected rays' slots and the caustic and vertex
  *               counts into the fronts, on the eigenray stream.
- *   k_cpa       rays x targets: closest-point-of-approach test
- *               (detect_eigenrays + is_closest_ray) with distance2
- *               recomputed from per-front terms; k_cpa_f32 is its FP32
- *               screen with an exact FP64 finish.
+ *   k_cpa       closest-point-of-approach test (detect_eigenrays +
+ *               is_closest_ray) over patches of neighbouring rays x tiles
+ *               of targets, with distance2 recomputed from per-front terms
+ *               and targets no ray of a patch can keep dropped first;
+ *               k_cpa_f32 screens each pair in FP32 before the FP64
+ *               comparisons.
  *   k_eigenray  one warp per CPA found: build_eigenray, compute_offsets,
  *               hybrid Gaussian or classic spreading, target angles.
  *
@@ -1349,47 +1353,8 @@ __device__ bool is_closest(const QueueDev& q, const FrontPtrs& V, const FrontPtr
 
 }  // namespace
 
-__global__ void __launch_bounds__(CPA_THREADS) k_cpa(__grid_constant__ const QueueDev q, int k) {
-    __shared__ TgtS tile[CPA_TARGETS];
-    const int64_t s = *q.d_base + k + 1; /* roles after this step's rotation */
-    const FrontPtrs& V = q.F[ring_slot(s + 1)];
-    const FrontPtrs& C = q.F[ring_slot(s + 2)];
-    const FrontPtrs& X = q.F[ring_slot(s + 3)];
-    const int t0 = blockIdx.y * CPA_TARGETS;
-    const int nt_tile = min(CPA_TARGETS, q.nt - t0);
-    for (int j = threadIdx.x; j < nt_tile; j += blockDim.x) {
-        const int t = t0 + j;
-        tile[j] = TgtS{q.tgt[1][t], q.tgt[2][t], q.tgt_sin[t], q.tgt_R2[t], q.tgt_2R[t]};
-    }
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= q.n) return;
-    /* the spreading models need a 3 x 3 fan (wave_queue.cc:88); the
-     * reference would dereference a null model on a wrapped 2-ray AZ fan */
-    if (q.nde < 3 || q.naz < 3) return;
-    const int de = i / q.naz, az = i % q.naz;
-    const int az_start = q.az_boundary ? 0 : 1;
-    if (de < 1 || de >= q.nde - 1 || az < az_start || az >= q.naz - 1) return;
-    if (C.on_edge[i]) return;
-    const double rC = C.cpa[0][i], tC = C.cpa[1][i], pC = C.cpa[2][i], sC = C.cpa[3][i];
-    const double rX = X.cpa[0][i], tX = X.cpa[1][i], pX = X.cpa[2][i], sX = X.cpa[3][i];
-    const double rV = V.cpa[0][i], tV = V.cpa[1][i], pV = V.cpa[2][i], sV = V.cpa[3][i];
-    const double rC2 = rC * rC, rX2 = rX * rX, rV2 = rV * rV;
-    for (int j = 0; j < nt_tile; ++j) {
-        const TgtS t = tile[j];
-        const double center = target_distance2(rC, rC2, tC, pC, sC, t.th, t.ph, t.sn, t.R2, t.twoR);
-        const double dn = target_distance2(rX, rX2, tX, pX, sX, t.th, t.ph, t.sn, t.R2, t.twoR);
-        if (dn <= center) continue;
-        const double dp = target_distance2(rV, rV2, tV, pV, sV, t.th, t.ph, t.sn, t.R2, t.twoR);
-        if (dp < center) continue;
-        double cube[3][3][3];
-        if (!is_closest(q, V, C, X, t, q.de_branch[t0 + j] != 0, de, az, center, cube)) continue;
-        cand_push(q, s, (uint32_t)(t0 + j), (uint32_t)i);
-    }
-}
-
 /* ------------------------------------------------------------------ */
-/* CPA search with an FP32 screen (FP32C form)                         */
+/* CPA search over ray patches, with an FP32 screen in the FP32C form     */
 /* ------------------------------------------------------------------ */
 /* The comparisons that reject almost every (ray, target) pair -- "next <=
  * curr" and "prev < curr" on distance2 (wave_queue.cc:386-393) -- are
@@ -1409,8 +1374,10 @@ __global__ void __launch_bounds__(CPA_THREADS) k_cpa(__grid_constant__ const Que
  * for the rounding of the reference's FP64 expression on the two fronts
  * (each within 5 x 2^-53 (rho^2 + R^2), 0.05 m^2 at earth radius).  The
  * screen only rejects; every pair it does not reject is queued per warp and
- * finished in FP64 exactly as k_cpa does, 32 at a time so the lanes stay
- * converged.  Hence the eigenrays equal the FP64 form's.
+ * finished with the FP64 comparisons, 32 at a time so the lanes stay
+ * converged.  Hence the eigenrays equal the FP64 form's, which runs the
+ * same patch search with every surviving pair going to those comparisons
+ * (k_cpa).
  *
  * A block holds a patch of CPA_PATCH_DE x CPA_PATCH_AZ neighbouring rays,
  * whose positions and directions are close, so for a given target the
@@ -1515,7 +1482,11 @@ __device__ __forceinline__ float screen_dot(const TgtW& g, const float* d) {
     return a + b;
 }
 
-__global__ void __launch_bounds__(CPA_THREADS, 3) k_cpa_f32(__grid_constant__ const QueueDev q, int k) {
+/* The patch search; SCREEN decides the per-pair comparisons in FP32 first
+ * (FP32C form), otherwise every pair of the patch's surviving targets goes
+ * to the FP64 comparisons (FP64 form) */
+template <bool SCREEN>
+__device__ __forceinline__ void cpa_patch(const QueueDev& q, int k) {
     __shared__ TgtS tile[F32_TARGETS];
     __shared__ TgtW tw[F32_TARGETS];
     __shared__ float wmax[CPA_THREADS / 32][8];
@@ -1677,12 +1648,16 @@ __global__ void __launch_bounds__(CPA_THREADS, 3) k_cpa_f32(__grid_constant__ co
         for (; sidx + 1 < ns; sidx += 2) {
             const int j0 = surv[sidx], j1 = surv[sidx + 1];
             const TgtW g0 = tw[j0], g1 = tw[j1];
-            const float a0 = screen_dot(g0, dxc), a1 = screen_dot(g1, dxc);
-            bool w0 = active && !(a0 < -gxc), w1 = active && !(a1 < -gxc);
-            if (w0 || w1) {
-                const float b0 = screen_dot(g0, dvc), b1 = screen_dot(g1, dvc);
-                w0 = w0 && !(b0 < -gvc);
-                w1 = w1 && !(b1 < -gvc);
+            bool w0 = active, w1 = active;
+            if (SCREEN) {
+                const float a0 = screen_dot(g0, dxc), a1 = screen_dot(g1, dxc);
+                w0 = w0 && !(a0 < -gxc);
+                w1 = w1 && !(a1 < -gxc);
+                if (w0 || w1) {
+                    const float b0 = screen_dot(g0, dvc), b1 = screen_dot(g1, dvc);
+                    w0 = w0 && !(b0 < -gvc);
+                    w1 = w1 && !(b1 < -gvc);
+                }
             }
             push(w0, j0);
             push(w1, j1);
@@ -1690,12 +1665,25 @@ __global__ void __launch_bounds__(CPA_THREADS, 3) k_cpa_f32(__grid_constant__ co
         if (sidx < ns) {
             const int j = surv[sidx];
             const TgtW g = tw[j];
-            bool want = active && !(screen_dot(g, dxc) < -gxc);
-            if (want) want = !(screen_dot(g, dvc) < -gvc);
+            bool want = active;
+            if (SCREEN) {
+                want = want && !(screen_dot(g, dxc) < -gxc);
+                if (want) want = !(screen_dot(g, dvc) < -gvc);
+            }
             push(want, j);
         }
         if (qn > 0) cpa_finish(q, s, V, C, X, tile, t0, de0, az0, myq, qn, lane);
     }
+}
+
+/* four resident blocks (128 registers): the reflection chain that runs
+ * beside the search keeps issue slots */
+__global__ void __launch_bounds__(CPA_THREADS, 3) k_cpa_f32(__grid_constant__ const QueueDev q, int k) {
+    cpa_patch<true>(q, k);
+}
+
+__global__ void __launch_bounds__(CPA_THREADS, 3) k_cpa(__grid_constant__ const QueueDev q, int k) {
+    cpa_patch<false>(q, k);
 }
 
 /* ------------------------------------------------------------------ */
