@@ -8,7 +8,10 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libwq3d.so")
+# WQ3D_LIBRARY=checked selects the build whose kernels test every index
+# they read from device data (libwq3d_checked.so, made by build.py)
+LIB_PATH = os.path.join(HERE, "libwq3d_checked.so" if os.environ.get("WQ3D_LIBRARY") == "checked"
+                        else "libwq3d.so")
 
 WQ3D_OK = 0
 WQ3D_ERR_INVALID = -1

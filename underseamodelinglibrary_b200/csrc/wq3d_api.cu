@@ -1006,6 +1006,9 @@ struct wq3d_queue {
         if (err & ERR_BAD_CANDIDATE)
             return fail(WQ3D_ERR_CUDA, "internal error: an eigenray candidate named a ray or target outside "
                                        "the fan (error bits " + std::to_string(err) + ")");
+        if (err & ERR_BOUNDS)
+            return fail(WQ3D_ERR_CUDA, "internal error: a bounds check of the checked build failed (error bits " +
+                                           std::to_string(err) + ")");
         if (err & ERR_SLOT_OVERFLOW)
             return fail(WQ3D_ERR_CUDA, "internal error: more reflecting rays in a step than rays (error bits " +
                                            std::to_string(err) + ")");

@@ -49,8 +49,31 @@ enum : uint32_t {
     ERR_NONFINITE = 64u,         /* a ray's new position or direction is NaN/Inf */
     ERR_ADJ_OVERFLOW = 128u,     /* adjoint checkpoint or record buffer full    */
     ERR_BAD_CANDIDATE = 256u,    /* a candidate names a ray or target outside the fan (skipped) */
-    ERR_SLOT_OVERFLOW = 512u     /* more inline reflections in a step than rays (skipped) */
+    ERR_SLOT_OVERFLOW = 512u,    /* more inline reflections in a step than rays (skipped) */
+    ERR_BOUNDS = 1024u           /* WQ3D_CHECKED build: an index read from device data was out of range */
 };
+
+/* The WQ3D_CHECKED build (libwq3d_checked.so) tests every index a kernel
+ * reads from device data -- worklist entries, shadow slot numbers,
+ * queued CPA pairs -- before it uses one: a failed test sets ERR_BOUNDS
+ * and takes the given way out instead of the access.  The default build
+ * compiles the tests away. */
+#ifndef WQ3D_CHECKED
+#define WQ3D_CHECKED 0
+#endif
+#if WQ3D_CHECKED
+#define WQ_CHECKED_OR(q, cond, action)         \
+    do {                                       \
+        if (!(cond)) {                         \
+            atomicOr((q).err, wq3d::ERR_BOUNDS); \
+            action;                            \
+        }                                      \
+    } while (0)
+#else
+#define WQ_CHECKED_OR(q, cond, action) \
+    do {                               \
+    } while (0)
+#endif
 
 /* k_advance's decisions for k_commit (QueueDev::commit_flag) */
 enum : uint8_t { COMMIT_REFLECT = 1, COMMIT_FOLD = 2, COMMIT_UPPER = 4, COMMIT_LOWER = 8 };

@@ -698,6 +698,7 @@ __device__ __forceinline__ const double* prev_step_slot(const QueueDev& q, int64
     const int p = shadow_set(s + SHADOW_SETS - 1); /* the set of step s-1 */
     if (!(__ldg(q.commit_flag[p] + i) & COMMIT_REFLECT)) return nullptr;
     const int32_t w = __ldg(q.shadow_slot[p] + i);
+    WQ_CHECKED_OR(q, w >= 0 && w < q.n, return nullptr);
     if (cnt) *cnt = q.shadow_cnt[p] + 3 * (size_t)w;
     return q.shadow[p] + (size_t)w * shadow_stride(q);
 }
@@ -894,6 +895,7 @@ __global__ void __launch_bounds__(64) k_reflect(__grid_constant__ const QueueDev
         /* list slot: surface part at the front, bottom part at the back */
         const uint32_t w = ww < nsurf ? ww : (uint32_t)q.n - 1 - (ww - nsurf);
         const int i = (int)work[w];
+        WQ_CHECKED_OR(q, i >= 0 && i < q.n, continue);
         RayLocal L;
         {
             /* the fronts are read-only here */
@@ -999,7 +1001,9 @@ __device__ __forceinline__ void advance_body(const QueueDev& q, int k) {
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
         if (fl[t]) {
-            const double* shj = q.shadow[set] + (size_t)__ldg(q.shadow_slot[set] + jrow[t]) * stride;
+            const int32_t wj = __ldg(q.shadow_slot[set] + jrow[t]);
+            WQ_CHECKED_OR(q, wj >= 0 && wj < q.n, return);
+            const double* shj = q.shadow[set] + (size_t)wj * stride;
             rr[t] = __ldg(shj + 34);
             nn[t] = __ldg(shj + 34 + 6);
         }
@@ -1011,6 +1015,7 @@ __device__ __forceinline__ void advance_body(const QueueDev& q, int k) {
          * writes them into the curr and next fronts once the previous
          * step's eigenray construction no longer reads those fronts */
         const int32_t w = __ldg(q.shadow_slot[set] + i);
+        WQ_CHECKED_OR(q, w >= 0 && w < q.n, return);
         sh = q.shadow[set] + (size_t)w * stride;
         ray_from(sh, y0);
         ray_from(sh + 17, y1);
@@ -1216,6 +1221,7 @@ __global__ void __launch_bounds__(128) k_commit(__grid_constant__ const QueueDev
          * the reflected prev state from the slot) but is the "past" front
          * a caller may look at after the step */
         const int32_t w = q.shadow_slot[set][i];
+        WQ_CHECKED_OR(q, w >= 0 && w < q.n, return);
         const double* sh = q.shadow[set] + (size_t)w * shadow_stride(q);
         const int32_t* cnt = q.shadow_cnt[set] + 3 * (size_t)w;
         RayS y;
@@ -1407,8 +1413,10 @@ __device__ __noinline__ void cpa_finish(const QueueDev& q, int64_t s, const Fron
     const uint32_t v = e[lane];
     const int j = (int)(v & 0xffffu);
     const int th = (int)(v >> 16);
+    WQ_CHECKED_OR(q, j < CPA_F32_TARGETS && th < CPA_THREADS, return);
     const int de = de0 + th / CPA_PATCH_AZ, az = az0 + th % CPA_PATCH_AZ;
     const int i = de * q.naz + az;
+    WQ_CHECKED_OR(q, de < q.nde && az < q.naz, return);
     const TgtS t = tile[j];
     const double center = d2_at(C, i, t);
     if (d2_at(X, i, t) <= center) return;
