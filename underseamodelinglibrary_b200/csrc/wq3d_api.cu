@@ -204,13 +204,12 @@ int make_grid(wq3d_ocean* o, const wq3d_grid_desc& d, int max_dims, GridDev* hg,
 }  // namespace
 
 /* The reflection-schedule plan learnt per queue shape (fan, targets,
- * frequencies, kernel build, precision, chunk length, sensitivities,
- * adjoint), shared by every queue of the process.  A run is cut into
- * buckets of TUNE_BUCKET steps, since which schedule wins changes as the
- * fan spreads and meets the boundaries; per bucket and schedule the plan
- * keeps the device time of the full chunks measured there.  A bucket's
- * first two chunks try each schedule once; after that the faster one runs
- * and its chunks keep refining the mean. */
+ * frequencies, kernel build, chunk length), shared by every queue of the
+ * process.  A run is cut into buckets of TUNE_BUCKET steps, since which
+ * schedule wins changes as the fan spreads and meets the boundaries.  The
+ * first two full chunks that reach a bucket try one schedule each and
+ * their device times are kept; every later chunk in that bucket, of this
+ * queue or a later one of the same shape, runs the faster. */
 constexpr int TUNE_BUCKET = 128;
 struct TunePlan {
     std::string key;
@@ -239,20 +238,25 @@ TunePlan& tune_plan(const std::string& key, size_t bucket) {
     return *e;
 }
 
-/* the schedule of a full chunk in this bucket: 1 inline, 0 side */
-int tune_choose(const std::string& key, size_t bucket) {
+/* the schedule of a full chunk in this bucket (1 inline, 0 side), and in
+ * *trial whether the chunk is one of the bucket's two timed trials */
+int tune_choose(const std::string& key, size_t bucket, bool* trial) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     TunePlan& t = tune_plan(key, bucket);
     int m;
-    if (t.cnt[1][bucket] + t.pend[1][bucket] == 0)
+    *trial = false;
+    if (t.cnt[1][bucket] + t.pend[1][bucket] == 0) {
         m = 1;
-    else if (t.cnt[0][bucket] + t.pend[0][bucket] == 0)
+        *trial = true;
+    } else if (t.cnt[0][bucket] + t.pend[0][bucket] == 0) {
         m = 0;
-    else if (t.cnt[0][bucket] == 0 || t.cnt[1][bucket] == 0)
+        *trial = true;
+    } else if (t.cnt[0][bucket] == 0 || t.cnt[1][bucket] == 0) {
         m = t.cnt[0][bucket] == 0 ? 1 : 0; /* the measured one until both are */
-    else
-        m = t.ms[1][bucket] / t.cnt[1][bucket] < t.ms[0][bucket] / t.cnt[0][bucket] ? 1 : 0;
-    t.pend[m][bucket] += 1;
+    } else {
+        m = t.ms[1][bucket] < t.ms[0][bucket] ? 1 : 0;
+    }
+    if (*trial) t.pend[m][bucket] += 1;
     return m;
 }
 
@@ -313,12 +317,12 @@ struct wq3d_queue {
     /* Reflection schedule (wq3d_queue_set_reflect_schedule).  Under
      * WQ3D_REFLECT_AUTO a queue run alone follows its shape's plan
      * (tune_choose) for every full chunk but a run's first, and times the
-     * chunk to refine the plan.  Both schedules give the same results bit
-     * for bit. */
+     * plan's trial chunks.  Both schedules give the same results bit for
+     * bit. */
     int refl_sched = WQ3D_REFLECT_AUTO;
     int last_inl = -1;             /* schedule of the last chunk launched */
     bool in_batch = false;         /* queues of a batch use the side stream */
-    bool chunk_trial[2] = {false, false}; /* per result set: the chunk in flight is timed */
+    bool chunk_trial[2] = {false, false}; /* per result set: the chunk in flight is a timed trial */
     int chunk_inl[2] = {0, 0};            /* its schedule */
     size_t chunk_bucket[2] = {0, 0};      /* and its bucket */
     cudaEvent_t tune_ev[2][2] = {};
@@ -735,11 +739,13 @@ struct wq3d_queue {
         return WQ3D_OK;
     }
 
-    /* the shape a tuned reflection schedule applies to */
+    /* the shape a tuned reflection schedule applies to: the fan, targets,
+     * frequencies, kernel build and chunk length (the arithmetic form,
+     * sensitivities and adjoint recording change the CPA and eigenray work
+     * beside the chain, not the chain itself, so they share a plan) */
     std::string tune_key() const {
         return std::to_string(h.nde) + "x" + std::to_string(h.naz) + " t" + std::to_string(h.nt) + " f" +
-               std::to_string(h.nf) + (gridded ? " g" : " a") + " p" + std::to_string(h.precision) + " c" +
-               std::to_string(chunk) + " s" + std::to_string(h.sens) + " j" + std::to_string(h.adj ? 1 : 0);
+               std::to_string(h.nf) + (gridded ? " g" : " a") + " c" + std::to_string(chunk);
     }
 
     int build_graph(int p, bool tail, bool inl) {
@@ -891,8 +897,7 @@ struct wq3d_queue {
                 /* not a run's first chunk, whose start-up reflections are
                  * not typical */
                 bucket = (size_t)(lsteps / TUNE_BUCKET);
-                inl = tune_choose(tune_key(), bucket) != 0;
-                trial = true;
+                inl = tune_choose(tune_key(), bucket, &trial) != 0;
             } else if (refl_sched == WQ3D_REFLECT_AUTO && !in_batch) {
                 inl = last_inl > 0;
             }
