@@ -586,7 +586,8 @@ int wq3d_queue_set_timing(wq3d_queue* q, int on);
  *                        the first queue of a shape tries both schedules
  *                        on one chunk of each bucket, every later chunk and
  *                        queue of that shape takes the faster.  Queues run
- *                        by wq3d_batch_run use the side stream.
+ *                        by wq3d_batch_run and queues recording for the
+ *                        adjoint use the side stream.
  * No reference counterpart (the reference reflects inside its step). */
 enum { WQ3D_REFLECT_AUTO = 0, WQ3D_REFLECT_SIDE = 1, WQ3D_REFLECT_INLINE = 2 };
 int wq3d_queue_set_reflect_schedule(wq3d_queue* q, int schedule);

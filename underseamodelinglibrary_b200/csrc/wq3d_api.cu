@@ -321,7 +321,8 @@ struct wq3d_queue {
      * bit. */
     int refl_sched = WQ3D_REFLECT_AUTO;
     int last_inl = -1;             /* schedule of the last chunk launched */
-    bool in_batch = false;         /* queues of a batch use the side stream */
+    bool in_batch = false;         /* queues of a batch use the side stream, as do
+                                    * queues recording for the adjoint */
     bool chunk_trial[2] = {false, false}; /* per result set: the chunk in flight is a timed trial */
     int chunk_inl[2] = {0, 0};            /* its schedule */
     size_t chunk_bucket[2] = {0, 0};      /* and its bucket */
@@ -893,12 +894,12 @@ struct wq3d_queue {
         if (can_inline) {
             if (refl_sched == WQ3D_REFLECT_INLINE) {
                 inl = true;
-            } else if (refl_sched == WQ3D_REFLECT_AUTO && !in_batch && K == chunk && lsteps > 0) {
+            } else if (refl_sched == WQ3D_REFLECT_AUTO && !in_batch && !h.adj && K == chunk && lsteps > 0) {
                 /* not a run's first chunk, whose start-up reflections are
                  * not typical */
                 bucket = (size_t)(lsteps / TUNE_BUCKET);
                 inl = tune_choose(tune_key(), bucket, &trial) != 0;
-            } else if (refl_sched == WQ3D_REFLECT_AUTO && !in_batch) {
+            } else if (refl_sched == WQ3D_REFLECT_AUTO && !in_batch && !h.adj) {
                 inl = last_inl > 0;
             }
         }
