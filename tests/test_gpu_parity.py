@@ -358,6 +358,40 @@ def test_listener_order_and_collection(engine):
         assert coll.total(t, 0).intensity[0] > 0.0
 
 
+def test_collection_takes_whole_lists(engine):
+    """An eigenray_collection alone on a queue receives each call's
+    eigenrays as one list (no per-ray callback during the run); the same
+    collection behind a per-ray listener must end up holding the same
+    eigenrays, per target and in the same order, and the same sums."""
+    sc = S.linear_slope_rayleigh(num_de=181, num_az=19, n_range=8, n_depth=8, time_max=10.0)
+
+    class PerRay(u.eigenray_collection):
+        bulk_eigenrays = False
+
+    colls = []
+    for cls in (u.eigenray_collection, PerRay):
+        q = S.build_queue(sc, u.wave_queue)
+        c = cls(sc["freq"], sc["pos"], sc["targets"])
+        q.add_eigenray_listener(c)
+        q.run(sc["time_max"] / 2)
+        q.run(sc["time_max"])
+        assert len(q.take_eigenrays()) == 0
+        c.sum_eigenrays()
+        colls.append(c)
+    a, b = colls
+    assert a.num_eigenrays() == b.num_eigenrays() > 10
+    for t1 in range(a.size1()):
+        for t2 in range(a.size2()):
+            ra, rb = a.eigenrays(t1, t2), b.eigenrays(t1, t2)
+            assert [key(r) for r in ra] == [key(r) for r in rb]
+            for x, y in zip(ra, rb):
+                assert x.travel_time == y.travel_time
+                assert np.array_equal(x.intensity, y.intensity) and np.array_equal(x.phase, y.phase)
+            if ra:
+                assert a.initial_time(t1, t2) == b.initial_time(t1, t2)
+                assert np.array_equal(a.total(t1, t2).intensity, b.total(t1, t2).intensity)
+
+
 def test_chunking_and_timing_mode_are_bit_identical(engine):
     """one step at a time, graph-replayed chunks and event-timed direct
     launches give identical eigenrays and fronts"""

@@ -42,12 +42,22 @@ class eigenray_collection(eigenray_listener):
     def num_eigenrays(self):
         return self._num
 
+    # a wave_queue hands this listener each call's eigenrays as one list
+    # (add_eigenray_list) instead of calling add_eigenray once per ray
+    bulk_eigenrays = True
+
     def add_eigenray(self, t1, t2, ray, run_id=0):
         self._rays[t1][t2].append(ray)
         old = self._initial[t1][t2]
         if old <= 0.0 or old > ray.travel_time:
             self._initial[t1][t2] = ray.travel_time
         self._num += 1
+
+    def add_eigenray_list(self, rays):
+        """add_eigenray for every ray of an eigenray_list, in its order (the
+        reference's delivery order), each to its own target"""
+        for ray in rays:
+            self.add_eigenray(ray.t1, ray.t2, ray)
 
     def eigenrays(self, t1, t2):
         return list(self._rays[t1][t2])

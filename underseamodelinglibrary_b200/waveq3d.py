@@ -346,8 +346,15 @@ class wave_queue:
         if not self._eig_listeners and not self._refl_listeners and not self._verb_listeners:
             _abi.check(self._lib, self._lib.wq3d_queue_set_callbacks(self._q, None, None))
             self._cb = None
+            self._bulk_listeners = []
             return
         freq = self._freq
+        # listeners that take a whole list at once (eigenray_collection) get
+        # it after each step() / run() call instead of one callback per ray,
+        # unless a per-ray listener is registered too
+        per_ray = [l for l in self._eig_listeners if not getattr(l, "bulk_eigenrays", False)]
+        self._bulk_listeners = [] if per_ray else list(self._eig_listeners)
+        want_rays = bool(per_ray)
 
         def add(ctx, t1, t2, rec, inten, phase, nf, run_id):
             r = eigenray_model.from_record(rec.contents, inten[:nf], phase[:nf], freq)
@@ -371,9 +378,13 @@ class wave_queue:
             for l in self._verb_listeners:
                 l.add_eigenverb(v, interface_num)
 
+        if not want_rays and not self._refl_listeners and not self._verb_listeners:
+            _abi.check(self._lib, self._lib.wq3d_queue_set_callbacks(self._q, None, None))
+            self._cb = None
+            return
         cb = _abi.wq3d_callbacks()
-        cb.add_eigenray = _abi.ADD_EIGENRAY(add) if self._eig_listeners else _abi.ADD_EIGENRAY()
-        cb.check_eigenrays = _abi.CHECK_EIGENRAYS(check) if self._eig_listeners else _abi.CHECK_EIGENRAYS()
+        cb.add_eigenray = _abi.ADD_EIGENRAY(add) if want_rays else _abi.ADD_EIGENRAY()
+        cb.check_eigenrays = _abi.CHECK_EIGENRAYS(check) if want_rays else _abi.CHECK_EIGENRAYS()
         cb.reflect = _abi.REFLECT(reflect) if self._refl_listeners else _abi.REFLECT()
         cb.add_eigenverb = _abi.ADD_EIGENVERB(verb) if self._verb_listeners else _abi.ADD_EIGENVERB()
         self._cb = cb
@@ -411,14 +422,28 @@ class wave_queue:
         self._install_callbacks()
 
     # ---------------- propagation ----------------
+    def _deliver_bulk(self):
+        """hands the eigenrays of the last call to the list-taking listeners"""
+        if getattr(self, "_bulk_listeners", None):
+            rays = self.take_eigenrays()
+            if len(rays):
+                for l in self._bulk_listeners:
+                    l.add_eigenray_list(rays)
+
     def step(self, nsteps=1):
         """wave_queue::step() (wave_queue.cc:155-192); nsteps > 1 runs several."""
-        _abi.check(self._lib, self._lib.wq3d_queue_step(self._q, int(nsteps)))
+        try:
+            _abi.check(self._lib, self._lib.wq3d_queue_step(self._q, int(nsteps)))
+        finally:
+            self._deliver_bulk()
 
     def run(self, time_max):
         """``while (time() < time_max) step();`` in one call."""
         n = C.c_size_t()
-        _abi.check(self._lib, self._lib.wq3d_queue_run(self._q, float(time_max), C.byref(n)))
+        try:
+            _abi.check(self._lib, self._lib.wq3d_queue_run(self._q, float(time_max), C.byref(n)))
+        finally:
+            self._deliver_bulk()
         return n.value
 
     def abort(self):
@@ -536,5 +561,9 @@ def run_batch(queues, time_max):
     steps = (C.c_size_t * n)()
     ms = C.c_double()
     lib = _abi.load_engine()
-    _abi.check(lib, lib.wq3d_batch_run(handles, n, _abi.as_dp(tm), steps, C.byref(ms)))
+    try:
+        _abi.check(lib, lib.wq3d_batch_run(handles, n, _abi.as_dp(tm), steps, C.byref(ms)))
+    finally:
+        for q in queues:
+            q._deliver_bulk()
     return [int(x) for x in steps], ms.value
