@@ -55,12 +55,34 @@ class eigenray_collection(eigenray_listener):
 
     def add_eigenray_list(self, rays):
         """add_eigenray for every ray of an eigenray_list, in its order (the
-        reference's delivery order), each to its own target"""
-        for ray in rays:
-            self.add_eigenray(ray.t1, ray.t2, ray)
+        reference's delivery order), each to its own target.  The rays stay
+        rows of the list's record arrays until they are read; a subclass
+        that overrides add_eigenray gets one call per ray."""
+        if type(self).add_eigenray is not eigenray_collection.add_eigenray:
+            for ray in rays:
+                self.add_eigenray(ray.t1, ray.t2, ray)
+            return
+        rec = rays.records
+        t1s, t2s, times = rec["t1"].tolist(), rec["t2"].tolist(), rec["time"].tolist()
+        for k in range(len(t1s)):
+            t1, t2, t = t1s[k], t2s[k], times[k]
+            self._rays[t1][t2].append((rays, k))
+            old = self._initial[t1][t2]
+            if old <= 0.0 or old > t:
+                self._initial[t1][t2] = t
+        self._num += len(t1s)
+
+    def _entries(self, t1, t2):
+        """the target's eigenrays, rows of added lists made into
+        eigenray_model objects on first read"""
+        lst = self._rays[t1][t2]
+        for k, e in enumerate(lst):
+            if isinstance(e, tuple):
+                lst[k] = e[0][e[1]]
+        return lst
 
     def eigenrays(self, t1, t2):
-        return list(self._rays[t1][t2])
+        return list(self._entries(t1, t2))
 
     def dead_reckon(self, t1, t2, source_new, target_new, profile):
         """eigenray_collection::dead_reckon (eigenray_collection.cc:361-368):
@@ -68,7 +90,7 @@ class eigenray_collection(eigenray_listener):
         to a new target position, by dead_reckon_one.  ``profile`` is the
         ocean_model (or profile_model) whose sound speed and attenuation are
         used."""
-        rays = dead_reckon_one(self._rays[t1][t2], self._source, source_new, profile)
+        rays = dead_reckon_one(self._entries(t1, t2), self._source, source_new, profile)
         old_target = wposition1()
         old_target.rho = float(self._targets.rho[t1, t2])
         old_target.theta = float(self._targets.theta[t1, t2])
@@ -99,7 +121,15 @@ class eigenray_collection(eigenray_listener):
         rec = (_abi.wq3d_eigenray * max(n, 1))()
         inten = np.zeros((max(n, 1), nf))
         phase = np.zeros((max(n, 1), nf))
+        # rows still held by their eigenray_list are copied list by list
+        recs = np.ctypeslib.as_array(rec)
+        groups = {}
         for k, (t1, t2, r) in enumerate(rays):
+            if isinstance(r, tuple):
+                g = groups.setdefault(id(r[0]), (r[0], [], []))
+                g[1].append(k)
+                g[2].append(r[1])
+                continue
             e = rec[k]
             e.time, e.source_de, e.source_az = r.travel_time, r.source_de, r.source_az
             e.target_de, e.target_az = r.target_de, r.target_az
@@ -107,6 +137,11 @@ class eigenray_collection(eigenray_listener):
             e.t1, e.t2 = t1, t2
             inten[k] = r.intensity
             phase[k] = r.phase
+        for lst, dst, rows in groups.values():
+            dst, rows = np.asarray(dst), np.asarray(rows)
+            recs[dst] = lst.records[rows]
+            inten[dst] = lst._inten[rows]
+            phase[dst] = lst._phase[rows]
         tot = (_abi.wq3d_eigenray * (n1 * n2))()
         ti = np.empty((n1 * n2, nf))
         tp = np.empty((n1 * n2, nf))
